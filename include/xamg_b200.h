@@ -1,0 +1,132 @@
+/* Extension and kernel-level entry points of libxamg_b200.so.
+ *
+ * Part 1 (XAMG_b200_*) extends the XAMG C API with what the reference exposes
+ * only through its C++ classes or its test driver: runtime NV, error text,
+ * residual histories, hierarchy export, generators and the binary system
+ * format.  Part 2 (xamg_*) is the device-pointer interface of the individual
+ * solve-phase kernels; each entry names the reference routine whose
+ * arithmetic it performs.  All pointers in part 2 are device pointers unless
+ * the name says host; `stream` is a cudaStream_t (NULL = the library stream).
+ * Precision codes: 0 = FP64, 1 = FP32.  nv must be one of 1, 2, 4, 8, 16, 32.
+ */
+#ifndef XAMG_B200_H_
+#define XAMG_B200_H_
+
+#include <stdint.h>
+#include <stddef.h>
+#include "xamg_c_api.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- Part 1: API extensions ------------------------------------------- */
+
+/* Set the right-hand-side width used by the NV-checked API calls
+ * (replaces the reference's compile-time XAMG_NV, xamg_c_api.cpp:56-60). */
+int XAMG_b200_set_nv(int nv);
+/* Text of the last error returned by any call of this library. */
+const char *XAMG_b200_last_error(void);
+/* Wait for all queued device work of the library. */
+int XAMG_b200_synchronize(void);
+/* Raw device pointer of a device-resident vector (FP64, size x nv). */
+void *XAMG_b200_vector_device_ptr(XAMG_vector_id vid);
+/* Convergence detail of the last solve: squared residual norms after each
+ * check (nv per entry, entry 0 = initial); returns the entry count. */
+int XAMG_b200_solver_get_residual_history(double *out, int cap, XAMG_solver_id sid);
+/* Squared initial residual norms (nv values) and per-column status. */
+int XAMG_b200_solver_get_res0(double *out, XAMG_solver_id sid);
+/* Device time of the last solve in milliseconds (CUDA events). */
+double XAMG_b200_solver_last_solve_ms(XAMG_solver_id sid);
+/* Multigrid hierarchy of a solver (levels from the host AMG setup). */
+int XAMG_b200_solver_num_levels(XAMG_solver_id sid);
+int XAMG_b200_solver_level_info(int64_t *info /* n, nnzA, ncolsP, nnzP, nlev_fwd, nlev_bwd */,
+                                int level, XAMG_solver_id sid);
+int XAMG_b200_solver_export_level(int *rpA, int *ciA, double *vA, int *rpP, int *ciP,
+                                  double *vP, int level, XAMG_solver_id sid);
+/* Gauss-Seidel wavefront levels of one level's pre-smoother (per row). */
+int XAMG_b200_solver_export_gs_levels(int *lf, int *lb, int level, XAMG_solver_id sid);
+/* Dense inverse of the coarsest operator (row-major n x n). */
+int XAMG_b200_solver_export_coarse_inverse(double *out, XAMG_solver_id sid);
+/* Human-readable description of the solver tree. */
+int XAMG_b200_solver_info(char *buf, int cap, XAMG_solver_id sid);
+
+/* Generators.  kind 0: reference cube (examples/common/generator/cube.inl),
+ * iargs = {nx, ny, nz, config}; kind 1: 27-point anisotropic, iargs = {n},
+ * dargs = {kx, ky, kz}; kind 2: 7-point from face coefficients, iargs =
+ * {nx, ny, nz}, faces = kx[(nx+1)ny nz] ky[nx(ny+1)nz] kz[nx ny(nz+1)]. */
+int XAMG_b200_csr_matrix_generate(int kind, const int64_t *iargs, const double *dargs,
+                                  const double *faces, XAMG_csr_matrix_id mcsrid);
+int64_t XAMG_b200_csr_matrix_get_nnz(XAMG_csr_matrix_id mcsrid);
+int XAMG_b200_csr_matrix_export(int *rp, int *ci, double *v, XAMG_csr_matrix_id mcsrid);
+/* Binary system file (examples/test/mtx_gen.cpp:116-146): matrix, then b and
+ * x if present.  b_out/x_out may be NULL (host arrays of nrows doubles). */
+int XAMG_b200_csr_matrix_read_bin(const char *path, double *b_out, double *x_out,
+                                  XAMG_csr_matrix_id mcsrid);
+int XAMG_b200_csr_matrix_write_bin(const char *path, const double *b, const double *x,
+                                   XAMG_csr_matrix_id mcsrid);
+
+/* Host-only AMG setup (the role of hypre BoomerAMG in hypre_base.h:121-217):
+ * builds the hierarchy of the MultiGrid role of pid on the host, without any
+ * device work.  info = {n, nnzA, ncolsP, nnzP}. */
+int XAMG_b200_amg_host_create(XAMG_csr_matrix_id cid, XAMG_param_id pid, size_t *hid);
+int XAMG_b200_amg_host_num_levels(size_t hid);
+int XAMG_b200_amg_host_level_info(int64_t *info, int level, size_t hid);
+int XAMG_b200_amg_host_export_level(int *rpA, int *ciA, double *vA, int *rpP, int *ciP,
+                                    double *vP, int level, size_t hid);
+int XAMG_b200_amg_host_destroy(size_t hid);
+/* Wavefront levels of the sequential (block_rows = 0) or hybrid Gauss-Seidel
+ * sweeps, computed on the host; nlev[2] = {forward, backward} level counts. */
+int XAMG_b200_gs_levels_host(int64_t n, const int *rp, const int *ci, int64_t block_rows,
+                             int *lf, int *lb, int *nlev);
+
+/* ---- Part 2: kernel-level device interface ----------------------------- */
+
+/* csr_Ax_y / csr_Axpy (blas2/detail/csr_matvec.inl:32-260):
+ * mode 0: y = A x; 1: y += A x; 2: y = b - A x. */
+int xamg_csr_spmv(int prec, int nv, int64_t n, const int *rp, const int *ci, const void *val,
+                  const void *x, void *y, int mode, const void *b, void *stream);
+
+/* Gauss-Seidel plan (wavefront schedule) for blas2::SGS / csr_SGS
+ * (blas2.h:184-281, csr_gs.inl:32-134).  rp/ci are HOST arrays.  block_rows
+ * = 0 gives the single-process sweep; > 0 the hybrid block semantics.
+ * persistent = 1 runs each sweep as one cooperative launch. */
+void *xamg_gs_plan_create(int64_t n, const int *rp_host, const int *ci_host,
+                          int64_t block_rows, int persistent);
+int xamg_gs_plan_levels(void *plan, int *nlev /* [2] */, int *lf, int *lb);
+int xamg_gs_plan_error(void *plan);
+void xamg_gs_plan_destroy(void *plan);
+/* One HSGS call: t = b - A_offblock x (when hybrid), forward then backward
+ * sweep updating x in place.  relax: nv values of the solver precision.
+ * t_scratch: n*nv elements (needed only when block_rows > 0). */
+int xamg_hsgs(void *plan, int prec, int nv, const int *rp, const int *ci, const void *val,
+              const void *invdiag, const void *b, void *x, const void *relax, void *t_scratch,
+              void *stream);
+
+/* Jacobi sweep (merged_jacobi, blas_merged_jacobi.inl:61-81): xo = xi +
+ * relax*invdiag*(b - A xi). */
+int xamg_jacobi(int prec, int nv, int64_t n, const int *rp, const int *ci, const void *val,
+                const void *invdiag, const void *b, const void *xi, void *xo,
+                const void *relax, void *stream);
+
+/* Inner products (blas::dot, blas.inl:521-589) of nd pairs, FP64 results
+ * out[d*nv + k]; part: xamg_dot_part_size(n, nd, nv) doubles of scratch. */
+int64_t xamg_dot_part_size(int64_t n, int nd, int nv);
+int xamg_dot(int prec, int nv, int64_t n, int nd, const void *const *a, const void *const *b,
+             double *part, double *out, void *stream);
+
+/* Block-vector BLAS-1 (blas.inl, blas_ext.inl) with FP64 per-column scalars:
+ * op 0 z=a*x+b*y, 1 z=a*x+b*y+c*z, 2 z=a*x, 3 z=x, 4 z=a, 5 z=z*x. */
+int xamg_blas(int prec, int nv, int64_t n, int op, const double *a, const void *x,
+              const double *b, const void *y, const double *c, void *z, void *stream);
+
+/* Dense coarse solve y = Ainv b (Direct, dense_matvec.inl:71-121) with the
+ * inverse stored transposed (AinvT[j*n + i] = Ainv[i][j]). */
+int xamg_dense_gemv(int prec, int nv, int n, const void *AinvT, const void *b, void *y,
+                    void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XAMG_B200_H_ */

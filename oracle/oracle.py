@@ -1,0 +1,201 @@
+"""ctypes loader of the CPU oracle (liboracle.so) — test infrastructure only.
+
+Only the tests, the smoke check and the CPU-baseline leg of bench.py use this
+module, always as the checker; the product library never imports it.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PATH = os.path.join(HERE, "liboracle.so")
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(PATH):
+            import subprocess
+            import sys
+            subprocess.check_call([sys.executable, os.path.join(os.path.dirname(HERE), "xamg-test_b200", "build.py")])
+        L = C.CDLL(PATH)
+        P = C.c_void_p
+        i64 = C.c_int64
+        sig = {
+            "orc_spmv_d": (None, [i64, P, P, P, P, P, C.c_int, C.c_int]),
+            "orc_spmv_f": (None, [i64, P, P, P, P, P, C.c_int, C.c_int]),
+            "orc_hsgs_d": (None, [i64, P, P, P, P, P, P, P, C.c_int, C.c_int, P]),
+            "orc_hsgs_f": (None, [i64, P, P, P, P, P, P, P, C.c_int, C.c_int, P]),
+            "orc_jacobi_d": (None, [i64, P, P, P, P, P, P, P, P, C.c_int]),
+            "orc_jacobi_f": (None, [i64, P, P, P, P, P, P, P, P, C.c_int]),
+            "orc_dot_d": (None, [i64, C.c_int, P, P, P]),
+            "orc_dot_fd": (None, [i64, C.c_int, P, P, P]),
+            "orc_dot_seq_d": (None, [i64, C.c_int, P, P, P]),
+            "orc_dense_inverse": (None, [C.c_int, P, P]),
+            "orc_dense_gemv_d": (None, [C.c_int, P, P, P, C.c_int]),
+            "orc_dense_gemv_f": (None, [C.c_int, P, P, P, C.c_int]),
+            "orc_transpose": (None, [i64, i64, P, P, P, P, P, P]),
+            "orc_gs_levels": (None, [i64, P, P, P, P]),
+            "orc_mg_create": (P, [C.c_int]),
+            "orc_mg_destroy": (None, [P]),
+            "orc_mg_set_A": (None, [P, C.c_int, i64, P, P, P]),
+            "orc_mg_set_P": (None, [P, C.c_int, i64, i64, P, P, P]),
+            "orc_mg_set_blocks": (None, [P, C.c_int, C.c_int, P]),
+            "orc_mg_set_smoothers": (None, [P, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_double]),
+            "orc_mg_finalize": (None, [P, C.c_int]),
+            "orc_mg_get_coarse_inverse": (None, [P, P]),
+            "orc_mg_get_R": (None, [P, C.c_int, P, P, P]),
+            "orc_mg_apply_d": (None, [P, P, P, C.c_int]),
+            "orc_mg_apply_f": (None, [P, P, P, C.c_int]),
+            "orc_pbicgstab_d": (C.c_int, [i64, P, P, P, P, P, P, C.c_int, C.c_int, C.c_double, C.c_double, P, C.c_int, P, P]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def spmv(rp, ci, v, x, nv, y=None, acc=False):
+    n = len(rp) - 1
+    f = lib().orc_spmv_d if v.dtype == np.float64 else lib().orc_spmv_f
+    y = np.zeros((n, nv), dtype=v.dtype) if y is None else y
+    f(n, p(rp), p(ci), p(v), p(x), p(y), nv, int(acc))
+    return y
+
+
+def dot(x, y):
+    n, nv = x.shape
+    out = np.zeros(nv)
+    if x.dtype == np.float64:
+        lib().orc_dot_d(n, nv, p(x), p(y), p(out))
+    else:
+        lib().orc_dot_fd(n, nv, p(x), p(y), p(out))
+    return out
+
+
+def dot_sequential(x, y):
+    n, nv = x.shape
+    out = np.zeros(nv)
+    lib().orc_dot_seq_d(n, nv, p(x), p(y), p(out))
+    return out
+
+
+def hsgs(rp, ci, v, invd, b, x, relax, block_rows=0):
+    n, nv = b.shape
+    if block_rows and block_rows < n:
+        bp = np.arange(0, n, block_rows, dtype=np.int64)
+        bp = np.append(bp, n).astype(np.int64)
+    else:
+        bp = np.array([0, n], dtype=np.int64)
+    f = lib().orc_hsgs_d if v.dtype == np.float64 else lib().orc_hsgs_f
+    f(n, p(rp), p(ci), p(v), p(invd), p(b), p(x), p(relax), nv, len(bp) - 1, p(bp))
+    return x
+
+
+def jacobi(rp, ci, v, invd, b, x, relax):
+    n, nv = b.shape
+    r = np.zeros_like(b)
+    f = lib().orc_jacobi_d if v.dtype == np.float64 else lib().orc_jacobi_f
+    f(n, p(rp), p(ci), p(v), p(invd), p(b), p(x), p(r), p(relax), nv)
+    return x
+
+
+def dense_inverse(A):
+    n = A.shape[0]
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    out = np.zeros_like(A)
+    lib().orc_dense_inverse(n, p(A), p(out))
+    return out
+
+
+def dense_gemv(Ainv, b):
+    n = Ainv.shape[0]
+    nv = b.shape[1]
+    y = np.zeros_like(b)
+    f = lib().orc_dense_gemv_d if b.dtype == np.float64 else lib().orc_dense_gemv_f
+    f(n, p(np.ascontiguousarray(Ainv, dtype=b.dtype)), p(b), p(y), nv)
+    return y
+
+
+def gs_levels(rp, ci):
+    n = len(rp) - 1
+    lf = np.zeros(n, np.int32)
+    lb = np.zeros(n, np.int32)
+    lib().orc_gs_levels(n, p(rp), p(ci), p(lf), p(lb))
+    return lf, lb
+
+
+def transpose(rp, ci, v, ncols):
+    n = len(rp) - 1
+    rrp = np.zeros(ncols + 1, np.int32)
+    rci = np.zeros(len(ci), np.int32)
+    rv = np.zeros(len(ci))
+    lib().orc_transpose(n, ncols, p(rp), p(ci), p(v), p(rrp), p(rci), p(rv))
+    return rrp, rci, rv
+
+
+SM_JACOBI, SM_HSGS = 0, 1
+
+
+class MG:
+    """Oracle multigrid hierarchy (levels exported from the product's setup)."""
+
+    def __init__(self, levels, fp32=False, pre=(SM_HSGS, 1, 0.99), post=(SM_HSGS, 1, 0.99), block_rows=None):
+        self.h = lib().orc_mg_create(len(levels))
+        self.keep = []
+        for l, lv in enumerate(levels):
+            rp, ci, v = lv["A"]
+            n = len(rp) - 1
+            lib().orc_mg_set_A(self.h, l, n, p(rp), p(ci), p(v))
+            if lv.get("P") is not None:
+                prp, pci, pv = lv["P"]
+                lib().orc_mg_set_P(self.h, l, n, lv["ncP"], p(prp), p(pci), p(pv))
+            br = (block_rows[l] if isinstance(block_rows, (list, tuple)) else block_rows) if block_rows else 0
+            if br and br < n:
+                bp = np.append(np.arange(0, n, br, dtype=np.int64), n).astype(np.int64)
+                self.keep.append(bp)
+                lib().orc_mg_set_blocks(self.h, l, len(bp) - 1, p(bp))
+            self.keep.append(lv)
+        lib().orc_mg_set_smoothers(self.h, pre[0], pre[1], pre[2], post[0], post[1], post[2])
+        lib().orc_mg_finalize(self.h, int(fp32))
+        self.nc = len(levels[-1]["A"][0]) - 1
+
+    def coarse_inverse(self):
+        out = np.zeros((self.nc, self.nc))
+        lib().orc_mg_get_coarse_inverse(self.h, p(out))
+        return out
+
+    def apply(self, b):
+        x = np.zeros_like(b)
+        if b.dtype == np.float64:
+            lib().orc_mg_apply_d(self.h, p(b), p(x), b.shape[1])
+        else:
+            lib().orc_mg_apply_f(self.h, p(b), p(x), b.shape[1])
+        return x
+
+    def __del__(self):
+        try:
+            lib().orc_mg_destroy(self.h)
+        except Exception:
+            pass
+
+
+def pbicgstab(rp, ci, v, b, x0, mg=None, max_iters=1000, abs_tol=0.0, rel_tol=1e-8):
+    """FP64 (P)BiCGStab; returns (x, iters, history[iters+1, nv], status, res0)."""
+    n, nv = b.shape
+    x = np.array(x0, dtype=np.float64, copy=True)
+    cap = max_iters + 2
+    hist = np.zeros((cap, nv))
+    status = np.zeros(nv, np.int32)
+    res0 = np.zeros(nv)
+    it = lib().orc_pbicgstab_d(n, p(rp), p(ci), p(v), mg.h if mg is not None else None, p(b), p(x), nv,
+                               max_iters, abs_tol, rel_tol, p(hist), cap, p(status), p(res0))
+    return x, it, hist[: it + 1], status, res0

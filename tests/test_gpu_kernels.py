@@ -1,0 +1,189 @@
+"""Kernel-level parity through the C ABI: every result is compared with the CPU
+oracle bit for bit (same operation order, same rounding)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle as orc
+import util
+import xamg
+
+pytestmark = pytest.mark.gpu
+
+NVS = [1, 2, 4, 8, 16, 32]
+
+
+def D(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def P(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def sync():
+    import torch
+    torch.cuda.synchronize()
+    xamg.check(xamg.lib().XAMG_b200_synchronize())
+    torch.cuda.synchronize()
+
+
+def H(t):
+    sync()
+    return t.cpu().numpy()
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("nv", NVS)
+def test_spmv_bit_exact(gpu, dtype, nv):
+    rng = np.random.default_rng(nv)
+    n, ncols = 1500, 1300
+    rp, ci, v = util.random_csr(n, ncols, rng, max_nnz=30, empty_rows=(0, 5, 1499))
+    v = v.astype(dtype)
+    x = rng.uniform(-1, 1, (ncols, nv)).astype(dtype)
+    y0 = rng.uniform(-1, 1, (n, nv)).astype(dtype)
+    b = rng.uniform(-1, 1, (n, nv)).astype(dtype)
+    prec = 0 if dtype == np.float64 else 1
+    drp, dci, dv, dx, db = D(rp), D(ci), D(v), D(x), D(b)
+    L = xamg.lib()
+    for mode in (0, 1, 2):
+        dy = D(y0)
+        sync()
+        xamg.check(L.xamg_csr_spmv(prec, nv, n, P(drp), P(dci), P(dv), P(dx), P(dy), mode, P(db), None))
+        got = H(dy)
+        if mode == 0:
+            ref = orc.spmv(rp, ci, v, x, nv)
+        elif mode == 1:
+            ref = orc.spmv(rp, ci, v, x, nv, y=y0.copy(), acc=True)
+        else:
+            ref = orc.spmv(rp, ci, v, x, nv)
+            ref = (dtype(1) * b + dtype(-1) * ref).astype(dtype)
+        assert np.array_equal(got, ref), (mode, np.abs(got - ref).max())
+
+
+def test_spmv_large_checksum(gpu):
+    """Full-size product through a size-independent property: y = A x for
+    x = e_k columns reproduces the CSR columns, checked by a bxor-style
+    checksum of the result bits (tst_spmv.h:63-91)."""
+    m = xamg.CsrMatrix.aniso27(64)
+    rp, ci, v = m.arrays()
+    n = m.nrows
+    nv = 16
+    rng = np.random.default_rng(5)
+    x = rng.uniform(-1, 1, (n, nv))
+    dy = D(np.zeros((n, nv)))
+    L = xamg.lib()
+    xamg.check(L.xamg_csr_spmv(0, nv, n, P(D(rp)), P(D(ci)), P(D(v)), P(D(x)), P(dy), 0, None, None))
+    got = H(dy)
+    ref = orc.spmv(rp, ci, v, x, nv)
+    xor = np.bitwise_xor.reduce(got.view(np.uint64), axis=0)
+    xref = np.bitwise_xor.reduce(ref.view(np.uint64), axis=0)
+    assert np.array_equal(xor, xref)
+
+
+@pytest.mark.parametrize("nv", NVS)
+@pytest.mark.parametrize("n", [1, 200, 256, 257, 70001])
+def test_dot_bit_exact(gpu, nv, n):
+    rng = np.random.default_rng(n + nv)
+    L = xamg.lib()
+    for dtype, prec in ((np.float64, 0), (np.float32, 1)):
+        vs = [rng.uniform(-1, 1, (n, nv)).astype(dtype) for _ in range(3)]
+        dvs = [D(a) for a in vs]
+        pairs = [(0, 1), (1, 1), (2, 0)]
+        A = (C.c_void_p * 3)(*[P(dvs[i]) for i, _ in pairs])
+        B = (C.c_void_p * 3)(*[P(dvs[j]) for _, j in pairs])
+        part = D(np.zeros(max(L.xamg_dot_part_size(n, 3, nv), 1)))
+        out = D(np.zeros(3 * nv))
+        xamg.check(L.xamg_dot(prec, nv, n, 3, A, B, P(part), P(out), None))
+        got = H(out).reshape(3, nv)
+        for d, (i, j) in enumerate(pairs):
+            assert np.array_equal(got[d], orc.dot(vs[i], vs[j])), (d, dtype)
+
+
+@pytest.mark.parametrize("nv", [1, 4, 16, 32])
+def test_blas_bit_exact(gpu, nv):
+    rng = np.random.default_rng(11)
+    n = 3001
+    L = xamg.lib()
+    a, b, c = (rng.uniform(-2, 2, nv) for _ in range(3))
+    da, db, dc = D(a), D(b), D(c)
+    for dtype, prec in ((np.float64, 0), (np.float32, 1)):
+        x, y, z = (rng.uniform(-1, 1, (n, nv)).astype(dtype) for _ in range(3))
+        x64, y64, z64 = (q.astype(np.float64) for q in (x, y, z))
+        refs = {
+            0: a * x64 + b * y64,
+            1: (a * x64 + b * y64) + c * z64,
+            2: a * x64,
+            3: x64,
+            4: np.broadcast_to(a, (n, nv)),
+            5: z64 * x64,
+        }
+        for op, ref in refs.items():
+            dz = D(z)
+            xamg.check(L.xamg_blas(prec, nv, n, op, P(da), P(D(x)), P(db), P(D(y)), P(dc), P(dz), None))
+            assert np.array_equal(H(dz), ref.astype(dtype)), (op, dtype)
+
+
+def _gs_case(rng, kind, n=500):
+    if kind == "dd":
+        return util.dd_csr(n, rng)
+    m = xamg.CsrMatrix.aniso27(9)
+    return m.arrays()
+
+
+@pytest.mark.parametrize("kind", ["dd", "27pt"])
+@pytest.mark.parametrize("block_rows", [0, 64])
+@pytest.mark.parametrize("persistent", [1, 0])
+@pytest.mark.parametrize("nv", [1, 4, 16])
+def test_hsgs_bit_exact(gpu, kind, block_rows, persistent, nv):
+    rng = np.random.default_rng(21)
+    rp, ci, v = _gs_case(rng, kind)
+    n = len(rp) - 1
+    L = xamg.lib()
+    plan = L.xamg_gs_plan_create(n, xamg._ptr(rp), xamg._ptr(ci), block_rows, persistent)
+    assert plan
+    try:
+        for dtype, prec in ((np.float64, 0), (np.float32, 1)):
+            vv = v.astype(dtype)
+            invd = np.zeros(n, dtype)
+            for i in range(n):
+                for j in range(rp[i], rp[i + 1]):
+                    if ci[j] == i:
+                        invd[i] = dtype(1.0 / np.float64(vv[j]))
+            b = rng.uniform(-1, 1, (n, nv)).astype(dtype)
+            x0 = rng.uniform(-1, 1, (n, nv)).astype(dtype)
+            relax = np.full(nv, 0.99, dtype)
+            dx = D(x0)
+            t = D(np.zeros((n, nv), dtype))
+            xamg.check(L.xamg_hsgs(plan, prec, nv, P(D(rp)), P(D(ci)), P(D(vv)), P(D(invd)), P(D(b)),
+                                   P(dx), P(D(relax)), P(t), None))
+            got = H(dx)
+            ref = orc.hsgs(rp, ci, vv, invd, b, x0.copy(), relax, block_rows=block_rows)
+            assert np.array_equal(got, ref), (dtype, np.abs(got - ref).max())
+        assert L.xamg_gs_plan_error(plan) == 0
+    finally:
+        L.xamg_gs_plan_destroy(plan)
+
+
+@pytest.mark.parametrize("nv", [1, 8, 32])
+def test_jacobi_and_dense_bit_exact(gpu, nv):
+    rng = np.random.default_rng(31)
+    rp, ci, v = util.dd_csr(700, rng)
+    n = 700
+    L = xamg.lib()
+    invd = np.array([1.0 / v[rp[i]] for i in range(n)])
+    b = rng.uniform(-1, 1, (n, nv))
+    x0 = rng.uniform(-1, 1, (n, nv))
+    relax = np.full(nv, 0.99)
+    dxo = D(np.zeros((n, nv)))
+    xamg.check(L.xamg_jacobi(0, nv, n, P(D(rp)), P(D(ci)), P(D(v)), P(D(invd)), P(D(b)), P(D(x0)), P(dxo), P(D(relax)), None))
+    ref = orc.jacobi(rp, ci, v, invd, b, x0.copy(), relax)
+    assert np.array_equal(H(dxo), ref)
+    nc = 123
+    Ai = rng.uniform(-1, 1, (nc, nc))
+    bb = rng.uniform(-1, 1, (nc, nv))
+    dy = D(np.zeros((nc, nv)))
+    xamg.check(L.xamg_dense_gemv(0, nv, nc, P(D(np.ascontiguousarray(Ai.T))), P(D(bb)), P(dy), None))
+    assert np.array_equal(H(dy), orc.dense_gemv(Ai, bb))

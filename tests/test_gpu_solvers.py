@@ -1,0 +1,147 @@
+"""Solver-level parity: the GPU solve through the XAMG C API against the CPU
+oracle on the same inputs and the same (exported) multigrid hierarchy.  In
+plain FP64 the iteration counts and residual histories must be identical; the
+tolerance written into each assertion is 1e-12 relative, and the runs are in
+fact bit-identical."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as orc
+import util
+import xamg
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def solve_api(csr, spec, B, X0=None):
+    n, nv = B.shape
+    xamg.set_nv(nv)
+    A = xamg.Matrix(csr)
+    x = xamg.Vector(n, nv)
+    b = xamg.Vector(n, nv)
+    x.upload(np.zeros((n, nv)) if X0 is None else X0)
+    b.upload(B)
+    s = xamg.Solver(A, xamg.Params(spec), x, b)
+    s.solve()
+    return s, x.download(), (A, x, b)
+
+
+def oracle_mg(s, spec):
+    levels = [s.level(l) for l in range(s.num_levels())]
+    sm = spec.get("pre_smoother", {})
+    kind = orc.SM_HSGS if sm.get("method", "HSGS") == "HSGS" else orc.SM_JACOBI
+    it = sm.get("max_iters", 1)
+    br = sm.get("hybrid_block_rows", 0)
+    return orc.MG(levels, pre=(kind, it, 0.99), post=(kind, it, 0.99), block_rows=br)
+
+
+def assert_same_history(h_gpu, h_orc):
+    assert h_gpu.shape == h_orc.shape, (h_gpu.shape, h_orc.shape)
+    np.testing.assert_allclose(h_gpu, h_orc, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("nv", [1, 4])
+def test_bicgstab_c1_parity(gpu, nv):
+    # 7-point Poisson (cube generator config 0), BiCGStab to 1e-8 rel.
+    csr = xamg.CsrMatrix.cube(32, 32, 32, 0)
+    rp, ci, v = csr.arrays()
+    rng = np.random.default_rng(1234)
+    B = rng.uniform(-1, 1, (csr.nrows, nv))
+    spec = util.amg_params(precond_mg=False, max_iters=1000)
+    s, X, keep = solve_api(csr, spec, B)
+    xo, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), None, 1000, 0.0, 1e-8)
+    assert s.iters()[0] == it
+    assert_same_history(s.history(), hist)
+    np.testing.assert_allclose(X, xo, rtol=1e-12, atol=1e-14 * np.abs(xo).max())
+    assert all(s.converged())
+
+
+@pytest.mark.parametrize("smoother,block_rows", [("HSGS", 0), ("HSGS", 512), ("Jacobi", 0)])
+def test_pbicgstab_amg_parity(gpu, smoother, block_rows):
+    csr = xamg.CsrMatrix.aniso27(24)
+    rp, ci, v = csr.arrays()
+    rng = np.random.default_rng(77)
+    B = rng.uniform(-1, 1, (csr.nrows, 4))
+    spec = util.amg_params(max_levels=6, smoother=smoother, sweeps=1 if smoother == "HSGS" else 2,
+                           block_rows=block_rows)
+    s, X, keep = solve_api(csr, spec, B)
+    mg = oracle_mg(s, spec)
+    xo, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg, 200, 0.0, 1e-8)
+    assert s.iters()[0] == it and it > 0
+    assert_same_history(s.history(), hist)
+    np.testing.assert_allclose(X, xo, rtol=1e-12, atol=1e-14 * np.abs(xo).max())
+    # bit-exact indexing: GS wavefront levels and coarse inverse agree with the oracle
+    if smoother == "HSGS" and block_rows == 0:
+        lf, lb = s.gs_levels(0)
+        of, ob = orc.gs_levels(rp, ci)
+        assert np.array_equal(lf, of) and np.array_equal(lb, ob)
+    assert np.array_equal(s.coarse_inverse(), mg.coarse_inverse())
+
+
+def test_recorded_2d_problem_through_api(gpu):
+    rec = json.load(open(os.path.join(GOLD, "recorded.json")))
+    rp, ci, v, b, u = util.gen2d(100)
+    csr = xamg.CsrMatrix.from_arrays(rp, ci, v)
+    spec = util.amg_params(max_levels=25)
+    s, X, keep = solve_api(csr, spec, b.reshape(-1, 1))
+    h = s.history()
+    assert np.sqrt(h[0, 0]) == pytest.approx(rec["initial_residual"], rel=4e-15)
+    assert abs(np.linalg.norm(X) - rec["X_norm"]) / rec["X_norm"] < 1e-7
+    assert np.linalg.norm(X[:, 0] - u) / np.sqrt(len(u)) < 1e-5
+
+
+def test_repeated_solves_identical(gpu):
+    # tst_solver.h:141-155: identical residuals on repeated solve() calls
+    csr = xamg.CsrMatrix.aniso27(20)
+    rng = np.random.default_rng(3)
+    B = rng.uniform(-1, 1, (csr.nrows, 8))
+    spec = util.amg_params(max_levels=6)
+    xamg.set_nv(8)
+    A = xamg.Matrix(csr)
+    x, b = xamg.Vector(csr.nrows, 8), xamg.Vector(csr.nrows, 8)
+    b.upload(B)
+    s = xamg.Solver(A, xamg.Params(spec), x, b)
+    hs = []
+    xs = []
+    for _ in range(3):
+        x.set(0.0)
+        s.solve()
+        hs.append(s.history())
+        xs.append(x.download())
+    for q in range(1, 3):
+        assert np.array_equal(hs[0], hs[q]) and np.array_equal(xs[0], xs[q])
+
+
+def test_large_27pt_true_residual(gpu):
+    """A larger anisotropic case checked by a size-independent property: the
+    true residual ||b - A x|| computed independently (torch, FP64) meets the
+    tolerance for every column."""
+    import torch
+    n = 64
+    csr = xamg.CsrMatrix.aniso27(n)
+    rp, ci, v = csr.arrays()
+    rng = np.random.default_rng(9)
+    B = rng.uniform(-1, 1, (csr.nrows, 16))
+    spec = util.amg_params(max_levels=6)
+    s, X, keep = solve_api(csr, spec, B)
+    assert all(s.converged())
+    At = torch.sparse_csr_tensor(torch.from_numpy(rp.astype(np.int64)), torch.from_numpy(ci.astype(np.int64)),
+                                 torch.from_numpy(v), size=(csr.nrows, csr.nrows)).cuda()
+    R = torch.from_numpy(B).cuda() - At @ torch.from_numpy(X).cuda()
+    rel = (R.norm(dim=0) / torch.from_numpy(B).cuda().norm(dim=0)).cpu().numpy()
+    assert np.all(rel <= 1e-8 * 1.05), rel
+
+
+def test_nonconvergence_and_bad_input_report(gpu):
+    csr = xamg.CsrMatrix.cube(16, 16, 16, 0)
+    rng = np.random.default_rng(4)
+    B = rng.uniform(-1, 1, (csr.nrows, 1))
+    spec = util.amg_params(precond_mg=False, max_iters=3)
+    s, X, keep = solve_api(csr, spec, B)
+    assert s.iters()[0] == 3 and not any(s.converged())
+    L = xamg.lib()
+    assert L.XAMG_solver_solve1(2, s.h) == 2  # nv mismatch is an error code, not an abort

@@ -1,0 +1,175 @@
+"""Host-side logic of the library: C ABI exports, parameters, generators, AMG
+setup and Gauss-Seidel schedules (no GPU needed)."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle as orc
+import util
+import xamg
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in ("xamg_c_api.h", "xamg_b200.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"\b((?:XAMG|xamg)_\w+)\s*\(", src):
+            if m.group(1) != "XAMG_id_get_comm":
+                names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    import ctypes
+    lib = ctypes.CDLL(xamg.LIB_PATH)
+    names = declared_symbols()
+    assert len(names) > 90
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_reference_api_surface_is_complete():
+    # every function of the reference's api/c/xamg_c_api.h:43-122
+    ref = """XAMG_init XAMG_finalize XAMG_get_nv XAMG_id_get_proc XAMG_id_get_nprocs
+    XAMG_id_get_comm_ptr XAMG_param_create XAMG_param_add_value_s XAMG_param_add_value_i
+    XAMG_param_add_value_d XAMG_param_add_value_b XAMG_param_forced_change_value_s
+    XAMG_param_forced_change_value_i XAMG_param_forced_change_value_d
+    XAMG_param_forced_change_value_b XAMG_param_change_value_s XAMG_param_change_value_i
+    XAMG_param_change_value_d XAMG_param_change_value_b XAMG_param_override_create
+    XAMG_param_override_add_value XAMG_param_override_apply XAMG_param_override_destroy
+    XAMG_param_set_default XAMG_param_print XAMG_param_destroy XAMG_part_create
+    XAMG_part_construct XAMG_part_get_numa_size XAMG_part_destroy XAMG_vector_create
+    XAMG_vector_offset XAMG_vector_alloc_d XAMG_vector_set_part XAMG_vector_set_val_d
+    XAMG_vector_download_d XAMG_vector_upload_v XAMG_vector_upload_d XAMG_vector_destroy
+    XAMG_csr_matrix_create XAMG_csr_matrix_alloc XAMG_csr_matrix_fill XAMG_csr_matrix_offset
+    XAMG_csr_matrix_get_nrows XAMG_csr_matrix_destroy XAMG_matrix_create XAMG_matrix_set_part
+    XAMG_matrix_construct XAMG_matrix_destroy XAMG_solver_create1 XAMG_solver_create2
+    XAMG_solver_renew_params XAMG_solver_solve1 XAMG_solver_solve2 XAMG_solver_print_info
+    XAMG_solver_get_convergence_info XAMG_solver_get_iter_info XAMG_solver_destroy
+    XAMG_timer XAMG_barrier""".split()
+    assert set(ref) <= declared_symbols()
+
+
+def test_params_defaults_and_overrides():
+    L = xamg.lib()
+    p = xamg.Params({"solver": {"method": "PBiCGStab"}, "preconditioner": {"method": "MultiGrid"}},
+                    overrides={"preconditioner": {"mg_coarsening_type": "8@lev0-1"}})
+    assert p.h >= 0
+    # unknown key and wrong type are refused with code 2
+    assert L.XAMG_param_add_value_i(b"solver", b"no_such_key", 1, p.h) == 2
+    assert L.XAMG_param_add_value_s(b"solver", b"max_iters", b"x", p.h) == 2
+    assert L.XAMG_param_change_value_d(b"solver", b"rel_tolerance", 1e-6, p.h) == 0
+    assert L.XAMG_param_print(12345) == 2
+    assert b"invalid param handle" in L.XAMG_b200_last_error()
+
+
+def test_nv_mismatch_and_bad_handles_return_codes():
+    L = xamg.lib()
+    xamg.check(L.XAMG_b200_set_nv(4))
+    h = xamg.C.c_size_t()
+    xamg.check(L.XAMG_vector_create(xamg.C.byref(h), xamg.MEM_LOCAL))
+    assert L.XAMG_vector_alloc_d(10, 2, h.value) == 2
+    assert L.XAMG_vector_alloc_d(10, 4, h.value) == 0
+    a = np.arange(40, dtype=np.float64)
+    assert L.XAMG_vector_upload_d(xamg._ptr(a), 10, 0, 4, h.value) == 0
+    out = np.zeros(40)
+    assert L.XAMG_vector_download_d(xamg._ptr(out), 10, 0, 4, h.value) == 0
+    assert np.all(out == a)
+    assert L.XAMG_vector_download_d(xamg._ptr(out), 11, 0, 4, h.value) == 2
+    assert L.XAMG_b200_set_nv(3) == 2
+    assert L.XAMG_solver_solve1(4, 999) == 2
+    xamg.check(L.XAMG_b200_set_nv(1))
+
+
+def test_cube_generator_matches_reference_layout():
+    m = xamg.CsrMatrix.cube(32, 32, 32, 0)
+    assert m.nrows == 32768 and m.nnz == 223232
+    rp, ci, v = m.arrays()
+    # row order: diagonal first, then ascending (b, s, w, e, n, t); row sums
+    # zero inside, positive (Dirichlet) on the boundary
+    for r in (0, 1000, 16912, 32767):
+        cols = ci[rp[r]:rp[r + 1]]
+        assert cols[0] == r and np.all(np.diff(cols[1:]) > 0)
+    inner = 16912
+    assert abs(v[rp[inner]:rp[inner + 1]].sum()) < 1e-9 * v[rp[inner]]
+    assert v[rp[inner]] == 6 * 32 * 32
+
+
+def test_27pt_generator():
+    m = xamg.CsrMatrix.aniso27(8)
+    rp, ci, v = m.arrays()
+    assert m.nnz == (3 * 8 - 2) ** 3
+    import scipy.sparse as sp
+    A = sp.csr_matrix((v, ci, rp), copy=True)
+    assert abs(A - A.T).max() < 1e-15
+    assert np.all(v[rp[:-1]] > 0) and np.all(np.delete(v, rp[:-1]) < 0)
+
+
+def test_amg_setup_structure():
+    m = xamg.CsrMatrix.aniso27(20)
+    prm = xamg.Params(util.amg_params(max_levels=6))
+    lv = xamg.amg_host(m, prm)
+    assert 2 <= len(lv) <= 6
+    for l in range(len(lv) - 1):
+        n, nc = lv[l]["n"], lv[l]["ncP"]
+        assert nc == lv[l + 1]["n"] and nc < n
+        prp, pci, pv = lv[l]["P"]
+        assert np.all(np.diff(prp) <= 4)  # P_max_elmts = 4
+        # coarse operator rows: diagonal first, then ascending
+        rp, ci, v = lv[l + 1]["A"]
+        for r in range(0, lv[l + 1]["n"], 7):
+            assert ci[rp[r]] == r and np.all(np.diff(ci[rp[r] + 1:rp[r + 1]]) > 0)
+        # Galerkin: A_c == P^T A P
+        import scipy.sparse as sp
+        A = sp.csr_matrix((lv[l]["A"][2], lv[l]["A"][1], lv[l]["A"][0]), shape=(n, n), copy=True)
+        P = sp.csr_matrix((pv, pci, prp), shape=(n, nc), copy=True)
+        Ac = sp.csr_matrix((v, ci, rp), shape=(nc, nc), copy=True)
+        D = (P.T @ A @ P - Ac)
+        assert abs(D).max() <= 1e-12 * abs(Ac).max()
+    # the setup is deterministic
+    lv2 = xamg.amg_host(m, prm)
+    for a, b in zip(lv, lv2):
+        for q in range(3):
+            assert np.array_equal(a["A"][q], b["A"][q])
+
+
+def test_amg_preconditioner_quality():
+    rng = np.random.default_rng(7)
+    m = xamg.CsrMatrix.aniso27(16)
+    rp, ci, v = m.arrays()
+    mg = orc.MG(xamg.amg_host(m, xamg.Params(util.amg_params(max_levels=6))))
+    b = rng.uniform(-1, 1, (m.nrows, 2))
+    x, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, b, np.zeros_like(b), mg=mg, max_iters=50, rel_tol=1e-8)
+    assert st.all() and it <= 10
+
+
+@pytest.mark.parametrize("brows", [0, 1, 7, 64])
+def test_gs_levels_host_match_oracle(brows):
+    rng = np.random.default_rng(8)
+    rp, ci, v = util.random_csr(400, 400, rng, max_nnz=7)
+    lf, lb, nl = xamg.gs_levels_host(rp, ci, brows)
+    if brows == 0:
+        of, ob = orc.gs_levels(rp, ci)
+        assert np.array_equal(lf, of) and np.array_equal(lb, ob)
+    for i in range(400):
+        for j in ci[rp[i]:rp[i + 1]]:
+            if brows and j // brows != i // brows:
+                continue
+            if j < i:
+                assert lf[j] < lf[i]
+            elif j > i:
+                assert lf[j] > lf[i] and lb[j] < lb[i]
+    assert nl[0] == lf.max() + 1 and nl[1] == lb.max() + 1
+
+
+def test_gs_levels_27pt_count():
+    m = xamg.CsrMatrix.aniso27(16)
+    rp, ci, v = m.arrays()
+    lf, lb, nl = xamg.gs_levels_host(rp, ci, 0)
+    # lexicographic 27-point: level(i,j,k) = i + 2j + 4k
+    assert nl == (7 * 16 - 6, 7 * 16 - 6)

@@ -1,0 +1,892 @@
+// Device objects and solver drivers of the XAMG B200 solve phase.
+#include "solve.h"
+#include "amg.h"
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <set>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace xamg {
+
+
+Context &ctx() {
+    static Context c;
+    c.init();
+    return c;
+}
+
+static bool quiet() { return std::getenv("XAMG_QUIET") != nullptr; }
+
+// ------------------------------------------------------------------ DCsr
+void DCsr::upload(const HostCsr &h, bool f64, bool f32) {
+    cudaStream_t s = ctx().stream;
+    n = h.n;
+    ncols = h.ncols;
+    nnz = h.nnz();
+    rp.alloc(sizeof(int) * (n + 1));
+    ci.alloc(sizeof(int) * std::max<i64>(nnz, 1));
+    XCUDA(cudaMemcpyAsync(rp.p, h.rp.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
+    if (nnz) XCUDA(cudaMemcpyAsync(ci.p, h.ci.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, s));
+    if (f64) {
+        v64.alloc(sizeof(double) * std::max<i64>(nnz, 1));
+        if (nnz) XCUDA(cudaMemcpyAsync(v64.p, h.v.data(), sizeof(double) * nnz, cudaMemcpyHostToDevice, s));
+    }
+    if (f32) {
+        std::vector<float> f(h.v.begin(), h.v.end());
+        v32.alloc(sizeof(float) * std::max<i64>(nnz, 1));
+        if (nnz) XCUDA(cudaMemcpyAsync(v32.p, f.data(), sizeof(float) * nnz, cudaMemcpyHostToDevice, s));
+        XCUDA(cudaStreamSynchronize(s));
+    }
+    XCUDA(cudaStreamSynchronize(s));
+}
+
+void Matrix::ensure32() {
+    if (has32) return;
+    std::vector<float> f(h.v.begin(), h.v.end());
+    d.v32.alloc(sizeof(float) * std::max<i64>(d.nnz, 1));
+    if (d.nnz)
+        XCUDA(cudaMemcpy(d.v32.p, f.data(), sizeof(float) * d.nnz, cudaMemcpyHostToDevice));
+    has32 = true;
+}
+
+// inverse diagonal, csr_matrix.h:344-349 (last diagonal entry wins; the FP32
+// copy is 1.0/(double)(float)a_ii rounded to float)
+static void make_invd(const HostCsr &A, bool f64, bool f32, DBuf &d64, DBuf &d32) {
+    std::vector<double> i64v(A.n, 0.0);
+    std::vector<float> i32v(A.n, 0.f);
+    for (i64 i = 0; i < A.n; ++i)
+        for (int j = A.rp[i]; j < A.rp[i + 1]; ++j)
+            if (A.ci[j] == i) {
+                i64v[i] = 1.0 / A.v[j];
+                i32v[i] = (float)(1.0 / (double)(float)A.v[j]);
+            }
+    if (f64) {
+        d64.alloc(sizeof(double) * std::max<i64>(A.n, 1));
+        XCUDA(cudaMemcpy(d64.p, i64v.data(), sizeof(double) * A.n, cudaMemcpyHostToDevice));
+    }
+    if (f32) {
+        d32.alloc(sizeof(float) * std::max<i64>(A.n, 1));
+        XCUDA(cudaMemcpy(d32.p, i32v.data(), sizeof(float) * A.n, cudaMemcpyHostToDevice));
+    }
+}
+
+// ------------------------------------------------------------------ GsPlan
+// Wavefront levels (one pass over the CSR, O(nnz)): row i's forward level is
+// one more than the largest level of any j < i that row i reads or that reads
+// row i; rows of equal level are independent and all their dependencies are
+// resolved in the sequential order.  The backward schedule mirrors it.
+void gs_levels_host(const HostCsr &A, i64 brows, std::vector<int> &lf, std::vector<int> &lb) {
+    i64 n = A.n;
+    auto inblk = [&](i64 i, i64 c) { return brows <= 0 || (c / brows) == (i / brows); };
+    lf.assign(n, 0);
+    lb.assign(n, 0);
+    std::vector<int> pend(n, 0);
+    for (i64 i = 0; i < n; ++i) {
+        int L = pend[i];
+        for (int j = A.rp[i]; j < A.rp[i + 1]; ++j) {
+            i64 c = A.ci[j];
+            if (c < i && inblk(i, c)) L = std::max(L, lf[c] + 1);
+        }
+        lf[i] = L;
+        for (int j = A.rp[i]; j < A.rp[i + 1]; ++j) {
+            i64 c = A.ci[j];
+            if (c > i && inblk(i, c)) pend[c] = std::max(pend[c], L + 1);
+        }
+    }
+    std::fill(pend.begin(), pend.end(), 0);
+    for (i64 i = n - 1; i >= 0; --i) {
+        int L = pend[i];
+        for (int j = A.rp[i]; j < A.rp[i + 1]; ++j) {
+            i64 c = A.ci[j];
+            if (c > i && inblk(i, c)) L = std::max(L, lb[c] + 1);
+        }
+        lb[i] = L;
+        for (int j = A.rp[i]; j < A.rp[i + 1]; ++j) {
+            i64 c = A.ci[j];
+            if (c < i && inblk(i, c)) pend[c] = std::max(pend[c], L + 1);
+        }
+    }
+}
+
+void GsPlan::build(const HostCsr &A, i64 brows_, bool persistent_) {
+    n = A.n;
+    brows = brows_;
+    persistent = persistent_;
+    gs_levels_host(A, brows, lf, lb);
+    auto sched = [&](const std::vector<int> &lev, std::vector<int> &lptr, DBuf &dperm, DBuf &dlptr) {
+        int nl = 0;
+        for (i64 i = 0; i < n; ++i) nl = std::max(nl, lev[i] + 1);
+        lptr.assign(nl + 1, 0);
+        for (i64 i = 0; i < n; ++i) lptr[lev[i] + 1]++;
+        for (int l = 0; l < nl; ++l) lptr[l + 1] += lptr[l];
+        std::vector<int> pos(lptr.begin(), lptr.end() - 1), perm(std::max<i64>(n, 1));
+        for (i64 i = 0; i < n; ++i) perm[pos[lev[i]]++] = (int)i;
+        dperm.alloc(sizeof(int) * perm.size());
+        XCUDA(cudaMemcpy(dperm.p, perm.data(), sizeof(int) * perm.size(), cudaMemcpyHostToDevice));
+        dlptr.alloc(sizeof(int) * lptr.size());
+        XCUDA(cudaMemcpy(dlptr.p, lptr.data(), sizeof(int) * lptr.size(), cudaMemcpyHostToDevice));
+        return nl;
+    };
+    nlf = sched(lf, hlf, permf, lptrf);
+    nlb = sched(lb, hlb, permb, lptrb);
+    sync.alloc(16);
+    XCUDA(cudaMemset(sync.p, 0, 16));
+}
+
+void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val,
+                   const void *invd, const void *t, void *x, const void *relax, bool forward,
+                   cudaStream_t s) {
+    int nl = forward ? nlf : nlb;
+    const std::vector<int> &hl = forward ? hlf : hlb;
+    const int *perm = (forward ? permf : permb).as<int>();
+    if (nl == 0) return;
+    if (persistent && nl > 2) {
+        unsigned *bar = sync.as<unsigned>();
+        int *err = (int *)(bar + 2);
+        XCUDA(xk::gs_sweep_persistent(p, nv, nl, (forward ? lptrf : lptrb).as<int>(), perm,
+                                      rp, ci, val, invd, t, x, relax, brows, bar, err, s));
+        return;
+    }
+    for (int l = 0; l < nl; ++l)
+        xk::gs_level(p, nv, hl[l + 1] - hl[l], perm + hl[l], rp, ci, val, invd, t, x, relax,
+                     brows, s);
+}
+
+int GsPlan::error_flag() const {
+    if (!sync.p) return 0;
+    unsigned h[4] = {0, 0, 0, 0};
+    XCUDA(cudaMemcpy(h, sync.p, 16, cudaMemcpyDeviceToHost));
+    return (int)h[2];
+}
+
+// ------------------------------------------------------------------ Conv
+double Conv::tol(int k) const {
+    if (!ptol.empty()) return ptol[k];
+    return std::max(abs_tol, rel_tol * std::sqrt(res0[k]));
+}
+void Conv::update(const double *r) {
+    for (int k = 0; k < nv; ++k)
+        if (!status[k]) res[k] = r[k];
+}
+bool Conv::check() {
+    if (!check_on) return false;
+    bool all = true;
+    for (int k = 0; k < nv; ++k) {
+        if (status[k]) continue;
+        double a = std::sqrt(res[k]);
+        if (a > tol(k)) all = false;
+        else status[k] = 1;
+    }
+    if (print_on && !quiet()) {
+        printf("%s %4d", prefix.c_str(), iters);
+        for (int k = 0; k < nv; ++k) printf(" %.3e", res0[k] > 0 ? std::sqrt(res[k] / res0[k]) : 0.0);
+        printf("\n");
+    }
+    return all;
+}
+
+static void parse_conv(const ParamList &l, Conv &c) {
+    std::set<std::string> cd;
+    std::string s = l.has("convergence_details") ? l.get_string("convergence_details") : "nocheck,noprint";
+    std::string cur;
+    for (char ch : s + ",") {
+        if (ch == ',') { if (!cur.empty()) cd.insert(cur); cur.clear(); }
+        else cur += ch;
+    }
+    c.print_on = cd.count("noprint") == 0;
+    c.check_on = cd.count("nocheck") == 0;
+    if (l.has("abs_tolerance")) c.abs_tol = l.get_float("abs_tolerance");
+    if (l.has("rel_tolerance")) c.rel_tol = l.get_float("rel_tolerance");
+}
+
+// ------------------------------------------------------------------ helpers
+static void dot1(const DVec &a, const DVec &b, DBuf &part, double *out, cudaStream_t s) {
+    const void *A[1] = {a.p()}, *B[1] = {b.p()};
+    xk::dots(a.prec, a.nv, a.n, 1, A, B, part.as<double>(), out, s);
+}
+static void ensure_part(DBuf &part, i64 n, int nd, int nv) {
+    size_t need = sizeof(double) * std::max<i64>(xk::dot_part_size(n, nd, nv), 1);
+    if (part.bytes < need) part.alloc(need);
+}
+
+struct Pinned {
+    double *h = nullptr;
+    size_t cnt = 0;
+    void alloc(size_t c) {
+        if (h) cudaFreeHost(h);
+        XCUDA(cudaMallocHost(&h, sizeof(double) * std::max<size_t>(c, 1)));
+        cnt = c;
+    }
+    ~Pinned() { if (h) cudaFreeHost(h); }
+};
+
+// ------------------------------------------------------------------ solvers
+struct Identity : Solver {
+    void solve(DVec &x, const DVec &b) override {
+        xk::blas(prec, nv, x.n, xk::Op::COPY, nullptr, b.p(), nullptr, nullptr, nullptr, x.p(), ctx().stream);
+    }
+};
+
+// Direct coarse solve: x = A^{-1} b with a dense inverse built at setup.
+struct Direct : Solver {
+    int n = 0;
+    DBuf AT;
+    void setup(const HostCsr &A, Prec p, std::vector<double> &inv_out) {
+        n = (int)A.n;
+        std::vector<double> D((size_t)n * n, 0.0);
+        for (int i = 0; i < n; ++i)
+            for (int j = A.rp[i]; j < A.rp[i + 1]; ++j) D[(size_t)i * n + A.ci[j]] = A.v[j];
+        inv_out.resize((size_t)n * n);
+        dense_inverse(n, D.data(), inv_out.data());
+        prec = p;
+        if (p == Prec::F64) {
+            std::vector<double> T((size_t)n * n);
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j) T[(size_t)j * n + i] = inv_out[(size_t)i * n + j];
+            AT.alloc(sizeof(double) * std::max<size_t>(T.size(), 1));
+            XCUDA(cudaMemcpy(AT.p, T.data(), sizeof(double) * T.size(), cudaMemcpyHostToDevice));
+        } else {
+            std::vector<float> T((size_t)n * n);
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j) T[(size_t)j * n + i] = (float)inv_out[(size_t)i * n + j];
+            AT.alloc(sizeof(float) * std::max<size_t>(T.size(), 1));
+            XCUDA(cudaMemcpy(AT.p, T.data(), sizeof(float) * T.size(), cudaMemcpyHostToDevice));
+        }
+    }
+    void solve(DVec &x, const DVec &b) override {
+        xk::dense_gemv(prec, nv, n, AT.p, b.p(), x.p(), ctx().stream);
+    }
+};
+
+// Smoothers operate on one level operator (device CSR + inverse diagonal).
+struct LevelOp {
+    const DCsr *A = nullptr;
+    const void *invd = nullptr;
+    GsPlan *gs = nullptr;
+};
+
+struct HSGS : Solver {
+    LevelOp op;
+    DVec t, r;
+    DBuf relax, ones, part;
+    Pinned hres;
+    void init(const LevelOp &o, i64 n) {
+        op = o;
+        parse_conv(prm, conv);
+        conv.init(nv);
+        std::vector<double> rl(nv, prm.get_float("relax_factor"));
+        relax.alloc(sizeof(double) * nv);
+        if (prec == Prec::F64) XCUDA(cudaMemcpy(relax.p, rl.data(), sizeof(double) * nv, cudaMemcpyHostToDevice));
+        else {
+            std::vector<float> rf(rl.begin(), rl.end());
+            XCUDA(cudaMemcpy(relax.p, rf.data(), sizeof(float) * nv, cudaMemcpyHostToDevice));
+        }
+        if (op.gs->brows > 0 && op.gs->brows < n) t.alloc(n, nv, prec);
+        if (conv.check_on) {
+            r.alloc(n, nv, prec);
+            ensure_part(part, n, 1, nv);
+            hres.alloc(nv);
+        }
+    }
+    // one blas2::SGS call (blas2.h:184-281)
+    void sgs(DVec &x, const DVec &b) {
+        cudaStream_t s = ctx().stream;
+        const void *tp = b.p();
+        if (t.n) {
+            xk::offblock_resid(prec, nv, x.n, op.A->rpp(), op.A->cip(), op.A->val(prec), b.p(), x.p(), t.p(), op.gs->brows, s);
+            tp = t.p();
+        }
+        const DCsr &A = *op.A;
+        op.gs->sweep(prec, nv, A.rpp(), A.cip(), A.val(prec), op.invd, tp, x.p(), relax.p, true, s);
+        op.gs->sweep(prec, nv, A.rpp(), A.cip(), A.val(prec), op.invd, tp, x.p(), relax.p, false, s);
+    }
+    bool residual_check(DVec &x, const DVec &b, bool initial) {
+        cudaStream_t s = ctx().stream;
+        xk::spmv(prec, nv, x.n, op.A->rpp(), op.A->cip(), op.A->val(prec), x.p(), r.p(), 2, b.p(), s);
+        double *d = part.as<double>();
+        DBuf out(sizeof(double) * nv);
+        dot1(r, r, part, out.as<double>(), s);
+        XCUDA(cudaMemcpyAsync(hres.h, out.p, sizeof(double) * nv, cudaMemcpyDeviceToHost, s));
+        XCUDA(cudaStreamSynchronize(s));
+        (void)d;
+        if (initial) conv.res0.assign(hres.h, hres.h + nv);
+        conv.update(hres.h);
+        conv.record();
+        return conv.check();
+    }
+    void solve(DVec &x, const DVec &b) override {
+        int iters = (int)prm.get_int("max_iters");
+        conv.init(nv);
+        if (conv.check_on && residual_check(x, b, true)) return;
+        for (int it = 1; it <= iters; ++it) {
+            conv.iters = it;
+            sgs(x, b);
+            if (conv.check_on && residual_check(x, b, false)) return;
+        }
+    }
+};
+
+struct Jacobi : Solver {
+    LevelOp op;
+    DVec tmp, r;
+    DBuf relax, part;
+    Pinned hres;
+    void init(const LevelOp &o, i64 n) {
+        op = o;
+        parse_conv(prm, conv);
+        conv.init(nv);
+        std::vector<double> rl(nv, prm.get_float("relax_factor"));
+        relax.alloc(sizeof(double) * nv);
+        if (prec == Prec::F64) XCUDA(cudaMemcpy(relax.p, rl.data(), sizeof(double) * nv, cudaMemcpyHostToDevice));
+        else {
+            std::vector<float> rf(rl.begin(), rl.end());
+            XCUDA(cudaMemcpy(relax.p, rf.data(), sizeof(float) * nv, cudaMemcpyHostToDevice));
+        }
+        tmp.alloc(n, nv, prec);
+        if (conv.check_on) {
+            r.alloc(n, nv, prec);
+            ensure_part(part, n, 1, nv);
+            hres.alloc(nv);
+        }
+    }
+    void solve(DVec &x, const DVec &b) override {
+        cudaStream_t s = ctx().stream;
+        int iters = (int)prm.get_int("max_iters");
+        conv.init(nv);
+        if (!conv.check_on) {
+            // nocheck path (jacobi.inl:91-100): x_{k+1} = x_k + relax*D^-1 (b - A x_k),
+            // ping-ponging between x and tmp
+            DVec *cur = &x, *nxt = &tmp;
+            for (int it = 1; it <= iters; ++it) {
+                xk::jacobi(prec, nv, x.n, op.A->rpp(), op.A->cip(), op.A->val(prec), op.invd, b.p(), cur->p(), nxt->p(), relax.p, s);
+                std::swap(cur, nxt);
+            }
+            if (cur != &x)
+                xk::blas(prec, nv, x.n, xk::Op::COPY, nullptr, cur->p(), nullptr, nullptr, nullptr, x.p(), s);
+            return;
+        }
+        // check path (jacobi.inl:76-89): r = b - A x; r *= invdiag; x = relax*r + 1*x
+        throw Error("Jacobi with convergence checks is not supported on the device path", 4);
+    }
+};
+
+// ------------------------------------------------------------------ MultiGrid
+struct MultiGrid : Solver {
+    std::vector<MGLevel> lv;
+    std::unique_ptr<Direct> coarse;
+    std::vector<double> coarse_inv;
+    Matrix *Afine = nullptr;
+    int cycle = 0;
+    DVec r;
+    DBuf part, ones;
+    Pinned hres;
+    bool reduced = false;
+
+    Prec lvprec(int l) const { return l == 0 ? prec : (reduced ? Prec::F32 : prec); }
+
+    void setup(const GlobalParams &gp, Matrix &A) {
+        Afine = &A;
+        parse_conv(prm, conv);
+        conv.init(nv);
+        conv.prefix = role == "preconditioner" ? "PREC" : "SOLV";
+        cycle = (int)prm.get_int("mg_cycle");
+        reduced = prec == Prec::F64 && prm.get_bool("mg_reduced_precision");
+        AmgParams ap;
+        ap.max_levels = (int)prm.get_int("mg_max_levels");
+        ap.coarse_size = (int)prm.get_int("mg_coarse_matrix_size");
+        ap.theta = prm.get_float("mg_strength_threshold");
+        ap.trunc = prm.get_float("mg_trunc_factor");
+        ap.pmax = (int)prm.get_int("mg_Pmax_elements");
+        ap.max_row_sum = prm.get_float("mg_max_row_sum");
+        ap.coarsen_type = (int)prm.get_int("mg_coarsening_type");
+        ap.interp_type = (int)prm.get_int("mg_interpolation_type");
+        std::vector<AmgLevel> al;
+        amg_setup(A.h, ap, al);
+        int L = (int)al.size();
+        lv.resize(L);
+        cudaStream_t s = ctx().stream;
+        for (int l = 0; l < L; ++l) {
+            MGLevel &m = lv[l];
+            m.prec = lvprec(l);
+            if (l > 0) m.hA = std::move(al[l].A);
+            m.hP = std::move(al[l].P);
+            const HostCsr &hA = l == 0 ? A.h : m.hA;
+            bool w64 = m.prec == Prec::F64, w32 = m.prec == Prec::F32;
+            if (l == 0) {
+                if (w32) A.ensure32();
+            } else {
+                m.A.upload(hA, w64, w32);
+            }
+            if (l + 1 < L) {
+                Prec cp = lvprec(l + 1);
+                HostCsr R;
+                csr_transpose(m.hP, R);
+                m.P.upload(m.hP, cp == Prec::F64, cp == Prec::F32);
+                m.R.upload(R, cp == Prec::F64, cp == Prec::F32);
+                m.tmp.alloc(hA.n, nv, m.prec);
+                if (cp != m.prec) m.tmp2.alloc(hA.n, nv, cp);
+                m.xH.alloc(m.hP.ncols, nv, cp);
+                m.bH.alloc(m.hP.ncols, nv, cp);
+                make_invd(hA, w64, w32, m.invd64, m.invd32);
+            }
+        }
+        (void)s;
+        // smoothers
+        for (int l = 0; l + 1 < L; ++l) {
+            MGLevel &m = lv[l];
+            const HostCsr &hA = l == 0 ? A.h : m.hA;
+            const DCsr &dA = l == 0 ? A.d : m.A;
+            ParamList pre = gp.get_level("pre_smoother", l), post = gp.get_level("post_smoother", l);
+            m.pre = make_smoother(pre, "pre_smoother", m, hA, dA, true);
+            m.post = make_smoother(post, "post_smoother", m, hA, dA, false);
+        }
+        // coarse-grid solver
+        ParamList cl = gp.get("coarse_grid_solver");
+        XCHECK(cl.get_string("method") == "Direct", "only the Direct coarse-grid solver is supported");
+        coarse.reset(new Direct());
+        coarse->nv = nv;
+        coarse->method = "Direct";
+        coarse->setup(L == 1 ? A.h : lv[L - 1].hA, lvprec(L - 1), coarse_inv);
+        if (conv.check_on) {
+            r.alloc(A.h.n, nv, prec);
+            ensure_part(part, A.h.n, 1, nv);
+            hres.alloc(nv);
+        }
+    }
+
+    std::unique_ptr<Solver> make_smoother(const ParamList &pl, const std::string &rl, MGLevel &m,
+                                          const HostCsr &hA, const DCsr &dA, bool pre) {
+        std::string meth = pl.get_string("method");
+        LevelOp op;
+        op.A = &dA;
+        op.invd = m.prec == Prec::F64 ? m.invd64.p : m.invd32.p;
+        if (meth == "HSGS") {
+            i64 br = pl.has("hybrid_block_rows") ? (i64)pl.get_int("hybrid_block_rows") : 0;
+            bool pers = !pl.has("gs_schedule") || pl.get_string("gs_schedule") != "levels";
+            GsPlan &g = pre ? m.gs_pre : m.gs_post;
+            if (!pre && m.gs_pre.n == hA.n && m.gs_pre.brows == br && m.gs_pre.persistent == pers) {
+                op.gs = &m.gs_pre;
+            } else {
+                g.build(hA, br, pers);
+                op.gs = &g;
+            }
+            auto h = std::unique_ptr<HSGS>(new HSGS());
+            h->role = rl; h->method = meth; h->prm = pl; h->nv = nv; h->prec = m.prec;
+            h->init(op, hA.n);
+            return h;
+        }
+        if (meth == "Jacobi") {
+            auto j = std::unique_ptr<Jacobi>(new Jacobi());
+            j->role = rl; j->method = meth; j->prm = pl; j->nv = nv; j->prec = m.prec;
+            j->init(op, hA.n);
+            return j;
+        }
+        throw Error("unsupported smoother method: " + meth, 4);
+    }
+
+    const DCsr &levA(int l) const { return l == 0 ? Afine->d : lv[l].A; }
+
+    // MG_cycle mg.inl:186-280
+    void mg_cycle(int l, DVec &x, const DVec &b, int cyc) {
+        cudaStream_t s = ctx().stream;
+        MGLevel &m = lv[l];
+        Prec p = m.prec, cp = lvprec(l + 1);
+        const DCsr &A = levA(l);
+        if (cyc != 1) m.pre->solve(x, b);
+        // temp = b - A x
+        xk::spmv(p, nv, x.n, A.rpp(), A.cip(), A.val(p), x.p(), m.tmp.p(), 2, b.p(), s);
+        // restriction (convert first when the next level is in FP32)
+        if (cp != p) {
+            xk::convert(p, cp, m.tmp.count(), m.tmp.p(), m.tmp2.p(), s);
+            xk::spmv(cp, nv, m.R.n, m.R.rpp(), m.R.cip(), m.R.val(cp), m.tmp2.p(), m.bH.p(), 0, nullptr, s);
+        } else {
+            xk::spmv(cp, nv, m.R.n, m.R.rpp(), m.R.cip(), m.R.val(cp), m.tmp.p(), m.bH.p(), 0, nullptr, s);
+        }
+        xk::fill(cp, m.xH.count(), 0.0, m.xH.p(), s);
+        if (l + 1 == (int)lv.size() - 1) {
+            coarse->solve(m.xH, m.bH);
+        } else {
+            mg_cycle(l + 1, m.xH, m.bH, cyc);
+            if (cyc == 2) mg_cycle(l + 1, m.xH, m.bH, 2);
+            else if (cyc == 1) mg_cycle(l + 1, m.xH, m.bH, 0);
+        }
+        // prolongation
+        if (cp != p) {
+            xk::spmv(cp, nv, m.P.n, m.P.rpp(), m.P.cip(), m.P.val(cp), m.xH.p(), m.tmp2.p(), 0, nullptr, s);
+            xk::convert(cp, p, m.tmp2.count(), m.tmp2.p(), m.tmp.p(), s);
+            if (!ones.p) {
+                std::vector<double> o(nv, 1.0);
+                ones.alloc(sizeof(double) * nv);
+                XCUDA(cudaMemcpy(ones.p, o.data(), sizeof(double) * nv, cudaMemcpyHostToDevice));
+            }
+            xk::blas(p, nv, x.n, xk::Op::AXPBY_Z, ones.as<double>(), m.tmp.p(), ones.as<double>(), x.p(), nullptr, x.p(), s);
+        } else {
+            xk::spmv(p, nv, m.P.n, m.P.rpp(), m.P.cip(), m.P.val(p), m.xH.p(), x.p(), 1, nullptr, s);
+        }
+        m.post->solve(x, b);
+    }
+
+    bool residual_check(DVec &x, const DVec &b, bool initial) {
+        cudaStream_t s = ctx().stream;
+        const DCsr &A = levA(0);
+        xk::spmv(prec, nv, x.n, A.rpp(), A.cip(), A.val(prec), x.p(), r.p(), 2, b.p(), s);
+        DBuf out(sizeof(double) * nv);
+        dot1(r, r, part, out.as<double>(), s);
+        XCUDA(cudaMemcpyAsync(hres.h, out.p, sizeof(double) * nv, cudaMemcpyDeviceToHost, s));
+        XCUDA(cudaStreamSynchronize(s));
+        if (initial) conv.res0.assign(hres.h, hres.h + nv);
+        conv.update(hres.h);
+        conv.record();
+        return conv.check();
+    }
+
+    void solve(DVec &x, const DVec &b) override {
+        int iters = (int)prm.get_int("max_iters");
+        conv.init(nv);
+        if (conv.check_on && residual_check(x, b, true)) return;
+        for (int it = 1; it <= iters; ++it) {
+            conv.iters = it;
+            if (lv.size() == 1) coarse->solve(x, b);
+            else mg_cycle(0, x, b, cycle);
+            if (conv.check_on && residual_check(x, b, false)) return;
+        }
+    }
+
+    std::string info() const override {
+        std::string s = "MultiGrid levels:";
+        for (size_t l = 0; l < lv.size(); ++l) {
+            const HostCsr &A = l == 0 ? Afine->h : lv[l].hA;
+            s += " " + std::to_string(A.n) + "/" + std::to_string(A.nnz());
+        }
+        return s;
+    }
+};
+
+MultiGrid *find_multigrid(Solver *s);
+
+// ------------------------------------------------------------------ Krylov
+// (P)BiCGStab.  Scalars live on the device; the host reads the NV residuals
+// once per iteration for the convergence check.
+struct Krylov : Solver {
+    Matrix *A = nullptr;
+    std::unique_ptr<Solver> M;
+    bool precond = false;
+    DVec r0, r, p, v, s, t, p_, s_;
+    DBuf part, sc;
+    Pinned hres;
+    enum { RHO, S1, S2, S3, S4, ALPHA, OMEGA, BETA, C1, RES, AC, OC, ICONV, ONES, NALPHA, NOMEGA, NSC };
+    double *S(int i) const { return sc.as<double>() + (size_t)i * nv; }
+
+    void setup(i64 n) {
+        parse_conv(prm, conv);
+        conv.init(nv);
+        conv.prefix = role == "meta_solver" ? "META" : "SOLV";
+        for (DVec *q : {&r0, &r, &p, &v, &s, &t}) q->alloc(n, nv, prec);
+        if (precond) { p_.alloc(n, nv, prec); s_.alloc(n, nv, prec); }
+        ensure_part(part, n, 3, nv);
+        sc.alloc(sizeof(double) * NSC * nv);
+        std::vector<double> z(NSC * nv, 0.0);
+        for (int k = 0; k < nv; ++k) { z[ONES * nv + k] = 1.0; z[ICONV * nv + k] = 1.0; }
+        XCUDA(cudaMemcpy(sc.p, z.data(), sizeof(double) * z.size(), cudaMemcpyHostToDevice));
+        hres.alloc(nv);
+    }
+
+    const DCsr &dA() const { return A->d; }
+
+    void read_res(int which, cudaStream_t st) {
+        XCUDA(cudaMemcpyAsync(hres.h, S(which), sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
+        XCUDA(cudaStreamSynchronize(st));
+    }
+
+    void set_iconv(cudaStream_t st) {
+        std::vector<double> ic(nv);
+        for (int k = 0; k < nv; ++k) ic[k] = conv.status[k] ? 0.0 : 1.0;
+        XCUDA(cudaMemcpyAsync(S(ICONV), ic.data(), sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+        XCUDA(cudaStreamSynchronize(st));
+    }
+
+    void spmv(const DVec &x, DVec &y, cudaStream_t st) {
+        const DCsr &a = dA();
+        xk::spmv(prec, nv, x.n, a.rpp(), a.cip(), a.val(prec), x.p(), y.p(), 0, nullptr, st);
+    }
+
+    void solve(DVec &x, const DVec &b) override {
+        cudaStream_t st = ctx().stream;
+        int max_iters = (int)prm.get_int("max_iters");
+        i64 n = x.n;
+        const DCsr &a = dA();
+        std::vector<double> ic(NSC * nv, 0.0);
+        conv.init(nv);
+        {
+            std::vector<double> one(nv, 1.0);
+            XCUDA(cudaMemcpyAsync(S(ICONV), one.data(), sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+        }
+        // r0 = b - A x; rho = (r0, r0)
+        xk::spmv(prec, nv, n, a.rpp(), a.cip(), a.val(prec), x.p(), r0.p(), 2, b.p(), st);
+        dot1(r0, r0, part, S(RHO), st);
+        read_res(RHO, st);
+        conv.res0.assign(hres.h, hres.h + nv);
+        conv.update(hres.h);
+        conv.record();
+        if (conv.check()) return;
+        set_iconv(st);
+        xk::blas(prec, nv, n, xk::Op::COPY, nullptr, r0.p(), nullptr, nullptr, nullptr, r.p(), st);
+        xk::blas(prec, nv, n, xk::Op::COPY, nullptr, r0.p(), nullptr, nullptr, nullptr, p.p(), st);
+        for (int it = 1;; ++it) {
+            conv.iters = it;
+            DVec *pp = &p, *ss = &s;
+            if (precond) {
+                xk::fill(prec, p_.count(), 0.0, p_.p(), st);
+                M->solve(p_, p);
+                pp = &p_;
+            }
+            spmv(*pp, v, st);
+            dot1(v, r0, part, S(S1), st);
+            xk::bicg_alpha(nv, S(RHO), S(S1), S(ALPHA), st);
+            xk::negate(nv, S(ALPHA), S(NALPHA), st);
+            xk::blas(prec, nv, n, xk::Op::AXPBY_Z, S(ONES), r.p(), S(NALPHA), v.p(), nullptr, s.p(), st);
+            if (precond) {
+                xk::fill(prec, s_.count(), 0.0, s_.p(), st);
+                M->solve(s_, s);
+                ss = &s_;
+            }
+            spmv(*ss, t, st);
+            {
+                const void *Aa[3] = {t.p(), t.p(), s.p()}, *Bb[3] = {s.p(), t.p(), s.p()};
+                xk::dots(prec, nv, n, 3, Aa, Bb, part.as<double>(), S(S2), st);
+            }
+            xk::bicg_omega(nv, S(S2), S(S3), S(S4), S(ALPHA), S(ICONV), S(OMEGA), S(RES), S(AC), S(OC), st);
+            xk::blas(prec, nv, n, xk::Op::AXPBYPCZ, S(AC), pp->p(), S(OC), ss->p(), S(ONES), x.p(), st);
+            read_res(RES, st);
+            conv.update(hres.h);
+            conv.record();
+            if (conv.check()) break;
+            if (it >= max_iters) break;
+            set_iconv(st);
+            xk::negate(nv, S(OMEGA), S(NOMEGA), st);
+            xk::blas(prec, nv, n, xk::Op::AXPBY_Z, S(ONES), s.p(), S(NOMEGA), t.p(), nullptr, r.p(), st);
+            dot1(r, r0, part, S(S1), st);
+            xk::bicg_beta(nv, S(S1), S(RHO), S(ALPHA), S(OMEGA), S(BETA), S(C1), st);
+            xk::blas(prec, nv, n, xk::Op::AXPBYPCZ, S(ONES), r.p(), S(C1), v.p(), S(BETA), p.p(), st);
+        }
+        XCUDA(cudaStreamSynchronize(st));
+    }
+    std::string info() const override { return method + (M ? "(" + M->info() + ")" : ""); }
+};
+
+// ------------------------------------------------------------------ IR
+// IterativeRefinement (ir.inl:107-194).  Outer loop in FP64: r = b - A x,
+// inner solve on r (FP32 when subsolver_reduced_precision), x += x_corr.
+struct IterRefine : Solver {
+    Matrix *A = nullptr;
+    std::unique_ptr<Solver> inner;
+    bool reduced = false;
+    double inner_rel = 0.0;
+    DVec r, xc, ix, ib;
+    DBuf part, ones;
+    Pinned hres;
+    void setup(i64 n) {
+        parse_conv(prm, conv);
+        conv.init(nv);
+        conv.prefix = "META";
+        r.alloc(n, nv, Prec::F64);
+        xc.alloc(n, nv, Prec::F64);
+        if (reduced) { ix.alloc(n, nv, Prec::F32); ib.alloc(n, nv, Prec::F32); }
+        ensure_part(part, n, 1, nv);
+        std::vector<double> o(nv, 1.0);
+        ones.alloc(sizeof(double) * nv);
+        XCUDA(cudaMemcpy(ones.p, o.data(), sizeof(double) * nv, cudaMemcpyHostToDevice));
+        hres.alloc(nv);
+    }
+    bool residual_check(DVec &x, const DVec &b, bool initial) {
+        cudaStream_t s = ctx().stream;
+        const DCsr &a = A->d;
+        xk::spmv(Prec::F64, nv, x.n, a.rpp(), a.cip(), a.val(Prec::F64), x.p(), r.p(), 2, b.p(), s);
+        DBuf out(sizeof(double) * nv);
+        dot1(r, r, part, out.as<double>(), s);
+        XCUDA(cudaMemcpyAsync(hres.h, out.p, sizeof(double) * nv, cudaMemcpyDeviceToHost, s));
+        XCUDA(cudaStreamSynchronize(s));
+        if (initial) conv.res0.assign(hres.h, hres.h + nv);
+        conv.update(hres.h);
+        conv.record();
+        return conv.check();
+    }
+    void solve(DVec &x, const DVec &b) override {
+        cudaStream_t s = ctx().stream;
+        int max_iters = (int)prm.get_int("max_iters");
+        conv.init(nv);
+        if (residual_check(x, b, true)) return;
+        for (int it = 1; it <= max_iters; ++it) {
+            conv.iters = it;
+            // inner tolerance per column: the outer absolute tolerance, or a
+            // fraction of the current residual (inner_rel_tolerance)
+            std::vector<double> tol(nv);
+            for (int k = 0; k < nv; ++k)
+                tol[k] = std::max(conv.tol(k), inner_rel * std::sqrt(std::max(hres.h[k], 0.0)));
+            inner->conv.ptol = tol;
+            if (reduced) {
+                xk::convert(Prec::F64, Prec::F32, r.count(), r.p(), ib.p(), s);
+                xk::fill(Prec::F32, ix.count(), 0.0, ix.p(), s);
+                inner->solve(ix, ib);
+                xk::convert(Prec::F32, Prec::F64, ix.count(), ix.p(), xc.p(), s);
+            } else {
+                xk::fill(Prec::F64, xc.count(), 0.0, xc.p(), s);
+                inner->solve(xc, r);
+            }
+            xk::blas(Prec::F64, nv, x.n, xk::Op::AXPBY_Z, ones.as<double>(), xc.p(), ones.as<double>(), x.p(), nullptr, x.p(), s);
+            conv.sub_iters += inner->conv.iters;
+            if (residual_check(x, b, false)) return;
+        }
+    }
+    std::string info() const override { return "IterativeRefinement(" + inner->info() + ")"; }
+};
+
+// ------------------------------------------------------------------ factory
+static std::unique_ptr<Solver> make_solver(const GlobalParams &gp, const std::string &role,
+                                           Matrix &A, int nv, Prec prec) {
+    const ParamList &pl = gp.get(role);
+    std::string m = pl.get_string("method");
+    i64 n = A.h.n;
+    if (prec == Prec::F32) A.ensure32();
+    if (m == "BiCGStab" || m == "MergedBiCGStab" || m == "PBiCGStab" || m == "MergedPBiCGStab") {
+        auto k = std::unique_ptr<Krylov>(new Krylov());
+        k->role = role; k->method = m; k->prm = pl; k->nv = nv; k->prec = prec; k->A = &A;
+        k->precond = (m == "PBiCGStab" || m == "MergedPBiCGStab");
+        if (k->precond) {
+            if (gp.has("preconditioner")) k->M = make_solver(gp, "preconditioner", A, nv, prec);
+            else {
+                auto id = std::unique_ptr<Identity>(new Identity());
+                id->nv = nv; id->prec = prec; id->method = "Identity";
+                k->M = std::move(id);
+            }
+        }
+        k->setup(n);
+        return k;
+    }
+    if (m == "MultiGrid") {
+        auto g = std::unique_ptr<MultiGrid>(new MultiGrid());
+        g->role = role; g->method = m; g->prm = pl; g->nv = nv; g->prec = prec;
+        g->setup(gp, A);
+        return g;
+    }
+    if (m == "Identity") {
+        auto id = std::unique_ptr<Identity>(new Identity());
+        id->role = role; id->method = m; id->prm = pl; id->nv = nv; id->prec = prec;
+        return id;
+    }
+    if (m == "HSGS" || m == "Jacobi") {
+        // standalone smoother solver on the fine operator
+        struct Own : Solver {
+            std::unique_ptr<Solver> s;
+            DBuf invd64, invd32;
+            GsPlan gs;
+            void solve(DVec &x, const DVec &b) override {
+                s->solve(x, b);
+                conv = s->conv;
+            }
+        };
+        auto o = std::unique_ptr<Own>(new Own());
+        o->role = role; o->method = m; o->prm = pl; o->nv = nv; o->prec = prec;
+        make_invd(A.h, prec == Prec::F64, prec == Prec::F32, o->invd64, o->invd32);
+        LevelOp op;
+        op.A = &A.d;
+        op.invd = prec == Prec::F64 ? o->invd64.p : o->invd32.p;
+        if (m == "HSGS") {
+            i64 br = pl.has("hybrid_block_rows") ? (i64)pl.get_int("hybrid_block_rows") : 0;
+            o->gs.build(A.h, br, !pl.has("gs_schedule") || pl.get_string("gs_schedule") != "levels");
+            op.gs = &o->gs;
+            auto h = std::unique_ptr<HSGS>(new HSGS());
+            h->role = role; h->method = m; h->prm = pl; h->nv = nv; h->prec = prec;
+            h->init(op, n);
+            o->s = std::move(h);
+        } else {
+            auto j = std::unique_ptr<Jacobi>(new Jacobi());
+            j->role = role; j->method = m; j->prm = pl; j->nv = nv; j->prec = prec;
+            j->init(op, n);
+            o->s = std::move(j);
+        }
+        return o;
+    }
+    throw Error("method not implemented on the device path: " + m, 4);
+}
+
+std::unique_ptr<Solver> build_solver_tree(const GlobalParams &gp, Matrix &A, int nv) {
+    if (gp.has("meta_solver")) {
+        const ParamList &ml = gp.get("meta_solver");
+        XCHECK(ml.get_string("method") == "IterativeRefinement",
+               "meta_solver must be IterativeRefinement");
+        auto ir = std::unique_ptr<IterRefine>(new IterRefine());
+        ir->role = "meta_solver"; ir->method = "IterativeRefinement"; ir->prm = ml; ir->nv = nv;
+        ir->A = &A;
+        ir->reduced = ml.has("subsolver_reduced_precision") && ml.get_bool("subsolver_reduced_precision");
+        ir->inner_rel = ml.has("inner_rel_tolerance") ? ml.get_float("inner_rel_tolerance") : 0.0;
+        ir->inner = make_solver(gp, "solver", A, nv, ir->reduced ? Prec::F32 : Prec::F64);
+        ir->setup(A.h.n);
+        return ir;
+    }
+    return make_solver(gp, "solver", A, nv, Prec::F64);
+}
+
+MultiGrid *find_multigrid(Solver *s) {
+    if (!s) return nullptr;
+    if (auto m = dynamic_cast<MultiGrid *>(s)) return m;
+    if (auto k = dynamic_cast<Krylov *>(s)) return find_multigrid(k->M.get());
+    if (auto ir = dynamic_cast<IterRefine *>(s)) return find_multigrid(ir->inner.get());
+    return nullptr;
+}
+int mg_num_levels(MultiGrid *mg) { return (int)mg->lv.size(); }
+const HostCsr &mg_level_A(MultiGrid *mg, int l) { return l == 0 ? mg->Afine->h : mg->lv[l].hA; }
+const HostCsr &mg_level_P(MultiGrid *mg, int l) { return mg->lv[l].hP; }
+const GsPlan &mg_level_gs(MultiGrid *mg, int l) { return mg->lv[l].gs_pre; }
+const std::vector<double> &mg_coarse_inverse(MultiGrid *mg) { return mg->coarse_inv; }
+
+// Gauss-Jordan without pivoting (inverse.inl:31-106, same operation order);
+// the independent row updates of each elimination step run in parallel.
+void dense_inverse(int n, const double *A, double *Ainv) {
+    int m = 2 * n;
+    std::vector<double> e((size_t)n * m, 0.0);
+    for (int i = 0; i < n; ++i) {
+        e[(size_t)i * m + i + n] = 1.0;
+        for (int j = 0; j < n; ++j) e[(size_t)i * m + j] = A[(size_t)i * n + j];
+    }
+    for (int i = 0; i < n; ++i) {
+        double *ri = &e[(size_t)i * m];
+        for (int k = m - 1; k > i; --k) ri[k] /= ri[i];
+        ri[i] = 1.0;
+#pragma omp parallel for schedule(static) if (n > 256)
+        for (int j = i + 1; j < n; ++j) {
+            double *rj = &e[(size_t)j * m];
+            for (int k = m - 1; k > i; --k) rj[k] -= rj[i] * ri[k];
+            rj[i] = 0.0;
+        }
+    }
+    for (int ii = 0; ii < n; ++ii) {
+        int row = n - 1 - ii;
+        double *ri = &e[(size_t)row * m];
+#pragma omp parallel for schedule(static) if (n > 256)
+        for (int j = 0; j < row; ++j) {
+            double *rj = &e[(size_t)j * m];
+            for (int k = n; k < m; ++k) rj[k] -= rj[row] * ri[k];
+            rj[row] = 0.0;
+        }
+    }
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) Ainv[(size_t)i * n + j] = e[(size_t)i * m + n + j];
+}
+
+}  // namespace xamg
+
+namespace xamg {
+// Sticky error flags of the bounded device waits in the Gauss-Seidel sweeps.
+int mg_device_errors(MultiGrid *mg) {
+    int e = 0;
+    for (auto &l : mg->lv) {
+        if (l.gs_pre.n) e |= l.gs_pre.error_flag();
+        if (l.gs_post.n) e |= l.gs_post.error_flag();
+    }
+    return e;
+}
+}  // namespace xamg

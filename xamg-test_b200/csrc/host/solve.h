@@ -1,0 +1,144 @@
+// Device-resident matrices, vectors, multigrid hierarchy and solvers.
+//
+// Class map to the reference (src/solvers/*):
+//   Krylov       <- BiCGStab / PBiCGStab (bicgstab.inl:44-197, pbicgstab.inl:48-207)
+//                   and their Merged* variants (same values, one code path)
+//   MultiGrid    <- MultiGrid (mg.inl:117-331), levels from the host AMG setup
+//   HSGS, Jacobi <- hsgs.inl:31-91, jacobi.inl:31-102
+//   Direct       <- direct.inl:31-59 (+ inverse.inl Gauss-Jordan at setup)
+//   IterRefine   <- IterativeRefinement (ir.inl:107-194)
+// A solver of precision F32 keeps its vectors and matrix values in FP32 and
+// accumulates inner products and scalar recurrences in FP64.
+#pragma once
+#include "common.h"
+#include "params.h"
+
+namespace xamg {
+
+struct AmgParams;
+struct AmgLevel;
+
+struct DVec {
+    i64 n = 0;
+    int nv = 1;
+    Prec prec = Prec::F64;
+    DBuf buf;
+    void alloc(i64 n_, int nv_, Prec p) {
+        n = n_;
+        nv = nv_;
+        prec = p;
+        buf.alloc((size_t)(n_ * nv_) * prec_size(p));
+    }
+    void *p() const { return buf.p; }
+    i64 count() const { return n * nv; }
+};
+
+struct DCsr {
+    i64 n = 0, ncols = 0, nnz = 0;
+    DBuf rp, ci, v64, v32;
+    void upload(const HostCsr &h, bool f64, bool f32);
+    const void *val(Prec p) const {
+        if (p == Prec::F64) { XCHECK(v64.p || nnz == 0, "FP64 values not resident"); return v64.p; }
+        XCHECK(v32.p || nnz == 0, "FP32 values not resident");
+        return v32.p;
+    }
+    const int *rpp() const { return rp.as<int>(); }
+    const int *cip() const { return ci.as<int>(); }
+};
+
+// Wavefront schedule of the forward and backward Gauss-Seidel sweeps of one
+// matrix (optionally restricted to hybrid blocks of `brows` rows).
+struct GsPlan {
+    i64 n = 0, brows = 0;
+    int nlf = 0, nlb = 0;
+    std::vector<int> hlf, hlb;         // level pointers (host)
+    std::vector<int> lf, lb;           // per-row levels (host, for export)
+    DBuf permf, permb, lptrf, lptrb;   // device copies
+    DBuf sync;                         // barrier words + error flag
+    bool persistent = true;
+    void build(const HostCsr &A, i64 brows_, bool persistent_);
+    void sweep(Prec p, int nv, const int *rp, const int *ci, const void *val, const void *invd,
+               const void *t, void *x, const void *relax, bool forward, cudaStream_t s);
+    int error_flag() const;
+};
+
+// Convergence bookkeeping, convergence.h:48-303 with conv_check/print flags.
+struct Conv {
+    int nv = 1;
+    bool check_on = true, print_on = false;
+    double abs_tol = 0, rel_tol = 0;
+    std::vector<double> ptol;  // per-column tolerance (IR inner solver)
+    std::vector<double> res0, res;
+    std::vector<int> status;
+    int iters = 0, sub_iters = 0;
+    std::vector<double> history;  // res after every check, nv per entry
+    std::string prefix = "SOLV";
+    void init(int nv_) {
+        nv = nv_;
+        res0.assign(nv, 0.0);
+        res.assign(nv, 0.0);
+        status.assign(nv, 0);
+        iters = sub_iters = 0;
+        history.clear();
+    }
+    double tol(int k) const;
+    void update(const double *r);
+    bool check();
+    void record() { history.insert(history.end(), res.begin(), res.end()); }
+};
+
+struct Solver;
+
+// One multigrid level on the device.
+struct MGLevel {
+    HostCsr hA, hP;         // host copies (setup output; exported for parity)
+    DCsr A, P, R;
+    DBuf invd64, invd32;
+    GsPlan gs_pre, gs_post;  // share one plan when the block sizes agree
+    Prec prec = Prec::F64;   // precision of this level's vectors/operator
+    DVec tmp, tmp2, xH, bH;  // work vectors: tmp/tmp2 on this level, xH/bH on the next
+    std::unique_ptr<Solver> pre, post;
+};
+
+struct SolveEnv {
+    cudaStream_t s;
+};
+
+struct Solver {
+    std::string role = "solver";
+    std::string method;
+    ParamList prm;
+    int nv = 1;
+    Prec prec = Prec::F64;
+    Conv conv;
+    virtual ~Solver() {}
+    // x: initial guess on entry (the preconditioner role zeroes it itself)
+    virtual void solve(DVec &x, const DVec &b) = 0;
+    virtual void renew(const GlobalParams &gp) {}
+    virtual std::string info() const { return method; }
+};
+
+// Build the solver tree for `gp` over the FP64 host operator A (kept alive by
+// the caller together with its device copy).
+struct Matrix {
+    HostCsr h;
+    DCsr d;        // FP64 (and FP32 on demand)
+    bool has32 = false;
+    void ensure32();
+};
+
+std::unique_ptr<Solver> build_solver_tree(const GlobalParams &gp, Matrix &A, int nv);
+
+// Export hooks for parity tests.
+struct MultiGrid;
+MultiGrid *find_multigrid(Solver *s);
+int mg_num_levels(MultiGrid *mg);
+const HostCsr &mg_level_A(MultiGrid *mg, int l);
+const HostCsr &mg_level_P(MultiGrid *mg, int l);
+const GsPlan &mg_level_gs(MultiGrid *mg, int l);
+const std::vector<double> &mg_coarse_inverse(MultiGrid *mg);
+
+void dense_inverse(int n, const double *A, double *Ainv);
+void csr_transpose(const HostCsr &P, HostCsr &R);
+
+}  // namespace xamg

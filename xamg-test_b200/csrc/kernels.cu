@@ -1,0 +1,677 @@
+// XAMG solve-phase kernels for sm_100a.  See kernels.cuh for the contract.
+//
+// Design notes (B200):
+//  * All kernels here are HBM-bound; they are written for coalesced 16-byte
+//    accesses: a CSR row is served by TPR = NV*sizeof(T)/16 threads, each
+//    owning 16 contiguous bytes of the NV-wide x/y rows, so a warp reads whole
+//    128-byte lines of x and writes whole lines of y.
+//  * Matrix entries are read once per product and are streamed with evict-first
+//    loads (__ldcs) so that the x block vector, which is re-read ~nnz/N times
+//    through the 126 MB L2, keeps its lines resident.
+//  * Row sums keep the stored CSR order (a sequential fma chain per (row,col)),
+//    which makes the result independent of the launch shape and bit-identical
+//    to the oracle.
+#include "kernels.cuh"
+#include <cooperative_groups.h>
+#include <cstdio>
+
+namespace xk {
+
+// ------------------------------------------------------------- vector access
+template <class T, int V> struct VT;
+template <> struct VT<double, 1> { typedef double type; };
+template <> struct VT<double, 2> { typedef double2 type; };
+template <> struct VT<float, 1> { typedef float type; };
+template <> struct VT<float, 2> { typedef float2 type; };
+template <> struct VT<float, 4> { typedef float4 type; };
+
+template <class T, int NV> struct Shape {
+    static constexpr int V = (NV * (int)sizeof(T) >= 16) ? 16 / (int)sizeof(T) : NV;
+    static constexpr int TPR = NV / V;  // threads per row
+};
+
+template <class T, int V>
+__device__ __forceinline__ void ld(const T *p, T (&r)[V]) {
+    typedef typename VT<T, V>::type W;
+    W w = __ldg(reinterpret_cast<const W *>(p));
+    memcpy(r, &w, sizeof(W));
+}
+template <class T, int V>
+__device__ __forceinline__ void ld_cg(const T *p, T (&r)[V]) {
+    typedef typename VT<T, V>::type W;
+    W w = __ldcg(reinterpret_cast<const W *>(p));
+    memcpy(r, &w, sizeof(W));
+}
+template <class T, int V>
+__device__ __forceinline__ void st(T *p, const T (&r)[V]) {
+    typedef typename VT<T, V>::type W;
+    W w;
+    memcpy(&w, r, sizeof(W));
+    *reinterpret_cast<W *>(p) = w;
+}
+template <class T, int V>
+__device__ __forceinline__ void st_cg(T *p, const T (&r)[V]) {
+    typedef typename VT<T, V>::type W;
+    W w;
+    memcpy(&w, r, sizeof(W));
+    __stcg(reinterpret_cast<W *>(p), w);
+}
+
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+template <class T> __device__ __forceinline__ T mul_rn(T a, T b);
+template <> __device__ __forceinline__ double mul_rn<double>(double a, double b) { return dmul(a, b); }
+template <> __device__ __forceinline__ float mul_rn<float>(float a, float b) { return fmul(a, b); }
+template <class T> __device__ __forceinline__ T add_rn(T a, T b);
+template <> __device__ __forceinline__ double add_rn<double>(double a, double b) { return dadd(a, b); }
+template <> __device__ __forceinline__ float add_rn<float>(float a, float b) { return fadd(a, b); }
+
+#define NV_DISPATCH(nv, FN)                                                                       \
+    switch (nv) {                                                                                  \
+    case 1: FN(1); break;                                                                          \
+    case 2: FN(2); break;                                                                          \
+    case 4: FN(4); break;                                                                          \
+    case 8: FN(8); break;                                                                          \
+    case 16: FN(16); break;                                                                        \
+    case 32: FN(32); break;                                                                        \
+    default: fprintf(stderr, "xamg: unsupported nv=%d\n", nv); break;                              \
+    }
+
+// ---------------------------------------------------------------- SpMV
+// mode 0: y = A x; mode 1: y += A x; mode 2: y = 1*b + (-1)*(A x)
+template <class T, int NV, int MODE>
+__global__ void __launch_bounds__(256) k_spmv(i64 n, const int *__restrict__ rp,
+                                              const int *__restrict__ ci,
+                                              const T *__restrict__ va, const T *__restrict__ x,
+                                              T *__restrict__ y, const T *__restrict__ b) {
+    constexpr int V = Shape<T, NV>::V, TPR = Shape<T, NV>::TPR, RPB = 256 / TPR;
+    i64 row = (i64)blockIdx.x * RPB + threadIdx.x / TPR;
+    int lane = threadIdx.x % TPR;
+    if (row >= n) return;
+    T acc[V];
+    if (MODE == 1) {
+        ld<T, V>(y + row * NV + lane * V, acc);
+    } else {
+#pragma unroll
+        for (int e = 0; e < V; ++e) acc[e] = T(0);
+    }
+    int j = __ldg(rp + row), j1 = __ldg(rp + row + 1);
+    const T *xb = x + lane * V;
+    for (; j + 4 <= j1; j += 4) {
+        int c0 = __ldcs(ci + j), c1 = __ldcs(ci + j + 1), c2 = __ldcs(ci + j + 2),
+            c3 = __ldcs(ci + j + 3);
+        T v0 = __ldcs(va + j), v1 = __ldcs(va + j + 1), v2 = __ldcs(va + j + 2),
+          v3 = __ldcs(va + j + 3);
+        T x0[V], x1[V], x2[V], x3[V];
+        ld<T, V>(xb + (i64)c0 * NV, x0);
+        ld<T, V>(xb + (i64)c1 * NV, x1);
+        ld<T, V>(xb + (i64)c2 * NV, x2);
+        ld<T, V>(xb + (i64)c3 * NV, x3);
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            acc[e] = fma(v0, x0[e], acc[e]);
+            acc[e] = fma(v1, x1[e], acc[e]);
+            acc[e] = fma(v2, x2[e], acc[e]);
+            acc[e] = fma(v3, x3[e], acc[e]);
+        }
+    }
+    for (; j < j1; ++j) {
+        int c0 = __ldcs(ci + j);
+        T v0 = __ldcs(va + j);
+        T x0[V];
+        ld<T, V>(xb + (i64)c0 * NV, x0);
+#pragma unroll
+        for (int e = 0; e < V; ++e) acc[e] = fma(v0, x0[e], acc[e]);
+    }
+    if (MODE == 2) {
+        T bb[V];
+        ld<T, V>(b + row * NV + lane * V, bb);
+#pragma unroll
+        for (int e = 0; e < V; ++e) acc[e] = add_rn<T>(mul_rn<T>(T(1), bb[e]), mul_rn<T>(T(-1), acc[e]));
+    }
+    st<T, V>(y + row * NV + lane * V, acc);
+}
+
+template <class T, int NV>
+static void spmv_t(i64 n, const int *rp, const int *ci, const T *va, const T *x, T *y, int mode,
+                   const T *b, cudaStream_t s) {
+    constexpr int RPB = 256 / Shape<T, NV>::TPR;
+    if (n <= 0) return;
+    unsigned g = (unsigned)((n + RPB - 1) / RPB);
+    if (mode == 0) k_spmv<T, NV, 0><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
+    else if (mode == 1) k_spmv<T, NV, 1><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
+    else k_spmv<T, NV, 2><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
+}
+
+void spmv(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val, const void *x,
+          void *y, int mode, const void *b, cudaStream_t s) {
+    if (p == Prec::F64) {
+#define F(NV) spmv_t<double, NV>(n, rp, ci, (const double *)val, (const double *)x, (double *)y, mode, (const double *)b, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    } else {
+#define F(NV) spmv_t<float, NV>(n, rp, ci, (const float *)val, (const float *)x, (float *)y, mode, (const float *)b, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    }
+}
+
+// ---------------------------------------------------------------- Gauss-Seidel
+template <class T, int NV>
+__device__ __forceinline__ void gs_row(i64 row, int lane, const int *__restrict__ rp,
+                                       const int *__restrict__ ci, const T *__restrict__ va,
+                                       const T *__restrict__ invd, const T *__restrict__ t, T *x,
+                                       const T *__restrict__ relax, i64 brows) {
+    constexpr int V = Shape<T, NV>::V;
+    T sum[V];
+    ld_cg<T, V>(t + row * NV + lane * V, sum);
+    int j = rp[row], j1 = rp[row + 1];
+    i64 lo = 0, hi = INT64_MAX;
+    if (brows > 0) { lo = (row / brows) * brows; hi = lo + brows; }
+    for (; j < j1; ++j) {
+        int c = __ldg(ci + j);
+        if (c < lo || c >= hi) continue;
+        T v = -__ldg(va + j);
+        T xv[V];
+        ld_cg<T, V>(x + (i64)c * NV + lane * V, xv);
+#pragma unroll
+        for (int e = 0; e < V; ++e) sum[e] = fma(v, xv[e], sum[e]);
+    }
+    T di = __ldg(invd + row);
+    T xo[V];
+    ld_cg<T, V>(x + row * NV + lane * V, xo);
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+        T cf = mul_rn<T>(__ldg(relax + lane * V + e), di);
+        xo[e] = fma(cf, sum[e], xo[e]);
+    }
+    st_cg<T, V>(x + row * NV + lane * V, xo);
+}
+
+template <class T, int NV>
+__global__ void __launch_bounds__(256) k_gs_level(int cnt, const int *__restrict__ rows,
+                                                  const int *__restrict__ rp,
+                                                  const int *__restrict__ ci,
+                                                  const T *__restrict__ va,
+                                                  const T *__restrict__ invd,
+                                                  const T *__restrict__ t, T *x,
+                                                  const T *__restrict__ relax, i64 brows) {
+    constexpr int TPR = Shape<T, NV>::TPR;
+    int item = blockIdx.x * 256 + threadIdx.x;
+    if (item >= cnt * TPR) return;
+    gs_row<T, NV>(__ldg(rows + item / TPR), item % TPR, rp, ci, va, invd, t, x, relax, brows);
+}
+
+void gs_level(Prec p, int nv, int cnt, const int *rows, const int *rp, const int *ci,
+              const void *val, const void *invd, const void *t, void *x, const void *relax,
+              i64 brows, cudaStream_t s) {
+    if (cnt <= 0) return;
+    if (p == Prec::F64) {
+#define F(NV) k_gs_level<double, NV><<<(cnt * Shape<double, NV>::TPR + 255) / 256, 256, 0, s>>>(cnt, rows, rp, ci, (const double *)val, (const double *)invd, (const double *)t, (double *)x, (const double *)relax, brows)
+        NV_DISPATCH(nv, F)
+#undef F
+    } else {
+#define F(NV) k_gs_level<float, NV><<<(cnt * Shape<float, NV>::TPR + 255) / 256, 256, 0, s>>>(cnt, rows, rp, ci, (const float *)val, (const float *)invd, (const float *)t, (float *)x, (const float *)relax, brows)
+        NV_DISPATCH(nv, F)
+#undef F
+    }
+}
+
+// Grid-wide barrier for cooperative launches.  bar[0] counts arrivals,
+// bar[1] is the generation.  Every wait is bounded by a wall-clock limit
+// (%globaltimer); on expiry the error flag is raised and the caller leaves.
+static constexpr unsigned long long kWaitLimitNs = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ unsigned long long gtime() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool grid_sync(unsigned *bar, int *err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = bar + 1;
+        unsigned g = *gen;
+        __threadfence();
+        unsigned arrived = atomicAdd(bar, 1u);
+        if (arrived == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned long long t0 = gtime();
+            while (*gen == g) {
+                if (*(volatile int *)err) break;
+                if (gtime() - t0 > kWaitLimitNs) {
+                    atomicExch(err, 1);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile int *)err == 0;
+}
+
+template <class T, int NV>
+__global__ void __launch_bounds__(256) k_gs_sweep(int nlev, const int *__restrict__ lptr,
+                                                  const int *__restrict__ perm,
+                                                  const int *__restrict__ rp,
+                                                  const int *__restrict__ ci,
+                                                  const T *__restrict__ va,
+                                                  const T *__restrict__ invd,
+                                                  const T *__restrict__ t, T *x,
+                                                  const T *__restrict__ relax, i64 brows,
+                                                  unsigned *bar, int *err) {
+    constexpr int TPR = Shape<T, NV>::TPR;
+    const int stride = gridDim.x * 256;
+    for (int l = 0; l < nlev; ++l) {
+        int lo = __ldg(lptr + l), hi = __ldg(lptr + l + 1);
+        int items = (hi - lo) * TPR;
+        for (int it = blockIdx.x * 256 + threadIdx.x; it < items; it += stride)
+            gs_row<T, NV>(__ldg(perm + lo + it / TPR), it % TPR, rp, ci, va, invd, t, x, relax, brows);
+        if (l + 1 < nlev) {
+            __threadfence();
+            if (!grid_sync(bar, err)) return;
+        }
+    }
+}
+
+template <class T, int NV>
+static cudaError_t gs_sweep_t(int nlev, const int *lptr, const int *perm, const int *rp,
+                              const int *ci, const T *va, const T *invd, const T *t, T *x,
+                              const T *relax, i64 brows, unsigned *bar, int *err, cudaStream_t s) {
+    static int nblk = 0;
+    if (nblk == 0) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_gs_sweep<T, NV>, 256, 0);
+        if (per < 1) per = 1;
+        if (per > 2) per = 2;
+        nblk = sms * per;
+    }
+    void *args[] = {&nlev, &lptr, &perm, &rp, &ci, &va, &invd, &t, &x, &relax, &brows, &bar, &err};
+    return cudaLaunchCooperativeKernel((const void *)k_gs_sweep<T, NV>, dim3(nblk), dim3(256),
+                                       args, 0, s);
+}
+
+cudaError_t gs_sweep_persistent(Prec p, int nv, int nlev, const int *lptr, const int *perm,
+                                const int *rp, const int *ci, const void *val, const void *invd,
+                                const void *t, void *x, const void *relax, i64 brows,
+                                unsigned *bar, int *err, cudaStream_t s) {
+    cudaError_t e = cudaErrorInvalidValue;
+    if (p == Prec::F64) {
+#define F(NV) e = gs_sweep_t<double, NV>(nlev, lptr, perm, rp, ci, (const double *)val, (const double *)invd, (const double *)t, (double *)x, (const double *)relax, brows, bar, err, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    } else {
+#define F(NV) e = gs_sweep_t<float, NV>(nlev, lptr, perm, rp, ci, (const float *)val, (const float *)invd, (const float *)t, (float *)x, (const float *)relax, brows, bar, err, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    }
+    return e;
+}
+
+// t = 1*b + (-1)*(off-block part of A x)
+template <class T, int NV>
+__global__ void __launch_bounds__(256) k_offblock(i64 n, const int *__restrict__ rp,
+                                                  const int *__restrict__ ci,
+                                                  const T *__restrict__ va,
+                                                  const T *__restrict__ b,
+                                                  const T *__restrict__ x, T *__restrict__ t,
+                                                  i64 brows) {
+    constexpr int V = Shape<T, NV>::V, TPR = Shape<T, NV>::TPR, RPB = 256 / TPR;
+    i64 row = (i64)blockIdx.x * RPB + threadIdx.x / TPR;
+    int lane = threadIdx.x % TPR;
+    if (row >= n) return;
+    i64 lo = (row / brows) * brows, hi = lo + brows;
+    T acc[V];
+#pragma unroll
+    for (int e = 0; e < V; ++e) acc[e] = T(0);
+    const T *xb = x + lane * V;
+    for (int j = __ldg(rp + row), j1 = __ldg(rp + row + 1); j < j1; ++j) {
+        int c = __ldg(ci + j);
+        if (c >= lo && c < hi) continue;
+        T v = __ldg(va + j);
+        T xv[V];
+        ld<T, V>(xb + (i64)c * NV, xv);
+#pragma unroll
+        for (int e = 0; e < V; ++e) acc[e] = fma(v, xv[e], acc[e]);
+    }
+    T bb[V];
+    ld<T, V>(b + row * NV + lane * V, bb);
+#pragma unroll
+    for (int e = 0; e < V; ++e) acc[e] = add_rn<T>(mul_rn<T>(T(1), bb[e]), mul_rn<T>(T(-1), acc[e]));
+    st<T, V>(t + row * NV + lane * V, acc);
+}
+
+void offblock_resid(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val,
+                    const void *b, const void *x, void *t, i64 brows, cudaStream_t s) {
+    if (n <= 0) return;
+    if (p == Prec::F64) {
+#define F(NV) k_offblock<double, NV><<<(unsigned)((n + 256 / Shape<double, NV>::TPR - 1) / (256 / Shape<double, NV>::TPR)), 256, 0, s>>>(n, rp, ci, (const double *)val, (const double *)b, (const double *)x, (double *)t, brows)
+        NV_DISPATCH(nv, F)
+#undef F
+    } else {
+#define F(NV) k_offblock<float, NV><<<(unsigned)((n + 256 / Shape<float, NV>::TPR - 1) / (256 / Shape<float, NV>::TPR)), 256, 0, s>>>(n, rp, ci, (const float *)val, (const float *)b, (const float *)x, (float *)t, brows)
+        NV_DISPATCH(nv, F)
+#undef F
+    }
+}
+
+// ---------------------------------------------------------------- Jacobi
+template <class T, int NV>
+__global__ void __launch_bounds__(256) k_jacobi(i64 n, const int *__restrict__ rp,
+                                                const int *__restrict__ ci,
+                                                const T *__restrict__ va,
+                                                const T *__restrict__ invd,
+                                                const T *__restrict__ b,
+                                                const T *__restrict__ xi, T *__restrict__ xo,
+                                                const T *__restrict__ relax) {
+    constexpr int V = Shape<T, NV>::V, TPR = Shape<T, NV>::TPR, RPB = 256 / TPR;
+    i64 row = (i64)blockIdx.x * RPB + threadIdx.x / TPR;
+    int lane = threadIdx.x % TPR;
+    if (row >= n) return;
+    T acc[V];
+#pragma unroll
+    for (int e = 0; e < V; ++e) acc[e] = T(0);
+    const T *xb = xi + lane * V;
+    for (int j = __ldg(rp + row), j1 = __ldg(rp + row + 1); j < j1; ++j) {
+        int c = __ldcs(ci + j);
+        T v = __ldcs(va + j);
+        T xv[V];
+        ld<T, V>(xb + (i64)c * NV, xv);
+#pragma unroll
+        for (int e = 0; e < V; ++e) acc[e] = fma(v, xv[e], acc[e]);
+    }
+    T bb[V], xx[V];
+    ld<T, V>(b + row * NV + lane * V, bb);
+    ld<T, V>(xi + row * NV + lane * V, xx);
+    T di = __ldg(invd + row);
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+        T cf = mul_rn<T>(__ldg(relax + lane * V + e), di);
+        T d = add_rn<T>(bb[e], -acc[e]);
+        xx[e] = fma(cf, d, xx[e]);
+    }
+    st<T, V>(xo + row * NV + lane * V, xx);
+}
+
+void jacobi(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val,
+            const void *invd, const void *b, const void *xi, void *xo, const void *relax,
+            cudaStream_t s) {
+    if (n <= 0) return;
+    if (p == Prec::F64) {
+#define F(NV) k_jacobi<double, NV><<<(unsigned)((n + 256 / Shape<double, NV>::TPR - 1) / (256 / Shape<double, NV>::TPR)), 256, 0, s>>>(n, rp, ci, (const double *)val, (const double *)invd, (const double *)b, (const double *)xi, (double *)xo, (const double *)relax)
+        NV_DISPATCH(nv, F)
+#undef F
+    } else {
+#define F(NV) k_jacobi<float, NV><<<(unsigned)((n + 256 / Shape<float, NV>::TPR - 1) / (256 / Shape<float, NV>::TPR)), 256, 0, s>>>(n, rp, ci, (const float *)val, (const float *)invd, (const float *)b, (const float *)xi, (float *)xo, (const float *)relax)
+        NV_DISPATCH(nv, F)
+#undef F
+    }
+}
+
+// ---------------------------------------------------------------- dense
+// thread (i, k): y[i,k] = sum_j AinvT[j*n + i] * b[j*nv + k], j ascending, fma
+template <class T>
+__global__ void __launch_bounds__(256) k_dense(int n, int nv, const T *__restrict__ AT,
+                                               const T *__restrict__ b, T *__restrict__ y) {
+    i64 idx = (i64)blockIdx.x * 256 + threadIdx.x;
+    if (idx >= (i64)n * nv) return;
+    int i = (int)(idx % n), k = (int)(idx / n);
+    T s = T(0);
+    for (int j = 0; j < n; ++j) s = fma(__ldg(AT + (i64)j * n + i), __ldg(b + (i64)j * nv + k), s);
+    y[(i64)i * nv + k] = s;
+}
+
+void dense_gemv(Prec p, int nv, int n, const void *AinvT, const void *b, void *y, cudaStream_t s) {
+    i64 tot = (i64)n * nv;
+    if (tot <= 0) return;
+    unsigned g = (unsigned)((tot + 255) / 256);
+    if (p == Prec::F64) k_dense<double><<<g, 256, 0, s>>>(n, nv, (const double *)AinvT, (const double *)b, (double *)y);
+    else k_dense<float><<<g, 256, 0, s>>>(n, nv, (const float *)AinvT, (const float *)b, (float *)y);
+}
+
+// ---------------------------------------------------------------- dots
+// Stage 1: one warp per 256-row chunk; lane l accumulates rows l, l+32, ...,
+// l+224 (fma, FP64), then a xor-butterfly over the 32 lanes (off = 16..1),
+// whose lane-0 value equals the pairwise tree s[l] += s[l+off].
+// Partials are stored dot-major: part[(d*nv + k) * nchunks + c].
+template <class TI, int NV, int ND>
+__global__ void __launch_bounds__(256) k_dot1(i64 n, i64 nch, const TI *__restrict__ a0,
+                                              const TI *__restrict__ b0,
+                                              const TI *__restrict__ a1,
+                                              const TI *__restrict__ b1,
+                                              const TI *__restrict__ a2,
+                                              const TI *__restrict__ b2, double *__restrict__ part) {
+    const int lane = threadIdx.x & 31;
+    const i64 c = (i64)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (c >= nch) return;
+    const TI *A[3] = {a0, a1, a2};
+    const TI *B[3] = {b0, b1, b2};
+    double acc[ND][NV];
+#pragma unroll
+    for (int d = 0; d < ND; ++d)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[d][k] = 0.0;
+    constexpr int V = Shape<TI, NV>::V;
+#pragma unroll 1
+    for (int m = 0; m < 8; ++m) {
+        i64 i = c * 256 + 32 * m + lane;
+        if (i < n) {
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+#pragma unroll
+                for (int k0 = 0; k0 < NV; k0 += V) {
+                    TI xa[V], xb[V];
+                    ld<TI, V>(A[d] + i * NV + k0, xa);
+                    ld<TI, V>(B[d] + i * NV + k0, xb);
+#pragma unroll
+                    for (int e = 0; e < V; ++e)
+                        acc[d][k0 + e] = fma((double)xa[e], (double)xb[e], acc[d][k0 + e]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < ND; ++d)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double v = acc[d][k];
+#pragma unroll
+            for (int off = 16; off >= 1; off >>= 1) v = dadd(v, __shfl_xor_sync(0xffffffffu, v, off));
+            if (lane == 0) part[((i64)d * NV + k) * nch + c] = v;
+        }
+}
+
+// Stage 2: block (d,k): slot t sums chunks t, t+256, ... in order from 0, then
+// the 256 slots fold pairwise (off = 128..1).
+__global__ void __launch_bounds__(256) k_dot2(i64 nch, const double *__restrict__ part,
+                                              double *__restrict__ out) {
+    __shared__ double q[256];
+    const double *p = part + (i64)blockIdx.x * nch;
+    double a = 0.0;
+    for (i64 c = threadIdx.x; c < nch; c += 256) a = dadd(a, p[c]);
+    q[threadIdx.x] = a;
+    __syncthreads();
+    for (int off = 128; off >= 32; off >>= 1) {
+        if (threadIdx.x < off) q[threadIdx.x] = dadd(q[threadIdx.x], q[threadIdx.x + off]);
+        __syncthreads();
+    }
+    if (threadIdx.x < 32) {
+        double v = q[threadIdx.x];
+        for (int off = 16; off >= 1; off >>= 1) v = dadd(v, __shfl_xor_sync(0xffffffffu, v, off));
+        if (threadIdx.x == 0) out[blockIdx.x] = v;
+    }
+}
+
+i64 dot_part_size(i64 n, int nd, int nv) { return ((n + 255) / 256) * nd * nv; }
+
+template <class TI, int NV>
+static void dots_t(i64 n, int nd, const void *const *a, const void *const *b, double *part,
+                   double *out, cudaStream_t s) {
+    i64 nch = (n + 255) / 256;
+    if (nch == 0) {
+        cudaMemsetAsync(out, 0, sizeof(double) * nd * NV, s);
+        return;
+    }
+    unsigned g = (unsigned)((nch + 7) / 8);
+    const TI *A0 = (const TI *)a[0], *B0 = (const TI *)b[0];
+    const TI *A1 = nd > 1 ? (const TI *)a[1] : A0, *B1 = nd > 1 ? (const TI *)b[1] : B0;
+    const TI *A2 = nd > 2 ? (const TI *)a[2] : A0, *B2 = nd > 2 ? (const TI *)b[2] : B0;
+    if (nd == 1) k_dot1<TI, NV, 1><<<g, 256, 0, s>>>(n, nch, A0, B0, A1, B1, A2, B2, part);
+    else if (nd == 2) k_dot1<TI, NV, 2><<<g, 256, 0, s>>>(n, nch, A0, B0, A1, B1, A2, B2, part);
+    else k_dot1<TI, NV, 3><<<g, 256, 0, s>>>(n, nch, A0, B0, A1, B1, A2, B2, part);
+    k_dot2<<<nd * NV, 256, 0, s>>>(nch, part, out);
+}
+
+void dots(Prec in, int nv, i64 n, int nd, const void *const *a, const void *const *b,
+          double *part, double *out, cudaStream_t s) {
+    if (in == Prec::F64) {
+#define F(NV) dots_t<double, NV>(n, nd, a, b, part, out, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    } else {
+#define F(NV) dots_t<float, NV>(n, nd, a, b, part, out, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    }
+}
+
+// ---------------------------------------------------------------- BLAS-1
+// Literal evaluation in FP64 with every product rounded (no contraction); FP32
+// storage is widened on load and rounded once on store.
+template <class T, int NV, int OP>
+__global__ void __launch_bounds__(256) k_blas(i64 total, const double *__restrict__ a,
+                                              const T *__restrict__ x,
+                                              const double *__restrict__ b,
+                                              const T *__restrict__ y,
+                                              const double *__restrict__ c, T *__restrict__ z) {
+    i64 q = (i64)blockIdx.x * 256 + threadIdx.x;
+    if (q >= total) return;
+    int k = (int)(q % NV);
+    double r;
+    if (OP == (int)Op::AXPBY_Z) {
+        r = dadd(dmul(a[k], (double)x[q]), dmul(b[k], (double)y[q]));
+    } else if (OP == (int)Op::AXPBYPCZ) {
+        r = dadd(dadd(dmul(a[k], (double)x[q]), dmul(b[k], (double)y[q])), dmul(c[k], (double)z[q]));
+    } else if (OP == (int)Op::AX_Y) {
+        r = dmul(a[k], (double)x[q]);
+    } else if (OP == (int)Op::COPY) {
+        r = (double)x[q];
+    } else if (OP == (int)Op::SET) {
+        r = a[k];
+    } else {  // SCAL_XY
+        r = dmul((double)z[q], (double)x[q]);
+    }
+    z[q] = (T)r;
+}
+
+template <class T, int NV>
+static void blas_t(i64 n, Op op, const double *a, const T *x, const double *b, const T *y,
+                   const double *c, T *z, cudaStream_t s) {
+    i64 tot = n * NV;
+    if (tot <= 0) return;
+    unsigned g = (unsigned)((tot + 255) / 256);
+    switch (op) {
+    case Op::AXPBY_Z: k_blas<T, NV, 0><<<g, 256, 0, s>>>(tot, a, x, b, y, c, z); break;
+    case Op::AXPBYPCZ: k_blas<T, NV, 1><<<g, 256, 0, s>>>(tot, a, x, b, y, c, z); break;
+    case Op::AX_Y: k_blas<T, NV, 2><<<g, 256, 0, s>>>(tot, a, x, b, y, c, z); break;
+    case Op::COPY: k_blas<T, NV, 3><<<g, 256, 0, s>>>(tot, a, x, b, y, c, z); break;
+    case Op::SET: k_blas<T, NV, 4><<<g, 256, 0, s>>>(tot, a, x, b, y, c, z); break;
+    case Op::SCAL_XY: k_blas<T, NV, 5><<<g, 256, 0, s>>>(tot, a, x, b, y, c, z); break;
+    }
+}
+
+void blas(Prec p, int nv, i64 n, Op op, const double *a, const void *x, const double *b,
+          const void *y, const double *c, void *z, cudaStream_t s) {
+    if (p == Prec::F64) {
+#define F(NV) blas_t<double, NV>(n, op, a, (const double *)x, b, (const double *)y, c, (double *)z, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    } else {
+#define F(NV) blas_t<float, NV>(n, op, a, (const float *)x, b, (const float *)y, c, (float *)z, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    }
+}
+
+template <class T>
+__global__ void k_fill(i64 cnt, T v, T *z) {
+    i64 q = (i64)blockIdx.x * 256 + threadIdx.x;
+    if (q < cnt) z[q] = v;
+}
+void fill(Prec p, i64 count, double v, void *z, cudaStream_t s) {
+    if (count <= 0) return;
+    unsigned g = (unsigned)((count + 255) / 256);
+    if (p == Prec::F64) k_fill<double><<<g, 256, 0, s>>>(count, v, (double *)z);
+    else k_fill<float><<<g, 256, 0, s>>>(count, (float)v, (float *)z);
+}
+
+template <class A, class B>
+__global__ void k_conv(i64 cnt, const A *x, B *y) {
+    i64 q = (i64)blockIdx.x * 256 + threadIdx.x;
+    if (q < cnt) y[q] = (B)x[q];
+}
+void convert(Prec from, Prec to, i64 count, const void *x, void *y, cudaStream_t s) {
+    if (count <= 0) return;
+    unsigned g = (unsigned)((count + 255) / 256);
+    if (from == Prec::F64 && to == Prec::F32) k_conv<double, float><<<g, 256, 0, s>>>(count, (const double *)x, (float *)y);
+    else if (from == Prec::F32 && to == Prec::F64) k_conv<float, double><<<g, 256, 0, s>>>(count, (const float *)x, (double *)y);
+    else if (from == Prec::F64) k_conv<double, double><<<g, 256, 0, s>>>(count, (const double *)x, (double *)y);
+    else k_conv<float, float><<<g, 256, 0, s>>>(count, (const float *)x, (float *)y);
+}
+
+// ---------------------------------------------------------------- scalars
+__global__ void k_alpha(int nv, const double *rho, const double *s1, double *alpha) {
+    int k = threadIdx.x;
+    if (k < nv) alpha[k] = __ddiv_rn(rho[k], s1[k]);
+}
+void bicg_alpha(int nv, const double *rho, const double *s1, double *alpha, cudaStream_t s) {
+    k_alpha<<<1, 32, 0, s>>>(nv, rho, s1, alpha);
+}
+__global__ void k_omega(int nv, const double *s2, const double *s3, const double *s4,
+                        const double *alpha, const double *iconv, double *omega, double *res,
+                        double *ac, double *oc) {
+    int k = threadIdx.x;
+    if (k >= nv) return;
+    double w = __ddiv_rn(s2[k], s3[k]);
+    omega[k] = w;
+    ac[k] = dmul(iconv[k], alpha[k]);
+    oc[k] = dmul(iconv[k], w);
+    double rr = dmul(w, s2[k]);
+    res[k] = dadd(dmul(1.0, s4[k]), dmul(-1.0, rr));
+}
+void bicg_omega(int nv, const double *s2, const double *s3, const double *s4,
+                const double *alpha, const double *iconv, double *omega, double *res,
+                double *ac, double *oc, cudaStream_t s) {
+    k_omega<<<1, 32, 0, s>>>(nv, s2, s3, s4, alpha, iconv, omega, res, ac, oc);
+}
+__global__ void k_beta(int nv, const double *s1, double *rho, const double *alpha,
+                       const double *omega, double *beta, double *c1) {
+    int k = threadIdx.x;
+    if (k >= nv) return;
+    double a2 = __ddiv_rn(s1[k], rho[k]);
+    double a3 = __ddiv_rn(alpha[k], omega[k]);
+    double bt = dmul(a2, a3);
+    beta[k] = bt;
+    rho[k] = s1[k];
+    c1[k] = dmul(-1.0, dmul(omega[k], bt));
+}
+void bicg_beta(int nv, const double *s1, double *rho, const double *alpha, const double *omega,
+               double *beta, double *c1, cudaStream_t s) {
+    k_beta<<<1, 32, 0, s>>>(nv, s1, rho, alpha, omega, beta, c1);
+}
+__global__ void k_neg(int nv, const double *in, double *out) {
+    int k = threadIdx.x;
+    if (k < nv) out[k] = dmul(-1.0, in[k]);
+}
+void negate(int nv, const double *in, double *out, cudaStream_t s) { k_neg<<<1, 32, 0, s>>>(nv, in, out); }
+
+}  // namespace xk

@@ -1,0 +1,94 @@
+// Device kernels of the XAMG solve phase (sm_100a).  Host-callable launchers.
+//
+// Data layout (same as the reference, csr_matvec.inl:224-229):
+//   block vectors are row-major N x NV: element (i, k) at x[i*NV + k];
+//   CSR matrices use int32 row pointers and column indices and FP64 or FP32
+//   values; per-column scalars (alpha, omega, ...) are NV doubles on device.
+// Arithmetic contract (identical to the CPU oracle, bit for bit):
+//   * CSR/dense row sums: acc = fma(a_ij, x_j, acc) in stored order;
+//   * Gauss-Seidel: sum = fma(-a_ij, x_j, sum); x_i = fma(relax*invdiag_i, sum, x_i);
+//   * BLAS-1: literal left-to-right evaluation, every product rounded;
+//   * inner products: the fixed chunk/lane/slot tree (see dot kernels).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+typedef int64_t i64;
+
+namespace xk {
+
+enum class Prec : int { F64 = 0, F32 = 1 };
+
+// ---- sparse matrix-vector products ---------------------------------------
+// y = A x (mode 0), y += A x (mode 1), y = b - A x (mode 2, b given).
+void spmv(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val, const void *x,
+          void *y, int mode, const void *b, cudaStream_t s);
+
+// ---- Gauss-Seidel sweeps ----------------------------------------------------
+// One wavefront level: rows[0..cnt) are independent and updated in place.
+// brows > 0 restricts each row to the columns of its own hybrid block
+// [ (i/brows)*brows, +brows ); brows == 0 uses the whole row.
+void gs_level(Prec p, int nv, int cnt, const int *rows, const int *rp, const int *ci,
+              const void *val, const void *invd, const void *t, void *x, const void *relax,
+              i64 brows, cudaStream_t s);
+
+// Whole sweep inside one cooperative persistent launch; level l covers
+// perm[lptr[l] .. lptr[l+1]).  Waits between levels are bounded: on timeout
+// *err is set and the kernel returns early.
+cudaError_t gs_sweep_persistent(Prec p, int nv, int nlev, const int *lptr, const int *perm,
+                                const int *rp, const int *ci, const void *val, const void *invd,
+                                const void *t, void *x, const void *relax, i64 brows,
+                                unsigned *bar, int *err, cudaStream_t s);
+
+// Hybrid Gauss-Seidel right-hand side: t = 1*b + (-1)*(sum over the entries
+// outside the row's block of a_ij x_j)   (blas2.h:226-259)
+void offblock_resid(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val,
+                    const void *b, const void *x, void *t, i64 brows, cudaStream_t s);
+
+// ---- Jacobi ---------------------------------------------------------------
+// xo = fma(relax_k * invd_i, b - A xi, xi)   (xi, xo distinct)
+void jacobi(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val,
+            const void *invd, const void *b, const void *xi, void *xo, const void *relax,
+            cudaStream_t s);
+
+// ---- dense coarse solve: y = Ainv b, AinvT stored transposed (n x n) --------
+void dense_gemv(Prec p, int nv, int n, const void *AinvT, const void *b, void *y, cudaStream_t s);
+
+// ---- inner products -------------------------------------------------------
+// nd pairs (a_d, b_d) of N x NV vectors (element type `in`), FP64 results
+// out[d*nv + k].  part must hold dot_part_size(n, nd, nv) doubles.
+i64 dot_part_size(i64 n, int nd, int nv);
+void dots(Prec in, int nv, i64 n, int nd, const void *const *a, const void *const *b,
+          double *part, double *out, cudaStream_t s);
+
+// ---- BLAS-1 (element type T, FP64 per-column scalars) ---------------------
+enum class Op : int {
+    AXPBY_Z = 0,   // z = a*x + b*y
+    AXPBYPCZ = 1,  // z = a*x + b*y + c*z
+    AX_Y = 2,      // z = a*x
+    COPY = 3,      // z = x
+    SET = 4,       // z = a
+    SCAL_XY = 5,   // z = z * x   (elementwise)
+};
+void blas(Prec p, int nv, i64 n, Op op, const double *a, const void *x, const double *b,
+          const void *y, const double *c, void *z, cudaStream_t s);
+
+// constant fill with a host value (set_const with a scalar)
+void fill(Prec p, i64 count, double v, void *z, cudaStream_t s);
+// element conversion
+void convert(Prec from, Prec to, i64 count, const void *x, void *y, cudaStream_t s);
+
+// ---- BiCGStab scalar recurrences (one thread per column, FP64) -------------
+// alpha = rho / s1
+void bicg_alpha(int nv, const double *rho, const double *s1, double *alpha, cudaStream_t s);
+// omega = s2/s3; res = 1*s4 + (-1)*(omega*s2); ac = iconv*alpha; oc = iconv*omega
+void bicg_omega(int nv, const double *s2, const double *s3, const double *s4,
+                const double *alpha, const double *iconv, double *omega, double *res,
+                double *ac, double *oc, cudaStream_t s);
+// beta = (s1/rho)*(alpha/omega); rho = s1; c1 = -(omega*beta); also -alpha, -omega
+void bicg_beta(int nv, const double *s1, double *rho, const double *alpha, const double *omega,
+               double *beta, double *c1, cudaStream_t s);
+// negate: out = -1 * in
+void negate(int nv, const double *in, double *out, cudaStream_t s);
+
+}  // namespace xk

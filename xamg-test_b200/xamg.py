@@ -1,0 +1,430 @@
+"""ctypes binding of libxamg_b200.so (the XAMG C API and the kernel interface).
+
+The classes mirror the reference's C API objects (api/c/xamg_c_api.h): Params,
+CsrMatrix, Matrix, Vector and Solver own one handle each.  The library must be
+built (build.py); importing this module on a machine with a GPU and no built
+library raises instead of falling back to anything else.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libxamg_b200.so")
+
+_lib = None
+
+F64, F32 = 0, 1
+MEM_LOCAL, MEM_SHARED, MEM_DISTRIBUTED = 0, 1, 2
+
+
+class XamgError(RuntimeError):
+    pass
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise XamgError("libxamg_b200.so is not built; run xamg-test_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        sz = C.c_size_t
+        P = C.c_void_p
+        i64 = C.c_int64
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        sig = {
+            "XAMG_init": (C.c_int, [C.c_int, P, C.c_char_p]),
+            "XAMG_finalize": (C.c_int, []),
+            "XAMG_get_nv": (C.c_int, []),
+            "XAMG_param_create": (C.c_int, [C.POINTER(sz)]),
+            "XAMG_param_add_value_s": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, sz]),
+            "XAMG_param_add_value_i": (C.c_int, [C.c_char_p, C.c_char_p, C.c_uint32, sz]),
+            "XAMG_param_add_value_d": (C.c_int, [C.c_char_p, C.c_char_p, C.c_double, sz]),
+            "XAMG_param_add_value_b": (C.c_int, [C.c_char_p, C.c_char_p, C.c_uint8, sz]),
+            "XAMG_param_change_value_d": (C.c_int, [C.c_char_p, C.c_char_p, C.c_double, sz]),
+            "XAMG_param_change_value_i": (C.c_int, [C.c_char_p, C.c_char_p, C.c_uint32, sz]),
+            "XAMG_param_override_create": (C.c_int, [C.POINTER(sz)]),
+            "XAMG_param_override_add_value": (C.c_int, [C.c_char_p, C.c_char_p, sz]),
+            "XAMG_param_override_apply": (C.c_int, [C.c_char_p, sz, sz]),
+            "XAMG_param_override_destroy": (C.c_int, [sz]),
+            "XAMG_param_set_default": (None, [sz]),
+            "XAMG_param_print": (C.c_int, [sz]),
+            "XAMG_param_destroy": (C.c_int, [sz]),
+            "XAMG_part_create": (C.c_int, [C.POINTER(sz)]),
+            "XAMG_part_construct": (C.c_int, [C.c_int, sz]),
+            "XAMG_part_get_numa_size": (C.c_int, [sz]),
+            "XAMG_vector_create": (C.c_int, [C.POINTER(sz), C.c_int]),
+            "XAMG_vector_offset": (C.c_int, [C.c_uint64, sz]),
+            "XAMG_vector_alloc_d": (C.c_int, [C.c_int, C.c_uint16, sz]),
+            "XAMG_vector_set_part": (C.c_int, [sz, sz]),
+            "XAMG_vector_set_val_d": (C.c_int, [C.c_double, sz]),
+            "XAMG_vector_download_d": (C.c_int, [P, C.c_uint64, C.c_uint64, C.c_uint16, sz]),
+            "XAMG_vector_upload_v": (C.c_int, [sz, sz]),
+            "XAMG_vector_upload_d": (C.c_int, [P, C.c_uint64, C.c_uint64, C.c_uint16, sz]),
+            "XAMG_vector_destroy": (C.c_int, [sz]),
+            "XAMG_csr_matrix_create": (C.c_int, [C.POINTER(sz)]),
+            "XAMG_csr_matrix_alloc": (C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, sz]),
+            "XAMG_csr_matrix_fill": (C.c_int, [P, P, P, sz]),
+            "XAMG_csr_matrix_get_nrows": (C.c_uint32, [sz]),
+            "XAMG_csr_matrix_destroy": (C.c_int, [sz]),
+            "XAMG_matrix_create": (C.c_int, [C.POINTER(sz)]),
+            "XAMG_matrix_set_part": (C.c_int, [sz, sz]),
+            "XAMG_matrix_construct": (C.c_int, [sz, sz]),
+            "XAMG_matrix_destroy": (C.c_int, [sz]),
+            "XAMG_solver_create1": (C.c_int, [sz, sz, C.POINTER(sz)]),
+            "XAMG_solver_create2": (C.c_int, [sz, sz, sz, sz, C.POINTER(sz)]),
+            "XAMG_solver_renew_params": (C.c_int, [sz, sz]),
+            "XAMG_solver_solve1": (C.c_int, [C.c_uint16, sz]),
+            "XAMG_solver_solve2": (C.c_int, [C.c_uint16, sz, sz, sz]),
+            "XAMG_solver_print_info": (C.c_int, [sz]),
+            "XAMG_solver_get_convergence_info": (C.c_int, [ip, C.c_uint16, sz]),
+            "XAMG_solver_get_iter_info": (C.c_int, [ip, sz]),
+            "XAMG_solver_destroy": (C.c_int, [sz]),
+            "XAMG_timer": (C.c_double, []),
+            "XAMG_barrier": (C.c_int, []),
+            "XAMG_b200_set_nv": (C.c_int, [C.c_int]),
+            "XAMG_b200_last_error": (C.c_char_p, []),
+            "XAMG_b200_synchronize": (C.c_int, []),
+            "XAMG_b200_vector_device_ptr": (P, [sz]),
+            "XAMG_b200_solver_get_residual_history": (C.c_int, [dp, C.c_int, sz]),
+            "XAMG_b200_solver_get_res0": (C.c_int, [dp, sz]),
+            "XAMG_b200_solver_last_solve_ms": (C.c_double, [sz]),
+            "XAMG_b200_solver_num_levels": (C.c_int, [sz]),
+            "XAMG_b200_solver_level_info": (C.c_int, [C.POINTER(i64), C.c_int, sz]),
+            "XAMG_b200_solver_export_level": (C.c_int, [P, P, P, P, P, P, C.c_int, sz]),
+            "XAMG_b200_solver_export_gs_levels": (C.c_int, [P, P, C.c_int, sz]),
+            "XAMG_b200_solver_export_coarse_inverse": (C.c_int, [P, sz]),
+            "XAMG_b200_solver_info": (C.c_int, [C.c_char_p, C.c_int, sz]),
+            "XAMG_b200_csr_matrix_generate": (C.c_int, [C.c_int, P, P, P, sz]),
+            "XAMG_b200_csr_matrix_get_nnz": (i64, [sz]),
+            "XAMG_b200_csr_matrix_export": (C.c_int, [P, P, P, sz]),
+            "XAMG_b200_csr_matrix_read_bin": (C.c_int, [C.c_char_p, P, P, sz]),
+            "XAMG_b200_csr_matrix_write_bin": (C.c_int, [C.c_char_p, P, P, sz]),
+            "XAMG_b200_amg_host_create": (C.c_int, [sz, sz, C.POINTER(sz)]),
+            "XAMG_b200_amg_host_num_levels": (C.c_int, [sz]),
+            "XAMG_b200_amg_host_level_info": (C.c_int, [C.POINTER(i64), C.c_int, sz]),
+            "XAMG_b200_amg_host_export_level": (C.c_int, [P, P, P, P, P, P, C.c_int, sz]),
+            "XAMG_b200_amg_host_destroy": (C.c_int, [sz]),
+            "XAMG_b200_gs_levels_host": (C.c_int, [i64, P, P, i64, P, P, P]),
+            "xamg_csr_spmv": (C.c_int, [C.c_int, C.c_int, i64, P, P, P, P, P, C.c_int, P, P]),
+            "xamg_gs_plan_create": (P, [i64, P, P, i64, C.c_int]),
+            "xamg_gs_plan_levels": (C.c_int, [P, P, P, P]),
+            "xamg_gs_plan_error": (C.c_int, [P]),
+            "xamg_gs_plan_destroy": (None, [P]),
+            "xamg_hsgs": (C.c_int, [P, C.c_int, C.c_int, P, P, P, P, P, P, P, P, P]),
+            "xamg_jacobi": (C.c_int, [C.c_int, C.c_int, i64, P, P, P, P, P, P, P, P, P]),
+            "xamg_dot_part_size": (i64, [i64, C.c_int, C.c_int]),
+            "xamg_dot": (C.c_int, [C.c_int, C.c_int, i64, C.c_int, P, P, P, P, P]),
+            "xamg_blas": (C.c_int, [C.c_int, C.c_int, i64, C.c_int, P, P, P, P, P, P, P]),
+            "xamg_dense_gemv": (C.c_int, [C.c_int, C.c_int, C.c_int, P, P, P, P]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != 0:
+        raise XamgError("xamg error %d: %s" % (rc, lib().XAMG_b200_last_error().decode()))
+    return rc
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def init(nv=1):
+    check(lib().XAMG_init(0, None, b""))
+    check(lib().XAMG_b200_set_nv(nv))
+
+
+def set_nv(nv):
+    check(lib().XAMG_b200_set_nv(nv))
+
+
+class Params:
+    """Parameter dictionary (roles/keys of the reference)."""
+
+    def __init__(self, spec=None, overrides=None):
+        h = C.c_size_t()
+        check(lib().XAMG_param_create(C.byref(h)))
+        self.h = h.value
+        for role, kv in (spec or {}).items():
+            for k, v in kv.items():
+                self.add(role, k, v)
+        for role, kv in (overrides or {}).items():
+            o = C.c_size_t()
+            check(lib().XAMG_param_override_create(C.byref(o)))
+            for k, v in kv.items():
+                check(lib().XAMG_param_override_add_value(k.encode(), str(v).encode(), o.value))
+            check(lib().XAMG_param_override_apply(role.encode(), self.h, o.value))
+            check(lib().XAMG_param_override_destroy(o.value))
+        lib().XAMG_param_set_default(self.h)
+
+    def add(self, role, key, v):
+        r, k = role.encode(), key.encode()
+        if isinstance(v, bool):
+            check(lib().XAMG_param_add_value_b(r, k, int(v), self.h))
+        elif isinstance(v, int):
+            check(lib().XAMG_param_add_value_i(r, k, v, self.h))
+        elif isinstance(v, float):
+            check(lib().XAMG_param_add_value_d(r, k, v, self.h))
+        else:
+            check(lib().XAMG_param_add_value_s(r, k, str(v).encode(), self.h))
+
+    def change(self, role, key, v):
+        if isinstance(v, float):
+            check(lib().XAMG_param_change_value_d(role.encode(), key.encode(), v, self.h))
+        else:
+            check(lib().XAMG_param_change_value_i(role.encode(), key.encode(), int(v), self.h))
+
+
+class CsrMatrix:
+    """Host CSR matrix object (XAMG_csr_matrix_*)."""
+
+    def __init__(self):
+        h = C.c_size_t()
+        check(lib().XAMG_csr_matrix_create(C.byref(h)))
+        self.h = h.value
+
+    @classmethod
+    def from_arrays(cls, rp, ci, v):
+        m = cls()
+        rp = np.ascontiguousarray(rp, dtype=np.int32)
+        ci = np.ascontiguousarray(ci, dtype=np.int32)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        n = len(rp) - 1
+        check(lib().XAMG_csr_matrix_alloc(n, n, len(ci), m.h))
+        check(lib().XAMG_csr_matrix_fill(_ptr(rp), _ptr(ci), _ptr(v), m.h))
+        return m
+
+    @classmethod
+    def cube(cls, nx, ny, nz, config=0):
+        m = cls()
+        ia = np.array([nx, ny, nz, config], dtype=np.int64)
+        check(lib().XAMG_b200_csr_matrix_generate(0, _ptr(ia), None, None, m.h))
+        return m
+
+    @classmethod
+    def aniso27(cls, n, kx=1.0, ky=1.0, kz=1e-3):
+        m = cls()
+        ia = np.array([n], dtype=np.int64)
+        da = np.array([kx, ky, kz], dtype=np.float64)
+        check(lib().XAMG_b200_csr_matrix_generate(1, _ptr(ia), _ptr(da), None, m.h))
+        return m
+
+    @classmethod
+    def faces7(cls, nx, ny, nz, kx, ky, kz):
+        m = cls()
+        ia = np.array([nx, ny, nz], dtype=np.int64)
+        f = np.ascontiguousarray(np.concatenate([np.ravel(kx), np.ravel(ky), np.ravel(kz)]), dtype=np.float64)
+        assert f.size == (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1)
+        check(lib().XAMG_b200_csr_matrix_generate(2, _ptr(ia), None, _ptr(f), m.h))
+        return m
+
+    @classmethod
+    def read_bin(cls, path):
+        m = cls()
+        check(lib().XAMG_b200_csr_matrix_read_bin(path.encode(), None, None, m.h))
+        n = m.nrows
+        b = np.zeros(n)
+        x = np.zeros(n)
+        check(lib().XAMG_b200_csr_matrix_read_bin(path.encode(), _ptr(b), _ptr(x), m.h))
+        return m, b, x
+
+    @property
+    def nrows(self):
+        return lib().XAMG_csr_matrix_get_nrows(self.h)
+
+    @property
+    def nnz(self):
+        return lib().XAMG_b200_csr_matrix_get_nnz(self.h)
+
+    def arrays(self):
+        n, nnz = self.nrows, self.nnz
+        rp = np.zeros(n + 1, np.int32)
+        ci = np.zeros(nnz, np.int32)
+        v = np.zeros(nnz, np.float64)
+        check(lib().XAMG_b200_csr_matrix_export(_ptr(rp), _ptr(ci), _ptr(v), self.h))
+        return rp, ci, v
+
+    def __del__(self):
+        try:
+            lib().XAMG_csr_matrix_destroy(self.h)
+        except Exception:
+            pass
+
+
+class Matrix:
+    """Device matrix (XAMG_matrix_*), built from a CsrMatrix."""
+
+    def __init__(self, csr):
+        h = C.c_size_t()
+        check(lib().XAMG_matrix_create(C.byref(h)))
+        self.h = h.value
+        check(lib().XAMG_matrix_construct(csr.h, self.h))
+        self.n = csr.nrows
+
+    def __del__(self):
+        try:
+            lib().XAMG_matrix_destroy(self.h)
+        except Exception:
+            pass
+
+
+class Vector:
+    """Block vector n x nv (device-resident unless mode == MEM_LOCAL)."""
+
+    def __init__(self, n, nv, mode=MEM_DISTRIBUTED):
+        h = C.c_size_t()
+        check(lib().XAMG_vector_create(C.byref(h), mode))
+        self.h = h.value
+        self.n, self.nv = n, nv
+        check(lib().XAMG_vector_alloc_d(n, nv, self.h))
+
+    def upload(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(self.n, self.nv)
+        check(lib().XAMG_vector_upload_d(_ptr(a), self.n, 0, self.nv, self.h))
+
+    def download(self, out=None):
+        out = np.empty((self.n, self.nv)) if out is None else out
+        check(lib().XAMG_vector_download_d(_ptr(out), self.n, 0, self.nv, self.h))
+        return out
+
+    def set(self, v):
+        check(lib().XAMG_vector_set_val_d(float(v), self.h))
+
+    @property
+    def device_ptr(self):
+        return lib().XAMG_b200_vector_device_ptr(self.h)
+
+    def __del__(self):
+        try:
+            lib().XAMG_vector_destroy(self.h)
+        except Exception:
+            pass
+
+
+class Solver:
+    """Solver tree (XAMG_solver_create2 / solve / stats)."""
+
+    def __init__(self, A, params, x=None, b=None):
+        h = C.c_size_t()
+        if x is None:
+            check(lib().XAMG_solver_create1(A.h, params.h, C.byref(h)))
+        else:
+            check(lib().XAMG_solver_create2(A.h, params.h, x.h, b.h, C.byref(h)))
+        self.h = h.value
+        self.A, self.params, self.x, self.b = A, params, x, b
+
+    def solve(self, x=None, b=None):
+        nv = lib().XAMG_get_nv()
+        if x is None:
+            check(lib().XAMG_solver_solve1(nv, self.h))
+        else:
+            check(lib().XAMG_solver_solve2(nv, x.h, b.h, self.h))
+
+    def renew(self, params):
+        check(lib().XAMG_solver_renew_params(params.h, self.h))
+
+    def iters(self):
+        it = (C.c_int * 2)()
+        check(lib().XAMG_solver_get_iter_info(it, self.h))
+        return it[0], it[1]
+
+    def converged(self):
+        nv = lib().XAMG_get_nv()
+        c = (C.c_int * nv)()
+        check(lib().XAMG_solver_get_convergence_info(c, nv, self.h))
+        return [bool(v) for v in c]
+
+    def history(self):
+        nv = lib().XAMG_get_nv()
+        cap = 100000
+        buf = np.zeros(cap * nv)
+        cnt = lib().XAMG_b200_solver_get_residual_history(buf.ctypes.data_as(C.POINTER(C.c_double)), cap, self.h)
+        return buf[: cnt * nv].reshape(cnt, nv)
+
+    def last_ms(self):
+        return lib().XAMG_b200_solver_last_solve_ms(self.h)
+
+    def info(self):
+        buf = C.create_string_buffer(4096)
+        check(lib().XAMG_b200_solver_info(buf, 4096, self.h))
+        return buf.value.decode()
+
+    def num_levels(self):
+        return lib().XAMG_b200_solver_num_levels(self.h)
+
+    def level(self, l):
+        info = (C.c_int64 * 6)()
+        check(lib().XAMG_b200_solver_level_info(info, l, self.h))
+        n, nnz, ncP, nnzP, nlf, nlb = list(info)
+        rpA = np.zeros(n + 1, np.int32)
+        ciA = np.zeros(nnz, np.int32)
+        vA = np.zeros(nnz)
+        rpP = np.zeros(n + 1, np.int32) if nnzP else None
+        ciP = np.zeros(nnzP, np.int32) if nnzP else None
+        vP = np.zeros(nnzP) if nnzP else None
+        check(lib().XAMG_b200_solver_export_level(_ptr(rpA), _ptr(ciA), _ptr(vA), _ptr(rpP), _ptr(ciP), _ptr(vP), l, self.h))
+        return dict(n=n, A=(rpA, ciA, vA), P=(rpP, ciP, vP) if nnzP else None, ncP=ncP, nlev=(nlf, nlb))
+
+    def gs_levels(self, l):
+        n = self.level(l)["n"]
+        lf = np.zeros(n, np.int32)
+        lb = np.zeros(n, np.int32)
+        check(lib().XAMG_b200_solver_export_gs_levels(_ptr(lf), _ptr(lb), l, self.h))
+        return lf, lb
+
+    def coarse_inverse(self):
+        L = self.num_levels()
+        n = self.level(L - 1)["n"]
+        out = np.zeros((n, n))
+        check(lib().XAMG_b200_solver_export_coarse_inverse(_ptr(out), self.h))
+        return out
+
+    def __del__(self):
+        try:
+            lib().XAMG_solver_destroy(self.h)
+        except Exception:
+            pass
+
+
+def amg_host(csr, params):
+    """Host-only AMG setup; returns the level list (A, P arrays) like Solver.level."""
+    h = C.c_size_t()
+    check(lib().XAMG_b200_amg_host_create(csr.h, params.h, C.byref(h)))
+    out = []
+    try:
+        for l in range(lib().XAMG_b200_amg_host_num_levels(h.value)):
+            info = (C.c_int64 * 4)()
+            check(lib().XAMG_b200_amg_host_level_info(info, l, h.value))
+            n, nnz, ncP, nnzP = list(info)
+            rpA, ciA, vA = np.zeros(n + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
+            rpP = np.zeros(n + 1, np.int32) if nnzP else None
+            ciP = np.zeros(nnzP, np.int32) if nnzP else None
+            vP = np.zeros(nnzP) if nnzP else None
+            check(lib().XAMG_b200_amg_host_export_level(_ptr(rpA), _ptr(ciA), _ptr(vA), _ptr(rpP), _ptr(ciP), _ptr(vP), l, h.value))
+            out.append(dict(n=n, A=(rpA, ciA, vA), P=(rpP, ciP, vP) if nnzP else None, ncP=ncP))
+    finally:
+        lib().XAMG_b200_amg_host_destroy(h.value)
+    return out
+
+
+def gs_levels_host(rp, ci, block_rows=0):
+    n = len(rp) - 1
+    lf = np.zeros(n, np.int32)
+    lb = np.zeros(n, np.int32)
+    nl = np.zeros(2, np.int32)
+    check(lib().XAMG_b200_gs_levels_host(n, _ptr(np.ascontiguousarray(rp, np.int32)), _ptr(np.ascontiguousarray(ci, np.int32)), block_rows, _ptr(lf), _ptr(lb), _ptr(nl)))
+    return lf, lb, tuple(nl)
+
+
+def device_ptr(t):
+    """Device pointer of a torch tensor (or None)."""
+    return None if t is None else C.c_void_p(t.data_ptr())
