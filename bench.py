@@ -122,35 +122,54 @@ def build_problem():
     return csr, B
 
 
-def spmv_roofline(csr, iters=20):
-    """Live CUDA-event timing of the FP64 NV=16 CSR SpMV on the benchmark
-    matrix, launched on a torch stream through the C ABI."""
+def spmv_time(csr, prec=0, variant=-1, iters=20):
+    """Live CUDA-event timing of the NV=16 CSR SpMV on the benchmark matrix,
+    launched on a torch stream through the C ABI; returns ms per launch."""
     import ctypes as C
     import torch
     import xamg
     rp, ci, v = csr.arrays()
-    n, nnz = csr.nrows, len(ci)
-    d = [torch.from_numpy(a).cuda() for a in (rp, ci, v)]
-    x = torch.rand(n, NV, dtype=torch.float64, device="cuda")
+    n = csr.nrows
+    dt = torch.float64 if prec == 0 else torch.float32
+    d = [torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), torch.from_numpy(v).to(dt).cuda()]
+    x = torch.rand(n, NV, dtype=dt, device="cuda")
     y = torch.empty_like(x)
     st = torch.cuda.Stream()
     P = lambda t: C.c_void_p(t.data_ptr())
     torch.cuda.synchronize()
     L = xamg.lib()
+    old = L.xamg_spmv_set_variant(variant)
     with torch.cuda.stream(st):
         for _ in range(3):
-            L.xamg_csr_spmv(0, NV, n, P(d[0]), P(d[1]), P(d[2]), P(x), P(y), 0, None, C.c_void_p(st.cuda_stream))
+            L.xamg_csr_spmv(prec, NV, n, P(d[0]), P(d[1]), P(d[2]), P(x), P(y), 0, None, C.c_void_p(st.cuda_stream))
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
         for _ in range(iters):
-            L.xamg_csr_spmv(0, NV, n, P(d[0]), P(d[1]), P(d[2]), P(x), P(y), 0, None, C.c_void_p(st.cuda_stream))
+            L.xamg_csr_spmv(prec, NV, n, P(d[0]), P(d[1]), P(d[2]), P(x), P(y), 0, None, C.c_void_p(st.cuda_stream))
         e1.record(st)
     st.synchronize()
-    ms = e0.elapsed_time(e1) / iters
+    L.xamg_spmv_set_variant(old)
+    return e0.elapsed_time(e1) / iters
+
+
+def tune_spmv(csr, prec=0):
+    """Autotune the SpMV kernel variant on this matrix (results are identical
+    for every variant; only the launch shape differs)."""
+    res = {}
+    for var in (0, -1, 1, 2, 4, 8, 16):
+        res[var] = spmv_time(csr, prec, var, iters=10)
+    best = min(res, key=res.get)
+    return best, res
+
+
+def spmv_roofline(csr, variant):
+    ms = spmv_time(csr, 0, variant, iters=20)
+    n, nnz = csr.nrows, csr.nnz
     byts = nnz * (8 + 4) + (n + 1) * 4 + 2 * n * NV * 8
     peak, src = peak_hbm()
     ach = byts / (ms * 1e-3) / 1e9
-    return {"bound": "hbm", "kernel": "k_spmv<double,16,0>", "achieved": round(ach, 1), "peak": peak,
+    kern = "k_spmv<double,16,0>" if variant == 0 else "k_spmv_stream<double,16,0>"
+    return {"bound": "hbm", "kernel": kern, "variant": variant, "achieved": round(ach, 1), "peak": peak,
             "peak_source": src, "unit": "GB/s", "frac": round(ach / peak, 4),
             "traffic": None, "algorithmic_bytes": byts, "launch_ms": round(ms, 4)}
 
@@ -278,6 +297,8 @@ def main():
     import xamg
     xamg.init(NV)
     csr, B = build_problem()
+    best_var, var_ms = tune_spmv(csr, 0)
+    xamg.lib().xamg_spmv_set_variant(best_var)
     forms = args.forms.split(",")
     res = {}
     keep = {}
@@ -302,7 +323,8 @@ def main():
     best = min(forms, key=lambda f: res[f]["ms"])
     spec_best = plain_spec() if best == "plain" else mixed_spec()
     e2e_ms = e2e_form(csr, B, spec_best, 1, max(2, args.steps // 2))
-    roof = spmv_roofline(csr)
+    roof = spmv_roofline(csr, best_var)
+    roof["variants_ms"] = {str(k): round(v, 4) for k, v in var_ms.items()}
     err = None
     if "plain" in X and "mixed" in X:
         err = float(np.linalg.norm(X["mixed"] - X["plain"]) / np.linalg.norm(X["plain"]))

@@ -86,13 +86,19 @@ int XAMG_b200_gs_levels_host(int64_t n, const int *rp, const int *ci, int64_t bl
  * mode 0: y = A x; 1: y += A x; 2: y = b - A x. */
 int xamg_csr_spmv(int prec, int nv, int64_t n, const int *rp, const int *ci, const void *val,
                   const void *x, void *y, int mode, const void *b, void *stream);
+/* Kernel variant used by every CSR product of the library (same results):
+ * 0 = one CTA per row tile; k > 0 = shared-memory staged streaming kernel
+ * walking k tiles per CTA; -1 = automatic.  Returns the previous setting. */
+int xamg_spmv_set_variant(int variant);
 
 /* Gauss-Seidel plan (wavefront schedule) for blas2::SGS / csr_SGS
  * (blas2.h:184-281, csr_gs.inl:32-134).  rp/ci are HOST arrays.  block_rows
  * = 0 gives the single-process sweep; > 0 the hybrid block semantics.
- * persistent = 1 runs each sweep as one cooperative launch. */
+ * schedule: 0 = one launch per wavefront level; 1 = automatic (one
+ * cooperative launch per sweep with a bounded grid barrier per level, or one
+ * CTA per block for hybrid plans); 2 = cooperative grid sweep always. */
 void *xamg_gs_plan_create(int64_t n, const int *rp_host, const int *ci_host,
-                          int64_t block_rows, int persistent);
+                          int64_t block_rows, int schedule);
 int xamg_gs_plan_levels(void *plan, int *nlev /* [2] */, int *lf, int *lb);
 int xamg_gs_plan_error(void *plan);
 void xamg_gs_plan_destroy(void *plan);

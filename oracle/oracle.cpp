@@ -476,6 +476,56 @@ int pbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
     return it;
 }
 
+// Precision form: FP64 iterative refinement (IterativeRefinement::solve,
+// ir.inl:107-194 with subsolver_reduced_precision) around an FP32 PBiCGStab
+// whose inner products and alpha/beta/omega recurrences stay in FP64, with an
+// FP32 V-cycle.  The inner tolerance per column is the outer tolerance, or
+// inner_rel times the current outer residual norm when that is larger.
+int ir_pbicgstab(const Csr &A, const MG &mg, const double *b, double *x, int nv, int max_outer,
+                 int max_inner, double abs_tol, double rel_tol, double inner_rel, Conv &cv,
+                 Hist &hist, int &sub_iters) {
+    i64 n = A.n;
+    size_t sz = (size_t)n * nv;
+    std::vector<double> r(sz), xc(sz), d(nv);
+    std::vector<float> ib(sz), ix(sz);
+    cv.nv = nv;
+    cv.abs_tol = abs_tol;
+    cv.rel_tol = rel_tol;
+    cv.res0.assign(nv, 0);
+    cv.res.assign(nv, 0);
+    cv.status.assign(nv, 0);
+    sub_iters = 0;
+    auto residual = [&]() {
+        spmv<double>(n, A.rp.data(), A.ci.data(), A.v64.data(), x, r.data(), nv, 0);
+        for (size_t q = 0; q < sz; ++q) r[q] = 1.0 * b[q] + (-1.0) * r[q];
+        dot_canonical<double, double>(n, nv, r.data(), r.data(), d.data());
+    };
+    residual();
+    for (int k = 0; k < nv; ++k) cv.res0[k] = d[k];
+    cv.update(d.data());
+    hist.push(cv.res, nv);
+    if (cv.check()) return 0;
+    int it = 0;
+    for (it = 1; it <= max_outer; ++it) {
+        Conv in;
+        in.ptol.resize(nv);
+        for (int k = 0; k < nv; ++k)
+            in.ptol[k] = std::max(cv.tol(k), inner_rel * std::sqrt(std::max(d[k], 0.0)));
+        for (size_t q = 0; q < sz; ++q) { ib[q] = (float)r[q]; ix[q] = 0.f; }
+        Hist ih{nullptr, 0};
+        sub_iters += pbicgstab<float>(A, &mg, ib.data(), ix.data(), nv, max_inner, in, ih);
+        for (size_t q = 0; q < sz; ++q) {
+            xc[q] = (double)ix[q];
+            x[q] = 1.0 * xc[q] + 1.0 * x[q];
+        }
+        residual();
+        cv.update(d.data());
+        hist.push(cv.res, nv);
+        if (cv.check()) return it;
+    }
+    return max_outer;
+}
+
 }  // namespace orc
 
 using namespace orc;
@@ -630,6 +680,23 @@ int orc_pbicgstab_d(i64 n, const int *rp, const int *ci, const double *v, void *
         status[k] = cv.status[k];
         res0[k] = cv.res0[k];
     }
+    return it;
+}
+
+// Precision form (see ir_pbicgstab).  mg must have been finalised with fp32=1.
+int orc_ir_pbicgstab(i64 n, const int *rp, const int *ci, const double *v, void *mg,
+                     const double *b, double *x, int nv, int max_outer, int max_inner,
+                     double abs_tol, double rel_tol, double inner_rel, double *hist, int hist_cap,
+                     int *status, int *sub_iters) {
+    Csr A;
+    fill(A, n, n, rp, ci, v);
+    Conv cv;
+    Hist H{hist, hist_cap};
+    int si = 0;
+    int it = ir_pbicgstab(A, *(MG *)mg, b, x, nv, max_outer, max_inner, abs_tol, rel_tol, inner_rel,
+                          cv, H, si);
+    for (int k = 0; k < nv; ++k) status[k] = cv.status[k];
+    *sub_iters = si;
     return it;
 }
 

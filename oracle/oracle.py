@@ -199,3 +199,22 @@ def pbicgstab(rp, ci, v, b, x0, mg=None, max_iters=1000, abs_tol=0.0, rel_tol=1e
     it = lib().orc_pbicgstab_d(n, p(rp), p(ci), p(v), mg.h if mg is not None else None, p(b), p(x), nv,
                                max_iters, abs_tol, rel_tol, p(hist), cap, p(status), p(res0))
     return x, it, hist[: it + 1], status, res0
+
+
+def ir_pbicgstab(rp, ci, v, b, x0, mg, max_outer=20, max_inner=200, abs_tol=0.0, rel_tol=1e-8,
+                 inner_rel=1e-4):
+    """Precision form: FP64 refinement around FP32 PBiCGStab + FP32 V-cycle
+    (mg built with fp32=True).  Returns (x, outer_iters, history, status, sub_iters)."""
+    n, nv = b.shape
+    x = np.array(x0, dtype=np.float64, copy=True)
+    cap = max_outer + 2
+    hist = np.zeros((cap, nv))
+    status = np.zeros(nv, np.int32)
+    sub = np.zeros(1, np.int32)
+    f = lib().orc_ir_pbicgstab
+    f.restype = C.c_int
+    f.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                  C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    it = f(n, p(rp), p(ci), p(v), mg.h, p(b), p(x), nv, max_outer, max_inner, abs_tol, rel_tol, inner_rel,
+           p(hist), cap, p(status), p(sub))
+    return x, it, hist[: it + 1], status, int(sub[0])

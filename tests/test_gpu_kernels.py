@@ -14,9 +14,23 @@ pytestmark = pytest.mark.gpu
 NVS = [1, 2, 4, 8, 16, 32]
 
 
+_alive = []
+
+
 def D(a):
+    """Device copy of a host array.  Every copy is kept alive until the next
+    test starts, so a pointer handed to the library never dangles."""
     import torch
-    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    t = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    _alive.append(t)
+    return t
+
+
+@pytest.fixture(autouse=True)
+def _release_device_copies():
+    yield
+    sync()
+    _alive.clear()
 
 
 def P(t):
@@ -48,19 +62,25 @@ def test_spmv_bit_exact(gpu, dtype, nv):
     prec = 0 if dtype == np.float64 else 1
     drp, dci, dv, dx, db = D(rp), D(ci), D(v), D(x), D(b)
     L = xamg.lib()
-    for mode in (0, 1, 2):
-        dy = D(y0)
-        sync()
-        xamg.check(L.xamg_csr_spmv(prec, nv, n, P(drp), P(dci), P(dv), P(dx), P(dy), mode, P(db), None))
-        got = H(dy)
-        if mode == 0:
-            ref = orc.spmv(rp, ci, v, x, nv)
-        elif mode == 1:
-            ref = orc.spmv(rp, ci, v, x, nv, y=y0.copy(), acc=True)
-        else:
-            ref = orc.spmv(rp, ci, v, x, nv)
-            ref = (dtype(1) * b + dtype(-1) * ref).astype(dtype)
-        assert np.array_equal(got, ref), (mode, np.abs(got - ref).max())
+    old = L.xamg_spmv_set_variant(-1)
+    try:
+        for variant in (0, -1, 1, 3):
+            L.xamg_spmv_set_variant(variant)
+            for mode in (0, 1, 2):
+                dy = D(y0)
+                sync()
+                xamg.check(L.xamg_csr_spmv(prec, nv, n, P(drp), P(dci), P(dv), P(dx), P(dy), mode, P(db), None))
+                got = H(dy)
+                if mode == 0:
+                    ref = orc.spmv(rp, ci, v, x, nv)
+                elif mode == 1:
+                    ref = orc.spmv(rp, ci, v, x, nv, y=y0.copy(), acc=True)
+                else:
+                    ref = orc.spmv(rp, ci, v, x, nv)
+                    ref = (dtype(1) * b + dtype(-1) * ref).astype(dtype)
+                assert np.array_equal(got, ref), (variant, mode, np.abs(got - ref).max())
+    finally:
+        L.xamg_spmv_set_variant(old)
 
 
 def test_spmv_large_checksum(gpu):
@@ -135,14 +155,14 @@ def _gs_case(rng, kind, n=500):
 
 @pytest.mark.parametrize("kind", ["dd", "27pt"])
 @pytest.mark.parametrize("block_rows", [0, 64])
-@pytest.mark.parametrize("persistent", [1, 0])
+@pytest.mark.parametrize("schedule", [0, 1, 2])
 @pytest.mark.parametrize("nv", [1, 4, 16])
-def test_hsgs_bit_exact(gpu, kind, block_rows, persistent, nv):
+def test_hsgs_bit_exact(gpu, kind, block_rows, schedule, nv):
     rng = np.random.default_rng(21)
     rp, ci, v = _gs_case(rng, kind)
     n = len(rp) - 1
     L = xamg.lib()
-    plan = L.xamg_gs_plan_create(n, xamg._ptr(rp), xamg._ptr(ci), block_rows, persistent)
+    plan = L.xamg_gs_plan_create(n, xamg._ptr(rp), xamg._ptr(ci), block_rows, schedule)
     assert plan
     try:
         for dtype, prec in ((np.float64, 0), (np.float32, 1)):

@@ -145,3 +145,28 @@ def test_nonconvergence_and_bad_input_report(gpu):
     assert s.iters()[0] == 3 and not any(s.converged())
     L = xamg.lib()
     assert L.XAMG_solver_solve1(2, s.h) == 2  # nv mismatch is an error code, not an abort
+
+
+@pytest.mark.parametrize("block_rows", [0, 576])
+def test_precision_form_parity(gpu, block_rows):
+    """FP64 refinement around the FP32 PBiCGStab / FP32 V-cycle: identical
+    outer and inner iteration counts and residual history as the oracle."""
+    csr = xamg.CsrMatrix.aniso27(24)
+    rp, ci, v = csr.arrays()
+    rng = np.random.default_rng(5)
+    B = rng.uniform(-1, 1, (csr.nrows, 4))
+    spec = util.amg_params(max_levels=6, block_rows=block_rows, max_iters=200,
+                           meta={"method": "IterativeRefinement", "max_iters": 20, "abs_tolerance": 0.0,
+                                 "rel_tolerance": 1e-8, "subsolver_reduced_precision": True,
+                                 "inner_rel_tolerance": 1e-4, "convergence_details": "check-L2,noprint"})
+    s, X, keep = solve_api(csr, spec, B)
+    levels = [s.level(l) for l in range(s.num_levels())]
+    mg = orc.MG(levels, fp32=True, block_rows=block_rows)
+    xo, it, hist, st, sub = orc.ir_pbicgstab(rp, ci, v, B, np.zeros_like(B), mg, 20, 200, 0.0, 1e-8, 1e-4)
+    assert s.iters() == (it, sub)
+    assert_same_history(s.history(), hist)
+    np.testing.assert_allclose(X, xo, rtol=1e-12, atol=1e-14 * np.abs(xo).max())
+    assert st.all() and all(s.converged())
+    # error against an FP64 solve of the same system
+    xp, _, _, _, _ = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), orc.MG(levels), 200, 0.0, 1e-10)
+    assert np.linalg.norm(X - xp) / np.linalg.norm(xp) < 1e-6

@@ -721,8 +721,13 @@ int xamg_csr_spmv(int prec, int nv, int64_t n, const int *rp, const int *ci, con
         XCUDA(cudaGetLastError());
     });
 }
+int xamg_spmv_set_variant(int variant) {
+    int old = xk::get_spmv_variant();
+    xk::set_spmv_variant(variant);
+    return old;
+}
 void *xamg_gs_plan_create(int64_t n, const int *rp, const int *ci, int64_t block_rows,
-                          int persistent) {
+                          int schedule) {
     PlanHandle *h = nullptr;
     int rc = guard([&] {
         ctx();
@@ -731,7 +736,8 @@ void *xamg_gs_plan_create(int64_t n, const int *rp, const int *ci, int64_t block
         A.rp.assign(rp, rp + n + 1);
         A.ci.assign(ci, ci + rp[n]);
         h = new PlanHandle();
-        h->plan.build(A, block_rows, persistent != 0);
+        GsMode md = schedule == 0 ? GsMode::LEVELS : (schedule == 2 ? GsMode::GRID : gs_mode_from("auto", block_rows, n));
+        h->plan.build(A, block_rows, md);
     });
     if (rc) { delete h; return nullptr; }
     return h;

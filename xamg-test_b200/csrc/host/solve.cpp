@@ -111,11 +111,51 @@ void gs_levels_host(const HostCsr &A, i64 brows, std::vector<int> &lf, std::vect
     }
 }
 
-void GsPlan::build(const HostCsr &A, i64 brows_, bool persistent_) {
+GsMode gs_mode_from(const std::string &s, i64 brows, i64 n) {
+    bool hybrid = brows > 0 && brows < n;
+    if (s == "levels") return GsMode::LEVELS;
+    if (s == "grid" || s == "persistent") return GsMode::GRID;
+    if (s == "blocks") return hybrid ? GsMode::BLOCKS : GsMode::GRID;
+    return hybrid ? GsMode::BLOCKS : GsMode::GRID;  // auto
+}
+
+static void upload_ints(DBuf &d, const std::vector<int> &h) {
+    d.alloc(sizeof(int) * std::max<size_t>(h.size(), 1));
+    if (!h.empty()) XCUDA(cudaMemcpy(d.p, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
+}
+
+void GsPlan::build(const HostCsr &A, i64 brows_, GsMode mode_) {
     n = A.n;
-    brows = brows_;
-    persistent = persistent_;
+    brows = brows_ > 0 && brows_ < A.n ? brows_ : 0;
+    mode = mode_;
+    if (mode == GsMode::BLOCKS && brows == 0) mode = GsMode::GRID;
     gs_levels_host(A, brows, lf, lb);
+    if (mode == GsMode::BLOCKS) {
+        // rows of each block in (level, row) order; levels of block b are the
+        // consecutive entries [blev[b], blev[b+1]) of lptr
+        nblocks = (int)((n + brows - 1) / brows);
+        auto bsched = [&](const std::vector<int> &lev, DBuf &dblev, DBuf &dlptr, DBuf &dperm) {
+            std::vector<int> blev(nblocks + 1, 0), lptr, perm(n);
+            lptr.push_back(0);
+            for (int b = 0; b < nblocks; ++b) {
+                i64 r0 = (i64)b * brows, r1 = std::min<i64>(n, r0 + brows);
+                int nl = 0;
+                for (i64 i = r0; i < r1; ++i) nl = std::max(nl, lev[i] + 1);
+                std::vector<int> cnt(nl + 1, 0);
+                for (i64 i = r0; i < r1; ++i) cnt[lev[i] + 1]++;
+                for (int l = 0; l < nl; ++l) cnt[l + 1] += cnt[l];
+                std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+                for (i64 i = r0; i < r1; ++i) perm[r0 + pos[lev[i]]++] = (int)i;
+                for (int l = 0; l < nl; ++l) lptr.push_back((int)(r0 + cnt[l + 1]));
+                blev[b + 1] = blev[b] + nl;
+            }
+            upload_ints(dblev, blev);
+            upload_ints(dlptr, lptr);
+            upload_ints(dperm, perm);
+        };
+        bsched(lf, bblevf, blptrf, bpermf);
+        bsched(lb, bblevb, blptrb, bpermb);
+    }
     auto sched = [&](const std::vector<int> &lev, std::vector<int> &lptr, DBuf &dperm, DBuf &dlptr) {
         int nl = 0;
         for (i64 i = 0; i < n; ++i) nl = std::max(nl, lev[i] + 1);
@@ -143,7 +183,14 @@ void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val
     const std::vector<int> &hl = forward ? hlf : hlb;
     const int *perm = (forward ? permf : permb).as<int>();
     if (nl == 0) return;
-    if (persistent && nl > 2) {
+    if (mode == GsMode::BLOCKS) {
+        if (forward)
+            xk::gs_blocks(p, nv, nblocks, bblevf.as<int>(), blptrf.as<int>(), bpermf.as<int>(),
+                          bblevb.as<int>(), blptrb.as<int>(), bpermb.as<int>(), rp, ci, val, invd, t,
+                          x, relax, brows, s);
+        return;
+    }
+    if (mode == GsMode::GRID && nl > 2) {
         unsigned *bar = sync.as<unsigned>();
         int *err = (int *)(bar + 2);
         XCUDA(xk::gs_sweep_persistent(p, nv, nl, (forward ? lptrf : lptrb).as<int>(), perm,
@@ -465,12 +512,13 @@ struct MultiGrid : Solver {
         op.invd = m.prec == Prec::F64 ? m.invd64.p : m.invd32.p;
         if (meth == "HSGS") {
             i64 br = pl.has("hybrid_block_rows") ? (i64)pl.get_int("hybrid_block_rows") : 0;
-            bool pers = !pl.has("gs_schedule") || pl.get_string("gs_schedule") != "levels";
+            GsMode md = gs_mode_from(pl.has("gs_schedule") ? pl.get_string("gs_schedule") : "auto", br, hA.n);
             GsPlan &g = pre ? m.gs_pre : m.gs_post;
-            if (!pre && m.gs_pre.n == hA.n && m.gs_pre.brows == br && m.gs_pre.persistent == pers) {
+            i64 brn = br > 0 && br < hA.n ? br : 0;
+            if (!pre && m.gs_pre.n == hA.n && m.gs_pre.brows == brn && m.gs_pre.mode == md) {
                 op.gs = &m.gs_pre;
             } else {
-                g.build(hA, br, pers);
+                g.build(hA, br, md);
                 op.gs = &g;
             }
             auto h = std::unique_ptr<HSGS>(new HSGS());
@@ -796,7 +844,7 @@ static std::unique_ptr<Solver> make_solver(const GlobalParams &gp, const std::st
         op.invd = prec == Prec::F64 ? o->invd64.p : o->invd32.p;
         if (m == "HSGS") {
             i64 br = pl.has("hybrid_block_rows") ? (i64)pl.get_int("hybrid_block_rows") : 0;
-            o->gs.build(A.h, br, !pl.has("gs_schedule") || pl.get_string("gs_schedule") != "levels");
+            o->gs.build(A.h, br, gs_mode_from(pl.has("gs_schedule") ? pl.get_string("gs_schedule") : "auto", br, A.h.n));
             op.gs = &o->gs;
             auto h = std::unique_ptr<HSGS>(new HSGS());
             h->role = role; h->method = m; h->prm = pl; h->nv = nv; h->prec = prec;

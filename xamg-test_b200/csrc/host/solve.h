@@ -48,19 +48,30 @@ struct DCsr {
 
 // Wavefront schedule of the forward and backward Gauss-Seidel sweeps of one
 // matrix (optionally restricted to hybrid blocks of `brows` rows).
+// Sweep schedules: LEVELS launches one kernel per wavefront level; GRID runs
+// a whole sweep in one cooperative launch with a bounded grid barrier per
+// level; BLOCKS (hybrid plans only) runs each block in its own CTA with CTA
+// barriers, both sweeps in one launch.
+enum class GsMode : int { LEVELS = 0, GRID = 1, BLOCKS = 2 };
+
 struct GsPlan {
     i64 n = 0, brows = 0;
     int nlf = 0, nlb = 0;
+    int nblocks = 1;
+    GsMode mode = GsMode::GRID;
     std::vector<int> hlf, hlb;         // level pointers (host)
     std::vector<int> lf, lb;           // per-row levels (host, for export)
-    DBuf permf, permb, lptrf, lptrb;   // device copies
+    DBuf permf, permb, lptrf, lptrb;   // device copies (global level order)
+    DBuf bblevf, bblevb, blptrf, blptrb, bpermf, bpermb;  // per-block order (BLOCKS)
     DBuf sync;                         // barrier words + error flag
-    bool persistent = true;
-    void build(const HostCsr &A, i64 brows_, bool persistent_);
+    void build(const HostCsr &A, i64 brows_, GsMode mode_);
+    // forward (or backward) sweep; in BLOCKS mode the forward call runs both
+    // sweeps and the backward call does nothing
     void sweep(Prec p, int nv, const int *rp, const int *ci, const void *val, const void *invd,
                const void *t, void *x, const void *relax, bool forward, cudaStream_t s);
     int error_flag() const;
 };
+GsMode gs_mode_from(const std::string &s, i64 brows, i64 n);
 
 // Convergence bookkeeping, convergence.h:48-303 with conv_check/print flags.
 struct Conv {

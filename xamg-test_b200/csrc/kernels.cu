@@ -13,6 +13,7 @@
 //    to the oracle.
 #include "kernels.cuh"
 #include <cooperative_groups.h>
+#include <algorithm>
 #include <cstdio>
 
 namespace xk {
@@ -134,15 +135,113 @@ __global__ void __launch_bounds__(256) k_spmv(i64 n, const int *__restrict__ rp,
     st<T, V>(y + row * NV + lane * V, acc);
 }
 
+// Streaming variant: a tile of RPB rows has its CSR entries copied into shared
+// memory with coalesced loads (when they fit), then every row is summed from
+// shared memory with its x gathers issued GB at a time.  Each CTA walks `tpc`
+// consecutive tiles, so the x rows of the stencil neighbourhood stay in L1
+// between tiles.  Same per-row summation order as k_spmv.
+template <class T, int NV, int MODE>
+__global__ void __launch_bounds__(256) k_spmv_stream(i64 n, int tpc, const int *__restrict__ rp,
+                                                     const int *__restrict__ ci,
+                                                     const T *__restrict__ va,
+                                                     const T *__restrict__ x, T *__restrict__ y,
+                                                     const T *__restrict__ b) {
+    constexpr int V = Shape<T, NV>::V, TPR = Shape<T, NV>::TPR, RPB = 256 / TPR, GB = 8;
+    constexpr int EMAX = sizeof(T) == 8 ? 2048 : 3072;
+    __shared__ int s_c[EMAX];
+    __shared__ T s_v[EMAX];
+    const int lane = threadIdx.x % TPR;
+    const i64 ntiles = (n + RPB - 1) / RPB;
+    for (i64 tile = (i64)blockIdx.x * tpc, te = min(ntiles, tile + tpc); tile < te; ++tile) {
+        const i64 r0 = tile * RPB, r1 = min(n, r0 + RPB);
+        const int e0 = __ldg(rp + r0), cnt = __ldg(rp + r1) - e0;
+        const bool staged = cnt <= EMAX;
+        if (staged) {
+            for (int q = threadIdx.x; q < cnt; q += 256) {
+                s_c[q] = __ldcs(ci + e0 + q);
+                s_v[q] = __ldcs(va + e0 + q);
+            }
+            __syncthreads();
+        }
+        const i64 row = r0 + threadIdx.x / TPR;
+        if (row < r1) {
+            T acc[V];
+            if (MODE == 1) {
+                ld<T, V>(y + row * NV + lane * V, acc);
+            } else {
+#pragma unroll
+                for (int e = 0; e < V; ++e) acc[e] = T(0);
+            }
+            const int j0 = __ldg(rp + row), j1 = __ldg(rp + row + 1);
+            const T *xb = x + lane * V;
+            for (int j = j0; j < j1; j += GB) {
+                int c[GB];
+                T v[GB];
+#pragma unroll
+                for (int k = 0; k < GB; ++k) {
+                    bool ok = j + k < j1;
+                    c[k] = ok ? (staged ? s_c[j + k - e0] : __ldcs(ci + j + k)) : 0;
+                    v[k] = ok ? (staged ? s_v[j + k - e0] : __ldcs(va + j + k)) : T(0);
+                }
+                T xv[GB][V];
+#pragma unroll
+                for (int k = 0; k < GB; ++k)
+                    if (j + k < j1) ld<T, V>(xb + (i64)c[k] * NV, xv[k]);
+#pragma unroll
+                for (int k = 0; k < GB; ++k)
+                    if (j + k < j1) {
+#pragma unroll
+                        for (int e = 0; e < V; ++e) acc[e] = fma(v[k], xv[k][e], acc[e]);
+                    }
+            }
+            if (MODE == 2) {
+                T bb[V];
+                ld<T, V>(b + row * NV + lane * V, bb);
+#pragma unroll
+                for (int e = 0; e < V; ++e) acc[e] = add_rn<T>(mul_rn<T>(T(1), bb[e]), mul_rn<T>(T(-1), acc[e]));
+            }
+            st<T, V>(y + row * NV + lane * V, acc);
+        }
+        if (staged) __syncthreads();
+    }
+}
+
+// SpMV variant selection: 0 = row kernel, >0 = streaming kernel with that
+// many tiles per CTA; <0 = automatic (streaming, about 8 CTAs per SM).
+static int g_spmv_variant = -1;
+void set_spmv_variant(int v) { g_spmv_variant = v; }
+int get_spmv_variant() { return g_spmv_variant; }
+
+static int sm_count() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
 template <class T, int NV>
 static void spmv_t(i64 n, const int *rp, const int *ci, const T *va, const T *x, T *y, int mode,
                    const T *b, cudaStream_t s) {
     constexpr int RPB = 256 / Shape<T, NV>::TPR;
     if (n <= 0) return;
-    unsigned g = (unsigned)((n + RPB - 1) / RPB);
-    if (mode == 0) k_spmv<T, NV, 0><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
-    else if (mode == 1) k_spmv<T, NV, 1><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
-    else k_spmv<T, NV, 2><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
+    i64 ntiles = (n + RPB - 1) / RPB;
+    int var = g_spmv_variant;
+    if (var == 0) {
+        unsigned g = (unsigned)ntiles;
+        if (mode == 0) k_spmv<T, NV, 0><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
+        else if (mode == 1) k_spmv<T, NV, 1><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
+        else k_spmv<T, NV, 2><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
+        return;
+    }
+    int tpc = var > 0 ? var : (int)std::max<i64>(1, ntiles / ((i64)sm_count() * 8));
+    unsigned g = (unsigned)((ntiles + tpc - 1) / tpc);
+    if (mode == 0) k_spmv_stream<T, NV, 0><<<g, 256, 0, s>>>(n, tpc, rp, ci, va, x, y, b);
+    else if (mode == 1) k_spmv_stream<T, NV, 1><<<g, 256, 0, s>>>(n, tpc, rp, ci, va, x, y, b);
+    else k_spmv_stream<T, NV, 2><<<g, 256, 0, s>>>(n, tpc, rp, ci, va, x, y, b);
 }
 
 void spmv(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val, const void *x,
@@ -159,35 +258,120 @@ void spmv(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val, 
 }
 
 // ---------------------------------------------------------------- Gauss-Seidel
-template <class T, int NV>
+// One Gauss-Seidel row update (csr_gs.inl:77-99): sum = t_i - sum_j a_ij x_j
+// in CSR order, x_i += relax*invdiag_i*sum.  The row's column indices and
+// values are fetched GB entries at a time and the x gathers of a batch are
+// issued together, so a level costs a few memory round trips instead of one
+// per entry; the fma chain itself keeps the stored order.  CG selects L2-only
+// access to x for sweeps whose rows are shared between CTAs.
+template <class T, int NV, bool CG>
 __device__ __forceinline__ void gs_row(i64 row, int lane, const int *__restrict__ rp,
                                        const int *__restrict__ ci, const T *__restrict__ va,
                                        const T *__restrict__ invd, const T *__restrict__ t, T *x,
                                        const T *__restrict__ relax, i64 brows) {
-    constexpr int V = Shape<T, NV>::V;
-    T sum[V];
-    ld_cg<T, V>(t + row * NV + lane * V, sum);
-    int j = rp[row], j1 = rp[row + 1];
+    constexpr int V = Shape<T, NV>::V, GB = 8;
+    T sum[V], xo[V];
+    if (CG) {
+        ld_cg<T, V>(t + row * NV + lane * V, sum);
+        ld_cg<T, V>(x + row * NV + lane * V, xo);
+    } else {
+        ld<T, V>(t + row * NV + lane * V, sum);
+        typedef typename VT<T, V>::type W;
+        W w = *reinterpret_cast<const W *>(x + row * NV + lane * V);
+        memcpy(xo, &w, sizeof(W));
+    }
+    const T di = __ldg(invd + row);
+    const int j0 = __ldg(rp + row), j1 = __ldg(rp + row + 1);
     i64 lo = 0, hi = INT64_MAX;
     if (brows > 0) { lo = (row / brows) * brows; hi = lo + brows; }
-    for (; j < j1; ++j) {
-        int c = __ldg(ci + j);
-        if (c < lo || c >= hi) continue;
-        T v = -__ldg(va + j);
-        T xv[V];
-        ld_cg<T, V>(x + (i64)c * NV + lane * V, xv);
+    for (int j = j0; j < j1; j += GB) {
+        int c[GB];
+        T v[GB];
 #pragma unroll
-        for (int e = 0; e < V; ++e) sum[e] = fma(v, xv[e], sum[e]);
+        for (int k = 0; k < GB; ++k) {
+            bool ok = j + k < j1;
+            c[k] = ok ? __ldg(ci + j + k) : -1;
+            v[k] = ok ? -__ldg(va + j + k) : T(0);
+        }
+        T xv[GB][V];
+#pragma unroll
+        for (int k = 0; k < GB; ++k) {
+            if (c[k] >= lo && c[k] < hi) {
+                if (CG) {
+                    ld_cg<T, V>(x + (i64)c[k] * NV + lane * V, xv[k]);
+                } else {
+                    typedef typename VT<T, V>::type W;
+                    W w = *reinterpret_cast<const W *>(x + (i64)c[k] * NV + lane * V);
+                    memcpy(xv[k], &w, sizeof(W));
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < GB; ++k)
+            if (c[k] >= lo && c[k] < hi) {
+#pragma unroll
+                for (int e = 0; e < V; ++e) sum[e] = fma(v[k], xv[k][e], sum[e]);
+            }
     }
-    T di = __ldg(invd + row);
-    T xo[V];
-    ld_cg<T, V>(x + row * NV + lane * V, xo);
 #pragma unroll
     for (int e = 0; e < V; ++e) {
         T cf = mul_rn<T>(__ldg(relax + lane * V + e), di);
         xo[e] = fma(cf, sum[e], xo[e]);
     }
-    st_cg<T, V>(x + row * NV + lane * V, xo);
+    if (CG) {
+        st_cg<T, V>(x + row * NV + lane * V, xo);
+    } else {
+        st<T, V>(x + row * NV + lane * V, xo);
+    }
+}
+
+// Hybrid Gauss-Seidel, one CTA per block of `brows` rows: the forward then the
+// backward sweep of the block run level by level with CTA barriers only (the
+// blocks are independent by construction, blas2.h:225-263).  Block b owns the
+// level range [blev[b], blev[b+1]) of lptr; level l covers perm[lptr[l]..lptr[l+1]).
+template <class T, int NV>
+__global__ void __launch_bounds__(256) k_gs_blocks(const int *__restrict__ blevf,
+                                                   const int *__restrict__ lptrf,
+                                                   const int *__restrict__ permf,
+                                                   const int *__restrict__ blevb,
+                                                   const int *__restrict__ lptrb,
+                                                   const int *__restrict__ permb,
+                                                   const int *__restrict__ rp,
+                                                   const int *__restrict__ ci,
+                                                   const T *__restrict__ va,
+                                                   const T *__restrict__ invd,
+                                                   const T *__restrict__ t, T *x,
+                                                   const T *__restrict__ relax, i64 brows) {
+    constexpr int TPR = Shape<T, NV>::TPR;
+    const int b = blockIdx.x;
+    for (int pass = 0; pass < 2; ++pass) {
+        const int *blev = pass ? blevb : blevf;
+        const int *lptr = pass ? lptrb : lptrf;
+        const int *perm = pass ? permb : permf;
+        for (int l = __ldg(blev + b), le = __ldg(blev + b + 1); l < le; ++l) {
+            int lo = __ldg(lptr + l), items = (__ldg(lptr + l + 1) - lo) * TPR;
+            for (int it = threadIdx.x; it < items; it += 256)
+                gs_row<T, NV, false>(__ldg(perm + lo + it / TPR), it % TPR, rp, ci, va, invd, t, x,
+                                     relax, brows);
+            __syncthreads();
+        }
+    }
+}
+
+void gs_blocks(Prec p, int nv, int nblocks, const int *blevf, const int *lptrf, const int *permf,
+               const int *blevb, const int *lptrb, const int *permb, const int *rp, const int *ci,
+               const void *val, const void *invd, const void *t, void *x, const void *relax,
+               i64 brows, cudaStream_t s) {
+    if (nblocks <= 0) return;
+    if (p == Prec::F64) {
+#define F(NV) k_gs_blocks<double, NV><<<nblocks, 256, 0, s>>>(blevf, lptrf, permf, blevb, lptrb, permb, rp, ci, (const double *)val, (const double *)invd, (const double *)t, (double *)x, (const double *)relax, brows)
+        NV_DISPATCH(nv, F)
+#undef F
+    } else {
+#define F(NV) k_gs_blocks<float, NV><<<nblocks, 256, 0, s>>>(blevf, lptrf, permf, blevb, lptrb, permb, rp, ci, (const float *)val, (const float *)invd, (const float *)t, (float *)x, (const float *)relax, brows)
+        NV_DISPATCH(nv, F)
+#undef F
+    }
 }
 
 template <class T, int NV>
@@ -201,7 +385,7 @@ __global__ void __launch_bounds__(256) k_gs_level(int cnt, const int *__restrict
     constexpr int TPR = Shape<T, NV>::TPR;
     int item = blockIdx.x * 256 + threadIdx.x;
     if (item >= cnt * TPR) return;
-    gs_row<T, NV>(__ldg(rows + item / TPR), item % TPR, rp, ci, va, invd, t, x, relax, brows);
+    gs_row<T, NV, true>(__ldg(rows + item / TPR), item % TPR, rp, ci, va, invd, t, x, relax, brows);
 }
 
 void gs_level(Prec p, int nv, int cnt, const int *rows, const int *rp, const int *ci,
@@ -273,7 +457,7 @@ __global__ void __launch_bounds__(256) k_gs_sweep(int nlev, const int *__restric
         int lo = __ldg(lptr + l), hi = __ldg(lptr + l + 1);
         int items = (hi - lo) * TPR;
         for (int it = blockIdx.x * 256 + threadIdx.x; it < items; it += stride)
-            gs_row<T, NV>(__ldg(perm + lo + it / TPR), it % TPR, rp, ci, va, invd, t, x, relax, brows);
+            gs_row<T, NV, true>(__ldg(perm + lo + it / TPR), it % TPR, rp, ci, va, invd, t, x, relax, brows);
         if (l + 1 < nlev) {
             __threadfence();
             if (!grid_sync(bar, err)) return;

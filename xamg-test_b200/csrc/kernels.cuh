@@ -23,6 +23,10 @@ enum class Prec : int { F64 = 0, F32 = 1 };
 // y = A x (mode 0), y += A x (mode 1), y = b - A x (mode 2, b given).
 void spmv(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val, const void *x,
           void *y, int mode, const void *b, cudaStream_t s);
+// Kernel variant for spmv(): 0 = one CTA per row tile; k > 0 = streaming
+// kernel (shared-memory staged entries) walking k tiles per CTA; -1 = auto.
+void set_spmv_variant(int v);
+int get_spmv_variant();
 
 // ---- Gauss-Seidel sweeps ----------------------------------------------------
 // One wavefront level: rows[0..cnt) are independent and updated in place.
@@ -39,6 +43,14 @@ cudaError_t gs_sweep_persistent(Prec p, int nv, int nlev, const int *lptr, const
                                 const int *rp, const int *ci, const void *val, const void *invd,
                                 const void *t, void *x, const void *relax, i64 brows,
                                 unsigned *bar, int *err, cudaStream_t s);
+
+// Hybrid Gauss-Seidel with one CTA per block of brows rows: forward and
+// backward sweeps of every block inside one launch, CTA barriers only.  Block
+// b owns levels [blev[b], blev[b+1]) of lptr; level l covers perm[lptr[l]..lptr[l+1]).
+void gs_blocks(Prec p, int nv, int nblocks, const int *blevf, const int *lptrf, const int *permf,
+               const int *blevb, const int *lptrb, const int *permb, const int *rp, const int *ci,
+               const void *val, const void *invd, const void *t, void *x, const void *relax,
+               i64 brows, cudaStream_t s);
 
 // Hybrid Gauss-Seidel right-hand side: t = 1*b + (-1)*(sum over the entries
 // outside the row's block of a_ij x_j)   (blas2.h:226-259)

@@ -109,6 +109,7 @@ def lib():
             "XAMG_b200_amg_host_destroy": (C.c_int, [sz]),
             "XAMG_b200_gs_levels_host": (C.c_int, [i64, P, P, i64, P, P, P]),
             "xamg_csr_spmv": (C.c_int, [C.c_int, C.c_int, i64, P, P, P, P, P, C.c_int, P, P]),
+            "xamg_spmv_set_variant": (C.c_int, [C.c_int]),
             "xamg_gs_plan_create": (P, [i64, P, P, i64, C.c_int]),
             "xamg_gs_plan_levels": (C.c_int, [P, P, P, P]),
             "xamg_gs_plan_error": (C.c_int, [P]),
