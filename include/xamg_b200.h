@@ -99,6 +99,11 @@ int xamg_spmv_set_variant(int variant);
  * CTA per block for hybrid plans); 2 = cooperative grid sweep always. */
 void *xamg_gs_plan_create(int64_t n, const int *rp_host, const int *ci_host,
                           int64_t block_rows, int schedule);
+/* Give the plan the matrix values (HOST array, CSR order of rp/ci): sweeps in
+ * precision prec then run over the plan's level-ordered copy of the matrix
+ * with TMA-staged entries (schedules 1 and 2); the val argument of xamg_hsgs
+ * is still used for the hybrid right-hand side. */
+int xamg_gs_plan_set_values(void *plan, const double *val_host, int prec);
 int xamg_gs_plan_levels(void *plan, int *nlev /* [2] */, int *lf, int *lb);
 int xamg_gs_plan_error(void *plan);
 void xamg_gs_plan_destroy(void *plan);

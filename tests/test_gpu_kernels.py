@@ -156,8 +156,9 @@ def _gs_case(rng, kind, n=500):
 @pytest.mark.parametrize("kind", ["dd", "27pt"])
 @pytest.mark.parametrize("block_rows", [0, 64])
 @pytest.mark.parametrize("schedule", [0, 1, 2])
+@pytest.mark.parametrize("lcsr", [False, True])
 @pytest.mark.parametrize("nv", [1, 4, 16])
-def test_hsgs_bit_exact(gpu, kind, block_rows, schedule, nv):
+def test_hsgs_bit_exact(gpu, kind, block_rows, schedule, lcsr, nv):
     rng = np.random.default_rng(21)
     rp, ci, v = _gs_case(rng, kind)
     n = len(rp) - 1
@@ -166,6 +167,8 @@ def test_hsgs_bit_exact(gpu, kind, block_rows, schedule, nv):
     assert plan
     try:
         for dtype, prec in ((np.float64, 0), (np.float32, 1)):
+            if lcsr:
+                xamg.check(L.xamg_gs_plan_set_values(plan, xamg._ptr(np.ascontiguousarray(v, np.float64)), prec))
             vv = v.astype(dtype)
             invd = np.zeros(n, dtype)
             for i in range(n):

@@ -1,0 +1,375 @@
+// Gauss-Seidel sweeps over a level-ordered copy of the matrix (sm_100a).
+//
+// The sweep's rows are stored in schedule order (level by level, and block by
+// block for hybrid plans); each row keeps its entries in the original CSR
+// order and is padded to a multiple of 4 entries with column -1, so any
+// contiguous row range starts on a 16-byte boundary and spans a multiple of 16
+// bytes.  A CTA processes one contiguous row range per level, and the entries
+// of its NEXT level are fetched into shared memory by a 1-D TMA bulk copy
+// (cp.async.bulk + mbarrier) while the current level computes; the dependent
+// chain of a level is then shared-memory reads, the x gathers and one barrier.
+//
+//   GRID   : all CTAs cooperate on every level (cooperative launch), with a
+//            bounded grid barrier between levels; x lives in global memory and
+//            is read through L2 (ld.cg) because other CTAs write it.
+//   BLOCKS : CTA b owns hybrid block b; CTA barriers only.  The block's x tile
+//            is held in shared memory when it fits (XS = true).
+//
+// Every wait (grid barrier, mbarrier) is bounded by a wall-clock limit; on
+// expiry the error word is set, the CTA waits (bounded) for its own copies in
+// flight and returns.
+#include "kernels.cuh"
+#include <cstdio>
+
+namespace xk {
+
+namespace {
+
+constexpr unsigned long long kLimitNs = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned cnt) {
+    asm volatile("mbarrier.init.shared.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(cnt) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes,
+                                         unsigned long long *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait on an mbarrier phase; false on timeout
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+    if (mbar_try(bar, parity)) return true;
+    unsigned long long t0 = now_ns();
+    while (!mbar_try(bar, parity))
+        if (now_ns() - t0 > kLimitNs) return false;
+    return true;
+}
+
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = bar + 1;
+        unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned long long t0 = now_ns();
+            unsigned spins = 0;
+            while (*gen == g) {
+                if ((++spins & 63) == 0) {
+                    if (*(volatile int *)err) break;
+                    if (now_ns() - t0 > kLimitNs) {
+                        atomicExch(err, 1);
+                        break;
+                    }
+                }
+                __nanosleep(40);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile int *)err == 0;
+}
+
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+
+template <class T, int V> struct VW;
+template <> struct VW<double, 1> { typedef double t; };
+template <> struct VW<double, 2> { typedef double2 t; };
+template <> struct VW<float, 1> { typedef float t; };
+template <> struct VW<float, 2> { typedef float2 t; };
+template <> struct VW<float, 4> { typedef float4 t; };
+
+template <class T, int NV> struct Sh {
+    static constexpr int V = (NV * (int)sizeof(T) >= 16) ? 16 / (int)sizeof(T) : NV;
+    static constexpr int TPR = NV / V;
+};
+
+template <class T, int V, bool CG>
+__device__ __forceinline__ void gld(const T *p, T (&r)[V]) {
+    typedef typename VW<T, V>::t W;
+    W w = CG ? __ldcg(reinterpret_cast<const W *>(p)) : *reinterpret_cast<const W *>(p);
+    memcpy(r, &w, sizeof(W));
+}
+template <class T, int V, bool CG>
+__device__ __forceinline__ void gst(T *p, const T (&r)[V]) {
+    typedef typename VW<T, V>::t W;
+    W w;
+    memcpy(&w, r, sizeof(W));
+    if (CG) __stcg(reinterpret_cast<W *>(p), w);
+    else *reinterpret_cast<W *>(p) = w;
+}
+
+}  // namespace
+
+// Shared-memory budget of one staging buffer (entries); two buffers per CTA.
+// (two buffers of E entries stay inside the 48 KB of static shared memory)
+template <class T> struct GsBuf { static constexpr int E = sizeof(T) == 8 ? 1792 : 2560; };
+
+// MODE 0 = GRID, 1 = BLOCKS.  XS: x tile of the block in shared memory.
+template <class T, int NV, int MODE, bool XS>
+__global__ void __launch_bounds__(256) k_gs3(int nlev, const int *__restrict__ lev_row,
+                                             const int *__restrict__ blev,
+                                             const int *__restrict__ lrp,
+                                             const int *__restrict__ lci,
+                                             const T *__restrict__ lva,
+                                             const int *__restrict__ lrow,
+                                             const T *__restrict__ invd,
+                                             const T *__restrict__ t, T *x,
+                                             const T *__restrict__ relax, i64 brows, i64 n,
+                                             unsigned *gbar, int *err) {
+    constexpr int V = Sh<T, NV>::V, TPR = Sh<T, NV>::TPR, E = GsBuf<T>::E;
+    constexpr bool CG = (MODE == 0);
+    extern __shared__ __align__(128) unsigned char dyn[];
+    __shared__ __align__(16) int s_ci[2][E];
+    __shared__ __align__(16) T s_va[2][E];
+    __shared__ __align__(8) unsigned long long mbar[2];
+    __shared__ int s_stage[2];
+    T *xs = reinterpret_cast<T *>(dyn);
+
+    const int b = blockIdx.x;
+    int l0 = 0, l1 = nlev;
+    i64 xbase = 0;
+    if (MODE == 1) {
+        l0 = __ldg(blev + b);
+        l1 = __ldg(blev + b + 1);
+        xbase = (i64)b * brows;
+    }
+    // row range of this CTA on level l
+    auto range = [&](int l, int &r0, int &r1) {
+        int a = __ldg(lev_row + l), z = __ldg(lev_row + l + 1);
+        if (MODE == 0) {
+            int cnt = z - a, per = (cnt + gridDim.x - 1) / gridDim.x;
+            r0 = min(z, a + b * per);
+            r1 = min(z, r0 + per);
+        } else {
+            r0 = a;
+            r1 = z;
+        }
+    };
+    if (threadIdx.x == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    const i64 xrows = MODE == 1 ? min((i64)brows, n - xbase) : 0;
+    if (XS) {
+        // block rows of x into shared memory
+        const i64 rows = xrows;
+        const T *xg = x + xbase * NV;
+        for (i64 q = threadIdx.x; q < rows * NV; q += 256) xs[q] = xg[q];
+    }
+    __syncthreads();
+    unsigned use[2] = {0u, 0u};
+    // issue the staging copy of level l into buffer l&1 (thread 0)
+    auto issue = [&](int l) {
+        int r0, r1;
+        range(l, r0, r1);
+        int e0 = __ldg(lrp + r0), e1 = __ldg(lrp + r1);
+        int cnt = e1 - e0, q = l & 1;
+        if (cnt > 0 && cnt <= E) {
+            unsigned bytes = (unsigned)cnt * (4u + (unsigned)sizeof(T));
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(&mbar[q], bytes);
+            bulk_g2s(&s_ci[q][0], lci + e0, (unsigned)cnt * 4u, &mbar[q]);
+            bulk_g2s(&s_va[q][0], lva + e0, (unsigned)cnt * (unsigned)sizeof(T), &mbar[q]);
+            s_stage[q] = 1;
+        } else {
+            s_stage[q] = 0;
+        }
+    };
+    if (threadIdx.x == 0 && l0 < l1) issue(l0);
+    __syncthreads();
+    bool ok = true;
+    for (int l = l0; l < l1; ++l) {
+        const int q = l & 1;
+        if (threadIdx.x == 0 && l + 1 < l1) issue(l + 1);
+        const bool staged = s_stage[q] != 0;
+        if (staged) {
+            if (!mbar_wait(&mbar[q], use[q] & 1u)) {
+                atomicExch(err, 1);
+                ok = false;
+            }
+            use[q]++;
+        }
+        int r0, r1;
+        range(l, r0, r1);
+        const int e0 = __ldg(lrp + r0);
+        const int items = (r1 - r0) * TPR;
+        for (int it = threadIdx.x; ok && it < items; it += 256) {
+            const int r = r0 + it / TPR, lane = it % TPR;
+            const i64 row = __ldg(lrow + r);
+            T sum[V], xo[V];
+            gld<T, V, CG>(t + row * NV + lane * V, sum);
+            if (XS) {
+                const T *p = xs + (row - xbase) * NV + lane * V;
+#pragma unroll
+                for (int e = 0; e < V; ++e) xo[e] = p[e];
+            } else {
+                gld<T, V, CG>(x + row * NV + lane * V, xo);
+            }
+            const T di = __ldg(invd + row);
+            const int j0 = __ldg(lrp + r), j1 = __ldg(lrp + r + 1);
+            for (int j = j0; j < j1; j += 4) {
+                int c[4];
+                T v[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    c[k] = staged ? s_ci[q][j + k - e0] : __ldg(lci + j + k);
+                    v[k] = staged ? s_va[q][j + k - e0] : __ldg(lva + j + k);
+                }
+                T xv[4][V];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (c[k] >= 0) {
+                        if (XS) {
+                            const T *p = xs + ((i64)c[k] - xbase) * NV + lane * V;
+#pragma unroll
+                            for (int e = 0; e < V; ++e) xv[k][e] = p[e];
+                        } else {
+                            gld<T, V, CG>(x + (i64)c[k] * NV + lane * V, xv[k]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (c[k] >= 0) {
+#pragma unroll
+                        for (int e = 0; e < V; ++e) sum[e] = fma(-v[k], xv[k][e], sum[e]);
+                    }
+            }
+#pragma unroll
+            for (int e = 0; e < V; ++e) {
+                T cf = rmul(relax[lane * V + e], di);
+                xo[e] = fma(cf, sum[e], xo[e]);
+            }
+            if (XS) {
+                T *p = xs + (row - xbase) * NV + lane * V;
+#pragma unroll
+                for (int e = 0; e < V; ++e) p[e] = xo[e];
+            } else {
+                gst<T, V, CG>(x + row * NV + lane * V, xo);
+            }
+        }
+        if (MODE == 0) {
+            if (l + 1 < l1) {
+                __threadfence();
+                if (!grid_barrier(gbar, err)) ok = false;
+            }
+        } else {
+            __syncthreads();
+        }
+        if (!ok) break;
+    }
+    // after an early exit, wait (bounded) for a staging copy still in flight
+    __syncthreads();
+    if (!ok && threadIdx.x == 0) {
+        for (int q = 0; q < 2; ++q)
+            if (s_stage[q]) mbar_wait(&mbar[q], use[q] & 1u);
+    }
+    __syncthreads();
+    if (XS && ok) {
+        const i64 rows = xrows;
+        T *xg = x + xbase * NV;
+        for (i64 q = threadIdx.x; q < rows * NV; q += 256) xg[q] = xs[q];
+    }
+}
+
+template <class T, int NV>
+static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *lev_row, const int *blev,
+                         const int *lrp, const int *lci, const void *lva, const int *lrow,
+                         const void *invd, const void *t, void *x, const void *relax, i64 brows,
+                         i64 n, unsigned *gbar, int *err, cudaStream_t s) {
+    const T *va = (const T *)lva;
+    const T *di = (const T *)invd;
+    const T *tt = (const T *)t;
+    T *xx = (T *)x;
+    const T *rl = (const T *)relax;
+    if (mode == 1) {
+        if (xs) {
+            size_t sm = (size_t)brows * NV * sizeof(T);
+            auto k = k_gs3<T, NV, 1, true>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, gbar, err);
+        } else {
+            k_gs3<T, NV, 1, false><<<ncta, 256, 0, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, gbar, err);
+        }
+        return cudaGetLastError();
+    }
+    static int nblk = 0;
+    if (nblk == 0) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        nblk = sms > 0 ? sms : 148;
+    }
+    void *args[] = {&nlev, &lev_row, &blev, &lrp, &lci, &va, &lrow, &di, &tt, &xx, &rl, &brows, &n, &gbar, &err};
+    return cudaLaunchCooperativeKernel((const void *)k_gs3<T, NV, 0, false>, dim3(nblk), dim3(256),
+                                       args, 0, s);
+}
+
+#define NV_SWITCH(nv, FN)                                                                         \
+    switch (nv) {                                                                                  \
+    case 1: return FN(1);                                                                          \
+    case 2: return FN(2);                                                                          \
+    case 4: return FN(4);                                                                          \
+    case 8: return FN(8);                                                                          \
+    case 16: return FN(16);                                                                        \
+    case 32: return FN(32);                                                                        \
+    default: return cudaErrorInvalidValue;                                                         \
+    }
+
+cudaError_t gs_sweep_lcsr(Prec p, int nv, int mode, int xs, int nlev, int ncta, const int *lev_row,
+                          const int *blev, const int *lrp, const int *lci, const void *lva,
+                          const int *lrow, const void *invd, const void *t, void *x,
+                          const void *relax, i64 brows, i64 n, unsigned *gbar, int *err,
+                          cudaStream_t s) {
+    if (p == Prec::F64) {
+#define F(NV) gs3_t<double, NV>(mode, xs, nlev, ncta, lev_row, blev, lrp, lci, lva, lrow, invd, t, x, relax, brows, n, gbar, err, s)
+        NV_SWITCH(nv, F)
+#undef F
+    } else {
+#define F(NV) gs3_t<float, NV>(mode, xs, nlev, ncta, lev_row, blev, lrp, lci, lva, lrow, invd, t, x, relax, brows, n, gbar, err, s)
+        NV_SWITCH(nv, F)
+#undef F
+    }
+}
+
+// dynamic shared memory available for the x tile next to the two staging buffers
+int gs_lcsr_max_xs_bytes() { return 170 * 1024; }
+
+}  // namespace xk

@@ -122,6 +122,7 @@ cudaStream_t strm(void *s) { return s ? (cudaStream_t)s : ctx().stream; }
 
 struct PlanHandle {
     GsPlan plan;
+    HostCsr pattern;
 };
 
 }  // namespace
@@ -738,9 +739,18 @@ void *xamg_gs_plan_create(int64_t n, const int *rp, const int *ci, int64_t block
         h = new PlanHandle();
         GsMode md = schedule == 0 ? GsMode::LEVELS : (schedule == 2 ? GsMode::GRID : gs_mode_from("auto", block_rows, n));
         h->plan.build(A, block_rows, md);
+        h->pattern = std::move(A);
     });
     if (rc) { delete h; return nullptr; }
     return h;
+}
+int xamg_gs_plan_set_values(void *plan, const double *val_host, int prec) {
+    return guard([&] {
+        XCHECK(plan, "null plan");
+        PlanHandle *h = (PlanHandle *)plan;
+        h->pattern.v.assign(val_host, val_host + h->pattern.nnz());
+        h->plan.build_lcsr(h->pattern, (Prec)prec);
+    });
 }
 int xamg_gs_plan_levels(void *plan, int *nlev, int *lf, int *lb) {
     return guard([&] {

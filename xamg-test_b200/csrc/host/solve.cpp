@@ -176,6 +176,75 @@ void GsPlan::build(const HostCsr &A, i64 brows_, GsMode mode_) {
     XCUDA(cudaMemset(sync.p, 0, 16));
 }
 
+// Level-ordered matrix copy of one sweep direction: rows in schedule order
+// ((block,) level, row), each row's in-block entries in CSR order, padded to a
+// multiple of 4 entries with column -1.
+void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
+    if (mode == GsMode::LEVELS) return;
+    lprec = p;
+    for (int d = 0; d < 2; ++d) {
+        const std::vector<int> &lev = d == 0 ? lf : lb;
+        std::vector<int> order;
+        order.reserve(n);
+        std::vector<int> levrow(1, 0), blev(1, 0);
+        auto emit = [&](i64 r0, i64 r1) {
+            int nl = 0;
+            for (i64 i = r0; i < r1; ++i) nl = std::max(nl, lev[i] + 1);
+            std::vector<int> cnt(nl + 1, 0);
+            for (i64 i = r0; i < r1; ++i) cnt[lev[i] + 1]++;
+            for (int l = 0; l < nl; ++l) cnt[l + 1] += cnt[l];
+            std::vector<int> pos(cnt.begin(), cnt.end() - 1), seg(r1 - r0);
+            for (i64 i = r0; i < r1; ++i) seg[pos[lev[i]]++] = (int)i;
+            size_t base = order.size();
+            order.insert(order.end(), seg.begin(), seg.end());
+            for (int l = 0; l < nl; ++l) levrow.push_back((int)(base + cnt[l + 1]));
+            return nl;
+        };
+        if (mode == GsMode::BLOCKS) {
+            for (int b = 0; b < nblocks; ++b) {
+                i64 r0 = (i64)b * brows, r1 = std::min<i64>(n, r0 + brows);
+                blev.push_back(blev.back() + emit(r0, r1));
+            }
+        } else {
+            emit(0, n);
+        }
+        std::vector<int> lrp(n + 1, 0);
+        auto inblk = [&](i64 i, i64 c) { return brows <= 0 || (c / brows) == (i / brows); };
+        for (i64 r = 0; r < n; ++r) {
+            int i = order[r], k = 0;
+            for (int j = A.rp[i]; j < A.rp[i + 1]; ++j) k += inblk(i, A.ci[j]);
+            lrp[r + 1] = lrp[r] + ((k + 3) & ~3);
+        }
+        std::vector<int> lci(std::max(lrp[n], 4), -1);
+        std::vector<double> lv(std::max(lrp[n], 4), 0.0);
+        for (i64 r = 0; r < n; ++r) {
+            int i = order[r], q = lrp[r];
+            for (int j = A.rp[i]; j < A.rp[i + 1]; ++j)
+                if (inblk(i, A.ci[j])) {
+                    lci[q] = A.ci[j];
+                    lv[q] = A.v[j];
+                    ++q;
+                }
+        }
+        Lcsr &L = lc[d];
+        L.nlev = (int)levrow.size() - 1;
+        upload_ints(L.lrp, lrp);
+        upload_ints(L.lci, lci);
+        upload_ints(L.lrow, order);
+        upload_ints(L.levrow, levrow);
+        upload_ints(L.blev, blev);
+        if (p == Prec::F64) {
+            L.lva.alloc(sizeof(double) * lv.size());
+            XCUDA(cudaMemcpy(L.lva.p, lv.data(), sizeof(double) * lv.size(), cudaMemcpyHostToDevice));
+        } else {
+            std::vector<float> f(lv.begin(), lv.end());
+            L.lva.alloc(sizeof(float) * f.size());
+            XCUDA(cudaMemcpy(L.lva.p, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice));
+        }
+    }
+    has_lcsr = true;
+}
+
 void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val,
                    const void *invd, const void *t, void *x, const void *relax, bool forward,
                    cudaStream_t s) {
@@ -183,6 +252,17 @@ void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val
     const std::vector<int> &hl = forward ? hlf : hlb;
     const int *perm = (forward ? permf : permb).as<int>();
     if (nl == 0) return;
+    if (has_lcsr && p == lprec && (mode == GsMode::GRID || mode == GsMode::BLOCKS)) {
+        const Lcsr &L = lc[forward ? 0 : 1];
+        unsigned *bar = sync.as<unsigned>();
+        int *err = (int *)(bar + 2);
+        int md = mode == GsMode::BLOCKS ? 1 : 0;
+        int xs = md == 1 && (i64)brows * nv * (i64)prec_size(p) <= xk::gs_lcsr_max_xs_bytes();
+        XCUDA(xk::gs_sweep_lcsr(p, nv, md, xs, L.nlev, md ? nblocks : 0, L.levrow.as<int>(),
+                                L.blev.as<int>(), L.lrp.as<int>(), L.lci.as<int>(), L.lva.p,
+                                L.lrow.as<int>(), invd, t, x, relax, brows, n, bar, err, s));
+        return;
+    }
     if (mode == GsMode::BLOCKS) {
         if (forward)
             xk::gs_blocks(p, nv, nblocks, bblevf.as<int>(), blptrf.as<int>(), bpermf.as<int>(),
@@ -519,6 +599,7 @@ struct MultiGrid : Solver {
                 op.gs = &m.gs_pre;
             } else {
                 g.build(hA, br, md);
+                g.build_lcsr(hA, m.prec);
                 op.gs = &g;
             }
             auto h = std::unique_ptr<HSGS>(new HSGS());
@@ -845,6 +926,7 @@ static std::unique_ptr<Solver> make_solver(const GlobalParams &gp, const std::st
         if (m == "HSGS") {
             i64 br = pl.has("hybrid_block_rows") ? (i64)pl.get_int("hybrid_block_rows") : 0;
             o->gs.build(A.h, br, gs_mode_from(pl.has("gs_schedule") ? pl.get_string("gs_schedule") : "auto", br, A.h.n));
+            o->gs.build_lcsr(A.h, prec);
             op.gs = &o->gs;
             auto h = std::unique_ptr<HSGS>(new HSGS());
             h->role = role; h->method = m; h->prm = pl; h->nv = nv; h->prec = prec;

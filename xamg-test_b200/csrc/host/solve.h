@@ -64,7 +64,16 @@ struct GsPlan {
     DBuf permf, permb, lptrf, lptrb;   // device copies (global level order)
     DBuf bblevf, bblevb, blptrf, blptrb, bpermf, bpermb;  // per-block order (BLOCKS)
     DBuf sync;                         // barrier words + error flag
+    // level-ordered copies of the matrix per direction (GRID/BLOCKS sweeps)
+    struct Lcsr {
+        DBuf lrp, lci, lva, lrow, levrow, blev;
+        int nlev = 0;
+    } lc[2];
+    bool has_lcsr = false;
+    Prec lprec = Prec::F64;
     void build(const HostCsr &A, i64 brows_, GsMode mode_);
+    // store the level-ordered matrix copies in precision p (values from A)
+    void build_lcsr(const HostCsr &A, Prec p);
     // forward (or backward) sweep; in BLOCKS mode the forward call runs both
     // sweeps and the backward call does nothing
     void sweep(Prec p, int nv, const int *rp, const int *ci, const void *val, const void *invd,

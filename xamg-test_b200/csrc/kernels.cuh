@@ -52,6 +52,17 @@ void gs_blocks(Prec p, int nv, int nblocks, const int *blevf, const int *lptrf, 
                const void *val, const void *invd, const void *t, void *x, const void *relax,
                i64 brows, cudaStream_t s);
 
+// Sweep over a level-ordered copy of the matrix (gs.cu).  mode 0: all CTAs per
+// level with a bounded grid barrier (cooperative launch); mode 1: CTA b owns
+// hybrid block b (ncta blocks).  xs = 1 keeps the block's x tile in shared
+// memory (mode 1 only, brows*nv*sizeof(T) <= gs_lcsr_max_xs_bytes()).
+cudaError_t gs_sweep_lcsr(Prec p, int nv, int mode, int xs, int nlev, int ncta, const int *lev_row,
+                          const int *blev, const int *lrp, const int *lci, const void *lva,
+                          const int *lrow, const void *invd, const void *t, void *x,
+                          const void *relax, i64 brows, i64 n, unsigned *gbar, int *err,
+                          cudaStream_t s);
+int gs_lcsr_max_xs_bytes();
+
 // Hybrid Gauss-Seidel right-hand side: t = 1*b + (-1)*(sum over the entries
 // outside the row's block of a_ij x_j)   (blas2.h:226-259)
 void offblock_resid(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val,
