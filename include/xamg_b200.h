@@ -126,6 +126,21 @@ int64_t xamg_dot_part_size(int64_t n, int nd, int nv);
 int xamg_dot(int prec, int nv, int64_t n, int nd, const void *const *a, const void *const *b,
              double *part, double *out, void *stream);
 
+/* Allocation-free inner products.  This entry point has no counterpart in
+ * the reference.  It returns exactly what xamg_dot returns, for callers that
+ * cannot allocate device memory when they need the result (a plug-in that is
+ * handed only its input and output buffers, a latency-critical loop where
+ * cudaMalloc's implicit synchronisation is not acceptable): the partial sums
+ * go to an 8 MiB array that is part of the library's device image, held on
+ * every GPU that loads the library until the process exits.  Limit:
+ * xamg_dot_part_size(n, nd, nv) <= 1048576, else code 2 and nothing runs.
+ * All calls share that array, so calls that overlap on the GPU race; calls on
+ * one stream are safe.  The first call on a device looks up the array's
+ * address with that device current; make it before any stream capture.
+ * stream NULL means the legacy default stream. */
+int xamg_dot_noalloc(int prec, int nv, int64_t n, int nd, const void *const *a,
+                     const void *const *b, double *out, void *stream);
+
 /* Block-vector BLAS-1 (blas.inl, blas_ext.inl) with FP64 per-column scalars:
  * op 0 z=a*x+b*y, 1 z=a*x+b*y+c*z, 2 z=a*x, 3 z=x, 4 z=a, 5 z=z*x. */
 int xamg_blas(int prec, int nv, int64_t n, int op, const double *a, const void *x,

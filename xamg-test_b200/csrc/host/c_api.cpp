@@ -818,3 +818,9 @@ int xamg_dense_gemv(int prec, int nv, int n, const void *AinvT, const void *b, v
 }
 
 }  // extern "C"
+
+namespace xamg {
+// Record the text returned by XAMG_b200_last_error() (used by entry points
+// that live outside this file).
+void set_last_error(const std::string &msg) { g_err = msg; }
+}  // namespace xamg
