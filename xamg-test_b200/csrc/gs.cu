@@ -136,121 +136,171 @@ __device__ __forceinline__ void gst(T *p, const T (&r)[V]) {
 
 }  // namespace
 
-// Shared-memory budget of one staging buffer (entries); two buffers per CTA.
-// (two buffers of E entries stay inside the 48 KB of static shared memory)
-template <class T> struct GsBuf { static constexpr int E = sizeof(T) == 8 ? 1792 : 2560; };
+// Staging buffers: three levels in flight, each with up to E entries and RB
+// rows (column indices, values, row offsets, row ids, inverse diagonals).
+template <class T> struct GsBuf {
+    static constexpr int E = sizeof(T) == 8 ? 1024 : 1536;
+    static constexpr int RB = 128;
+};
+
+// One level of one CTA: rows [r0, r1) and entries [e0, e1) of the
+// level-ordered copy (all multiples of 4).
+struct Desc {
+    int r0, r1, e0, e1;
+};
 
 // MODE 0 = GRID, 1 = BLOCKS.  XS: x tile of the block in shared memory.
+// desc: GRID -> desc[l*gridDim.x + b]; BLOCKS -> desc[blev[b] + (l - l0)].
 template <class T, int NV, int MODE, bool XS>
-__global__ void __launch_bounds__(256) k_gs3(int nlev, const int *__restrict__ lev_row,
+__global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ desc,
                                              const int *__restrict__ blev,
                                              const int *__restrict__ lrp,
                                              const int *__restrict__ lci,
                                              const T *__restrict__ lva,
                                              const int *__restrict__ lrow,
-                                             const T *__restrict__ invd,
+                                             const T *__restrict__ linvd,
                                              const T *__restrict__ t, T *x,
                                              const T *__restrict__ relax, i64 brows, i64 n,
                                              unsigned *gbar, int *err) {
-    constexpr int V = Sh<T, NV>::V, TPR = Sh<T, NV>::TPR, E = GsBuf<T>::E;
+    constexpr int V = Sh<T, NV>::V, TPR = Sh<T, NV>::TPR, E = GsBuf<T>::E, RB = GsBuf<T>::RB;
+    constexpr int NB = 3;
     constexpr bool CG = (MODE == 0);
     extern __shared__ __align__(128) unsigned char dyn[];
-    __shared__ __align__(16) int s_ci[2][E];
-    __shared__ __align__(16) T s_va[2][E];
-    __shared__ __align__(8) unsigned long long mbar[2];
-    __shared__ int s_stage[2];
+    __shared__ __align__(16) int s_ci[NB][E];
+    __shared__ __align__(16) T s_va[NB][E];
+    __shared__ __align__(16) int s_rp[NB][RB + 4];
+    __shared__ __align__(16) int s_row[NB][RB];
+    __shared__ __align__(16) T s_di[NB][RB];
+    __shared__ __align__(8) unsigned long long mbar[NB];
+    __shared__ int s_stage[NB];
     T *xs = reinterpret_cast<T *>(dyn);
 
-    const int b = blockIdx.x;
-    int l0 = 0, l1 = nlev;
+    const int b = blockIdx.x, tid = threadIdx.x;
+    int l0 = 0, l1 = nlev, dbase = 0;
     i64 xbase = 0;
     if (MODE == 1) {
-        l0 = __ldg(blev + b);
-        l1 = __ldg(blev + b + 1);
+        dbase = __ldg(blev + b);
+        l1 = __ldg(blev + b + 1) - dbase;
         xbase = (i64)b * brows;
     }
-    // row range of this CTA on level l
-    auto range = [&](int l, int &r0, int &r1) {
-        int a = __ldg(lev_row + l), z = __ldg(lev_row + l + 1);
-        if (MODE == 0) {
-            int cnt = z - a, per = (cnt + gridDim.x - 1) / gridDim.x;
-            r0 = min(z, a + b * per);
-            r1 = min(z, r0 + per);
-        } else {
-            r0 = a;
-            r1 = z;
-        }
+    auto dget = [&](int l) -> Desc {
+        int4 v = MODE == 0 ? __ldg(desc + (i64)l * gridDim.x + b) : __ldg(desc + dbase + l);
+        return Desc{v.x, v.y, v.z, v.w};
     };
-    if (threadIdx.x == 0) {
-        mbar_init(&mbar[0], 1);
-        mbar_init(&mbar[1], 1);
+    if (tid == 0) {
+        for (int q = 0; q < NB; ++q) mbar_init(&mbar[q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     const i64 xrows = MODE == 1 ? min((i64)brows, n - xbase) : 0;
     if (XS) {
-        // block rows of x into shared memory
-        const i64 rows = xrows;
         const T *xg = x + xbase * NV;
-        for (i64 q = threadIdx.x; q < rows * NV; q += 256) xs[q] = xg[q];
+        for (i64 q = tid; q < xrows * NV; q += 256) xs[q] = xg[q];
     }
     __syncthreads();
-    unsigned use[2] = {0u, 0u};
-    // issue the staging copy of level l into buffer l&1 (thread 0)
-    auto issue = [&](int l) {
-        int r0, r1;
-        range(l, r0, r1);
-        int e0 = __ldg(lrp + r0), e1 = __ldg(lrp + r1);
-        int cnt = e1 - e0, q = l & 1;
-        if (cnt > 0 && cnt <= E) {
-            unsigned bytes = (unsigned)cnt * (4u + (unsigned)sizeof(T));
+    unsigned use[NB] = {0u, 0u, 0u};
+    // issuer: the last thread, which rarely owns a row of a level
+    const bool issuer = tid == 255;
+    auto issue = [&](int l, const Desc &d) {
+        int q = l % NB;
+        int nr = d.r1 - d.r0, ne = d.e1 - d.e0;
+        if (nr > 0 && nr <= RB && ne <= E) {
+            unsigned bytes = (unsigned)ne * (4u + (unsigned)sizeof(T)) + (unsigned)(nr + 4) * 4u +
+                             (unsigned)nr * 4u + (unsigned)nr * (unsigned)sizeof(T);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_expect_tx(&mbar[q], bytes);
-            bulk_g2s(&s_ci[q][0], lci + e0, (unsigned)cnt * 4u, &mbar[q]);
-            bulk_g2s(&s_va[q][0], lva + e0, (unsigned)cnt * (unsigned)sizeof(T), &mbar[q]);
+            if (ne > 0) {
+                bulk_g2s(&s_ci[q][0], lci + d.e0, (unsigned)ne * 4u, &mbar[q]);
+                bulk_g2s(&s_va[q][0], lva + d.e0, (unsigned)ne * (unsigned)sizeof(T), &mbar[q]);
+            }
+            bulk_g2s(&s_rp[q][0], lrp + d.r0, (unsigned)(nr + 4) * 4u, &mbar[q]);
+            bulk_g2s(&s_row[q][0], lrow + d.r0, (unsigned)nr * 4u, &mbar[q]);
+            bulk_g2s(&s_di[q][0], linvd + d.r0, (unsigned)nr * (unsigned)sizeof(T), &mbar[q]);
             s_stage[q] = 1;
         } else {
             s_stage[q] = 0;
         }
     };
-    if (threadIdx.x == 0 && l0 < l1) issue(l0);
+    Desc dn1{0, 0, 0, 0}, dn2{0, 0, 0, 0};
+    if (issuer) {
+        if (l0 < l1) issue(l0, dget(l0));
+        if (l0 + 1 < l1) { dn1 = dget(l0 + 1); issue(l0 + 1, dn1); }
+        if (l0 + 2 < l1) dn2 = dget(l0 + 2);
+    }
     __syncthreads();
     bool ok = true;
-    for (int l = l0; l < l1; ++l) {
-        const int q = l & 1;
-        if (threadIdx.x == 0 && l + 1 < l1) issue(l + 1);
-        const bool staged = s_stage[q] != 0;
-        if (staged) {
+    // register prefetch of this thread's first row of the current level
+    bool pv = false;
+    int pr = 0;
+    T pt[V], px[V];
+    auto wait_q = [&](int q) {
+        if (s_stage[q]) {
             if (!mbar_wait(&mbar[q], use[q] & 1u)) {
                 atomicExch(err, 1);
                 ok = false;
             }
             use[q]++;
         }
-        int r0, r1;
-        range(l, r0, r1);
-        const int e0 = __ldg(lrp + r0);
-        const int items = (r1 - r0) * TPR;
-        for (int it = threadIdx.x; ok && it < items; it += 256) {
-            const int r = r0 + it / TPR, lane = it % TPR;
-            const i64 row = __ldg(lrow + r);
+    };
+    auto prefetch = [&](int l, const Desc &d) {
+        int q = l % NB;
+        pv = false;
+        if (!ok) return;  // staging buffers are not trustworthy after a timeout
+        int items = (d.r1 - d.r0) * TPR;
+        if (tid < items) {
+            int r = d.r0 + tid / TPR, lane = tid % TPR;
+            int row = s_stage[q] ? s_row[q][r - d.r0] : __ldg(lrow + r);
+            if (row >= 0) {
+                pv = true;
+                pr = row;
+                gld<T, V, CG>(t + (i64)row * NV + lane * V, pt);
+                if (!XS) gld<T, V, CG>(x + (i64)row * NV + lane * V, px);
+            }
+        }
+    };
+    Desc dc = l0 < l1 ? dget(l0) : Desc{0, 0, 0, 0};
+    if (l0 < l1) {
+        wait_q(l0 % NB);
+        prefetch(l0, dc);
+    }
+    for (int l = l0; ok && l < l1; ++l) {
+        const int q = l % NB;
+        if (issuer && l + 2 < l1) {
+            issue(l + 2, dn2);
+            if (l + 3 < l1) dn2 = dget(l + 3);
+        }
+        const bool staged = s_stage[q] != 0;
+        const int items = (dc.r1 - dc.r0) * TPR;
+        for (int it = tid; ok && it < items; it += 256) {
+            const int r = dc.r0 + it / TPR, lane = it % TPR;
+            const int row = it == tid ? (pv ? pr : -1) : (staged ? s_row[q][r - dc.r0] : __ldg(lrow + r));
+            if (row < 0) continue;
             T sum[V], xo[V];
-            gld<T, V, CG>(t + row * NV + lane * V, sum);
+            if (it == tid) {
+#pragma unroll
+                for (int e = 0; e < V; ++e) sum[e] = pt[e];
+            } else {
+                gld<T, V, CG>(t + (i64)row * NV + lane * V, sum);
+            }
             if (XS) {
-                const T *p = xs + (row - xbase) * NV + lane * V;
+                const T *p = xs + ((i64)row - xbase) * NV + lane * V;
 #pragma unroll
                 for (int e = 0; e < V; ++e) xo[e] = p[e];
+            } else if (it == tid) {
+#pragma unroll
+                for (int e = 0; e < V; ++e) xo[e] = px[e];
             } else {
-                gld<T, V, CG>(x + row * NV + lane * V, xo);
+                gld<T, V, CG>(x + (i64)row * NV + lane * V, xo);
             }
-            const T di = __ldg(invd + row);
-            const int j0 = __ldg(lrp + r), j1 = __ldg(lrp + r + 1);
+            const T di = staged ? s_di[q][r - dc.r0] : __ldg(linvd + r);
+            const int j0 = staged ? s_rp[q][r - dc.r0] : __ldg(lrp + r);
+            const int j1 = staged ? s_rp[q][r - dc.r0 + 1] : __ldg(lrp + r + 1);
             for (int j = j0; j < j1; j += 4) {
                 int c[4];
                 T v[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    c[k] = staged ? s_ci[q][j + k - e0] : __ldg(lci + j + k);
-                    v[k] = staged ? s_va[q][j + k - e0] : __ldg(lva + j + k);
+                    c[k] = staged ? s_ci[q][j + k - dc.e0] : __ldg(lci + j + k);
+                    v[k] = staged ? s_va[q][j + k - dc.e0] : __ldg(lva + j + k);
                 }
                 T xv[4][V];
 #pragma unroll
@@ -278,12 +328,19 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int *__restrict__ l
                 xo[e] = fma(cf, sum[e], xo[e]);
             }
             if (XS) {
-                T *p = xs + (row - xbase) * NV + lane * V;
+                T *p = xs + ((i64)row - xbase) * NV + lane * V;
 #pragma unroll
                 for (int e = 0; e < V; ++e) p[e] = xo[e];
             } else {
-                gst<T, V, CG>(x + row * NV + lane * V, xo);
+                gst<T, V, CG>(x + (i64)row * NV + lane * V, xo);
             }
+        }
+        // next level: its staging copy was issued a level earlier; read this
+        // thread's next row and start its t (and x) loads before the barrier
+        if (l + 1 < l1) {
+            dc = dget(l + 1);
+            wait_q((l + 1) % NB);
+            prefetch(l + 1, dc);
         }
         if (MODE == 0) {
             if (l + 1 < l1) {
@@ -293,28 +350,27 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int *__restrict__ l
         } else {
             __syncthreads();
         }
-        if (!ok) break;
     }
-    // after an early exit, wait (bounded) for a staging copy still in flight
+    // after an early exit, wait (bounded) for staging copies still in flight
     __syncthreads();
-    if (!ok && threadIdx.x == 0) {
-        for (int q = 0; q < 2; ++q)
+    if (!ok && tid == 0) {
+        for (int q = 0; q < NB; ++q)
             if (s_stage[q]) mbar_wait(&mbar[q], use[q] & 1u);
     }
     __syncthreads();
     if (XS && ok) {
-        const i64 rows = xrows;
         T *xg = x + xbase * NV;
-        for (i64 q = threadIdx.x; q < rows * NV; q += 256) xg[q] = xs[q];
+        for (i64 q = tid; q < xrows * NV; q += 256) xg[q] = xs[q];
     }
 }
 
 template <class T, int NV>
-static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *lev_row, const int *blev,
+static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp, const int *blev,
                          const int *lrp, const int *lci, const void *lva, const int *lrow,
                          const void *invd, const void *t, void *x, const void *relax, i64 brows,
                          i64 n, unsigned *gbar, int *err, cudaStream_t s) {
     const T *va = (const T *)lva;
+    const int4 *lev_row = (const int4 *)descp;
     const T *di = (const T *)invd;
     const T *tt = (const T *)t;
     T *xx = (T *)x;
@@ -330,14 +386,9 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *lev_ro
         }
         return cudaGetLastError();
     }
-    static int nblk = 0;
-    if (nblk == 0) {
-        int dev = 0, sms = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        nblk = sms > 0 ? sms : 148;
-    }
-    void *args[] = {&nlev, &lev_row, &blev, &lrp, &lci, &va, &lrow, &di, &tt, &xx, &rl, &brows, &n, &gbar, &err};
+    // the grid must match the per-(level, CTA) descriptors built on the host
+    int nblk = ncta;
+    void *args[] ={&nlev, &lev_row, &blev, &lrp, &lci, &va, &lrow, &di, &tt, &xx, &rl, &brows, &n, &gbar, &err};
     return cudaLaunchCooperativeKernel((const void *)k_gs3<T, NV, 0, false>, dim3(nblk), dim3(256),
                                        args, 0, s);
 }

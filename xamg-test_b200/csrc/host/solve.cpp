@@ -176,17 +176,34 @@ void GsPlan::build(const HostCsr &A, i64 brows_, GsMode mode_) {
     XCUDA(cudaMemset(sync.p, 0, 16));
 }
 
-// Level-ordered matrix copy of one sweep direction: rows in schedule order
-// ((block,) level, row), each row's in-block entries in CSR order, padded to a
-// multiple of 4 entries with column -1.
+// Level-ordered matrix copy of one sweep direction.  Rows are stored in
+// schedule order ((block,) level, row); every level group is padded with
+// empty rows (row id -1) to a multiple of 4 rows and every row's in-block
+// entries (CSR order) are padded with column -1 to a multiple of 4, so all row
+// and entry ranges handed to one CTA start on 16-byte boundaries and span
+// multiples of 16 bytes (the TMA bulk-copy rule).  One descriptor {r0, r1, e0,
+// e1} per (level, CTA) tells each CTA what to stage.
 void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
     if (mode == GsMode::LEVELS) return;
     lprec = p;
+    int G = 0;
+    if (mode == GsMode::GRID) {
+        int dev = 0;
+        XCUDA(cudaGetDevice(&dev));
+        XCUDA(cudaDeviceGetAttribute(&G, cudaDevAttrMultiProcessorCount, dev));
+        if (G <= 0) G = 148;
+    }
+    std::vector<double> dinv(n, 0.0);
+    for (i64 i = 0; i < n; ++i)
+        for (int j = A.rp[i]; j < A.rp[i + 1]; ++j)
+            if (A.ci[j] == i) dinv[i] = p == Prec::F64 ? 1.0 / A.v[j] : (double)(float)(1.0 / (double)(float)A.v[j]);
+    auto inblk = [&](i64 i, i64 c) { return brows <= 0 || (c / brows) == (i / brows); };
     for (int d = 0; d < 2; ++d) {
         const std::vector<int> &lev = d == 0 ? lf : lb;
-        std::vector<int> order;
-        order.reserve(n);
-        std::vector<int> levrow(1, 0), blev(1, 0);
+        std::vector<int> order;        // row id per level-ordered row (-1 = padding)
+        std::vector<int> groups(1, 0); // level-group boundaries in `order`
+        std::vector<int> blev(1, 0);
+        order.reserve(n + n / 2);
         auto emit = [&](i64 r0, i64 r1) {
             int nl = 0;
             for (i64 i = r0; i < r1; ++i) nl = std::max(nl, lev[i] + 1);
@@ -195,9 +212,11 @@ void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
             for (int l = 0; l < nl; ++l) cnt[l + 1] += cnt[l];
             std::vector<int> pos(cnt.begin(), cnt.end() - 1), seg(r1 - r0);
             for (i64 i = r0; i < r1; ++i) seg[pos[lev[i]]++] = (int)i;
-            size_t base = order.size();
-            order.insert(order.end(), seg.begin(), seg.end());
-            for (int l = 0; l < nl; ++l) levrow.push_back((int)(base + cnt[l + 1]));
+            for (int l = 0; l < nl; ++l) {
+                for (int q = cnt[l]; q < cnt[l + 1]; ++q) order.push_back(seg[q]);
+                while (order.size() % 4) order.push_back(-1);
+                groups.push_back((int)order.size());
+            }
             return nl;
         };
         if (mode == GsMode::BLOCKS) {
@@ -208,17 +227,22 @@ void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
         } else {
             emit(0, n);
         }
-        std::vector<int> lrp(n + 1, 0);
-        auto inblk = [&](i64 i, i64 c) { return brows <= 0 || (c / brows) == (i / brows); };
-        for (i64 r = 0; r < n; ++r) {
+        const i64 nr = (i64)order.size();
+        std::vector<int> lrp(nr + 5, 0);
+        for (i64 r = 0; r < nr; ++r) {
             int i = order[r], k = 0;
-            for (int j = A.rp[i]; j < A.rp[i + 1]; ++j) k += inblk(i, A.ci[j]);
+            if (i >= 0)
+                for (int j = A.rp[i]; j < A.rp[i + 1]; ++j) k += inblk(i, A.ci[j]);
             lrp[r + 1] = lrp[r] + ((k + 3) & ~3);
         }
-        std::vector<int> lci(std::max(lrp[n], 4), -1);
-        std::vector<double> lv(std::max(lrp[n], 4), 0.0);
-        for (i64 r = 0; r < n; ++r) {
+        for (int q = 1; q <= 4; ++q) lrp[nr + q] = lrp[nr];
+        XCHECK(lrp[nr] >= 0 && (i64)lrp[nr] < (1ll << 31) - 8, "level-ordered matrix too large");
+        std::vector<int> lci(std::max(lrp[nr], 4), -1);
+        std::vector<double> lv(std::max(lrp[nr], 4), 0.0), li(std::max<i64>(nr, 4), 0.0);
+        for (i64 r = 0; r < nr; ++r) {
             int i = order[r], q = lrp[r];
+            if (i < 0) continue;
+            li[r] = dinv[i];
             for (int j = A.rp[i]; j < A.rp[i + 1]; ++j)
                 if (inblk(i, A.ci[j])) {
                     lci[q] = A.ci[j];
@@ -226,20 +250,47 @@ void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
                     ++q;
                 }
         }
+        // descriptors
+        std::vector<int> desc;
+        const int ngroups = (int)groups.size() - 1;
+        if (mode == GsMode::GRID) {
+            desc.resize((size_t)ngroups * G * 4);
+            for (int l = 0; l < ngroups; ++l) {
+                int a = groups[l], z = groups[l + 1];
+                int per = ((z - a + G - 1) / G + 3) & ~3;
+                for (int b = 0; b < G; ++b) {
+                    int r0 = std::min(z, a + b * per), r1 = std::min(z, r0 + per);
+                    int *dd = &desc[((size_t)l * G + b) * 4];
+                    dd[0] = r0; dd[1] = r1; dd[2] = lrp[r0]; dd[3] = lrp[r1];
+                }
+            }
+        } else {
+            desc.resize((size_t)std::max(ngroups, 1) * 4);
+            for (int l = 0; l < ngroups; ++l) {
+                int *dd = &desc[(size_t)l * 4];
+                dd[0] = groups[l]; dd[1] = groups[l + 1]; dd[2] = lrp[groups[l]]; dd[3] = lrp[groups[l + 1]];
+            }
+        }
+        if (order.empty()) order.push_back(-1);
         Lcsr &L = lc[d];
-        L.nlev = (int)levrow.size() - 1;
+        L.nlev = ngroups;
+        L.ncta = mode == GsMode::GRID ? G : nblocks;
         upload_ints(L.lrp, lrp);
         upload_ints(L.lci, lci);
         upload_ints(L.lrow, order);
-        upload_ints(L.levrow, levrow);
+        upload_ints(L.desc, desc);
         upload_ints(L.blev, blev);
         if (p == Prec::F64) {
             L.lva.alloc(sizeof(double) * lv.size());
             XCUDA(cudaMemcpy(L.lva.p, lv.data(), sizeof(double) * lv.size(), cudaMemcpyHostToDevice));
+            L.linvd.alloc(sizeof(double) * li.size());
+            XCUDA(cudaMemcpy(L.linvd.p, li.data(), sizeof(double) * li.size(), cudaMemcpyHostToDevice));
         } else {
-            std::vector<float> f(lv.begin(), lv.end());
+            std::vector<float> f(lv.begin(), lv.end()), g(li.begin(), li.end());
             L.lva.alloc(sizeof(float) * f.size());
             XCUDA(cudaMemcpy(L.lva.p, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice));
+            L.linvd.alloc(sizeof(float) * g.size());
+            XCUDA(cudaMemcpy(L.linvd.p, g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice));
         }
     }
     has_lcsr = true;
@@ -258,9 +309,9 @@ void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val
         int *err = (int *)(bar + 2);
         int md = mode == GsMode::BLOCKS ? 1 : 0;
         int xs = md == 1 && (i64)brows * nv * (i64)prec_size(p) <= xk::gs_lcsr_max_xs_bytes();
-        XCUDA(xk::gs_sweep_lcsr(p, nv, md, xs, L.nlev, md ? nblocks : 0, L.levrow.as<int>(),
-                                L.blev.as<int>(), L.lrp.as<int>(), L.lci.as<int>(), L.lva.p,
-                                L.lrow.as<int>(), invd, t, x, relax, brows, n, bar, err, s));
+        XCUDA(xk::gs_sweep_lcsr(p, nv, md, xs, L.nlev, L.ncta, L.desc.as<int>(), L.blev.as<int>(),
+                                L.lrp.as<int>(), L.lci.as<int>(), L.lva.p, L.lrow.as<int>(),
+                                L.linvd.p, t, x, relax, brows, n, bar, err, s));
         return;
     }
     if (mode == GsMode::BLOCKS) {

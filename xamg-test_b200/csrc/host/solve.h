@@ -66,8 +66,9 @@ struct GsPlan {
     DBuf sync;                         // barrier words + error flag
     // level-ordered copies of the matrix per direction (GRID/BLOCKS sweeps)
     struct Lcsr {
-        DBuf lrp, lci, lva, lrow, levrow, blev;
-        int nlev = 0;
+        DBuf lrp, lci, lva, lrow, linvd, desc, blev;
+        int nlev = 0;  // GRID: levels; BLOCKS: unused (per-block counts in blev)
+        int ncta = 0;  // CTAs of the launch the descriptors were built for
     } lc[2];
     bool has_lcsr = false;
     Prec lprec = Prec::F64;

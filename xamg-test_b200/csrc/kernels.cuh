@@ -52,10 +52,13 @@ void gs_blocks(Prec p, int nv, int nblocks, const int *blevf, const int *lptrf, 
                const void *val, const void *invd, const void *t, void *x, const void *relax,
                i64 brows, cudaStream_t s);
 
-// Sweep over a level-ordered copy of the matrix (gs.cu).  mode 0: all CTAs per
-// level with a bounded grid barrier (cooperative launch); mode 1: CTA b owns
-// hybrid block b (ncta blocks).  xs = 1 keeps the block's x tile in shared
-// memory (mode 1 only, brows*nv*sizeof(T) <= gs_lcsr_max_xs_bytes()).
+// Sweep over a level-ordered copy of the matrix (gs.cu).  mode 0: ncta CTAs
+// share every level with a bounded grid barrier (cooperative launch); mode 1:
+// CTA b owns hybrid block b (ncta blocks).  desc holds one int4 {r0, r1, e0,
+// e1} per (level, CTA): mode 0 at [l*ncta + b], mode 1 at [blev[b] + l].
+// lrow/invd are in level order (lrow = -1 marks padding rows).  xs = 1 keeps
+// the block's x tile in shared memory (mode 1, brows*nv*sizeof(T) <=
+// gs_lcsr_max_xs_bytes()).
 cudaError_t gs_sweep_lcsr(Prec p, int nv, int mode, int xs, int nlev, int ncta, const int *lev_row,
                           const int *blev, const int *lrp, const int *lci, const void *lva,
                           const int *lrow, const void *invd, const void *t, void *x,
