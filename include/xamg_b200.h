@@ -87,8 +87,9 @@ int XAMG_b200_gs_levels_host(int64_t n, const int *rp, const int *ci, int64_t bl
 int xamg_csr_spmv(int prec, int nv, int64_t n, const int *rp, const int *ci, const void *val,
                   const void *x, void *y, int mode, const void *b, void *stream);
 /* Kernel variant used by every CSR product of the library (same results):
- * 0 = one CTA per row tile; k > 0 = shared-memory staged streaming kernel
- * walking k tiles per CTA; -1 = automatic.  Returns the previous setting. */
+ * 0, 1, 2 = one CTA per row tile with x gathers issued 4, 8 or 16 entries at
+ * a time; 10 + k = shared-memory staged streaming kernel walking k tiles per
+ * CTA; -1 = default (batches of 8).  Returns the previous setting. */
 int xamg_spmv_set_variant(int variant);
 
 /* Gauss-Seidel plan (wavefront schedule) for blas2::SGS / csr_SGS

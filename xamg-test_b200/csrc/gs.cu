@@ -294,17 +294,21 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
             const T di = staged ? s_di[q][r - dc.r0] : __ldg(linvd + r);
             const int j0 = staged ? s_rp[q][r - dc.r0] : __ldg(lrp + r);
             const int j1 = staged ? s_rp[q][r - dc.r0 + 1] : __ldg(lrp + r + 1);
-            for (int j = j0; j < j1; j += 4) {
-                int c[4];
-                T v[4];
+            // gathers from L2 (GRID) are issued 16 at a time so a row costs
+            // one or two round trips; shared-memory gathers need no batching
+            constexpr int GB = XS ? 4 : 16;
+            for (int j = j0; j < j1; j += GB) {
+                int c[GB];
+                T v[GB];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    c[k] = staged ? s_ci[q][j + k - dc.e0] : __ldg(lci + j + k);
-                    v[k] = staged ? s_va[q][j + k - dc.e0] : __ldg(lva + j + k);
+                for (int k = 0; k < GB; ++k) {
+                    const bool in = j + k < j1;
+                    c[k] = in ? (staged ? s_ci[q][j + k - dc.e0] : __ldg(lci + j + k)) : -1;
+                    v[k] = in ? (staged ? s_va[q][j + k - dc.e0] : __ldg(lva + j + k)) : T(0);
                 }
-                T xv[4][V];
+                T xv[GB][V];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+                for (int k = 0; k < GB; ++k) {
                     if (c[k] >= 0) {
                         if (XS) {
                             const T *p = xs + ((i64)c[k] - xbase) * NV + lane * V;
@@ -316,7 +320,7 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
                     }
                 }
 #pragma unroll
-                for (int k = 0; k < 4; ++k)
+                for (int k = 0; k < GB; ++k)
                     if (c[k] >= 0) {
 #pragma unroll
                         for (int e = 0; e < V; ++e) sum[e] = fma(-v[k], xv[k][e], sum[e]);

@@ -82,7 +82,10 @@ template <> __device__ __forceinline__ float add_rn<float>(float a, float b) { r
 
 // ---------------------------------------------------------------- SpMV
 // mode 0: y = A x; mode 1: y += A x; mode 2: y = 1*b + (-1)*(A x)
-template <class T, int NV, int MODE>
+// GB entries of a row are fetched per batch (column indices and values first,
+// then all GB x gathers), so a row costs about nnz_row/GB dependent memory
+// round trips; the accumulation order is the stored order for every GB.
+template <class T, int NV, int MODE, int GB>
 __global__ void __launch_bounds__(256) k_spmv(i64 n, const int *__restrict__ rp,
                                               const int *__restrict__ ci,
                                               const T *__restrict__ va, const T *__restrict__ x,
@@ -98,33 +101,27 @@ __global__ void __launch_bounds__(256) k_spmv(i64 n, const int *__restrict__ rp,
 #pragma unroll
         for (int e = 0; e < V; ++e) acc[e] = T(0);
     }
-    int j = __ldg(rp + row), j1 = __ldg(rp + row + 1);
+    const int j0 = __ldg(rp + row), j1 = __ldg(rp + row + 1);
     const T *xb = x + lane * V;
-    for (; j + 4 <= j1; j += 4) {
-        int c0 = __ldcs(ci + j), c1 = __ldcs(ci + j + 1), c2 = __ldcs(ci + j + 2),
-            c3 = __ldcs(ci + j + 3);
-        T v0 = __ldcs(va + j), v1 = __ldcs(va + j + 1), v2 = __ldcs(va + j + 2),
-          v3 = __ldcs(va + j + 3);
-        T x0[V], x1[V], x2[V], x3[V];
-        ld<T, V>(xb + (i64)c0 * NV, x0);
-        ld<T, V>(xb + (i64)c1 * NV, x1);
-        ld<T, V>(xb + (i64)c2 * NV, x2);
-        ld<T, V>(xb + (i64)c3 * NV, x3);
+    for (int j = j0; j < j1; j += GB) {
+        int c[GB];
+        T v[GB];
 #pragma unroll
-        for (int e = 0; e < V; ++e) {
-            acc[e] = fma(v0, x0[e], acc[e]);
-            acc[e] = fma(v1, x1[e], acc[e]);
-            acc[e] = fma(v2, x2[e], acc[e]);
-            acc[e] = fma(v3, x3[e], acc[e]);
+        for (int k = 0; k < GB; ++k) {
+            const bool in = j + k < j1;
+            c[k] = in ? __ldcs(ci + j + k) : 0;
+            v[k] = in ? __ldcs(va + j + k) : T(0);
         }
-    }
-    for (; j < j1; ++j) {
-        int c0 = __ldcs(ci + j);
-        T v0 = __ldcs(va + j);
-        T x0[V];
-        ld<T, V>(xb + (i64)c0 * NV, x0);
+        T xv[GB][V];
 #pragma unroll
-        for (int e = 0; e < V; ++e) acc[e] = fma(v0, x0[e], acc[e]);
+        for (int k = 0; k < GB; ++k)
+            if (j + k < j1) ld<T, V>(xb + (i64)c[k] * NV, xv[k]);
+#pragma unroll
+        for (int k = 0; k < GB; ++k)
+            if (j + k < j1) {
+#pragma unroll
+                for (int e = 0; e < V; ++e) acc[e] = fma(v[k], xv[k][e], acc[e]);
+            }
     }
     if (MODE == 2) {
         T bb[V];
@@ -206,8 +203,9 @@ __global__ void __launch_bounds__(256) k_spmv_stream(i64 n, int tpc, const int *
     }
 }
 
-// SpMV variant selection: 0 = row kernel, >0 = streaming kernel with that
-// many tiles per CTA; <0 = automatic (streaming, about 8 CTAs per SM).
+// SpMV variant selection: 0, 1, 2 = row kernel with gather batches of 4, 8,
+// 16 entries; 10 + k = streaming kernel walking k tiles per CTA; -1 = the
+// row kernel with batches of 8.
 static int g_spmv_variant = -1;
 void set_spmv_variant(int v) { g_spmv_variant = v; }
 int get_spmv_variant() { return g_spmv_variant; }
@@ -229,15 +227,18 @@ static void spmv_t(i64 n, const int *rp, const int *ci, const T *va, const T *x,
     constexpr int RPB = 256 / Shape<T, NV>::TPR;
     if (n <= 0) return;
     i64 ntiles = (n + RPB - 1) / RPB;
-    int var = g_spmv_variant;
-    if (var == 0) {
+    int var = g_spmv_variant < 0 ? 1 : g_spmv_variant;
+    if (var < 10) {
         unsigned g = (unsigned)ntiles;
-        if (mode == 0) k_spmv<T, NV, 0><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
-        else if (mode == 1) k_spmv<T, NV, 1><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
-        else k_spmv<T, NV, 2><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
+#define L(GB)                                                                                      \
+    if (mode == 0) k_spmv<T, NV, 0, GB><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);                \
+    else if (mode == 1) k_spmv<T, NV, 1, GB><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);           \
+    else k_spmv<T, NV, 2, GB><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
+        if (var == 0) { L(4) } else if (var == 2) { L(16) } else { L(8) }
+#undef L
         return;
     }
-    int tpc = var > 0 ? var : (int)std::max<i64>(1, ntiles / ((i64)sm_count() * 8));
+    int tpc = var - 10 > 0 ? var - 10 : (int)std::max<i64>(1, ntiles / ((i64)sm_count() * 8));
     unsigned g = (unsigned)((ntiles + tpc - 1) / tpc);
     if (mode == 0) k_spmv_stream<T, NV, 0><<<g, 256, 0, s>>>(n, tpc, rp, ci, va, x, y, b);
     else if (mode == 1) k_spmv_stream<T, NV, 1><<<g, 256, 0, s>>>(n, tpc, rp, ci, va, x, y, b);

@@ -23,8 +23,9 @@ enum class Prec : int { F64 = 0, F32 = 1 };
 // y = A x (mode 0), y += A x (mode 1), y = b - A x (mode 2, b given).
 void spmv(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val, const void *x,
           void *y, int mode, const void *b, cudaStream_t s);
-// Kernel variant for spmv(): 0 = one CTA per row tile; k > 0 = streaming
-// kernel (shared-memory staged entries) walking k tiles per CTA; -1 = auto.
+// Kernel variant for spmv(): 0, 1, 2 = one CTA per row tile with gather
+// batches of 4, 8, 16 entries; 10 + k = streaming kernel (shared-memory staged
+// entries) walking k tiles per CTA; -1 = default (batches of 8).
 void set_spmv_variant(int v);
 int get_spmv_variant();
 
