@@ -19,6 +19,7 @@
 // expiry the error word is set, the CTA waits (bounded) for its own copies in
 // flight and returns.
 #include "kernels.cuh"
+#include <algorithm>
 #include <cstdio>
 
 namespace xk {
@@ -161,7 +162,7 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
                                              const T *__restrict__ linvd,
                                              const T *__restrict__ t, T *x,
                                              const T *__restrict__ relax, i64 brows, i64 n,
-                                             unsigned *gbar, int *err) {
+                                             int eg, unsigned *gbar, int *err) {
     constexpr int V = Sh<T, NV>::V, TPR = Sh<T, NV>::TPR, E = GsBuf<T>::E, RB = GsBuf<T>::RB;
     constexpr int NB = 3;
     constexpr bool CG = (MODE == 0);
@@ -270,6 +271,25 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
         }
         const bool staged = s_stage[q] != 0;
         const int items = (dc.r1 - dc.r0) * TPR;
+        // GRID: gather every x value this level's entries need into shared
+        // memory in one parallel round trip (xs holds eg entries x NV)
+        const bool gath = MODE == 0 && ok && staged && (dc.e1 - dc.e0) <= eg;
+        if (MODE == 0) {
+            if (gath) {
+                const int ne = dc.e1 - dc.e0;
+                for (int w = tid; w < ne * TPR; w += 256) {
+                    const int qq = w / TPR, ln = w % TPR;
+                    const int c = s_ci[q][qq];
+                    if (c >= 0) {
+                        T tmp[V];
+                        gld<T, V, true>(x + (i64)c * NV + ln * V, tmp);
+#pragma unroll
+                        for (int e = 0; e < V; ++e) xs[((i64)qq * TPR + ln) * V + e] = tmp[e];
+                    }
+                }
+            }
+            __syncthreads();
+        }
         for (int it = tid; ok && it < items; it += 256) {
             const int r = dc.r0 + it / TPR, lane = it % TPR;
             const int row = it == tid ? (pv ? pr : -1) : (staged ? s_row[q][r - dc.r0] : __ldg(lrow + r));
@@ -312,6 +332,10 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
                     if (c[k] >= 0) {
                         if (XS) {
                             const T *p = xs + ((i64)c[k] - xbase) * NV + lane * V;
+#pragma unroll
+                            for (int e = 0; e < V; ++e) xv[k][e] = p[e];
+                        } else if (gath) {
+                            const T *p = xs + ((i64)(j + k - dc.e0) * TPR + lane) * V;
 #pragma unroll
                             for (int e = 0; e < V; ++e) xv[k][e] = p[e];
                         } else {
@@ -384,17 +408,22 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp,
             size_t sm = (size_t)brows * NV * sizeof(T);
             auto k = k_gs3<T, NV, 1, true>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, gbar, err);
+            k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, 0, gbar, err);
         } else {
-            k_gs3<T, NV, 1, false><<<ncta, 256, 0, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, gbar, err);
+            k_gs3<T, NV, 1, false><<<ncta, 256, 0, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, 0, gbar, err);
         }
         return cudaGetLastError();
     }
-    // the grid must match the per-(level, CTA) descriptors built on the host
+    // the grid must match the per-(level, CTA) descriptors built on the host;
+    // dynamic shared memory holds the per-level x gather buffer (eg entries)
     int nblk = ncta;
-    void *args[] ={&nlev, &lev_row, &blev, &lrp, &lci, &va, &lrow, &di, &tt, &xx, &rl, &brows, &n, &gbar, &err};
-    return cudaLaunchCooperativeKernel((const void *)k_gs3<T, NV, 0, false>, dim3(nblk), dim3(256),
-                                       args, 0, s);
+    int eg = (int)std::min<long>(GsBuf<T>::E, (176l * 1024) / ((long)NV * (long)sizeof(T)));
+    size_t sm = (size_t)eg * NV * sizeof(T);
+    auto k = k_gs3<T, NV, 0, false>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    void *args[] = {&nlev, &lev_row, &blev, &lrp, &lci, &va, &lrow, &di, &tt, &xx, &rl, &brows, &n, &eg, &gbar, &err};
+    return cudaLaunchCooperativeKernel((const void *)k, dim3(nblk), dim3(256), args, sm, s);
 }
 
 #define NV_SWITCH(nv, FN)                                                                         \
