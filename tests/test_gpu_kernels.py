@@ -64,7 +64,7 @@ def test_spmv_bit_exact(gpu, dtype, nv):
     L = xamg.lib()
     old = L.xamg_spmv_set_variant(-1)
     try:
-        for variant in (0, -1, 1, 2, 11, 13):
+        for variant in (0, -1, 1, 2, 3, 4, 5, 6, 11, 13):
             L.xamg_spmv_set_variant(variant)
             for mode in (0, 1, 2):
                 dy = D(y0)

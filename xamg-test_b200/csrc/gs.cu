@@ -75,20 +75,26 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
     return true;
 }
 
-__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
+// Grid barrier on two words that the launcher zeroes before the launch, on
+// separate 128-byte lines so that arrivals and polls do not queue on one L2
+// line: words[0] counts arrivals, words[16] is the release word.  Barrier k
+// is complete when the counter reaches target = (k + 1) * gridDim.x; the CTA
+// whose arrival completes it publishes target in the release word, the others
+// poll that word (bounded: on timeout *err is set).  Thread 0's fences order
+// the whole CTA's stores (they follow the CTA barrier).
+__device__ __forceinline__ bool grid_barrier(unsigned long long *words, unsigned long long target,
+                                             int *err) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned *gen = bar + 1;
-        unsigned g = *gen;
         __threadfence();
-        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-            atomicExch(bar, 0u);
+        volatile unsigned long long *rel = words + 16;
+        if (atomicAdd(words, 1ull) + 1 == target) {
             __threadfence();
-            atomicAdd(bar + 1, 1u);
+            *rel = target;
         } else {
             unsigned long long t0 = now_ns();
             unsigned spins = 0;
-            while (*gen == g) {
+            while (*rel < target) {
                 if ((++spins & 63) == 0) {
                     if (*(volatile int *)err) break;
                     if (now_ns() - t0 > kLimitNs) {
@@ -96,7 +102,6 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
                         break;
                     }
                 }
-                __nanosleep(40);
             }
         }
         __threadfence();
@@ -145,10 +150,15 @@ template <class T> struct GsBuf {
 };
 
 // One level of one CTA: rows [r0, r1) and entries [e0, e1) of the
-// level-ordered copy (all multiples of 4).
+// level-ordered copy.  e0 and e1 are multiples of 4 (rows are padded to 4
+// entries); r0 and r1 are arbitrary, and the per-row arrays are staged from
+// r0 rounded down to the 4-row boundary (level groups are padded to 4 rows, so
+// the rounded range stays inside the arrays).
 struct Desc {
     int r0, r1, e0, e1;
 };
+__device__ __forceinline__ int rlo(const Desc &d) { return d.r0 & ~3; }
+__device__ __forceinline__ int rspan(const Desc &d) { return ((d.r1 + 3) & ~3) - (d.r0 & ~3); }
 
 // MODE 0 = GRID, 1 = BLOCKS.  XS: x tile of the block in shared memory.
 // desc: GRID -> desc[l*gridDim.x + b]; BLOCKS -> desc[blev[b] + (l - l0)].
@@ -203,8 +213,8 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
     const bool issuer = tid == 255;
     auto issue = [&](int l, const Desc &d) {
         int q = l % NB;
-        int nr = d.r1 - d.r0, ne = d.e1 - d.e0;
-        if (nr > 0 && nr <= RB && ne <= E) {
+        int nr = rspan(d), ne = d.e1 - d.e0, ra = rlo(d);
+        if (d.r1 > d.r0 && nr <= RB && ne <= E) {
             unsigned bytes = (unsigned)ne * (4u + (unsigned)sizeof(T)) + (unsigned)(nr + 4) * 4u +
                              (unsigned)nr * 4u + (unsigned)nr * (unsigned)sizeof(T);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -213,9 +223,9 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
                 bulk_g2s(&s_ci[q][0], lci + d.e0, (unsigned)ne * 4u, &mbar[q]);
                 bulk_g2s(&s_va[q][0], lva + d.e0, (unsigned)ne * (unsigned)sizeof(T), &mbar[q]);
             }
-            bulk_g2s(&s_rp[q][0], lrp + d.r0, (unsigned)(nr + 4) * 4u, &mbar[q]);
-            bulk_g2s(&s_row[q][0], lrow + d.r0, (unsigned)nr * 4u, &mbar[q]);
-            bulk_g2s(&s_di[q][0], linvd + d.r0, (unsigned)nr * (unsigned)sizeof(T), &mbar[q]);
+            bulk_g2s(&s_rp[q][0], lrp + ra, (unsigned)(nr + 4) * 4u, &mbar[q]);
+            bulk_g2s(&s_row[q][0], lrow + ra, (unsigned)nr * 4u, &mbar[q]);
+            bulk_g2s(&s_di[q][0], linvd + ra, (unsigned)nr * (unsigned)sizeof(T), &mbar[q]);
             s_stage[q] = 1;
         } else {
             s_stage[q] = 0;
@@ -249,7 +259,7 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
         int items = (d.r1 - d.r0) * TPR;
         if (tid < items) {
             int r = d.r0 + tid / TPR, lane = tid % TPR;
-            int row = s_stage[q] ? s_row[q][r - d.r0] : __ldg(lrow + r);
+            int row = s_stage[q] ? s_row[q][r - rlo(d)] : __ldg(lrow + r);
             if (row >= 0) {
                 pv = true;
                 pr = row;
@@ -276,23 +286,34 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
         const bool gath = MODE == 0 && ok && staged && (dc.e1 - dc.e0) <= eg;
         if (MODE == 0) {
             if (gath) {
-                const int ne = dc.e1 - dc.e0;
-                for (int w = tid; w < ne * TPR; w += 256) {
-                    const int qq = w / TPR, ln = w % TPR;
-                    const int c = s_ci[q][qq];
-                    if (c >= 0) {
-                        T tmp[V];
-                        gld<T, V, true>(x + (i64)c * NV + ln * V, tmp);
+                // every thread issues up to GU independent loads before it
+                // stores any, so the gather costs one or two L2 round trips
+                constexpr int GU = 8;
+                const int tot = (dc.e1 - dc.e0) * TPR;
+                for (int w0 = tid; w0 < tot; w0 += 256 * GU) {
+                    int c[GU];
+                    T tmp[GU][V];
 #pragma unroll
-                        for (int e = 0; e < V; ++e) xs[((i64)qq * TPR + ln) * V + e] = tmp[e];
+                    for (int u = 0; u < GU; ++u) {
+                        const int w = w0 + u * 256;
+                        c[u] = w < tot ? s_ci[q][w / TPR] : -1;
+                        if (c[u] >= 0) gld<T, V, true>(x + (i64)c[u] * NV + (w % TPR) * V, tmp[u]);
                     }
+#pragma unroll
+                    for (int u = 0; u < GU; ++u)
+                        if (c[u] >= 0) {
+                            T *p = xs + (i64)(w0 + u * 256) * V;
+#pragma unroll
+                            for (int e = 0; e < V; ++e) p[e] = tmp[u][e];
+                        }
                 }
             }
             __syncthreads();
         }
+        const int ra = rlo(dc);
         for (int it = tid; ok && it < items; it += 256) {
             const int r = dc.r0 + it / TPR, lane = it % TPR;
-            const int row = it == tid ? (pv ? pr : -1) : (staged ? s_row[q][r - dc.r0] : __ldg(lrow + r));
+            const int row = it == tid ? (pv ? pr : -1) : (staged ? s_row[q][r - ra] : __ldg(lrow + r));
             if (row < 0) continue;
             T sum[V], xo[V];
             if (it == tid) {
@@ -311,13 +332,42 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
             } else {
                 gld<T, V, CG>(x + (i64)row * NV + lane * V, xo);
             }
-            const T di = staged ? s_di[q][r - dc.r0] : __ldg(linvd + r);
-            const int j0 = staged ? s_rp[q][r - dc.r0] : __ldg(lrp + r);
-            const int j1 = staged ? s_rp[q][r - dc.r0 + 1] : __ldg(lrp + r + 1);
-            // gathers from L2 (GRID) are issued 16 at a time so a row costs
-            // one or two round trips; shared-memory gathers need no batching
-            constexpr int GB = XS ? 4 : 16;
-            for (int j = j0; j < j1; j += GB) {
+            const T di = staged ? s_di[q][r - ra] : __ldg(linvd + r);
+            const int j0 = staged ? s_rp[q][r - ra] : __ldg(lrp + r);
+            const int j1 = staged ? s_rp[q][r - ra + 1] : __ldg(lrp + r + 1);
+            if (staged && (XS || gath)) {
+                // every operand is in shared memory: a plain loop over the
+                // row's entries (the padding, column -1, is only at its tail)
+                const int o = j0 - dc.e0;
+                int m = j1 - j0;
+                while (m > 0 && s_ci[q][o + m - 1] < 0) --m;
+                const T *vr = &s_va[q][o];
+                if (XS) {
+                    const int *cr = &s_ci[q][o];
+#pragma unroll 4
+                    for (int k = 0; k < m; ++k) {
+                        T xv[V];
+                        gld<T, V, false>(xs + ((i64)cr[k] - xbase) * NV + lane * V, xv);
+                        const T a = vr[k];
+#pragma unroll
+                        for (int e = 0; e < V; ++e) sum[e] = fma(-a, xv[e], sum[e]);
+                    }
+                } else {
+                    const T *xr = xs + (i64)o * NV + lane * V;
+#pragma unroll 8
+                    for (int k = 0; k < m; ++k) {
+                        T xv[V];
+                        gld<T, V, false>(xr + (i64)k * NV, xv);
+                        const T a = vr[k];
+#pragma unroll
+                        for (int e = 0; e < V; ++e) sum[e] = fma(-a, xv[e], sum[e]);
+                    }
+                }
+            } else
+            // entries read from global memory: gathers from L2 are issued 16
+            // at a time so a row costs one or two round trips
+            for (int j = j0; j < j1; j += 16) {
+                constexpr int GB = 16;
                 int c[GB];
                 T v[GB];
 #pragma unroll
@@ -371,10 +421,10 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
             prefetch(l + 1, dc);
         }
         if (MODE == 0) {
-            if (l + 1 < l1) {
-                __threadfence();
-                if (!grid_barrier(gbar, err)) ok = false;
-            }
+            if (l + 1 < l1 &&
+                !grid_barrier(reinterpret_cast<unsigned long long *>(gbar),
+                              (unsigned long long)(l + 1) * gridDim.x, err))
+                ok = false;
         } else {
             __syncthreads();
         }
@@ -421,6 +471,9 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp,
     size_t sm = (size_t)eg * NV * sizeof(T);
     auto k = k_gs3<T, NV, 0, false>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    // the grid barrier's arrival counter and release word start from zero
+    e = cudaMemsetAsync(gbar, 0, 256, s);
     if (e != cudaSuccess) return e;
     void *args[] = {&nlev, &lev_row, &blev, &lrp, &lci, &va, &lrow, &di, &tt, &xx, &rl, &brows, &n, &eg, &gbar, &err};
     return cudaLaunchCooperativeKernel((const void *)k, dim3(nblk), dim3(256), args, sm, s);

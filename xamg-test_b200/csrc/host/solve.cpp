@@ -172,8 +172,8 @@ void GsPlan::build(const HostCsr &A, i64 brows_, GsMode mode_) {
     };
     nlf = sched(lf, hlf, permf, lptrf);
     nlb = sched(lb, hlb, permb, lptrb);
-    sync.alloc(16);
-    XCUDA(cudaMemset(sync.p, 0, 16));
+    sync.alloc(kSyncBytes);
+    XCUDA(cudaMemset(sync.p, 0, kSyncBytes));
 }
 
 // Level-ordered matrix copy of one sweep direction.  Rows are stored in
@@ -255,13 +255,24 @@ void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
         const int ngroups = (int)groups.size() - 1;
         if (mode == GsMode::GRID) {
             desc.resize((size_t)ngroups * G * 4);
+            // contiguous row ranges of about equal cost (entries + 4 per row),
+            // any row granularity: a level of a few long rows spreads over as
+            // many CTAs as it has rows
             for (int l = 0; l < ngroups; ++l) {
-                int a = groups[l], z = groups[l + 1];
-                int per = ((z - a + G - 1) / G + 3) & ~3;
+                const int a = groups[l], z = groups[l + 1];
+                auto cost = [&](int r) { return (i64)(lrp[r] - lrp[a]) + 4 * (i64)(r - a); };
+                const i64 tot = cost(z);
+                int r = a;
                 for (int b = 0; b < G; ++b) {
-                    int r0 = std::min(z, a + b * per), r1 = std::min(z, r0 + per);
+                    const int r0 = r;
+                    if (b == G - 1) {
+                        r = z;
+                    } else {
+                        const i64 goal = tot * (b + 1) / G;
+                        while (r < z && cost(r + 1) <= goal) ++r;
+                    }
                     int *dd = &desc[((size_t)l * G + b) * 4];
-                    dd[0] = r0; dd[1] = r1; dd[2] = lrp[r0]; dd[3] = lrp[r1];
+                    dd[0] = r0; dd[1] = r; dd[2] = lrp[r0]; dd[3] = lrp[r];
                 }
             }
         } else {
@@ -306,7 +317,7 @@ void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val
     if (has_lcsr && p == lprec && (mode == GsMode::GRID || mode == GsMode::BLOCKS)) {
         const Lcsr &L = lc[forward ? 0 : 1];
         unsigned *bar = sync.as<unsigned>();
-        int *err = (int *)(bar + 2);
+        int *err = (int *)(sync.as<char>() + kSyncErrOffset);
         int md = mode == GsMode::BLOCKS ? 1 : 0;
         int xs = md == 1 && (i64)brows * nv * (i64)prec_size(p) <= xk::gs_lcsr_max_xs_bytes();
         XCUDA(xk::gs_sweep_lcsr(p, nv, md, xs, L.nlev, L.ncta, L.desc.as<int>(), L.blev.as<int>(),
@@ -323,7 +334,10 @@ void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val
     }
     if (mode == GsMode::GRID && nl > 2) {
         unsigned *bar = sync.as<unsigned>();
-        int *err = (int *)(bar + 2);
+        int *err = (int *)(sync.as<char>() + kSyncErrOffset);
+        // {count, generation} start from zero (the level-ordered sweep leaves
+        // its own arrival counter in the same words)
+        XCUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s));
         XCUDA(xk::gs_sweep_persistent(p, nv, nl, (forward ? lptrf : lptrb).as<int>(), perm,
                                       rp, ci, val, invd, t, x, relax, brows, bar, err, s));
         return;
@@ -335,9 +349,9 @@ void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val
 
 int GsPlan::error_flag() const {
     if (!sync.p) return 0;
-    unsigned h[4] = {0, 0, 0, 0};
-    XCUDA(cudaMemcpy(h, sync.p, 16, cudaMemcpyDeviceToHost));
-    return (int)h[2];
+    int h = 0;
+    XCUDA(cudaMemcpy(&h, sync.as<char>() + kSyncErrOffset, sizeof(int), cudaMemcpyDeviceToHost));
+    return h;
 }
 
 // ------------------------------------------------------------------ Conv

@@ -54,6 +54,12 @@ struct DCsr {
 // barriers, both sweeps in one launch.
 enum class GsMode : int { LEVELS = 0, GRID = 1, BLOCKS = 2 };
 
+// Synchronisation words of a plan's sweeps, each group on its own 128-byte
+// line: grid-barrier words at 0 (arrival counter) and 128 (release word), the
+// error flag at kSyncErrOffset.
+constexpr size_t kSyncBytes = 384;
+constexpr size_t kSyncErrOffset = 256;
+
 struct GsPlan {
     i64 n = 0, brows = 0;
     int nlf = 0, nlb = 0;
@@ -63,7 +69,7 @@ struct GsPlan {
     std::vector<int> lf, lb;           // per-row levels (host, for export)
     DBuf permf, permb, lptrf, lptrb;   // device copies (global level order)
     DBuf bblevf, bblevb, blptrf, blptrb, bpermf, bpermb;  // per-block order (BLOCKS)
-    DBuf sync;                         // barrier words + error flag
+    DBuf sync;                         // barrier words + error flag (kSyncBytes)
     // level-ordered copies of the matrix per direction (GRID/BLOCKS sweeps)
     struct Lcsr {
         DBuf lrp, lci, lva, lrow, linvd, desc, blev;

@@ -203,9 +203,129 @@ __global__ void __launch_bounds__(256) k_spmv_stream(i64 n, int tpc, const int *
     }
 }
 
+// x gather with an L2 evict-last policy: the stencil neighbourhood of x is
+// read by the rows of three planes, while the matrix entries (loaded with the
+// streaming hint) are read once.
+__device__ __forceinline__ unsigned long long l2_keep_policy() {
+    unsigned long long p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+template <class T, int V>
+__device__ __forceinline__ void ld_keep(const T *p, T (&r)[V], unsigned long long pol) {
+    if constexpr (sizeof(T) * V == 16) {
+        unsigned a, b, c, d;
+        asm volatile("ld.global.nc.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+                     : "=r"(a), "=r"(b), "=r"(c), "=r"(d)
+                     : "l"(p), "l"(pol));
+        unsigned w[4] = {a, b, c, d};
+        memcpy(r, w, 16);
+    } else if constexpr (sizeof(T) * V == 8) {
+        unsigned a, b;
+        asm volatile("ld.global.nc.L2::cache_hint.v2.u32 {%0,%1}, [%2], %3;"
+                     : "=r"(a), "=r"(b)
+                     : "l"(p), "l"(pol));
+        unsigned w[2] = {a, b};
+        memcpy(r, w, 8);
+    } else {
+        unsigned a;
+        asm volatile("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(a) : "l"(p), "l"(pol));
+        memcpy(r, &a, 4);
+    }
+}
+
+// Row sum over entries [j0, j1) read at cidx/vals[j - off] (shared memory
+// when SMEM, global with the streaming hint otherwise), gathers GB at a time.
+template <class T, int NV, int V, int GB, bool KEEP, bool SMEM>
+__device__ __forceinline__ void tile_row_sum(int j0, int j1, int off, const int *cidx,
+                                             const T *vals, const T *xb, T (&acc)[V],
+                                             unsigned long long pol) {
+    for (int j = j0; j < j1; j += GB) {
+        int c[GB];
+        T v[GB];
+#pragma unroll
+        for (int k = 0; k < GB; ++k) {
+            const bool in = j + k < j1;
+            if (SMEM) {
+                c[k] = in ? cidx[j + k - off] : 0;
+                v[k] = in ? vals[j + k - off] : T(0);
+            } else {
+                c[k] = in ? __ldcs(cidx + j + k) : 0;
+                v[k] = in ? __ldcs(vals + j + k) : T(0);
+            }
+        }
+        T xv[GB][V];
+#pragma unroll
+        for (int k = 0; k < GB; ++k)
+            if (j + k < j1) {
+                if (KEEP) ld_keep<T, V>(xb + (i64)c[k] * NV, xv[k], pol);
+                else ld<T, V>(xb + (i64)c[k] * NV, xv[k]);
+            }
+#pragma unroll
+        for (int k = 0; k < GB; ++k)
+            if (j + k < j1) {
+#pragma unroll
+                for (int e = 0; e < V; ++e) acc[e] = fma(v[k], xv[k][e], acc[e]);
+            }
+    }
+}
+
+// Tile-staged variant: the CSR entries of a tile of RPB rows are copied into
+// shared memory with coalesced streaming loads, so the per-entry column index
+// and value reads of the row sums are shared-memory broadcasts (one wavefront
+// serves every row of a warp) and L1 carries only the x gathers.  Tiles with
+// more than EMAX entries read their entries from global memory.  Same
+// per-row summation order as k_spmv.
+template <class T, int NV, int MODE, int GB, bool KEEP>
+__global__ void __launch_bounds__(256) k_spmv_tile(i64 n, const int *__restrict__ rp,
+                                                   const int *__restrict__ ci,
+                                                   const T *__restrict__ va,
+                                                   const T *__restrict__ x, T *__restrict__ y,
+                                                   const T *__restrict__ b) {
+    constexpr int V = Shape<T, NV>::V, TPR = Shape<T, NV>::TPR, RPB = 256 / TPR;
+    constexpr int EMAX = RPB * 32 < 2048 ? RPB * 32 : 2048;
+    __shared__ int s_c[EMAX];
+    __shared__ T s_v[EMAX];
+    const i64 r0 = (i64)blockIdx.x * RPB, r1 = min(n, r0 + RPB);
+    const int e0 = __ldg(rp + r0), cnt = __ldg(rp + r1) - e0;
+    const bool staged = cnt <= EMAX;
+    if (staged)
+        for (int q = threadIdx.x; q < cnt; q += 256) {
+            s_c[q] = __ldcs(ci + e0 + q);
+            s_v[q] = __ldcs(va + e0 + q);
+        }
+    const i64 row = r0 + threadIdx.x / TPR;
+    const int lane = threadIdx.x % TPR;
+    const bool live = row < r1;
+    int j0 = 0, j1 = 0;
+    T acc[V];
+#pragma unroll
+    for (int e = 0; e < V; ++e) acc[e] = T(0);
+    if (live) {
+        j0 = __ldg(rp + row);
+        j1 = __ldg(rp + row + 1);
+        if (MODE == 1) ld<T, V>(y + row * NV + lane * V, acc);
+    }
+    unsigned long long pol = 0;
+    if (KEEP) pol = l2_keep_policy();
+    __syncthreads();
+    if (!live) return;
+    const T *xb = x + lane * V;
+    if (staged) tile_row_sum<T, NV, V, GB, KEEP, true>(j0, j1, e0, s_c, s_v, xb, acc, pol);
+    else tile_row_sum<T, NV, V, GB, KEEP, false>(j0, j1, 0, ci, va, xb, acc, pol);
+    if (MODE == 2) {
+        T bb[V];
+        ld<T, V>(b + row * NV + lane * V, bb);
+#pragma unroll
+        for (int e = 0; e < V; ++e) acc[e] = add_rn<T>(mul_rn<T>(T(1), bb[e]), mul_rn<T>(T(-1), acc[e]));
+    }
+    st<T, V>(y + row * NV + lane * V, acc);
+}
+
 // SpMV variant selection: 0, 1, 2 = row kernel with gather batches of 4, 8,
-// 16 entries; 10 + k = streaming kernel walking k tiles per CTA; -1 = the
-// row kernel with batches of 8.
+// 16 entries; 3, 4 = tile-staged kernel with batches of 4, 8; 5, 6 = the same
+// with the L2 evict-last hint on the x gathers; 10 + k = streaming kernel
+// walking k tiles per CTA; -1 = the row kernel with batches of 8.
 static int g_spmv_variant = -1;
 void set_spmv_variant(int v) { g_spmv_variant = v; }
 int get_spmv_variant() { return g_spmv_variant; }
@@ -228,6 +348,16 @@ static void spmv_t(i64 n, const int *rp, const int *ci, const T *va, const T *x,
     if (n <= 0) return;
     i64 ntiles = (n + RPB - 1) / RPB;
     int var = g_spmv_variant < 0 ? 1 : g_spmv_variant;
+    if (var >= 3 && var <= 6) {
+        unsigned g = (unsigned)ntiles;
+#define L(GB, KEEP)                                                                                \
+    if (mode == 0) k_spmv_tile<T, NV, 0, GB, KEEP><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);      \
+    else if (mode == 1) k_spmv_tile<T, NV, 1, GB, KEEP><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b); \
+    else k_spmv_tile<T, NV, 2, GB, KEEP><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
+        if (var == 3) { L(4, false) } else if (var == 4) { L(8, false) } else if (var == 5) { L(4, true) } else { L(8, true) }
+#undef L
+        return;
+    }
     if (var < 10) {
         unsigned g = (unsigned)ntiles;
 #define L(GB)                                                                                      \

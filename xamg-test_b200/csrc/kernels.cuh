@@ -59,7 +59,9 @@ void gs_blocks(Prec p, int nv, int nblocks, const int *blevf, const int *lptrf, 
 // e1} per (level, CTA): mode 0 at [l*ncta + b], mode 1 at [blev[b] + l].
 // lrow/invd are in level order (lrow = -1 marks padding rows).  xs = 1 keeps
 // the block's x tile in shared memory (mode 1, brows*nv*sizeof(T) <=
-// gs_lcsr_max_xs_bytes()).
+// gs_lcsr_max_xs_bytes()).  Mode 0 uses the first 256 bytes of gbar
+// (8-byte aligned) for the grid barrier and zeroes them before the launch;
+// err must lie outside them.
 cudaError_t gs_sweep_lcsr(Prec p, int nv, int mode, int xs, int nlev, int ncta, const int *lev_row,
                           const int *blev, const int *lrp, const int *lci, const void *lva,
                           const int *lrow, const void *invd, const void *t, void *x,
