@@ -156,7 +156,7 @@ def tune_spmv(csr, prec=0):
     """Autotune the SpMV kernel variant on this matrix (results are identical
     for every variant; only the launch shape differs)."""
     res = {}
-    for var in (0, 1, 2, 11, 12, 14, 18):
+    for var in (0, 3, 5, 6):
         res[var] = spmv_time(csr, prec, var, iters=10)
     best = min(res, key=res.get)
     return best, res
@@ -168,7 +168,9 @@ def spmv_roofline(csr, variant):
     byts = nnz * (8 + 4) + (n + 1) * 4 + 2 * n * NV * 8
     peak, src = peak_hbm()
     ach = byts / (ms * 1e-3) / 1e9
-    kern = ("k_spmv<double,16,0,%d>" % {0: 4, 2: 16}.get(variant, 8)) if variant < 10 else "k_spmv_stream<double,16,0>"
+    kern = {0: "k_spmv<double,16,0,4>", 1: "k_spmv<double,16,0,8>", 2: "k_spmv<double,16,0,16>",
+            3: "k_spmv_tile<double,16,0,4,0>", 4: "k_spmv_tile<double,16,0,8,0>",
+            5: "k_spmv_tile<double,16,0,4,1>", 6: "k_spmv_tile<double,16,0,8,1>"}.get(variant, "k_spmv_stream<double,16,0>")
     return {"bound": "hbm", "kernel": kern, "variant": variant, "achieved": round(ach, 1), "peak": peak,
             "peak_source": src, "unit": "GB/s", "frac": round(ach / peak, 4),
             "traffic": None, "algorithmic_bytes": byts, "launch_ms": round(ms, 4)}
@@ -272,6 +274,51 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def kernel_case(args):
+    """One hot kernel alone on a grid of side --n (for profiler captures):
+    spmv = the NV=16 FP64 CSR product (variant --variant), gs = one forward +
+    backward sequential Gauss-Seidel sweep (cooperative level-ordered kernel)."""
+    import ctypes as C
+    import torch
+    import xamg
+    global N_GRID
+    N_GRID = args.n
+    xamg.init(NV)
+    csr, B = build_problem()
+    if args.kernel == "spmv":
+        ms = spmv_time(csr, 0, args.variant, iters=args.steps)
+        print(json.dumps({"kernel": "spmv", "n": args.n, "variant": args.variant, "ms": round(ms, 4)}))
+        return
+    L = xamg.lib()
+    rp, ci, v = csr.arrays()
+    n = csr.nrows
+    plan = L.xamg_gs_plan_create(n, xamg._ptr(rp), xamg._ptr(ci), 0, 1)
+    assert plan
+    try:
+        xamg.check(L.xamg_gs_plan_set_values(plan, xamg._ptr(np.ascontiguousarray(v)), 0))
+        rows = np.repeat(np.arange(n), np.diff(rp))
+        diag = ci == rows
+        invd = np.zeros(n)
+        invd[rows[diag]] = 1.0 / v[diag]
+        d = [torch.from_numpy(a).cuda() for a in (rp, ci, v, invd, B, np.zeros_like(B), np.ones(NV))]
+        P = lambda t: C.c_void_p(t.data_ptr())
+        times = []
+        for _ in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            xamg.check(L.xamg_hsgs(plan, 0, NV, P(d[0]), P(d[1]), P(d[2]), P(d[3]), P(d[4]), P(d[5]),
+                                   P(d[6]), None, None))
+            xamg.check(L.XAMG_b200_synchronize())
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        assert L.xamg_gs_plan_error(plan) == 0
+        print(json.dumps({"kernel": "gs", "n": args.n, "ms": round(float(np.mean(times[args.warmup:])), 4)}))
+    finally:
+        L.xamg_gs_plan_destroy(plan)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -281,7 +328,12 @@ def main():
     ap.add_argument("--forms", default="plain,mixed")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-iters", type=int, default=12)
+    ap.add_argument("--kernel", choices=["spmv", "gs"], help="time one hot kernel alone (profiling)")
+    ap.add_argument("--n", type=int, default=96, help="grid side of --kernel")
+    ap.add_argument("--variant", type=int, default=-1, help="SpMV variant of --kernel spmv")
     args = ap.parse_args()
+    if args.kernel:
+        return kernel_case(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -88,8 +88,10 @@ int xamg_csr_spmv(int prec, int nv, int64_t n, const int *rp, const int *ci, con
                   const void *x, void *y, int mode, const void *b, void *stream);
 /* Kernel variant used by every CSR product of the library (same results):
  * 0, 1, 2 = one CTA per row tile with x gathers issued 4, 8 or 16 entries at
- * a time; 10 + k = shared-memory staged streaming kernel walking k tiles per
- * CTA; -1 = default (batches of 8).  Returns the previous setting. */
+ * a time; 3, 4 = the tile's entries staged in shared memory, gathers 4 or 8 at
+ * a time; 5, 6 = staged entries with a plain row loop unrolled 4 or 8 times;
+ * 10 + k = staged streaming kernel walking k tiles per CTA; -1 = default (6
+ * when nv * element size >= 64 bytes, else 0).  Returns the previous setting. */
 int xamg_spmv_set_variant(int variant);
 
 /* Gauss-Seidel plan (wavefront schedule) for blas2::SGS / csr_SGS

@@ -203,48 +203,34 @@ __global__ void __launch_bounds__(256) k_spmv_stream(i64 n, int tpc, const int *
     }
 }
 
-// x gather with an L2 evict-last policy: the stencil neighbourhood of x is
-// read by the rows of three planes, while the matrix entries (loaded with the
-// streaming hint) are read once.
-__device__ __forceinline__ unsigned long long l2_keep_policy() {
-    unsigned long long p;
-    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-template <class T, int V>
-__device__ __forceinline__ void ld_keep(const T *p, T (&r)[V], unsigned long long pol) {
-    if constexpr (sizeof(T) * V == 16) {
-        unsigned a, b, c, d;
-        asm volatile("ld.global.nc.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
-                     : "=r"(a), "=r"(b), "=r"(c), "=r"(d)
-                     : "l"(p), "l"(pol));
-        unsigned w[4] = {a, b, c, d};
-        memcpy(r, w, 16);
-    } else if constexpr (sizeof(T) * V == 8) {
-        unsigned a, b;
-        asm volatile("ld.global.nc.L2::cache_hint.v2.u32 {%0,%1}, [%2], %3;"
-                     : "=r"(a), "=r"(b)
-                     : "l"(p), "l"(pol));
-        unsigned w[2] = {a, b};
-        memcpy(r, w, 8);
-    } else {
-        unsigned a;
-        asm volatile("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(a) : "l"(p), "l"(pol));
-        memcpy(r, &a, 4);
-    }
-}
-
 // Row sum over entries [j0, j1) read at cidx/vals[j - off] (shared memory
-// when SMEM, global with the streaming hint otherwise), gathers GB at a time.
-template <class T, int NV, int V, int GB, bool KEEP, bool SMEM>
+// when SMEM, global with the streaming hint otherwise).  LOOP 0: the entries
+// are fetched GB at a time into register arrays, then the GB gathers, then
+// the GB FMAs; LOOP 1: a plain loop over the entries unrolled GB times (the
+// compiler hoists the unrolled gathers ahead of the FMA chain).
+template <class T, int NV, int V, int GB, int LOOP, bool SMEM>
 __device__ __forceinline__ void tile_row_sum(int j0, int j1, int off, const int *cidx,
-                                             const T *vals, const T *xb, T (&acc)[V],
-                                             unsigned long long pol) {
-    for (int j = j0; j < j1; j += GB) {
-        int c[GB];
-        T v[GB];
+                                             const T *vals, const T *xb, T (&acc)[V]) {
+    if (LOOP == 1 && SMEM) {
+        const int *cr = cidx + (j0 - off);
+        const T *vr = vals + (j0 - off);
+        const int m = j1 - j0;
+#pragma unroll GB
+        for (int k = 0; k < m; ++k) {
+            T xv[V];
+            ld<T, V>(xb + (i64)cr[k] * NV, xv);
+            const T a = vr[k];
 #pragma unroll
-        for (int k = 0; k < GB; ++k) {
+            for (int e = 0; e < V; ++e) acc[e] = fma(a, xv[e], acc[e]);
+        }
+        return;
+    }
+    constexpr int GBB = LOOP == 1 ? 2 : GB;  // batch of the global-memory fallback
+    for (int j = j0; j < j1; j += GBB) {
+        int c[GBB];
+        T v[GBB];
+#pragma unroll
+        for (int k = 0; k < GBB; ++k) {
             const bool in = j + k < j1;
             if (SMEM) {
                 c[k] = in ? cidx[j + k - off] : 0;
@@ -254,15 +240,12 @@ __device__ __forceinline__ void tile_row_sum(int j0, int j1, int off, const int 
                 v[k] = in ? __ldcs(vals + j + k) : T(0);
             }
         }
-        T xv[GB][V];
+        T xv[GBB][V];
 #pragma unroll
-        for (int k = 0; k < GB; ++k)
-            if (j + k < j1) {
-                if (KEEP) ld_keep<T, V>(xb + (i64)c[k] * NV, xv[k], pol);
-                else ld<T, V>(xb + (i64)c[k] * NV, xv[k]);
-            }
+        for (int k = 0; k < GBB; ++k)
+            if (j + k < j1) ld<T, V>(xb + (i64)c[k] * NV, xv[k]);
 #pragma unroll
-        for (int k = 0; k < GB; ++k)
+        for (int k = 0; k < GBB; ++k)
             if (j + k < j1) {
 #pragma unroll
                 for (int e = 0; e < V; ++e) acc[e] = fma(v[k], xv[k][e], acc[e]);
@@ -276,8 +259,8 @@ __device__ __forceinline__ void tile_row_sum(int j0, int j1, int off, const int 
 // serves every row of a warp) and L1 carries only the x gathers.  Tiles with
 // more than EMAX entries read their entries from global memory.  Same
 // per-row summation order as k_spmv.
-template <class T, int NV, int MODE, int GB, bool KEEP>
-__global__ void __launch_bounds__(256) k_spmv_tile(i64 n, const int *__restrict__ rp,
+template <class T, int NV, int MODE, int GB, int LOOP>
+__global__ void __launch_bounds__(256, LOOP == 1 ? 6 : 1) k_spmv_tile(i64 n, const int *__restrict__ rp,
                                                    const int *__restrict__ ci,
                                                    const T *__restrict__ va,
                                                    const T *__restrict__ x, T *__restrict__ y,
@@ -306,13 +289,11 @@ __global__ void __launch_bounds__(256) k_spmv_tile(i64 n, const int *__restrict_
         j1 = __ldg(rp + row + 1);
         if (MODE == 1) ld<T, V>(y + row * NV + lane * V, acc);
     }
-    unsigned long long pol = 0;
-    if (KEEP) pol = l2_keep_policy();
     __syncthreads();
     if (!live) return;
     const T *xb = x + lane * V;
-    if (staged) tile_row_sum<T, NV, V, GB, KEEP, true>(j0, j1, e0, s_c, s_v, xb, acc, pol);
-    else tile_row_sum<T, NV, V, GB, KEEP, false>(j0, j1, 0, ci, va, xb, acc, pol);
+    if (staged) tile_row_sum<T, NV, V, GB, LOOP, true>(j0, j1, e0, s_c, s_v, xb, acc);
+    else tile_row_sum<T, NV, V, GB, LOOP, false>(j0, j1, 0, ci, va, xb, acc);
     if (MODE == 2) {
         T bb[V];
         ld<T, V>(b + row * NV + lane * V, bb);
@@ -324,8 +305,9 @@ __global__ void __launch_bounds__(256) k_spmv_tile(i64 n, const int *__restrict_
 
 // SpMV variant selection: 0, 1, 2 = row kernel with gather batches of 4, 8,
 // 16 entries; 3, 4 = tile-staged kernel with batches of 4, 8; 5, 6 = the same
-// with the L2 evict-last hint on the x gathers; 10 + k = streaming kernel
-// walking k tiles per CTA; -1 = the row kernel with batches of 8.
+// with a plain row loop unrolled 4, 8 times; 10 + k = streaming kernel
+// walking k tiles per CTA; -1 = default (6 when NV*sizeof(T) >= 64 bytes,
+// else 0).
 static int g_spmv_variant = -1;
 void set_spmv_variant(int v) { g_spmv_variant = v; }
 int get_spmv_variant() { return g_spmv_variant; }
@@ -347,14 +329,16 @@ static void spmv_t(i64 n, const int *rp, const int *ci, const T *va, const T *x,
     constexpr int RPB = 256 / Shape<T, NV>::TPR;
     if (n <= 0) return;
     i64 ntiles = (n + RPB - 1) / RPB;
-    int var = g_spmv_variant < 0 ? 1 : g_spmv_variant;
+    // default: the tile-staged kernel when a row spans at least 4 threads (its
+    // tile of RPB rows then fits the shared-memory stage), else batches of 4
+    int var = g_spmv_variant >= 0 ? g_spmv_variant : (Shape<T, NV>::TPR >= 4 ? 6 : 0);
     if (var >= 3 && var <= 6) {
         unsigned g = (unsigned)ntiles;
-#define L(GB, KEEP)                                                                                \
-    if (mode == 0) k_spmv_tile<T, NV, 0, GB, KEEP><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);      \
-    else if (mode == 1) k_spmv_tile<T, NV, 1, GB, KEEP><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b); \
-    else k_spmv_tile<T, NV, 2, GB, KEEP><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
-        if (var == 3) { L(4, false) } else if (var == 4) { L(8, false) } else if (var == 5) { L(4, true) } else { L(8, true) }
+#define L(GB, LOOP)                                                                                \
+    if (mode == 0) k_spmv_tile<T, NV, 0, GB, LOOP><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);      \
+    else if (mode == 1) k_spmv_tile<T, NV, 1, GB, LOOP><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b); \
+    else k_spmv_tile<T, NV, 2, GB, LOOP><<<g, 256, 0, s>>>(n, rp, ci, va, x, y, b);
+        if (var == 3) { L(4, 0) } else if (var == 4) { L(8, 0) } else if (var == 5) { L(4, 1) } else { L(8, 1) }
 #undef L
         return;
     }

@@ -24,8 +24,10 @@ enum class Prec : int { F64 = 0, F32 = 1 };
 void spmv(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val, const void *x,
           void *y, int mode, const void *b, cudaStream_t s);
 // Kernel variant for spmv(): 0, 1, 2 = one CTA per row tile with gather
-// batches of 4, 8, 16 entries; 10 + k = streaming kernel (shared-memory staged
-// entries) walking k tiles per CTA; -1 = default (batches of 8).
+// batches of 4, 8, 16 entries; 3, 4 = tile-staged entries (shared memory) with
+// gather batches of 4, 8; 5, 6 = tile-staged with a plain row loop unrolled 4,
+// 8 times; 10 + k = streaming kernel walking k tiles per CTA; -1 = default
+// (6 when NV*sizeof(T) >= 64 bytes, else 0).  All give identical results.
 void set_spmv_variant(int v);
 int get_spmv_variant();
 
