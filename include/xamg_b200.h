@@ -80,6 +80,33 @@ int XAMG_b200_amg_host_destroy(size_t hid);
 int XAMG_b200_gs_levels_host(int64_t n, const int *rp, const int *ci, int64_t block_rows,
                              int *lf, int *lb, int *nlev);
 
+/* Batching form.  These entry points have no counterpart in the reference.
+ * nsys independent systems (host CSR arrays, int32 indices, FP64 values;
+ * n[q] rows, nv[q] in {1,2,4,8,16,32} right-hand sides each) are solved
+ * together by PBiCGStab (FP64 vectors, inner products and recurrences, one
+ * set of scalars per system and column) preconditioned by AMG in FP32.  The
+ * systems with equal nv form one block-diagonal group; pid supplies the
+ * solver (max_iters, tolerances) and preconditioner/smoother roles.  The
+ * SpMV kernel variant of each group is autotuned at creation.  A solve is one
+ * CUDA-graph launch: every group's iteration runs inside a device-controlled
+ * while loop, so no host round trip happens until all systems converge. */
+int XAMG_b200_batch_create(int nsys, const int64_t *n, const int *const *rp, const int *const *ci,
+                           const double *const *val, const int *nv, XAMG_param_id pid, size_t *bid);
+/* b, x0: host arrays of n[sys] x nv[sys] doubles (row-major); x0 NULL = 0. */
+int XAMG_b200_batch_upload(size_t bid, int sys, const double *b, const double *x0);
+/* use_graph 0: the same steps launched from the host, one check per iteration. */
+int XAMG_b200_batch_set_graph(size_t bid, int use_graph);
+int XAMG_b200_batch_solve(size_t bid);
+int XAMG_b200_batch_download(size_t bid, int sys, double *x);
+/* per column: iterations at convergence (-1 = not converged) and the final
+ * relative residual estimate of the recurrence */
+int XAMG_b200_batch_stats(size_t bid, int sys, int *iters, double *relres);
+double XAMG_b200_batch_last_ms(size_t bid);
+/* groups: {nv, systems, FP64 SpMV variant, FP32 SpMV variant} each (cap ints
+ * in out); returns the group count */
+int XAMG_b200_batch_groups(size_t bid, int *out, int cap);
+int XAMG_b200_batch_destroy(size_t bid);
+
 /* ---- Part 2: kernel-level device interface ----------------------------- */
 
 /* csr_Ax_y / csr_Axpy (blas2/detail/csr_matvec.inl:32-260):

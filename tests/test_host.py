@@ -15,10 +15,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     names = set()
-    for h in ("xamg_c_api.h", "xamg_b200.h"):
+    for h in ("xamg_c_api.h", "xamg_b200.h", "xamg_learned.h"):
         src = open(os.path.join(ROOT, "include", h)).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-        for m in re.finditer(r"\b((?:XAMG|xamg)_\w+)\s*\(", src):
+        for m in re.finditer(r"\b((?:XAMG|xamg|xcnn)_\w+)\s*\(", src):
             if m.group(1) != "XAMG_id_get_comm":
                 names.add(m.group(1))
     return names

@@ -20,8 +20,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB = os.path.join(HERE, "libxamg_b200.so")
 ORACLE_LIB = os.path.join(ROOT, "oracle", "liboracle.so")
 
-CU_SOURCES = ["kernels.cu", "gs.cu", "noalloc.cu", "cnn.cu"]
-CPP_SOURCES = ["host/gen.cpp", "host/amg.cpp", "host/params.cpp", "host/solve.cpp", "host/c_api.cpp"]
+CU_SOURCES = ["kernels.cu", "gs.cu", "noalloc.cu", "cnn.cu", "batch.cu"]
+CPP_SOURCES = ["host/gen.cpp", "host/amg.cpp", "host/params.cpp", "host/solve.cpp", "host/batch.cpp",
+               "host/c_api.cpp"]
 
 
 def _run(cmd):

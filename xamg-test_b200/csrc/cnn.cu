@@ -104,7 +104,8 @@ __device__ __forceinline__ i64 nbr(const Vol &g, i64 v, int t) {
 constexpr int BM = 128;  // voxels per CTA tile
 constexpr int NS = 4;    // pipeline stages
 
-// conv3d: out[v][oc0 + n] (+)= act(bias[n] + sum_t sum_c in[v+off(t)][ic0 + c] w[n][t][c])
+// conv3d: out[v][oc0 + n] (+)= act(bias[n] + sum_t sum_c in[v+off(t)][ic0 + c] w[n][t][c]);
+// flags: 1 ReLU, 2 accumulate, 4 FP32 output (out is then a float buffer)
 template <int BN>
 __global__ void __launch_bounds__(128) k_conv3d(const bf16 *__restrict__ in, int ics, int ic0,
                                                 int cin, const bf16 *__restrict__ w,
@@ -194,7 +195,7 @@ __global__ void __launch_bounds__(128) k_conv3d(const bf16 *__restrict__ in, int
     }
     cp_wait<0>();
     // epilogue: rows g = lane/4 (+8), columns 2*(lane%4) (+1)
-    const bool relu = flags & 1, accum = flags & 2;
+    const bool relu = flags & 1, accum = flags & 2, f32out = flags & 4;
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -212,6 +213,16 @@ __global__ void __launch_bounds__(128) k_conv3d(const bf16 *__restrict__ in, int
                 if (relu) {
                     y0 = fmaxf(y0, 0.f);
                     y1 = fmaxf(y1, 0.f);
+                }
+                if (f32out) {
+                    float2 *pf = reinterpret_cast<float2 *>(reinterpret_cast<float *>(out) + v * ocs + oc0 + n);
+                    if (accum) {
+                        const float2 o = *pf;
+                        y0 += o.x;
+                        y1 += o.y;
+                    }
+                    *pf = make_float2(y0, y1);
+                    continue;
                 }
                 __nv_bfloat162 *po = reinterpret_cast<__nv_bfloat162 *>(out + v * ocs + oc0 + n);
                 if (accum) {
@@ -416,13 +427,13 @@ __global__ void k_up2_bwd(const bf16 *__restrict__ gfine, int gcs, int gc0, bf16
     }
 }
 
-// loss = mean (pred - target)^2 over nvox voxels (pred = channel pc0 of a
-// BF16 volume); grad[p][gc0] = 2 (pred - target) / nvox, other grad channels 0
-__global__ void k_mse(const bf16 *__restrict__ pred, int pcs, int pc0, const float *__restrict__ tgt,
+// loss = mean (pred - target)^2 over nvox voxels (pred = channel pc0 of an
+// FP32 volume); grad[p][0] = 2 (pred - target) / nvox, other grad channels 0
+__global__ void k_mse(const float *__restrict__ pred, int pcs, int pc0, const float *__restrict__ tgt,
                       bf16 *grad, int gcs, i64 nvox, float *loss) {
     float s = 0.f;
     for (i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x; p < nvox; p += (i64)gridDim.x * blockDim.x) {
-        const float d = __bfloat162float(pred[p * pcs + pc0]) - tgt[p];
+        const float d = pred[p * pcs + pc0] - tgt[p];
         s += d * d;
         if (grad) {
             for (int k = 0; k < gcs; ++k) grad[p * gcs + k] = __float2bfloat16(0.f);
@@ -458,10 +469,21 @@ __global__ void k_pack2(const float *__restrict__ a, const float *__restrict__ b
 }
 
 // f32 out[p] = scale[p / per] * bf16 in[p][c0]
-__global__ void k_unpack(const bf16 *__restrict__ in, int cs, int c0, const float *__restrict__ scale,
+__global__ void k_unpack(const float *__restrict__ in, int cs, int c0, const float *__restrict__ scale,
                          i64 per, float *out, i64 nvox) {
     for (i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x; p < nvox; p += (i64)gridDim.x * blockDim.x)
-        out[p] = __bfloat162float(in[p * cs + c0]) * (scale ? scale[p / per] : 1.f);
+        out[p] = in[p * cs + c0] * (scale ? scale[p / per] : 1.f);
+}
+
+// x0 in the solver's block-vector layout: x[v * nv + s] = scale[s] * in[s * per + v][c0]
+__global__ void k_unpack_x0(const float *__restrict__ in, int cs, int c0, const float *__restrict__ scale,
+                            int nv, i64 per, double *x) {
+    const i64 total = per * nv;
+    for (i64 q = (i64)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (i64)gridDim.x * blockDim.x) {
+        const i64 v = q / nv;
+        const int sidx = (int)(q % nv);
+        x[q] = (double)in[(sidx * per + v) * cs + c0] * (double)scale[sidx];
+    }
 }
 
 int grid_for(i64 n) {
@@ -578,7 +600,7 @@ int xcnn_up2_bwd(const void *gfine, int gcs, int gc0, void *gin, int ics, int ic
 
 int xcnn_mse(const void *pred, int pcs, int pc0, const float *tgt, void *grad, int gcs, int64_t nvox,
              float *loss, void *stream) {
-    k_mse<<<grid_for(nvox), 256, 0, (cudaStream_t)stream>>>((const bf16 *)pred, pcs, pc0, tgt, (bf16 *)grad,
+    k_mse<<<grid_for(nvox), 256, 0, (cudaStream_t)stream>>>((const float *)pred, pcs, pc0, tgt, (bf16 *)grad,
                                                             gcs, nvox, loss);
     return last_err();
 }
@@ -597,7 +619,14 @@ int xcnn_pack2(const float *a, const float *b, void *out, int64_t nvox, void *st
 
 int xcnn_unpack(const void *in, int cs, int c0, const float *scale, int64_t per, float *out, int64_t nvox,
                 void *stream) {
-    k_unpack<<<grid_for(nvox), 256, 0, (cudaStream_t)stream>>>((const bf16 *)in, cs, c0, scale, per, out, nvox);
+    k_unpack<<<grid_for(nvox), 256, 0, (cudaStream_t)stream>>>((const float *)in, cs, c0, scale, per, out, nvox);
+    return last_err();
+}
+
+int xcnn_unpack_x0(const void *in, int cs, int c0, const float *scale, int nv, int64_t per, double *x,
+                   void *stream) {
+    if (nv <= 0 || per <= 0 || !scale) return 2;
+    k_unpack_x0<<<grid_for(per * nv), 256, 0, (cudaStream_t)stream>>>((const float *)in, cs, c0, scale, nv, per, x);
     return last_err();
 }
 

@@ -3,6 +3,7 @@
 // include/xamg_b200.h.  Handles are indices into process-global lists and are
 // never reused, as in the reference (xamg_c_api.cpp:66-85).
 #include "solve.h"
+#include "batch.h"
 #include "amg.h"
 #include <chrono>
 #include <cstdlib>
@@ -824,3 +825,61 @@ namespace xamg {
 // that live outside this file).
 void set_last_error(const std::string &msg) { g_err = msg; }
 }  // namespace xamg
+
+// ---- batching form (no counterpart in the reference) -----------------------
+static std::vector<Batch *> blist;
+
+extern "C" {
+int XAMG_b200_batch_create(int nsys, const int64_t *n, const int *const *rp, const int *const *ci,
+                           const double *const *val, const int *nv, XAMG_param_id pid, size_t *bid) {
+    return guard([&] {
+        XCHECK(n && rp && ci && val && nv && bid, "null argument");
+        std::unique_ptr<Batch> B(new Batch());
+        std::vector<i64> nn(n, n + nsys);
+        B->create(nsys, nn.data(), rp, ci, val, nv, *get(plist, pid, "param"));
+        blist.push_back(B.release());
+        *bid = blist.size() - 1;
+    });
+}
+int XAMG_b200_batch_upload(size_t bid, int sys, const double *b, const double *x0) {
+    return guard([&] { get(blist, bid, "batch")->upload(sys, b, x0); });
+}
+int XAMG_b200_batch_set_graph(size_t bid, int use_graph) {
+    return guard([&] { get(blist, bid, "batch")->use_graph = use_graph != 0; });
+}
+int XAMG_b200_batch_solve(size_t bid) {
+    return guard([&] { get(blist, bid, "batch")->solve(); });
+}
+int XAMG_b200_batch_download(size_t bid, int sys, double *x) {
+    return guard([&] { get(blist, bid, "batch")->download(sys, x); });
+}
+int XAMG_b200_batch_stats(size_t bid, int sys, int *iters, double *relres) {
+    return guard([&] { get(blist, bid, "batch")->stats(sys, iters, relres); });
+}
+double XAMG_b200_batch_last_ms(size_t bid) {
+    if (bid >= blist.size() || !blist[bid]) return -1.0;
+    return blist[bid]->last_ms;
+}
+int XAMG_b200_batch_groups(size_t bid, int *out, int cap) {
+    if (bid >= blist.size() || !blist[bid]) return -2;
+    const Batch *B = blist[bid];
+    int g = 0;
+    for (auto &G : B->groups) {
+        if (out && 4 * g + 3 < cap) {
+            out[4 * g] = G->nv;
+            out[4 * g + 1] = (int)G->sys.size();
+            out[4 * g + 2] = G->var64;
+            out[4 * g + 3] = G->var32;
+        }
+        ++g;
+    }
+    return g;
+}
+int XAMG_b200_batch_destroy(size_t bid) {
+    return guard([&] {
+        Batch *B = get(blist, bid, "batch");
+        delete B;
+        blist[bid] = nullptr;
+    });
+}
+}  // extern "C"

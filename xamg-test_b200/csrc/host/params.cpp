@@ -214,7 +214,8 @@ std::string GlobalParams::validate(const std::string &key, char type) {
         {"mg_agg_P12_trunc_factor", 'F'}, {"mg_agg_Pmax_elements", 'I'},
         {"mg_agg_P12max_elements", 'I'},
         // extensions of this library (no reference counterpart)
-        {"hybrid_block_rows", 'I'}, {"inner_rel_tolerance", 'F'}, {"gs_schedule", 'S'}};
+        {"hybrid_block_rows", 'I'}, {"inner_rel_tolerance", 'F'}, {"gs_schedule", 'S'},
+        {"rel_tolerance_base", 'S'}};
     auto it = known.find(key);
     if (it == known.end()) return "unknown parameter: " + key;
     if (it->second != type && !(it->second == 'F' && type == 'I'))

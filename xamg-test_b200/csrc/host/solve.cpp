@@ -357,7 +357,8 @@ int GsPlan::error_flag() const {
 // ------------------------------------------------------------------ Conv
 double Conv::tol(int k) const {
     if (!ptol.empty()) return ptol[k];
-    return std::max(abs_tol, rel_tol * std::sqrt(res0[k]));
+    const double b2 = rhs_base && (int)base.size() == nv ? base[k] : res0[k];
+    return std::max(abs_tol, rel_tol * std::sqrt(b2));
 }
 void Conv::update(const double *r) {
     for (int k = 0; k < nv; ++k)
@@ -392,6 +393,11 @@ static void parse_conv(const ParamList &l, Conv &c) {
     c.check_on = cd.count("nocheck") == 0;
     if (l.has("abs_tolerance")) c.abs_tol = l.get_float("abs_tolerance");
     if (l.has("rel_tolerance")) c.rel_tol = l.get_float("rel_tolerance");
+    if (l.has("rel_tolerance_base")) {
+        const std::string b = l.get_string("rel_tolerance_base");
+        if (b != "rhs" && b != "initial") throw Error("rel_tolerance_base must be \"initial\" or \"rhs\"", 4);
+        c.rhs_base = b == "rhs";
+    }
 }
 
 // ------------------------------------------------------------------ helpers
@@ -402,6 +408,18 @@ static void dot1(const DVec &a, const DVec &b, DBuf &part, double *out, cudaStre
 static void ensure_part(DBuf &part, i64 n, int nd, int nv) {
     size_t need = sizeof(double) * std::max<i64>(xk::dot_part_size(n, nd, nv), 1);
     if (part.bytes < need) part.alloc(need);
+}
+
+// ||b||^2 per column as the base of the relative tolerance (rel_tolerance_base = rhs)
+static void set_rhs_base(Conv &c, const DVec &b, DBuf &part) {
+    if (!c.rhs_base) return;
+    cudaStream_t s = ctx().stream;
+    ensure_part(part, b.n, 1, b.nv);
+    DBuf out(sizeof(double) * b.nv);
+    dot1(b, b, part, out.as<double>(), s);
+    c.base.assign(b.nv, 0.0);
+    XCUDA(cudaMemcpyAsync(c.base.data(), out.p, sizeof(double) * b.nv, cudaMemcpyDeviceToHost, s));
+    XCUDA(cudaStreamSynchronize(s));
 }
 
 struct Pinned {
@@ -512,6 +530,7 @@ struct HSGS : Solver {
     void solve(DVec &x, const DVec &b) override {
         int iters = (int)prm.get_int("max_iters");
         conv.init(nv);
+        set_rhs_base(conv, b, part);
         if (conv.check_on && residual_check(x, b, true)) return;
         for (int it = 1; it <= iters; ++it) {
             conv.iters = it;
@@ -548,6 +567,7 @@ struct Jacobi : Solver {
         cudaStream_t s = ctx().stream;
         int iters = (int)prm.get_int("max_iters");
         conv.init(nv);
+        set_rhs_base(conv, b, part);
         if (!conv.check_on) {
             // nocheck path (jacobi.inl:91-100): x_{k+1} = x_k + relax*D^-1 (b - A x_k),
             // ping-ponging between x and tmp
@@ -740,6 +760,7 @@ struct MultiGrid : Solver {
     void solve(DVec &x, const DVec &b) override {
         int iters = (int)prm.get_int("max_iters");
         conv.init(nv);
+        set_rhs_base(conv, b, part);
         if (conv.check_on && residual_check(x, b, true)) return;
         for (int it = 1; it <= iters; ++it) {
             conv.iters = it;
@@ -814,6 +835,7 @@ struct Krylov : Solver {
         const DCsr &a = dA();
         std::vector<double> ic(NSC * nv, 0.0);
         conv.init(nv);
+        set_rhs_base(conv, b, part);
         {
             std::vector<double> one(nv, 1.0);
             XCUDA(cudaMemcpyAsync(S(ICONV), one.data(), sizeof(double) * nv, cudaMemcpyHostToDevice, st));
@@ -912,6 +934,7 @@ struct IterRefine : Solver {
         cudaStream_t s = ctx().stream;
         int max_iters = (int)prm.get_int("max_iters");
         conv.init(nv);
+        set_rhs_base(conv, b, part);
         if (residual_check(x, b, true)) return;
         for (int it = 1; it <= max_iters; ++it) {
             conv.iters = it;
@@ -1006,6 +1029,11 @@ static std::unique_ptr<Solver> make_solver(const GlobalParams &gp, const std::st
         return o;
     }
     throw Error("method not implemented on the device path: " + m, 4);
+}
+
+std::unique_ptr<Solver> make_role_solver(const GlobalParams &gp, const std::string &role, Matrix &A,
+                                         int nv, Prec prec) {
+    return make_solver(gp, role, A, nv, prec);
 }
 
 std::unique_ptr<Solver> build_solver_tree(const GlobalParams &gp, Matrix &A, int nv) {

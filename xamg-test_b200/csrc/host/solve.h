@@ -95,6 +95,10 @@ struct Conv {
     bool check_on = true, print_on = false;
     double abs_tol = 0, rel_tol = 0;
     std::vector<double> ptol;  // per-column tolerance (IR inner solver)
+    // rel_tolerance applies to ||b|| instead of the initial residual
+    // (extension key rel_tolerance_base = "rhs"); base holds ||b||^2
+    bool rhs_base = false;
+    std::vector<double> base;
     std::vector<double> res0, res;
     std::vector<int> status;
     int iters = 0, sub_iters = 0;
@@ -155,6 +159,9 @@ struct Matrix {
 };
 
 std::unique_ptr<Solver> build_solver_tree(const GlobalParams &gp, Matrix &A, int nv);
+// The solver of one role of gp (e.g. the preconditioner) in precision prec.
+std::unique_ptr<Solver> make_role_solver(const GlobalParams &gp, const std::string &role, Matrix &A,
+                                         int nv, Prec prec);
 
 // Export hooks for parity tests.
 struct MultiGrid;

@@ -929,16 +929,18 @@ void convert(Prec from, Prec to, i64 count, const void *x, void *y, cudaStream_t
 
 // ---------------------------------------------------------------- scalars
 __global__ void k_alpha(int nv, const double *rho, const double *s1, double *alpha) {
-    int k = threadIdx.x;
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < nv) alpha[k] = __ddiv_rn(rho[k], s1[k]);
 }
+// one thread per column; nv may exceed a warp (batched systems: nsys * nv columns)
+static unsigned sblocks(int nv) { return (unsigned)((nv + 127) / 128); }
 void bicg_alpha(int nv, const double *rho, const double *s1, double *alpha, cudaStream_t s) {
-    k_alpha<<<1, 32, 0, s>>>(nv, rho, s1, alpha);
+    k_alpha<<<sblocks(nv), 128, 0, s>>>(nv, rho, s1, alpha);
 }
 __global__ void k_omega(int nv, const double *s2, const double *s3, const double *s4,
                         const double *alpha, const double *iconv, double *omega, double *res,
                         double *ac, double *oc) {
-    int k = threadIdx.x;
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nv) return;
     double w = __ddiv_rn(s2[k], s3[k]);
     omega[k] = w;
@@ -950,11 +952,11 @@ __global__ void k_omega(int nv, const double *s2, const double *s3, const double
 void bicg_omega(int nv, const double *s2, const double *s3, const double *s4,
                 const double *alpha, const double *iconv, double *omega, double *res,
                 double *ac, double *oc, cudaStream_t s) {
-    k_omega<<<1, 32, 0, s>>>(nv, s2, s3, s4, alpha, iconv, omega, res, ac, oc);
+    k_omega<<<sblocks(nv), 128, 0, s>>>(nv, s2, s3, s4, alpha, iconv, omega, res, ac, oc);
 }
 __global__ void k_beta(int nv, const double *s1, double *rho, const double *alpha,
                        const double *omega, double *beta, double *c1) {
-    int k = threadIdx.x;
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nv) return;
     double a2 = __ddiv_rn(s1[k], rho[k]);
     double a3 = __ddiv_rn(alpha[k], omega[k]);
@@ -965,12 +967,14 @@ __global__ void k_beta(int nv, const double *s1, double *rho, const double *alph
 }
 void bicg_beta(int nv, const double *s1, double *rho, const double *alpha, const double *omega,
                double *beta, double *c1, cudaStream_t s) {
-    k_beta<<<1, 32, 0, s>>>(nv, s1, rho, alpha, omega, beta, c1);
+    k_beta<<<sblocks(nv), 128, 0, s>>>(nv, s1, rho, alpha, omega, beta, c1);
 }
 __global__ void k_neg(int nv, const double *in, double *out) {
-    int k = threadIdx.x;
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < nv) out[k] = dmul(-1.0, in[k]);
 }
-void negate(int nv, const double *in, double *out, cudaStream_t s) { k_neg<<<1, 32, 0, s>>>(nv, in, out); }
+void negate(int nv, const double *in, double *out, cudaStream_t s) {
+    k_neg<<<sblocks(nv), 128, 0, s>>>(nv, in, out);
+}
 
 }  // namespace xk

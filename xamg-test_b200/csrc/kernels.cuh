@@ -122,4 +122,30 @@ void bicg_beta(int nv, const double *s1, double *rho, const double *alpha, const
 // negate: out = -1 * in
 void negate(int nv, const double *in, double *out, cudaStream_t s);
 
+// ---- batched independent systems (batch.cu) ---------------------------------
+// Segment s owns rows [segoff[s], segoff[s+1]) of the concatenated system;
+// its scalars for column k are at [s*nv + k] (nsc = nseg*nv of them).
+// Inner products per segment, identical to dots() run on each segment alone:
+// cstart[s] = first chunk of segment s (256-row chunks counted per segment,
+// nseg+1 entries), part: nchunks*nd*nv doubles, out[d*nsc + s*nv + k].
+void seg_dots(Prec in, int nv, int nseg, const i64 *segoff, const i64 *cstart, i64 nchunks, int nd,
+              const void *const *a, const void *const *b, double *part, double *out, cudaStream_t s);
+// FP64 z = a*x + b*y (op 0) or z = a*x + b*y + c*z (op 1), per-segment scalars
+void seg_blas(int nv, int nseg, const i64 *segoff, i64 n, int op, const double *a, const double *x,
+              const double *b, const double *y, const double *c, double *z, cudaStream_t s);
+// tol2 = max(abs, rel*sqrt(res0))^2; iconv = 1 where the column is not yet
+// converged; conv_it = 0; ctr = {iterations = 0, active columns}
+void batch_init(int nsc, const double *res0, double rel, double abs_tol, double *tol2, double *iconv,
+                int *conv_it, int *ctr, cudaStream_t s);
+// omega = s2/s3; res = s4 - omega*s2; ac, oc = alpha, omega on active columns
+// and exactly 0 on the others (so a finished column's x never changes)
+void batch_omega(int nsc, const double *s2, const double *s3, const double *s4, const double *alpha,
+                 const double *iconv, double *omega, double *res, double *ac, double *oc, cudaStream_t s);
+// end of an iteration: active columns with res <= tol2 stop (conv_it = the
+// iteration); ctr[0] += 1, ctr[1] = active columns; under a CUDA graph the
+// while-loop condition `handle` is set to (active && ctr[0] < max_iters)
+void batch_check(int nsc, const double *res, const double *tol2, double *iconv, int *conv_it,
+                 double *res_last, int *ctr, int max_iters, unsigned long long handle, int use_graph,
+                 cudaStream_t s);
+
 }  // namespace xk

@@ -122,6 +122,15 @@ def lib():
             "xamg_dot_noalloc": (C.c_int, [C.c_int, C.c_int, i64, C.c_int, P, P, P, P]),
             "xamg_blas": (C.c_int, [C.c_int, C.c_int, i64, C.c_int, P, P, P, P, P, P, P]),
             "xamg_dense_gemv": (C.c_int, [C.c_int, C.c_int, C.c_int, P, P, P, P]),
+            "XAMG_b200_batch_create": (C.c_int, [C.c_int, P, P, P, P, P, sz, C.POINTER(sz)]),
+            "XAMG_b200_batch_upload": (C.c_int, [sz, C.c_int, P, P]),
+            "XAMG_b200_batch_set_graph": (C.c_int, [sz, C.c_int]),
+            "XAMG_b200_batch_solve": (C.c_int, [sz]),
+            "XAMG_b200_batch_download": (C.c_int, [sz, C.c_int, P]),
+            "XAMG_b200_batch_stats": (C.c_int, [sz, C.c_int, P, P]),
+            "XAMG_b200_batch_last_ms": (C.c_double, [sz]),
+            "XAMG_b200_batch_groups": (C.c_int, [sz, P, C.c_int]),
+            "XAMG_b200_batch_destroy": (C.c_int, [sz]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -431,3 +440,61 @@ def gs_levels_host(rp, ci, block_rows=0):
 def device_ptr(t):
     """Device pointer of a torch tensor (or None)."""
     return None if t is None else C.c_void_p(t.data_ptr())
+
+
+class Batch:
+    """Independent systems solved together (XAMG_b200_batch_*): systems is a
+    list of (CsrMatrix, nv); params supplies the solver and preconditioner."""
+
+    def __init__(self, systems, params):
+        arrs = [m.arrays() for m, _ in systems]
+        self._keep = [(np.ascontiguousarray(rp, np.int32), np.ascontiguousarray(ci, np.int32),
+                       np.ascontiguousarray(v, np.float64)) for rp, ci, v in arrs]
+        ns = len(systems)
+        self.n = [len(k[0]) - 1 for k in self._keep]
+        self.nv = [int(nv) for _, nv in systems]
+        n = np.array(self.n, np.int64)
+        nv = np.array(self.nv, np.int32)
+        rp = (C.c_void_p * ns)(*[k[0].ctypes.data for k in self._keep])
+        ci = (C.c_void_p * ns)(*[k[1].ctypes.data for k in self._keep])
+        v = (C.c_void_p * ns)(*[k[2].ctypes.data for k in self._keep])
+        h = C.c_size_t()
+        check(lib().XAMG_b200_batch_create(ns, _ptr(n), rp, ci, v, _ptr(nv), params.h, C.byref(h)))
+        self.h = h.value
+        self.params = params
+
+    def upload(self, sys, b, x0=None):
+        b = np.ascontiguousarray(b, np.float64).reshape(self.n[sys], self.nv[sys])
+        x0 = None if x0 is None else np.ascontiguousarray(x0, np.float64).reshape(self.n[sys], self.nv[sys])
+        check(lib().XAMG_b200_batch_upload(self.h, sys, _ptr(b), None if x0 is None else _ptr(x0)))
+
+    def set_graph(self, on):
+        check(lib().XAMG_b200_batch_set_graph(self.h, int(bool(on))))
+
+    def solve(self):
+        check(lib().XAMG_b200_batch_solve(self.h))
+
+    def download(self, sys):
+        out = np.empty((self.n[sys], self.nv[sys]))
+        check(lib().XAMG_b200_batch_download(self.h, sys, _ptr(out)))
+        return out
+
+    def stats(self, sys):
+        it = np.zeros(self.nv[sys], np.int32)
+        rr = np.zeros(self.nv[sys])
+        check(lib().XAMG_b200_batch_stats(self.h, sys, _ptr(it), _ptr(rr)))
+        return it, rr
+
+    def last_ms(self):
+        return lib().XAMG_b200_batch_last_ms(self.h)
+
+    def groups(self):
+        out = np.zeros(4 * 64, np.int32)
+        g = lib().XAMG_b200_batch_groups(self.h, _ptr(out), out.size)
+        return [tuple(int(v) for v in out[4 * i:4 * i + 4]) for i in range(g)]
+
+    def __del__(self):
+        try:
+            lib().XAMG_b200_batch_destroy(self.h)
+        except Exception:
+            pass
