@@ -29,6 +29,8 @@ int XAMG_b200_set_nv(int nv);
 const char *XAMG_b200_last_error(void);
 /* Wait for all queued device work of the library. */
 int XAMG_b200_synchronize(void);
+/* Kernels launched by this library since it was loaded (every launcher counts). */
+long long XAMG_b200_kernel_launches(void);
 /* Raw device pointer of a device-resident vector (FP64, size x nv). */
 void *XAMG_b200_vector_device_ptr(XAMG_vector_id vid);
 /* Convergence detail of the last solve: squared residual norms after each
@@ -102,6 +104,8 @@ int XAMG_b200_batch_download(size_t bid, int sys, double *x);
  * relative residual estimate of the recurrence */
 int XAMG_b200_batch_stats(size_t bid, int sys, int *iters, double *relres);
 double XAMG_b200_batch_last_ms(size_t bid);
+/* kernels executed by the last batch solve (graph: init + iterations x body) */
+long long XAMG_b200_batch_last_kernels(size_t bid);
 /* groups: {nv, systems, FP64 SpMV variant, FP32 SpMV variant} each (cap ints
  * in out); returns the group count */
 int XAMG_b200_batch_groups(size_t bid, int *out, int cap);

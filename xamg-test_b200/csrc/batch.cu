@@ -178,6 +178,7 @@ template <class TI, int NV>
 static void segdots_t(int nseg, const i64 *segoff, const i64 *cstart, i64 nch, int nd,
                       const void *const *a, const void *const *b, double *part, double *out,
                       cudaStream_t s) {
+    note_launch(nch > 0 ? 2 : 1);
     if (nch > 0) {
         const unsigned g = (unsigned)((nch + 7) / 8);
         const TI *A0 = (const TI *)a[0], *B0 = (const TI *)b[0];
@@ -224,23 +225,27 @@ void seg_blas(int nv, int nseg, const i64 *segoff, i64 n, int op, const double *
     const i64 total = n * nv;
     if (total <= 0) return;
     const unsigned g = (unsigned)((total + 255) / 256);
+    note_launch();
     if (op == 0) k_segblas<0><<<g, 256, 0, s>>>(nv, nseg, segoff, total, a, x, b, y, c, z);
     else k_segblas<1><<<g, 256, 0, s>>>(nv, nseg, segoff, total, a, x, b, y, c, z);
 }
 
 void batch_init(int nsc, const double *res0, double rel, double abs_tol, double *tol2, double *iconv,
                 int *conv_it, int *ctr, cudaStream_t s) {
+    note_launch();
     k_binit<<<1, 1024, 0, s>>>(nsc, res0, rel, abs_tol, tol2, iconv, conv_it, ctr);
 }
 
 void batch_omega(int nsc, const double *s2, const double *s3, const double *s4, const double *alpha,
                  const double *iconv, double *omega, double *res, double *ac, double *oc, cudaStream_t s) {
+    note_launch();
     k_bomega<<<(unsigned)((nsc + 127) / 128), 128, 0, s>>>(nsc, s2, s3, s4, alpha, iconv, omega, res, ac, oc);
 }
 
 void batch_check(int nsc, const double *res, const double *tol2, double *iconv, int *conv_it,
                  double *res_last, int *ctr, int max_iters, unsigned long long handle, int use_graph,
                  cudaStream_t s) {
+    note_launch();
     k_bcheck<<<1, 1024, 0, s>>>(nsc, res, tol2, iconv, conv_it, res_last, ctr, max_iters,
                                 (cudaGraphConditionalHandle)handle, use_graph);
 }

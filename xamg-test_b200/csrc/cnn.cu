@@ -21,11 +21,11 @@
 //              weights (weight_flip).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include "kernels.cuh"
 #include <cstdint>
 #include <cstdio>
 
 typedef __nv_bfloat16 bf16;
-typedef int64_t i64;
 
 namespace {
 
@@ -492,6 +492,7 @@ int grid_for(i64 n) {
 }
 
 int last_err() {
+    xk::note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         fprintf(stderr, "xcnn: %s\n", cudaGetErrorString(e));

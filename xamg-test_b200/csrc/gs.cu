@@ -453,6 +453,7 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp,
     const T *tt = (const T *)t;
     T *xx = (T *)x;
     const T *rl = (const T *)relax;
+    note_launch();
     if (mode == 1) {
         if (xs) {
             size_t sm = (size_t)brows * NV * sizeof(T);

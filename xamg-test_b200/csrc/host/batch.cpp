@@ -214,7 +214,9 @@ void Batch::build_graph() {
         G.cond = (unsigned long long)h;
         // initialisation: new root nodes of the graph (groups are independent)
         XCUDA(cudaStreamBeginCaptureToGraph(st, graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        long long k0 = xk::launch_count();
         run_init(G);
+        G.init_kernels = xk::launch_count() - k0;
         cudaStreamCaptureStatus cst;
         const cudaGraphNode_t *deps = nullptr;
         size_t nd = 0;
@@ -232,7 +234,9 @@ void Batch::build_graph() {
         XCUDA(cudaGraphAddNode(&cn, graph, last.data(), last.size(), &cp));
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         XCUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        k0 = xk::launch_count();
         run_body(G, 1);
+        G.body_kernels = xk::launch_count() - k0;
         cudaGraph_t b2 = nullptr;
         XCUDA(cudaStreamEndCapture(st, &b2));
     }
@@ -262,6 +266,7 @@ void Batch::solve() {
         xk::set_spmv_variant(old);
         build_graph();
     }
+    const long long k0 = xk::launch_count();
     XCUDA(cudaEventRecord(e0, st));
     if (use_graph) {
         XCUDA(cudaGraphLaunch(exec, st));
@@ -291,6 +296,17 @@ void Batch::solve() {
     last_ms = ms;
     XCUDA(cudaEventDestroy(e0));
     XCUDA(cudaEventDestroy(e1));
+    if (use_graph) {
+        // kernels the graph executed: every group's init plus its iterations
+        last_kernels = 0;
+        for (auto &G : groups) {
+            int c[2];
+            XCUDA(cudaMemcpy(c, G->ctr.p, sizeof(c), cudaMemcpyDeviceToHost));
+            last_kernels += G->init_kernels + (long long)c[0] * G->body_kernels;
+        }
+    } else {
+        last_kernels = xk::launch_count() - k0;
+    }
 }
 
 void Batch::upload(int sys, const double *b, const double *x0) {

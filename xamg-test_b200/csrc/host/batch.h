@@ -26,6 +26,7 @@ struct BatchGroup {
     int nsc = 0;
     int var64 = -1, var32 = -1;             // autotuned SpMV variants (FP64 outer, FP32 hierarchy)
     unsigned long long cond = 0;            // CUDA-graph while-loop handle
+    long long init_kernels = 0, body_kernels = 0;  // kernels of the init steps / one iteration
     double *S(int i) const;
 };
 
@@ -40,6 +41,7 @@ struct Batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     double last_ms = 0.0;
+    long long last_kernels = 0;  // kernel executions of the last solve
     bool use_graph = true;
 
     void create(int nsys, const i64 *n, const int *const *rp, const int *const *ci,

@@ -860,6 +860,11 @@ double XAMG_b200_batch_last_ms(size_t bid) {
     if (bid >= blist.size() || !blist[bid]) return -1.0;
     return blist[bid]->last_ms;
 }
+long long XAMG_b200_batch_last_kernels(size_t bid) {
+    if (bid >= blist.size() || !blist[bid]) return -1;
+    return blist[bid]->last_kernels;
+}
+long long XAMG_b200_kernel_launches(void) { return xk::launch_count(); }
 int XAMG_b200_batch_groups(size_t bid, int *out, int cap) {
     if (bid >= blist.size() || !blist[bid]) return -2;
     const Batch *B = blist[bid];

@@ -381,6 +381,18 @@ bool Conv::check() {
     return all;
 }
 
+// Rows per hybrid Gauss-Seidel block of an n-row level: hybrid_blocks = P
+// splits every level into P equal blocks (the reference's semantics on P
+// cores, whose partition divides each level's rows among the processes);
+// otherwise hybrid_block_rows, 0 meaning the single-process sweep.
+static i64 hsgs_block_rows(const ParamList &pl, i64 n) {
+    if (pl.has("hybrid_blocks") && pl.get_int("hybrid_blocks") > 0) {
+        const i64 P = pl.get_int("hybrid_blocks");
+        return P >= 2 ? (n + P - 1) / P : 0;
+    }
+    return pl.has("hybrid_block_rows") ? (i64)pl.get_int("hybrid_block_rows") : 0;
+}
+
 static void parse_conv(const ParamList &l, Conv &c) {
     std::set<std::string> cd;
     std::string s = l.has("convergence_details") ? l.get_string("convergence_details") : "nocheck,noprint";
@@ -676,7 +688,7 @@ struct MultiGrid : Solver {
         op.A = &dA;
         op.invd = m.prec == Prec::F64 ? m.invd64.p : m.invd32.p;
         if (meth == "HSGS") {
-            i64 br = pl.has("hybrid_block_rows") ? (i64)pl.get_int("hybrid_block_rows") : 0;
+            i64 br = hsgs_block_rows(pl, hA.n);
             GsMode md = gs_mode_from(pl.has("gs_schedule") ? pl.get_string("gs_schedule") : "auto", br, hA.n);
             GsPlan &g = pre ? m.gs_pre : m.gs_post;
             i64 brn = br > 0 && br < hA.n ? br : 0;
@@ -1012,7 +1024,7 @@ static std::unique_ptr<Solver> make_solver(const GlobalParams &gp, const std::st
         op.A = &A.d;
         op.invd = prec == Prec::F64 ? o->invd64.p : o->invd32.p;
         if (m == "HSGS") {
-            i64 br = pl.has("hybrid_block_rows") ? (i64)pl.get_int("hybrid_block_rows") : 0;
+            i64 br = hsgs_block_rows(pl, A.h.n);
             o->gs.build(A.h, br, gs_mode_from(pl.has("gs_schedule") ? pl.get_string("gs_schedule") : "auto", br, A.h.n));
             o->gs.build_lcsr(A.h, prec);
             op.gs = &o->gs;

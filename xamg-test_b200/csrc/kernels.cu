@@ -13,6 +13,7 @@
 //    to the oracle.
 #include "kernels.cuh"
 #include <cooperative_groups.h>
+#include <atomic>
 #include <algorithm>
 #include <cstdio>
 
@@ -310,6 +311,11 @@ __global__ void __launch_bounds__(256, LOOP == 1 ? 6 : 1) k_spmv_tile(i64 n, con
 // else 0).
 static int g_spmv_variant = -1;
 void set_spmv_variant(int v) { g_spmv_variant = v; }
+
+// kernels launched by this library (all launchers count here)
+static std::atomic<long long> g_launches{0};
+void note_launch(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 int get_spmv_variant() { return g_spmv_variant; }
 
 static int sm_count() {
@@ -328,6 +334,7 @@ static void spmv_t(i64 n, const int *rp, const int *ci, const T *va, const T *x,
                    const T *b, cudaStream_t s) {
     constexpr int RPB = 256 / Shape<T, NV>::TPR;
     if (n <= 0) return;
+    note_launch();
     i64 ntiles = (n + RPB - 1) / RPB;
     // default: the tile-staged kernel when a row spans at least 4 threads (its
     // tile of RPB rows then fits the shared-memory stage), else batches of 4
@@ -478,6 +485,7 @@ void gs_blocks(Prec p, int nv, int nblocks, const int *blevf, const int *lptrf, 
                const void *val, const void *invd, const void *t, void *x, const void *relax,
                i64 brows, cudaStream_t s) {
     if (nblocks <= 0) return;
+    note_launch();
     if (p == Prec::F64) {
 #define F(NV) k_gs_blocks<double, NV><<<nblocks, 256, 0, s>>>(blevf, lptrf, permf, blevb, lptrb, permb, rp, ci, (const double *)val, (const double *)invd, (const double *)t, (double *)x, (const double *)relax, brows)
         NV_DISPATCH(nv, F)
@@ -507,6 +515,7 @@ void gs_level(Prec p, int nv, int cnt, const int *rows, const int *rp, const int
               const void *val, const void *invd, const void *t, void *x, const void *relax,
               i64 brows, cudaStream_t s) {
     if (cnt <= 0) return;
+    note_launch();
     if (p == Prec::F64) {
 #define F(NV) k_gs_level<double, NV><<<(cnt * Shape<double, NV>::TPR + 255) / 256, 256, 0, s>>>(cnt, rows, rp, ci, (const double *)val, (const double *)invd, (const double *)t, (double *)x, (const double *)relax, brows)
         NV_DISPATCH(nv, F)
@@ -595,6 +604,7 @@ static cudaError_t gs_sweep_t(int nlev, const int *lptr, const int *perm, const 
         nblk = sms * per;
     }
     void *args[] = {&nlev, &lptr, &perm, &rp, &ci, &va, &invd, &t, &x, &relax, &brows, &bar, &err};
+    note_launch();
     return cudaLaunchCooperativeKernel((const void *)k_gs_sweep<T, NV>, dim3(nblk), dim3(256),
                                        args, 0, s);
 }
@@ -652,6 +662,7 @@ __global__ void __launch_bounds__(256) k_offblock(i64 n, const int *__restrict__
 void offblock_resid(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val,
                     const void *b, const void *x, void *t, i64 brows, cudaStream_t s) {
     if (n <= 0) return;
+    note_launch();
     if (p == Prec::F64) {
 #define F(NV) k_offblock<double, NV><<<(unsigned)((n + 256 / Shape<double, NV>::TPR - 1) / (256 / Shape<double, NV>::TPR)), 256, 0, s>>>(n, rp, ci, (const double *)val, (const double *)b, (const double *)x, (double *)t, brows)
         NV_DISPATCH(nv, F)
@@ -705,6 +716,7 @@ void jacobi(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val
             const void *invd, const void *b, const void *xi, void *xo, const void *relax,
             cudaStream_t s) {
     if (n <= 0) return;
+    note_launch();
     if (p == Prec::F64) {
 #define F(NV) k_jacobi<double, NV><<<(unsigned)((n + 256 / Shape<double, NV>::TPR - 1) / (256 / Shape<double, NV>::TPR)), 256, 0, s>>>(n, rp, ci, (const double *)val, (const double *)invd, (const double *)b, (const double *)xi, (double *)xo, (const double *)relax)
         NV_DISPATCH(nv, F)
@@ -732,6 +744,7 @@ __global__ void __launch_bounds__(256) k_dense(int n, int nv, const T *__restric
 void dense_gemv(Prec p, int nv, int n, const void *AinvT, const void *b, void *y, cudaStream_t s) {
     i64 tot = (i64)n * nv;
     if (tot <= 0) return;
+    note_launch();
     unsigned g = (unsigned)((tot + 255) / 256);
     if (p == Prec::F64) k_dense<double><<<g, 256, 0, s>>>(n, nv, (const double *)AinvT, (const double *)b, (double *)y);
     else k_dense<float><<<g, 256, 0, s>>>(n, nv, (const float *)AinvT, (const float *)b, (float *)y);
@@ -824,6 +837,7 @@ static void dots_t(i64 n, int nd, const void *const *a, const void *const *b, do
     const TI *A0 = (const TI *)a[0], *B0 = (const TI *)b[0];
     const TI *A1 = nd > 1 ? (const TI *)a[1] : A0, *B1 = nd > 1 ? (const TI *)b[1] : B0;
     const TI *A2 = nd > 2 ? (const TI *)a[2] : A0, *B2 = nd > 2 ? (const TI *)b[2] : B0;
+    note_launch(2);
     if (nd == 1) k_dot1<TI, NV, 1><<<g, 256, 0, s>>>(n, nch, A0, B0, A1, B1, A2, B2, part);
     else if (nd == 2) k_dot1<TI, NV, 2><<<g, 256, 0, s>>>(n, nch, A0, B0, A1, B1, A2, B2, part);
     else k_dot1<TI, NV, 3><<<g, 256, 0, s>>>(n, nch, A0, B0, A1, B1, A2, B2, part);
@@ -877,6 +891,7 @@ static void blas_t(i64 n, Op op, const double *a, const T *x, const double *b, c
                    const double *c, T *z, cudaStream_t s) {
     i64 tot = n * NV;
     if (tot <= 0) return;
+    note_launch();
     unsigned g = (unsigned)((tot + 255) / 256);
     switch (op) {
     case Op::AXPBY_Z: k_blas<T, NV, 0><<<g, 256, 0, s>>>(tot, a, x, b, y, c, z); break;
@@ -908,6 +923,7 @@ __global__ void k_fill(i64 cnt, T v, T *z) {
 }
 void fill(Prec p, i64 count, double v, void *z, cudaStream_t s) {
     if (count <= 0) return;
+    note_launch();
     unsigned g = (unsigned)((count + 255) / 256);
     if (p == Prec::F64) k_fill<double><<<g, 256, 0, s>>>(count, v, (double *)z);
     else k_fill<float><<<g, 256, 0, s>>>(count, (float)v, (float *)z);
@@ -920,6 +936,7 @@ __global__ void k_conv(i64 cnt, const A *x, B *y) {
 }
 void convert(Prec from, Prec to, i64 count, const void *x, void *y, cudaStream_t s) {
     if (count <= 0) return;
+    note_launch();
     unsigned g = (unsigned)((count + 255) / 256);
     if (from == Prec::F64 && to == Prec::F32) k_conv<double, float><<<g, 256, 0, s>>>(count, (const double *)x, (float *)y);
     else if (from == Prec::F32 && to == Prec::F64) k_conv<float, double><<<g, 256, 0, s>>>(count, (const float *)x, (double *)y);
@@ -935,6 +952,7 @@ __global__ void k_alpha(int nv, const double *rho, const double *s1, double *alp
 // one thread per column; nv may exceed a warp (batched systems: nsys * nv columns)
 static unsigned sblocks(int nv) { return (unsigned)((nv + 127) / 128); }
 void bicg_alpha(int nv, const double *rho, const double *s1, double *alpha, cudaStream_t s) {
+    note_launch();
     k_alpha<<<sblocks(nv), 128, 0, s>>>(nv, rho, s1, alpha);
 }
 __global__ void k_omega(int nv, const double *s2, const double *s3, const double *s4,
@@ -952,6 +970,7 @@ __global__ void k_omega(int nv, const double *s2, const double *s3, const double
 void bicg_omega(int nv, const double *s2, const double *s3, const double *s4,
                 const double *alpha, const double *iconv, double *omega, double *res,
                 double *ac, double *oc, cudaStream_t s) {
+    note_launch();
     k_omega<<<sblocks(nv), 128, 0, s>>>(nv, s2, s3, s4, alpha, iconv, omega, res, ac, oc);
 }
 __global__ void k_beta(int nv, const double *s1, double *rho, const double *alpha,
@@ -967,6 +986,7 @@ __global__ void k_beta(int nv, const double *s1, double *rho, const double *alph
 }
 void bicg_beta(int nv, const double *s1, double *rho, const double *alpha, const double *omega,
                double *beta, double *c1, cudaStream_t s) {
+    note_launch();
     k_beta<<<sblocks(nv), 128, 0, s>>>(nv, s1, rho, alpha, omega, beta, c1);
 }
 __global__ void k_neg(int nv, const double *in, double *out) {
@@ -974,6 +994,7 @@ __global__ void k_neg(int nv, const double *in, double *out) {
     if (k < nv) out[k] = dmul(-1.0, in[k]);
 }
 void negate(int nv, const double *in, double *out, cudaStream_t s) {
+    note_launch();
     k_neg<<<sblocks(nv), 128, 0, s>>>(nv, in, out);
 }
 

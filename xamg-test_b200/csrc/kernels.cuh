@@ -19,6 +19,10 @@ namespace xk {
 
 enum class Prec : int { F64 = 0, F32 = 1 };
 
+// Count of kernels this library has launched (every launcher adds its own).
+void note_launch(int k = 1);
+long long launch_count();
+
 // ---- sparse matrix-vector products ---------------------------------------
 // y = A x (mode 0), y += A x (mode 1), y = b - A x (mode 2, b given).
 void spmv(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val, const void *x,

@@ -129,6 +129,8 @@ def lib():
             "XAMG_b200_batch_download": (C.c_int, [sz, C.c_int, P]),
             "XAMG_b200_batch_stats": (C.c_int, [sz, C.c_int, P, P]),
             "XAMG_b200_batch_last_ms": (C.c_double, [sz]),
+            "XAMG_b200_batch_last_kernels": (C.c_longlong, [sz]),
+            "XAMG_b200_kernel_launches": (C.c_longlong, []),
             "XAMG_b200_batch_groups": (C.c_int, [sz, P, C.c_int]),
             "XAMG_b200_batch_destroy": (C.c_int, [sz]),
         }
@@ -148,6 +150,11 @@ def check(rc):
 
 def _ptr(a):
     return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def kernel_launches():
+    """Kernels launched by the library so far (its own launch counter)."""
+    return lib().XAMG_b200_kernel_launches()
 
 
 def init(nv=1):
@@ -487,6 +494,9 @@ class Batch:
 
     def last_ms(self):
         return lib().XAMG_b200_batch_last_ms(self.h)
+
+    def last_kernels(self):
+        return lib().XAMG_b200_batch_last_kernels(self.h)
 
     def groups(self):
         out = np.zeros(4 * 64, np.int32)
