@@ -8,8 +8,15 @@ guess.  Forms:
   mixed  - FP64 iterative refinement around an FP32 PBiCGStab (FP64 inner
            products and recurrences) with an FP32 AMG V-cycle whose SGS runs
            the reference's hybrid block semantics with GPU-sized blocks.
-The headline `value` is the fastest form's device time per RHS; `e2e` repeats
-it through the XAMG C API with host buffers (pinned), copies included.
+  batch  - 64 independent 7-point lognormal-coefficient systems (sides 16..96,
+           nv in {1,2,4,8}) solved together in one CUDA-graph launch (FP64
+           Krylov, FP32 AMG, autotuned SpMV per group); reported beside;
+  learned - held-out 64^3 bump-coefficient systems (nv = 8) from a zero guess
+           and from the trained network's guess; reported beside.
+The headline `value` is the faster of plain/mixed's device time per RHS on the
+128^3 problem; `e2e` repeats it through the XAMG C API with host buffers
+(pinned), copies included.  `gpu_launches` is the library's own count of the
+kernels it launched in the timed steps of that form.
 
 --impl reference times the CPU restatement of the reference's algorithm (the
 reference itself cannot be built here: it needs MPI, hypre, argsparser and
@@ -47,13 +54,13 @@ def plain_spec():
     }
 
 
-def mixed_spec(block_rows=N_GRID * N_GRID, inner_rel=1e-4):
+def mixed_spec(blocks=128, inner_rel=1e-4):
     s = plain_spec()
     s["meta_solver"] = {"method": "IterativeRefinement", "max_iters": 20, "abs_tolerance": 0.0,
                         "rel_tolerance": 1e-8, "subsolver_reduced_precision": True,
                         "inner_rel_tolerance": inner_rel, "convergence_details": "check-L2,noprint"}
-    s["pre_smoother"]["hybrid_block_rows"] = block_rows
-    s["post_smoother"]["hybrid_block_rows"] = block_rows
+    s["pre_smoother"]["hybrid_blocks"] = blocks
+    s["post_smoother"]["hybrid_blocks"] = blocks
     return s
 
 
@@ -190,15 +197,17 @@ def run_form(csr, B, spec, warmup, steps):
         x.set(0.0)
         s.solve()
     times = []
+    k0 = xamg.kernel_launches()
     for _ in range(steps):
         x.set(0.0)
         s.solve()
         times.append(s.last_ms())
+    launches = xamg.kernel_launches() - k0
     X = x.download()
     it = s.iters()
     return {"ms": float(np.mean(times)), "ms_all": [round(t, 3) for t in times], "iters": it[0],
             "sub_iters": it[1], "converged": all(s.converged()), "setup_s": round(setup_s, 1),
-            "levels": s.info()}, X, (s, A, x, b)
+            "levels": s.info(), "launches": launches}, X, (s, A, x, b)
 
 
 def e2e_form(csr, B, spec, warmup, steps):
@@ -227,6 +236,80 @@ def e2e_form(csr, B, spec, warmup, steps):
     for _ in range(steps):
         step()
     return (time.perf_counter() - t0) / steps * 1e3
+
+
+def batch_form(rank, world, warmup, steps):
+    """Batching form: 64 independent 7-point lognormal-coefficient systems
+    (sides log-uniform in [16, 96], nv in {1, 2, 4, 8}) solved together, one
+    CUDA-graph launch per solve; whole systems are sharded over the ranks."""
+    import scipy.sparse as sp
+    import xamg
+    import families
+    mem = [families.batch_member(sd) for sd in range(1, 65)]
+    w = [A.nnz * nv for A, nv, _ in mem]
+    mine = families.shard(w, world)[rank]
+    t0 = time.time()
+    batch = xamg.Batch([(mem[i][0], mem[i][1]) for i in mine], xamg.Params(families.batch_spec(block_rows=1024)))
+    setup_s = time.time() - t0
+
+    def load():
+        for q, i in enumerate(mine):
+            batch.upload(q, mem[i][2])
+
+    for _ in range(max(warmup, 1)):
+        load()
+        batch.solve()
+    ms, kern = [], 0
+    for _ in range(steps):
+        load()
+        batch.solve()
+        ms.append(batch.last_ms())
+        kern += batch.last_kernels()
+    # end to end: host right-hand sides in, host solutions out
+    t0 = time.perf_counter()
+    load()
+    batch.solve()
+    Xs = [batch.download(q) for q in range(len(mine))]
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    its, res = [], []
+    for q, i in enumerate(mine):
+        A, nv, B = mem[i]
+        it, _ = batch.stats(q)
+        its.append(it)
+        rp, ci, v = A.arrays()
+        M = sp.csr_matrix((v, ci, rp), shape=(A.nrows, A.nrows))
+        res.append(float(np.max(np.linalg.norm(B - M @ Xs[q], axis=0) / np.linalg.norm(B, axis=0))))
+    its = np.concatenate(its)
+    rhs = sum(mem[i][1] for i in mine)
+    return {"ms": float(np.mean(ms)), "ms_all": [round(t, 2) for t in ms], "systems": len(mine), "rhs": int(rhs),
+            "rows": int(sum(mem[i][0].nrows for i in mine)), "iters_min": int(its.min()), "iters_max": int(its.max()),
+            "converged": bool(np.all(its >= 0)), "max_true_rel_residual": max(res), "setup_s": round(setup_s, 1),
+            "groups": batch.groups(), "e2e_ms": round(e2e_ms, 2), "launches": int(kern),
+            "h2d_bytes": int(sum(mem[i][2].nbytes for i in mine)), "d2h_bytes": int(sum(x.nbytes for x in Xs))}
+
+
+LEARNED_WEIGHTS = os.path.join(ROOT, "xamg-test_b200", "weights", "learned_64.npz")
+
+
+def learned_form(nsys=16):
+    """Learned form: held-out 64^3 bump-coefficient systems (nv = 8) solved
+    from a zero guess and from the trained network's guess (4 symmetric
+    Gauss-Seidel sweeps on it first); time to 1e-8 relative to ||b|| with the
+    inference and the sweeps included."""
+    if not os.path.exists(LEARNED_WEIGHTS):
+        return {"unavailable": "no trained weights at xamg-test_b200/weights/learned_64.npz"}
+    import learned
+    net = learned.Net(seed=1)
+    net.load(LEARNED_WEIGHTS)
+    ev = learned.evaluate(net, list(range(200001, 200001 + nsys)), 64, 8)
+    out = {"systems": nsys, "rhs": nsys * 8, "n": 64}
+    for k in ("its_zero", "its_x0", "ms_zero", "ms_x0", "ms_infer", "ms_smooth", "guess_rel_res", "guess_rel_err",
+              "rel_diff"):
+        out["mean_" + k] = round(float(np.mean([e[k] for e in ev])), 5)
+    out["ms_per_rhs_zero"] = round(out["mean_ms_zero"] / 8, 4)
+    out["ms_per_rhs_x0"] = round(out["mean_ms_x0"] / 8, 4)
+    out["converged"] = all(e["converged"] for e in ev)
+    return out
 
 
 def cpu_sample(csr, B, s_plain):
@@ -325,7 +408,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--forms", default="plain,mixed")
+    ap.add_argument("--forms", default="plain,mixed,batch,learned")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-iters", type=int, default=12)
     ap.add_argument("--kernel", choices=["spmv", "gs"], help="time one hot kernel alone (profiling)")
@@ -351,7 +434,8 @@ def main():
     csr, B = build_problem()
     best_var, var_ms = tune_spmv(csr, 0)
     xamg.lib().xamg_spmv_set_variant(best_var)
-    forms = args.forms.split(",")
+    allforms = args.forms.split(",")
+    forms = [f for f in allforms if f in ("plain", "mixed")]
     res = {}
     keep = {}
     X = {}
@@ -372,6 +456,19 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         for i, f in enumerate(forms):
             res[f]["ms"] = float(t[i])
+    extra = {}
+    if "batch" in allforms:
+        extra["batch"] = batch_form(rank, world, args.warmup, args.steps)
+        if dist:
+            t = torch.tensor([extra["batch"]["ms"], extra["batch"]["rhs"]], device="cuda", dtype=torch.float64)
+            mx = t.clone()
+            dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+            dist.all_reduce(t, op=dist.ReduceOp.SUM)
+            extra["batch"]["ms"], extra["batch"]["rhs_all_ranks"] = float(mx[0]), int(t[1])
+        tot = extra["batch"].get("rhs_all_ranks", extra["batch"]["rhs"])
+        extra["batch"]["ms_per_rhs"] = round(extra["batch"]["ms"] / tot, 4)
+    if "learned" in allforms and rank == 0:
+        extra["learned"] = learned_form()
     best = min(forms, key=lambda f: res[f]["ms"])
     spec_best = plain_spec() if best == "plain" else mixed_spec()
     e2e_ms = e2e_form(csr, B, spec_best, 1, max(2, args.steps // 2))
@@ -397,12 +494,13 @@ def main():
         "config": {"workload": "27pt-aniso-128^3 AMG-PBiCGStab nv=16", "n": N_GRID, "nv": NV,
                    "rows": csr.nrows, "nnz": csr.nnz, "parallelism": "replicas" if world > 1 else "1gpu",
                    "form": best, "l2": "inputs larger than L2 (matrix 669 MB)"},
-        "forms": {f: {k: res[f][k] for k in ("ms", "iters", "sub_iters", "converged", "setup_s")} for f in forms},
+        "forms": dict({f: {k: res[f][k] for k in ("ms", "iters", "sub_iters", "converged", "setup_s", "launches")}
+                       for f in forms}, **extra),
         "mixed_vs_plain_rel_err": err,
         "e2e": {"value": round(e2e_ms / NV, 4), "unit": "ms/RHS", "h2d_bytes_per_step": csr.nrows * NV * 8,
                 "d2h_bytes_per_step": csr.nrows * NV * 8},
         "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-        "gpu_launches": None,
+        "gpu_launches": res[best]["launches"],
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -190,5 +190,5 @@ def test_trained_network_saves_iterations(gpu):
     ev = learned.evaluate(net, [900001, 900002, 900003, 900004, 900005, 900006], n, nv)
     assert all(e["converged"] for e in ev)
     assert np.mean([e["guess_rel_err"] for e in ev]) < 0.3
-    assert np.mean([e["inner_x0"] for e in ev]) < np.mean([e["inner_zero"] for e in ev])
+    assert np.mean([e["its_x0"] for e in ev]) < np.mean([e["its_zero"] for e in ev])
     assert max(e["rel_diff"] for e in ev) < 1e-6

@@ -305,20 +305,23 @@ class Net:
         return out
 
     def save(self, path):
+        """Weights as used by the forward pass (BF16 bits) and FP32 biases."""
+        torch = self.torch
         d = {"scale": np.array([self.scale])}
         for name, *_ in LAYERS:
-            d["w_" + name] = self.w32[name].cpu().numpy()
+            d["wb_" + name] = self.wbf[name].view(torch.int16).cpu().numpy()
             d["b_" + name] = self.b32[name].cpu().numpy()
-        np.savez(path, **d)
+        np.savez_compressed(path, **d)
 
     def load(self, path):
         torch = self.torch
         z = np.load(path)
         self.scale = float(z["scale"][0])
         for name, *_ in LAYERS:
-            self.w32[name].copy_(torch.from_numpy(z["w_" + name]))
+            wb = torch.from_numpy(z["wb_" + name]).view(torch.bfloat16).cuda()
+            self.wbf[name].copy_(wb)
+            self.w32[name].copy_(wb.float())
             self.b32[name].copy_(torch.from_numpy(z["b_" + name]))
-            self.wbf[name].copy_(self.w32[name].to(torch.bfloat16))
 
 
 # ------------------------------------------------------------------ family
@@ -367,21 +370,33 @@ def make_system(seed, n):
     return A, (np.log(k) / 4.0).astype(np.float32), rng
 
 
-def solver_spec(rel_tol=1e-8, base="rhs", block_rows=4096):
-    """AMG-PBiCGStab (FP32 hierarchy inside FP64 iterative refinement) with the
-    relative tolerance measured against ||b|| so that a good x0 pays off."""
-    return {
-        "meta_solver": {"method": "IterativeRefinement", "max_iters": 30, "abs_tolerance": 0.0,
-                        "rel_tolerance": rel_tol, "rel_tolerance_base": base, "subsolver_reduced_precision": True,
-                        "inner_rel_tolerance": 1e-4, "convergence_details": "check-L2,noprint"},
+def solver_spec(rel_tol=1e-8, base="rhs", blocks=256, mixed=False):
+    """AMG-PBiCGStab with the relative tolerance measured against ||b|| (so
+    that a good x0 pays off) and hybrid SGS on `blocks` blocks per level.
+    mixed = True wraps an FP32 solver in FP64 iterative refinement."""
+    sp = {
         "solver": {"method": "PBiCGStab", "max_iters": 200, "abs_tolerance": 0.0, "rel_tolerance": rel_tol,
-                   "convergence_details": "check-L2,noprint"},
+                   "rel_tolerance_base": base, "convergence_details": "check-L2,noprint"},
         "preconditioner": {"method": "MultiGrid", "mg_coarsening_type": 10, "mg_interpolation_type": 6,
                            "mg_strength_threshold": 0.25, "mg_max_levels": 6, "mg_agg_num_levels": 0},
-        "pre_smoother": {"method": "HSGS", "max_iters": 1, "hybrid_block_rows": block_rows},
-        "post_smoother": {"method": "HSGS", "max_iters": 1, "hybrid_block_rows": block_rows},
+        "pre_smoother": {"method": "HSGS", "max_iters": 1, "hybrid_blocks": blocks},
+        "post_smoother": {"method": "HSGS", "max_iters": 1, "hybrid_blocks": blocks},
         "coarse_grid_solver": {"method": "Direct"},
     }
+    if mixed:
+        sp["meta_solver"] = {"method": "IterativeRefinement", "max_iters": 30, "abs_tolerance": 0.0,
+                             "rel_tolerance": rel_tol, "rel_tolerance_base": base,
+                             "subsolver_reduced_precision": True, "inner_rel_tolerance": 1e-4,
+                             "convergence_details": "check-L2,noprint"}
+        sp["solver"].pop("rel_tolerance_base")
+    return sp
+
+
+def smoother_spec(sweeps=2, blocks=256):
+    """Symmetric Gauss-Seidel sweeps applied to the network's guess before the
+    solve: they remove the guess's high-frequency error, which otherwise
+    dominates its residual."""
+    return {"solver": {"method": "HSGS", "max_iters": sweeps, "hybrid_blocks": blocks}}
 
 
 # ------------------------------------------------------- data and training
@@ -454,11 +469,12 @@ def train(net, data, epochs, batch=8, lr=1e-3, seed=0, log=None):
     return hist, ev0.elapsed_time(ev1)
 
 
-def evaluate(net, seeds, n, nv, log=None):
-    """Per held-out system: iterations and device time to 1e-8 (relative to
-    ||b||) from a zero guess and from the network's guess (inference time
-    included), the initial relative residual of the guess, and the difference
-    of the two solutions."""
+def evaluate(net, seeds, n, nv, log=None, sweeps=4, mixed=False):
+    """Per held-out system: Krylov iterations and device time to 1e-8
+    (relative to ||b||) from a zero guess and from the network's guess
+    smoothed by `sweeps` symmetric Gauss-Seidel sweeps (inference and
+    smoothing time included), the guess's relative error before smoothing and
+    relative residual after it, and the difference of the two solutions."""
     import torch
     L = klib()
     out = []
@@ -471,7 +487,8 @@ def evaluate(net, seeds, n, nv, log=None):
         M = xamg.Matrix(A)
         xv, bv = xamg.Vector(A.nrows, nv), xamg.Vector(A.nrows, nv)
         bv.upload(Bm)
-        s = xamg.Solver(M, xamg.Params(solver_spec()), xv, bv)
+        s = xamg.Solver(M, xamg.Params(solver_spec(mixed=mixed)), xv, bv)
+        sm = xamg.Solver(M, xamg.Params(smoother_spec(sweeps)), xv, bv) if sweeps > 0 else None
         # zero guess (run twice: the first solve also warms up the plan)
         for _ in range(2):
             xv.set(0.0)
@@ -497,6 +514,10 @@ def evaluate(net, seeds, n, nv, log=None):
         ms_inf = e0.elapsed_time(e1)
         G = xv.download()
         err0 = float(np.linalg.norm(G - X0) / np.linalg.norm(X0))
+        ms_sm = 0.0
+        if sm is not None:
+            sm.solve()
+            ms_sm = sm.last_ms()
         s.solve()
         it1, ms1 = s.iters(), s.last_ms()
         X1 = xv.download()
@@ -505,14 +526,14 @@ def evaluate(net, seeds, n, nv, log=None):
         bb2 = np.sum(Bm * Bm, axis=0)
         rel0 = float(np.sqrt(np.mean(h1[0] / bb2)))
         diff = float(np.linalg.norm(X1 - X0) / np.linalg.norm(X0))
-        # iterations: refinement steps and the FP32 PBiCGStab iterations inside them
-        out.append({"seed": seed, "iters_zero": it0[0], "inner_zero": it0[1], "ms_zero": ms0,
-                    "iters_x0": it1[0], "inner_x0": it1[1], "ms_x0": ms1 + ms_inf,
-                    "ms_infer": ms_inf, "guess_rel_res": rel0, "guess_rel_err": err0, "rel_diff": diff,
+        # Krylov iterations (the inner FP32 ones under iterative refinement)
+        out.append({"seed": seed, "its_zero": it0[1] if mixed else it0[0], "its_x0": it1[1] if mixed else it1[0],
+                    "ms_zero": ms0, "ms_x0": ms1 + ms_inf + ms_sm, "ms_infer": ms_inf, "ms_smooth": ms_sm,
+                    "guess_rel_res": rel0, "guess_rel_err": err0, "rel_diff": diff,
                     "converged": bool(all(s.converged()))})
         if log:
-            log("seed %d: zero %d/%d it %.2f ms | x0 %d/%d it %.2f ms (infer %.2f) | guess res %.3e err %.3e" %
-                (seed, it0[0], it0[1], ms0, it1[0], it1[1], ms1 + ms_inf, ms_inf, rel0, err0))
+            log("seed %d: zero %d it %.2f ms | x0 %d it %.2f ms (infer %.2f smooth %.2f) | res %.3e err %.3e" %
+                (seed, out[-1]["its_zero"], ms0, out[-1]["its_x0"], ms1 + ms_inf + ms_sm, ms_inf, ms_sm, rel0, err0))
     return out
 
 
@@ -551,7 +572,7 @@ def main():
         if args.weights:
             net.save(args.weights)
     ev = evaluate(net, list(range(100001, 100001 + args.eval_systems)), args.n, args.nv, log=log)
-    for k in ("iters_zero", "inner_zero", "iters_x0", "inner_x0", "ms_zero", "ms_x0", "ms_infer", "guess_rel_res",
+    for k in ("its_zero", "its_x0", "ms_zero", "ms_x0", "ms_infer", "ms_smooth", "guess_rel_res",
               "guess_rel_err", "rel_diff"):
         res["mean_" + k] = float(np.mean([e[k] for e in ev]))
     res["all_converged"] = all(e["converged"] for e in ev)
