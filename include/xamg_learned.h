@@ -28,6 +28,11 @@ extern "C" {
 int xcnn_conv3d(const void *in, int ics, int ic0, int cin, const void *w, const float *bias,
                 void *out, int ocs, int oc0, int cout, int nb, int d, int h, int wd, int flags,
                 void *stream);
+/* Kernel choice of xcnn_conv3d (same convolution either way): 1 (default) =
+ * box kernel where the volume tiles into 2 x 8 x 8 voxel boxes (each input
+ * voxel staged once per 16-channel chunk), 0 = voxel-tile kernel.  Returns the
+ * previous setting. */
+int xcnn_set_box_conv(int on);
 /* dw[co][t][ci] += sum_p grad[p][gc0+co] * in[p + off(t)][ic0+ci]; cout is
  * 16, 32, 64 or 128. */
 int xcnn_conv3d_wgrad(const void *in, int ics, int ic0, int cin, const void *grad, int gcs,

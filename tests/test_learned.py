@@ -65,12 +65,14 @@ def _np(t):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("dims", [(2, 8, 8, 8), (1, 6, 10, 12)])
+@pytest.mark.parametrize("dims", [(2, 8, 8, 8), (1, 6, 10, 12), (1, 4, 16, 24)])
 @pytest.mark.parametrize("cin,cout", [(16, 16), (48, 64), (32, 48), (16, 128)])
-def test_conv3d_matches_oracle(gpu, dims, cin, cout):
+@pytest.mark.parametrize("box", [1, 0])
+def test_conv3d_matches_oracle(gpu, dims, cin, cout, box):
     import torch
     import learned
     L = learned.klib()
+    old = L.xcnn_set_box_conv(box)
     rng = np.random.default_rng(cin * 7 + cout)
     nb, d, h, w = dims
     # input window: channels [16, 16 + cin) of a buffer with cin + 32 channels
@@ -104,6 +106,7 @@ def test_conv3d_matches_oracle(gpu, dims, cin, cout):
                          nb, d, h, w, 4, None) == 0
     got = _np(O)[..., 16:16 + cout]
     assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max()
+    L.xcnn_set_box_conv(old)
 
 
 @pytest.mark.gpu

@@ -234,6 +234,130 @@ __global__ void __launch_bounds__(128) k_conv3d(const bf16 *__restrict__ in, int
             }
 }
 
+// conv3d on boxes: the CTA's 128 output voxels form a bz x by x bx box (the
+// volume's sides are multiples of it); for every 16-channel chunk the box's
+// halo ((bz+2)(by+2)(bx+2) voxels) and the chunk's weights for all 27 taps are
+// staged once in shared memory, and the A operand of tap t is read by
+// ldmatrix straight from the halo with per-lane row addresses, so each input
+// voxel is fetched once per chunk instead of once per tap.  Same result
+// definition as k_conv3d (the FP32 summation runs chunk-major).
+template <int BN>
+__global__ void __launch_bounds__(128) k_conv3d_box(const bf16 *__restrict__ in, int ics, int ic0,
+                                                    int cin, const bf16 *__restrict__ w,
+                                                    const float *__restrict__ bias, bf16 *out, int ocs,
+                                                    int oc0, int cout, Vol g, int bz, int by, int bx,
+                                                    int flags) {
+    extern __shared__ __align__(128) unsigned char dyn[];
+    const int hz = bz + 2, hy = by + 2, hx = bx + 2, nh = hz * hy * hx;
+    unsigned char *sa = dyn;                 // nh rows of 32 bytes
+    unsigned char *sb = dyn + nh * 32;       // 27 * BN rows of 32 bytes
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // box origin
+    const int nbx = g.w / bx, nby = g.h / by, nbz = g.d / bz;
+    int q = blockIdx.x;
+    const int ix = q % nbx; q /= nbx;
+    const int iy = q % nby; q /= nby;
+    const int iz = q % nbz;
+    const int b = q / nbz;
+    const int x0 = ix * bx, y0 = iy * by, z0 = iz * bz;
+    const int n0 = blockIdx.y * BN;
+    const int kc = cin / 16;
+
+    float acc[2][BN / 8][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < BN / 8; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+
+    // halo row of this lane's A rows, relative to the tap offset (0,0,0)
+    int hrow[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const int m = warp * 32 + i * 16 + (lane & 15);
+        const int mx = m % bx, my = (m / bx) % by, mz = m / (bx * by);
+        hrow[i] = (mz * hy + my) * hx + mx;
+    }
+    for (int c = 0; c < kc; ++c) {
+        const int cb = c * 16;
+        __syncthreads();  // the previous chunk's reads are done
+        for (int r = tid; r < nh * 2; r += 128) {
+            const int hrw = r >> 1, hh = r & 1;
+            const int lx = hrw % hx, ly = (hrw / hx) % hy, lz = hrw / (hx * hy);
+            const int gx = x0 + lx - 1, gy = y0 + ly - 1, gz = z0 + lz - 1;
+            const bool inside = (unsigned)gx < (unsigned)g.w && (unsigned)gy < (unsigned)g.h &&
+                                (unsigned)gz < (unsigned)g.d;
+            const i64 v = inside ? (((i64)b * g.d + gz) * g.h + gy) * g.w + gx : 0;
+            cp16(sa + sw32(hrw, hh), in + v * ics + ic0 + cb + hh * 8, inside ? 16u : 0u);
+        }
+        for (int r = tid; r < 27 * BN * 2; r += 128) {
+            const int row = r >> 1, hh = r & 1;  // row = t * BN + n
+            const int t = row / BN, nn = row % BN;
+            cp16(sb + sw32(row, hh), w + ((i64)(n0 + nn) * 27 + t) * cin + cb + hh * 8, 16u);
+        }
+        cp_commit();
+        cp_wait<0>();
+        __syncthreads();
+#pragma unroll 1
+        for (int t = 0; t < 27; ++t) {
+            const int toff = ((t / 9) * hy + (t / 3) % 3) * hx + t % 3;
+            unsigned a[2][4];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) ldm_x4(a[i], sa + sw32(hrow[i] + toff, lane >> 4));
+#pragma unroll
+            for (int j = 0; j < BN / 16; ++j) {
+                const int r = t * BN + j * 16 + (lane & 7) + ((lane >> 4) << 3);
+                unsigned bq[4];
+                ldm_x4(bq, sb + sw32(r, (lane >> 3) & 1));
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    mma16816(acc[i][2 * j], a[i], bq[0], bq[1]);
+                    mma16816(acc[i][2 * j + 1], a[i], bq[2], bq[3]);
+                }
+            }
+        }
+    }
+    const bool relu = flags & 1, accum = flags & 2, f32out = flags & 4;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < BN / 8; ++j)
+#pragma unroll
+            for (int hr = 0; hr < 2; ++hr) {
+                const int m = warp * 32 + i * 16 + (lane >> 2) + hr * 8;
+                const int mx = m % bx, my = (m / bx) % by, mz = m / (bx * by);
+                const i64 v = (((i64)b * g.d + z0 + mz) * g.h + y0 + my) * g.w + x0 + mx;
+                const int n = n0 + j * 8 + 2 * (lane & 3);
+                float y0v = acc[i][j][2 * hr], y1v = acc[i][j][2 * hr + 1];
+                if (bias) {
+                    y0v += bias[n];
+                    y1v += bias[n + 1];
+                }
+                if (relu) {
+                    y0v = fmaxf(y0v, 0.f);
+                    y1v = fmaxf(y1v, 0.f);
+                }
+                if (f32out) {
+                    float2 *pf = reinterpret_cast<float2 *>(reinterpret_cast<float *>(out) + v * ocs + oc0 + n);
+                    if (accum) {
+                        const float2 o = *pf;
+                        y0v += o.x;
+                        y1v += o.y;
+                    }
+                    *pf = make_float2(y0v, y1v);
+                    continue;
+                }
+                __nv_bfloat162 *po = reinterpret_cast<__nv_bfloat162 *>(out + v * ocs + oc0 + n);
+                if (accum) {
+                    const float2 o = __bfloat1622float2(*po);
+                    y0v += o.x;
+                    y1v += o.y;
+                }
+                *po = __floats2bfloat162_rn(y0v, y1v);
+            }
+}
+
 // wgrad: dw[co][t][ci] += sum over the CTA's voxel slice of g[p][co] * in[p + off(t)][ci]
 // grid (slices, 27, cin/16); 4 warps split the slice, then reduce in shared memory.
 template <int CO>
@@ -486,6 +610,11 @@ __global__ void k_unpack_x0(const float *__restrict__ in, int cs, int c0, const 
     }
 }
 
+// the box kernel is the default; xcnn_set_box_conv(0) selects the
+// voxel-tile kernel (both compute the same convolution)
+int g_box_conv = 1;
+bool box_conv_enabled() { return g_box_conv != 0; }
+
 int grid_for(i64 n) {
     i64 g = (n + 255) / 256;
     return (int)(g < 148 * 16 ? (g < 1 ? 1 : g) : 148 * 16);
@@ -516,10 +645,26 @@ int xcnn_conv3d(const void *in, int ics, int ic0, int cin, const void *w, const 
     const i64 nvox = (i64)nb * d * h * wd;
     cudaStream_t s = (cudaStream_t)stream;
     const int bn = cout % 64 == 0 ? 64 : (cout % 32 == 0 ? 32 : 16);
-    dim3 grid((unsigned)((nvox + BM - 1) / BM), (unsigned)(cout / bn));
     const bf16 *pi = (const bf16 *)in;
     const bf16 *pw = (const bf16 *)w;
     bf16 *po = (bf16 *)out;
+    // box kernel when the volume tiles into 128-voxel boxes of at least 8 x 8
+    // in (y, x): sides multiples of 8 and a depth that is a multiple of 2
+    const int bx = 8, by = 8, bz = 2;
+    if (box_conv_enabled() && wd % bx == 0 && h % by == 0 && d % bz == 0) {
+        dim3 gb((unsigned)((i64)nb * (d / bz) * (h / by) * (wd / bx)), (unsigned)(cout / bn));
+        const int sm = (bz + 2) * (by + 2) * (bx + 2) * 32 + 27 * bn * 32;
+#define LB(BN)                                                                                     \
+    {                                                                                              \
+        auto k = k_conv3d_box<BN>;                                                                 \
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);                 \
+        k<<<gb, 128, sm, s>>>(pi, ics, ic0, cin, pw, bias, po, ocs, oc0, cout, g, bz, by, bx, flags); \
+    }
+        if (bn == 64) LB(64) else if (bn == 32) LB(32) else LB(16)
+#undef LB
+        return last_err();
+    }
+    dim3 grid((unsigned)((nvox + BM - 1) / BM), (unsigned)(cout / bn));
     if (bn == 64) k_conv3d<64><<<grid, 128, 0, s>>>(pi, ics, ic0, cin, pw, bias, po, ocs, oc0, cout, g, flags);
     else if (bn == 32) k_conv3d<32><<<grid, 128, 0, s>>>(pi, ics, ic0, cin, pw, bias, po, ocs, oc0, cout, g, flags);
     else k_conv3d<16><<<grid, 128, 0, s>>>(pi, ics, ic0, cin, pw, bias, po, ocs, oc0, cout, g, flags);
@@ -629,6 +774,12 @@ int xcnn_unpack_x0(const void *in, int cs, int c0, const float *scale, int nv, i
     if (nv <= 0 || per <= 0 || !scale) return 2;
     k_unpack_x0<<<grid_for(per * nv), 256, 0, (cudaStream_t)stream>>>((const float *)in, cs, c0, scale, nv, per, x);
     return last_err();
+}
+
+int xcnn_set_box_conv(int on) {
+    const int old = g_box_conv;
+    g_box_conv = on != 0;
+    return old;
 }
 
 }  // extern "C"

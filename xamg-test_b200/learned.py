@@ -63,6 +63,7 @@ _SIGS = {
                   C.c_float, C.c_float, C.c_int, C.c_void_p],
     "xcnn_pack2": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p],
     "xcnn_unpack": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p],
+    "xcnn_set_box_conv": [C.c_int],
     "xcnn_unpack_x0": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p],
 }
 
@@ -396,7 +397,8 @@ def smoother_spec(sweeps=2, blocks=256):
     """Symmetric Gauss-Seidel sweeps applied to the network's guess before the
     solve: they remove the guess's high-frequency error, which otherwise
     dominates its residual."""
-    return {"solver": {"method": "HSGS", "max_iters": sweeps, "hybrid_blocks": blocks}}
+    return {"solver": {"method": "HSGS", "max_iters": sweeps, "hybrid_blocks": blocks,
+                       "convergence_details": "nocheck,noprint"}}
 
 
 # ------------------------------------------------------- data and training
