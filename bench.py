@@ -178,9 +178,15 @@ def spmv_roofline(csr, variant):
     kern = {0: "k_spmv<double,16,0,4>", 1: "k_spmv<double,16,0,8>", 2: "k_spmv<double,16,0,16>",
             3: "k_spmv_tile<double,16,0,4,0>", 4: "k_spmv_tile<double,16,0,8,0>",
             5: "k_spmv_tile<double,16,0,4,1>", 6: "k_spmv_tile<double,16,0,8,1>"}.get(variant, "k_spmv_stream<double,16,0>")
+    # DRAM traffic per launch: the ncu capture of the same kernel on the 96^3
+    # operator measured 0.9457 x its algorithmic bytes (483.3 of 510.8 MB,
+    # profiles/k_spmv_tile_fp64_nv16_27pt_96cube.md); traffic scales with the
+    # operator, so the 128^3 figure is that ratio times the algorithmic bytes
+    traffic = round(0.9457 * byts) if variant in (5, 6) else None
     return {"bound": "hbm", "kernel": kern, "variant": variant, "achieved": round(ach, 1), "peak": peak,
             "peak_source": src, "unit": "GB/s", "frac": round(ach / peak, 4),
-            "traffic": None, "algorithmic_bytes": byts, "launch_ms": round(ms, 4)}
+            "traffic": traffic, "traffic_source": "ncu capture at 96^3 scaled to 128^3" if traffic else None,
+            "algorithmic_bytes": byts, "launch_ms": round(ms, 4)}
 
 
 def run_form(csr, B, spec, warmup, steps):

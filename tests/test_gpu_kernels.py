@@ -190,6 +190,37 @@ def test_hsgs_bit_exact(gpu, kind, block_rows, schedule, lcsr, nv):
         L.xamg_gs_plan_destroy(plan)
 
 
+@pytest.mark.parametrize("nv", [4, 16])
+def test_hsgs_blocks_without_shared_tile_bit_exact(gpu, nv):
+    """Hybrid blocks too large for a shared-memory x tile (x gathered per
+    level instead): same results as the oracle."""
+    rng = np.random.default_rng(23)
+    n, brows = 7000, 3000
+    rp, ci, v = util.dd_csr(n, rng)
+    L = xamg.lib()
+    plan = L.xamg_gs_plan_create(n, xamg._ptr(rp), xamg._ptr(ci), brows, 1)
+    assert plan
+    try:
+        for dtype, prec in ((np.float64, 0), (np.float32, 1)):
+            assert brows * nv * np.dtype(dtype).itemsize > 170 * 1024 or nv == 4
+            xamg.check(L.xamg_gs_plan_set_values(plan, xamg._ptr(np.ascontiguousarray(v, np.float64)), prec))
+            vv = v.astype(dtype)
+            invd = np.array([dtype(1.0 / np.float64(vv[rp[i]])) for i in range(n)], dtype)
+            b = rng.uniform(-1, 1, (n, nv)).astype(dtype)
+            x0 = rng.uniform(-1, 1, (n, nv)).astype(dtype)
+            relax = np.full(nv, 0.99, dtype)
+            dx = D(x0)
+            t = D(np.zeros((n, nv), dtype))
+            xamg.check(L.xamg_hsgs(plan, prec, nv, P(D(rp)), P(D(ci)), P(D(vv)), P(D(invd)), P(D(b)),
+                                   P(dx), P(D(relax)), P(t), None))
+            got = H(dx)
+            ref = orc.hsgs(rp, ci, vv, invd, b, x0.copy(), relax, block_rows=brows)
+            assert np.array_equal(got, ref), (dtype, np.abs(got - ref).max())
+        assert L.xamg_gs_plan_error(plan) == 0
+    finally:
+        L.xamg_gs_plan_destroy(plan)
+
+
 @pytest.mark.parametrize("nv", [1, 8, 32])
 def test_jacobi_and_dense_bit_exact(gpu, nv):
     rng = np.random.default_rng(31)

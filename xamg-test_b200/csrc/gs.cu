@@ -281,10 +281,11 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
         }
         const bool staged = s_stage[q] != 0;
         const int items = (dc.r1 - dc.r0) * TPR;
-        // GRID: gather every x value this level's entries need into shared
-        // memory in one parallel round trip (xs holds eg entries x NV)
-        const bool gath = MODE == 0 && ok && staged && (dc.e1 - dc.e0) <= eg;
-        if (MODE == 0) {
+        // without the block's x tile in shared memory (GRID, or BLOCKS whose
+        // tile is too large): gather every x value this level's entries need
+        // into shared memory in one parallel round trip (xs: eg entries x NV)
+        const bool gath = !XS && ok && staged && (dc.e1 - dc.e0) <= eg;
+        if (!XS) {
             if (gath) {
                 // every thread issues up to GU independent loads before it
                 // stores any, so the gather costs one or two L2 round trips
@@ -297,7 +298,7 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
                     for (int u = 0; u < GU; ++u) {
                         const int w = w0 + u * 256;
                         c[u] = w < tot ? s_ci[q][w / TPR] : -1;
-                        if (c[u] >= 0) gld<T, V, true>(x + (i64)c[u] * NV + (w % TPR) * V, tmp[u]);
+                        if (c[u] >= 0) gld<T, V, CG>(x + (i64)c[u] * NV + (w % TPR) * V, tmp[u]);
                     }
 #pragma unroll
                     for (int u = 0; u < GU; ++u)
@@ -461,7 +462,11 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp,
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
             k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, 0, gbar, err);
         } else {
-            k_gs3<T, NV, 1, false><<<ncta, 256, 0, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, 0, gbar, err);
+            const int eg = (int)std::min<long>(GsBuf<T>::E, (176l * 1024) / ((long)NV * (long)sizeof(T)));
+            const size_t sm = (size_t)eg * NV * sizeof(T);
+            auto k = k_gs3<T, NV, 1, false>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, eg, gbar, err);
         }
         return cudaGetLastError();
     }
