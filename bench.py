@@ -54,7 +54,18 @@ def plain_spec():
     }
 
 
-def mixed_spec(blocks=128, inner_rel=1e-4):
+def gpu_sms():
+    try:
+        import torch
+        return torch.cuda.get_device_properties(0).multi_processor_count
+    except Exception:
+        return 148
+
+
+def mixed_spec(blocks=None, inner_rel=1e-4):
+    """Precision form.  Hybrid SGS on two blocks per SM on every level (two
+    resident CTAs per SM interleave their latency-bound block sweeps)."""
+    blocks = blocks or 2 * gpu_sms()
     s = plain_spec()
     s["meta_solver"] = {"method": "IterativeRefinement", "max_iters": 20, "abs_tolerance": 0.0,
                         "rel_tolerance": 1e-8, "subsolver_reduced_precision": True,

@@ -163,7 +163,7 @@ __device__ __forceinline__ int rspan(const Desc &d) { return ((d.r1 + 3) & ~3) -
 // MODE 0 = GRID, 1 = BLOCKS.  XS: x tile of the block in shared memory.
 // desc: GRID -> desc[l*gridDim.x + b]; BLOCKS -> desc[blev[b] + (l - l0)].
 template <class T, int NV, int MODE, bool XS>
-__global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ desc,
+__global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const int4 *__restrict__ desc,
                                              const int *__restrict__ blev,
                                              const int *__restrict__ lrp,
                                              const int *__restrict__ lci,
@@ -365,10 +365,10 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
                     }
                 }
             } else
-            // entries read from global memory: gathers from L2 are issued 16
-            // at a time so a row costs one or two round trips
-            for (int j = j0; j < j1; j += 16) {
-                constexpr int GB = 16;
+            // fallback for levels too large for the staging buffers: entries
+            // and x read from global memory, 4 gathers at a time
+            for (int j = j0; j < j1; j += 4) {
+                constexpr int GB = 4;
                 int c[GB];
                 T v[GB];
 #pragma unroll
@@ -443,11 +443,20 @@ __global__ void __launch_bounds__(256) k_gs3(int nlev, const int4 *__restrict__ 
     }
 }
 
+// entries of the per-level x gather buffer: the largest level of any CTA
+// (emax, from the plan; <= 0 = unknown), capped by the staging buffer and by
+// 176 KB of shared memory
+template <class T> static int gather_entries(int nv, int emax) {
+    int eg = (int)std::min<long>(GsBuf<T>::E, (176l * 1024) / ((long)nv * (long)sizeof(T)));
+    if (emax > 0) eg = std::min(eg, (emax + 3) & ~3);
+    return std::max(eg, 4);
+}
+
 template <class T, int NV>
 static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp, const int *blev,
                          const int *lrp, const int *lci, const void *lva, const int *lrow,
                          const void *invd, const void *t, void *x, const void *relax, i64 brows,
-                         i64 n, unsigned *gbar, int *err, cudaStream_t s) {
+                         i64 n, unsigned *gbar, int *err, int emax, cudaStream_t s) {
     const T *va = (const T *)lva;
     const int4 *lev_row = (const int4 *)descp;
     const T *di = (const T *)invd;
@@ -462,7 +471,7 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp,
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
             k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, 0, gbar, err);
         } else {
-            const int eg = (int)std::min<long>(GsBuf<T>::E, (176l * 1024) / ((long)NV * (long)sizeof(T)));
+            const int eg = gather_entries<T>(NV, emax);
             const size_t sm = (size_t)eg * NV * sizeof(T);
             auto k = k_gs3<T, NV, 1, false>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -473,7 +482,7 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp,
     // the grid must match the per-(level, CTA) descriptors built on the host;
     // dynamic shared memory holds the per-level x gather buffer (eg entries)
     int nblk = ncta;
-    int eg = (int)std::min<long>(GsBuf<T>::E, (176l * 1024) / ((long)NV * (long)sizeof(T)));
+    int eg = gather_entries<T>(NV, emax);
     size_t sm = (size_t)eg * NV * sizeof(T);
     auto k = k_gs3<T, NV, 0, false>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -500,13 +509,13 @@ cudaError_t gs_sweep_lcsr(Prec p, int nv, int mode, int xs, int nlev, int ncta, 
                           const int *blev, const int *lrp, const int *lci, const void *lva,
                           const int *lrow, const void *invd, const void *t, void *x,
                           const void *relax, i64 brows, i64 n, unsigned *gbar, int *err,
-                          cudaStream_t s) {
+                          int emax, cudaStream_t s) {
     if (p == Prec::F64) {
-#define F(NV) gs3_t<double, NV>(mode, xs, nlev, ncta, lev_row, blev, lrp, lci, lva, lrow, invd, t, x, relax, brows, n, gbar, err, s)
+#define F(NV) gs3_t<double, NV>(mode, xs, nlev, ncta, lev_row, blev, lrp, lci, lva, lrow, invd, t, x, relax, brows, n, gbar, err, emax, s)
         NV_SWITCH(nv, F)
 #undef F
     } else {
-#define F(NV) gs3_t<float, NV>(mode, xs, nlev, ncta, lev_row, blev, lrp, lci, lva, lrow, invd, t, x, relax, brows, n, gbar, err, s)
+#define F(NV) gs3_t<float, NV>(mode, xs, nlev, ncta, lev_row, blev, lrp, lci, lva, lrow, invd, t, x, relax, brows, n, gbar, err, emax, s)
         NV_SWITCH(nv, F)
 #undef F
     }

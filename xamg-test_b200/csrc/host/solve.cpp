@@ -286,6 +286,8 @@ void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
         Lcsr &L = lc[d];
         L.nlev = ngroups;
         L.ncta = mode == GsMode::GRID ? G : nblocks;
+        L.emax = 0;
+        for (size_t q = 0; q + 3 < desc.size(); q += 4) L.emax = std::max(L.emax, desc[q + 3] - desc[q + 2]);
         upload_ints(L.lrp, lrp);
         upload_ints(L.lci, lci);
         upload_ints(L.lrow, order);
@@ -322,7 +324,7 @@ void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val
         int xs = md == 1 && (i64)brows * nv * (i64)prec_size(p) <= xk::gs_lcsr_max_xs_bytes();
         XCUDA(xk::gs_sweep_lcsr(p, nv, md, xs, L.nlev, L.ncta, L.desc.as<int>(), L.blev.as<int>(),
                                 L.lrp.as<int>(), L.lci.as<int>(), L.lva.p, L.lrow.as<int>(),
-                                L.linvd.p, t, x, relax, brows, n, bar, err, s));
+                                L.linvd.p, t, x, relax, brows, n, bar, err, L.emax, s));
         return;
     }
     if (mode == GsMode::BLOCKS) {

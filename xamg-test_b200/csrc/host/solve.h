@@ -75,6 +75,7 @@ struct GsPlan {
         DBuf lrp, lci, lva, lrow, linvd, desc, blev;
         int nlev = 0;  // GRID: levels; BLOCKS: unused (per-block counts in blev)
         int ncta = 0;  // CTAs of the launch the descriptors were built for
+        int emax = 0;  // most entries of one CTA in one level
     } lc[2];
     bool has_lcsr = false;
     Prec lprec = Prec::F64;

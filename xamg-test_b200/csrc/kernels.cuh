@@ -67,12 +67,13 @@ void gs_blocks(Prec p, int nv, int nblocks, const int *blevf, const int *lptrf, 
 // the block's x tile in shared memory (mode 1, brows*nv*sizeof(T) <=
 // gs_lcsr_max_xs_bytes()).  Mode 0 uses the first 256 bytes of gbar
 // (8-byte aligned) for the grid barrier and zeroes them before the launch;
-// err must lie outside them.
+// err must lie outside them.  emax: the most entries any CTA processes in one
+// level (sizes the shared-memory gather buffer; <= 0 = unknown).
 cudaError_t gs_sweep_lcsr(Prec p, int nv, int mode, int xs, int nlev, int ncta, const int *lev_row,
                           const int *blev, const int *lrp, const int *lci, const void *lva,
                           const int *lrow, const void *invd, const void *t, void *x,
                           const void *relax, i64 brows, i64 n, unsigned *gbar, int *err,
-                          cudaStream_t s);
+                          int emax, cudaStream_t s);
 int gs_lcsr_max_xs_bytes();
 
 // Hybrid Gauss-Seidel right-hand side: t = 1*b + (-1)*(sum over the entries
