@@ -266,7 +266,7 @@ def batch_form(rank, world, warmup, steps):
     w = [A.nnz * nv for A, nv, _ in mem]
     mine = families.shard(w, world)[rank]
     t0 = time.time()
-    batch = xamg.Batch([(mem[i][0], mem[i][1]) for i in mine], xamg.Params(families.batch_spec(block_rows=1024)))
+    batch = xamg.Batch([(mem[i][0], mem[i][1]) for i in mine], xamg.Params(families.batch_spec(blocks=gpu_sms())))
     setup_s = time.time() - t0
 
     def load():
@@ -310,7 +310,7 @@ LEARNED_WEIGHTS = os.path.join(ROOT, "xamg-test_b200", "weights", "learned_64.np
 
 def learned_form(nsys=16):
     """Learned form: held-out 64^3 bump-coefficient systems (nv = 8) solved
-    from a zero guess and from the trained network's guess (4 symmetric
+    from a zero guess and from the trained network's guess (2 symmetric
     Gauss-Seidel sweeps on it first); time to 1e-8 relative to ||b|| with the
     inference and the sweeps included."""
     if not os.path.exists(LEARNED_WEIGHTS):

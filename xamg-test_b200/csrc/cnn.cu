@@ -487,67 +487,117 @@ __global__ void k_bias_grad(const bf16 *__restrict__ g, int gcs, int gc0, int c,
     atomicAdd(db + k, s);
 }
 
-// 2x2x2 average pooling of volume g (even sides) and its backward (dIn (+)= dOut/8)
+// Elementwise volume kernels work on groups of 8 channels (16 bytes), which
+// every channel count and offset here allows (multiples of 16).
+struct Oct {
+    float v[8];
+};
+__device__ __forceinline__ Oct ld8(const bf16 *p) {
+    const uint4 u = *reinterpret_cast<const uint4 *>(p);
+    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
+    Oct o;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 f = __bfloat1622float2(h[k]);
+        o.v[2 * k] = f.x;
+        o.v[2 * k + 1] = f.y;
+    }
+    return o;
+}
+__device__ __forceinline__ void st8(bf16 *p, const Oct &o) {
+    uint4 u;
+    __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&u);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) h[k] = __floats2bfloat162_rn(o.v[2 * k], o.v[2 * k + 1]);
+    *reinterpret_cast<uint4 *>(p) = u;
+}
+
+// 2x2x2 average pooling of volume g (even sides): one thread per coarse voxel
+// and 8 channels
 __global__ void k_pool2(const bf16 *__restrict__ in, int ics, int ic0, bf16 *out, int ocs, int oc0,
                         int c, Vol g) {
-    const int D = g.d / 2, H = g.h / 2, W = g.w / 2;
-    const i64 total = (i64)g.nb * D * H * W * c;
+    const int D = g.d / 2, H = g.h / 2, W = g.w / 2, c8 = c / 8;
+    const i64 total = (i64)g.nb * D * H * W * c8;
     for (i64 q = (i64)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (i64)gridDim.x * blockDim.x) {
-        const int k = (int)(q % c);
-        i64 r = q / c;
+        const int k = (int)(q % c8) * 8;
+        const i64 cv = q / c8;
+        i64 r = cv;
         const int x = (int)(r % W); r /= W;
         const int y = (int)(r % H); r /= H;
         const int z = (int)(r % D);
         const i64 b = r / D;
-        float s = 0.f;
+        Oct s;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) s.v[e] = 0.f;
 #pragma unroll
         for (int o = 0; o < 8; ++o) {
             const i64 v = ((b * g.d + 2 * z + (o >> 2)) * g.h + 2 * y + ((o >> 1) & 1)) * g.w + 2 * x + (o & 1);
-            s += __bfloat162float(in[v * ics + ic0 + k]);
+            const Oct t = ld8(in + v * ics + ic0 + k);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) s.v[e] += t.v[e];
         }
-        out[(q / c) * ocs + oc0 + k] = __float2bfloat16(s * 0.125f);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) s.v[e] *= 0.125f;
+        st8(out + cv * ocs + oc0 + k, s);
     }
 }
 
 // nearest upsampling of a (d/2, h/2, w/2) volume to g; mode 1 adds the
-// pooled-gradient share (x 1/8) for the pooling backward, mode 0 copies
+// pooled-gradient share (x 1/8) for the pooling backward, mode 0 copies.
+// One thread per coarse voxel and 8 channels writes its 8 fine voxels.
 __global__ void k_up2(const bf16 *__restrict__ in, int ics, int ic0, bf16 *out, int ocs, int oc0,
                       int c, Vol g, int mode) {
-    const i64 total = g.count() * c;
+    const int D = g.d / 2, H = g.h / 2, W = g.w / 2, c8 = c / 8;
+    const i64 total = (i64)g.nb * D * H * W * c8;
     for (i64 q = (i64)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (i64)gridDim.x * blockDim.x) {
-        const int k = (int)(q % c);
-        i64 r = q / c;
-        const int x = (int)(r % g.w); r /= g.w;
-        const int y = (int)(r % g.h); r /= g.h;
-        const int z = (int)(r % g.d);
-        const i64 b = r / g.d;
-        const i64 src = ((b * (g.d / 2) + z / 2) * (g.h / 2) + y / 2) * (g.w / 2) + x / 2;
-        float v = __bfloat162float(in[src * ics + ic0 + k]);
-        bf16 *po = out + (q / c) * ocs + oc0 + k;
-        if (mode == 1) v = __bfloat162float(*po) + v * 0.125f;
-        *po = __float2bfloat16(v);
+        const int k = (int)(q % c8) * 8;
+        const i64 cv = q / c8;
+        i64 r = cv;
+        const int x = (int)(r % W); r /= W;
+        const int y = (int)(r % H); r /= H;
+        const int z = (int)(r % D);
+        const i64 b = r / D;
+        const Oct src = ld8(in + cv * ics + ic0 + k);
+#pragma unroll
+        for (int o = 0; o < 8; ++o) {
+            const i64 v = ((b * g.d + 2 * z + (o >> 2)) * g.h + 2 * y + ((o >> 1) & 1)) * g.w + 2 * x + (o & 1);
+            bf16 *po = out + v * ocs + oc0 + k;
+            if (mode == 1) {
+                Oct t = ld8(po);
+#pragma unroll
+                for (int e = 0; e < 8; ++e) t.v[e] += src.v[e] * 0.125f;
+                st8(po, t);
+            } else {
+                st8(po, src);
+            }
+        }
     }
 }
 
 // backward of nearest upsampling: dIn[coarse] = sum of the 8 fine gradients
 __global__ void k_up2_bwd(const bf16 *__restrict__ gfine, int gcs, int gc0, bf16 *gin, int ics,
                           int ic0, int c, Vol g) {
-    const int D = g.d / 2, H = g.h / 2, W = g.w / 2;
-    const i64 total = (i64)g.nb * D * H * W * c;
+    const int D = g.d / 2, H = g.h / 2, W = g.w / 2, c8 = c / 8;
+    const i64 total = (i64)g.nb * D * H * W * c8;
     for (i64 q = (i64)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (i64)gridDim.x * blockDim.x) {
-        const int k = (int)(q % c);
-        i64 r = q / c;
+        const int k = (int)(q % c8) * 8;
+        const i64 cv = q / c8;
+        i64 r = cv;
         const int x = (int)(r % W); r /= W;
         const int y = (int)(r % H); r /= H;
         const int z = (int)(r % D);
         const i64 b = r / D;
-        float s = 0.f;
+        Oct s;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) s.v[e] = 0.f;
 #pragma unroll
         for (int o = 0; o < 8; ++o) {
             const i64 v = ((b * g.d + 2 * z + (o >> 2)) * g.h + 2 * y + ((o >> 1) & 1)) * g.w + 2 * x + (o & 1);
-            s += __bfloat162float(gfine[v * gcs + gc0 + k]);
+            const Oct t = ld8(gfine + v * gcs + gc0 + k);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) s.v[e] += t.v[e];
         }
-        gin[(q / c) * ics + ic0 + k] = __float2bfloat16(s);
+        st8(gin + cv * ics + ic0 + k, s);
     }
 }
 
@@ -586,9 +636,11 @@ __global__ void k_adam(float *w, const float *__restrict__ gw, float *m, float *
 // network input: channel 0 = a[p], channel 1 = b[p], channels 2..15 = 0
 __global__ void k_pack2(const float *__restrict__ a, const float *__restrict__ b, bf16 *out, i64 nvox) {
     for (i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x; p < nvox; p += (i64)gridDim.x * blockDim.x) {
-        out[p * 16] = __float2bfloat16(a[p]);
-        out[p * 16 + 1] = __float2bfloat16(b[p]);
-        for (int k = 2; k < 16; ++k) out[p * 16 + k] = __float2bfloat16(0.f);
+        uint4 u0 = make_uint4(0u, 0u, 0u, 0u);
+        *reinterpret_cast<__nv_bfloat162 *>(&u0.x) = __floats2bfloat162_rn(a[p], b[p]);
+        uint4 *po = reinterpret_cast<uint4 *>(out + p * 16);
+        po[0] = u0;
+        po[1] = make_uint4(0u, 0u, 0u, 0u);
     }
 }
 
@@ -718,9 +770,9 @@ int xcnn_bias_grad(const void *g, int gcs, int gc0, int c, int64_t nvox, float *
 
 int xcnn_pool2(const void *in, int ics, int ic0, void *out, int ocs, int oc0, int c, int nb, int d, int h,
                int w, void *stream) {
-    if (d % 2 || h % 2 || w % 2) return 2;
+    if (d % 2 || h % 2 || w % 2 || c % 8 || ic0 % 8 || ics % 8 || oc0 % 8 || ocs % 8) return 2;
     Vol g{nb, d, h, w};
-    k_pool2<<<grid_for(g.count() / 8 * c), 256, 0, (cudaStream_t)stream>>>((const bf16 *)in, ics, ic0,
+    k_pool2<<<grid_for(g.count() / 8 * (c / 8)), 256, 0, (cudaStream_t)stream>>>((const bf16 *)in, ics, ic0,
                                                                               (bf16 *)out, ocs, oc0, c, g);
     return last_err();
 }
@@ -728,18 +780,18 @@ int xcnn_pool2(const void *in, int ics, int ic0, void *out, int ocs, int oc0, in
 // fine volume (nb, d, h, w): mode 0 out = up(in); mode 1 out += up(in) / 8
 int xcnn_up2(const void *in, int ics, int ic0, void *out, int ocs, int oc0, int c, int nb, int d, int h,
              int w, int mode, void *stream) {
-    if (d % 2 || h % 2 || w % 2) return 2;
+    if (d % 2 || h % 2 || w % 2 || c % 8 || ic0 % 8 || ics % 8 || oc0 % 8 || ocs % 8) return 2;
     Vol g{nb, d, h, w};
-    k_up2<<<grid_for(g.count() * c), 256, 0, (cudaStream_t)stream>>>((const bf16 *)in, ics, ic0, (bf16 *)out,
-                                                                        ocs, oc0, c, g, mode);
+    k_up2<<<grid_for(g.count() / 8 * (c / 8)), 256, 0, (cudaStream_t)stream>>>((const bf16 *)in, ics, ic0,
+                                                                                 (bf16 *)out, ocs, oc0, c, g, mode);
     return last_err();
 }
 
 int xcnn_up2_bwd(const void *gfine, int gcs, int gc0, void *gin, int ics, int ic0, int c, int nb, int d,
                  int h, int w, void *stream) {
-    if (d % 2 || h % 2 || w % 2) return 2;
+    if (d % 2 || h % 2 || w % 2 || c % 8 || gc0 % 8 || gcs % 8 || ic0 % 8 || ics % 8) return 2;
     Vol g{nb, d, h, w};
-    k_up2_bwd<<<grid_for(g.count() / 8 * c), 256, 0, (cudaStream_t)stream>>>(
+    k_up2_bwd<<<grid_for(g.count() / 8 * (c / 8)), 256, 0, (cudaStream_t)stream>>>(
         (const bf16 *)gfine, gcs, gc0, (bf16 *)gin, ics, ic0, c, g);
     return last_err();
 }

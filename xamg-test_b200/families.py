@@ -48,13 +48,15 @@ def shard(weights, world):
     return [sorted(o) for o in out]
 
 
-def batch_spec(rel_tol=1e-8, max_iters=200, block_rows=256):
-    """PBiCGStab (FP64) + AMG (FP32 inside the batch) with hybrid SGS."""
+def batch_spec(rel_tol=1e-8, max_iters=200, block_rows=256, blocks=0):
+    """PBiCGStab (FP64) + AMG (FP32 inside the batch) with hybrid SGS on
+    blocks of block_rows rows, or on `blocks` blocks per level when > 0."""
+    hyb = {"hybrid_blocks": blocks} if blocks > 0 else {"hybrid_block_rows": block_rows}
     return {
         "solver": {"method": "PBiCGStab", "max_iters": max_iters, "abs_tolerance": 0.0, "rel_tolerance": rel_tol},
         "preconditioner": {"method": "MultiGrid", "mg_coarsening_type": 10, "mg_interpolation_type": 6,
                            "mg_strength_threshold": 0.25, "mg_max_levels": 6, "mg_agg_num_levels": 0},
-        "pre_smoother": {"method": "HSGS", "max_iters": 1, "hybrid_block_rows": block_rows},
-        "post_smoother": {"method": "HSGS", "max_iters": 1, "hybrid_block_rows": block_rows},
+        "pre_smoother": dict({"method": "HSGS", "max_iters": 1}, **hyb),
+        "post_smoother": dict({"method": "HSGS", "max_iters": 1}, **hyb),
         "coarse_grid_solver": {"method": "Direct"},
     }

@@ -371,7 +371,7 @@ def make_system(seed, n):
     return A, (np.log(k) / 4.0).astype(np.float32), rng
 
 
-def solver_spec(rel_tol=1e-8, base="rhs", blocks=256, mixed=False):
+def solver_spec(rel_tol=1e-8, base="rhs", blocks=296, mixed=False):
     """AMG-PBiCGStab with the relative tolerance measured against ||b|| (so
     that a good x0 pays off) and hybrid SGS on `blocks` blocks per level.
     mixed = True wraps an FP32 solver in FP64 iterative refinement."""
@@ -393,7 +393,7 @@ def solver_spec(rel_tol=1e-8, base="rhs", blocks=256, mixed=False):
     return sp
 
 
-def smoother_spec(sweeps=2, blocks=256):
+def smoother_spec(sweeps=2, blocks=296):
     """Symmetric Gauss-Seidel sweeps applied to the network's guess before the
     solve: they remove the guess's high-frequency error, which otherwise
     dominates its residual."""
@@ -471,7 +471,7 @@ def train(net, data, epochs, batch=8, lr=1e-3, seed=0, log=None):
     return hist, ev0.elapsed_time(ev1)
 
 
-def evaluate(net, seeds, n, nv, log=None, sweeps=4, mixed=False):
+def evaluate(net, seeds, n, nv, log=None, sweeps=2, mixed=False):
     """Per held-out system: Krylov iterations and device time to 1e-8
     (relative to ||b||) from a zero guess and from the network's guess
     smoothed by `sweeps` symmetric Gauss-Seidel sweeps (inference and
