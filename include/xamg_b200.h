@@ -50,6 +50,10 @@ int XAMG_b200_solver_export_level(int *rpA, int *ciA, double *vA, int *rpP, int 
 int XAMG_b200_solver_export_gs_levels(int *lf, int *lb, int level, XAMG_solver_id sid);
 /* Dense inverse of the coarsest operator (row-major n x n). */
 int XAMG_b200_solver_export_coarse_inverse(double *out, XAMG_solver_id sid);
+/* Spectrum bounds {min, max} of D^-1/2 A D^-1/2 used by a level's Chebyshev
+ * smoother (the reference takes them from hypre, hypre_base.inl:370-375; here
+ * they come from a 10-step CG/Lanczos estimate); {0, 0} without one. */
+int XAMG_b200_solver_level_eig(double *out, int level, XAMG_solver_id sid);
 /* Human-readable description of the solver tree. */
 int XAMG_b200_solver_info(char *buf, int cap, XAMG_solver_id sid);
 
@@ -176,7 +180,8 @@ int xamg_dot_noalloc(int prec, int nv, int64_t n, int nd, const void *const *a,
                      const void *const *b, double *out, void *stream);
 
 /* Block-vector BLAS-1 (blas.inl, blas_ext.inl) with FP64 per-column scalars:
- * op 0 z=a*x+b*y, 1 z=a*x+b*y+c*z, 2 z=a*x, 3 z=x, 4 z=a, 5 z=z*x. */
+ * op 0 z=a*x+b*y, 1 z=a*x+b*y+c*z, 2 z=a*x, 3 z=x, 4 z=a, 5 z=z*x,
+ * 6 z[i,k] = z[i,k]*x[i] (x: n values, one per row). */
 int xamg_blas(int prec, int nv, int64_t n, int op, const double *a, const void *x,
               const double *b, const void *y, const double *c, void *z, void *stream);
 

@@ -269,7 +269,7 @@ struct Csr {
     std::vector<float> v32;
 };
 
-enum { SM_JACOBI = 0, SM_HSGS = 1 };
+enum { SM_JACOBI = 0, SM_HSGS = 1, SM_CHEB = 2 };
 
 struct Level {
     Csr A, P, R;
@@ -283,6 +283,9 @@ struct MG {
     int fp32 = 0;  // whole V-cycle in FP32
     int pre_m = SM_HSGS, post_m = SM_HSGS, pre_it = 1, post_it = 1;
     double pre_relax = 0.99, post_relax = 0.99;
+    int cheb_order = 2;        // Chebyshev smoother (chebyshev.inl)
+    double cheb_fraction = 0.3;
+    std::vector<double> min_eig, max_eig;  // per level
     int nc = 0;
     std::vector<double> Ainv64;
     std::vector<float> Ainv32;
@@ -301,10 +304,67 @@ template <> const float *ainv<float>(const MG &m) { return m.Ainv32.data(); }
 // Smoother call (HSGS::solve hsgs.inl:53-91 / Jacobi::solve jacobi.inl:91-100);
 // both are used with nocheck, so exactly `iters` sweeps run.  The convergence
 // mask of the preconditioner is all ones (PBiCGStab calls precond->solve(x,b)).
+// Chebyshev polynomial coefficients, chebyshev.inl:51-128
+static std::vector<double> cheby_coeffs(double min_eig, double max_eig, int order, double fraction) {
+    const double upper = max_eig * 1.1;
+    const double lower = (upper - min_eig) * fraction + min_eig;
+    const double th = (upper + lower) / 2., de = (upper - lower) / 2.;
+    double den;
+    switch (order) {
+    case 1: return {1. / th};
+    case 2: den = de * de - 2 * th * th; return {-4 * th / den, 2 / den};
+    case 3:
+        den = 3 * (de * de) * th - 4 * (th * th * th);
+        return {(3 * de * de - 12 * th * th) / den, 12 * th / den, -4 / den};
+    default:
+        den = std::pow(de, 4) - 8 * de * de * th * th + 8 * std::pow(th, 4);
+        return {(32 * std::pow(th, 3) - 16 * de * de * th) / den, (8 * de * de - 48 * th * th) / den,
+                32 * th / den, -8 / den};
+    }
+}
+
+// Chebyshev smoother, chebyshev.inl:142-183.  Vector updates follow the
+// library's BLAS contract: FP64 products of the stored values, rounded once
+// to T; coefficients rounded to T first (the reference stores them as F).
+template <class T>
+void chebyshev(const MG &mg, int l, const T *b, T *x, int nv) {
+    const Level &L = mg.lv[l];
+    const i64 n = L.A.n;
+    std::vector<T> isd(n, T(0));
+    for (i64 i = 0; i < n; ++i)
+        for (int j = L.A.rp[i]; j < L.A.rp[i + 1]; ++j)
+            if (L.A.ci[j] == i) isd[i] = (T)std::sqrt(1.0 / (double)vals<T>(L.A)[j]);
+    std::vector<double> cd = cheby_coeffs(mg.min_eig[l], mg.max_eig[l], mg.cheb_order, mg.cheb_fraction);
+    std::vector<double> c(cd.size());
+    for (size_t i = 0; i < cd.size(); ++i) c[i] = (double)(T)cd[i];
+    const int p = mg.cheb_order;
+    const size_t sz = (size_t)n * nv;
+    std::vector<T> r(sz), t1(sz), t2(sz);
+    spmv<T>(n, L.A.rp.data(), L.A.ci.data(), vals<T>(L.A), x, r.data(), nv, 0);
+    for (size_t q = 0; q < sz; ++q) r[q] = T(1) * b[q] + T(-1) * r[q];
+    auto rowscal = [&](std::vector<T> &z) {
+        for (size_t q = 0; q < sz; ++q) z[q] = (T)((double)z[q] * (double)isd[q / nv]);
+    };
+    rowscal(r);
+    for (size_t q = 0; q < sz; ++q) t1[q] = (T)(c[p - 1] * (double)r[q]);
+    for (int i = p - 2; i >= 0; --i) {
+        rowscal(t1);
+        spmv<T>(n, L.A.rp.data(), L.A.ci.data(), vals<T>(L.A), t1.data(), t2.data(), nv, 0);
+        rowscal(t2);
+        for (size_t q = 0; q < sz; ++q) t1[q] = (T)(c[i] * (double)r[q] + 1.0 * (double)t2[q]);
+    }
+    rowscal(t1);
+    for (size_t q = 0; q < sz; ++q) x[q] = (T)(1.0 * (double)t1[q] + 1.0 * (double)x[q]);
+}
+
 template <class T>
 void smooth(const MG &mg, int l, int method, int iters, double relaxd, const T *b, T *x, int nv) {
     const Level &L = mg.lv[l];
     std::vector<T> relax(nv, (T)relaxd);
+    if (method == SM_CHEB) {
+        chebyshev<T>(mg, l, b, x, nv);
+        return;
+    }
     if (method == SM_HSGS) {
         for (int it = 0; it < iters; ++it)
             hsgs<T>(L.A.n, L.A.rp.data(), L.A.ci.data(), vals<T>(L.A), invd<T>(L), b, x, relax.data(),
@@ -622,6 +682,13 @@ void orc_mg_set_P(void *h, int l, i64 n, i64 ncols, const int *rp, const int *ci
 void orc_mg_set_blocks(void *h, int l, int nb, const i64 *bp) {
     MG *m = (MG *)h;
     m->lv[l].bp.assign(bp, bp + nb + 1);
+}
+void orc_mg_set_cheb(void *h, int order, double fraction, const double *min_eig, const double *max_eig) {
+    MG *m = (MG *)h;
+    m->cheb_order = order;
+    m->cheb_fraction = fraction;
+    m->min_eig.assign(min_eig, min_eig + m->lv.size());
+    m->max_eig.assign(max_eig, max_eig + m->lv.size());
 }
 void orc_mg_set_smoothers(void *h, int pre_m, int pre_it, double pre_relax, int post_m,
                           int post_it, double post_relax) {

@@ -44,6 +44,7 @@ def lib():
             "orc_mg_set_P": (None, [P, C.c_int, i64, i64, P, P, P]),
             "orc_mg_set_blocks": (None, [P, C.c_int, C.c_int, P]),
             "orc_mg_set_smoothers": (None, [P, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_double]),
+            "orc_mg_set_cheb": (None, [P, C.c_int, C.c_double, P, P]),
             "orc_mg_finalize": (None, [P, C.c_int]),
             "orc_mg_get_coarse_inverse": (None, [P, P]),
             "orc_mg_get_R": (None, [P, C.c_int, P, P, P]),
@@ -142,13 +143,16 @@ def transpose(rp, ci, v, ncols):
     return rrp, rci, rv
 
 
-SM_JACOBI, SM_HSGS = 0, 1
+SM_JACOBI, SM_HSGS, SM_CHEB = 0, 1, 2
 
 
 class MG:
     """Oracle multigrid hierarchy (levels exported from the product's setup)."""
 
-    def __init__(self, levels, fp32=False, pre=(SM_HSGS, 1, 0.99), post=(SM_HSGS, 1, 0.99), block_rows=None):
+    def __init__(self, levels, fp32=False, pre=(SM_HSGS, 1, 0.99), post=(SM_HSGS, 1, 0.99), block_rows=None,
+                 cheb=None):
+        """cheb = (order, spectrum_fraction, [(min_eig, max_eig) per level])
+        for the Chebyshev smoother (method SM_CHEB)."""
         self.h = lib().orc_mg_create(len(levels))
         self.keep = []
         for l, lv in enumerate(levels):
@@ -165,6 +169,12 @@ class MG:
                 lib().orc_mg_set_blocks(self.h, l, len(bp) - 1, p(bp))
             self.keep.append(lv)
         lib().orc_mg_set_smoothers(self.h, pre[0], pre[1], pre[2], post[0], post[1], post[2])
+        if cheb is not None:
+            order, frac, eig = cheb
+            mn = np.array([e[0] for e in eig], np.float64)
+            mx = np.array([e[1] for e in eig], np.float64)
+            self.keep += [mn, mx]
+            lib().orc_mg_set_cheb(self.h, int(order), float(frac), p(mn), p(mx))
         lib().orc_mg_finalize(self.h, int(fp32))
         self.nc = len(levels[-1]["A"][0]) - 1
 

@@ -82,6 +82,30 @@ def test_pbicgstab_amg_parity(gpu, smoother, block_rows):
     assert np.array_equal(s.coarse_inverse(), mg.coarse_inverse())
 
 
+@pytest.mark.parametrize("order,nv", [(2, 4), (3, 1), (4, 2)])
+def test_pbicgstab_chebyshev_parity(gpu, order, nv):
+    """Chebyshev smoothing (chebyshev.inl) in the V-cycle: the oracle is given
+    the library's spectrum estimates and must reproduce the iterations and
+    the residual history."""
+    csr = xamg.CsrMatrix.aniso27(20)
+    rp, ci, v = csr.arrays()
+    rng = np.random.default_rng(order)
+    B = rng.uniform(-1, 1, (csr.nrows, nv))
+    spec = util.amg_params(max_levels=6)
+    for role in ("pre_smoother", "post_smoother"):
+        spec[role] = {"method": "Chebyshev", "polynomial_order": order, "spectrum_fraction": 0.3}
+    s, X, keep = solve_api(csr, spec, B)
+    levels = [s.level(l) for l in range(s.num_levels())]
+    eig = [s.level_eig(l) for l in range(s.num_levels())]
+    for mn, mx in eig[:-1]:
+        assert 0 < mn < mx < 4.0, eig
+    mg = orc.MG(levels, pre=(orc.SM_CHEB, 1, 0.0), post=(orc.SM_CHEB, 1, 0.0), cheb=(order, 0.3, eig))
+    xo, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg, 200, 0.0, 1e-8)
+    assert s.iters()[0] == it and it > 0 and all(s.converged())
+    assert_same_history(s.history(), hist)
+    np.testing.assert_allclose(X, xo, rtol=1e-12, atol=1e-14 * np.abs(xo).max())
+
+
 def test_recorded_2d_problem_through_api(gpu):
     rec = json.load(open(os.path.join(GOLD, "recorded.json")))
     rp, ci, v, b, u = util.gen2d(100)

@@ -581,6 +581,13 @@ int XAMG_b200_solver_export_coarse_inverse(double *out, XAMG_solver_id sid) {
         std::memcpy(out, ci.data(), sizeof(double) * ci.size());
     });
 }
+int XAMG_b200_solver_level_eig(double *out, int level, XAMG_solver_id sid) {
+    return guard([&] {
+        MultiGrid *mg = find_multigrid(get(slist, sid, "solver")->s.get());
+        XCHECK(mg, "solver has no multigrid");
+        mg_level_eig(mg, level, out, out + 1);
+    });
+}
 int XAMG_b200_solver_info(char *buf, int cap, XAMG_solver_id sid) {
     return guard([&] {
         std::string s = get(slist, sid, "solver")->s->info();
@@ -805,7 +812,7 @@ int xamg_dot(int prec, int nv, int64_t n, int nd, const void *const *a, const vo
 int xamg_blas(int prec, int nv, int64_t n, int op, const double *a, const void *x, const double *b,
               const void *y, const double *c, void *z, void *stream) {
     return guard([&] {
-        XCHECK(op >= 0 && op <= 5, "op must be 0..5");
+        XCHECK(op >= 0 && op <= 6, "op must be 0..6");
         xk::blas((Prec)prec, nv, n, (xk::Op)op, a, x, b, y, c, z, strm(stream));
         XCUDA(cudaGetLastError());
     });

@@ -554,6 +554,162 @@ struct HSGS : Solver {
     }
 };
 
+// Spectrum bounds of D^-1/2 A D^-1/2 for the Chebyshev smoother.  The
+// reference takes them from hypre's BoomerAMG setup (hypre_base.inl:370-375,
+// CG-based estimates); hypre is not available here, so the same kind of
+// estimate is made: `iters` CG steps on the scaled operator from a fixed
+// pseudo-random start give the Lanczos tridiagonal matrix
+// (T_kk = 1/alpha_k + beta_{k-1}/alpha_{k-1}, T_k,k+1 = sqrt(beta_k)/alpha_k)
+// whose extreme eigenvalues (cyclic Jacobi rotations) are the bounds.
+void eig_estimate(const HostCsr &A, int iters, double &mn, double &mx) {
+    const i64 n = A.n;
+    std::vector<double> d(n, 0.0), r(n), p(n), w(n);
+    for (i64 i = 0; i < n; ++i)
+        for (int j = A.rp[i]; j < A.rp[i + 1]; ++j)
+            if (A.ci[j] == i) d[i] = 1.0 / std::sqrt(std::fabs(A.v[j]));
+    unsigned long long st = 0x9E3779B97F4A7C15ull;
+    for (i64 i = 0; i < n; ++i) {
+        st = st * 6364136223846793005ull + 1442695040888963407ull;
+        r[i] = (double)(st >> 11) / 9007199254740992.0 - 0.5;
+    }
+    auto dot = [&](const std::vector<double> &a, const std::vector<double> &b) {
+        double s = 0.0;
+        for (i64 i = 0; i < n; ++i) s += a[i] * b[i];
+        return s;
+    };
+    p = r;
+    double rr = dot(r, r);
+    std::vector<double> al, be;
+    const int k = (int)std::min<i64>(iters, n);
+    for (int it = 0; it < k && rr > 0; ++it) {
+        for (i64 i = 0; i < n; ++i) {
+            double s = 0.0;
+            for (int j = A.rp[i]; j < A.rp[i + 1]; ++j) s += A.v[j] * d[A.ci[j]] * p[A.ci[j]];
+            w[i] = d[i] * s;
+        }
+        const double pw = dot(p, w);
+        if (!(pw > 0)) break;
+        const double a = rr / pw;
+        for (i64 i = 0; i < n; ++i) r[i] -= a * w[i];
+        const double rr2 = dot(r, r);
+        al.push_back(a);
+        be.push_back(rr2 / rr);
+        rr = rr2;
+        for (i64 i = 0; i < n; ++i) p[i] = r[i] + be.back() * p[i];
+    }
+    const int m = (int)al.size();
+    if (m == 0) { mn = mx = 1.0; return; }
+    std::vector<double> T((size_t)m * m, 0.0);
+    for (int q = 0; q < m; ++q) {
+        T[(size_t)q * m + q] = 1.0 / al[q] + (q > 0 ? be[q - 1] / al[q - 1] : 0.0);
+        if (q + 1 < m) T[(size_t)q * m + q + 1] = T[(size_t)(q + 1) * m + q] = std::sqrt(be[q]) / al[q];
+    }
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        double off = 0.0;
+        for (int i = 0; i < m; ++i)
+            for (int j = i + 1; j < m; ++j) off += T[(size_t)i * m + j] * T[(size_t)i * m + j];
+        if (off < 1e-30) break;
+        for (int i = 0; i < m; ++i)
+            for (int j = i + 1; j < m; ++j) {
+                const double aij = T[(size_t)i * m + j];
+                if (std::fabs(aij) < 1e-300) continue;
+                const double th = (T[(size_t)j * m + j] - T[(size_t)i * m + i]) / (2.0 * aij);
+                const double t = (th >= 0 ? 1.0 : -1.0) / (std::fabs(th) + std::sqrt(th * th + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+                for (int q = 0; q < m; ++q) {
+                    const double tqi = T[(size_t)q * m + i], tqj = T[(size_t)q * m + j];
+                    T[(size_t)q * m + i] = c * tqi - s * tqj;
+                    T[(size_t)q * m + j] = s * tqi + c * tqj;
+                }
+                for (int q = 0; q < m; ++q) {
+                    const double tiq = T[(size_t)i * m + q], tjq = T[(size_t)j * m + q];
+                    T[(size_t)i * m + q] = c * tiq - s * tjq;
+                    T[(size_t)j * m + q] = s * tiq + c * tjq;
+                }
+            }
+    }
+    mn = mx = T[0];
+    for (int q = 1; q < m; ++q) {
+        mn = std::min(mn, T[(size_t)q * m + q]);
+        mx = std::max(mx, T[(size_t)q * m + q]);
+    }
+}
+
+// Chebyshev polynomial coefficients (chebyshev.inl:51-128), orders 1..4.
+std::vector<double> cheby_coeffs(double min_eig, double max_eig, int order, double fraction) {
+    const double upper = max_eig * 1.1;
+    const double lower = (upper - min_eig) * fraction + min_eig;
+    const double th = (upper + lower) / 2., de = (upper - lower) / 2.;
+    std::vector<double> c;
+    double den;
+    switch (order) {
+    case 1: c = {1. / th}; break;
+    case 2:
+        den = de * de - 2 * th * th;
+        c = {-4 * th / den, 2 / den};
+        break;
+    case 3:
+        den = 3 * (de * de) * th - 4 * (th * th * th);
+        c = {(3 * de * de - 12 * th * th) / den, 12 * th / den, -4 / den};
+        break;
+    case 4:
+        den = std::pow(de, 4) - 8 * de * de * th * th + 8 * std::pow(th, 4);
+        c = {(32 * std::pow(th, 3) - 16 * de * de * th) / den, (8 * de * de - 48 * th * th) / den,
+             32 * th / den, -8 / den};
+        break;
+    default: throw Error("polynomial_order must be 1..4", 2);
+    }
+    return c;
+}
+
+// Chebyshev smoother (chebyshev.inl:142-183): r = D^-1/2 (b - A x);
+// t1 = c_{p-1} r; for i = p-2..0: t1 = c_i r + D^-1/2 A D^-1/2 t1;
+// x += D^-1/2 t1.  Coefficients in the level's precision (the reference
+// stores them as F).
+struct Chebyshev : Solver {
+    const DCsr *A = nullptr;
+    const void *isd = nullptr;
+    DVec r, t1, t2;
+    DBuf coef, ones;  // coef: order x nv per-column copies
+    int order = 2;
+    void init(const DCsr *a, const void *isd_, i64 n, double min_eig, double max_eig) {
+        A = a;
+        isd = isd_;
+        parse_conv(prm, conv);
+        conv.init(nv);
+        order = (int)prm.get_int("polynomial_order");
+        std::vector<double> c = cheby_coeffs(min_eig, max_eig, order, prm.get_float("spectrum_fraction"));
+        std::vector<double> cv((size_t)order * nv);
+        for (int i = 0; i < order; ++i)
+            for (int k = 0; k < nv; ++k) cv[(size_t)i * nv + k] = prec == Prec::F32 ? (double)(float)c[i] : c[i];
+        coef.alloc(sizeof(double) * cv.size());
+        XCUDA(cudaMemcpy(coef.p, cv.data(), sizeof(double) * cv.size(), cudaMemcpyHostToDevice));
+        std::vector<double> o(nv, 1.0);
+        ones.alloc(sizeof(double) * nv);
+        XCUDA(cudaMemcpy(ones.p, o.data(), sizeof(double) * nv, cudaMemcpyHostToDevice));
+        r.alloc(n, nv, prec);
+        t1.alloc(n, nv, prec);
+        t2.alloc(n, nv, prec);
+    }
+    void solve(DVec &x, const DVec &b) override {
+        cudaStream_t s = ctx().stream;
+        const i64 n = x.n;
+        const double *C = coef.as<double>();
+        const double *one = ones.as<double>();
+        xk::spmv(prec, nv, n, A->rpp(), A->cip(), A->val(prec), x.p(), r.p(), 2, b.p(), s);
+        xk::blas(prec, nv, n, xk::Op::ROW_SCAL, nullptr, isd, nullptr, nullptr, nullptr, r.p(), s);
+        xk::blas(prec, nv, n, xk::Op::AX_Y, C + (size_t)(order - 1) * nv, r.p(), nullptr, nullptr, nullptr, t1.p(), s);
+        for (int i = order - 2; i >= 0; --i) {
+            xk::blas(prec, nv, n, xk::Op::ROW_SCAL, nullptr, isd, nullptr, nullptr, nullptr, t1.p(), s);
+            xk::spmv(prec, nv, n, A->rpp(), A->cip(), A->val(prec), t1.p(), t2.p(), 0, nullptr, s);
+            xk::blas(prec, nv, n, xk::Op::ROW_SCAL, nullptr, isd, nullptr, nullptr, nullptr, t2.p(), s);
+            xk::blas(prec, nv, n, xk::Op::AXPBY_Z, C + (size_t)i * nv, r.p(), one, t2.p(), nullptr, t1.p(), s);
+        }
+        xk::blas(prec, nv, n, xk::Op::ROW_SCAL, nullptr, isd, nullptr, nullptr, nullptr, t1.p(), s);
+        xk::blas(prec, nv, n, xk::Op::AXPBY_Z, one, t1.p(), one, x.p(), nullptr, x.p(), s);
+    }
+};
+
 struct Jacobi : Solver {
     LevelOp op;
     DVec tmp, r;
@@ -705,6 +861,30 @@ struct MultiGrid : Solver {
             h->role = rl; h->method = meth; h->prm = pl; h->nv = nv; h->prec = m.prec;
             h->init(op, hA.n);
             return h;
+        }
+        if (meth == "Chebyshev") {
+            // sqrt(1/a_ii) as csr_matrix.h:357-389 computes it (last diagonal
+            // entry wins; the FP32 copy from the FP32 value)
+            DBuf &isd = m.prec == Prec::F64 ? m.isd64 : m.isd32;
+            if (!isd.p) {
+                std::vector<double> d(hA.n, 0.0);
+                std::vector<float> f(hA.n, 0.f);
+                for (i64 i = 0; i < hA.n; ++i)
+                    for (int j = hA.rp[i]; j < hA.rp[i + 1]; ++j)
+                        if (hA.ci[j] == i) {
+                            d[i] = std::sqrt(1.0 / hA.v[j]);
+                            f[i] = (float)std::sqrt(1.0 / (double)(float)hA.v[j]);
+                        }
+                const size_t es = m.prec == Prec::F64 ? sizeof(double) : sizeof(float);
+                isd.alloc(es * std::max<i64>(hA.n, 1));
+                XCUDA(cudaMemcpy(isd.p, m.prec == Prec::F64 ? (const void *)d.data() : (const void *)f.data(),
+                                 es * hA.n, cudaMemcpyHostToDevice));
+                eig_estimate(hA, 10, m.min_eig, m.max_eig);
+            }
+            auto c = std::unique_ptr<Chebyshev>(new Chebyshev());
+            c->role = rl; c->method = meth; c->prm = pl; c->nv = nv; c->prec = m.prec;
+            c->init(&dA, isd.p, hA.n, m.min_eig, m.max_eig);
+            return c;
         }
         if (meth == "Jacobi") {
             auto j = std::unique_ptr<Jacobi>(new Jacobi());
@@ -1079,6 +1259,11 @@ const HostCsr &mg_level_A(MultiGrid *mg, int l) { return l == 0 ? mg->Afine->h :
 const HostCsr &mg_level_P(MultiGrid *mg, int l) { return mg->lv[l].hP; }
 const GsPlan &mg_level_gs(MultiGrid *mg, int l) { return mg->lv[l].gs_pre; }
 const std::vector<double> &mg_coarse_inverse(MultiGrid *mg) { return mg->coarse_inv; }
+void mg_level_eig(MultiGrid *mg, int l, double *mn, double *mx) {
+    XCHECK(l >= 0 && l < (int)mg->lv.size(), "level out of range");
+    *mn = mg->lv[l].min_eig;
+    *mx = mg->lv[l].max_eig;
+}
 
 // Gauss-Jordan without pivoting (inverse.inl:31-106, same operation order);
 // the independent row updates of each elimination step run in parallel.

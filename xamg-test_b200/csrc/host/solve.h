@@ -126,6 +126,8 @@ struct MGLevel {
     HostCsr hA, hP;         // host copies (setup output; exported for parity)
     DCsr A, P, R;
     DBuf invd64, invd32;
+    DBuf isd64, isd32;       // sqrt(1/a_ii) (Chebyshev smoother), on demand
+    double min_eig = 0.0, max_eig = 0.0;  // spectrum estimate of D^-1/2 A D^-1/2 (Chebyshev)
     GsPlan gs_pre, gs_post;  // share one plan when the block sizes agree
     Prec prec = Prec::F64;   // precision of this level's vectors/operator
     DVec tmp, tmp2, xH, bH;  // work vectors: tmp/tmp2 on this level, xH/bH on the next
@@ -172,6 +174,8 @@ const HostCsr &mg_level_A(MultiGrid *mg, int l);
 const HostCsr &mg_level_P(MultiGrid *mg, int l);
 const GsPlan &mg_level_gs(MultiGrid *mg, int l);
 const std::vector<double> &mg_coarse_inverse(MultiGrid *mg);
+// spectrum bounds used by a level's Chebyshev smoother (0, 0 when none)
+void mg_level_eig(MultiGrid *mg, int l, double *mn, double *mx);
 
 void dense_inverse(int n, const double *A, double *Ainv);
 void csr_transpose(const HostCsr &P, HostCsr &R);

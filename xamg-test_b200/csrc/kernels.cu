@@ -880,8 +880,10 @@ __global__ void __launch_bounds__(256) k_blas(i64 total, const double *__restric
         r = (double)x[q];
     } else if (OP == (int)Op::SET) {
         r = a[k];
-    } else {  // SCAL_XY
+    } else if (OP == (int)Op::SCAL_XY) {
         r = dmul((double)z[q], (double)x[q]);
+    } else {  // ROW_SCAL: x holds one value per row
+        r = dmul((double)z[q], (double)x[q / NV]);
     }
     z[q] = (T)r;
 }
@@ -900,6 +902,7 @@ static void blas_t(i64 n, Op op, const double *a, const T *x, const double *b, c
     case Op::COPY: k_blas<T, NV, 3><<<g, 256, 0, s>>>(tot, a, x, b, y, c, z); break;
     case Op::SET: k_blas<T, NV, 4><<<g, 256, 0, s>>>(tot, a, x, b, y, c, z); break;
     case Op::SCAL_XY: k_blas<T, NV, 5><<<g, 256, 0, s>>>(tot, a, x, b, y, c, z); break;
+    case Op::ROW_SCAL: k_blas<T, NV, 6><<<g, 256, 0, s>>>(tot, a, x, b, y, c, z); break;
     }
 }
 

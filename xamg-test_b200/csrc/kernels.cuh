@@ -105,6 +105,7 @@ enum class Op : int {
     COPY = 3,      // z = x
     SET = 4,       // z = a
     SCAL_XY = 5,   // z = z * x   (elementwise)
+    ROW_SCAL = 6,  // z[i,k] = z[i,k] * x[i]  (x: one value per row; blas::scal, blas.inl:182-189)
 };
 void blas(Prec p, int nv, i64 n, Op op, const double *a, const void *x, const double *b,
           const void *y, const double *c, void *z, cudaStream_t s);

@@ -97,6 +97,7 @@ def lib():
             "XAMG_b200_solver_export_gs_levels": (C.c_int, [P, P, C.c_int, sz]),
             "XAMG_b200_solver_export_coarse_inverse": (C.c_int, [P, sz]),
             "XAMG_b200_solver_info": (C.c_int, [C.c_char_p, C.c_int, sz]),
+            "XAMG_b200_solver_level_eig": (C.c_int, [P, C.c_int, sz]),
             "XAMG_b200_csr_matrix_generate": (C.c_int, [C.c_int, P, P, P, sz]),
             "XAMG_b200_csr_matrix_get_nnz": (i64, [sz]),
             "XAMG_b200_csr_matrix_export": (C.c_int, [P, P, P, sz]),
@@ -379,6 +380,11 @@ class Solver:
 
     def num_levels(self):
         return lib().XAMG_b200_solver_num_levels(self.h)
+
+    def level_eig(self, l):
+        out = np.zeros(2)
+        check(lib().XAMG_b200_solver_level_eig(_ptr(out), l, self.h))
+        return float(out[0]), float(out[1])
 
     def level(self, l):
         info = (C.c_int64 * 6)()
