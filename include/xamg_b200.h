@@ -158,8 +158,8 @@ int xamg_jacobi(int prec, int nv, int64_t n, const int *rp, const int *ci, const
                 const void *invdiag, const void *b, const void *xi, void *xo,
                 const void *relax, void *stream);
 
-/* Inner products (blas::dot, blas.inl:521-589) of nd pairs, FP64 results
- * out[d*nv + k]; part: xamg_dot_part_size(n, nd, nv) doubles of scratch. */
+/* Inner products (blas::dot, blas.inl:521-589) of nd pairs (1..4), FP64
+ * results out[d*nv + k]; part: xamg_dot_part_size(n, nd, nv) doubles of scratch. */
 int64_t xamg_dot_part_size(int64_t n, int nd, int nv);
 int xamg_dot(int prec, int nv, int64_t n, int nd, const void *const *a, const void *const *b,
              double *part, double *out, void *stream);

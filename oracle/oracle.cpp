@@ -536,6 +536,89 @@ int pbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
     return it;
 }
 
+// RBiCGStab, rbicgstab.inl:48-225 (the reference always has a preconditioner;
+// mg == nullptr applies the identity, z = copy of the right-hand side).
+// Step numbers are the reference's comments.
+template <class T>
+int rbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iters, Conv &cv,
+              Hist &hist) {
+    i64 n = A.n;
+    size_t sz = (size_t)n * nv;
+    const T *av = vals<T>(A);
+    std::vector<T> r0(sz), r(sz), z(sz), v_(sz), v(sz), s(sz), t_(sz), t(sz);
+    std::vector<double> rho(nv), delta(nv), alpha(nv), theta(nv), phi(nv), psi(nv), eta(nv),
+        omega(nv), beta(nv), res(nv), iconv(nv, 1.0);
+    auto precond = [&](std::vector<T> &out, const std::vector<T> &in) {
+        if (mg) mg_apply<T>(*mg, out.data(), in.data(), nv);
+        else out = in;
+    };
+    auto at = [](size_t q, int nv_) { return (int)(q % (size_t)nv_); };
+    cv.nv = nv;
+    cv.res0.assign(nv, 0);
+    cv.res.assign(nv, 0);
+    cv.status.assign(nv, 0);
+    // 1-2. r0 = b - A x, rho = (r0, r0)  (solver.h:183-190)
+    spmv<T>(n, A.rp.data(), A.ci.data(), av, x, r0.data(), nv, 0);
+    for (size_t q = 0; q < sz; ++q) r0[q] = T(1) * b[q] + T(-1) * r0[q];
+    dot_canonical<T, double>(n, nv, r0.data(), r0.data(), rho.data());
+    for (int k = 0; k < nv; ++k) cv.res0[k] = rho[k];
+    cv.update(rho.data());
+    hist.push(cv.res, nv);
+    if (cv.check()) return 0;
+    for (int k = 0; k < nv; ++k) if (cv.status[k]) iconv[k] = 0;
+    r = r0;
+    precond(z, r0);  // 3
+    v_ = z;          // 4
+    int it = 0;
+    for (bool last = false; !last;) {
+        it++;
+        if (it >= max_iters) last = true;
+        spmv<T>(n, A.rp.data(), A.ci.data(), av, v_.data(), v.data(), nv, 0);  // 6
+        dot_canonical<T, double>(n, nv, v.data(), r0.data(), delta.data());   // 7
+        precond(s, v);                                                        // 8
+        for (int k = 0; k < nv; ++k) alpha[k] = rho[k] / delta[k];            // 9
+        for (size_t q = 0; q < sz; ++q)                                       // 10
+            t_[q] = (T)(1.0 * (double)z[q] + (-alpha[at(q, nv)]) * (double)s[q]);
+        spmv<T>(n, A.rp.data(), A.ci.data(), av, t_.data(), t.data(), nv, 0);  // 11
+        for (size_t q = 0; q < sz; ++q)                                       // 12
+            r[q] = (T)((-alpha[at(q, nv)]) * (double)v[q] + 1.0 * (double)r[q]);
+        dot_canonical<T, double>(n, nv, t.data(), r.data(), theta.data());    // 13
+        dot_canonical<T, double>(n, nv, t.data(), t.data(), phi.data());
+        dot_canonical<T, double>(n, nv, t.data(), r0.data(), psi.data());
+        dot_canonical<T, double>(n, nv, r.data(), r.data(), eta.data());
+        precond(z, t);                                                        // 14
+        for (int k = 0; k < nv; ++k) omega[k] = theta[k] / phi[k];            // 15
+        for (size_t q = 0; q < sz; ++q)                                       // 16
+            r[q] = (T)((-omega[at(q, nv)]) * (double)t[q] + 1.0 * (double)r[q]);
+        for (int k = 0; k < nv; ++k) {                                        // 17
+            double ot = omega[k] * theta[k];
+            res[k] = 1.0 * eta[k] + (-1.0) * ot;
+        }
+        for (size_t q = 0; q < sz; ++q) {                                     // 23
+            int k = at(q, nv);
+            double ac = iconv[k] * alpha[k], oc = iconv[k] * omega[k];
+            x[q] = (T)(ac * (double)v_[q] + oc * (double)t_[q] + 1.0 * (double)x[q]);
+        }
+        cv.update(res.data());
+        hist.push(cv.res, nv);
+        if (cv.check()) return it;
+        for (int k = 0; k < nv; ++k) if (cv.status[k]) iconv[k] = 0;
+        for (int k = 0; k < nv; ++k) {
+            rho[k] = -1.0 * (omega[k] * psi[k]);                              // 21
+            double temp = delta[k] * omega[k];                                // 22
+            beta[k] = rho[k] / temp;
+            delta[k] = (-omega[k]) * beta[k];                                 // 25 (coefficient of s)
+        }
+        for (size_t q = 0; q < sz; ++q)                                       // 24
+            z[q] = (T)(1.0 * (double)t_[q] + (-omega[at(q, nv)]) * (double)z[q]);
+        for (size_t q = 0; q < sz; ++q) {                                     // 25
+            int k = at(q, nv);
+            v_[q] = (T)(1.0 * (double)z[q] + delta[k] * (double)s[q] + beta[k] * (double)v_[q]);
+        }
+    }
+    return it;
+}
+
 // Precision form: FP64 iterative refinement (IterativeRefinement::solve,
 // ir.inl:107-194 with subsolver_reduced_precision) around an FP32 PBiCGStab
 // whose inner products and alpha/beta/omega recurrences stay in FP64, with an
@@ -743,6 +826,25 @@ int orc_pbicgstab_d(i64 n, const int *rp, const int *ci, const double *v, void *
     cv.rel_tol = rel_tol;
     Hist H{hist, hist_cap};
     int it = pbicgstab<double>(A, (MG *)mg, b, x, nv, max_iters, cv, H);
+    for (int k = 0; k < nv; ++k) {
+        status[k] = cv.status[k];
+        res0[k] = cv.res0[k];
+    }
+    return it;
+}
+
+// FP64 RBiCGStab; arguments and outputs as orc_pbicgstab_d (mg == NULL: identity
+// preconditioner).
+int orc_rbicgstab_d(i64 n, const int *rp, const int *ci, const double *v, void *mg,
+                    const double *b, double *x, int nv, int max_iters, double abs_tol,
+                    double rel_tol, double *hist, int hist_cap, int *status, double *res0) {
+    Csr A;
+    fill(A, n, n, rp, ci, v);
+    Conv cv;
+    cv.abs_tol = abs_tol;
+    cv.rel_tol = rel_tol;
+    Hist H{hist, hist_cap};
+    int it = rbicgstab<double>(A, (MG *)mg, b, x, nv, max_iters, cv, H);
     for (int k = 0; k < nv; ++k) {
         status[k] = cv.status[k];
         res0[k] = cv.res0[k];

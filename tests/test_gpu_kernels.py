@@ -111,15 +111,18 @@ def test_dot_bit_exact(gpu, nv, n):
     for dtype, prec in ((np.float64, 0), (np.float32, 1)):
         vs = [rng.uniform(-1, 1, (n, nv)).astype(dtype) for _ in range(3)]
         dvs = [D(a) for a in vs]
-        pairs = [(0, 1), (1, 1), (2, 0)]
-        A = (C.c_void_p * 3)(*[P(dvs[i]) for i, _ in pairs])
-        B = (C.c_void_p * 3)(*[P(dvs[j]) for _, j in pairs])
-        part = D(np.zeros(max(L.xamg_dot_part_size(n, 3, nv), 1)))
-        out = D(np.zeros(3 * nv))
-        xamg.check(L.xamg_dot(prec, nv, n, 3, A, B, P(part), P(out), None))
-        got = H(out).reshape(3, nv)
-        for d, (i, j) in enumerate(pairs):
-            assert np.array_equal(got[d], orc.dot(vs[i], vs[j])), (d, dtype)
+        # three pairs, and the four of RBiCGStab's step 13 (one pass up to
+        # nv 8, two passes of two pairs above)
+        for pairs in ([(0, 1), (1, 1), (2, 0)], [(0, 1), (0, 0), (0, 2), (1, 1)]):
+            nd = len(pairs)
+            A = (C.c_void_p * nd)(*[P(dvs[i]) for i, _ in pairs])
+            B = (C.c_void_p * nd)(*[P(dvs[j]) for _, j in pairs])
+            part = D(np.zeros(max(L.xamg_dot_part_size(n, nd, nv), 1)))
+            out = D(np.zeros(nd * nv))
+            xamg.check(L.xamg_dot(prec, nv, n, nd, A, B, P(part), P(out), None))
+            got = H(out).reshape(nd, nv)
+            for d, (i, j) in enumerate(pairs):
+                assert np.array_equal(got[d], orc.dot(vs[i], vs[j])), (d, nd, dtype)
 
 
 @pytest.mark.parametrize("nv", [1, 4, 16, 32])

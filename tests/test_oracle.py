@@ -67,6 +67,27 @@ def test_recorded_solution_norm_and_analytic_check():
     assert np.linalg.norm(x[:, 0] - u) / np.sqrt(len(u)) < 1e-5
 
 
+@pytest.mark.parametrize("with_mg", [True, False])
+def test_rbicgstab_restatement_solves_recorded_problem(with_mg):
+    # rbicgstab.inl on the recorded 2-D problem: same solution as the recorded
+    # PBiCGStab run, and its recurrence residual is the true residual
+    rp, ci, v, b, u = util.gen2d(100 if with_mg else 40)
+    B = b.reshape(-1, 1)
+    mg = None
+    if with_mg:
+        csr = xamg.CsrMatrix.from_arrays(rp, ci, v)
+        mg = orc.MG(xamg.amg_host(csr, xamg.Params(util.amg_params(max_levels=25))))
+    x, it, hist, st, r0 = orc.rbicgstab(rp, ci, v, B, np.zeros_like(B), mg=mg, max_iters=2000, rel_tol=1e-8)
+    assert st[0] == 1 and it > 0 and hist.shape == (it + 1, 1)
+    true = B - orc.spmv(rp, ci, v, x, 1)
+    assert np.sqrt(orc.dot(true, true)[0]) <= 1.01e-8 * np.sqrt(r0[0])
+    assert abs(np.sqrt(hist[-1, 0]) - np.linalg.norm(true)) <= 1e-3 * np.sqrt(r0[0]) * 1e-8 + 1e-12
+    if with_mg:
+        assert abs(np.linalg.norm(x) - REC["X_norm"]) / REC["X_norm"] < 1e-7
+        xp, itp, _, _, _ = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg=mg, max_iters=100, rel_tol=1e-8)
+        assert abs(it - itp) <= 2
+
+
 def test_dot_orders_agree_to_rounding():
     rng = np.random.default_rng(1)
     for n, nv in [(1, 1), (255, 2), (257, 4), (70000, 16), (1000, 32)]:

@@ -804,7 +804,7 @@ int64_t xamg_dot_part_size(int64_t n, int nd, int nv) { return xk::dot_part_size
 int xamg_dot(int prec, int nv, int64_t n, int nd, const void *const *a, const void *const *b,
              double *part, double *out, void *stream) {
     return guard([&] {
-        XCHECK(nd >= 1 && nd <= 3, "nd must be 1..3");
+        XCHECK(nd >= 1 && nd <= 4, "nd must be 1..4");
         xk::dots((Prec)prec, nv, n, nd, a, b, part, out, strm(stream));
         XCUDA(cudaGetLastError());
     });

@@ -977,16 +977,18 @@ struct MultiGrid : Solver {
 MultiGrid *find_multigrid(Solver *s);
 
 // ------------------------------------------------------------------ Krylov
-// (P)BiCGStab.  Scalars live on the device; the host reads the NV residuals
-// once per iteration for the convergence check.
+// (P)BiCGStab and RBiCGStab.  Scalars live on the device; the host reads the
+// NV residuals once per iteration for the convergence check.
 struct Krylov : Solver {
     Matrix *A = nullptr;
     std::unique_ptr<Solver> M;
     bool precond = false;
+    bool reordered = false;  // RBiCGStab
     DVec r0, r, p, v, s, t, p_, s_;
     DBuf part, sc;
     Pinned hres;
-    enum { RHO, S1, S2, S3, S4, ALPHA, OMEGA, BETA, C1, RES, AC, OC, ICONV, ONES, NALPHA, NOMEGA, NSC };
+    enum { RHO, S1, S2, S3, S4, ALPHA, OMEGA, BETA, C1, RES, AC, OC, ICONV, ONES, NALPHA, NOMEGA,
+           THETA, PHI, PSI, ETA, DELTA, NSC };
     double *S(int i) const { return sc.as<double>() + (size_t)i * nv; }
 
     void setup(i64 n) {
@@ -994,8 +996,8 @@ struct Krylov : Solver {
         conv.init(nv);
         conv.prefix = role == "meta_solver" ? "META" : "SOLV";
         for (DVec *q : {&r0, &r, &p, &v, &s, &t}) q->alloc(n, nv, prec);
-        if (precond) { p_.alloc(n, nv, prec); s_.alloc(n, nv, prec); }
-        ensure_part(part, n, 3, nv);
+        if (precond || reordered) { p_.alloc(n, nv, prec); s_.alloc(n, nv, prec); }
+        ensure_part(part, n, reordered ? 4 : 3, nv);
         sc.alloc(sizeof(double) * NSC * nv);
         std::vector<double> z(NSC * nv, 0.0);
         for (int k = 0; k < nv; ++k) { z[ONES * nv + k] = 1.0; z[ICONV * nv + k] = 1.0; }
@@ -1023,11 +1025,11 @@ struct Krylov : Solver {
     }
 
     void solve(DVec &x, const DVec &b) override {
+        if (reordered) { solve_reordered(x, b); return; }
         cudaStream_t st = ctx().stream;
         int max_iters = (int)prm.get_int("max_iters");
         i64 n = x.n;
         const DCsr &a = dA();
-        std::vector<double> ic(NSC * nv, 0.0);
         conv.init(nv);
         set_rhs_base(conv, b, part);
         {
@@ -1081,6 +1083,76 @@ struct Krylov : Solver {
             dot1(r, r0, part, S(S1), st);
             xk::bicg_beta(nv, S(S1), S(RHO), S(ALPHA), S(OMEGA), S(BETA), S(C1), st);
             xk::blas(prec, nv, n, xk::Op::AXPBYPCZ, S(ONES), r.p(), S(C1), v.p(), S(BETA), p.p(), st);
+        }
+        XCUDA(cudaStreamSynchronize(st));
+    }
+
+    // RBiCGStab (rbicgstab.inl:48-225): the preconditioner is applied to r0 once
+    // and to v and t in every iteration; x is updated before the convergence
+    // check, so a converged iteration needs no further vector work.  The four
+    // inner products of step 13 are one fused launch.
+    void solve_reordered(DVec &x, const DVec &b) {
+        cudaStream_t st = ctx().stream;
+        int max_iters = (int)prm.get_int("max_iters");
+        i64 n = x.n;
+        const DCsr &a = dA();
+        DVec &z = p, &v_ = p_, &t_ = s_;
+        auto axpby = [&](const double *ca, const DVec &xx, const double *cb, const DVec &yy, DVec &zz) {
+            xk::blas(prec, nv, n, xk::Op::AXPBY_Z, ca, xx.p(), cb, yy.p(), nullptr, zz.p(), st);
+        };
+        auto apply_m = [&](DVec &out, const DVec &in) {
+            xk::fill(prec, out.count(), 0.0, out.p(), st);
+            M->solve(out, in);
+        };
+        conv.init(nv);
+        set_rhs_base(conv, b, part);
+        {
+            std::vector<double> one(nv, 1.0);
+            XCUDA(cudaMemcpyAsync(S(ICONV), one.data(), sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+        }
+        // 1-2: r0 = b - A x; rho = (r0, r0)
+        xk::spmv(prec, nv, n, a.rpp(), a.cip(), a.val(prec), x.p(), r0.p(), 2, b.p(), st);
+        dot1(r0, r0, part, S(RHO), st);
+        read_res(RHO, st);
+        conv.res0.assign(hres.h, hres.h + nv);
+        conv.update(hres.h);
+        conv.record();
+        if (conv.check()) return;
+        set_iconv(st);
+        xk::blas(prec, nv, n, xk::Op::COPY, nullptr, r0.p(), nullptr, nullptr, nullptr, r.p(), st);
+        apply_m(z, r0);                                                      // 3
+        xk::blas(prec, nv, n, xk::Op::COPY, nullptr, z.p(), nullptr, nullptr, nullptr, v_.p(), st);
+        for (int it = 1;; ++it) {
+            conv.iters = it;
+            spmv(v_, v, st);                                                 // 6
+            dot1(v, r0, part, S(DELTA), st);                                 // 7
+            apply_m(s, v);                                                   // 8
+            xk::rbicg_alpha(nv, S(RHO), S(DELTA), S(ALPHA), S(NALPHA), st);  // 9
+            axpby(S(ONES), z, S(NALPHA), s, t_);                             // 10
+            spmv(t_, t, st);                                                 // 11
+            axpby(S(NALPHA), v, S(ONES), r, r);                              // 12
+            {                                                                // 13
+                const void *Aa[4] = {t.p(), t.p(), t.p(), r.p()}, *Bb[4] = {r.p(), t.p(), r0.p(), r.p()};
+                xk::dots(prec, nv, n, 4, Aa, Bb, part.as<double>(), S(THETA), st);
+            }
+            apply_m(z, t);                                                   // 14
+            // 15, 17: omega = theta/phi; res = 1*eta + (-1)*(omega*theta);
+            // alpha_conv, omega_conv = iconv*alpha, iconv*omega
+            xk::bicg_omega(nv, S(THETA), S(PHI), S(ETA), S(ALPHA), S(ICONV), S(OMEGA), S(RES), S(AC),
+                           S(OC), st);
+            xk::negate(nv, S(OMEGA), S(NOMEGA), st);
+            axpby(S(NOMEGA), t, S(ONES), r, r);                              // 16
+            xk::blas(prec, nv, n, xk::Op::AXPBYPCZ, S(AC), v_.p(), S(OC), t_.p(), S(ONES), x.p(), st);
+            read_res(RES, st);
+            conv.update(hres.h);
+            conv.record();
+            if (conv.check()) break;
+            if (it >= max_iters) break;
+            set_iconv(st);
+            // 21-22, 25: rho = -(omega*psi); beta = rho/(delta*omega); delta = (-omega)*beta
+            xk::rbicg_beta(nv, S(OMEGA), S(PSI), S(DELTA), S(RHO), S(BETA), S(NOMEGA), st);
+            axpby(S(ONES), t_, S(NOMEGA), z, z);                             // 24
+            xk::blas(prec, nv, n, xk::Op::AXPBYPCZ, S(ONES), z.p(), S(DELTA), s.p(), S(BETA), v_.p(), st);
         }
         XCUDA(cudaStreamSynchronize(st));
     }
@@ -1162,10 +1234,12 @@ static std::unique_ptr<Solver> make_solver(const GlobalParams &gp, const std::st
     std::string m = pl.get_string("method");
     i64 n = A.h.n;
     if (prec == Prec::F32) A.ensure32();
-    if (m == "BiCGStab" || m == "MergedBiCGStab" || m == "PBiCGStab" || m == "MergedPBiCGStab") {
+    if (m == "BiCGStab" || m == "MergedBiCGStab" || m == "PBiCGStab" || m == "MergedPBiCGStab" ||
+        m == "RBiCGStab" || m == "MergedRBiCGStab") {
         auto k = std::unique_ptr<Krylov>(new Krylov());
         k->role = role; k->method = m; k->prm = pl; k->nv = nv; k->prec = prec; k->A = &A;
-        k->precond = (m == "PBiCGStab" || m == "MergedPBiCGStab");
+        k->reordered = (m == "RBiCGStab" || m == "MergedRBiCGStab");
+        k->precond = (m == "PBiCGStab" || m == "MergedPBiCGStab" || k->reordered);
         if (k->precond) {
             if (gp.has("preconditioner")) k->M = make_solver(gp, "preconditioner", A, nv, prec);
             else {

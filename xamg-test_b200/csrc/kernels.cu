@@ -755,18 +755,20 @@ void dense_gemv(Prec p, int nv, int n, const void *AinvT, const void *b, void *y
 // l+224 (fma, FP64), then a xor-butterfly over the 32 lanes (off = 16..1),
 // whose lane-0 value equals the pairwise tree s[l] += s[l+off].
 // Partials are stored dot-major: part[(d*nv + k) * nchunks + c].
+template <class TI>
+struct DotPairs {
+    const TI *a[4];
+    const TI *b[4];
+};
 template <class TI, int NV, int ND>
-__global__ void __launch_bounds__(256) k_dot1(i64 n, i64 nch, const TI *__restrict__ a0,
-                                              const TI *__restrict__ b0,
-                                              const TI *__restrict__ a1,
-                                              const TI *__restrict__ b1,
-                                              const TI *__restrict__ a2,
-                                              const TI *__restrict__ b2, double *__restrict__ part) {
+__global__ void __launch_bounds__(256) k_dot1(i64 n, i64 nch, DotPairs<TI> pr, double *__restrict__ part) {
     const int lane = threadIdx.x & 31;
     const i64 c = (i64)blockIdx.x * 8 + (threadIdx.x >> 5);
     if (c >= nch) return;
-    const TI *A[3] = {a0, a1, a2};
-    const TI *B[3] = {b0, b1, b2};
+    const TI *__restrict__ A[ND];
+    const TI *__restrict__ B[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) { A[d] = pr.a[d]; B[d] = pr.b[d]; }
     double acc[ND][NV];
 #pragma unroll
     for (int d = 0; d < ND; ++d)
@@ -834,13 +836,25 @@ static void dots_t(i64 n, int nd, const void *const *a, const void *const *b, do
         return;
     }
     unsigned g = (unsigned)((nch + 7) / 8);
-    const TI *A0 = (const TI *)a[0], *B0 = (const TI *)b[0];
-    const TI *A1 = nd > 1 ? (const TI *)a[1] : A0, *B1 = nd > 1 ? (const TI *)b[1] : B0;
-    const TI *A2 = nd > 2 ? (const TI *)a[2] : A0, *B2 = nd > 2 ? (const TI *)b[2] : B0;
+    DotPairs<TI> pr;
+    for (int d = 0; d < 4; ++d) {
+        pr.a[d] = (const TI *)a[d < nd ? d : 0];
+        pr.b[d] = (const TI *)b[d < nd ? d : 0];
+    }
     note_launch(2);
-    if (nd == 1) k_dot1<TI, NV, 1><<<g, 256, 0, s>>>(n, nch, A0, B0, A1, B1, A2, B2, part);
-    else if (nd == 2) k_dot1<TI, NV, 2><<<g, 256, 0, s>>>(n, nch, A0, B0, A1, B1, A2, B2, part);
-    else k_dot1<TI, NV, 3><<<g, 256, 0, s>>>(n, nch, A0, B0, A1, B1, A2, B2, part);
+    if (nd == 1) k_dot1<TI, NV, 1><<<g, 256, 0, s>>>(n, nch, pr, part);
+    else if (nd == 2) k_dot1<TI, NV, 2><<<g, 256, 0, s>>>(n, nch, pr, part);
+    else if (nd == 3) k_dot1<TI, NV, 3><<<g, 256, 0, s>>>(n, nch, pr, part);
+    else if constexpr (NV <= 8) k_dot1<TI, NV, 4><<<g, 256, 0, s>>>(n, nch, pr, part);
+    else {
+        // four pairs at wide NV: two passes of two pairs (register budget);
+        // each pair's partials are the same as in one pass
+        DotPairs<TI> hi;
+        for (int d = 0; d < 2; ++d) { hi.a[d] = pr.a[d + 2]; hi.b[d] = pr.b[d + 2]; hi.a[d + 2] = hi.a[d]; hi.b[d + 2] = hi.b[d]; }
+        note_launch();
+        k_dot1<TI, NV, 2><<<g, 256, 0, s>>>(n, nch, pr, part);
+        k_dot1<TI, NV, 2><<<g, 256, 0, s>>>(n, nch, hi, part + (i64)2 * NV * nch);
+    }
     k_dot2<<<nd * NV, 256, 0, s>>>(nch, part, out);
 }
 
@@ -991,6 +1005,38 @@ void bicg_beta(int nv, const double *s1, double *rho, const double *alpha, const
                double *beta, double *c1, cudaStream_t s) {
     note_launch();
     k_beta<<<sblocks(nv), 128, 0, s>>>(nv, s1, rho, alpha, omega, beta, c1);
+}
+// RBiCGStab recurrences (rbicgstab.inl:130-134 and 193-211)
+__global__ void k_ralpha(int nv, const double *rho, const double *delta, double *alpha,
+                         double *nalpha) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nv) return;
+    double a = __ddiv_rn(rho[k], delta[k]);
+    alpha[k] = a;
+    nalpha[k] = dmul(-1.0, a);
+}
+void rbicg_alpha(int nv, const double *rho, const double *delta, double *alpha, double *nalpha,
+                 cudaStream_t s) {
+    note_launch();
+    k_ralpha<<<sblocks(nv), 128, 0, s>>>(nv, rho, delta, alpha, nalpha);
+}
+__global__ void k_rbeta(int nv, const double *omega, const double *psi, double *delta, double *rho,
+                        double *beta, double *nomega) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nv) return;
+    double w = omega[k];
+    double r = dmul(-1.0, dmul(w, psi[k]));
+    double bt = __ddiv_rn(r, dmul(delta[k], w));
+    double nw = dmul(-1.0, w);
+    rho[k] = r;
+    beta[k] = bt;
+    nomega[k] = nw;
+    delta[k] = dmul(nw, bt);
+}
+void rbicg_beta(int nv, const double *omega, const double *psi, double *delta, double *rho,
+                double *beta, double *nomega, cudaStream_t s) {
+    note_launch();
+    k_rbeta<<<sblocks(nv), 128, 0, s>>>(nv, omega, psi, delta, rho, beta, nomega);
 }
 __global__ void k_neg(int nv, const double *in, double *out) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;

@@ -91,8 +91,8 @@ void jacobi(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val
 void dense_gemv(Prec p, int nv, int n, const void *AinvT, const void *b, void *y, cudaStream_t s);
 
 // ---- inner products -------------------------------------------------------
-// nd pairs (a_d, b_d) of N x NV vectors (element type `in`), FP64 results
-// out[d*nv + k].  part must hold dot_part_size(n, nd, nv) doubles.
+// nd (1..4) pairs (a_d, b_d) of N x NV vectors (element type `in`), FP64
+// results out[d*nv + k].  part must hold dot_part_size(n, nd, nv) doubles.
 i64 dot_part_size(i64 n, int nd, int nv);
 void dots(Prec in, int nv, i64 n, int nd, const void *const *a, const void *const *b,
           double *part, double *out, cudaStream_t s);
@@ -125,6 +125,13 @@ void bicg_omega(int nv, const double *s2, const double *s3, const double *s4,
 // beta = (s1/rho)*(alpha/omega); rho = s1; c1 = -(omega*beta); also -alpha, -omega
 void bicg_beta(int nv, const double *s1, double *rho, const double *alpha, const double *omega,
                double *beta, double *c1, cudaStream_t s);
+// RBiCGStab: alpha = rho/delta, nalpha = -1*alpha
+void rbicg_alpha(int nv, const double *rho, const double *delta, double *alpha, double *nalpha,
+                 cudaStream_t s);
+// RBiCGStab: rho = -1*(omega*psi); beta = rho/(delta*omega); nomega = -1*omega;
+// delta = nomega*beta (the coefficient of s in the v_ update)
+void rbicg_beta(int nv, const double *omega, const double *psi, double *delta, double *rho,
+                double *beta, double *nomega, cudaStream_t s);
 // negate: out = -1 * in
 void negate(int nv, const double *in, double *out, cudaStream_t s);
 
