@@ -140,64 +140,121 @@ def build_problem():
     return csr, B
 
 
-def spmv_time(csr, prec=0, variant=-1, iters=20):
-    """Live CUDA-event timing of the NV=16 CSR SpMV on the benchmark matrix,
-    launched on a torch stream through the C ABI; returns ms per launch."""
+# SpMV kernels timed for the roofline: CSR variants of xamg_spmv_set_variant,
+# and RUN8 = the shifted-row run kernel (chunks of 8 rows)
+RUN8 = 108
+
+
+def spmv_time(csr, prec=0, variant=-1, iters=20, info=None):
+    """Live CUDA-event timing of the NV=16 SpMV on the benchmark matrix,
+    launched on a torch stream through the C ABI; returns ms per launch.  For
+    the run kernel `info` (a dict) receives the plan's sizes."""
     import ctypes as C
     import torch
     import xamg
     rp, ci, v = csr.arrays()
     n = csr.nrows
     dt = torch.float64 if prec == 0 else torch.float32
-    d = [torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), torch.from_numpy(v).to(dt).cuda()]
     x = torch.rand(n, NV, dtype=dt, device="cuda")
     y = torch.empty_like(x)
     st = torch.cuda.Stream()
     P = lambda t: C.c_void_p(t.data_ptr())
-    torch.cuda.synchronize()
     L = xamg.lib()
-    old = L.xamg_spmv_set_variant(variant)
-    with torch.cuda.stream(st):
-        for _ in range(3):
-            L.xamg_csr_spmv(prec, NV, n, P(d[0]), P(d[1]), P(d[2]), P(x), P(y), 0, None, C.c_void_p(st.cuda_stream))
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        for _ in range(iters):
-            L.xamg_csr_spmv(prec, NV, n, P(d[0]), P(d[1]), P(d[2]), P(x), P(y), 0, None, C.c_void_p(st.cuda_stream))
-        e1.record(st)
-    st.synchronize()
-    L.xamg_spmv_set_variant(old)
+    plan = None
+    if variant == RUN8:
+        plan = L.xamg_spmv_runs_plan_create(n, xamg._ptr(rp), xamg._ptr(ci), xamg._ptr(np.ascontiguousarray(v)),
+                                            8, int(prec == 1))
+        assert plan, L.XAMG_b200_last_error()
+        if info is not None:
+            a = np.zeros(4, np.int64)
+            cov = np.zeros(1)
+            xamg.check(L.xamg_spmv_runs_plan_info(plan, xamg._ptr(a[0:]), xamg._ptr(cov), xamg._ptr(a[1:]),
+                                                  xamg._ptr(a[2:])))
+            info.update(nchunks=int(a[0]), coverage=float(cov[0]), segments=int(a[1]), value_slots=int(a[2]))
+        launch = lambda: L.xamg_spmv_runs(plan, prec, NV, P(x), P(y), 0, None, C.c_void_p(st.cuda_stream))
+    else:
+        d = [torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), torch.from_numpy(v).to(dt).cuda()]
+        launch = lambda: L.xamg_csr_spmv(prec, NV, n, P(d[0]), P(d[1]), P(d[2]), P(x), P(y), 0, None,
+                                         C.c_void_p(st.cuda_stream))
+    torch.cuda.synchronize()
+    old = L.xamg_spmv_set_variant(variant if plan is None else -1)
+    try:
+        with torch.cuda.stream(st):
+            for _ in range(3):
+                xamg.check(launch())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(iters):
+                launch()
+            e1.record(st)
+        st.synchronize()
+    finally:
+        L.xamg_spmv_set_variant(old)
+        if plan:
+            L.xamg_spmv_runs_plan_destroy(plan)
     return e0.elapsed_time(e1) / iters
 
 
 def tune_spmv(csr, prec=0):
-    """Autotune the SpMV kernel variant on this matrix (results are identical
-    for every variant; only the launch shape differs)."""
+    """Autotune the SpMV kernel on this matrix (results are identical for
+    every kernel; only the data layout and launch shape differ)."""
     res = {}
-    for var in (0, 3, 5, 6):
+    for var in (0, 3, 5, 6, RUN8):
         res[var] = spmv_time(csr, prec, var, iters=10)
     best = min(res, key=res.get)
     return best, res
 
 
+def apply_spmv_choice(var):
+    """Make the library use the tuned kernel: the run kernel (through the run
+    plans built at matrix construction) or a CSR variant everywhere."""
+    import xamg
+    L = xamg.lib()
+    if var == RUN8:
+        L.xamg_spmv_set_run_rows(8)
+        L.xamg_spmv_set_variant(-1)
+    else:
+        L.xamg_spmv_set_run_rows(0)
+        L.xamg_spmv_set_variant(var)
+
+
 def spmv_roofline(csr, variant):
-    ms = spmv_time(csr, 0, variant, iters=20)
+    info = {}
+    ms = spmv_time(csr, 0, variant, iters=20, info=info)
     n, nnz = csr.nrows, csr.nnz
-    byts = nnz * (8 + 4) + (n + 1) * 4 + 2 * n * NV * 8
+    xy = 2 * n * NV * 8
+    if variant == RUN8:
+        # run format: each value once, each chunk's segments once (4 B), the
+        # chunk descriptors (16 B) and tile offsets (16 B per four chunks), x and y
+        byts = nnz * 8 + info["segments"] * 4 + info["nchunks"] * 20 + xy
+        kern = "k_spmv_runs<double,16,0>"
+    else:
+        byts = nnz * (8 + 4) + (n + 1) * 4 + xy
+        kern = {0: "k_spmv<double,16,0,4>", 1: "k_spmv<double,16,0,8>", 2: "k_spmv<double,16,0,16>",
+                3: "k_spmv_tile<double,16,0,4,0>", 4: "k_spmv_tile<double,16,0,8,0>",
+                5: "k_spmv_tile<double,16,0,4,1>", 6: "k_spmv_tile<double,16,0,8,1>"}.get(
+                    variant, "k_spmv_stream<double,16,0>")
     peak, src = peak_hbm()
     ach = byts / (ms * 1e-3) / 1e9
-    kern = {0: "k_spmv<double,16,0,4>", 1: "k_spmv<double,16,0,8>", 2: "k_spmv<double,16,0,16>",
-            3: "k_spmv_tile<double,16,0,4,0>", 4: "k_spmv_tile<double,16,0,8,0>",
-            5: "k_spmv_tile<double,16,0,4,1>", 6: "k_spmv_tile<double,16,0,8,1>"}.get(variant, "k_spmv_stream<double,16,0>")
     # DRAM traffic per launch: the ncu capture of the same kernel on the 96^3
-    # operator measured 0.9457 x its algorithmic bytes (483.3 of 510.8 MB,
-    # profiles/k_spmv_tile_fp64_nv16_27pt_96cube.md); traffic scales with the
-    # operator, so the 128^3 figure is that ratio times the algorithmic bytes
-    traffic = round(0.9457 * byts) if variant in (5, 6) else None
-    return {"bound": "hbm", "kernel": kern, "variant": variant, "achieved": round(ach, 1), "peak": peak,
-            "peak_source": src, "unit": "GB/s", "frac": round(ach / peak, 4),
-            "traffic": traffic, "traffic_source": "ncu capture at 96^3 scaled to 128^3" if traffic else None,
-            "algorithmic_bytes": byts, "launch_ms": round(ms, 4)}
+    # operator measured TRAFFIC_RATIO x its algorithmic bytes; traffic scales
+    # with the operator, so the 128^3 figure is that ratio times the
+    # algorithmic bytes
+    ratio = TRAFFIC_RATIO.get(variant)
+    traffic = round(ratio * byts) if ratio else None
+    out = {"bound": "hbm", "kernel": kern, "variant": variant, "achieved": round(ach, 1), "peak": peak,
+           "peak_source": src, "unit": "GB/s", "frac": round(ach / peak, 4),
+           "traffic": traffic, "traffic_source": "ncu capture at 96^3 scaled to 128^3" if traffic else None,
+           "algorithmic_bytes": byts, "launch_ms": round(ms, 4)}
+    if info:
+        out["run_plan"] = info
+    return out
+
+
+# DRAM bytes / algorithmic bytes of one launch in the ncu captures on the 96^3
+# operator (profiles/k_spmv_tile_fp64_nv16_27pt_96cube.md: 483.3 of 510.8 MB;
+# profiles/k_spmv_runs_fp64_nv16_27pt_96cube.md: 433.9 of 421.8 MB)
+TRAFFIC_RATIO = {5: 0.9457, 6: 0.9457, RUN8: 1.0287}
 
 
 def run_form(csr, B, spec, warmup, steps):
@@ -322,7 +379,7 @@ def learned_form(nsys=16):
     out = {"systems": nsys, "rhs": nsys * 8, "n": 64}
     for k in ("its_zero", "its_x0", "ms_zero", "ms_x0", "ms_infer", "ms_smooth", "guess_rel_res", "guess_rel_err",
               "rel_diff"):
-        out["mean_" + k] = round(float(np.mean([e[k] for e in ev])), 5)
+        out["mean_" + k] = float("%.5g" % np.mean([e[k] for e in ev]))
     out["ms_per_rhs_zero"] = round(out["mean_ms_zero"] / 8, 4)
     out["ms_per_rhs_x0"] = round(out["mean_ms_x0"] / 8, 4)
     out["converged"] = all(e["converged"] for e in ev)
@@ -431,6 +488,8 @@ def main():
     ap.add_argument("--kernel", choices=["spmv", "gs"], help="time one hot kernel alone (profiling)")
     ap.add_argument("--n", type=int, default=96, help="grid side of --kernel")
     ap.add_argument("--variant", type=int, default=-1, help="SpMV variant of --kernel spmv")
+    ap.add_argument("--spmv", type=int, default=None,
+                    help="use this SpMV kernel instead of tuning (0-6: CSR variants, 108: run kernel)")
     args = ap.parse_args()
     if args.kernel:
         return kernel_case(args)
@@ -449,8 +508,11 @@ def main():
     import xamg
     xamg.init(NV)
     csr, B = build_problem()
-    best_var, var_ms = tune_spmv(csr, 0)
-    xamg.lib().xamg_spmv_set_variant(best_var)
+    if args.spmv is not None:  # fixed kernel (profiler runs: timing under a profiler misleads the tuner)
+        best_var, var_ms = args.spmv, {}
+    else:
+        best_var, var_ms = tune_spmv(csr, 0)
+    apply_spmv_choice(best_var)
     allforms = args.forms.split(",")
     forms = [f for f in allforms if f in ("plain", "mixed")]
     res = {}
@@ -494,6 +556,16 @@ def main():
     err = None
     if "plain" in X and "mixed" in X:
         err = float(np.linalg.norm(X["mixed"] - X["plain"]) / np.linalg.norm(X["plain"]))
+    # FP64 check of every form's solution on the host: max over columns of
+    # ||b - A x|| / ||b||
+    true_res = {}
+    if rank == 0:
+        import scipy.sparse as sp
+        rp, ci, v = csr.arrays()
+        Ah = sp.csr_matrix((v, ci, rp), shape=(csr.nrows, csr.nrows))
+        for f, Xf in X.items():
+            R = B - Ah @ Xf
+            true_res[f] = float(np.max(np.linalg.norm(R, axis=0) / np.linalg.norm(B, axis=0)))
     cpu = None
     if rank == 0 and not args.no_cpu and "plain" in keep:
         sec = cpu_sample(csr, B, keep["plain"][0])
@@ -513,7 +585,7 @@ def main():
                    "form": best, "l2": "inputs larger than L2 (matrix 669 MB)"},
         "forms": dict({f: {k: res[f][k] for k in ("ms", "iters", "sub_iters", "converged", "setup_s", "launches")}
                        for f in forms}, **extra),
-        "mixed_vs_plain_rel_err": err,
+        "mixed_vs_plain_rel_err": err, "true_rel_residual": true_res,
         "e2e": {"value": round(e2e_ms / NV, 4), "unit": "ms/RHS", "h2d_bytes_per_step": csr.nrows * NV * 8,
                 "d2h_bytes_per_step": csr.nrows * NV * 8},
         "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,

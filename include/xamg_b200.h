@@ -126,8 +126,36 @@ int xamg_csr_spmv(int prec, int nv, int64_t n, const int *rp, const int *ci, con
  * a time; 3, 4 = the tile's entries staged in shared memory, gathers 4 or 8 at
  * a time; 5, 6 = staged entries with a plain row loop unrolled 4 or 8 times;
  * 10 + k = staged streaming kernel walking k tiles per CTA; -1 = default (6
- * when nv * element size >= 64 bytes, else 0).  Returns the previous setting. */
+ * when nv * element size >= 64 bytes, else 0).  Under -1 and 7 the products
+ * of operators that have a shifted-row run plan (below) use the run kernel
+ * (7 elsewhere = the default).  Returns the previous setting. */
 int xamg_spmv_set_variant(int variant);
+
+/* Shifted-row run SpMV (no counterpart in the reference; the same results as
+ * xamg_csr_spmv, bit for bit).  The plan groups the rows into chunks of up to
+ * `rows` (4 or 8) consecutive rows whose column indices are the first row's
+ * shifted by the row offset, ci(r0+q, e) = ci(r0, e) + q (the interior rows
+ * of stencil operators), and stores the values chunk-interleaved; for a run
+ * of up to 3 consecutive columns the chunk's rows gather the x rows they
+ * share once (len + rows - 1 gathers instead of len * rows).  Every row lies in some chunk (irregular rows in
+ * chunks of one), so a plan serves any square matrix.  rp/ci/val are HOST
+ * arrays; values are kept in FP64 and, when fp32 != 0, in FP32.  Shapes with
+ * nv * element size >= 64 bytes (FP64 nv 8, 16, 32; FP32 nv 16, 32).
+ * Matrices constructed through the C API get a plan (rows set by
+ * xamg_spmv_set_run_rows, default 4, 0 = none) when they have at least 4096
+ * rows and half of their entries lie in full chunks.
+ * plan_info (any output may be NULL): chunk count, fraction of the entries
+ * in full chunks, segments (runs of at most 3 consecutive columns of each
+ * chunk's first row, summed over the chunks) and stored value slots (entries
+ * times rows per chunk, padding included). */
+void *xamg_spmv_runs_plan_create(int64_t n, const int *rp_host, const int *ci_host,
+                                 const double *val_host, int rows, int fp32);
+int xamg_spmv_runs_plan_info(void *plan, int64_t *nchunks, double *coverage, int64_t *segments,
+                             int64_t *value_slots);
+int xamg_spmv_runs(void *plan, int prec, int nv, const void *x, void *y, int mode, const void *b,
+                   void *stream);
+int xamg_spmv_runs_plan_destroy(void *plan);
+int xamg_spmv_set_run_rows(int rows);
 
 /* Gauss-Seidel plan (wavefront schedule) for blas2::SGS / csr_SGS
  * (blas2.h:184-281, csr_gs.inl:32-134).  rp/ci are HOST arrays.  block_rows

@@ -83,6 +83,84 @@ def test_spmv_bit_exact(gpu, dtype, nv):
         L.xamg_spmv_set_variant(old)
 
 
+def _run_matrices():
+    """Square test operators for the shifted-row run kernel: stencils (runs
+    along the grid lines), a ragged random matrix (every row a chunk of one,
+    unsorted columns, empty rows) and a block-diagonal mix of both with one
+    long row, so chunks of every length and tiles with unequal entry counts
+    occur."""
+    import scipy.sparse as sp
+    rng = np.random.default_rng(42)
+    out = [xamg.CsrMatrix.aniso27(13).arrays(), xamg.CsrMatrix.cube(11, 7, 5, 0).arrays(),
+           util.random_csr(1200, 1200, rng, max_nnz=30, empty_rows=(0, 7, 1199))]
+    arp, aci, av = xamg.CsrMatrix.aniso27(9).arrays()
+    a = sp.csr_matrix((av, aci, arp), shape=(len(arp) - 1,) * 2)
+    rp, ci, v = util.random_csr(301, 301, rng, max_nnz=9, empty_rows=(3,))
+    r = sp.csr_matrix((v, ci, rp), shape=(301, 301))
+    blk = sp.block_diag([a, r, sp.identity(5), a], format="lil")
+    blk[7, :200] = rng.uniform(-1, 1, 200)  # one long row
+    blk = blk.tocsr()
+    blk.sort_indices()
+    out.append((blk.indptr.astype(np.int32), blk.indices.astype(np.int32), blk.data.astype(np.float64)))
+    return out
+
+
+@pytest.mark.parametrize("dtype,nv", [(np.float64, 8), (np.float64, 16), (np.float64, 32),
+                                      (np.float32, 16), (np.float32, 32)])
+def test_spmv_runs_bit_exact(gpu, dtype, nv):
+    """Shifted-row run kernel: identical bits to the oracle's CSR product in
+    all three modes, on stencil, irregular and mixed operators."""
+    L = xamg.lib()
+    prec = 0 if dtype == np.float64 else 1
+    for mi, (rp, ci, v) in enumerate(_run_matrices()):
+        n = len(rp) - 1
+        plan = L.xamg_spmv_runs_plan_create(n, xamg._ptr(rp), xamg._ptr(ci), xamg._ptr(v), 8, 1)
+        assert plan, xamg.lib().XAMG_b200_last_error()
+        try:
+            nch = np.zeros(1, np.int64)
+            cov = np.zeros(1)
+            ns = np.zeros(1, np.int64)
+            xamg.check(L.xamg_spmv_runs_plan_info(plan, xamg._ptr(nch), xamg._ptr(cov), xamg._ptr(ns), None))
+            assert ns[0] <= len(ci)
+            if mi == 0:
+                assert ns[0] < len(ci) / 6  # 27-point rows: 9 segments of 3, chunks of several rows
+            if mi == 0:
+                assert cov[0] > 0.6 and nch[0] < n / 2, (cov, nch, n)
+            if mi == 2:
+                assert cov[0] == 0.0 and nch[0] == n
+            vv = v.astype(dtype)
+            rng = np.random.default_rng(nv + mi)
+            x = rng.uniform(-1, 1, (n, nv)).astype(dtype)
+            y0 = rng.uniform(-1, 1, (n, nv)).astype(dtype)
+            b = rng.uniform(-1, 1, (n, nv)).astype(dtype)
+            dx, db = D(x), D(b)
+            for mode in (0, 1, 2):
+                dy = D(y0)
+                sync()
+                xamg.check(L.xamg_spmv_runs(plan, prec, nv, P(dx), P(dy), mode, P(db), None))
+                got = H(dy)
+                ref = orc.spmv(rp, ci, vv, x, nv, y=y0.copy() if mode == 1 else None, acc=mode == 1)
+                if mode == 2:
+                    ref = (dtype(1) * b + dtype(-1) * ref).astype(dtype)
+                assert np.array_equal(got, ref), (mi, mode, np.abs(got - ref).max())
+        finally:
+            L.xamg_spmv_runs_plan_destroy(plan)
+
+
+def test_spmv_runs_rejects_narrow_shapes(gpu):
+    rp, ci, v = xamg.CsrMatrix.aniso27(6).arrays()
+    L = xamg.lib()
+    plan = L.xamg_spmv_runs_plan_create(len(rp) - 1, xamg._ptr(rp), xamg._ptr(ci), xamg._ptr(v), 8, 0)
+    try:
+        n = len(rp) - 1
+        dx, dy = D(np.zeros((n, 4))), D(np.zeros((n, 4)))
+        assert L.xamg_spmv_runs(plan, 0, 4, P(dx), P(dy), 0, None, None) == 2   # nv 4: not a run shape
+        assert L.xamg_spmv_runs(plan, 1, 16, P(dx), P(dy), 0, None, None) == 2  # no FP32 values
+    finally:
+        L.xamg_spmv_runs_plan_destroy(plan)
+    assert L.xamg_spmv_runs_plan_create(len(rp) - 1, xamg._ptr(rp), xamg._ptr(ci), xamg._ptr(v), 4, 0) is None
+
+
 def test_spmv_large_checksum(gpu):
     """Full-size product through a size-independent property: y = A x for
     x = e_k columns reproduces the CSR columns, checked by a bxor-style

@@ -21,8 +21,8 @@ LIB = os.path.join(HERE, "libxamg_b200.so")
 ORACLE_LIB = os.path.join(ROOT, "oracle", "liboracle.so")
 
 CU_SOURCES = ["kernels.cu", "gs.cu", "noalloc.cu", "cnn.cu", "batch.cu"]
-CPP_SOURCES = ["host/gen.cpp", "host/amg.cpp", "host/params.cpp", "host/solve.cpp", "host/batch.cpp",
-               "host/c_api.cpp"]
+CPP_SOURCES = ["host/gen.cpp", "host/amg.cpp", "host/params.cpp", "host/solve.cpp", "host/runs.cpp",
+               "host/batch.cpp", "host/c_api.cpp"]
 
 
 def _run(cmd):

@@ -104,7 +104,7 @@ void Batch::create(int nsys, const i64 *n, const int *const *rp, const int *cons
 void Batch::autotune(BatchGroup &G) {
     cudaStream_t st = ctx().stream;
     const DCsr &a = G.A.d;
-    const int vars[] = {0, 1, 2, 3, 5, 6};
+    const int vars[] = {0, 1, 2, 3, 5, 6, 7};  // 7: shifted-row runs where the operator has a plan
     cudaEvent_t e0, e1;
     XCUDA(cudaEventCreate(&e0));
     XCUDA(cudaEventCreate(&e1));
@@ -117,10 +117,10 @@ void Batch::autotune(BatchGroup &G) {
         int bv = -1;
         for (int v : vars) {
             xk::set_spmv_variant(v);
-            xk::spmv(p, G.nv, a.n, a.rpp(), a.cip(), a.val(p), xv, yv, 0, nullptr, st);
+            a.spmv(p, G.nv, xv, yv, 0, nullptr, st);
             XCUDA(cudaEventRecord(e0, st));
             for (int q = 0; q < 5; ++q)
-                xk::spmv(p, G.nv, a.n, a.rpp(), a.cip(), a.val(p), xv, yv, 0, nullptr, st);
+                a.spmv(p, G.nv, xv, yv, 0, nullptr, st);
             XCUDA(cudaEventRecord(e1, st));
             XCUDA(cudaEventSynchronize(e1));
             float ms = 0.f;
@@ -142,7 +142,7 @@ void Batch::run_init(BatchGroup &G) {
     const i64 *so = G.segoff.as<i64>(), *cs = G.cstart.as<i64>();
     double *part = G.part.as<double>();
     xk::set_spmv_variant(G.var64);
-    xk::spmv(Prec::F64, G.nv, N, a.rpp(), a.cip(), a.val(Prec::F64), G.x.p(), G.r0.p(), 2, G.b.p(), st);
+    a.spmv(Prec::F64, G.nv, G.x.p(), G.r0.p(), 2, G.b.p(), st);
     const void *A1[1] = {G.r0.p()}, *B1[1] = {G.r0.p()};
     xk::seg_dots(Prec::F64, G.nv, nseg, so, cs, G.nch, 1, A1, B1, part, G.S(RHO), st);
     XCUDA(cudaMemcpyAsync(G.S(RES0), G.S(RHO), sizeof(double) * G.nsc, cudaMemcpyDeviceToDevice, st));
@@ -168,7 +168,7 @@ void Batch::run_body(BatchGroup &G, int graph_mode) {
         xk::set_spmv_variant(G.var64);
     };
     auto spmv = [&](const DVec &x, DVec &y) {
-        xk::spmv(Prec::F64, nv, N, a.rpp(), a.cip(), a.val(Prec::F64), x.p(), y.p(), 0, nullptr, st);
+        a.spmv(Prec::F64, nv, x.p(), y.p(), 0, nullptr, st);
     };
     auto dot1 = [&](const DVec &x, const DVec &y, double *out) {
         const void *A1[1] = {x.p()}, *B1[1] = {y.p()};

@@ -735,6 +735,64 @@ int xamg_spmv_set_variant(int variant) {
     xk::set_spmv_variant(variant);
     return old;
 }
+int xamg_spmv_set_run_rows(int rows) {
+    int old = xk::get_spmv_run_rows();
+    xk::set_spmv_run_rows(rows);
+    return old;
+}
+void *xamg_spmv_runs_plan_create(int64_t n, const int *rp, const int *ci, const double *val, int rows, int fp32) {
+    RunPlan *h = nullptr;
+    int rc = guard([&] {
+        XCHECK(n > 0 && rp && ci && val, "bad CSR arrays");
+        XCHECK(rows == 8, "rows must be 8");
+        ctx();
+        HostCsr A;
+        A.n = A.ncols = n;
+        A.rp.assign(rp, rp + n + 1);
+        A.ci.assign(ci, ci + rp[n]);
+        A.v.assign(val, val + rp[n]);
+        h = new RunPlan();
+        XCHECK(h->build(A, rows, true, fp32 != 0, 0.0), "run plan not built");
+    });
+    if (rc) { delete h; return nullptr; }
+    return h;
+}
+int xamg_spmv_runs_plan_info(void *plan, int64_t *nchunks, double *coverage, int64_t *segments,
+                             int64_t *value_slots) {
+    return guard([&] {
+        XCHECK(plan, "null plan");
+        RunPlan *h = (RunPlan *)plan;
+        if (coverage) *coverage = h->coverage;
+        if (nchunks) {  // chunks holding rows (the padding excluded)
+            int64_t k = 0;
+            for (i64 c = 0; c < h->nchunks; ++c) k += h->hchunks[(size_t)c * 4 + 1] > 0;
+            *nchunks = k;
+        }
+        if (segments) {
+            int64_t s = 0;
+            for (i64 c = 0; c < h->nchunks; ++c) s += h->hchunks[(size_t)c * 4 + 3];
+            *segments = s;
+        }
+        if (value_slots) *value_slots = h->hvoff.empty() ? 0 : h->hvoff.back() * h->R;
+    });
+}
+int xamg_spmv_runs(void *plan, int prec, int nv, const void *x, void *y, int mode, const void *b, void *stream) {
+    return guard([&] {
+        XCHECK(plan, "null plan");
+        RunPlan *h = (RunPlan *)plan;
+        XCHECK(prec == 0 || prec == 1, "prec must be 0 or 1");
+        XCHECK(mode >= 0 && mode <= 2, "mode must be 0, 1 or 2");
+        XCHECK(mode != 2 || b, "mode 2 needs b");
+        XCHECK(xk::spmv_runs_supported((Prec)prec, nv), "shape not supported (FP64 nv 8, 16, 32; FP32 nv 16, 32)");
+        XCHECK(h->has((Prec)prec), "plan has no values in this precision");
+        xk::spmv_runs((Prec)prec, nv, h->nchunks, h->ntiles, h->chunks.as<int4>(), h->toff.as<longlong2>(),
+                      h->sg.as<int>(), prec == 0 ? h->v64.p : h->v32.p, x, y, mode, b, strm(stream));
+        XCUDA(cudaGetLastError());
+    });
+}
+int xamg_spmv_runs_plan_destroy(void *plan) {
+    return guard([&] { delete (RunPlan *)plan; });
+}
 void *xamg_gs_plan_create(int64_t n, const int *rp, const int *ci, int64_t block_rows,
                           int schedule) {
     PlanHandle *h = nullptr;

@@ -41,6 +41,11 @@ void DCsr::upload(const HostCsr &h, bool f64, bool f32) {
         XCUDA(cudaStreamSynchronize(s));
     }
     XCUDA(cudaStreamSynchronize(s));
+    // shifted-row run plan for large square operators whose rows mostly form
+    // runs (stencil operators); irregular operators keep only the CSR arrays
+    runs.clear();
+    const int R = xk::get_spmv_run_rows();
+    if (R > 0 && n >= 4096) runs.build(h, R, f64, f32, 0.5);
 }
 
 void Matrix::ensure32() {
@@ -49,6 +54,7 @@ void Matrix::ensure32() {
     d.v32.alloc(sizeof(float) * std::max<i64>(d.nnz, 1));
     if (d.nnz)
         XCUDA(cudaMemcpy(d.v32.p, f.data(), sizeof(float) * d.nnz, cudaMemcpyHostToDevice));
+    d.runs.add_values(h, Prec::F32);
     has32 = true;
 }
 
@@ -529,7 +535,7 @@ struct HSGS : Solver {
     }
     bool residual_check(DVec &x, const DVec &b, bool initial) {
         cudaStream_t s = ctx().stream;
-        xk::spmv(prec, nv, x.n, op.A->rpp(), op.A->cip(), op.A->val(prec), x.p(), r.p(), 2, b.p(), s);
+        op.A->spmv(prec, nv, x.p(), r.p(), 2, b.p(), s);
         double *d = part.as<double>();
         DBuf out(sizeof(double) * nv);
         dot1(r, r, part, out.as<double>(), s);
@@ -696,12 +702,12 @@ struct Chebyshev : Solver {
         const i64 n = x.n;
         const double *C = coef.as<double>();
         const double *one = ones.as<double>();
-        xk::spmv(prec, nv, n, A->rpp(), A->cip(), A->val(prec), x.p(), r.p(), 2, b.p(), s);
+        A->spmv(prec, nv, x.p(), r.p(), 2, b.p(), s);
         xk::blas(prec, nv, n, xk::Op::ROW_SCAL, nullptr, isd, nullptr, nullptr, nullptr, r.p(), s);
         xk::blas(prec, nv, n, xk::Op::AX_Y, C + (size_t)(order - 1) * nv, r.p(), nullptr, nullptr, nullptr, t1.p(), s);
         for (int i = order - 2; i >= 0; --i) {
             xk::blas(prec, nv, n, xk::Op::ROW_SCAL, nullptr, isd, nullptr, nullptr, nullptr, t1.p(), s);
-            xk::spmv(prec, nv, n, A->rpp(), A->cip(), A->val(prec), t1.p(), t2.p(), 0, nullptr, s);
+            A->spmv(prec, nv, t1.p(), t2.p(), 0, nullptr, s);
             xk::blas(prec, nv, n, xk::Op::ROW_SCAL, nullptr, isd, nullptr, nullptr, nullptr, t2.p(), s);
             xk::blas(prec, nv, n, xk::Op::AXPBY_Z, C + (size_t)i * nv, r.p(), one, t2.p(), nullptr, t1.p(), s);
         }
@@ -905,13 +911,13 @@ struct MultiGrid : Solver {
         const DCsr &A = levA(l);
         if (cyc != 1) m.pre->solve(x, b);
         // temp = b - A x
-        xk::spmv(p, nv, x.n, A.rpp(), A.cip(), A.val(p), x.p(), m.tmp.p(), 2, b.p(), s);
+        A.spmv(p, nv, x.p(), m.tmp.p(), 2, b.p(), s);
         // restriction (convert first when the next level is in FP32)
         if (cp != p) {
             xk::convert(p, cp, m.tmp.count(), m.tmp.p(), m.tmp2.p(), s);
-            xk::spmv(cp, nv, m.R.n, m.R.rpp(), m.R.cip(), m.R.val(cp), m.tmp2.p(), m.bH.p(), 0, nullptr, s);
+            m.R.spmv(cp, nv, m.tmp2.p(), m.bH.p(), 0, nullptr, s);
         } else {
-            xk::spmv(cp, nv, m.R.n, m.R.rpp(), m.R.cip(), m.R.val(cp), m.tmp.p(), m.bH.p(), 0, nullptr, s);
+            m.R.spmv(cp, nv, m.tmp.p(), m.bH.p(), 0, nullptr, s);
         }
         xk::fill(cp, m.xH.count(), 0.0, m.xH.p(), s);
         if (l + 1 == (int)lv.size() - 1) {
@@ -923,7 +929,7 @@ struct MultiGrid : Solver {
         }
         // prolongation
         if (cp != p) {
-            xk::spmv(cp, nv, m.P.n, m.P.rpp(), m.P.cip(), m.P.val(cp), m.xH.p(), m.tmp2.p(), 0, nullptr, s);
+            m.P.spmv(cp, nv, m.xH.p(), m.tmp2.p(), 0, nullptr, s);
             xk::convert(cp, p, m.tmp2.count(), m.tmp2.p(), m.tmp.p(), s);
             if (!ones.p) {
                 std::vector<double> o(nv, 1.0);
@@ -932,7 +938,7 @@ struct MultiGrid : Solver {
             }
             xk::blas(p, nv, x.n, xk::Op::AXPBY_Z, ones.as<double>(), m.tmp.p(), ones.as<double>(), x.p(), nullptr, x.p(), s);
         } else {
-            xk::spmv(p, nv, m.P.n, m.P.rpp(), m.P.cip(), m.P.val(p), m.xH.p(), x.p(), 1, nullptr, s);
+            m.P.spmv(p, nv, m.xH.p(), x.p(), 1, nullptr, s);
         }
         m.post->solve(x, b);
     }
@@ -940,7 +946,7 @@ struct MultiGrid : Solver {
     bool residual_check(DVec &x, const DVec &b, bool initial) {
         cudaStream_t s = ctx().stream;
         const DCsr &A = levA(0);
-        xk::spmv(prec, nv, x.n, A.rpp(), A.cip(), A.val(prec), x.p(), r.p(), 2, b.p(), s);
+        A.spmv(prec, nv, x.p(), r.p(), 2, b.p(), s);
         DBuf out(sizeof(double) * nv);
         dot1(r, r, part, out.as<double>(), s);
         XCUDA(cudaMemcpyAsync(hres.h, out.p, sizeof(double) * nv, cudaMemcpyDeviceToHost, s));
@@ -1021,7 +1027,7 @@ struct Krylov : Solver {
 
     void spmv(const DVec &x, DVec &y, cudaStream_t st) {
         const DCsr &a = dA();
-        xk::spmv(prec, nv, x.n, a.rpp(), a.cip(), a.val(prec), x.p(), y.p(), 0, nullptr, st);
+        a.spmv(prec, nv, x.p(), y.p(), 0, nullptr, st);
     }
 
     void solve(DVec &x, const DVec &b) override {
@@ -1037,7 +1043,7 @@ struct Krylov : Solver {
             XCUDA(cudaMemcpyAsync(S(ICONV), one.data(), sizeof(double) * nv, cudaMemcpyHostToDevice, st));
         }
         // r0 = b - A x; rho = (r0, r0)
-        xk::spmv(prec, nv, n, a.rpp(), a.cip(), a.val(prec), x.p(), r0.p(), 2, b.p(), st);
+        a.spmv(prec, nv, x.p(), r0.p(), 2, b.p(), st);
         dot1(r0, r0, part, S(RHO), st);
         read_res(RHO, st);
         conv.res0.assign(hres.h, hres.h + nv);
@@ -1111,7 +1117,7 @@ struct Krylov : Solver {
             XCUDA(cudaMemcpyAsync(S(ICONV), one.data(), sizeof(double) * nv, cudaMemcpyHostToDevice, st));
         }
         // 1-2: r0 = b - A x; rho = (r0, r0)
-        xk::spmv(prec, nv, n, a.rpp(), a.cip(), a.val(prec), x.p(), r0.p(), 2, b.p(), st);
+        a.spmv(prec, nv, x.p(), r0.p(), 2, b.p(), st);
         dot1(r0, r0, part, S(RHO), st);
         read_res(RHO, st);
         conv.res0.assign(hres.h, hres.h + nv);
@@ -1186,7 +1192,7 @@ struct IterRefine : Solver {
     bool residual_check(DVec &x, const DVec &b, bool initial) {
         cudaStream_t s = ctx().stream;
         const DCsr &a = A->d;
-        xk::spmv(Prec::F64, nv, x.n, a.rpp(), a.cip(), a.val(Prec::F64), x.p(), r.p(), 2, b.p(), s);
+        a.spmv(Prec::F64, nv, x.p(), r.p(), 2, b.p(), s);
         DBuf out(sizeof(double) * nv);
         dot1(r, r, part, out.as<double>(), s);
         XCUDA(cudaMemcpyAsync(hres.h, out.p, sizeof(double) * nv, cudaMemcpyDeviceToHost, s));

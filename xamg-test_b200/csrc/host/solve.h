@@ -34,10 +34,32 @@ struct DVec {
     i64 count() const { return n * nv; }
 };
 
+// Shifted-row run plan of a square operator (xk::spmv_runs): chunks of up to
+// R = 8 consecutive rows whose column indices are the first row's shifted by
+// the row offset, with the values reordered entry-major per chunk.
+struct RunPlan {
+    int R = 0;
+    i64 nchunks = 0, ntiles = 0, nseg = 0;
+    double coverage = 0.0;     // fraction of the entries that lie in chunks of R rows
+    std::vector<int> hchunks;  // {r0, cnt, m, segments} per chunk (host)
+    std::vector<i64> hvoff;    // per tile of four chunks: first value slot (host, ntiles + 1)
+    DBuf chunks, toff, sg, v64, v32;
+    // Detect the chunks of h; keeps the plan (FP64 and/or FP32 values) when at
+    // least min_cov of the entries lie in chunks of R rows, else clears it.
+    bool build(const HostCsr &h, int R_, bool f64, bool f32, double min_cov);
+    void add_values(const HostCsr &h, Prec p);  // values of another precision
+    bool has(Prec p) const { return nchunks > 0 && (p == Prec::F64 ? v64.p != nullptr : v32.p != nullptr); }
+    void clear();
+};
+
 struct DCsr {
     i64 n = 0, ncols = 0, nnz = 0;
     DBuf rp, ci, v64, v32;
+    RunPlan runs;
     void upload(const HostCsr &h, bool f64, bool f32);
+    // y = A x (mode 0), y += A x (1), y = b - A x (2): the run kernel when this
+    // operator has a plan in precision p and the shape suits it, else xk::spmv
+    void spmv(Prec p, int nv, const void *x, void *y, int mode, const void *b, cudaStream_t s) const;
     const void *val(Prec p) const {
         if (p == Prec::F64) { XCHECK(v64.p || nnz == 0, "FP64 values not resident"); return v64.p; }
         XCHECK(v32.p || nnz == 0, "FP32 values not resident");

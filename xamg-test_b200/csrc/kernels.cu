@@ -311,6 +311,9 @@ __global__ void __launch_bounds__(256, LOOP == 1 ? 6 : 1) k_spmv_tile(i64 n, con
 // else 0).
 static int g_spmv_variant = -1;
 void set_spmv_variant(int v) { g_spmv_variant = v; }
+static int g_run_rows = 8;
+void set_spmv_run_rows(int r) { g_run_rows = r == 8 ? 8 : 0; }
+int get_spmv_run_rows() { return g_run_rows; }
 
 // kernels launched by this library (all launchers count here)
 static std::atomic<long long> g_launches{0};
@@ -338,7 +341,7 @@ static void spmv_t(i64 n, const int *rp, const int *ci, const T *va, const T *x,
     i64 ntiles = (n + RPB - 1) / RPB;
     // default: the tile-staged kernel when a row spans at least 4 threads (its
     // tile of RPB rows then fits the shared-memory stage), else batches of 4
-    int var = g_spmv_variant >= 0 ? g_spmv_variant : (Shape<T, NV>::TPR >= 4 ? 6 : 0);
+    int var = (g_spmv_variant >= 0 && g_spmv_variant != 7) ? g_spmv_variant : (Shape<T, NV>::TPR >= 4 ? 6 : 0);
     if (var >= 3 && var <= 6) {
         unsigned g = (unsigned)ntiles;
 #define L(GB, LOOP)                                                                                \
@@ -374,6 +377,188 @@ void spmv(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val, 
 #undef F
     } else {
 #define F(NV) spmv_t<float, NV>(n, rp, ci, (const float *)val, (const float *)x, (float *)y, mode, (const float *)b, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    }
+}
+
+// ---------------------------------------------------------------- shifted-row runs
+// A chunk is up to R = 8 consecutive rows r0 .. r0+cnt-1 with the same entry
+// count m whose column indices are those of row r0 shifted by the row offset,
+// ci(r0+q, e) = ci(r0, e) + q (the interior rows of a stencil operator).  The
+// first row's column list is cut into segments of at most 3 consecutive
+// columns, stored as c0 | len << 30; row q's entry j of a segment has column
+// c0 + q + j, so the chunk's rows gather the len + cnt - 1 x rows c0 ..
+// c0+len+cnt-2 once, into registers, instead of len * cnt times.  TPR threads
+// (NV/TPR elements each) evaluate one chunk.  Chunks are grouped four
+// to a tile; tile t stores its segments segment-major, sg[toff[t].y + 4s +
+// slot], and its values entry-major, vt[(toff[t].x + 4e + slot) * R + q], so
+// the loads of one entry by the chunks of a warp fall in one or two 128-byte
+// lines.  A CTA of 128 threads first copies the segments and values of its
+// chunks (one contiguous range of each) into shared memory with 16-byte
+// cp.async; five CTAs share an SM (96 registers a thread), so one CTA's copy
+// overlaps the others' gathers.  Each
+// row's FMA chain runs over its entries in CSR order starting from 0 (or y),
+// the order of every other SpMV kernel here.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <class T, int R, bool SMEM>
+__device__ __forceinline__ void ld_vals(const T *p, T (&a)[R]) {
+    constexpr int PER = 16 / (int)sizeof(T), NB = R / PER;
+    typedef typename VT<T, PER>::type W;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+        W w = SMEM ? reinterpret_cast<const W *>(p)[k] : __ldcs(reinterpret_cast<const W *>(p) + k);
+        memcpy(a + k * PER, &w, sizeof(W));
+    }
+}
+
+constexpr int RUN_ROWS = 8, RUN_SEG = 3;
+// chunks per CTA of NT threads and the value slots a CTA can stage (32
+// entries per chunk on average)
+template <class T, int NV, int NT> struct RunShape {
+    static constexpr int TPR = Shape<T, NV>::TPR, CPC = NT / TPR, TPC = CPC / 4, SLOTS = TPC * 128;
+    static constexpr int SMEM_BYTES = SLOTS * (4 + RUN_ROWS * (int)sizeof(T));
+};
+
+template <class T, int NV, int MODE, bool SMEM>
+__device__ __forceinline__ void run_rows(const int4 cd, int smax, const int *sg, const T *val, const T *xb,
+                                         T *__restrict__ y, const T *__restrict__ b, int l) {
+    constexpr int V = Shape<T, NV>::V, R = RUN_ROWS, NX = RUN_SEG + R - 1;
+    T acc[R][V];
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[q][v] = T(0);
+    if (MODE == 1) {
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+            if (q < cd.y) ld<T, V>(y + ((i64)cd.x + q) * NV + l * V, acc[q]);
+    }
+    auto seg = [&](int s) { return s < cd.w ? (SMEM ? sg[4 * s] : __ldcs(sg + 4 * s)) : 0; };
+    int e = 0;
+    int sc = seg(0);
+    for (int s = 0; s < smax; ++s) {
+        const int c0 = sc & 0x3fffffff, len = (int)((unsigned)sc >> 30);
+        const int nx = len + cd.y - 1;
+        T X[NX][V];
+#pragma unroll
+        for (int k = 0; k < NX; ++k)
+            if (k < nx) ld<T, V>(xb + ((i64)c0 + k) * NV, X[k]);
+        sc = seg(s + 1);
+#pragma unroll
+        for (int j = 0; j < RUN_SEG; ++j) {
+            if (j < len) {
+                T a[R];
+                ld_vals<T, R, SMEM>(val + (i64)4 * (e + j) * R, a);
+#pragma unroll
+                for (int q = 0; q < R; ++q)
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[q][v] = fma(a[q], X[q + j][v], acc[q][v]);
+            }
+        }
+        e += len;
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+        if (q >= cd.y) break;
+        const i64 row = (i64)cd.x + q;
+        if (MODE == 2) {
+            T bb[V];
+            ld<T, V>(b + row * NV + l * V, bb);
+#pragma unroll
+            for (int v = 0; v < V; ++v)
+                acc[q][v] = add_rn<T>(mul_rn<T>(T(1), bb[v]), mul_rn<T>(T(-1), acc[q][v]));
+        }
+        st<T, V>(y + row * NV + l * V, acc[q]);
+    }
+}
+
+constexpr int RUN_NT = 128;
+template <class T, int NV, int MODE, int NT>
+__global__ void __launch_bounds__(NT, 5) k_spmv_runs(i64 nchunks, i64 ntiles, const int4 *__restrict__ chunks,
+                                                      const longlong2 *__restrict__ toff,
+                                                      const int *__restrict__ sg,
+                                                      const T *__restrict__ vt,
+                                                      const T *__restrict__ x, T *__restrict__ y,
+                                                      const T *__restrict__ b) {
+    typedef RunShape<T, NV, NT> RS;
+    constexpr int V = Shape<T, NV>::V, TPR = RS::TPR, CPC = RS::CPC, TPC = RS::TPC, SLOTS = RS::SLOTS;
+    static_assert(TPR >= 4 && (RUN_ROWS * (int)sizeof(T)) % 16 == 0, "run kernel shape");
+    extern __shared__ __align__(16) unsigned char run_smem[];
+    int *s_sg = reinterpret_cast<int *>(run_smem);
+    T *s_vt = reinterpret_cast<T *>(run_smem + SLOTS * 4);
+    const i64 t0 = (i64)blockIdx.x * TPC, t1 = min(ntiles, t0 + TPC);
+    const longlong2 o0 = __ldg(toff + t0), o1 = __ldg(toff + t1);
+    const i64 ne = o1.x - o0.x, nsg = o1.y - o0.y;
+    const bool staged = ne <= SLOTS;  // segments never outnumber entries
+    if (staged) {
+        const int np = (int)(nsg / 4), nvb = (int)(ne * RUN_ROWS * (int)sizeof(T) / 16);
+        for (int k = threadIdx.x; k < np; k += NT) cp_async16(s_sg + 4 * k, sg + o0.y + 4 * k);
+        const char *gv = reinterpret_cast<const char *>(vt + o0.x * RUN_ROWS);
+        for (int k = threadIdx.x; k < nvb; k += NT)
+            cp_async16(reinterpret_cast<char *>(s_vt) + 16 * k, gv + 16 * k);
+        cp_async_wait_all();
+    }
+    __syncthreads();
+    const i64 gid = (i64)blockIdx.x * CPC + threadIdx.x / TPR;
+    const int l = threadIdx.x % TPR;
+    const bool live = gid < nchunks;
+    const int4 cd = live ? __ldg(chunks + gid) : make_int4(0, 0, 0, 0);  // r0, cnt, m, segments
+    const int smax = __reduce_max_sync(0xffffffffu, cd.w);
+    const longlong2 ot = live ? __ldg(toff + (gid >> 2)) : o0;
+    const int slot = (int)(gid & 3);
+    const i64 le = ot.x - o0.x + slot, ls = ot.y - o0.y + slot;  // CTA-local first value / segment slot
+    const T *xb = x + l * V;
+    if (staged) run_rows<T, NV, MODE, true>(cd, smax, s_sg + ls, s_vt + le * RUN_ROWS, xb, y, b, l);
+    else run_rows<T, NV, MODE, false>(cd, smax, sg + o0.y + ls, vt + (o0.x + le) * RUN_ROWS, xb, y, b, l);
+}
+
+bool spmv_runs_supported(Prec p, int nv) {
+    return p == Prec::F64 ? (nv == 8 || nv == 16 || nv == 32) : (nv == 16 || nv == 32);
+}
+
+template <class T, int NV, int NT>
+static void spmv_runs_p(i64 nchunks, i64 ntiles, const int4 *chunks, const longlong2 *toff, const int *sg,
+                        const T *vt, const T *x, T *y, int mode, const T *b, cudaStream_t s) {
+    typedef RunShape<T, NV, NT> RS;
+    constexpr int SM = RS::SMEM_BYTES;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_spmv_runs<T, NV, 0, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+        cudaFuncSetAttribute(k_spmv_runs<T, NV, 1, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+        cudaFuncSetAttribute(k_spmv_runs<T, NV, 2, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+        attr = true;
+    }
+    unsigned g = (unsigned)((ntiles + RS::TPC - 1) / RS::TPC);
+    if (mode == 0) k_spmv_runs<T, NV, 0, NT><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
+    else if (mode == 1) k_spmv_runs<T, NV, 1, NT><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
+    else k_spmv_runs<T, NV, 2, NT><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
+}
+
+template <class T, int NV>
+static void spmv_runs_t(i64 nchunks, i64 ntiles, const int4 *chunks, const longlong2 *toff, const int *sg,
+                        const T *vt, const T *x, T *y, int mode, const T *b, cudaStream_t s) {
+    if constexpr (NV >= 8 && NV * sizeof(T) >= 64) {
+        if (nchunks <= 0) return;
+        note_launch();
+        spmv_runs_p<T, NV, RUN_NT>(nchunks, ntiles, chunks, toff, sg, vt, x, y, mode, b, s);
+    }
+}
+
+void spmv_runs(Prec p, int nv, i64 nchunks, i64 ntiles, const int4 *chunks, const longlong2 *toff, const int *sg,
+               const void *vt, const void *x, void *y, int mode, const void *b, cudaStream_t s) {
+    if (p == Prec::F64) {
+#define F(NV) spmv_runs_t<double, NV>(nchunks, ntiles, chunks, toff, sg, (const double *)vt, (const double *)x, (double *)y, mode, (const double *)b, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    } else {
+#define F(NV) spmv_runs_t<float, NV>(nchunks, ntiles, chunks, toff, sg, (const float *)vt, (const float *)x, (float *)y, mode, (const float *)b, s)
         NV_DISPATCH(nv, F)
 #undef F
     }

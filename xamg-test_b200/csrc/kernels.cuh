@@ -32,8 +32,27 @@ void spmv(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val, 
 // gather batches of 4, 8; 5, 6 = tile-staged with a plain row loop unrolled 4,
 // 8 times; 10 + k = streaming kernel walking k tiles per CTA; -1 = default
 // (6 when NV*sizeof(T) >= 64 bytes, else 0).  All give identical results.
+// Operators with a shifted-row run plan use the run kernel under -1 and 7
+// (7 elsewhere = the default).
 void set_spmv_variant(int v);
 int get_spmv_variant();
+// Rows per chunk of the run plans built when operators are uploaded (8; 0 =
+// build no run plans).
+void set_spmv_run_rows(int r);
+int get_spmv_run_rows();
+
+// ---- shifted-row runs (stencil-structured operators) ------------------------
+// Chunks of up to 8 consecutive rows whose column indices are the first row's
+// shifted by the row offset; chunks[c] = {r0, cnt, m, segments}, four chunks
+// per tile (ntiles tiles; toff has ntiles + 1 entries {value offset, segment
+// offset}, both multiples of 4).  Tile t's segments (runs of at most 3
+// consecutive columns of each chunk's first row, c0 | len << 30) at
+// sg[toff[t].y + 4s + slot], its values at vt[(toff[t].x + 4e + slot) * 8 + q].
+// Same modes and the same results, bit for bit, as spmv().  FP64 nv 8, 16, 32
+// and FP32 nv 16, 32.
+bool spmv_runs_supported(Prec p, int nv);
+void spmv_runs(Prec p, int nv, i64 nchunks, i64 ntiles, const int4 *chunks, const longlong2 *toff, const int *sg,
+               const void *vt, const void *x, void *y, int mode, const void *b, cudaStream_t s);
 
 // ---- Gauss-Seidel sweeps ----------------------------------------------------
 // One wavefront level: rows[0..cnt) are independent and updated in place.

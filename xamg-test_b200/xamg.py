@@ -111,6 +111,11 @@ def lib():
             "XAMG_b200_gs_levels_host": (C.c_int, [i64, P, P, i64, P, P, P]),
             "xamg_csr_spmv": (C.c_int, [C.c_int, C.c_int, i64, P, P, P, P, P, C.c_int, P, P]),
             "xamg_spmv_set_variant": (C.c_int, [C.c_int]),
+            "xamg_spmv_set_run_rows": (C.c_int, [C.c_int]),
+            "xamg_spmv_runs_plan_create": (P, [i64, P, P, P, C.c_int, C.c_int]),
+            "xamg_spmv_runs_plan_info": (C.c_int, [P, P, P, P, P]),
+            "xamg_spmv_runs": (C.c_int, [P, C.c_int, C.c_int, P, P, C.c_int, P, P]),
+            "xamg_spmv_runs_plan_destroy": (C.c_int, [P]),
             "xamg_gs_plan_create": (P, [i64, P, P, i64, C.c_int]),
             "xamg_gs_plan_levels": (C.c_int, [P, P, P, P]),
             "xamg_gs_plan_set_values": (C.c_int, [P, P, C.c_int]),
