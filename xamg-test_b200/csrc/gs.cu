@@ -56,6 +56,13 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
         : "memory");
 }
 
+// 16-byte global -> shared copy through L2 only (other CTAs' and this CTA's
+// earlier stores are visible to it), tracked per thread
+__device__ __forceinline__ void cp_async16_cg(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parity) {
     unsigned ok;
     asm volatile(
@@ -286,7 +293,18 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
         // into shared memory in one parallel round trip (xs: eg entries x NV)
         const bool gath = !XS && ok && staged && (dc.e1 - dc.e0) <= eg;
         if (!XS) {
-            if (gath) {
+            if (gath && V * (int)sizeof(T) == 16) {
+                // 16-byte pieces: every piece is copied by cp.async straight
+                // into shared memory, all in flight together (one L2 round
+                // trip, no registers held); padding entries (column -1) are
+                // skipped and never read
+                const int tot = (dc.e1 - dc.e0) * TPR;
+                for (int w = tid; w < tot; w += 256) {
+                    const int c = s_ci[q][w / TPR];
+                    if (c >= 0) cp_async16_cg(xs + (i64)w * V, x + (i64)c * NV + (w % TPR) * V);
+                }
+                cp_async_wait_all();
+            } else if (gath) {
                 // every thread issues up to GU independent loads before it
                 // stores any, so the gather costs one or two L2 round trips
                 constexpr int GU = 8;

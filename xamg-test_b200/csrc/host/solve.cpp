@@ -189,6 +189,25 @@ void GsPlan::build(const HostCsr &A, i64 brows_, GsMode mode_) {
 // and entry ranges handed to one CTA start on 16-byte boundaries and span
 // multiples of 16 bytes (the TMA bulk-copy rule).  One descriptor {r0, r1, e0,
 // e1} per (level, CTA) tells each CTA what to stage.
+void GsPlan::build_offblock(const HostCsr &A, Prec p) {
+    if (brows == 0) return;
+    HostCsr off;
+    off.n = A.n;
+    off.ncols = A.ncols;
+    off.rp.assign((size_t)A.n + 1, 0);
+    for (i64 i = 0; i < A.n; ++i) {
+        const i64 blk = i / brows;
+        for (int j = A.rp[i]; j < A.rp[i + 1]; ++j)
+            if (A.ci[j] / brows != blk) {
+                off.ci.push_back(A.ci[j]);
+                off.v.push_back(A.v[j]);
+            }
+        off.rp[i + 1] = (int)off.ci.size();
+    }
+    aprec = p;
+    aoff.upload(off, p == Prec::F64, p == Prec::F32);
+}
+
 void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
     if (mode == GsMode::LEVELS) return;
     lprec = p;
@@ -526,7 +545,12 @@ struct HSGS : Solver {
         cudaStream_t s = ctx().stream;
         const void *tp = b.p();
         if (t.n) {
-            xk::offblock_resid(prec, nv, x.n, op.A->rpp(), op.A->cip(), op.A->val(prec), b.p(), x.p(), t.p(), op.gs->brows, s);
+            // t = 1*b + (-1)*(A_off x), the chain over the off-block entries in CSR order
+            if (op.gs->aoff.n == x.n && op.gs->aprec == prec)
+                op.gs->aoff.spmv(prec, nv, x.p(), t.p(), 2, b.p(), s);
+            else
+                xk::offblock_resid(prec, nv, x.n, op.A->rpp(), op.A->cip(), op.A->val(prec), b.p(), x.p(), t.p(),
+                                   op.gs->brows, s);
             tp = t.p();
         }
         const DCsr &A = *op.A;
@@ -861,6 +885,7 @@ struct MultiGrid : Solver {
             } else {
                 g.build(hA, br, md);
                 g.build_lcsr(hA, m.prec);
+                g.build_offblock(hA, m.prec);
                 op.gs = &g;
             }
             auto h = std::unique_ptr<HSGS>(new HSGS());
@@ -1289,6 +1314,7 @@ static std::unique_ptr<Solver> make_solver(const GlobalParams &gp, const std::st
             i64 br = hsgs_block_rows(pl, A.h.n);
             o->gs.build(A.h, br, gs_mode_from(pl.has("gs_schedule") ? pl.get_string("gs_schedule") : "auto", br, A.h.n));
             o->gs.build_lcsr(A.h, prec);
+            o->gs.build_offblock(A.h, prec);
             op.gs = &o->gs;
             auto h = std::unique_ptr<HSGS>(new HSGS());
             h->role = role; h->method = m; h->prm = pl; h->nv = nv; h->prec = prec;

@@ -102,9 +102,15 @@ struct GsPlan {
     } lc[2];
     bool has_lcsr = false;
     Prec lprec = Prec::F64;
+    // hybrid plans: the entries of A outside each row's block, in CSR order
+    // (values in precision aprec), so that the right-hand side of the block
+    // sweeps, t = b - A_off x, is one SpMV of this operator in mode 2
+    DCsr aoff;
+    Prec aprec = Prec::F64;
     void build(const HostCsr &A, i64 brows_, GsMode mode_);
     // store the level-ordered matrix copies in precision p (values from A)
     void build_lcsr(const HostCsr &A, Prec p);
+    void build_offblock(const HostCsr &A, Prec p);
     // forward (or backward) sweep; in BLOCKS mode the forward call runs both
     // sweeps and the backward call does nothing
     void sweep(Prec p, int nv, const int *rp, const int *ci, const void *val, const void *invd,
