@@ -536,6 +536,62 @@ int pbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
     return it;
 }
 
+// PCG, pcg.inl:48-160 (mg == nullptr: identity preconditioner, z = copy of r).
+template <class T>
+int pcg(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iters, Conv &cv, Hist &hist) {
+    i64 n = A.n;
+    size_t sz = (size_t)n * nv;
+    const T *av = vals<T>(A);
+    std::vector<T> r(sz), z(sz), p(sz), Ap(sz);
+    std::vector<double> s1(nv), s2(nv), s3(nv), alpha(nv), beta(nv), res(nv), iconv(nv, 1.0);
+    auto precond = [&](std::vector<T> &out, const std::vector<T> &in) {
+        if (mg) mg_apply<T>(*mg, out.data(), in.data(), nv);
+        else out = in;
+    };
+    auto at = [nv](size_t q) { return (int)(q % (size_t)nv); };
+    cv.nv = nv;
+    cv.res0.assign(nv, 0);
+    cv.res.assign(nv, 0);
+    cv.status.assign(nv, 0);
+    // r = b - A x, res = (r, r)  (solver.h:183-190)
+    spmv<T>(n, A.rp.data(), A.ci.data(), av, x, r.data(), nv, 0);
+    for (size_t q = 0; q < sz; ++q) r[q] = T(1) * b[q] + T(-1) * r[q];
+    dot_canonical<T, double>(n, nv, r.data(), r.data(), res.data());
+    for (int k = 0; k < nv; ++k) cv.res0[k] = res[k];
+    cv.update(res.data());
+    hist.push(cv.res, nv);
+    if (cv.check()) return 0;
+    for (int k = 0; k < nv; ++k) if (cv.status[k]) iconv[k] = 0;
+    precond(z, r);
+    p = z;
+    int it = 0;
+    for (bool last = false; !last;) {
+        it++;
+        if (it >= max_iters) last = true;
+        spmv<T>(n, A.rp.data(), A.ci.data(), av, p.data(), Ap.data(), nv, 0);
+        dot_canonical<T, double>(n, nv, r.data(), z.data(), s1.data());
+        dot_canonical<T, double>(n, nv, p.data(), Ap.data(), s2.data());
+        for (int k = 0; k < nv; ++k) alpha[k] = s1[k] / s2[k];
+        for (size_t q = 0; q < sz; ++q) {  // x = (iconv*alpha)*p + 1*x
+            double ac = iconv[at(q)] * alpha[at(q)];
+            x[q] = (T)(ac * (double)p[q] + 1.0 * (double)x[q]);
+        }
+        for (size_t q = 0; q < sz; ++q)  // r = (-alpha)*Ap + 1*r
+            r[q] = (T)((-1.0 * alpha[at(q)]) * (double)Ap[q] + 1.0 * (double)r[q]);
+        precond(z, r);
+        dot_canonical<T, double>(n, nv, r.data(), z.data(), s3.data());
+        for (int k = 0; k < nv; ++k) beta[k] = s3[k] / s1[k];
+        for (size_t q = 0; q < sz; ++q)  // p = 1*z + beta*p
+            p[q] = (T)(1.0 * (double)z[q] + beta[at(q)] * (double)p[q]);
+        dot_canonical<T, double>(n, nv, r.data(), r.data(), res.data());
+        cv.update(res.data());
+        hist.push(cv.res, nv);
+        if (cv.check()) return it;
+        for (int k = 0; k < nv; ++k) if (cv.status[k]) iconv[k] = 0;
+    }
+    return it;
+}
+
 // RBiCGStab, rbicgstab.inl:48-225 (the reference always has a preconditioner;
 // mg == nullptr applies the identity, z = copy of the right-hand side).
 // Step numbers are the reference's comments.
@@ -826,6 +882,25 @@ int orc_pbicgstab_d(i64 n, const int *rp, const int *ci, const double *v, void *
     cv.rel_tol = rel_tol;
     Hist H{hist, hist_cap};
     int it = pbicgstab<double>(A, (MG *)mg, b, x, nv, max_iters, cv, H);
+    for (int k = 0; k < nv; ++k) {
+        status[k] = cv.status[k];
+        res0[k] = cv.res0[k];
+    }
+    return it;
+}
+
+// FP64 PCG; arguments and outputs as orc_pbicgstab_d (mg == NULL: identity
+// preconditioner).
+int orc_pcg_d(i64 n, const int *rp, const int *ci, const double *v, void *mg, const double *b, double *x,
+              int nv, int max_iters, double abs_tol, double rel_tol, double *hist, int hist_cap, int *status,
+              double *res0) {
+    Csr A;
+    fill(A, n, n, rp, ci, v);
+    Conv cv;
+    cv.abs_tol = abs_tol;
+    cv.rel_tol = rel_tol;
+    Hist H{hist, hist_cap};
+    int it = pcg<double>(A, (MG *)mg, b, x, nv, max_iters, cv, H);
     for (int k = 0; k < nv; ++k) {
         status[k] = cv.status[k];
         res0[k] = cv.res0[k];

@@ -126,6 +126,24 @@ def test_rbicgstab_parity(gpu, method, with_mg, nv):
     np.testing.assert_allclose(X, xo, rtol=1e-12, atol=1e-14 * np.abs(xo).max())
 
 
+@pytest.mark.parametrize("with_mg,nv", [(True, 4), (False, 1), (True, 16)])
+def test_pcg_parity(gpu, with_mg, nv):
+    """PCG (pcg.inl) on the symmetric 7-point operator: identical iterations,
+    residual history and solution to the oracle's restatement."""
+    csr = xamg.CsrMatrix.cube(24, 24, 24, 0)
+    rp, ci, v = csr.arrays()
+    rng = np.random.default_rng(5 + nv)
+    B = rng.uniform(-1, 1, (csr.nrows, nv))
+    spec = util.amg_params(precond_mg=with_mg, max_levels=6, max_iters=1000)
+    spec["solver"]["method"] = "PCG"
+    s, X, keep = solve_api(csr, spec, B)
+    mg = oracle_mg(s, spec) if with_mg else None
+    xo, it, hist, st, r0 = orc.pcg(rp, ci, v, B, np.zeros_like(B), mg, 1000, 0.0, 1e-8)
+    assert s.iters()[0] == it and it > 0 and all(s.converged())
+    assert_same_history(s.history(), hist)
+    np.testing.assert_allclose(X, xo, rtol=1e-12, atol=1e-14 * np.abs(xo).max())
+
+
 def test_recorded_2d_problem_through_api(gpu):
     rec = json.load(open(os.path.join(GOLD, "recorded.json")))
     rp, ci, v, b, u = util.gen2d(100)

@@ -88,6 +88,29 @@ def test_rbicgstab_restatement_solves_recorded_problem(with_mg):
         assert abs(it - itp) <= 2
 
 
+@pytest.mark.parametrize("with_mg", [True, False])
+def test_pcg_restatement_solves_recorded_problem(with_mg):
+    # pcg.inl: with AMG on the recorded 2-D problem, without a preconditioner
+    # on the symmetric positive definite 7-point operator
+    if with_mg:
+        rp, ci, v, b, u = util.gen2d(100)
+        B = b.reshape(-1, 1)
+    else:
+        rp, ci, v = xamg.CsrMatrix.cube(12, 12, 12, 0).arrays()
+        B = np.random.default_rng(9).uniform(-1, 1, (len(rp) - 1, 1))
+    mg = None
+    if with_mg:
+        csr = xamg.CsrMatrix.from_arrays(rp, ci, v)
+        mg = orc.MG(xamg.amg_host(csr, xamg.Params(util.amg_params(max_levels=25))))
+    x, it, hist, st, r0 = orc.pcg(rp, ci, v, B, np.zeros_like(B), mg=mg, max_iters=2000, rel_tol=1e-8)
+    assert st[0] == 1 and it > 0 and hist.shape == (it + 1, 1)
+    true = B - orc.spmv(rp, ci, v, x, 1)
+    # the recurrence residual tracks the true one to rounding
+    assert np.sqrt(orc.dot(true, true)[0]) <= 1.05e-8 * np.sqrt(r0[0])
+    if with_mg:
+        assert abs(np.linalg.norm(x) - REC["X_norm"]) / REC["X_norm"] < 1e-7
+
+
 def test_dot_orders_agree_to_rounding():
     rng = np.random.default_rng(1)
     for n, nv in [(1, 1), (255, 2), (257, 4), (70000, 16), (1000, 32)]:

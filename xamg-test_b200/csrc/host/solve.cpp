@@ -1015,6 +1015,7 @@ struct Krylov : Solver {
     std::unique_ptr<Solver> M;
     bool precond = false;
     bool reordered = false;  // RBiCGStab
+    bool cg = false;         // PCG
     DVec r0, r, p, v, s, t, p_, s_;
     DBuf part, sc;
     Pinned hres;
@@ -1027,7 +1028,7 @@ struct Krylov : Solver {
         conv.init(nv);
         conv.prefix = role == "meta_solver" ? "META" : "SOLV";
         for (DVec *q : {&r0, &r, &p, &v, &s, &t}) q->alloc(n, nv, prec);
-        if (precond || reordered) { p_.alloc(n, nv, prec); s_.alloc(n, nv, prec); }
+        if (precond || reordered || cg) { p_.alloc(n, nv, prec); s_.alloc(n, nv, prec); }
         ensure_part(part, n, reordered ? 4 : 3, nv);
         sc.alloc(sizeof(double) * NSC * nv);
         std::vector<double> z(NSC * nv, 0.0);
@@ -1057,6 +1058,7 @@ struct Krylov : Solver {
 
     void solve(DVec &x, const DVec &b) override {
         if (reordered) { solve_reordered(x, b); return; }
+        if (cg) { solve_cg(x, b); return; }
         cudaStream_t st = ctx().stream;
         int max_iters = (int)prm.get_int("max_iters");
         i64 n = x.n;
@@ -1114,6 +1116,65 @@ struct Krylov : Solver {
             dot1(r, r0, part, S(S1), st);
             xk::bicg_beta(nv, S(S1), S(RHO), S(ALPHA), S(OMEGA), S(BETA), S(C1), st);
             xk::blas(prec, nv, n, xk::Op::AXPBYPCZ, S(ONES), r.p(), S(C1), v.p(), S(BETA), p.p(), st);
+        }
+        XCUDA(cudaStreamSynchronize(st));
+    }
+
+    // PCG (pcg.inl:48-160).  The step's two inner products (r,z), (p,Ap) are
+    // one fused launch, and so are (r,z) and (r,r) after the preconditioner;
+    // beta and the new direction are formed after the convergence check
+    // (they do not touch x).
+    void solve_cg(DVec &x, const DVec &b) {
+        cudaStream_t st = ctx().stream;
+        int max_iters = (int)prm.get_int("max_iters");
+        i64 n = x.n;
+        const DCsr &a = dA();
+        DVec &z = p_, &Ap = v;
+        auto axpby = [&](const double *ca, const DVec &xx, const double *cb, const DVec &yy, DVec &zz) {
+            xk::blas(prec, nv, n, xk::Op::AXPBY_Z, ca, xx.p(), cb, yy.p(), nullptr, zz.p(), st);
+        };
+        conv.init(nv);
+        set_rhs_base(conv, b, part);
+        {
+            std::vector<double> one(nv, 1.0);
+            XCUDA(cudaMemcpyAsync(S(ICONV), one.data(), sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+        }
+        // r = b - A x; res = (r, r)
+        a.spmv(prec, nv, x.p(), r.p(), 2, b.p(), st);
+        dot1(r, r, part, S(RES), st);
+        read_res(RES, st);
+        conv.res0.assign(hres.h, hres.h + nv);
+        conv.update(hres.h);
+        conv.record();
+        if (conv.check()) return;
+        set_iconv(st);
+        xk::fill(prec, z.count(), 0.0, z.p(), st);
+        M->solve(z, r);
+        xk::blas(prec, nv, n, xk::Op::COPY, nullptr, z.p(), nullptr, nullptr, nullptr, p.p(), st);
+        for (int it = 1;; ++it) {
+            conv.iters = it;
+            a.spmv(prec, nv, p.p(), Ap.p(), 0, nullptr, st);
+            {
+                const void *Aa[2] = {r.p(), p.p()}, *Bb[2] = {z.p(), Ap.p()};
+                xk::dots(prec, nv, n, 2, Aa, Bb, part.as<double>(), S(S1), st);
+            }
+            xk::pcg_alpha(nv, S(S1), S(S2), S(ICONV), S(ALPHA), S(AC), S(NALPHA), st);
+            axpby(S(AC), p, S(ONES), x, x);
+            axpby(S(NALPHA), Ap, S(ONES), r, r);
+            xk::fill(prec, z.count(), 0.0, z.p(), st);
+            M->solve(z, r);
+            {
+                const void *Aa[2] = {r.p(), r.p()}, *Bb[2] = {z.p(), r.p()};
+                xk::dots(prec, nv, n, 2, Aa, Bb, part.as<double>(), S(S3), st);  // S3 = (r,z), S4 = (r,r)
+            }
+            read_res(S4, st);
+            conv.update(hres.h);
+            conv.record();
+            if (conv.check()) break;
+            if (it >= max_iters) break;
+            set_iconv(st);
+            xk::bicg_alpha(nv, S(S3), S(S1), S(BETA), st);  // beta = (r,z)_new / (r,z)_old
+            axpby(S(ONES), z, S(BETA), p, p);
         }
         XCUDA(cudaStreamSynchronize(st));
     }
@@ -1266,11 +1327,12 @@ static std::unique_ptr<Solver> make_solver(const GlobalParams &gp, const std::st
     i64 n = A.h.n;
     if (prec == Prec::F32) A.ensure32();
     if (m == "BiCGStab" || m == "MergedBiCGStab" || m == "PBiCGStab" || m == "MergedPBiCGStab" ||
-        m == "RBiCGStab" || m == "MergedRBiCGStab") {
+        m == "RBiCGStab" || m == "MergedRBiCGStab" || m == "PCG") {
         auto k = std::unique_ptr<Krylov>(new Krylov());
         k->role = role; k->method = m; k->prm = pl; k->nv = nv; k->prec = prec; k->A = &A;
         k->reordered = (m == "RBiCGStab" || m == "MergedRBiCGStab");
-        k->precond = (m == "PBiCGStab" || m == "MergedPBiCGStab" || k->reordered);
+        k->cg = m == "PCG";
+        k->precond = (m == "PBiCGStab" || m == "MergedPBiCGStab" || k->reordered || k->cg);
         if (k->precond) {
             if (gp.has("preconditioner")) k->M = make_solver(gp, "preconditioner", A, nv, prec);
             else {

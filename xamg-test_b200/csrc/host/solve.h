@@ -2,7 +2,7 @@
 //
 // Class map to the reference (src/solvers/*):
 //   Krylov       <- BiCGStab / PBiCGStab (bicgstab.inl:44-197, pbicgstab.inl:48-207)
-//                   RBiCGStab (rbicgstab.inl:48-225)
+//                   RBiCGStab (rbicgstab.inl:48-225), PCG (pcg.inl:48-160)
 //                   and their Merged* variants (same values, one code path)
 //   MultiGrid    <- MultiGrid (mg.inl:117-331), levels from the host AMG setup
 //   HSGS, Jacobi <- hsgs.inl:31-91, jacobi.inl:31-102

@@ -1191,6 +1191,21 @@ void bicg_beta(int nv, const double *s1, double *rho, const double *alpha, const
     note_launch();
     k_beta<<<sblocks(nv), 128, 0, s>>>(nv, s1, rho, alpha, omega, beta, c1);
 }
+// PCG step length (pcg.inl:125-134): alpha = s1/s2; ac = iconv*alpha; nalpha = -1*alpha
+__global__ void k_pcg_alpha(int nv, const double *s1, const double *s2, const double *iconv, double *alpha,
+                            double *ac, double *nalpha) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nv) return;
+    double a = __ddiv_rn(s1[k], s2[k]);
+    alpha[k] = a;
+    ac[k] = dmul(iconv[k], a);
+    nalpha[k] = dmul(-1.0, a);
+}
+void pcg_alpha(int nv, const double *s1, const double *s2, const double *iconv, double *alpha, double *ac,
+               double *nalpha, cudaStream_t s) {
+    note_launch();
+    k_pcg_alpha<<<sblocks(nv), 128, 0, s>>>(nv, s1, s2, iconv, alpha, ac, nalpha);
+}
 // RBiCGStab recurrences (rbicgstab.inl:130-134 and 193-211)
 __global__ void k_ralpha(int nv, const double *rho, const double *delta, double *alpha,
                          double *nalpha) {

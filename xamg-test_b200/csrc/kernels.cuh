@@ -144,6 +144,9 @@ void bicg_omega(int nv, const double *s2, const double *s3, const double *s4,
 // beta = (s1/rho)*(alpha/omega); rho = s1; c1 = -(omega*beta); also -alpha, -omega
 void bicg_beta(int nv, const double *s1, double *rho, const double *alpha, const double *omega,
                double *beta, double *c1, cudaStream_t s);
+// PCG: alpha = s1/s2; ac = iconv*alpha; nalpha = -1*alpha
+void pcg_alpha(int nv, const double *s1, const double *s2, const double *iconv, double *alpha, double *ac,
+               double *nalpha, cudaStream_t s);
 // RBiCGStab: alpha = rho/delta, nalpha = -1*alpha
 void rbicg_alpha(int nv, const double *rho, const double *delta, double *alpha, double *nalpha,
                  cudaStream_t s);
