@@ -246,10 +246,14 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
     }
     __syncthreads();
     bool ok = true;
-    // register prefetch of this thread's first row of the current level
-    bool pv = false;
-    int pr = 0;
-    T pt[V], px[V];
+    // register prefetch of this thread's first row of a level: row index, t
+    // and (without the x tile) the row's old x.  Neither changes during the
+    // sweep before the row's own level (one launch per sweep direction, every
+    // row updated once), so level l+1's are loaded at the start of level l
+    // and arrive while level l computes.
+    bool pv = false, nf = false;
+    int pr = 0, nr = 0;
+    T pt[V], px[V], nt[V], nx[V];
     auto wait_q = [&](int q) {
         if (s_stage[q]) {
             if (!mbar_wait(&mbar[q], use[q] & 1u)) {
@@ -259,32 +263,48 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
             use[q]++;
         }
     };
-    auto prefetch = [&](int l, const Desc &d) {
+    auto prefetch = [&](int l, const Desc &d) {  // into nf, nr, nt, nx
         int q = l % NB;
-        pv = false;
+        nf = false;
         if (!ok) return;  // staging buffers are not trustworthy after a timeout
         int items = (d.r1 - d.r0) * TPR;
         if (tid < items) {
             int r = d.r0 + tid / TPR, lane = tid % TPR;
             int row = s_stage[q] ? s_row[q][r - rlo(d)] : __ldg(lrow + r);
             if (row >= 0) {
-                pv = true;
-                pr = row;
-                gld<T, V, CG>(t + (i64)row * NV + lane * V, pt);
-                if (!XS) gld<T, V, CG>(x + (i64)row * NV + lane * V, px);
+                nf = true;
+                nr = row;
+                gld<T, V, CG>(t + (i64)row * NV + lane * V, nt);
+                if (!XS) gld<T, V, CG>(x + (i64)row * NV + lane * V, nx);
             }
+        }
+    };
+    auto rotate = [&]() {
+        pv = nf;
+        pr = nr;
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            pt[e] = nt[e];
+            px[e] = nx[e];
         }
     };
     Desc dc = l0 < l1 ? dget(l0) : Desc{0, 0, 0, 0};
     if (l0 < l1) {
         wait_q(l0 % NB);
         prefetch(l0, dc);
+        rotate();
     }
     for (int l = l0; ok && l < l1; ++l) {
         const int q = l % NB;
         if (issuer && l + 2 < l1) {
             issue(l + 2, dn2);
             if (l + 3 < l1) dn2 = dget(l + 3);
+        }
+        Desc dnx{0, 0, 0, 0};
+        if (l + 1 < l1) {
+            dnx = dget(l + 1);
+            wait_q((l + 1) % NB);
+            prefetch(l + 1, dnx);
         }
         const bool staged = s_stage[q] != 0;
         const int items = (dc.r1 - dc.r0) * TPR;
@@ -432,12 +452,10 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
                 gst<T, V, CG>(x + (i64)row * NV + lane * V, xo);
             }
         }
-        // next level: its staging copy was issued a level earlier; read this
-        // thread's next row and start its t (and x) loads before the barrier
+        // next level: its row, t and x were prefetched at the start of this one
         if (l + 1 < l1) {
-            dc = dget(l + 1);
-            wait_q((l + 1) % NB);
-            prefetch(l + 1, dc);
+            dc = dnx;
+            rotate();
         }
         if (MODE == 0) {
             if (l + 1 < l1 &&
