@@ -152,6 +152,10 @@ void *xamg_spmv_runs_plan_create(int64_t n, const int *rp_host, const int *ci_ho
                                  const double *val_host, int rows, int fp32);
 int xamg_spmv_runs_plan_info(void *plan, int64_t *nchunks, double *coverage, int64_t *segments,
                              int64_t *value_slots);
+/* The run detection alone, on the host (no device work): what plan_info
+ * would report for a plan of these HOST arrays. */
+int xamg_spmv_runs_analyze(int64_t n, const int *rp_host, const int *ci_host, int rows, int64_t *nchunks,
+                           double *coverage, int64_t *segments);
 int xamg_spmv_runs(void *plan, int prec, int nv, const void *x, void *y, int mode, const void *b,
                    void *stream);
 int xamg_spmv_runs_plan_destroy(void *plan);

@@ -173,3 +173,57 @@ def test_gs_levels_27pt_count():
     lf, lb, nl = xamg.gs_levels_host(rp, ci, 0)
     # lexicographic 27-point: level(i,j,k) = i + 2j + 4k
     assert nl == (7 * 16 - 6, 7 * 16 - 6)
+
+
+def _run_model(rp, ci, R=8):
+    """Independent model of the run detection: chunks of up to R consecutive
+    rows with equal entry counts whose columns are the previous row's plus
+    one; segments = runs of at most 3 consecutive columns of a chunk's first row."""
+    n = len(rp) - 1
+    chunks = segs = full = 0
+    r = 0
+    while r < n:
+        m = rp[r + 1] - rp[r]
+        cnt = 1
+        while cnt < R and r + cnt < n:
+            a, b = rp[r + cnt - 1], rp[r + cnt]
+            if rp[r + cnt + 1] - b != m or not np.array_equal(ci[b:b + m], ci[a:a + m] + 1):
+                break
+            cnt += 1
+        cols = ci[rp[r]:rp[r] + m]
+        e = 0
+        while e < m:
+            ln = 1
+            while ln < 3 and e + ln < m and cols[e + ln] == cols[e + ln - 1] + 1:
+                ln += 1
+            segs += 1
+            e += ln
+        chunks += 1
+        if cnt == R:
+            full += cnt * m
+        r += cnt
+    return chunks, (full / len(ci) if len(ci) else 0.0), segs
+
+
+def test_run_detection_matches_model():
+    rng = np.random.default_rng(4)
+    cases = [xamg.CsrMatrix.aniso27(9).arrays()[:2], xamg.CsrMatrix.cube(7, 5, 3, 0).arrays()[:2],
+             util.random_csr(300, 300, rng, max_nnz=9, empty_rows=(0, 5))[:2]]
+    # a band matrix: every row a shifted copy, runs cut only by the chunk size
+    n = 100
+    rp = np.arange(0, 3 * n + 1, 3, dtype=np.int32)
+    ci = (np.arange(n)[:, None] + np.arange(3)[None, :]).ravel().astype(np.int32) % n
+    cases.append((rp, ci))
+    L = xamg.lib()
+    for rp, ci in cases:
+        rp = np.ascontiguousarray(rp, np.int32)
+        ci = np.ascontiguousarray(ci, np.int32)
+        out = np.zeros(2, np.int64)
+        cov = np.zeros(1)
+        xamg.check(L.xamg_spmv_runs_analyze(len(rp) - 1, xamg._ptr(rp), xamg._ptr(ci), 8, xamg._ptr(out[0:]),
+                                            xamg._ptr(cov), xamg._ptr(out[1:])))
+        chunks, coverage, segs = _run_model(rp, ci)
+        assert (out[0], out[1]) == (chunks, segs)
+        assert cov[0] == pytest.approx(coverage, abs=1e-15)
+    assert L.xamg_spmv_runs_analyze(len(rp) - 1, xamg._ptr(rp), xamg._ptr(ci), 4, xamg._ptr(out[0:]),
+                                    xamg._ptr(cov), xamg._ptr(out[1:])) == 2

@@ -559,5 +559,8 @@ cudaError_t gs_sweep_lcsr(Prec p, int nv, int mode, int xs, int nlev, int ncta, 
 
 // dynamic shared memory available for the x tile next to the two staging buffers
 int gs_lcsr_max_xs_bytes() { return 170 * 1024; }
+// an x tile this small leaves room for two CTAs per SM next to the staging
+// buffers (about 43 KB of static shared memory each)
+int gs_lcsr_xs_bytes_two_per_sm() { return 64 * 1024; }
 
 }  // namespace xk

@@ -757,6 +757,17 @@ void *xamg_spmv_runs_plan_create(int64_t n, const int *rp, const int *ci, const 
     if (rc) { delete h; return nullptr; }
     return h;
 }
+int xamg_spmv_runs_analyze(int64_t n, const int *rp, const int *ci, int rows, int64_t *nchunks, double *coverage,
+                           int64_t *segments) {
+    return guard([&] {
+        XCHECK(n >= 0 && rp && (n == 0 || ci) && nchunks && coverage && segments, "bad arguments");
+        XCHECK(rows == 8, "rows must be 8");
+        i64 nc = 0, ns = 0;
+        run_plan_analyze(n, rp, ci, rows, &nc, coverage, &ns);
+        *nchunks = nc;
+        *segments = ns;
+    });
+}
 int xamg_spmv_runs_plan_info(void *plan, int64_t *nchunks, double *coverage, int64_t *segments,
                              int64_t *value_slots) {
     return guard([&] {

@@ -52,28 +52,47 @@ static int segments(const int *c, int m, int *out) {
     return ns;
 }
 
+// Chunks of up to R rows, {r0, cnt, m, segments} each; returns the entries
+// that lie in chunks of exactly R rows.
+static i64 detect_chunks(i64 n, const int *rp, const int *ci, int R, std::vector<int> &ch) {
+    ch.clear();
+    ch.reserve((size_t)n);
+    i64 full = 0;
+    for (i64 r = 0; r < n;) {
+        const int m = rp[r + 1] - rp[r];
+        int cnt = 1;
+        while (cnt < R && r + cnt < n) {
+            const i64 a = rp[r + cnt - 1], b = rp[r + cnt];
+            if (rp[r + cnt + 1] - b != m) break;
+            bool ok = true;
+            for (int e = 0; e < m && ok; ++e) ok = ci[b + e] == ci[a + e] + 1;
+            if (!ok) break;
+            ++cnt;
+        }
+        const int ns = segments(ci + rp[r], m, nullptr);
+        ch.insert(ch.end(), {(int)r, cnt, m, ns});
+        if (cnt == R) full += (i64)cnt * m;
+        r += cnt;
+    }
+    return full;
+}
+
+void run_plan_analyze(i64 n, const int *rp, const int *ci, int R, i64 *nchunks, double *coverage, i64 *nseg) {
+    std::vector<int> ch;
+    const i64 full = detect_chunks(n, rp, ci, R, ch);
+    const i64 nnz = n > 0 ? rp[n] : 0;
+    *nchunks = (i64)ch.size() / 4;
+    *coverage = nnz ? (double)full / (double)nnz : 0.0;
+    i64 s = 0;
+    for (size_t c = 0; c < ch.size(); c += 4) s += ch[c + 3];
+    *nseg = s;
+}
+
 bool RunPlan::build(const HostCsr &h, int R_, bool f64, bool f32, double min_cov) {
     clear();
     if (h.n <= 0 || h.n != h.ncols || h.n >= (i64(1) << 30) || R_ != 8) return false;
     std::vector<int> ch;
-    ch.reserve((size_t)h.n);
-    i64 full = 0;
-    for (i64 r = 0; r < h.n;) {
-        const int m = h.rp[r + 1] - h.rp[r];
-        int cnt = 1;
-        while (cnt < R_ && r + cnt < h.n) {
-            const i64 a = h.rp[r + cnt - 1], b = h.rp[r + cnt];
-            if (h.rp[r + cnt + 1] - b != m) break;
-            bool ok = true;
-            for (int e = 0; e < m && ok; ++e) ok = h.ci[b + e] == h.ci[a + e] + 1;
-            if (!ok) break;
-            ++cnt;
-        }
-        const int ns = segments(&h.ci[h.rp[r]], m, nullptr);
-        ch.insert(ch.end(), {(int)r, cnt, m, ns});
-        if (cnt == R_) full += (i64)cnt * m;
-        r += cnt;
-    }
+    const i64 full = detect_chunks(h.n, h.rp.data(), h.ci.data(), R_, ch);
     const i64 nnz = h.nnz();
     coverage = nnz ? (double)full / (double)nnz : 0.0;
     if (coverage < min_cov) {

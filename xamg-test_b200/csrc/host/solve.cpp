@@ -20,6 +20,17 @@ Context &ctx() {
 
 static bool quiet() { return std::getenv("XAMG_QUIET") != nullptr; }
 
+static int sm_count() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        XCUDA(cudaGetDevice(&dev));
+        XCUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
 // ------------------------------------------------------------------ DCsr
 void DCsr::upload(const HostCsr &h, bool f64, bool f32) {
     cudaStream_t s = ctx().stream;
@@ -346,7 +357,12 @@ void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val
         unsigned *bar = sync.as<unsigned>();
         int *err = (int *)(sync.as<char>() + kSyncErrOffset);
         int md = mode == GsMode::BLOCKS ? 1 : 0;
-        int xs = md == 1 && (i64)brows * nv * (i64)prec_size(p) <= xk::gs_lcsr_max_xs_bytes();
+        // the block's x tile in shared memory when it fits; a tile that allows
+        // only one CTA per SM only when the blocks fit in one wave anyway
+        // (otherwise the gather form, two CTAs per SM, finishes sooner)
+        const i64 tile = (i64)brows * nv * (i64)prec_size(p);
+        int xs = md == 1 && (tile <= xk::gs_lcsr_xs_bytes_two_per_sm() ||
+                             (tile <= xk::gs_lcsr_max_xs_bytes() && nblocks <= sm_count()));
         XCUDA(xk::gs_sweep_lcsr(p, nv, md, xs, L.nlev, L.ncta, L.desc.as<int>(), L.blev.as<int>(),
                                 L.lrp.as<int>(), L.lci.as<int>(), L.lva.p, L.lrow.as<int>(),
                                 L.linvd.p, t, x, relax, brows, n, bar, err, L.emax, s));

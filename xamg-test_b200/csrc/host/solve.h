@@ -52,6 +52,11 @@ struct RunPlan {
     void clear();
 };
 
+// Run detection alone (host only): chunk count, fraction of the entries in
+// chunks of R rows, and segments (runs of at most 3 consecutive columns of
+// each chunk's first row).
+void run_plan_analyze(i64 n, const int *rp, const int *ci, int R, i64 *nchunks, double *coverage, i64 *nseg);
+
 struct DCsr {
     i64 n = 0, ncols = 0, nnz = 0;
     DBuf rp, ci, v64, v32;

@@ -94,6 +94,7 @@ cudaError_t gs_sweep_lcsr(Prec p, int nv, int mode, int xs, int nlev, int ncta, 
                           const void *relax, i64 brows, i64 n, unsigned *gbar, int *err,
                           int emax, cudaStream_t s);
 int gs_lcsr_max_xs_bytes();
+int gs_lcsr_xs_bytes_two_per_sm();
 
 // Hybrid Gauss-Seidel right-hand side: t = 1*b + (-1)*(sum over the entries
 // outside the row's block of a_ij x_j)   (blas2.h:226-259)
