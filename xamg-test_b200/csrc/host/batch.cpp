@@ -163,7 +163,7 @@ void Batch::run_body(BatchGroup &G, int graph_mode) {
         xk::convert(Prec::F64, Prec::F32, in.count(), in.p(), G.z32.p(), st);
         xk::fill(Prec::F32, G.w32.count(), 0.0, G.w32.p(), st);
         xk::set_spmv_variant(G.var32);
-        G.M->solve(G.w32, G.z32);
+        G.M->solve_from_zero(G.w32, G.z32);
         xk::convert(Prec::F32, Prec::F64, G.w32.count(), G.w32.p(), out.p(), st);
         xk::set_spmv_variant(G.var64);
     };

@@ -556,11 +556,13 @@ struct HSGS : Solver {
             hres.alloc(nv);
         }
     }
-    // one blas2::SGS call (blas2.h:184-281)
-    void sgs(DVec &x, const DVec &b) {
+    // one blas2::SGS call (blas2.h:184-281).  With x zero the off-block
+    // product is +0 in every entry, so t = 1*b + (-1)*(+0) is b itself, bit
+    // for bit, and is not formed
+    void sgs(DVec &x, const DVec &b, bool xzero = false) {
         cudaStream_t s = ctx().stream;
         const void *tp = b.p();
-        if (t.n) {
+        if (t.n && !xzero) {
             // t = 1*b + (-1)*(A_off x), the chain over the off-block entries in CSR order
             if (op.gs->aoff.n == x.n && op.gs->aprec == prec)
                 op.gs->aoff.spmv(prec, nv, x.p(), t.p(), 2, b.p(), s);
@@ -587,17 +589,19 @@ struct HSGS : Solver {
         conv.record();
         return conv.check();
     }
-    void solve(DVec &x, const DVec &b) override {
+    void run(DVec &x, const DVec &b, bool xzero) {
         int iters = (int)prm.get_int("max_iters");
         conv.init(nv);
         set_rhs_base(conv, b, part);
         if (conv.check_on && residual_check(x, b, true)) return;
         for (int it = 1; it <= iters; ++it) {
             conv.iters = it;
-            sgs(x, b);
+            sgs(x, b, xzero && it == 1);
             if (conv.check_on && residual_check(x, b, false)) return;
         }
     }
+    void solve(DVec &x, const DVec &b) override { run(x, b, false); }
+    void solve_from_zero(DVec &x, const DVec &b) override { run(x, b, true); }
 };
 
 // Spectrum bounds of D^-1/2 A D^-1/2 for the Chebyshev smoother.  The
@@ -945,12 +949,15 @@ struct MultiGrid : Solver {
     const DCsr &levA(int l) const { return l == 0 ? Afine->d : lv[l].A; }
 
     // MG_cycle mg.inl:186-280
-    void mg_cycle(int l, DVec &x, const DVec &b, int cyc) {
+    void mg_cycle(int l, DVec &x, const DVec &b, int cyc, bool xzero = false) {
         cudaStream_t s = ctx().stream;
         MGLevel &m = lv[l];
         Prec p = m.prec, cp = lvprec(l + 1);
         const DCsr &A = levA(l);
-        if (cyc != 1) m.pre->solve(x, b);
+        if (cyc != 1) {
+            if (xzero) m.pre->solve_from_zero(x, b);
+            else m.pre->solve(x, b);
+        }
         // temp = b - A x
         A.spmv(p, nv, x.p(), m.tmp.p(), 2, b.p(), s);
         // restriction (convert first when the next level is in FP32)
@@ -964,7 +971,7 @@ struct MultiGrid : Solver {
         if (l + 1 == (int)lv.size() - 1) {
             coarse->solve(m.xH, m.bH);
         } else {
-            mg_cycle(l + 1, m.xH, m.bH, cyc);
+            mg_cycle(l + 1, m.xH, m.bH, cyc, true);  // x_H was just zeroed
             if (cyc == 2) mg_cycle(l + 1, m.xH, m.bH, 2);
             else if (cyc == 1) mg_cycle(l + 1, m.xH, m.bH, 0);
         }
@@ -998,7 +1005,7 @@ struct MultiGrid : Solver {
         return conv.check();
     }
 
-    void solve(DVec &x, const DVec &b) override {
+    void run(DVec &x, const DVec &b, bool xzero) {
         int iters = (int)prm.get_int("max_iters");
         conv.init(nv);
         set_rhs_base(conv, b, part);
@@ -1006,10 +1013,12 @@ struct MultiGrid : Solver {
         for (int it = 1; it <= iters; ++it) {
             conv.iters = it;
             if (lv.size() == 1) coarse->solve(x, b);
-            else mg_cycle(0, x, b, cycle);
+            else mg_cycle(0, x, b, cycle, xzero && it == 1);
             if (conv.check_on && residual_check(x, b, false)) return;
         }
     }
+    void solve(DVec &x, const DVec &b) override { run(x, b, false); }
+    void solve_from_zero(DVec &x, const DVec &b) override { run(x, b, true); }
 
     std::string info() const override {
         std::string s = "MultiGrid levels:";
@@ -1101,7 +1110,7 @@ struct Krylov : Solver {
             DVec *pp = &p, *ss = &s;
             if (precond) {
                 xk::fill(prec, p_.count(), 0.0, p_.p(), st);
-                M->solve(p_, p);
+                M->solve_from_zero(p_, p);
                 pp = &p_;
             }
             spmv(*pp, v, st);
@@ -1111,7 +1120,7 @@ struct Krylov : Solver {
             xk::blas(prec, nv, n, xk::Op::AXPBY_Z, S(ONES), r.p(), S(NALPHA), v.p(), nullptr, s.p(), st);
             if (precond) {
                 xk::fill(prec, s_.count(), 0.0, s_.p(), st);
-                M->solve(s_, s);
+                M->solve_from_zero(s_, s);
                 ss = &s_;
             }
             spmv(*ss, t, st);
@@ -1165,7 +1174,7 @@ struct Krylov : Solver {
         if (conv.check()) return;
         set_iconv(st);
         xk::fill(prec, z.count(), 0.0, z.p(), st);
-        M->solve(z, r);
+        M->solve_from_zero(z, r);
         xk::blas(prec, nv, n, xk::Op::COPY, nullptr, z.p(), nullptr, nullptr, nullptr, p.p(), st);
         for (int it = 1;; ++it) {
             conv.iters = it;
@@ -1178,7 +1187,7 @@ struct Krylov : Solver {
             axpby(S(AC), p, S(ONES), x, x);
             axpby(S(NALPHA), Ap, S(ONES), r, r);
             xk::fill(prec, z.count(), 0.0, z.p(), st);
-            M->solve(z, r);
+            M->solve_from_zero(z, r);
             {
                 const void *Aa[2] = {r.p(), r.p()}, *Bb[2] = {z.p(), r.p()};
                 xk::dots(prec, nv, n, 2, Aa, Bb, part.as<double>(), S(S3), st);  // S3 = (r,z), S4 = (r,r)
@@ -1210,7 +1219,7 @@ struct Krylov : Solver {
         };
         auto apply_m = [&](DVec &out, const DVec &in) {
             xk::fill(prec, out.count(), 0.0, out.p(), st);
-            M->solve(out, in);
+            M->solve_from_zero(out, in);
         };
         conv.init(nv);
         set_rhs_base(conv, b, part);

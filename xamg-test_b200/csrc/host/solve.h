@@ -182,6 +182,10 @@ struct Solver {
     virtual ~Solver() {}
     // x: initial guess on entry (the preconditioner role zeroes it itself)
     virtual void solve(DVec &x, const DVec &b) = 0;
+    // the same with x known to be zero on entry (the caller has just zeroed
+    // it): a solver may skip products with x whose result is then exactly
+    // known; the results are identical to solve()
+    virtual void solve_from_zero(DVec &x, const DVec &b) { solve(x, b); }
     virtual void renew(const GlobalParams &gp) {}
     virtual std::string info() const { return method; }
 };
