@@ -31,13 +31,18 @@
 //     stated order and dot_sequential() gives the reference's 1-core order for
 //     comparison.
 // Compile with -ffp-contract=off so that no expression is contracted behind
-// the source's back.
+// the source's back, and with -fopenmp: loops whose iterations write disjoint
+// outputs (rows of products, elements of vector updates, chunks of the inner
+// product tree) run on all host threads with unchanged results; the
+// Gauss-Seidel sweeps stay sequential, as the reference's single-process
+// order requires.
 
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <vector>
+#include <omp.h>
 #include <algorithm>
 #include <memory>
 
@@ -51,6 +56,7 @@ namespace orc {
 // and csr_Axpy csr_matvec.inl:104-141.  Row sums run in CSR order with fma.
 template <class T>
 void spmv(i64 n, const int *rp, const int *ci, const T *v, const T *x, T *y, int nv, int acc) {
+    #pragma omp parallel for schedule(static)
     for (i64 i = 0; i < n; ++i) {
         for (int k = 0; k < nv; ++k) {
             T s = acc ? y[i * nv + k] : T(0);
@@ -76,6 +82,7 @@ void hsgs(i64 n, const int *rp, const int *ci, const T *v, const T *invd, const 
     for (int q = 0; q < nb; ++q)
         for (i64 i = bp[q]; i < bp[q + 1]; ++i) blk[i] = q;
     // t = b - A_off x   (blas2.h:226-259: t=0; t += A_offd x; t = 1*b + (-1)*t)
+    #pragma omp parallel for schedule(static)
     for (i64 i = 0; i < n; ++i) {
         for (int k = 0; k < nv; ++k) {
             T s = T(0);
@@ -111,6 +118,7 @@ template <class T>
 void jacobi_sweep(i64 n, const int *rp, const int *ci, const T *v, const T *invd, const T *b,
                   T *x, T *r, const T *relax, int nv) {
     spmv<T>(n, rp, ci, v, x, r, nv, 0);
+    #pragma omp parallel for schedule(static)
     for (i64 i = 0; i < n; ++i)
         for (int k = 0; k < nv; ++k) {
             T c = relax[k] * invd[i];
@@ -132,6 +140,7 @@ template <class TI, class TA>
 void dot_canonical(i64 n, int nv, const TI *x, const TI *y, TA *out) {
     i64 nc = (n + 255) / 256;
     std::vector<TA> P((size_t)std::max<i64>(nc, 1) * nv, TA(0));
+    #pragma omp parallel for schedule(static)
     for (i64 c = 0; c < nc; ++c) {
         for (int k = 0; k < nv; ++k) {
             TA s[32];
@@ -208,6 +217,7 @@ void dense_inverse(int n, const double *A, double *Ainv) {
 // y = Ainv b, dense_Ax_y dense_matvec.inl:109-117, fma in column order.
 template <class T>
 void dense_gemv(int n, const T *Ainv, const T *b, T *y, int nv) {
+    #pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i)
         for (int k = 0; k < nv; ++k) {
             T s = T(0);
@@ -341,19 +351,24 @@ void chebyshev(const MG &mg, int l, const T *b, T *x, int nv) {
     const size_t sz = (size_t)n * nv;
     std::vector<T> r(sz), t1(sz), t2(sz);
     spmv<T>(n, L.A.rp.data(), L.A.ci.data(), vals<T>(L.A), x, r.data(), nv, 0);
+    #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < sz; ++q) r[q] = T(1) * b[q] + T(-1) * r[q];
     auto rowscal = [&](std::vector<T> &z) {
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q) z[q] = (T)((double)z[q] * (double)isd[q / nv]);
     };
     rowscal(r);
+    #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < sz; ++q) t1[q] = (T)(c[p - 1] * (double)r[q]);
     for (int i = p - 2; i >= 0; --i) {
         rowscal(t1);
         spmv<T>(n, L.A.rp.data(), L.A.ci.data(), vals<T>(L.A), t1.data(), t2.data(), nv, 0);
         rowscal(t2);
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q) t1[q] = (T)(c[i] * (double)r[q] + 1.0 * (double)t2[q]);
     }
     rowscal(t1);
+    #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < sz; ++q) x[q] = (T)(1.0 * (double)t1[q] + 1.0 * (double)x[q]);
 }
 
@@ -386,6 +401,7 @@ void vcycle(const MG &mg, int l, T *x, const T *b, int nv) {
     smooth<T>(mg, l, mg.pre_m, mg.pre_it, mg.pre_relax, b, x, nv);
     std::vector<T> tmp((size_t)n * nv), bH((size_t)nc * nv), xH((size_t)nc * nv, T(0));
     spmv<T>(n, L.A.rp.data(), L.A.ci.data(), vals<T>(L.A), x, tmp.data(), nv, 0);
+    #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < tmp.size(); ++q) tmp[q] = T(1) * b[q] + T(-1) * tmp[q];  // axpby(1,b,-1,temp)
     spmv<T>(L.R.n, L.R.rp.data(), L.R.ci.data(), vals<T>(L.R), tmp.data(), bH.data(), nv, 0);
     if (l + 1 == (int)mg.lv.size() - 1) {
@@ -400,6 +416,7 @@ void vcycle(const MG &mg, int l, T *x, const T *b, int nv) {
 template <class T>
 void mg_apply(const MG &mg, T *x, const T *b, int nv) {
     size_t sz = (size_t)mg.lv[0].A.n * nv;
+    #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < sz; ++q) x[q] = T(0);  // set_const(p_,0) pbicgstab.inl:116
     if (mg.lv.size() == 1) {
         dense_gemv<T>((int)mg.lv[0].A.n, ainv<T>(mg), b, x, nv);
@@ -465,6 +482,7 @@ int pbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
     cv.status.assign(nv, 0);
     // r0 = b - A x  (solver.h:183-190: Ax_y then axpby(1.0,b,-1.0,r))
     spmv<T>(n, A.rp.data(), A.ci.data(), av, x, r0.data(), nv, 0);
+    #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < sz; ++q) r0[q] = T(1) * b[q] + T(-1) * r0[q];
     dot_canonical<T, double>(n, nv, r0.data(), r0.data(), rho.data());
     for (int k = 0; k < nv; ++k) cv.res0[k] = rho[k];
@@ -484,6 +502,7 @@ int pbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
         dot_canonical<T, double>(n, nv, v.data(), r0.data(), s1.data());
         for (int k = 0; k < nv; ++k) alpha[k] = rho[k] / s1[k];
         // s = 1*r + (-alpha)*v
+        #pragma omp parallel for schedule(static)
         for (i64 i = 0; i < n; ++i)
             for (int k = 0; k < nv; ++k) {
                 size_t q = (size_t)i * nv + k;
@@ -497,6 +516,7 @@ int pbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
         dot_canonical<T, double>(n, nv, s.data(), s.data(), s4.data());
         for (int k = 0; k < nv; ++k) omega[k] = s2[k] / s3[k];
         // x = alpha_c*p_ + omega_c*s_ + 1*x
+        #pragma omp parallel for schedule(static)
         for (i64 i = 0; i < n; ++i)
             for (int k = 0; k < nv; ++k) {
                 size_t q = (size_t)i * nv + k;
@@ -512,6 +532,7 @@ int pbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
         if (cv.check()) return it;
         for (int k = 0; k < nv; ++k) if (cv.status[k]) iconv[k] = 0;
         // r = 1*s + (-omega)*t
+        #pragma omp parallel for schedule(static)
         for (i64 i = 0; i < n; ++i)
             for (int k = 0; k < nv; ++k) {
                 size_t q = (size_t)i * nv + k;
@@ -527,6 +548,7 @@ int pbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
             s1[k] = c1;
         }
         // p = 1*r + c1*v + beta*p
+        #pragma omp parallel for schedule(static)
         for (i64 i = 0; i < n; ++i)
             for (int k = 0; k < nv; ++k) {
                 size_t q = (size_t)i * nv + k;
@@ -555,6 +577,7 @@ int pcg(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iters, Con
     cv.status.assign(nv, 0);
     // r = b - A x, res = (r, r)  (solver.h:183-190)
     spmv<T>(n, A.rp.data(), A.ci.data(), av, x, r.data(), nv, 0);
+    #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < sz; ++q) r[q] = T(1) * b[q] + T(-1) * r[q];
     dot_canonical<T, double>(n, nv, r.data(), r.data(), res.data());
     for (int k = 0; k < nv; ++k) cv.res0[k] = res[k];
@@ -572,15 +595,18 @@ int pcg(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iters, Con
         dot_canonical<T, double>(n, nv, r.data(), z.data(), s1.data());
         dot_canonical<T, double>(n, nv, p.data(), Ap.data(), s2.data());
         for (int k = 0; k < nv; ++k) alpha[k] = s1[k] / s2[k];
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q) {  // x = (iconv*alpha)*p + 1*x
             double ac = iconv[at(q)] * alpha[at(q)];
             x[q] = (T)(ac * (double)p[q] + 1.0 * (double)x[q]);
         }
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q)  // r = (-alpha)*Ap + 1*r
             r[q] = (T)((-1.0 * alpha[at(q)]) * (double)Ap[q] + 1.0 * (double)r[q]);
         precond(z, r);
         dot_canonical<T, double>(n, nv, r.data(), z.data(), s3.data());
         for (int k = 0; k < nv; ++k) beta[k] = s3[k] / s1[k];
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q)  // p = 1*z + beta*p
             p[q] = (T)(1.0 * (double)z[q] + beta[at(q)] * (double)p[q]);
         dot_canonical<T, double>(n, nv, r.data(), r.data(), res.data());
@@ -615,6 +641,7 @@ int rbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
     cv.status.assign(nv, 0);
     // 1-2. r0 = b - A x, rho = (r0, r0)  (solver.h:183-190)
     spmv<T>(n, A.rp.data(), A.ci.data(), av, x, r0.data(), nv, 0);
+    #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < sz; ++q) r0[q] = T(1) * b[q] + T(-1) * r0[q];
     dot_canonical<T, double>(n, nv, r0.data(), r0.data(), rho.data());
     for (int k = 0; k < nv; ++k) cv.res0[k] = rho[k];
@@ -633,9 +660,11 @@ int rbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
         dot_canonical<T, double>(n, nv, v.data(), r0.data(), delta.data());   // 7
         precond(s, v);                                                        // 8
         for (int k = 0; k < nv; ++k) alpha[k] = rho[k] / delta[k];            // 9
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q)                                       // 10
             t_[q] = (T)(1.0 * (double)z[q] + (-alpha[at(q, nv)]) * (double)s[q]);
         spmv<T>(n, A.rp.data(), A.ci.data(), av, t_.data(), t.data(), nv, 0);  // 11
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q)                                       // 12
             r[q] = (T)((-alpha[at(q, nv)]) * (double)v[q] + 1.0 * (double)r[q]);
         dot_canonical<T, double>(n, nv, t.data(), r.data(), theta.data());    // 13
@@ -644,12 +673,14 @@ int rbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
         dot_canonical<T, double>(n, nv, r.data(), r.data(), eta.data());
         precond(z, t);                                                        // 14
         for (int k = 0; k < nv; ++k) omega[k] = theta[k] / phi[k];            // 15
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q)                                       // 16
             r[q] = (T)((-omega[at(q, nv)]) * (double)t[q] + 1.0 * (double)r[q]);
         for (int k = 0; k < nv; ++k) {                                        // 17
             double ot = omega[k] * theta[k];
             res[k] = 1.0 * eta[k] + (-1.0) * ot;
         }
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q) {                                     // 23
             int k = at(q, nv);
             double ac = iconv[k] * alpha[k], oc = iconv[k] * omega[k];
@@ -665,8 +696,10 @@ int rbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
             beta[k] = rho[k] / temp;
             delta[k] = (-omega[k]) * beta[k];                                 // 25 (coefficient of s)
         }
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q)                                       // 24
             z[q] = (T)(1.0 * (double)t_[q] + (-omega[at(q, nv)]) * (double)z[q]);
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q) {                                     // 25
             int k = at(q, nv);
             v_[q] = (T)(1.0 * (double)z[q] + delta[k] * (double)s[q] + beta[k] * (double)v_[q]);
@@ -696,6 +729,7 @@ int ir_pbicgstab(const Csr &A, const MG &mg, const double *b, double *x, int nv,
     sub_iters = 0;
     auto residual = [&]() {
         spmv<double>(n, A.rp.data(), A.ci.data(), A.v64.data(), x, r.data(), nv, 0);
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q) r[q] = 1.0 * b[q] + (-1.0) * r[q];
         dot_canonical<double, double>(n, nv, r.data(), r.data(), d.data());
     };
@@ -710,9 +744,11 @@ int ir_pbicgstab(const Csr &A, const MG &mg, const double *b, double *x, int nv,
         in.ptol.resize(nv);
         for (int k = 0; k < nv; ++k)
             in.ptol[k] = std::max(cv.tol(k), inner_rel * std::sqrt(std::max(d[k], 0.0)));
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q) { ib[q] = (float)r[q]; ix[q] = 0.f; }
         Hist ih{nullptr, 0};
         sub_iters += pbicgstab<float>(A, &mg, ib.data(), ix.data(), nv, max_inner, in, ih);
+        #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q) {
             xc[q] = (double)ix[q];
             x[q] = 1.0 * xc[q] + 1.0 * x[q];
@@ -731,6 +767,10 @@ using namespace orc;
 
 // ======================================================================== C ABI
 extern "C" {
+
+// Host threads the oracle's parallel loops use (products, inner products and
+// vector updates; the Gauss-Seidel sweeps stay sequential).
+int orc_num_threads() { return omp_get_max_threads(); }
 
 void orc_spmv_d(i64 n, const int *rp, const int *ci, const double *v, const double *x, double *y,
                 int nv, int acc) { spmv<double>(n, rp, ci, v, x, y, nv, acc); }

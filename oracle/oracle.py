@@ -52,6 +52,7 @@ def lib():
             "orc_mg_apply_f": (None, [P, P, P, C.c_int]),
             "orc_pbicgstab_d": (C.c_int, [i64, P, P, P, P, P, P, C.c_int, C.c_int, C.c_double, C.c_double, P, C.c_int, P, P]),
             "orc_rbicgstab_d": (C.c_int, [i64, P, P, P, P, P, P, C.c_int, C.c_int, C.c_double, C.c_double, P, C.c_int, P, P]),
+            "orc_num_threads": (C.c_int, []),
             "orc_pcg_d": (C.c_int, [i64, P, P, P, P, P, P, C.c_int, C.c_int, C.c_double, C.c_double, P, C.c_int, P, P]),
         }
         for name, (res, args) in sig.items():
@@ -211,6 +212,11 @@ def pbicgstab(rp, ci, v, b, x0, mg=None, max_iters=1000, abs_tol=0.0, rel_tol=1e
     it = lib().orc_pbicgstab_d(n, p(rp), p(ci), p(v), mg.h if mg is not None else None, p(b), p(x), nv,
                                max_iters, abs_tol, rel_tol, p(hist), cap, p(status), p(res0))
     return x, it, hist[: it + 1], status, res0
+
+
+def num_threads():
+    """Host threads of the oracle's parallel loops."""
+    return int(lib().orc_num_threads())
 
 
 def pcg(rp, ci, v, b, x0, mg=None, max_iters=1000, abs_tol=0.0, rel_tol=1e-8):

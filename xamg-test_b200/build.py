@@ -75,7 +75,7 @@ def build_library(verbose=False):
 def build_oracle():
     src = os.path.join(ROOT, "oracle", "oracle.cpp")
     if _newer(src, ORACLE_LIB):
-        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-o", ORACLE_LIB, src])
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-o", ORACLE_LIB, src])
     return ORACLE_LIB
 
 
