@@ -16,7 +16,11 @@ guess.  Forms:
 The headline `value` is the faster of plain/mixed's device time per RHS on the
 128^3 problem; `e2e` repeats it through the XAMG C API with host buffers
 (pinned), copies included.  `gpu_launches` is the library's own count of the
-kernels it launched in the timed steps of that form.
+kernels it launched in the timed steps of that form.  `true_rel_residual`
+checks every form's solution in FP64 on the host (max over columns of
+||b - A x|| / ||b||).  The SpMV kernel is tuned first (CSR variants and the
+shifted-row run kernel, `--spmv` fixes it); `roofline` reports the FP64
+NV=16 product of the tuned kernel on the same operator.
 
 --impl reference times the CPU restatement of the reference's algorithm (the
 reference itself cannot be built here: it needs MPI, hypre, argsparser and
