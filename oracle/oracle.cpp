@@ -771,6 +771,7 @@ extern "C" {
 // Host threads the oracle's parallel loops use (products, inner products and
 // vector updates; the Gauss-Seidel sweeps stay sequential).
 int orc_num_threads() { return omp_get_max_threads(); }
+void orc_set_num_threads(int t) { omp_set_num_threads(t > 0 ? t : 1); }
 
 void orc_spmv_d(i64 n, const int *rp, const int *ci, const double *v, const double *x, double *y,
                 int nv, int acc) { spmv<double>(n, rp, ci, v, x, y, nv, acc); }

@@ -53,6 +53,7 @@ def lib():
             "orc_pbicgstab_d": (C.c_int, [i64, P, P, P, P, P, P, C.c_int, C.c_int, C.c_double, C.c_double, P, C.c_int, P, P]),
             "orc_rbicgstab_d": (C.c_int, [i64, P, P, P, P, P, P, C.c_int, C.c_int, C.c_double, C.c_double, P, C.c_int, P, P]),
             "orc_num_threads": (C.c_int, []),
+            "orc_set_num_threads": (None, [C.c_int]),
             "orc_pcg_d": (C.c_int, [i64, P, P, P, P, P, P, C.c_int, C.c_int, C.c_double, C.c_double, P, C.c_int, P, P]),
         }
         for name, (res, args) in sig.items():
@@ -217,6 +218,10 @@ def pbicgstab(rp, ci, v, b, x0, mg=None, max_iters=1000, abs_tol=0.0, rel_tol=1e
 def num_threads():
     """Host threads of the oracle's parallel loops."""
     return int(lib().orc_num_threads())
+
+
+def set_num_threads(t):
+    lib().orc_set_num_threads(int(t))
 
 
 def pcg(rp, ci, v, b, x0, mg=None, max_iters=1000, abs_tol=0.0, rel_tol=1e-8):

@@ -183,3 +183,26 @@ def test_gs_levels_respect_sequential_order():
                 assert lf[j] < lf[i]
             elif j > i:
                 assert lf[j] > lf[i] and lb[j] < lb[i]
+
+
+def test_threaded_oracle_is_bit_identical():
+    """The oracle's parallel loops write disjoint outputs: one thread and all
+    threads give the same bits (products, inner products, a preconditioned
+    solve with its hybrid smoother)."""
+    rp, ci, v = xamg.CsrMatrix.aniso27(14).arrays()
+    rng = np.random.default_rng(21)
+    B = rng.uniform(-1, 1, (len(rp) - 1, 4))
+    csr = xamg.CsrMatrix.from_arrays(rp, ci, v)
+    lv = xamg.amg_host(csr, xamg.Params(util.amg_params(max_levels=4)))
+    full = orc.num_threads()
+    out = []
+    try:
+        for t in (1, max(full, 2)):
+            orc.set_num_threads(t)
+            mg = orc.MG(lv, block_rows=300)
+            x, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg, 100, 0.0, 1e-8)
+            out.append((orc.spmv(rp, ci, v, B, 4), orc.dot(B, B), x, hist))
+    finally:
+        orc.set_num_threads(full)
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
