@@ -227,3 +227,34 @@ def test_run_detection_matches_model():
         assert cov[0] == pytest.approx(coverage, abs=1e-15)
     assert L.xamg_spmv_runs_analyze(len(rp) - 1, xamg._ptr(rp), xamg._ptr(ci), 4, xamg._ptr(out[0:]),
                                     xamg._ptr(cov), xamg._ptr(out[1:])) == 2
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_run_detection_random_stencils(seed):
+    """Random stencil-like matrices (a shifted pattern per row with random
+    breaks: changed entry counts, perturbed columns, empty rows) against the
+    independent model of the run detection."""
+    rng = np.random.default_rng(100 + seed)
+    n = int(rng.integers(50, 400))
+    offs = np.sort(rng.choice(np.arange(-40, 41), size=int(rng.integers(1, 12)), replace=False))
+    rp, ci = [0], []
+    for r in range(n):
+        cols = [r + o for o in offs if 0 <= r + o < n]
+        u = rng.random()
+        if u < 0.05:
+            cols = []
+        elif u < 0.12 and cols:
+            cols[int(rng.integers(len(cols)))] = int(rng.integers(n))
+        elif u < 0.18:
+            cols = cols + [int(rng.integers(n))]
+        ci += cols
+        rp.append(len(ci))
+    rp = np.array(rp, np.int32)
+    ci = np.array(ci, np.int32)
+    out = np.zeros(2, np.int64)
+    cov = np.zeros(1)
+    xamg.check(xamg.lib().xamg_spmv_runs_analyze(n, xamg._ptr(rp), xamg._ptr(ci), 8, xamg._ptr(out[0:]),
+                                                 xamg._ptr(cov), xamg._ptr(out[1:])))
+    chunks, coverage, segs = _run_model(rp, ci)
+    assert (out[0], out[1]) == (chunks, segs)
+    assert cov[0] == pytest.approx(coverage, abs=1e-15)
