@@ -115,6 +115,27 @@ long long XAMG_b200_batch_last_kernels(size_t bid);
 int XAMG_b200_batch_groups(size_t bid, int *out, int cap);
 int XAMG_b200_batch_destroy(size_t bid);
 
+/* ---- Row partition of one system (host side of a multi-GPU solve) ------- */
+/* Rank `rank` of `nranks` owns the contiguous rows of the reference's block
+ * partition (part.h: equal blocks, the remainder on the last).  rp/ci are the
+ * HOST arrays of the whole system.  The local matrix keeps each owned row's
+ * entries in CSR order with columns renumbered: owned columns first (global
+ * column - first row), then the halo slots (rows owned by other ranks, in
+ * ascending global order, hence grouped by owner), so a product over
+ * [owned x | halo x] gives every row exactly the single-system bits.
+ * info: out[0] first row, out[1] rows, out[2] local entries, out[3] halo slots.
+ * local_csr: rows + 1 row pointers, the renumbered columns and (optional) the
+ * global entry index of every local entry.  halo: global row and owner of
+ * every halo slot.  sends: the owned rows (global) `peer` needs, in the order
+ * of the peer's halo; *count alone when rows_out is NULL. */
+int XAMG_b200_rowpart_create(int64_t n, const int *rp_host, const int *ci_host, int nranks, int rank,
+                             size_t *id);
+int XAMG_b200_rowpart_info(size_t id, int64_t *out);
+int XAMG_b200_rowpart_local_csr(size_t id, int *rp_out, int *ci_out, int64_t *src_out);
+int XAMG_b200_rowpart_halo(size_t id, int64_t *rows_out, int *owner_out);
+int XAMG_b200_rowpart_sends(size_t id, int peer, int64_t *rows_out, int64_t *count);
+int XAMG_b200_rowpart_destroy(size_t id);
+
 /* ---- Part 2: kernel-level device interface ----------------------------- */
 
 /* csr_Ax_y / csr_Axpy (blas2/detail/csr_matvec.inl:32-260):

@@ -3,6 +3,7 @@
 // include/xamg_b200.h.  Handles are indices into process-global lists and are
 // never reused, as in the reference (xamg_c_api.cpp:66-85).
 #include "solve.h"
+#include "dist.h"
 #include "batch.h"
 #include "amg.h"
 #include <chrono>
@@ -961,6 +962,61 @@ int XAMG_b200_batch_destroy(size_t bid) {
         Batch *B = get(blist, bid, "batch");
         delete B;
         blist[bid] = nullptr;
+    });
+}
+
+// ---------------------------------------------------------------- row partition
+static std::vector<RowPart *> rplist;
+int XAMG_b200_rowpart_create(int64_t n, const int *rp, const int *ci, int nranks, int rank, size_t *id) {
+    return guard([&] {
+        XCHECK(rp && ci && id && n > 0, "bad arguments");
+        std::unique_ptr<RowPart> P(new RowPart());
+        P->build(n, rp, ci, nranks, rank);
+        rplist.push_back(P.release());
+        *id = rplist.size() - 1;
+    });
+}
+int XAMG_b200_rowpart_info(size_t id, int64_t *out) {
+    return guard([&] {
+        RowPart *P = get(rplist, id, "row partition");
+        out[0] = P->first[P->rank];
+        out[1] = P->nrows();
+        out[2] = (int64_t)P->lci.size();
+        out[3] = (int64_t)P->halo.size();
+    });
+}
+int XAMG_b200_rowpart_local_csr(size_t id, int *rp_out, int *ci_out, int64_t *src_out) {
+    return guard([&] {
+        RowPart *P = get(rplist, id, "row partition");
+        std::memcpy(rp_out, P->lrp.data(), sizeof(int) * P->lrp.size());
+        if (!P->lci.empty()) std::memcpy(ci_out, P->lci.data(), sizeof(int) * P->lci.size());
+        if (src_out && !P->lsrc.empty()) std::memcpy(src_out, P->lsrc.data(), sizeof(int64_t) * P->lsrc.size());
+    });
+}
+int XAMG_b200_rowpart_halo(size_t id, int64_t *rows_out, int *owner_out) {
+    return guard([&] {
+        RowPart *P = get(rplist, id, "row partition");
+        for (size_t h = 0; h < P->halo.size(); ++h) {
+            if (rows_out) rows_out[h] = P->halo[h];
+            if (owner_out) owner_out[h] = P->halo_owner[h];
+        }
+    });
+}
+int XAMG_b200_rowpart_sends(size_t id, int peer, int64_t *rows_out, int64_t *count) {
+    return guard([&] {
+        RowPart *P = get(rplist, id, "row partition");
+        XCHECK(peer >= 0 && peer < P->nranks, "bad peer");
+        const std::vector<i64> &v = P->sends[peer];
+        *count = (int64_t)v.size();
+        if (rows_out)
+            for (size_t k = 0; k < v.size(); ++k) rows_out[k] = v[k];
+    });
+}
+int XAMG_b200_rowpart_destroy(size_t id) {
+    return guard([&] {
+        RowPart *P = get(rplist, id, "row partition");
+        delete P;
+        rplist[id] = nullptr;
     });
 }
 }  // extern "C"

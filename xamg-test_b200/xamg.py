@@ -115,6 +115,12 @@ def lib():
             "xamg_spmv_runs_plan_create": (P, [i64, P, P, P, C.c_int, C.c_int]),
             "xamg_spmv_runs_plan_info": (C.c_int, [P, P, P, P, P]),
             "xamg_spmv_runs_analyze": (C.c_int, [i64, P, P, C.c_int, P, P, P]),
+            "XAMG_b200_rowpart_create": (C.c_int, [i64, P, P, C.c_int, C.c_int, P]),
+            "XAMG_b200_rowpart_info": (C.c_int, [C.c_size_t, P]),
+            "XAMG_b200_rowpart_local_csr": (C.c_int, [C.c_size_t, P, P, P]),
+            "XAMG_b200_rowpart_halo": (C.c_int, [C.c_size_t, P, P]),
+            "XAMG_b200_rowpart_sends": (C.c_int, [C.c_size_t, C.c_int, P, P]),
+            "XAMG_b200_rowpart_destroy": (C.c_int, [C.c_size_t]),
             "xamg_spmv_runs": (C.c_int, [P, C.c_int, C.c_int, P, P, C.c_int, P, P]),
             "xamg_spmv_runs_plan_destroy": (C.c_int, [P]),
             "xamg_gs_plan_create": (P, [i64, P, P, i64, C.c_int]),
@@ -445,6 +451,43 @@ def amg_host(csr, params):
     finally:
         lib().XAMG_b200_amg_host_destroy(h.value)
     return out
+
+
+class RowPart:
+    """One rank's rows of a system for a multi-GPU solve: the local matrix with
+    columns renumbered [owned | halo], the halo slots and the per-peer send
+    lists (host arrays; see XAMG_b200_rowpart_* in include/xamg_b200.h)."""
+
+    def __init__(self, rp, ci, nranks, rank):
+        rp = np.ascontiguousarray(rp, np.int32)
+        ci = np.ascontiguousarray(ci, np.int32)
+        self.h = C.c_size_t()
+        check(lib().XAMG_b200_rowpart_create(len(rp) - 1, _ptr(rp), _ptr(ci), nranks, rank, C.byref(self.h)))
+        info = np.zeros(4, np.int64)
+        check(lib().XAMG_b200_rowpart_info(self.h.value, _ptr(info)))
+        self.first, self.nrows, nnz, nhalo = (int(v) for v in info)
+        self.rp = np.zeros(self.nrows + 1, np.int32)
+        self.ci = np.zeros(nnz, np.int32)
+        self.src = np.zeros(nnz, np.int64)
+        check(lib().XAMG_b200_rowpart_local_csr(self.h.value, _ptr(self.rp), _ptr(self.ci), _ptr(self.src)))
+        self.halo = np.zeros(nhalo, np.int64)
+        self.owner = np.zeros(nhalo, np.int32)
+        check(lib().XAMG_b200_rowpart_halo(self.h.value, _ptr(self.halo), _ptr(self.owner)))
+        self.sends = {}
+        for peer in range(nranks):
+            if peer == rank:
+                continue
+            cnt = np.zeros(1, np.int64)
+            check(lib().XAMG_b200_rowpart_sends(self.h.value, peer, None, _ptr(cnt)))
+            rows = np.zeros(int(cnt[0]), np.int64)
+            check(lib().XAMG_b200_rowpart_sends(self.h.value, peer, _ptr(rows), _ptr(cnt)))
+            self.sends[peer] = rows
+
+    def __del__(self):
+        try:
+            lib().XAMG_b200_rowpart_destroy(self.h.value)
+        except Exception:
+            pass
 
 
 def gs_levels_host(rp, ci, block_rows=0):
