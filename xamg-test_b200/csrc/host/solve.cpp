@@ -578,12 +578,10 @@ struct HSGS : Solver {
     bool residual_check(DVec &x, const DVec &b, bool initial) {
         cudaStream_t s = ctx().stream;
         op.A->spmv(prec, nv, x.p(), r.p(), 2, b.p(), s);
-        double *d = part.as<double>();
         DBuf out(sizeof(double) * nv);
         dot1(r, r, part, out.as<double>(), s);
         XCUDA(cudaMemcpyAsync(hres.h, out.p, sizeof(double) * nv, cudaMemcpyDeviceToHost, s));
         XCUDA(cudaStreamSynchronize(s));
-        (void)d;
         if (initial) conv.res0.assign(hres.h, hres.h + nv);
         conv.update(hres.h);
         conv.record();
@@ -839,7 +837,6 @@ struct MultiGrid : Solver {
         amg_setup(A.h, ap, al);
         int L = (int)al.size();
         lv.resize(L);
-        cudaStream_t s = ctx().stream;
         for (int l = 0; l < L; ++l) {
             MGLevel &m = lv[l];
             m.prec = lvprec(l);
@@ -865,7 +862,6 @@ struct MultiGrid : Solver {
                 make_invd(hA, w64, w32, m.invd64, m.invd32);
             }
         }
-        (void)s;
         // smoothers
         for (int l = 0; l + 1 < L; ++l) {
             MGLevel &m = lv[l];
