@@ -258,3 +258,15 @@ def test_run_detection_random_stencils(seed):
     chunks, coverage, segs = _run_model(rp, ci)
     assert (out[0], out[1]) == (chunks, segs)
     assert cov[0] == pytest.approx(coverage, abs=1e-15)
+
+
+def test_run_plan_of_the_benchmark_operator():
+    # the 128^3 27-point operator of the benchmark: 94.2 % of its entries in
+    # full chunks of 8 rows, 9 segments of 3 columns per interior row
+    rp, ci, v = xamg.CsrMatrix.aniso27(128).arrays()
+    out = np.zeros(2, np.int64)
+    cov = np.zeros(1)
+    xamg.check(xamg.lib().xamg_spmv_runs_analyze(len(rp) - 1, xamg._ptr(rp), xamg._ptr(ci), 8, xamg._ptr(out[0:]),
+                                                 xamg._ptr(cov), xamg._ptr(out[1:])))
+    assert out[0] == 294912 and out[1] == 3183687
+    assert cov[0] == pytest.approx(0.9424083769633508, abs=1e-12)
