@@ -270,3 +270,21 @@ def test_run_plan_of_the_benchmark_operator():
                                                  xamg._ptr(cov), xamg._ptr(out[1:])))
     assert out[0] == 294912 and out[1] == 3183687
     assert cov[0] == pytest.approx(0.9424083769633508, abs=1e-12)
+
+
+REF_EXAMPLES = os.path.join(os.environ.get("XAMG_REFERENCE_ROOT", "/root/reference"), "examples", "c")
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference sources not present")
+@pytest.mark.parametrize("name", ["example", "example_ir"])
+def test_reference_c_examples_build_unchanged(name, tmp_path):
+    """The reference's own C callers compile against include/xamg_c_api.h and
+    link against the library with no source change (the drop-in claim)."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    obj, exe = str(tmp_path / (name + ".o")), str(tmp_path / name)
+    subprocess.run(["gcc", "-O1", "-c", os.path.join(REF_EXAMPLES, name + ".c"), "-I",
+                    os.path.join(root, "include"), "-o", obj], check=True)
+    libdir = os.path.join(root, "xamg-test_b200")
+    subprocess.run(["gcc", obj, "-L", libdir, "-lxamg_b200", "-Wl,-rpath," + libdir, "-lm", "-o", exe], check=True)
+    assert os.path.exists(exe)
