@@ -2,29 +2,39 @@
 128^3 27-point anisotropic AMG-PBiCGStab problem with 16 RHS (one B200).
 
 A step is one complete solve of the 16 right-hand sides from a zero initial
-guess.  Forms:
-  plain  - FP64 PBiCGStab + FP64 AMG V-cycle, hybrid-SGS smoothing in the
-           reference's single-process row order (parity form);
-  mixed  - FP64 iterative refinement around an FP32 PBiCGStab (FP64 inner
-           products and recurrences) with an FP32 AMG V-cycle whose SGS runs
-           the reference's hybrid block semantics with GPU-sized blocks.
-  batch  - 64 independent 7-point lognormal-coefficient systems (sides 16..96,
-           nv in {1,2,4,8}) solved together in one CUDA-graph launch (FP64
-           Krylov, FP32 AMG, autotuned SpMV per group); reported beside;
-  learned - held-out 64^3 bump-coefficient systems (nv = 8) from a zero guess
-           and from the trained network's guess; reported beside.
-The headline `value` is the faster of plain/mixed's device time per RHS on the
-128^3 problem; `e2e` repeats it through the XAMG C API with host buffers
-(pinned), copies included.  `gpu_launches` is the library's own count of the
-kernels it launched in the timed steps of that form.  `true_rel_residual`
-checks every form's solution in FP64 on the host (max over columns of
-||b - A x|| / ||b||).  The SpMV kernel is tuned first (CSR variants and the
-shifted-row run kernel, `--spmv` fixes it); `roofline` reports the FP64
-NV=16 product of the tuned kernel on the same operator.
+guess.  Forms (all on the same operator and right-hand sides):
+  plain        - FP64 PBiCGStab + FP64 AMG V-cycle, Gauss-Seidel in the
+                 reference's single-process row order (parity form);
+  plain_hybrid - the same FP64 method with the hybrid smoother split of the
+                 mixed form (every level in 296 blocks: Gauss-Seidel inside a
+                 block, Jacobi across blocks);
+  mixed        - FP64 iterative refinement around an FP32 PBiCGStab (FP64
+                 inner products and recurrences) with an FP32 AMG V-cycle on
+                 the hybrid split;
+  mixed_tight  - the mixed form with its outer refinement run to --tight-tol,
+                 so that its error against the FP64 solution is <= 1e-8;
+  sweep        - the mixed form for nv in {1, 4, 8, 16, 32} with error against
+                 an FP64 solve converged to 1e-12;
+  batch        - 64 independent 7-point lognormal-coefficient systems (sides
+                 16..96, nv in {1,2,4,8}) in one CUDA-graph launch;
+  learned      - held-out 64^3 bump-coefficient systems (nv = 8) from a zero
+                 guess and from the trained network's guess.
+The headline `value` is the fastest of plain / plain_hybrid / mixed in device
+time per RHS; `e2e` repeats it (and the plain form) through the XAMG C API
+with the right-hand sides copied in from pinned host memory and the solution
+copied out, every step.  `parity.c2_iter1` compares the plain form's first
+iteration at full size with the oracle's on the same hierarchy, bit for bit;
+`err_vs_fp64` is each form's error against the FP64 solution converged to
+1e-12.  `roofline` is the dominant kernel of the headline step (the hybrid
+Gauss-Seidel sweep on the finest level), timed with CUDA events inside one
+solve; `roofline.spmv` is the FP64 NV=16 product of the tuned SpMV kernel
+timed alone.  `gpu_launches` is the library's own count of the kernels it
+launched in the timed steps of the headline form.
 
---impl reference times the CPU restatement of the reference's algorithm (the
-reference itself cannot be built here: it needs MPI, hypre, argsparser and
-yaml-cpp) on the host cores on a bounded sample of the same workload.
+--impl reference runs the reference's method on the host cores through the
+oracle alone (the reference itself cannot be built here: it needs MPI,
+hypre, argsparser and yaml-cpp): the same operator and right-hand sides, the
+oracle's own AMG setup, one complete FP64 solve timed.
 """
 import argparse
 import json
@@ -149,7 +159,7 @@ def build_problem():
 RUN8 = 108
 
 
-def spmv_time(csr, prec=0, variant=-1, iters=20, info=None):
+def spmv_time(csr, prec=0, variant=-1, iters=20, info=None, mode=0):
     """Live CUDA-event timing of the NV=16 SpMV on the benchmark matrix,
     launched on a torch stream through the C ABI; returns ms per launch.  For
     the run kernel `info` (a dict) receives the plan's sizes."""
@@ -175,11 +185,12 @@ def spmv_time(csr, prec=0, variant=-1, iters=20, info=None):
             xamg.check(L.xamg_spmv_runs_plan_info(plan, xamg._ptr(a[0:]), xamg._ptr(cov), xamg._ptr(a[1:]),
                                                   xamg._ptr(a[2:])))
             info.update(nchunks=int(a[0]), coverage=float(cov[0]), segments=int(a[1]), value_slots=int(a[2]))
-        launch = lambda: L.xamg_spmv_runs(plan, prec, NV, P(x), P(y), 0, None, C.c_void_p(st.cuda_stream))
+        launch = lambda: L.xamg_spmv_runs(plan, prec, NV, P(x), P(y), mode, P(x) if mode == 2 else None,
+                                          C.c_void_p(st.cuda_stream))
     else:
         d = [torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), torch.from_numpy(v).to(dt).cuda()]
-        launch = lambda: L.xamg_csr_spmv(prec, NV, n, P(d[0]), P(d[1]), P(d[2]), P(x), P(y), 0, None,
-                                         C.c_void_p(st.cuda_stream))
+        launch = lambda: L.xamg_csr_spmv(prec, NV, n, P(d[0]), P(d[1]), P(d[2]), P(x), P(y), mode,
+                                         P(x) if mode == 2 else None, C.c_void_p(st.cuda_stream))
     torch.cuda.synchronize()
     old = L.xamg_spmv_set_variant(variant if plan is None else -1)
     try:
@@ -261,59 +272,154 @@ def spmv_roofline(csr, variant):
 TRAFFIC_RATIO = {5: 0.9457, 6: 0.9457, RUN8: 1.0287}
 
 
-def run_form(csr, B, spec, warmup, steps):
-    import xamg
-    xamg.set_nv(NV)
-    A = xamg.Matrix(csr)
-    x = xamg.Vector(csr.nrows, NV)
-    b = xamg.Vector(csr.nrows, NV)
-    b.upload(B)
-    t0 = time.time()
-    s = xamg.Solver(A, xamg.Params(spec), x, b)
-    setup_s = time.time() - t0
-    for _ in range(warmup):
-        x.set(0.0)
-        s.solve()
-    times = []
-    k0 = xamg.kernel_launches()
-    for _ in range(steps):
-        x.set(0.0)
-        s.solve()
-        times.append(s.last_ms())
-    launches = xamg.kernel_launches() - k0
-    X = x.download()
-    it = s.iters()
-    return {"ms": float(np.mean(times)), "ms_all": [round(t, 3) for t in times], "iters": it[0],
-            "sub_iters": it[1], "converged": all(s.converged()), "setup_s": round(setup_s, 1),
-            "levels": s.info(), "launches": launches}, X, (s, A, x, b)
+def plain_hybrid_spec(blocks=None):
+    """FP64 PBiCGStab + FP64 V-cycle with the mixed form's smoother split
+    (hybrid blocks, two per SM): separates the smoother's share of the mixed
+    form's gain from the FP32 share."""
+    blocks = blocks or 2 * gpu_sms()
+    s = plain_spec()
+    s["pre_smoother"]["hybrid_blocks"] = blocks
+    s["post_smoother"]["hybrid_blocks"] = blocks
+    return s
 
 
-def e2e_form(csr, B, spec, warmup, steps):
-    """Same solve through the C API with pinned host buffers, copies timed."""
-    import torch
-    import xamg
-    xamg.set_nv(NV)
-    A = xamg.Matrix(csr)
-    x = xamg.Vector(csr.nrows, NV)
-    b = xamg.Vector(csr.nrows, NV)
-    s = xamg.Solver(A, xamg.Params(spec), x, b)
-    hb = torch.from_numpy(B).pin_memory()
-    hx = torch.empty((csr.nrows, NV), dtype=torch.float64).pin_memory()
-    L = xamg.lib()
-    import ctypes as C
+def with_top(spec, **kv):
+    """A copy of spec whose top solver (meta_solver when present) has the
+    given keys changed (for Solver.renew)."""
+    import copy
+    s = copy.deepcopy(spec)
+    top = "meta_solver" if "meta_solver" in s else "solver"
+    s[top].update(kv)
+    return s
 
-    def step():
-        xamg.check(L.XAMG_vector_upload_d(C.c_void_p(hb.data_ptr()), csr.nrows, 0, NV, b.h))
-        x.set(0.0)
-        s.solve()
-        xamg.check(L.XAMG_vector_download_d(C.c_void_p(hx.data_ptr()), csr.nrows, 0, NV, x.h))
 
-    for _ in range(warmup):
-        step()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        step()
-    return (time.perf_counter() - t0) / steps * 1e3
+class Form:
+    """One solver configuration on the device with its own x and b."""
+
+    def __init__(self, csr, B, spec):
+        import xamg
+        self.nv = B.shape[1]
+        xamg.set_nv(self.nv)
+        self.spec = spec
+        self.A = xamg.Matrix(csr)
+        self.x = xamg.Vector(csr.nrows, self.nv)
+        self.b = xamg.Vector(csr.nrows, self.nv)
+        self.b.upload(B)
+        t0 = time.time()
+        self.s = xamg.Solver(self.A, xamg.Params(spec), self.x, self.b)
+        self.setup_s = time.time() - t0
+
+    def renew(self, spec):
+        import xamg
+        self.s.renew(xamg.Params(spec))
+
+    def solve(self):
+        import xamg
+        xamg.set_nv(self.nv)
+        self.x.set(0.0)
+        self.s.solve()
+        return self.s.last_ms()
+
+    def run(self, warmup, steps):
+        import xamg
+        for _ in range(warmup):
+            self.solve()
+        k0 = xamg.kernel_launches()
+        times = [self.solve() for _ in range(steps)]
+        launches = xamg.kernel_launches() - k0
+        it = self.s.iters()
+        return {"ms": float(np.mean(times)), "ms_all": [round(t, 3) for t in times], "iters": it[0],
+                "sub_iters": it[1], "converged": all(self.s.converged()), "setup_s": round(self.setup_s, 1),
+                "launches": launches}
+
+    def e2e(self, B, warmup, steps):
+        """The same solve through the C API with the right-hand sides copied
+        in from pinned host memory and the solution copied out, every step."""
+        import ctypes as C
+        import torch
+        import xamg
+        xamg.set_nv(self.nv)
+        n = B.shape[0]
+        hb = torch.from_numpy(np.ascontiguousarray(B)).pin_memory()
+        hx = torch.empty((n, self.nv), dtype=torch.float64).pin_memory()
+        L = xamg.lib()
+
+        def step():
+            xamg.check(L.XAMG_vector_upload_d(C.c_void_p(hb.data_ptr()), n, 0, self.nv, self.b.h))
+            self.x.set(0.0)
+            self.s.solve()
+            xamg.check(L.XAMG_vector_download_d(C.c_void_p(hx.data_ptr()), n, 0, self.nv, self.x.h))
+
+        for _ in range(warmup):
+            step()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            step()
+        return (time.perf_counter() - t0) / steps * 1e3
+
+    def kernel_times(self):
+        """One more solve with the library's CUDA-event timing of the
+        Gauss-Seidel sweeps and sparse products on; per (kernel, rows)."""
+        import xamg
+        xamg.kernel_timing(True)
+        try:
+            ms = self.solve()
+            rec = xamg.kernel_timing_read()
+        finally:
+            xamg.kernel_timing(False)
+        return ms, rec
+
+
+def col_err(X, Xref):
+    """max over columns of ||x - x_ref|| / ||x_ref||"""
+    return float(np.max(np.linalg.norm(X - Xref, axis=0) / np.linalg.norm(Xref, axis=0)))
+
+
+def true_res(Ah, B, X):
+    """max over columns of ||b - A x|| / ||b|| in FP64 on the host"""
+    return float(np.max(np.linalg.norm(B - Ah @ X, axis=0) / np.linalg.norm(B, axis=0)))
+
+
+def gs_roofline(rec, solve_ms, rows):
+    """Roofline of the dominant kernel of the mixed step: the hybrid
+    Gauss-Seidel sweep kernel on the finest level (one launch per sweep
+    direction), achieved = algorithmic bytes per launch / CUDA-event time per
+    launch."""
+    peak, src = peak_hbm()
+    tot = {k: sum(r["ms"] for r in rec if r["kernel"] == k) for k in ("gs", "spmv")}
+    fine = [r for r in rec if r["kernel"] == "gs" and r["rows"] == rows]
+    if not fine:
+        return None
+    f = fine[0]
+    per_ms = f["ms"] / f["launches"]
+    per_b = f["bytes"] / f["launches"]
+    ach = per_b / (per_ms * 1e-3) / 1e9
+    levels = {}
+    for r in rec:
+        levels.setdefault(r["kernel"], []).append(
+            {"rows": r["rows"], "launches": r["launches"], "ms": round(r["ms"], 3),
+             "gbs": round(r["bytes"] / (r["ms"] * 1e-3) / 1e9, 1) if r["ms"] > 0 else None})
+    return {"bound": "hbm", "kernel": "k_gs3<float,16,1,0> (hybrid blocks, finest level)",
+            "achieved": round(ach, 1), "peak": peak, "peak_source": src, "unit": "GB/s",
+            "frac": round(ach / peak, 4), "traffic": None,
+            "algorithmic_bytes": round(per_b), "launch_ms": round(per_ms, 4), "launches": f["launches"],
+            "share_of_step": {"gs_all_levels": round(tot["gs"] / solve_ms, 3),
+                              "spmv_all_operators": round(tot["spmv"] / solve_ms, 3),
+                              "finest_gs": round(f["ms"] / solve_ms, 3)},
+            "per_level": levels, "timed_solve_ms": round(solve_ms, 3)}
+
+
+def bench_config(csr, world):
+    """The workload as both arms report it."""
+    return {"workload": "27pt-aniso-128^3 AMG-PBiCGStab nv=16", "n": N_GRID, "nv": NV, "rows": csr.nrows,
+            "nnz": csr.nnz, "parallelism": "replicas" if world > 1 else "1gpu",
+            "l2": "inputs larger than L2 (matrix 669 MB)"}
+
+
+def oracle_mod():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    return orc
 
 
 def batch_form(rank, world, warmup, steps):
@@ -394,57 +500,71 @@ def cpu_sample(csr, B, s_plain):
     """One FP64 PBiCGStab iteration of the oracle (the reference's
     single-process order: Gauss-Seidel sequential, products, inner products
     and vector updates on all host threads) on the same matrix, RHS and
-    hierarchy; per-iteration time x the GPU iteration count estimates
-    time-to-solution.  Returns (seconds, threads)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as orc
+    hierarchy as the GPU's plain form.  Returns (seconds, threads, x, history)
+    so that the GPU's first iteration can be compared bit for bit."""
+    orc = oracle_mod()
     rp, ci, v = csr.arrays()
     levels = [s_plain.level(l) for l in range(s_plain.num_levels())]
     mg = orc.MG(levels)
     t0 = time.perf_counter()
-    orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg=mg, max_iters=1, rel_tol=1e-8)
-    return time.perf_counter() - t0, orc.num_threads()
+    x, it, hist, _, _ = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg=mg, max_iters=1, rel_tol=1e-8)
+    return time.perf_counter() - t0, orc.num_threads(), x, hist
+
+
+class Rows:
+    """Row count and nnz of the generated operator (the reference arm's config)."""
+
+    def __init__(self, rp):
+        self.nrows = len(rp) - 1
+        self.nnz = int(rp[-1])
 
 
 def reference_arm(args, rank, world):
+    """The reference's method on the host cores, through the oracle alone
+    (the reference needs MPI, hypre, argsparser and yaml-cpp and cannot be
+    built here): the same 27-point operator and right-hand sides, the
+    oracle's own AMG setup (its restatement of the hypre algorithms the
+    reference configures), and one complete FP64 AMG-PBiCGStab solve to 1e-8
+    timed end to end.  Loads no product library and touches no GPU."""
     if rank != 0:
         return
-    import xamg
-    xamg.set_nv(NV)  # host-only: generator, AMG setup and the oracle need no device
-    csr, B = build_problem()
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as orc
-    rp, ci, v = csr.arrays()
-    spec = plain_spec()
-    lv = xamg.amg_host(csr, xamg.Params(spec))
-    mg = orc.MG(lv)
-    per_iter = []
-    # one sampled iteration per step, at most 3 (each takes tens of seconds)
-    for _ in range(min(max(args.steps, 1), 3)):
-        t0 = time.perf_counter()
-        orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg=mg, max_iters=1, rel_tol=1e-8)
-        per_iter.append(time.perf_counter() - t0)
-    # iterations to 1e-8 of this FP64 method on this workload: 4, the count of
-    # the GPU parity form, whose arithmetic is identical bit for bit (a full
-    # oracle solve would take minutes per step)
-    iters = args.ref_iters
-    ms_rhs = float(np.mean(per_iter)) * iters / NV * 1e3
+    orc = oracle_mod()
+    t0 = time.perf_counter()
+    rp, ci, v = orc.gen27(N_GRID, 1.0, 1.0, 1e-3)
+    B = np.random.default_rng(SEED).uniform(-1.0, 1.0, (len(rp) - 1, NV))
+    p = plain_spec()["preconditioner"]
+    levels = orc.amg_setup(rp, ci, v, **{k: p[k] for k in ("mg_coarsening_type", "mg_strength_threshold",
+                                                           "mg_max_levels")})
+    mg = orc.MG(levels)
+    setup_s = time.perf_counter() - t0
+    # one complete solve is the timed unit (about two minutes on the host);
+    # the steps/warmup of the GPU arm do not apply to it
+    t0 = time.perf_counter()
+    x, it, hist, st, _ = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg=mg, max_iters=200, rel_tol=1e-8)
+    sec = time.perf_counter() - t0
+    ms_rhs = sec / NV * 1e3
+    thr = orc.num_threads()
     line = {"impl": "reference", "metric": "time-to-1e-8 residual per RHS", "value": round(ms_rhs, 3),
             "unit": "ms/RHS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": False, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "27pt-aniso-128^3 AMG-PBiCGStab nv=16", "n": N_GRID, "nv": NV},
-            "cpu_baseline": {"value": round(ms_rhs, 3), "unit": "ms/RHS", "cores": orc.num_threads(), "kind": "port",
-                             "sample": "%d timed single PBiCGStab iterations (FP64 oracle on %d host threads, "
-                                       "Gauss-Seidel sweeps sequential), x %d iterations"
-                             % (len(per_iter), orc.num_threads(), iters)},
+            "config": bench_config(Rows(rp), world), "form": "plain FP64 (oracle on the host)",
+            "iters": int(it), "converged": bool(np.all(st > 0)), "setup_s": round(setup_s, 1),
+            "levels": [l["n"] for l in levels],
+            "cpu_baseline": {"value": round(ms_rhs, 3), "unit": "ms/RHS", "cores": thr, "kind": "port",
+                             "sample": "one complete FP64 AMG-PBiCGStab solve of the 16 RHS to 1e-8 (%d iterations, "
+                                       "%.1f s) by the oracle on %d host threads, Gauss-Seidel sweeps sequential; "
+                                       "oracle AMG setup (%.1f s) untimed" % (it, sec, thr, setup_s)},
             "e2e": {"value": round(ms_rhs, 3), "unit": "ms/RHS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def kernel_case(args):
     """One hot kernel alone on a grid of side --n (for profiler captures):
-    spmv = the NV=16 FP64 CSR product (variant --variant), gs = one forward +
-    backward sequential Gauss-Seidel sweep (cooperative level-ordered kernel)."""
+    spmv = the NV=16 product in precision --prec and mode --mode (variant
+    --variant; 108 = run kernel); gs = one Gauss-Seidel call (forward and
+    backward sweep) in precision --prec, sequential order (--blocks 0, one
+    cooperative level-ordered launch per sweep) or --blocks hybrid blocks
+    (one CTA per block, one launch per sweep direction)."""
     import ctypes as C
     import torch
     import xamg
@@ -453,37 +573,76 @@ def kernel_case(args):
     xamg.init(NV)
     csr, B = build_problem()
     if args.kernel == "spmv":
-        ms = spmv_time(csr, 0, args.variant, iters=args.steps)
-        print(json.dumps({"kernel": "spmv", "n": args.n, "variant": args.variant, "ms": round(ms, 4)}))
+        ms = spmv_time(csr, args.prec, args.variant, iters=args.steps, mode=args.mode)
+        print(json.dumps({"kernel": "spmv", "n": args.n, "variant": args.variant, "prec": args.prec,
+                          "mode": args.mode, "ms": round(ms, 4)}))
         return
     L = xamg.lib()
     rp, ci, v = csr.arrays()
     n = csr.nrows
-    plan = L.xamg_gs_plan_create(n, xamg._ptr(rp), xamg._ptr(ci), 0, 1)
-    assert plan
+    brows = -(-n // args.blocks) if args.blocks > 0 else 0
+    plan = L.xamg_gs_plan_create(n, xamg._ptr(rp), xamg._ptr(ci), brows, 1)
+    assert plan, L.XAMG_b200_last_error()
     try:
-        xamg.check(L.xamg_gs_plan_set_values(plan, xamg._ptr(np.ascontiguousarray(v)), 0))
+        xamg.check(L.xamg_gs_plan_set_values(plan, xamg._ptr(np.ascontiguousarray(v)), args.prec))
+        dt = np.float64 if args.prec == 0 else np.float32
         rows = np.repeat(np.arange(n), np.diff(rp))
         diag = ci == rows
         invd = np.zeros(n)
         invd[rows[diag]] = 1.0 / v[diag]
-        d = [torch.from_numpy(a).cuda() for a in (rp, ci, v, invd, B, np.zeros_like(B), np.ones(NV))]
+        if args.prec == 1:
+            invd = (1.0 / v[diag].astype(np.float32).astype(np.float64)).astype(np.float32)
+        d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in
+             (rp, ci, v.astype(dt), invd.astype(dt), B.astype(dt), np.zeros_like(B, dtype=dt),
+              np.full(NV, 0.99, dt), np.zeros_like(B, dtype=dt))]
         P = lambda t: C.c_void_p(t.data_ptr())
         times = []
         for _ in range(args.warmup + args.steps):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            xamg.check(L.xamg_hsgs(plan, 0, NV, P(d[0]), P(d[1]), P(d[2]), P(d[3]), P(d[4]), P(d[5]),
-                                   P(d[6]), None, None))
+            xamg.check(L.xamg_hsgs(plan, args.prec, NV, P(d[0]), P(d[1]), P(d[2]), P(d[3]), P(d[4]), P(d[5]),
+                                   P(d[6]), P(d[7]) if brows else None, None))
             xamg.check(L.XAMG_b200_synchronize())
             e1.record()
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1))
         assert L.xamg_gs_plan_error(plan) == 0
-        print(json.dumps({"kernel": "gs", "n": args.n, "ms": round(float(np.mean(times[args.warmup:])), 4)}))
+        print(json.dumps({"kernel": "gs", "n": args.n, "prec": args.prec, "blocks": args.blocks,
+                          "ms": round(float(np.mean(times[args.warmup:])), 4)}))
     finally:
         L.xamg_gs_plan_destroy(plan)
+
+
+SWEEP_NV = (1, 4, 8, 16, 32)
+
+
+def precision_sweep(csr, Ah, warmup, steps):
+    """Precision form over nv in {1, 4, 8, 16, 32} (the first nv columns of a
+    32-column uniform[-1,1] block): iterations, time per solve and per RHS,
+    true residual and error against an FP64 solve of the same columns
+    converged to 1e-12."""
+    import xamg
+    B32 = np.random.default_rng(SEED + 1).uniform(-1.0, 1.0, (csr.nrows, 32))
+    ref = Form(csr, B32, with_top(plain_hybrid_spec(), rel_tolerance=1e-12))
+    ref.solve()
+    Xref = ref.x.download()
+    ref_info = {"iters": ref.s.iters()[0], "converged": all(ref.s.converged()),
+                "true_rel_residual": true_res(Ah, B32, Xref)}
+    del ref
+    out = []
+    for nv in SWEEP_NV:
+        Bn = np.ascontiguousarray(B32[:, :nv])
+        f = Form(csr, Bn, mixed_spec())
+        r = f.run(warmup, steps)
+        X = f.x.download()
+        out.append({"nv": nv, "ms": round(r["ms"], 3), "ms_per_rhs": round(r["ms"] / nv, 4),
+                    "outer_iters": r["iters"], "inner_iters": r["sub_iters"], "converged": r["converged"],
+                    "true_rel_residual": true_res(Ah, Bn, X), "err_vs_fp64": col_err(X, Xref[:, :nv]),
+                    "setup_s": r["setup_s"]})
+        del f
+    xamg.set_nv(NV)
+    return {"fp64_reference": ref_info, "points": out}
 
 
 def main():
@@ -492,13 +651,16 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--forms", default="plain,mixed,batch,learned")
+    ap.add_argument("--forms", default="plain,plain_hybrid,mixed,mixed_tight,sweep,batch,learned")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--ref-iters", type=int, default=4,
-                    help="PBiCGStab iterations to 1e-8 on the benchmark problem (scales the sampled iteration)")
+    ap.add_argument("--tight-tol", type=float, default=1e-10,
+                    help="outer tolerance of the mixed form run to the error target (error vs FP64 <= 1e-8)")
     ap.add_argument("--kernel", choices=["spmv", "gs"], help="time one hot kernel alone (profiling)")
     ap.add_argument("--n", type=int, default=96, help="grid side of --kernel")
     ap.add_argument("--variant", type=int, default=-1, help="SpMV variant of --kernel spmv")
+    ap.add_argument("--prec", type=int, default=0, help="precision of --kernel (0 FP64, 1 FP32)")
+    ap.add_argument("--blocks", type=int, default=0, help="hybrid blocks of --kernel gs (0: sequential order)")
+    ap.add_argument("--mode", type=int, default=0, help="mode of --kernel spmv (0 y=Ax, 1 y+=Ax, 2 y=b-Ax)")
     ap.add_argument("--spmv", type=int, default=None,
                     help="use this SpMV kernel instead of tuning (0-6: CSR variants, 108: run kernel)")
     args = ap.parse_args()
@@ -516,37 +678,104 @@ def main():
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    import scipy.sparse as sp
     import xamg
     xamg.init(NV)
     csr, B = build_problem()
+    rp, ci, v = csr.arrays()
+    Ah = sp.csr_matrix((v, ci, rp), shape=(csr.nrows, csr.nrows))
     if args.spmv is not None:  # fixed kernel (profiler runs: timing under a profiler misleads the tuner)
         best_var, var_ms = args.spmv, {}
     else:
         best_var, var_ms = tune_spmv(csr, 0)
     apply_spmv_choice(best_var)
     allforms = args.forms.split(",")
-    forms = [f for f in allforms if f in ("plain", "mixed")]
-    res = {}
-    keep = {}
-    X = {}
+    specs = {"plain": plain_spec(), "plain_hybrid": plain_hybrid_spec(), "mixed": mixed_spec()}
+    forms = [f for f in allforms if f in specs]
+    res, X, objs = {}, {}, {}
     clocks = None
     for f in forms:
-        spec = plain_spec() if f == "plain" else mixed_spec()
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
+        fo = Form(csr, B, specs[f])
         with Clocks(local) as ck:
-            r, Xf, k = run_form(csr, B, spec, args.warmup, args.steps)
-        res[f], keep[f], X[f] = r, k, Xf
+            r = fo.run(args.warmup, args.steps)
         r["clocks"] = ck.summary()
-        if f == forms[-1]:
-            clocks = r["clocks"]
+        X[f] = fo.x.download()
+        r["true_rel_residual"] = true_res(Ah, B, X[f])
+        res[f] = r
+        objs[f] = fo
     if dist:
         t = torch.tensor([res[f]["ms"] for f in forms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         for i, f in enumerate(forms):
             res[f]["ms"] = float(t[i])
+    best = min(forms, key=lambda f: res[f]["ms"])
+    clocks = res[best]["clocks"]
+    parity = {}
+    fp64 = None
+    # FP64 solution converged to 1e-12 (the plain form's arithmetic, hybrid
+    # smoother): the yardstick of every form's error
+    ref_form = objs.get("plain_hybrid") or objs.get("plain")
+    if ref_form is not None and rank == 0:
+        ref_form.renew(with_top(ref_form.spec, rel_tolerance=1e-12))
+        ref_form.solve()
+        fp64 = ref_form.x.download()
+        parity["fp64_reference"] = {"form": "plain_hybrid" if "plain_hybrid" in objs else "plain",
+                                    "iters": ref_form.s.iters()[0],
+                                    "true_rel_residual": true_res(Ah, B, fp64)}
+        ref_form.renew(ref_form.spec)
+        for f in forms:
+            res[f]["err_vs_fp64"] = col_err(X[f], fp64)
     extra = {}
+    # the precision form run to the error target: outer refinement to a
+    # tighter residual so that the error against the FP64 solution is <= 1e-8
+    if "mixed_tight" in allforms and "mixed" in objs and rank == 0:
+        fo = objs["mixed"]
+        fo.renew(with_top(fo.spec, rel_tolerance=args.tight_tol))
+        r = fo.run(args.warmup, args.steps)
+        Xt = fo.x.download()
+        r.update(outer_rel_tolerance=args.tight_tol, true_rel_residual=true_res(Ah, B, Xt),
+                 ms_per_rhs=round(r["ms"] / NV, 4))
+        if fp64 is not None:
+            r["err_vs_fp64"] = col_err(Xt, fp64)
+            r["meets_err_1e-8"] = r["err_vs_fp64"] <= 1e-8
+        fo.renew(fo.spec)
+        extra["mixed_tight"] = r
+    # kernel time shares of the headline step and the roofline of its
+    # dominant kernel (CUDA events around every sweep and product of one solve)
+    roof_gs = None
+    if best in objs:
+        ms_t, rec = objs[best].kernel_times()
+        roof_gs = gs_roofline(rec, ms_t, csr.nrows)
+    # e2e: host right-hand sides in, host solution out, through the C API
+    e2e = {}
+    for f in (best, "plain"):
+        if f in objs and f not in e2e:
+            e2e[f] = round(objs[f].e2e(B, 1, max(2, args.steps // 2) if f != "plain" else 2) / NV, 4)
+    # parity of the plain form at full size: the GPU's first iteration against
+    # the oracle's on the same hierarchy (x and residual history, bit for bit)
+    cpu = None
+    if rank == 0 and not args.no_cpu and "plain" in objs:
+        fo = objs["plain"]
+        sec, thr, xo, ho = cpu_sample(csr, B, fo.s)
+        fo.renew(with_top(fo.spec, max_iters=1))
+        fo.solve()
+        xg, hg = fo.x.download(), fo.s.history()
+        fo.renew(fo.spec)
+        same_x, same_h = bool(np.array_equal(xg, xo)), bool(np.array_equal(hg, ho))
+        parity["c2_iter1"] = "bit-exact" if (same_x and same_h) else "differs"
+        parity["c2_iter1_detail"] = {"x_identical": same_x, "history_identical": same_h,
+                                     "x_max_rel_diff": float(np.max(np.abs(xg - xo)) / np.max(np.abs(xo))),
+                                     "history_rows": int(len(ho))}
+        iters = res["plain"]["iters"]
+        cpu = {"value": round(sec * iters / NV * 1e3, 3), "unit": "ms/RHS", "cores": thr, "kind": "port",
+               "sample": "1 FP64 PBiCGStab iteration of the same problem and hierarchy on %d host threads "
+                         "(Gauss-Seidel sweeps sequential) (%.1f s), x %d iterations / %d RHS" % (thr, sec, iters, NV)}
+    objs.clear()
+    if "sweep" in allforms and rank == 0:
+        extra["precision_sweep"] = precision_sweep(csr, Ah, 1, 3)
     if "batch" in allforms:
         extra["batch"] = batch_form(rank, world, args.warmup, args.steps)
         if dist:
@@ -559,47 +788,27 @@ def main():
         extra["batch"]["ms_per_rhs"] = round(extra["batch"]["ms"] / tot, 4)
     if "learned" in allforms and rank == 0:
         extra["learned"] = learned_form()
-    best = min(forms, key=lambda f: res[f]["ms"])
-    spec_best = plain_spec() if best == "plain" else mixed_spec()
-    e2e_ms = e2e_form(csr, B, spec_best, 1, max(2, args.steps // 2))
     roof = spmv_roofline(csr, best_var)
     roof["variants_ms"] = {str(k): round(v, 4) for k, v in var_ms.items()}
-    err = None
-    if "plain" in X and "mixed" in X:
-        err = float(np.linalg.norm(X["mixed"] - X["plain"]) / np.linalg.norm(X["plain"]))
-    # FP64 check of every form's solution on the host: max over columns of
-    # ||b - A x|| / ||b||
-    true_res = {}
-    if rank == 0:
-        import scipy.sparse as sp
-        rp, ci, v = csr.arrays()
-        Ah = sp.csr_matrix((v, ci, rp), shape=(csr.nrows, csr.nrows))
-        for f, Xf in X.items():
-            R = B - Ah @ Xf
-            true_res[f] = float(np.max(np.linalg.norm(R, axis=0) / np.linalg.norm(B, axis=0)))
-    cpu = None
-    if rank == 0 and not args.no_cpu and "plain" in keep:
-        sec, thr = cpu_sample(csr, B, keep["plain"][0])
-        iters = res["plain"]["iters"]
-        cpu = {"value": round(sec * iters / NV * 1e3, 3), "unit": "ms/RHS", "cores": thr, "kind": "port",
-               "sample": "1 FP64 PBiCGStab iteration of the same problem and hierarchy on %d host threads "
-                         "(Gauss-Seidel sweeps sequential) (%.1f s), x %d iterations / %d RHS" % (thr, sec, iters, NV)}
+    if roof_gs is not None:
+        roof_gs["spmv"] = roof
+        roofline = roof_gs
+    else:
+        roofline = roof
     value = res[best]["ms"] / (NV * world) if world > 1 else res[best]["ms"] / NV
     line = {
         "metric": "time-to-1e-8 residual per RHS", "value": round(value, 4), "unit": "ms/RHS",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(res[best]["ms"], 3), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if best == "plain" else "f32+f64",
-        "data": "synthetic",
-        "config": {"workload": "27pt-aniso-128^3 AMG-PBiCGStab nv=16", "n": N_GRID, "nv": NV,
-                   "rows": csr.nrows, "nnz": csr.nnz, "parallelism": "replicas" if world > 1 else "1gpu",
-                   "form": best, "l2": "inputs larger than L2 (matrix 669 MB)"},
-        "forms": dict({f: {k: res[f][k] for k in ("ms", "iters", "sub_iters", "converged", "setup_s", "launches")}
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if best.startswith("plain") else "f32+f64",
+        "data": "synthetic", "config": bench_config(csr, world), "form": best,
+        "forms": dict({f: {k: res[f][k] for k in ("ms", "iters", "sub_iters", "converged", "setup_s", "launches",
+                                                   "true_rel_residual", "err_vs_fp64") if k in res[f]}
                        for f in forms}, **extra),
-        "mixed_vs_plain_rel_err": err, "true_rel_residual": true_res,
-        "e2e": {"value": round(e2e_ms / NV, 4), "unit": "ms/RHS", "h2d_bytes_per_step": csr.nrows * NV * 8,
-                "d2h_bytes_per_step": csr.nrows * NV * 8},
-        "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+        "parity": parity,
+        "e2e": {"value": e2e.get(best), "unit": "ms/RHS", "h2d_bytes_per_step": csr.nrows * NV * 8,
+                "d2h_bytes_per_step": csr.nrows * NV * 8, "by_form": e2e},
+        "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
         "gpu_launches": res[best]["launches"],
     }
     if rank == 0:

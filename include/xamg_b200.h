@@ -31,6 +31,18 @@ const char *XAMG_b200_last_error(void);
 int XAMG_b200_synchronize(void);
 /* Kernels launched by this library since it was loaded (every launcher counts). */
 long long XAMG_b200_kernel_launches(void);
+/* CUDA-event timing of the hot kernels inside solves (an extension; off by
+ * default, it adds two event records per timed launch): on = 1 starts
+ * recording every Gauss-Seidel sweep (class 0) and sparse product (class 1)
+ * with its algorithmic bytes, on = 0 stops and discards; returns the previous
+ * state. */
+int XAMG_b200_kernel_timing(int on);
+/* Waits for the device, then writes per (class, operator rows) the launch
+ * count, total milliseconds and total algorithmic bytes of the records so far
+ * (at most cap groups) and clears them; returns the number of groups, or a
+ * negative error code. */
+int XAMG_b200_kernel_timing_read(int cap, int *kclass, int64_t *rows, int64_t *launches, double *ms,
+                                 double *bytes);
 /* Raw device pointer of a device-resident vector (FP64, size x nv). */
 void *XAMG_b200_vector_device_ptr(XAMG_vector_id vid);
 /* Convergence detail of the last solve: squared residual norms after each
@@ -217,8 +229,8 @@ int64_t xamg_dot_part_size(int64_t n, int nd, int nv);
 int xamg_dot(int prec, int nv, int64_t n, int nd, const void *const *a, const void *const *b,
              double *part, double *out, void *stream);
 
-/* Allocation-free inner products.  This entry point has no counterpart in
- * the reference.  It returns exactly what xamg_dot returns, for callers that
+/* Allocation-free inner products (nd = 1..4 pairs).  This entry point has no
+ * counterpart in the reference.  It returns exactly what xamg_dot returns, for callers that
  * cannot allocate device memory when they need the result (a plug-in that is
  * handed only its input and output buffers, a latency-critical loop where
  * cudaMalloc's implicit synchronisation is not acceptable): the partial sums
@@ -226,9 +238,9 @@ int xamg_dot(int prec, int nv, int64_t n, int nd, const void *const *a, const vo
  * every GPU that loads the library until the process exits.  Limit:
  * xamg_dot_part_size(n, nd, nv) <= 1048576, else code 2 and nothing runs.
  * All calls share that array, so calls that overlap on the GPU race; calls on
- * one stream are safe.  The first call on a device looks up the array's
- * address with that device current; make it before any stream capture.
- * stream NULL means the legacy default stream. */
+ * one stream are safe.  The first call in a CUDA context looks up the array's
+ * address with that context current; make it before any stream capture.
+ * stream NULL means the library's own stream, as for xamg_dot. */
 int xamg_dot_noalloc(int prec, int nv, int64_t n, int nd, const void *const *a,
                      const void *const *b, double *out, void *stream);
 

@@ -55,6 +55,14 @@ def lib():
             "orc_num_threads": (C.c_int, []),
             "orc_set_num_threads": (None, [C.c_int]),
             "orc_pcg_d": (C.c_int, [i64, P, P, P, P, P, P, C.c_int, C.c_int, C.c_double, C.c_double, P, C.c_int, P, P]),
+            "orc_gen27_size": (None, [i64, P, P]),
+            "orc_gen27": (None, [i64, C.c_double, C.c_double, C.c_double, P, P, P]),
+            "orc_amg_setup": (P, [i64, P, P, P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_double,
+                                  C.c_int]),
+            "orc_amg_num_levels": (C.c_int, [P]),
+            "orc_amg_level_info": (None, [P, C.c_int, P]),
+            "orc_amg_level_export": (None, [P, C.c_int, P, P, P, P, P, P]),
+            "orc_amg_destroy": (None, [P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -267,3 +275,49 @@ def ir_pbicgstab(rp, ci, v, b, x0, mg, max_outer=20, max_inner=200, abs_tol=0.0,
     it = f(n, p(rp), p(ci), p(v), mg.h, p(b), p(x), nv, max_outer, max_inner, abs_tol, rel_tol, inner_rel,
            p(hist), cap, p(status), p(sub))
     return x, it, hist[: it + 1], status, int(sub[0])
+
+
+def gen27(n, kx=1.0, ky=1.0, kz=1e-3):
+    """The 27-point anisotropic operator on an n^3 grid: (rp, ci, v)."""
+    rows = np.zeros(1, np.int64)
+    nnz = np.zeros(1, np.int64)
+    lib().orc_gen27_size(n, p(rows), p(nnz))
+    rp = np.zeros(int(rows[0]) + 1, np.int32)
+    ci = np.zeros(int(nnz[0]), np.int32)
+    v = np.zeros(int(nnz[0]))
+    lib().orc_gen27(n, kx, ky, kz, p(rp), p(ci), p(v))
+    return rp, ci, v
+
+
+# defaults of the reference's MultiGrid parameter family
+# (src/param/xamg_params_details.h:244-267) for the keys this setup reads
+AMG_DEFAULTS = dict(mg_max_levels=25, mg_coarse_matrix_size=100, mg_strength_threshold=0.5, mg_trunc_factor=0.25,
+                    mg_Pmax_elements=4, mg_max_row_sum=0.9, mg_coarsening_type=6)
+
+
+def amg_setup(rp, ci, v, **prm):
+    """Oracle AMG hierarchy (classical strength, Ruge-Stueben first pass [+
+    second pass for coarsening types 1/3/6], extended+i interpolation with
+    truncation, Galerkin products) from the reference's parameter keys.
+    Returns the level list in the form MG() takes."""
+    q = dict(AMG_DEFAULTS, **prm)
+    rp = np.ascontiguousarray(rp, np.int32)
+    ci = np.ascontiguousarray(ci, np.int32)
+    v = np.ascontiguousarray(v, np.float64)
+    h = lib().orc_amg_setup(len(rp) - 1, p(rp), p(ci), p(v), int(q["mg_max_levels"]), int(q["mg_coarse_matrix_size"]),
+                            float(q["mg_strength_threshold"]), float(q["mg_trunc_factor"]), int(q["mg_Pmax_elements"]),
+                            float(q["mg_max_row_sum"]), int(q["mg_coarsening_type"]))
+    out = []
+    try:
+        for l in range(lib().orc_amg_num_levels(h)):
+            info = np.zeros(4, np.int64)
+            lib().orc_amg_level_info(h, l, p(info))
+            n, nnz, ncP, nnzP = (int(t) for t in info)
+            A = (np.zeros(n + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz))
+            P = (np.zeros(n + 1, np.int32), np.zeros(nnzP, np.int32), np.zeros(nnzP)) if nnzP else None
+            lib().orc_amg_level_export(h, l, p(A[0]), p(A[1]), p(A[2]), p(P[0]) if P else None,
+                                       p(P[1]) if P else None, p(P[2]) if P else None)
+            out.append(dict(n=n, A=A, P=P, ncP=ncP))
+    finally:
+        lib().orc_amg_destroy(h)
+    return out

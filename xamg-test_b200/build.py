@@ -72,10 +72,14 @@ def build_library(verbose=False):
     return LIB
 
 
+ORACLE_SOURCES = ["oracle.cpp", "amg_oracle.cpp"]
+
+
 def build_oracle():
-    src = os.path.join(ROOT, "oracle", "oracle.cpp")
-    if _newer(src, ORACLE_LIB):
-        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-o", ORACLE_LIB, src])
+    srcs = [os.path.join(ROOT, "oracle", s) for s in ORACLE_SOURCES]
+    if any(_newer(s, ORACLE_LIB) for s in srcs):
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-o", ORACLE_LIB,
+              *srcs])
     return ORACLE_LIB
 
 

@@ -901,6 +901,10 @@ namespace xamg {
 // Record the text returned by XAMG_b200_last_error() (used by entry points
 // that live outside this file).
 void set_last_error(const std::string &msg) { g_err = msg; }
+// The stream that a NULL stream argument means for every kernel-level entry
+// point: the library's own non-blocking stream (created on first use; a
+// stream holds no device allocation of this library).
+cudaStream_t library_stream() { return ctx().stream; }
 }  // namespace xamg
 
 // ---- batching form (no counterpart in the reference) -----------------------
@@ -942,6 +946,13 @@ long long XAMG_b200_batch_last_kernels(size_t bid) {
     return blist[bid]->last_kernels;
 }
 long long XAMG_b200_kernel_launches(void) { return xk::launch_count(); }
+int XAMG_b200_kernel_timing(int on) { return ktime_enable(on); }
+int XAMG_b200_kernel_timing_read(int cap, int *kclass, int64_t *rows, int64_t *launches, double *ms,
+                                 double *bytes) {
+    int g = -1;
+    int rc = guard([&] { g = ktime_read(cap, kclass, rows, launches, ms, bytes); });
+    return rc ? -rc : g;
+}
 int XAMG_b200_batch_groups(size_t bid, int *out, int cap) {
     if (bid >= blist.size() || !blist[bid]) return -2;
     const Batch *B = blist[bid];

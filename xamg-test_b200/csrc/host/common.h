@@ -95,4 +95,18 @@ struct Context {
 };
 Context &ctx();
 
+// Optional CUDA-event timing of the hot kernels inside solves (off unless
+// enabled through XAMG_b200_kernel_timing).  A record is one launch: its
+// kernel class, the rows of its operator, its algorithmic bytes and the
+// event pair around it on the launching stream.
+enum class KClass : int { GS = 0, SPMV = 1 };
+bool ktime_on();
+struct KTimeScope {
+    bool on;
+    int slot = -1;
+    KTimeScope(KClass k, i64 rows, double bytes, cudaStream_t s);
+    ~KTimeScope();
+    cudaStream_t s;
+};
+
 }  // namespace xamg

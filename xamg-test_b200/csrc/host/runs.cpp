@@ -161,11 +161,18 @@ void RunPlan::add_values(const HostCsr &h, Prec p) {
 
 void DCsr::spmv(Prec p, int nv, const void *x, void *y, int mode, const void *b, cudaStream_t s) const {
     const int var = xk::get_spmv_variant();
+    const double sv = (double)prec_size(p);
+    // x read once, y written, y or b read for modes 1 and 2
+    const double xy = (double)ncols * nv * sv + (double)n * nv * sv * (mode >= 1 ? 2 : 1);
     if ((var < 0 || var == 7) && runs.has(p) && xk::spmv_runs_supported(p, nv)) {
+        // run format: values once, 4 B per segment, 20 B per chunk (descriptor
+        // and its share of the tile offsets)
+        KTimeScope kt(KClass::SPMV, n, (double)nnz * sv + 4.0 * runs.nseg + 20.0 * runs.nchunks + xy, s);
         xk::spmv_runs(p, nv, runs.nchunks, runs.ntiles, runs.chunks.as<int4>(), runs.toff.as<longlong2>(),
                       runs.sg.as<int>(), p == Prec::F64 ? runs.v64.p : runs.v32.p, x, y, mode, b, s);
         return;
     }
+    KTimeScope kt(KClass::SPMV, n, (double)nnz * (sv + 4) + (double)(n + 1) * 4 + xy, s);
     xk::spmv(p, nv, n, rpp(), cip(), val(p), x, y, mode, b, s);
 }
 

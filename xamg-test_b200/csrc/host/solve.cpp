@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <set>
+#include <tuple>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -19,6 +20,83 @@ Context &ctx() {
 }
 
 static bool quiet() { return std::getenv("XAMG_QUIET") != nullptr; }
+
+// ------------------------------------------------------------ kernel timing
+namespace {
+struct KRec {
+    int kclass;
+    i64 rows;
+    double bytes;
+    cudaEvent_t e0, e1;
+};
+bool g_ktime = false;
+std::vector<KRec> g_krecs;
+std::vector<cudaEvent_t> g_kpool;
+cudaEvent_t kevent() {
+    if (!g_kpool.empty()) {
+        cudaEvent_t e = g_kpool.back();
+        g_kpool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    XCUDA(cudaEventCreate(&e));
+    return e;
+}
+void kclear() {
+    for (KRec &r : g_krecs) {
+        g_kpool.push_back(r.e0);
+        g_kpool.push_back(r.e1);
+    }
+    g_krecs.clear();
+}
+}  // namespace
+
+bool ktime_on() { return g_ktime; }
+
+KTimeScope::KTimeScope(KClass k, i64 rows, double bytes, cudaStream_t st) : on(g_ktime), s(st) {
+    if (!on) return;
+    KRec r{(int)k, rows, bytes, kevent(), kevent()};
+    XCUDA(cudaEventRecord(r.e0, s));
+    slot = (int)g_krecs.size();
+    g_krecs.push_back(r);
+}
+KTimeScope::~KTimeScope() {
+    if (on && slot >= 0) cudaEventRecord(g_krecs[slot].e1, s);
+}
+
+int ktime_enable(int on) {
+    int old = g_ktime;
+    if (!on) kclear();
+    g_ktime = on != 0;
+    return old;
+}
+
+// Aggregate the records by (class, rows) after the device has finished them;
+// clears the records.  Returns the number of groups written (at most cap).
+int ktime_read(int cap, int *kclass, i64 *rows, i64 *launches, double *ms, double *bytes) {
+    XCUDA(cudaDeviceSynchronize());
+    std::map<std::pair<int, i64>, std::tuple<i64, double, double>> agg;
+    for (KRec &r : g_krecs) {
+        float t = 0.f;
+        XCUDA(cudaEventElapsedTime(&t, r.e0, r.e1));
+        auto &a = agg[{r.kclass, r.rows}];
+        std::get<0>(a) += 1;
+        std::get<1>(a) += t;
+        std::get<2>(a) += r.bytes;
+    }
+    kclear();
+    int g = 0;
+    for (auto &kv : agg) {
+        if (g >= cap) break;
+        kclass[g] = kv.first.first;
+        rows[g] = kv.first.second;
+        launches[g] = std::get<0>(kv.second);
+        ms[g] = std::get<1>(kv.second);
+        bytes[g] = std::get<2>(kv.second);
+        ++g;
+    }
+    return g;
+}
 
 static int sm_count() {
     static int sms = 0;
@@ -234,6 +312,9 @@ void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
         for (int j = A.rp[i]; j < A.rp[i + 1]; ++j)
             if (A.ci[j] == i) dinv[i] = p == Prec::F64 ? 1.0 / A.v[j] : (double)(float)(1.0 / (double)(float)A.v[j]);
     auto inblk = [&](i64 i, i64 c) { return brows <= 0 || (c / brows) == (i / brows); };
+    nnz_in = 0;
+    for (i64 i = 0; i < n; ++i)
+        for (int j = A.rp[i]; j < A.rp[i + 1]; ++j) nnz_in += inblk(i, A.ci[j]);
     for (int d = 0; d < 2; ++d) {
         const std::vector<int> &lev = d == 0 ? lf : lb;
         std::vector<int> order;        // row id per level-ordered row (-1 = padding)
@@ -363,6 +444,10 @@ void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val
         const i64 tile = (i64)brows * nv * (i64)prec_size(p);
         int xs = md == 1 && (tile <= xk::gs_lcsr_xs_bytes_two_per_sm() ||
                              (tile <= xk::gs_lcsr_max_xs_bytes() && nblocks <= sm_count()));
+        // one sweep: in-block entries (column + value), per row its id, offset
+        // and inverse diagonal, and t read, x read, x written
+        const double sv = (double)prec_size(p);
+        KTimeScope kt(KClass::GS, n, (double)nnz_in * (4 + sv) + (double)n * (8 + sv) + 3.0 * n * nv * sv, s);
         XCUDA(xk::gs_sweep_lcsr(p, nv, md, xs, L.nlev, L.ncta, L.desc.as<int>(), L.blev.as<int>(),
                                 L.lrp.as<int>(), L.lci.as<int>(), L.lva.p, L.lrow.as<int>(),
                                 L.linvd.p, t, x, relax, brows, n, bar, err, L.emax, s));

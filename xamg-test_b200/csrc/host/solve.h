@@ -106,6 +106,7 @@ struct GsPlan {
         int emax = 0;  // most entries of one CTA in one level
     } lc[2];
     bool has_lcsr = false;
+    i64 nnz_in = 0;  // entries inside the rows' blocks (all entries without blocks)
     Prec lprec = Prec::F64;
     // hybrid plans: the entries of A outside each row's block, in CSR order
     // (values in precision aprec), so that the right-hand side of the block
@@ -214,6 +215,11 @@ const GsPlan &mg_level_gs(MultiGrid *mg, int l);
 const std::vector<double> &mg_coarse_inverse(MultiGrid *mg);
 // spectrum bounds used by a level's Chebyshev smoother (0, 0 when none)
 void mg_level_eig(MultiGrid *mg, int l, double *mn, double *mx);
+
+// Kernel timing (see KTimeScope): enable/disable (returns the old state) and
+// read the per-(class, rows) aggregates.
+int ktime_enable(int on);
+int ktime_read(int cap, int *kclass, i64 *rows, i64 *launches, double *ms, double *bytes);
 
 void dense_inverse(int n, const double *A, double *Ainv);
 void csr_transpose(const HostCsr &P, HostCsr &R);

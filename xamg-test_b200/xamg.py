@@ -144,6 +144,8 @@ def lib():
             "XAMG_b200_batch_last_ms": (C.c_double, [sz]),
             "XAMG_b200_batch_last_kernels": (C.c_longlong, [sz]),
             "XAMG_b200_kernel_launches": (C.c_longlong, []),
+            "XAMG_b200_kernel_timing": (C.c_int, [C.c_int]),
+            "XAMG_b200_kernel_timing_read": (C.c_int, [C.c_int, P, P, P, P, P]),
             "XAMG_b200_batch_groups": (C.c_int, [sz, P, C.c_int]),
             "XAMG_b200_batch_destroy": (C.c_int, [sz]),
         }
@@ -168,6 +170,30 @@ def _ptr(a):
 def kernel_launches():
     """Kernels launched by the library so far (its own launch counter)."""
     return lib().XAMG_b200_kernel_launches()
+
+
+KCLASS = {0: "gs", 1: "spmv"}
+
+
+def kernel_timing(on):
+    """Start (True) or stop and discard (False) the CUDA-event timing of the
+    Gauss-Seidel sweeps and sparse products inside solves."""
+    return bool(lib().XAMG_b200_kernel_timing(int(bool(on))))
+
+
+def kernel_timing_read(cap=256):
+    """Per (kernel class, operator rows): launches, total ms and total
+    algorithmic bytes of the timed launches so far; clears the records."""
+    kc = np.zeros(cap, np.int32)
+    rows = np.zeros(cap, np.int64)
+    nl = np.zeros(cap, np.int64)
+    ms = np.zeros(cap)
+    by = np.zeros(cap)
+    g = lib().XAMG_b200_kernel_timing_read(cap, _ptr(kc), _ptr(rows), _ptr(nl), _ptr(ms), _ptr(by))
+    if g < 0:
+        check(-g)
+    return [dict(kernel=KCLASS[int(kc[i])], rows=int(rows[i]), launches=int(nl[i]), ms=float(ms[i]),
+                 bytes=float(by[i])) for i in range(g)]
 
 
 def init(nv=1):
