@@ -645,20 +645,12 @@ int XAMG_b200_amg_host_create(XAMG_csr_matrix_id cid, XAMG_param_id pid, size_t 
     return guard([&] {
         ApiCsr *c = get(mcsrlist, cid, "csr matrix");
         GlobalParams *p = get(plist, pid, "param");
-        const ParamList *pl = nullptr;
+        const char *role = nullptr;
         for (const char *r : {"preconditioner", "solver"})
             if (p->has(r) && p->get(r).has("method") && p->get(r).get_string("method") == "MultiGrid")
-                pl = &p->get(r);
-        XCHECK(pl, "no MultiGrid role in the parameter list");
-        AmgParams ap;
-        ap.max_levels = (int)pl->get_int("mg_max_levels");
-        ap.coarse_size = (int)pl->get_int("mg_coarse_matrix_size");
-        ap.theta = pl->get_float("mg_strength_threshold");
-        ap.trunc = pl->get_float("mg_trunc_factor");
-        ap.pmax = (int)pl->get_int("mg_Pmax_elements");
-        ap.max_row_sum = pl->get_float("mg_max_row_sum");
-        ap.coarsen_type = (int)pl->get_int("mg_coarsening_type");
-        ap.interp_type = (int)pl->get_int("mg_interpolation_type");
+                role = r;
+        XCHECK(role, "no MultiGrid role in the parameter list");
+        std::vector<AmgParams> ap = amg_params_for(*p, role);
         auto *h = new std::vector<AmgLevel>();
         amg_setup(c->h, ap, *h);
         amglist.push_back(h);

@@ -909,17 +909,8 @@ struct MultiGrid : Solver {
         conv.prefix = role == "preconditioner" ? "PREC" : "SOLV";
         cycle = (int)prm.get_int("mg_cycle");
         reduced = prec == Prec::F64 && prm.get_bool("mg_reduced_precision");
-        AmgParams ap;
-        ap.max_levels = (int)prm.get_int("mg_max_levels");
-        ap.coarse_size = (int)prm.get_int("mg_coarse_matrix_size");
-        ap.theta = prm.get_float("mg_strength_threshold");
-        ap.trunc = prm.get_float("mg_trunc_factor");
-        ap.pmax = (int)prm.get_int("mg_Pmax_elements");
-        ap.max_row_sum = prm.get_float("mg_max_row_sum");
-        ap.coarsen_type = (int)prm.get_int("mg_coarsening_type");
-        ap.interp_type = (int)prm.get_int("mg_interpolation_type");
         std::vector<AmgLevel> al;
-        amg_setup(A.h, ap, al);
+        amg_setup(A.h, amg_params_for(gp, role), al);
         int L = (int)al.size();
         lv.resize(L);
         for (int l = 0; l < L; ++l) {
@@ -1126,7 +1117,20 @@ struct Krylov : Solver {
     DBuf part, sc;
     Pinned hres;
     enum { RHO, S1, S2, S3, S4, ALPHA, OMEGA, BETA, C1, RES, AC, OC, ICONV, ONES, NALPHA, NOMEGA,
-           THETA, PHI, PSI, ETA, DELTA, NSC };
+           THETA, PHI, PSI, ETA, DELTA, STAT, TOLS, NSC };
+    Pinned hres_async;
+    cudaEvent_t res_ready = nullptr;
+    ~Krylov() override {
+        if (res_ready) cudaEventDestroy(res_ready);
+    }
+    xk::BicgScalars scalars() const {
+        xk::BicgScalars b;
+        b.rho = S(RHO); b.alpha = S(ALPHA); b.omega = S(OMEGA); b.beta = S(BETA); b.c1 = S(C1);
+        b.ac = S(AC); b.oc = S(OC); b.res = S(RES); b.iconv = S(ICONV); b.status = S(STAT);
+        b.tol = S(TOLS);
+        b.check = conv.check_on ? 1 : 0;
+        return b;
+    }
     double *S(int i) const { return sc.as<double>() + (size_t)i * nv; }
 
     void setup(i64 n) {
@@ -1141,9 +1145,26 @@ struct Krylov : Solver {
         for (int k = 0; k < nv; ++k) { z[ONES * nv + k] = 1.0; z[ICONV * nv + k] = 1.0; }
         XCUDA(cudaMemcpy(sc.p, z.data(), sizeof(double) * z.size(), cudaMemcpyHostToDevice));
         hres.alloc(nv);
+        hres_async.alloc(nv);
+        XCUDA(cudaEventCreateWithFlags(&res_ready, cudaEventDisableTiming));
     }
 
     const DCsr &dA() const { return A->d; }
+
+    // per-column tolerances and convergence status after the initial check,
+    // and the matching masks, for the device-side convergence bookkeeping of
+    // the fused iteration
+    void set_conv_state(cudaStream_t st) {
+        std::vector<double> h(3 * nv);
+        for (int k = 0; k < nv; ++k) {
+            h[k] = conv.status[k] ? 0.0 : 1.0;        // ICONV
+            h[nv + k] = conv.status[k] ? 1.0 : 0.0;   // STAT
+            h[2 * nv + k] = conv.tol(k);              // TOLS
+        }
+        XCUDA(cudaMemcpyAsync(S(ICONV), h.data(), sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+        XCUDA(cudaMemcpyAsync(S(STAT), h.data() + nv, sizeof(double) * 2 * nv, cudaMemcpyHostToDevice, st));
+        XCUDA(cudaStreamSynchronize(st));
+    }
 
     void read_res(int which, cudaStream_t st) {
         XCUDA(cudaMemcpyAsync(hres.h, S(which), sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
@@ -1183,45 +1204,55 @@ struct Krylov : Solver {
         conv.update(hres.h);
         conv.record();
         if (conv.check()) return;
-        set_iconv(st);
+        set_conv_state(st);
         xk::blas(prec, nv, n, xk::Op::COPY, nullptr, r0.p(), nullptr, nullptr, nullptr, r.p(), st);
         xk::blas(prec, nv, n, xk::Op::COPY, nullptr, r0.p(), nullptr, nullptr, nullptr, p.p(), st);
+        if (precond) xk::fill(prec, p_.count(), 0.0, p_.p(), st);
+        // One iteration in the reference's step order (pbicgstab.inl:108-204)
+        // as the merged groups of MergedPBiCGStab: the scalar recurrences run
+        // in the reduction stage of their inner products, s = r - alpha v
+        // zeroes s_ for the preconditioner in the same pass, x, r and the
+        // partial sums of (r, r0) are one pass, and p's update zeroes p_.
+        // The convergence masks are kept on the device; the host reads the
+        // NV residuals once per iteration while the last two kernels run.
+        const xk::BicgScalars sc = scalars();
         for (int it = 1;; ++it) {
             conv.iters = it;
             DVec *pp = &p, *ss = &s;
             if (precond) {
-                xk::fill(prec, p_.count(), 0.0, p_.p(), st);
                 M->solve_from_zero(p_, p);
                 pp = &p_;
             }
             spmv(*pp, v, st);
-            dot1(v, r0, part, S(S1), st);
-            xk::bicg_alpha(nv, S(RHO), S(S1), S(ALPHA), st);
-            xk::negate(nv, S(ALPHA), S(NALPHA), st);
-            xk::blas(prec, nv, n, xk::Op::AXPBY_Z, S(ONES), r.p(), S(NALPHA), v.p(), nullptr, s.p(), st);
+            {
+                const void *Aa[1] = {v.p()}, *Bb[1] = {r0.p()};
+                xk::dot_partials(prec, nv, n, 1, Aa, Bb, part.as<double>(), st);
+                xk::dot_reduce_epi(0, n, 1, nv, part.as<double>(), S(S1), sc, st);
+            }
+            xk::bicg_s(prec, nv, n, sc, r.p(), v.p(), s.p(), precond ? s_.p() : nullptr, st);
             if (precond) {
-                xk::fill(prec, s_.count(), 0.0, s_.p(), st);
                 M->solve_from_zero(s_, s);
                 ss = &s_;
             }
             spmv(*ss, t, st);
             {
                 const void *Aa[3] = {t.p(), t.p(), s.p()}, *Bb[3] = {s.p(), t.p(), s.p()};
-                xk::dots(prec, nv, n, 3, Aa, Bb, part.as<double>(), S(S2), st);
+                xk::dot_partials(prec, nv, n, 3, Aa, Bb, part.as<double>(), st);
+                xk::dot_reduce_epi(1, n, 3, nv, part.as<double>(), S(S2), sc, st);
             }
-            xk::bicg_omega(nv, S(S2), S(S3), S(S4), S(ALPHA), S(ICONV), S(OMEGA), S(RES), S(AC), S(OC), st);
-            xk::blas(prec, nv, n, xk::Op::AXPBYPCZ, S(AC), pp->p(), S(OC), ss->p(), S(ONES), x.p(), st);
-            read_res(RES, st);
-            conv.update(hres.h);
+            xk::bicg_xr(prec, nv, n, sc, pp->p(), ss->p(), x.p(), s.p(), t.p(), r.p(), r0.p(), part.as<double>(),
+                        st);
+            XCUDA(cudaMemcpyAsync(hres_async.h, S(RES), sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
+            XCUDA(cudaEventRecord(res_ready, st));
+            // the next direction is formed before the host has looked at the
+            // residuals; after the last iteration it is simply not used
+            xk::dot_reduce_epi(2, n, 1, nv, part.as<double>(), S(S1), sc, st);
+            xk::bicg_p(prec, nv, n, sc, r.p(), v.p(), p.p(), precond ? p_.p() : nullptr, st);
+            XCUDA(cudaEventSynchronize(res_ready));
+            conv.update(hres_async.h);
             conv.record();
             if (conv.check()) break;
             if (it >= max_iters) break;
-            set_iconv(st);
-            xk::negate(nv, S(OMEGA), S(NOMEGA), st);
-            xk::blas(prec, nv, n, xk::Op::AXPBY_Z, S(ONES), s.p(), S(NOMEGA), t.p(), nullptr, r.p(), st);
-            dot1(r, r0, part, S(S1), st);
-            xk::bicg_beta(nv, S(S1), S(RHO), S(ALPHA), S(OMEGA), S(BETA), S(C1), st);
-            xk::blas(prec, nv, n, xk::Op::AXPBYPCZ, S(ONES), r.p(), S(C1), v.p(), S(BETA), p.p(), st);
         }
         XCUDA(cudaStreamSynchronize(st));
     }

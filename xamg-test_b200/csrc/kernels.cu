@@ -1014,10 +1014,10 @@ i64 dot_part_size(i64 n, int nd, int nv) { return ((n + 255) / 256) * nd * nv; }
 
 template <class TI, int NV>
 static void dots_t(i64 n, int nd, const void *const *a, const void *const *b, double *part,
-                   double *out, cudaStream_t s) {
+                   double *out, cudaStream_t s, bool reduce = true) {
     i64 nch = (n + 255) / 256;
     if (nch == 0) {
-        cudaMemsetAsync(out, 0, sizeof(double) * nd * NV, s);
+        if (reduce) cudaMemsetAsync(out, 0, sizeof(double) * nd * NV, s);
         return;
     }
     unsigned g = (unsigned)((nch + 7) / 8);
@@ -1039,6 +1039,10 @@ static void dots_t(i64 n, int nd, const void *const *a, const void *const *b, do
         note_launch();
         k_dot1<TI, NV, 2><<<g, 256, 0, s>>>(n, nch, pr, part);
         k_dot1<TI, NV, 2><<<g, 256, 0, s>>>(n, nch, hi, part + (i64)2 * NV * nch);
+    }
+    if (!reduce) {
+        note_launch(-1);
+        return;
     }
     k_dot2<<<nd * NV, 256, 0, s>>>(nch, part, out);
 }
@@ -1245,6 +1249,233 @@ __global__ void k_neg(int nv, const double *in, double *out) {
 void negate(int nv, const double *in, double *out, cudaStream_t s) {
     note_launch();
     k_neg<<<sblocks(nv), 128, 0, s>>>(nv, in, out);
+}
+
+
+// ---------------------------------------------------------------- fused BiCGStab groups
+// The merged groups of the reference's MergedBiCGStab / MergedPBiCGStab
+// (blas_merged_bicgstab.inl: group 2 `s = r - alpha v`, group 4 `r = s -
+// omega t, rho = (r, r0)`, group 5 `x += alpha p + omega s, p = r + beta p -
+// beta omega v`) as single passes, with the scalar recurrences folded into the
+// reduction stage of the inner products.  Every element and every partial sum
+// is computed exactly as by the separate BLAS-1, dot and scalar kernels above
+// (same expressions, same chunk/lane/slot tree), so the fused iteration gives
+// the same bits.
+
+// s = 1*r + (-alpha)*v; sz (the preconditioned copy about to be formed) = 0
+template <class T, int NV>
+__global__ void __launch_bounds__(256) k_bicg_s(i64 total, const double *__restrict__ alpha,
+                                                const T *__restrict__ r, const T *__restrict__ v,
+                                                T *__restrict__ s, T *__restrict__ sz) {
+    i64 q = (i64)blockIdx.x * 256 + threadIdx.x;
+    if (q >= total) return;
+    int k = (int)(q % NV);
+    double na = dmul(-1.0, alpha[k]);
+    s[q] = (T)dadd(dmul(1.0, (double)r[q]), dmul(na, (double)v[q]));
+    if (sz) sz[q] = T(0);
+}
+
+// p = 1*r + c1*v + beta*p; pz = 0
+template <class T, int NV>
+__global__ void __launch_bounds__(256) k_bicg_p(i64 total, const double *__restrict__ c1,
+                                                const double *__restrict__ beta, const T *__restrict__ r,
+                                                const T *__restrict__ v, T *__restrict__ p, T *__restrict__ pz) {
+    i64 q = (i64)blockIdx.x * 256 + threadIdx.x;
+    if (q >= total) return;
+    int k = (int)(q % NV);
+    p[q] = (T)dadd(dadd(dmul(1.0, (double)r[q]), dmul(c1[k], (double)v[q])), dmul(beta[k], (double)p[q]));
+    if (pz) pz[q] = T(0);
+}
+
+// x = ac*pp + oc*ss + 1*x;  r = 1*s + (-omega)*t;  chunk partials of (r, r0)
+// in the layout of k_dot1 (warp = chunk of 256 rows, lane l sums rows
+// l + 32m, m = 0..7, then the lanes fold 16..1).
+template <class T, int NV>
+__global__ void __launch_bounds__(256) k_bicg_xr(i64 n, i64 nch, const double *__restrict__ ac,
+                                                 const double *__restrict__ oc, const double *__restrict__ omega,
+                                                 const T *__restrict__ pp, const T *__restrict__ ss,
+                                                 T *__restrict__ x, const T *__restrict__ s,
+                                                 const T *__restrict__ t, T *__restrict__ r,
+                                                 const T *__restrict__ r0, double *__restrict__ part) {
+    const int lane = threadIdx.x & 31;
+    const i64 c = (i64)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (c >= nch) return;
+    constexpr int V = Shape<T, NV>::V;
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+#pragma unroll 1
+    for (int m = 0; m < 8; ++m) {
+        i64 i = c * 256 + 32 * m + lane;
+        if (i >= n) continue;
+#pragma unroll
+        for (int k0 = 0; k0 < NV; k0 += V) {
+            const i64 o = i * NV + k0;
+            T a[V], b[V], xx[V], sv[V], tv[V], z[V], xo[V], ro[V];
+            ld<T, V>(pp + o, a);
+            ld<T, V>(ss + o, b);
+            ld_cg<T, V>(x + o, xx);
+            ld<T, V>(s + o, sv);
+            ld<T, V>(t + o, tv);
+            ld<T, V>(r0 + o, z);
+#pragma unroll
+            for (int e = 0; e < V; ++e) {
+                const int k = k0 + e;
+                xo[e] = (T)dadd(dadd(dmul(__ldg(ac + k), (double)a[e]), dmul(__ldg(oc + k), (double)b[e])),
+                                dmul(1.0, (double)xx[e]));
+                const double nw = dmul(-1.0, __ldg(omega + k));
+                ro[e] = (T)dadd(dmul(1.0, (double)sv[e]), dmul(nw, (double)tv[e]));
+                acc[k] = fma((double)ro[e], (double)z[e], acc[k]);
+            }
+            st<T, V>(x + o, xo);
+            st<T, V>(r + o, ro);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double v = acc[k];
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) v = dadd(v, __shfl_xor_sync(0xffffffffu, v, off));
+        if (lane == 0) part[(i64)k * nch + c] = v;
+    }
+}
+
+// Stage 2 of the inner products (the k_dot2 tree) for all nd pairs of one
+// column k per block, then that column's scalar recurrence.
+enum { EPI_ALPHA = 0, EPI_OMEGA = 1, EPI_BETA = 2 };
+template <int EPI>
+__global__ void __launch_bounds__(256) k_dot2_epi(i64 nch, int nd, int nv, const double *__restrict__ part,
+                                                  double *__restrict__ out, BicgScalars sc) {
+    __shared__ double q[256];
+    __shared__ double val[4];
+    const int k = blockIdx.x;
+    for (int d = 0; d < nd; ++d) {
+        const double *p = part + ((i64)d * nv + k) * nch;
+        double a = 0.0;
+        for (i64 c = threadIdx.x; c < nch; c += 256) a = dadd(a, p[c]);
+        q[threadIdx.x] = a;
+        __syncthreads();
+        for (int off = 128; off >= 32; off >>= 1) {
+            if (threadIdx.x < off) q[threadIdx.x] = dadd(q[threadIdx.x], q[threadIdx.x + off]);
+            __syncthreads();
+        }
+        if (threadIdx.x < 32) {
+            double v = q[threadIdx.x];
+            for (int off = 16; off >= 1; off >>= 1) v = dadd(v, __shfl_xor_sync(0xffffffffu, v, off));
+            if (threadIdx.x == 0) {
+                val[d] = v;
+                out[(i64)d * nv + k] = v;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    if (EPI == EPI_ALPHA) {  // alpha = rho / (v, r0)
+        sc.alpha[k] = __ddiv_rn(sc.rho[k], val[0]);
+    } else if (EPI == EPI_OMEGA) {  // omega = (t,s)/(t,t); res = (s,s) - omega (t,s)
+        const double s2 = val[0], s3 = val[1], s4 = val[2];
+        const double w = __ddiv_rn(s2, s3);
+        sc.omega[k] = w;
+        const double ic = sc.iconv[k];
+        sc.ac[k] = dmul(ic, sc.alpha[k]);
+        sc.oc[k] = dmul(ic, w);
+        const double rr = dmul(w, s2);
+        const double res = dadd(dmul(1.0, s4), dmul(-1.0, rr));
+        sc.res[k] = res;
+        // the host's convergence rule (sqrt(res) > tol: not converged; a
+        // column once converged stays frozen), evaluated here so that the next
+        // iteration's masks are ready without a host round trip
+        if (sc.check && sc.status[k] == 0.0 && !(__dsqrt_rn(res) > sc.tol[k])) sc.status[k] = 1.0;
+        sc.iconv[k] = sc.status[k] != 0.0 ? 0.0 : 1.0;
+    } else {  // beta = (rho'/rho)(alpha/omega); rho = rho'; c1 = -(omega beta)
+        const double s1 = val[0];
+        const double a2 = __ddiv_rn(s1, sc.rho[k]);
+        const double a3 = __ddiv_rn(sc.alpha[k], sc.omega[k]);
+        const double bt = dmul(a2, a3);
+        sc.beta[k] = bt;
+        sc.rho[k] = s1;
+        sc.c1[k] = dmul(-1.0, dmul(sc.omega[k], bt));
+    }
+}
+
+template <class T, int NV>
+static void bicg_groups_t(int grp, i64 n, const BicgScalars &sc, const void *a0, const void *a1, void *a2,
+                          const void *a3, const void *a4, void *a5, const void *a6, double *part, cudaStream_t s) {
+    const i64 tot = n * NV;
+    if (tot <= 0) return;
+    const unsigned g = (unsigned)((tot + 255) / 256);
+    note_launch();
+    if (grp == 0) {
+        k_bicg_s<T, NV><<<g, 256, 0, s>>>(tot, sc.alpha, (const T *)a0, (const T *)a1, (T *)a2, (T *)a5);
+    } else if (grp == 1) {
+        k_bicg_p<T, NV><<<g, 256, 0, s>>>(tot, sc.c1, sc.beta, (const T *)a0, (const T *)a1, (T *)a2, (T *)a5);
+    } else {
+        const i64 nch = (n + 255) / 256;
+        k_bicg_xr<T, NV><<<(unsigned)((nch + 7) / 8), 256, 0, s>>>(
+            n, nch, sc.ac, sc.oc, sc.omega, (const T *)a0, (const T *)a1, (T *)a2, (const T *)a3, (const T *)a4,
+            (T *)a5, (const T *)a6, part);
+    }
+}
+
+void bicg_s(Prec p, int nv, i64 n, const BicgScalars &sc, const void *r, const void *v, void *s_out, void *sz,
+            cudaStream_t s) {
+    if (p == Prec::F64) {
+#define F(NV) bicg_groups_t<double, NV>(0, n, sc, r, v, s_out, nullptr, nullptr, sz, nullptr, nullptr, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    } else {
+#define F(NV) bicg_groups_t<float, NV>(0, n, sc, r, v, s_out, nullptr, nullptr, sz, nullptr, nullptr, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    }
+}
+
+void bicg_p(Prec p, int nv, i64 n, const BicgScalars &sc, const void *r, const void *v, void *pv, void *pz,
+            cudaStream_t s) {
+    if (p == Prec::F64) {
+#define F(NV) bicg_groups_t<double, NV>(1, n, sc, r, v, pv, nullptr, nullptr, pz, nullptr, nullptr, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    } else {
+#define F(NV) bicg_groups_t<float, NV>(1, n, sc, r, v, pv, nullptr, nullptr, pz, nullptr, nullptr, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    }
+}
+
+void bicg_xr(Prec p, int nv, i64 n, const BicgScalars &sc, const void *pp, const void *ss, void *x, const void *sv,
+             const void *t, void *r, const void *r0, double *part, cudaStream_t s) {
+    if (p == Prec::F64) {
+#define F(NV) bicg_groups_t<double, NV>(2, n, sc, pp, ss, x, sv, t, r, r0, part, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    } else {
+#define F(NV) bicg_groups_t<float, NV>(2, n, sc, pp, ss, x, sv, t, r, r0, part, s)
+        NV_DISPATCH(nv, F)
+#undef F
+    }
+}
+
+void dot_reduce_epi(int epi, i64 n, int nd, int nv, const double *part, double *out, const BicgScalars &sc,
+                    cudaStream_t s) {
+    const i64 nch = (n + 255) / 256;
+    note_launch();
+    if (epi == EPI_ALPHA) k_dot2_epi<EPI_ALPHA><<<nv, 256, 0, s>>>(nch, nd, nv, part, out, sc);
+    else if (epi == EPI_OMEGA) k_dot2_epi<EPI_OMEGA><<<nv, 256, 0, s>>>(nch, nd, nv, part, out, sc);
+    else k_dot2_epi<EPI_BETA><<<nv, 256, 0, s>>>(nch, nd, nv, part, out, sc);
+}
+
+void dot_partials(Prec in, int nv, i64 n, int nd, const void *const *a, const void *const *b, double *part,
+                  cudaStream_t s) {
+    if (in == Prec::F64) {
+#define F(NV) dots_t<double, NV>(n, nd, a, b, part, nullptr, s, false)
+        NV_DISPATCH(nv, F)
+#undef F
+    } else {
+#define F(NV) dots_t<float, NV>(n, nd, a, b, part, nullptr, s, false)
+        NV_DISPATCH(nv, F)
+#undef F
+    }
 }
 
 }  // namespace xk

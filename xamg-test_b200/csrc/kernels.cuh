@@ -117,6 +117,31 @@ i64 dot_part_size(i64 n, int nd, int nv);
 void dots(Prec in, int nv, i64 n, int nd, const void *const *a, const void *const *b,
           double *part, double *out, cudaStream_t s);
 
+// ---- fused BiCGStab groups (one pass each, bits of the separate kernels) ---
+// Per-column device scalars of one (P)BiCGStab solve (nv doubles each).
+struct BicgScalars {
+    double *rho, *alpha, *omega, *beta, *c1, *ac, *oc, *res, *iconv, *status, *tol;
+    int check;  // 1: update status/iconv from res and tol in the omega stage
+};
+// first stage of dots() alone: chunk partials of nd pairs into part
+void dot_partials(Prec in, int nv, i64 n, int nd, const void *const *a, const void *const *b, double *part,
+                  cudaStream_t s);
+// second stage for nd pairs of every column (out[d*nv + k]) followed by the
+// scalar recurrence epi: 0 alpha = rho/out0; 1 omega = out0/out1, res =
+// out2 - omega*out0, ac/oc = iconv*alpha/omega, convergence status and the
+// next iconv; 2 beta = (out0/rho)(alpha/omega), rho = out0, c1 = -(omega*beta)
+void dot_reduce_epi(int epi, i64 n, int nd, int nv, const double *part, double *out, const BicgScalars &sc,
+                    cudaStream_t s);
+// s = r - alpha v (blas AXPBY_Z with 1 and -alpha); sz = 0 when given
+void bicg_s(Prec p, int nv, i64 n, const BicgScalars &sc, const void *r, const void *v, void *s_out, void *sz,
+            cudaStream_t s);
+// p = r + c1 v + beta p (blas AXPBYPCZ); pz = 0 when given
+void bicg_p(Prec p, int nv, i64 n, const BicgScalars &sc, const void *r, const void *v, void *pv, void *pz,
+            cudaStream_t s);
+// x = ac pp + oc ss + x; r = s - omega t; chunk partials of (r, r0) into part
+void bicg_xr(Prec p, int nv, i64 n, const BicgScalars &sc, const void *pp, const void *ss, void *x, const void *sv,
+             const void *t, void *r, const void *r0, double *part, cudaStream_t s);
+
 // ---- BLAS-1 (element type T, FP64 per-column scalars) ---------------------
 enum class Op : int {
     AXPBY_Z = 0,   // z = a*x + b*y
