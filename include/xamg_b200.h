@@ -208,6 +208,10 @@ void *xamg_gs_plan_create(int64_t n, const int *rp_host, const int *ci_host,
  * is still used for the hybrid right-hand side. */
 int xamg_gs_plan_set_values(void *plan, const double *val_host, int prec);
 int xamg_gs_plan_levels(void *plan, int *nlev /* [2] */, int *lf, int *lb);
+/* Slots of the shared-memory x window of each sweep direction of a hybrid
+ * plan with values (0: no window; the window is used when slots * nv * the
+ * value size <= 64 KB and the block's x tile does not fit in shared memory). */
+int xamg_gs_plan_slots(void *plan, int *nslots /* [2] */);
 int xamg_gs_plan_error(void *plan);
 void xamg_gs_plan_destroy(void *plan);
 /* One HSGS call: t = b - A_offblock x (when hybrid), forward then backward

@@ -302,6 +302,48 @@ def test_hsgs_blocks_without_shared_tile_bit_exact(gpu, nv):
         L.xamg_gs_plan_destroy(plan)
 
 
+@pytest.mark.parametrize("nv", [8, 16, 32])
+def test_hsgs_blocks_slot_window_bit_exact(gpu, nv):
+    """Hybrid blocks of one 56x56 plane of the 27-point operator (56^3): the
+    block's x tile is too large for shared memory, but the rows live at once
+    fit a slot window, so every x value is read from shared memory and
+    first-use rows are loaded ahead.  Same results as the oracle, and the
+    window really is the path taken."""
+    rng = np.random.default_rng(29)
+    n3 = 56
+    rp, ci, v = xamg.CsrMatrix.aniso27(n3).arrays()
+    n = len(rp) - 1
+    brows = n3 * n3
+    L = xamg.lib()
+    plan = L.xamg_gs_plan_create(n, xamg._ptr(rp), xamg._ptr(ci), brows, 1)
+    assert plan
+    try:
+        for dtype, prec in ((np.float64, 0), (np.float32, 1)):
+            xamg.check(L.xamg_gs_plan_set_values(plan, xamg._ptr(np.ascontiguousarray(v, np.float64)), prec))
+            sz = np.dtype(dtype).itemsize
+            ns = np.zeros(2, np.int32)
+            xamg.check(L.xamg_gs_plan_slots(plan, xamg._ptr(ns)))
+            if brows * nv * sz <= 170 * 1024 or ns.max() * nv * sz > 64 * 1024:
+                continue  # the tile or the gather form applies at this width
+            assert 0 < ns.max() < brows // 4
+            vv = v.astype(dtype)
+            invd = np.array([dtype(1.0 / np.float64(vv[rp[i]])) for i in range(n)], dtype)
+            b = rng.uniform(-1, 1, (n, nv)).astype(dtype)
+            x0 = rng.uniform(-1, 1, (n, nv)).astype(dtype)
+            relax = np.full(nv, 0.99, dtype)
+            for rep in range(2):  # two calls in a row on the same plan
+                dx = D(x0)
+                t = D(np.zeros((n, nv), dtype))
+                xamg.check(L.xamg_hsgs(plan, prec, nv, P(D(rp)), P(D(ci)), P(D(vv)), P(D(invd)), P(D(b)),
+                                       P(dx), P(D(relax)), P(t), None))
+                got = H(dx)
+                ref = orc.hsgs(rp, ci, vv, invd, b, x0.copy(), relax, block_rows=brows)
+                assert np.array_equal(got, ref), (dtype, rep, np.abs(got - ref).max())
+        assert L.xamg_gs_plan_error(plan) == 0
+    finally:
+        L.xamg_gs_plan_destroy(plan)
+
+
 @pytest.mark.parametrize("nv", [1, 8, 32])
 def test_jacobi_and_dense_bit_exact(gpu, nv):
     rng = np.random.default_rng(31)

@@ -9,7 +9,9 @@ the same hierarchy: identical iteration count, residual histories within
 Two smoother forms: the reference's single-process order (one Gauss-Seidel
 sweep over each whole level) and the hybrid split the benchmark's mixed form
 uses (every level cut into 296 equal blocks: Gauss-Seidel inside a block,
-Jacobi across blocks, the reference's semantics on 296 processes)."""
+Jacobi across blocks, the reference's semantics on 296 processes), and 48
+blocks, one z-plane each on the finest level, whose x tiles are too large for
+shared memory (the slot-window form of the sweep)."""
 import numpy as np
 import pytest
 
@@ -36,7 +38,7 @@ def _spec(blocks):
     }
 
 
-@pytest.mark.parametrize("blocks", [0, 296], ids=["sequential", "hybrid296"])
+@pytest.mark.parametrize("blocks", [0, 296, 48], ids=["sequential", "hybrid296", "hybrid48"])
 def test_c2_family_full_solve_parity(gpu, blocks):
     n = 48
     csr = xamg.CsrMatrix.aniso27(n, 1.0, 1.0, 1e-3)

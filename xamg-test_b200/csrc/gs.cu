@@ -13,7 +13,13 @@
 //            bounded grid barrier between levels; x lives in global memory and
 //            is read through L2 (ld.cg) because other CTAs write it.
 //   BLOCKS : CTA b owns hybrid block b; CTA barriers only.  The block's x tile
-//            is held in shared memory when it fits (XS = true).
+//            is held in shared memory when it fits (XS = true); otherwise,
+//            when the rows live at once fit, in a slot window (SL = true): every
+//            row has a shared-memory slot for its live range, entries carry slot
+//            numbers, and the old x of a row is copied into its slot
+//            kGsSlotAhead levels before its first use (cp.async, off the
+//            level's critical path); new values go to the slot and to global
+//            memory.  Failing both, each level gathers its x values.
 //
 // Every wait (grid barrier, mbarrier) is bounded by a wall-clock limit; on
 // expiry the error word is set, the CTA waits (bounded) for its own copies in
@@ -62,6 +68,10 @@ __device__ __forceinline__ void cp_async16_cg(void *dst, const void *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait_group() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 __device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parity) {
     unsigned ok;
@@ -154,6 +164,7 @@ __device__ __forceinline__ void gst(T *p, const T (&r)[V]) {
 template <class T> struct GsBuf {
     static constexpr int E = sizeof(T) == 8 ? 1024 : 1536;
     static constexpr int RB = 128;
+    static constexpr int LB = sizeof(T) == 8 ? 160 : 192;  // slot-window loads staged per level (int2 each)
 };
 
 // One level of one CTA: rows [r0, r1) and entries [e0, e1) of the
@@ -167,9 +178,10 @@ struct Desc {
 __device__ __forceinline__ int rlo(const Desc &d) { return d.r0 & ~3; }
 __device__ __forceinline__ int rspan(const Desc &d) { return ((d.r1 + 3) & ~3) - (d.r0 & ~3); }
 
-// MODE 0 = GRID, 1 = BLOCKS.  XS: x tile of the block in shared memory.
+// MODE 0 = GRID, 1 = BLOCKS.  XS: x tile of the block in shared memory; SL:
+// slot window (lci then holds slot numbers).
 // desc: GRID -> desc[l*gridDim.x + b]; BLOCKS -> desc[blev[b] + (l - l0)].
-template <class T, int NV, int MODE, bool XS>
+template <class T, int NV, int MODE, bool XS, bool SL = false>
 __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const int4 *__restrict__ desc,
                                              const int *__restrict__ blev,
                                              const int *__restrict__ lrp,
@@ -179,18 +191,24 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
                                              const T *__restrict__ linvd,
                                              const T *__restrict__ t, T *x,
                                              const T *__restrict__ relax, i64 brows, i64 n,
-                                             int eg, unsigned *gbar, int *err) {
+                                             int eg, unsigned *gbar, int *err, GsSlotWin sw) {
     constexpr int V = Sh<T, NV>::V, TPR = Sh<T, NV>::TPR, E = GsBuf<T>::E, RB = GsBuf<T>::RB;
     constexpr int NB = 3;
+    constexpr int LB = SL ? GsBuf<T>::LB : 2;
     constexpr bool CG = (MODE == 0);
+    constexpr bool TILE = XS || SL;  // every x value is read from shared memory
+    constexpr int AH = kGsSlotAhead;
     extern __shared__ __align__(128) unsigned char dyn[];
     __shared__ __align__(16) int s_ci[NB][E];
     __shared__ __align__(16) T s_va[NB][E];
     __shared__ __align__(16) int s_rp[NB][RB + 4];
     __shared__ __align__(16) int s_row[NB][RB];
+    __shared__ __align__(16) int s_sl[NB][SL ? RB : 4];
+    __shared__ __align__(16) int2 s_ld[NB][LB];
     __shared__ __align__(16) T s_di[NB][RB];
     __shared__ __align__(8) unsigned long long mbar[NB];
     __shared__ int s_stage[NB];
+    __shared__ int s_ldn[NB];
     T *xs = reinterpret_cast<T *>(dyn);
 
     const int b = blockIdx.x, tid = threadIdx.x;
@@ -199,7 +217,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
     if (MODE == 1) {
         dbase = __ldg(blev + b);
         l1 = __ldg(blev + b + 1) - dbase;
-        xbase = (i64)b * brows;
+        xbase = SL ? 0 : (i64)b * brows;
     }
     auto dget = [&](int l) -> Desc {
         int4 v = MODE == 0 ? __ldg(desc + (i64)l * gridDim.x + b) : __ldg(desc + dbase + l);
@@ -209,7 +227,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
         for (int q = 0; q < NB; ++q) mbar_init(&mbar[q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    const i64 xrows = MODE == 1 ? min((i64)brows, n - xbase) : 0;
+    const i64 xrows = MODE == 1 && XS ? min((i64)brows, n - xbase) : 0;
     if (XS) {
         const T *xg = x + xbase * NV;
         for (i64 q = tid; q < xrows * NV; q += 256) xs[q] = xg[q];
@@ -221,9 +239,13 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
     auto issue = [&](int l, const Desc &d) {
         int q = l % NB;
         int nr = rspan(d), ne = d.e1 - d.e0, ra = rlo(d);
-        if (d.r1 > d.r0 && nr <= RB && ne <= E) {
+        int2 lr = make_int2(0, 0);
+        if (SL) lr = __ldg(sw.ldd + dbase + l);
+        const int nl = lr.y - lr.x;
+        if (d.r1 > d.r0 && nr <= RB && ne <= E && nl <= LB) {
             unsigned bytes = (unsigned)ne * (4u + (unsigned)sizeof(T)) + (unsigned)(nr + 4) * 4u +
                              (unsigned)nr * 4u + (unsigned)nr * (unsigned)sizeof(T);
+            if (SL) bytes += (unsigned)nr * 4u + (unsigned)nl * 8u;
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_expect_tx(&mbar[q], bytes);
             if (ne > 0) {
@@ -233,9 +255,22 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
             bulk_g2s(&s_rp[q][0], lrp + ra, (unsigned)(nr + 4) * 4u, &mbar[q]);
             bulk_g2s(&s_row[q][0], lrow + ra, (unsigned)nr * 4u, &mbar[q]);
             bulk_g2s(&s_di[q][0], linvd + ra, (unsigned)nr * (unsigned)sizeof(T), &mbar[q]);
+            if (SL) {
+                bulk_g2s(&s_sl[q][0], sw.lslot + ra, (unsigned)nr * 4u, &mbar[q]);
+                if (nl > 0) bulk_g2s(&s_ld[q][0], sw.ld + lr.x, (unsigned)nl * 8u, &mbar[q]);
+            }
             s_stage[q] = 1;
         } else {
             s_stage[q] = 0;
+        }
+        s_ldn[q] = nl;
+    };
+    // slot window: copy the old x of the listed rows into their slots, one
+    // 16-byte piece per thread and pass (entries {-1, -1} are padding)
+    auto load_rows = [&](const int2 *lst, int cnt) {
+        for (int w = tid; w < cnt * TPR; w += 256) {
+            const int2 e = lst[w / TPR];
+            if (e.x >= 0) cp_async16_cg(xs + (i64)e.y * NV + (w % TPR) * V, x + (i64)e.x * NV + (w % TPR) * V);
         }
     };
     Desc dn1{0, 0, 0, 0}, dn2{0, 0, 0, 0};
@@ -275,7 +310,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
                 nf = true;
                 nr = row;
                 gld<T, V, CG>(t + (i64)row * NV + lane * V, nt);
-                if (!XS) gld<T, V, CG>(x + (i64)row * NV + lane * V, nx);
+                if (!TILE) gld<T, V, CG>(x + (i64)row * NV + lane * V, nx);
             }
         }
     };
@@ -289,6 +324,15 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
         }
     };
     Desc dc = l0 < l1 ? dget(l0) : Desc{0, 0, 0, 0};
+    if (SL) {
+        // rows first used in the first AH levels, then AH - 1 empty groups so
+        // that level l's rows are in the group that wait_group<AH> completes
+        const int2 pr2 = __ldg(sw.ldpre + b);
+        if (pr2.y > pr2.x) load_rows(sw.ld + pr2.x, pr2.y - pr2.x);
+        cp_async_commit();
+#pragma unroll
+        for (int g = 1; g < AH; ++g) cp_async_commit();
+    }
     if (l0 < l1) {
         wait_q(l0 % NB);
         prefetch(l0, dc);
@@ -299,6 +343,16 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
         if (issuer && l + 2 < l1) {
             issue(l + 2, dn2);
             if (l + 3 < l1) dn2 = dget(l + 3);
+        }
+        if (SL) {
+            // the rows first used AH levels from now (list staged with this level)
+            if (s_stage[q]) {
+                load_rows(&s_ld[q][0], s_ldn[q]);
+            } else {
+                const int2 lr = __ldg(sw.ldd + dbase + l);
+                if (lr.y > lr.x) load_rows(sw.ld + lr.x, lr.y - lr.x);
+            }
+            cp_async_commit();
         }
         Desc dnx{0, 0, 0, 0};
         if (l + 1 < l1) {
@@ -311,8 +365,13 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
         // without the block's x tile in shared memory (GRID, or BLOCKS whose
         // tile is too large): gather every x value this level's entries need
         // into shared memory in one parallel round trip (xs: eg entries x NV)
-        const bool gath = !XS && ok && staged && (dc.e1 - dc.e0) <= eg;
-        if (!XS) {
+        const bool gath = !TILE && ok && staged && (dc.e1 - dc.e0) <= eg;
+        if (SL) {
+            // this level's rows are in (the groups finish in order)
+            cp_async_wait_group<AH>();
+            __syncthreads();
+        }
+        if (!TILE) {
             if (gath && V * (int)sizeof(T) == 16) {
                 // 16-byte pieces: every piece is copied by cp.async straight
                 // into shared memory, all in flight together (one L2 round
@@ -361,8 +420,9 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
             } else {
                 gld<T, V, CG>(t + (i64)row * NV + lane * V, sum);
             }
-            if (XS) {
-                const T *p = xs + ((i64)row - xbase) * NV + lane * V;
+            const i64 xrow = SL ? (i64)(staged ? s_sl[q][r - ra] : __ldg(sw.lslot + r)) : (i64)row - xbase;
+            if (TILE) {
+                const T *p = xs + xrow * NV + lane * V;
 #pragma unroll
                 for (int e = 0; e < V; ++e) xo[e] = p[e];
             } else if (it == tid) {
@@ -374,14 +434,14 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
             const T di = staged ? s_di[q][r - ra] : __ldg(linvd + r);
             const int j0 = staged ? s_rp[q][r - ra] : __ldg(lrp + r);
             const int j1 = staged ? s_rp[q][r - ra + 1] : __ldg(lrp + r + 1);
-            if (staged && (XS || gath)) {
+            if (staged && (TILE || gath)) {
                 // every operand is in shared memory: a plain loop over the
                 // row's entries (the padding, column -1, is only at its tail)
                 const int o = j0 - dc.e0;
                 int m = j1 - j0;
                 while (m > 0 && s_ci[q][o + m - 1] < 0) --m;
                 const T *vr = &s_va[q][o];
-                if (XS) {
+                if (TILE) {
                     const int *cr = &s_ci[q][o];
 #pragma unroll 4
                     for (int k = 0; k < m; ++k) {
@@ -419,7 +479,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
 #pragma unroll
                 for (int k = 0; k < GB; ++k) {
                     if (c[k] >= 0) {
-                        if (XS) {
+                        if (TILE) {
                             const T *p = xs + ((i64)c[k] - xbase) * NV + lane * V;
 #pragma unroll
                             for (int e = 0; e < V; ++e) xv[k][e] = p[e];
@@ -444,13 +504,12 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
                 T cf = rmul(relax[lane * V + e], di);
                 xo[e] = fma(cf, sum[e], xo[e]);
             }
-            if (XS) {
-                T *p = xs + ((i64)row - xbase) * NV + lane * V;
+            if (TILE) {
+                T *p = xs + xrow * NV + lane * V;
 #pragma unroll
                 for (int e = 0; e < V; ++e) p[e] = xo[e];
-            } else {
-                gst<T, V, CG>(x + (i64)row * NV + lane * V, xo);
             }
+            if (!XS) gst<T, V, CG>(x + (i64)row * NV + lane * V, xo);
         }
         // next level: its row, t and x were prefetched at the start of this one
         if (l + 1 < l1) {
@@ -466,7 +525,9 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
             __syncthreads();
         }
     }
-    // after an early exit, wait (bounded) for staging copies still in flight
+    // after an early exit, wait (bounded) for staging copies still in flight;
+    // window copies of this thread complete by themselves
+    if (SL) cp_async_wait_all();
     __syncthreads();
     if (!ok && tid == 0) {
         for (int q = 0; q < NB; ++q)
@@ -492,26 +553,37 @@ template <class T, int NV>
 static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp, const int *blev,
                          const int *lrp, const int *lci, const void *lva, const int *lrow,
                          const void *invd, const void *t, void *x, const void *relax, i64 brows,
-                         i64 n, unsigned *gbar, int *err, int emax, cudaStream_t s) {
+                         i64 n, unsigned *gbar, int *err, int emax, const GsSlotWin *win, cudaStream_t s) {
     const T *va = (const T *)lva;
     const int4 *lev_row = (const int4 *)descp;
     const T *di = (const T *)invd;
     const T *tt = (const T *)t;
     T *xx = (T *)x;
     const T *rl = (const T *)relax;
+    GsSlotWin none{};
     note_launch();
     if (mode == 1) {
         if (xs) {
             size_t sm = (size_t)brows * NV * sizeof(T);
             auto k = k_gs3<T, NV, 1, true>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, 0, gbar, err);
+            k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, 0, gbar, err,
+                                    none);
+        } else if (win && win->nslots > 0 && Sh<T, NV>::V * (int)sizeof(T) == 16 &&
+                   (size_t)win->nslots * NV * sizeof(T) <= (size_t)gs_slot_window_bytes()) {
+            // lci holds slot numbers (the plan's slot-mapped copy)
+            const size_t sm = (size_t)win->nslots * NV * sizeof(T);
+            auto k = k_gs3<T, NV, 1, false, true>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, 0, gbar, err,
+                                    *win);
         } else {
             const int eg = gather_entries<T>(NV, emax);
             const size_t sm = (size_t)eg * NV * sizeof(T);
             auto k = k_gs3<T, NV, 1, false>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, eg, gbar, err);
+            k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, eg, gbar, err,
+                                    none);
         }
         return cudaGetLastError();
     }
@@ -526,7 +598,8 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp,
     // the grid barrier's arrival counter and release word start from zero
     e = cudaMemsetAsync(gbar, 0, 256, s);
     if (e != cudaSuccess) return e;
-    void *args[] = {&nlev, &lev_row, &blev, &lrp, &lci, &va, &lrow, &di, &tt, &xx, &rl, &brows, &n, &eg, &gbar, &err};
+    void *args[] = {&nlev, &lev_row, &blev, &lrp, &lci, &va, &lrow, &di, &tt, &xx, &rl, &brows, &n, &eg, &gbar, &err,
+                    &none};
     return cudaLaunchCooperativeKernel((const void *)k, dim3(nblk), dim3(256), args, sm, s);
 }
 
@@ -545,17 +618,20 @@ cudaError_t gs_sweep_lcsr(Prec p, int nv, int mode, int xs, int nlev, int ncta, 
                           const int *blev, const int *lrp, const int *lci, const void *lva,
                           const int *lrow, const void *invd, const void *t, void *x,
                           const void *relax, i64 brows, i64 n, unsigned *gbar, int *err,
-                          int emax, cudaStream_t s) {
+                          int emax, const GsSlotWin *win, cudaStream_t s) {
     if (p == Prec::F64) {
-#define F(NV) gs3_t<double, NV>(mode, xs, nlev, ncta, lev_row, blev, lrp, lci, lva, lrow, invd, t, x, relax, brows, n, gbar, err, emax, s)
+#define F(NV) gs3_t<double, NV>(mode, xs, nlev, ncta, lev_row, blev, lrp, lci, lva, lrow, invd, t, x, relax, brows, n, gbar, err, emax, win, s)
         NV_SWITCH(nv, F)
 #undef F
     } else {
-#define F(NV) gs3_t<float, NV>(mode, xs, nlev, ncta, lev_row, blev, lrp, lci, lva, lrow, invd, t, x, relax, brows, n, gbar, err, emax, s)
+#define F(NV) gs3_t<float, NV>(mode, xs, nlev, ncta, lev_row, blev, lrp, lci, lva, lrow, invd, t, x, relax, brows, n, gbar, err, emax, win, s)
         NV_SWITCH(nv, F)
 #undef F
     }
 }
+
+// dynamic shared memory of a slot window that still leaves two CTAs per SM
+int gs_slot_window_bytes() { return 64 * 1024; }
 
 // dynamic shared memory available for the x tile next to the two staging buffers
 int gs_lcsr_max_xs_bytes() { return 170 * 1024; }

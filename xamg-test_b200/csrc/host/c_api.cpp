@@ -832,6 +832,14 @@ int xamg_gs_plan_levels(void *plan, int *nlev, int *lf, int *lb) {
         if (lb) std::memcpy(lb, g.lb.data(), sizeof(int) * g.n);
     });
 }
+int xamg_gs_plan_slots(void *plan, int *nslots) {
+    return guard([&] {
+        XCHECK(plan, "null plan");
+        GsPlan &g = ((PlanHandle *)plan)->plan;
+        nslots[0] = g.has_lcsr ? g.lc[0].nslots : 0;
+        nslots[1] = g.has_lcsr ? g.lc[1].nslots : 0;
+    });
+}
 int xamg_gs_plan_error(void *plan) {
     if (!plan) return -1;
     return ((PlanHandle *)plan)->plan.error_flag();

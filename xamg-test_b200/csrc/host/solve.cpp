@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <queue>
 #include <set>
 #include <tuple>
 #ifdef _OPENMP
@@ -297,6 +298,103 @@ void GsPlan::build_offblock(const HostCsr &A, Prec p) {
     aoff.upload(off, p == Prec::F64, p == Prec::F32);
 }
 
+// Slot-mapped x window of hybrid blocks whose x tile does not fit in shared
+// memory.  Within one block the sweep reads, at each level, the x rows of that
+// level's entries: rows of earlier levels (written by this CTA) and rows of
+// later ones (old values).  Every row of the block is given a shared-memory
+// slot for its live range: from kSlotAhead levels before its first use (when
+// its old value is loaded from global memory) to its last use; slots are
+// reused by interval colouring.  The sweep then reads every x value from
+// shared memory and loads only first-use rows, ahead of time, off the
+// level's critical path.  No window is kept when a block needs more than
+// kMaxSlots slots at once.
+constexpr int kSlotAhead = xk::kGsSlotAhead;
+constexpr int kMaxSlots = 4096;
+
+void GsPlan::build_slots(int d, const std::vector<int> &order, const std::vector<int> &groups,
+                         const std::vector<int> &blev, const std::vector<int> &lrp, const std::vector<int> &lci) {
+    Lcsr &L = lc[d];
+    L.nslots = 0;
+    const i64 nr = (i64)order.size();
+    const int ngroups = (int)groups.size() - 1;
+    std::vector<int> slot(n, -1), first(n, INT32_MAX), last(n, -1);
+    // {row, slot} pairs; ldd per level group and ldpre per block are {first, end}
+    std::vector<int> ld, ldd(2 * (size_t)std::max(ngroups, 1), 0), ldpre(2 * (size_t)nblocks, 0);
+    auto put_list = [&](std::vector<int> &rows, int *range) {
+        std::sort(rows.begin(), rows.end());
+        range[0] = (int)(ld.size() / 2);
+        for (int c : rows) { ld.push_back(c); ld.push_back(slot[c]); }
+        if (rows.size() & 1) { ld.push_back(-1); ld.push_back(-1); }  // even length: 16-byte ranges
+        range[1] = (int)(ld.size() / 2);
+    };
+    int smax = 0;
+    for (int b = 0; b < nblocks; ++b) {
+        const int g0 = blev[b], g1 = blev[b + 1];
+        std::vector<int> rows;
+        for (int g = g0; g < g1; ++g)
+            for (int r = groups[g]; r < groups[g + 1]; ++r) {
+                const int i = order[r];
+                if (i < 0) continue;
+                const int lv = g - g0;
+                auto use = [&](int c) {
+                    if (first[c] == INT32_MAX) rows.push_back(c);
+                    first[c] = std::min(first[c], lv);
+                    last[c] = std::max(last[c], lv);
+                };
+                use(i);
+                for (int q = lrp[r]; q < lrp[r + 1]; ++q)
+                    if (lci[q] >= 0) use(lci[q]);
+            }
+        // live interval [first - ahead (or -1: loaded before the sweep), last]
+        std::vector<std::pair<int, int>> iv;  // (start, row)
+        iv.reserve(rows.size());
+        for (int c : rows) iv.push_back({std::max(first[c] - kSlotAhead, -1), c});
+        std::sort(iv.begin(), iv.end());
+        std::priority_queue<std::pair<int, int>, std::vector<std::pair<int, int>>, std::greater<>> active;
+        std::priority_queue<int, std::vector<int>, std::greater<>> freed;
+        int used = 0;
+        for (auto &e : iv) {
+            while (!active.empty() && active.top().first < e.first) {
+                freed.push(active.top().second);
+                active.pop();
+            }
+            int sl;
+            if (!freed.empty()) { sl = freed.top(); freed.pop(); }
+            else sl = used++;
+            slot[e.second] = sl;
+            active.push({last[e.second], sl});
+        }
+        smax = std::max(smax, used);
+        if (smax > kMaxSlots) return;
+        // loads: before the first level the rows first used in levels
+        // [0, ahead); with level group g those first used `ahead` levels later
+        const int nl = g1 - g0;
+        std::vector<std::vector<int>> per(nl);
+        for (int c : rows) per[first[c]].push_back(c);
+        std::vector<int> pre;
+        for (int lv = 0; lv < std::min(nl, kSlotAhead); ++lv) pre.insert(pre.end(), per[lv].begin(), per[lv].end());
+        put_list(pre, &ldpre[2 * (size_t)b]);
+        for (int g = g0; g < g1; ++g) {
+            std::vector<int> none;
+            const int lv = g - g0 + kSlotAhead;
+            put_list(lv < nl ? per[lv] : none, &ldd[2 * (size_t)g]);
+        }
+        for (int c : rows) { first[c] = INT32_MAX; last[c] = -1; }
+    }
+    std::vector<int> lcs(lci.size(), -1), lslot(std::max<i64>(nr, 4), -1);
+    for (size_t q = 0; q < lci.size(); ++q)
+        if (lci[q] >= 0) lcs[q] = slot[lci[q]];
+    for (i64 r = 0; r < nr; ++r)
+        if (order[r] >= 0) lslot[r] = slot[order[r]];
+    if (ld.empty()) ld.assign(4, -1);
+    upload_ints(L.lcs, lcs);
+    upload_ints(L.lslot, lslot);
+    upload_ints(L.ldd, ldd);
+    upload_ints(L.ldpre, ldpre);
+    upload_ints(L.ld, ld);
+    L.nslots = std::max(smax, 1);
+}
+
 void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
     if (mode == GsMode::LEVELS) return;
     lprec = p;
@@ -410,6 +508,7 @@ void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
         upload_ints(L.lrow, order);
         upload_ints(L.desc, desc);
         upload_ints(L.blev, blev);
+        if (mode == GsMode::BLOCKS) build_slots(d, order, groups, blev, lrp, lci);
         if (p == Prec::F64) {
             L.lva.alloc(sizeof(double) * lv.size());
             XCUDA(cudaMemcpy(L.lva.p, lv.data(), sizeof(double) * lv.size(), cudaMemcpyHostToDevice));
@@ -424,6 +523,13 @@ void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
         }
     }
     has_lcsr = true;
+}
+
+// The slot window can be switched off (XAMG_GS_NO_SLOT_WINDOW set) to run
+// the per-level gather form of the same sweeps, whose results are identical.
+static bool slot_window_on() {
+    static const bool on = std::getenv("XAMG_GS_NO_SLOT_WINDOW") == nullptr;
+    return on;
 }
 
 void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val,
@@ -448,9 +554,14 @@ void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val
         // and inverse diagonal, and t read, x read, x written
         const double sv = (double)prec_size(p);
         KTimeScope kt(KClass::GS, n, (double)nnz_in * (4 + sv) + (double)n * (8 + sv) + 3.0 * n * nv * sv, s);
+        xk::GsSlotWin win{L.lslot.as<int>(), L.ldd.as<int2>(), L.ldpre.as<int2>(), L.ld.as<int2>(), L.nslots};
+        const bool slots = md == 1 && !xs && L.nslots > 0 && slot_window_on() &&
+                           (size_t)L.nslots * nv * prec_size(p) <= (size_t)xk::gs_slot_window_bytes() &&
+                           nv * prec_size(p) >= 16;
         XCUDA(xk::gs_sweep_lcsr(p, nv, md, xs, L.nlev, L.ncta, L.desc.as<int>(), L.blev.as<int>(),
-                                L.lrp.as<int>(), L.lci.as<int>(), L.lva.p, L.lrow.as<int>(),
-                                L.linvd.p, t, x, relax, brows, n, bar, err, L.emax, s));
+                                L.lrp.as<int>(), slots ? L.lcs.as<int>() : L.lci.as<int>(), L.lva.p,
+                                L.lrow.as<int>(), L.linvd.p, t, x, relax, brows, n, bar, err, L.emax,
+                                slots ? &win : nullptr, s));
         return;
     }
     if (mode == GsMode::BLOCKS) {

@@ -104,6 +104,12 @@ struct GsPlan {
         int nlev = 0;  // GRID: levels; BLOCKS: unused (per-block counts in blev)
         int ncta = 0;  // CTAs of the launch the descriptors were built for
         int emax = 0;  // most entries of one CTA in one level
+        // BLOCKS: slot-mapped x window (see build_slots): column indices
+        // remapped to window slots, each level-ordered row's slot, and per
+        // level the rows whose old x is loaded into their slot kSlotAhead
+        // levels ahead of their first use
+        DBuf lcs, lslot, ldd, ldpre, ld;
+        int nslots = 0;  // 0: no window (too many rows live at once)
     } lc[2];
     bool has_lcsr = false;
     i64 nnz_in = 0;  // entries inside the rows' blocks (all entries without blocks)
@@ -117,6 +123,9 @@ struct GsPlan {
     // store the level-ordered matrix copies in precision p (values from A)
     void build_lcsr(const HostCsr &A, Prec p);
     void build_offblock(const HostCsr &A, Prec p);
+    // slot window of one sweep direction of a BLOCKS plan (called by build_lcsr)
+    void build_slots(int d, const std::vector<int> &order, const std::vector<int> &groups,
+                     const std::vector<int> &blev, const std::vector<int> &lrp, const std::vector<int> &lci);
     // forward (or backward) sweep; in BLOCKS mode the forward call runs both
     // sweeps and the backward call does nothing
     void sweep(Prec p, int nv, const int *rp, const int *ci, const void *val, const void *invd,

@@ -88,13 +88,29 @@ void gs_blocks(Prec p, int nv, int nblocks, const int *blevf, const int *lptrf, 
 // (8-byte aligned) for the grid barrier and zeroes them before the launch;
 // err must lie outside them.  emax: the most entries any CTA processes in one
 // level (sizes the shared-memory gather buffer; <= 0 = unknown).
+//
+// Slot window of a BLOCKS sweep whose x tile does not fit (win may be null):
+// lci then holds slot numbers instead of columns, lslot gives each
+// level-ordered row's slot, and ld holds {row, slot} pairs: for level group g
+// the range ldd[g] = {first, end} lists the rows first used kGsSlotAhead
+// levels after g, ldpre[b] those first used in block b's first kGsSlotAhead
+// levels (each range starts at an even index and has an even length, padded
+// with {-1, -1}).  Used when nslots * nv * sizeof(T) <= gs_slot_window_bytes()
+// and a row of x is a multiple of 16 bytes; otherwise the level gathers.
+constexpr int kGsSlotAhead = 4;
+struct GsSlotWin {
+    const int *lslot;
+    const int2 *ldd, *ldpre, *ld;
+    int nslots;
+};
 cudaError_t gs_sweep_lcsr(Prec p, int nv, int mode, int xs, int nlev, int ncta, const int *lev_row,
                           const int *blev, const int *lrp, const int *lci, const void *lva,
                           const int *lrow, const void *invd, const void *t, void *x,
                           const void *relax, i64 brows, i64 n, unsigned *gbar, int *err,
-                          int emax, cudaStream_t s);
+                          int emax, const GsSlotWin *win, cudaStream_t s);
 int gs_lcsr_max_xs_bytes();
 int gs_lcsr_xs_bytes_two_per_sm();
+int gs_slot_window_bytes();
 
 // Hybrid Gauss-Seidel right-hand side: t = 1*b + (-1)*(sum over the entries
 // outside the row's block of a_ij x_j)   (blas2.h:226-259)
