@@ -208,6 +208,13 @@ void *xamg_gs_plan_create(int64_t n, const int *rp_host, const int *ci_host,
  * is still used for the hybrid right-hand side. */
 int xamg_gs_plan_set_values(void *plan, const double *val_host, int prec);
 int xamg_gs_plan_levels(void *plan, int *nlev /* [2] */, int *lf, int *lb);
+/* Self-test of the device-side bounded waits (an extension): makes a wait
+ * run out on purpose with a limit of limit_s seconds (at most 2) and reports
+ * it the way a solve does, code 3 with the message in XAMG_b200_last_error.
+ * which = 0: cooperative grid of ncta (2..64) CTAs whose barrier misses one
+ * arrival; 1: an mbarrier phase that nothing completes.  The device stays
+ * usable afterwards. */
+int XAMG_b200_wait_selftest(int which, int ncta, double limit_s);
 /* Slots of the shared-memory x window of each sweep direction of a hybrid
  * plan with values (0: no window; the window is used when slots * nv * the
  * value size <= 64 KB and the block's x tile does not fit in shared memory). */

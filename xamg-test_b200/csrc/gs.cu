@@ -84,11 +84,12 @@ __device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parit
 }
 
 // bounded wait on an mbarrier phase; false on timeout
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity,
+                                          unsigned long long limit = kLimitNs) {
     if (mbar_try(bar, parity)) return true;
     unsigned long long t0 = now_ns();
     while (!mbar_try(bar, parity))
-        if (now_ns() - t0 > kLimitNs) return false;
+        if (now_ns() - t0 > limit) return false;
     return true;
 }
 
@@ -100,7 +101,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
 // poll that word (bounded: on timeout *err is set).  Thread 0's fences order
 // the whole CTA's stores (they follow the CTA barrier).
 __device__ __forceinline__ bool grid_barrier(unsigned long long *words, unsigned long long target,
-                                             int *err) {
+                                             int *err, unsigned long long limit = kLimitNs) {
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
@@ -114,7 +115,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long *words, unsigned
             while (*rel < target) {
                 if ((++spins & 63) == 0) {
                     if (*(volatile int *)err) break;
-                    if (now_ns() - t0 > kLimitNs) {
+                    if (now_ns() - t0 > limit) {
                         atomicExch(err, 1);
                         break;
                     }
@@ -638,5 +639,46 @@ int gs_lcsr_max_xs_bytes() { return 170 * 1024; }
 // an x tile this small leaves room for two CTAs per SM next to the staging
 // buffers (about 43 KB of static shared memory each)
 int gs_lcsr_xs_bytes_two_per_sm() { return 64 * 1024; }
+
+
+// ---------------------------------------------------------------- wait self-test
+// The bounded waits above, made to run out on purpose with a short limit:
+// which = 0: a cooperative grid of ncta CTAs meets at the grid barrier but
+// CTA 0 never arrives, so the others give up after `limit` ns and set *err;
+// which = 1: one CTA waits on an mbarrier phase that nothing completes and
+// records the expiry in *err.  Every thread returns; nothing is left in
+// flight.  Used by the tests to check that an expired wait surfaces as an
+// error status instead of a hang.
+__global__ void k_wait_selftest(int which, unsigned long long limit, unsigned long long *words, int *err) {
+    if (which == 0) {
+        if (blockIdx.x == 0) return;  // the missing arrival
+        grid_barrier(words, (unsigned long long)gridDim.x, err, limit);
+        return;
+    }
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && !mbar_wait(&bar, 0u, limit)) atomicExch(err, 2);
+    __syncthreads();
+}
+
+cudaError_t wait_selftest(int which, int ncta, unsigned long long limit_ns, unsigned *words, int *err,
+                          cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(words, 0, 256, s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(err, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    note_launch();
+    unsigned long long *w = reinterpret_cast<unsigned long long *>(words);
+    if (which == 0) {
+        void *args[] = {&which, &limit_ns, &w, &err};
+        return cudaLaunchCooperativeKernel((const void *)k_wait_selftest, dim3(ncta), dim3(128), args, 0, s);
+    }
+    k_wait_selftest<<<1, 128, 0, s>>>(which, limit_ns, w, err);
+    return cudaGetLastError();
+}
 
 }  // namespace xk

@@ -840,6 +840,23 @@ int xamg_gs_plan_slots(void *plan, int *nslots) {
         nslots[1] = g.has_lcsr ? g.lc[1].nslots : 0;
     });
 }
+int XAMG_b200_wait_selftest(int which, int ncta, double limit_s) {
+    return guard([&] {
+        XCHECK(which == 0 || which == 1, "which must be 0 (grid barrier) or 1 (mbarrier)");
+        XCHECK(ncta >= 2 && ncta <= 64, "ncta must be 2..64");
+        XCHECK(limit_s > 0.0 && limit_s <= 2.0, "limit must be in (0, 2] seconds");
+        cudaStream_t s = ctx().stream;
+        DBuf words(256), err(sizeof(int));
+        XCUDA(xk::wait_selftest(which, ncta, (unsigned long long)(limit_s * 1e9), words.as<unsigned>(),
+                                err.as<int>(), s));
+        XCUDA(cudaStreamSynchronize(s));
+        int h = 0;
+        XCUDA(cudaMemcpy(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) throw Error(std::string(which == 0 ? "grid barrier" : "mbarrier") +
+                               ": bounded wait expired on the device (error word " + std::to_string(h) + ")",
+                           3);
+    });
+}
 int xamg_gs_plan_error(void *plan) {
     if (!plan) return -1;
     return ((PlanHandle *)plan)->plan.error_flag();

@@ -108,6 +108,11 @@ cudaError_t gs_sweep_lcsr(Prec p, int nv, int mode, int xs, int nlev, int ncta, 
                           const int *lrow, const void *invd, const void *t, void *x,
                           const void *relax, i64 brows, i64 n, unsigned *gbar, int *err,
                           int emax, const GsSlotWin *win, cudaStream_t s);
+// Bounded-wait self-test (which 0: grid barrier with one CTA missing; 1:
+// mbarrier phase that nothing completes), limit in ns; words: 256 bytes of
+// device scratch, err: one device int (0 after a wait that did not run out).
+cudaError_t wait_selftest(int which, int ncta, unsigned long long limit_ns, unsigned *words, int *err,
+                          cudaStream_t s);
 int gs_lcsr_max_xs_bytes();
 int gs_lcsr_xs_bytes_two_per_sm();
 int gs_slot_window_bytes();

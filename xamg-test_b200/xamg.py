@@ -128,6 +128,7 @@ def lib():
             "xamg_gs_plan_set_values": (C.c_int, [P, P, C.c_int]),
             "xamg_gs_plan_error": (C.c_int, [P]),
             "xamg_gs_plan_slots": (C.c_int, [P, P]),
+            "XAMG_b200_wait_selftest": (C.c_int, [C.c_int, C.c_int, C.c_double]),
             "xamg_gs_plan_destroy": (None, [P]),
             "xamg_hsgs": (C.c_int, [P, C.c_int, C.c_int, P, P, P, P, P, P, P, P, P]),
             "xamg_jacobi": (C.c_int, [C.c_int, C.c_int, i64, P, P, P, P, P, P, P, P, P]),
