@@ -161,7 +161,9 @@ int xamg_csr_spmv(int prec, int nv, int64_t n, const int *rp, const int *ci, con
  * 10 + k = staged streaming kernel walking k tiles per CTA; -1 = default (6
  * when nv * element size >= 64 bytes, else 0).  Under -1 and 7 the products
  * of operators that have a shifted-row run plan (below) use the run kernel
- * (7 elsewhere = the default).  Returns the previous setting. */
+ * (7 elsewhere = the default).  The setting belongs to the calling host
+ * thread; a batch's autotuned choices are held by its own operators and are
+ * not affected by it.  Returns the previous setting. */
 int xamg_spmv_set_variant(int variant);
 
 /* Shifted-row run SpMV (no counterpart in the reference; the same results as
@@ -175,7 +177,7 @@ int xamg_spmv_set_variant(int variant);
  * arrays; values are kept in FP64 and, when fp32 != 0, in FP32.  Shapes with
  * nv * element size >= 64 bytes (FP64 nv 8, 16, 32; FP32 nv 16, 32).
  * Matrices constructed through the C API get a plan (rows set by
- * xamg_spmv_set_run_rows, default 4, 0 = none) when they have at least 4096
+ * xamg_spmv_set_run_rows, default 8, 0 = none) when they have at least 4096
  * rows and half of their entries lie in full chunks.
  * plan_info (any output may be NULL): chunk count, fraction of the entries
  * in full chunks, segments (runs of at most 3 consecutive columns of each

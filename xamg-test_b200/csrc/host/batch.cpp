@@ -108,7 +108,6 @@ void Batch::autotune(BatchGroup &G) {
     cudaEvent_t e0, e1;
     XCUDA(cudaEventCreate(&e0));
     XCUDA(cudaEventCreate(&e1));
-    const int old = xk::get_spmv_variant();
     for (int pass = 0; pass < 2; ++pass) {
         const Prec p = pass == 0 ? Prec::F64 : Prec::F32;
         const void *xv = pass == 0 ? G.r.p() : G.z32.p();
@@ -116,7 +115,7 @@ void Batch::autotune(BatchGroup &G) {
         float best = 1e30f;
         int bv = -1;
         for (int v : vars) {
-            xk::set_spmv_variant(v);
+            a.variant[pass] = v;
             a.spmv(p, G.nv, xv, yv, 0, nullptr, st);
             XCUDA(cudaEventRecord(e0, st));
             for (int q = 0; q < 5; ++q)
@@ -129,7 +128,11 @@ void Batch::autotune(BatchGroup &G) {
         }
         (pass == 0 ? G.var64 : G.var32) = bv;
     }
-    xk::set_spmv_variant(old);
+    // every product of the group's FP64 iteration uses var64, every product
+    // of its FP32 hierarchy var32 (choices held by the operators themselves)
+    a.variant[0] = G.var64;
+    a.variant[1] = -1;
+    if (MultiGrid *mg = find_multigrid(G.M.get())) mg_set_spmv_variant(mg, Prec::F32, G.var32);
     XCUDA(cudaEventDestroy(e0));
     XCUDA(cudaEventDestroy(e1));
 }
@@ -141,7 +144,6 @@ void Batch::run_init(BatchGroup &G) {
     const int nseg = (int)G.sys.size();
     const i64 *so = G.segoff.as<i64>(), *cs = G.cstart.as<i64>();
     double *part = G.part.as<double>();
-    xk::set_spmv_variant(G.var64);
     a.spmv(Prec::F64, G.nv, G.x.p(), G.r0.p(), 2, G.b.p(), st);
     const void *A1[1] = {G.r0.p()}, *B1[1] = {G.r0.p()};
     xk::seg_dots(Prec::F64, G.nv, nseg, so, cs, G.nch, 1, A1, B1, part, G.S(RHO), st);
@@ -162,10 +164,8 @@ void Batch::run_body(BatchGroup &G, int graph_mode) {
     auto precond = [&](const DVec &in, DVec &out) {
         xk::convert(Prec::F64, Prec::F32, in.count(), in.p(), G.z32.p(), st);
         xk::fill(Prec::F32, G.w32.count(), 0.0, G.w32.p(), st);
-        xk::set_spmv_variant(G.var32);
         G.M->solve_from_zero(G.w32, G.z32);
         xk::convert(Prec::F32, Prec::F64, G.w32.count(), G.w32.p(), out.p(), st);
-        xk::set_spmv_variant(G.var64);
     };
     auto spmv = [&](const DVec &x, DVec &y) {
         a.spmv(Prec::F64, nv, x.p(), y.p(), 0, nullptr, st);
@@ -205,7 +205,6 @@ void Batch::run_body(BatchGroup &G, int graph_mode) {
 
 void Batch::build_graph() {
     cudaStream_t st = ctx().stream;
-    const int old = xk::get_spmv_variant();
     XCUDA(cudaGraphCreate(&graph, 0));
     for (auto &Gp : groups) {
         BatchGroup &G = *Gp;
@@ -241,7 +240,6 @@ void Batch::build_graph() {
         XCUDA(cudaStreamEndCapture(st, &b2));
     }
     XCUDA(cudaGraphInstantiate(&exec, graph, 0));
-    xk::set_spmv_variant(old);
 }
 
 void Batch::solve() {
@@ -252,7 +250,6 @@ void Batch::solve() {
     if (use_graph && !exec) {
         // one eager pass of every step first: allocations and function
         // attributes of the hierarchy happen outside the capture
-        const int old = xk::get_spmv_variant();
         std::vector<DVec> keep(groups.size());
         for (size_t g = 0; g < groups.size(); ++g) {
             BatchGroup &G = *groups[g];
@@ -263,7 +260,6 @@ void Batch::solve() {
             XCUDA(cudaMemcpyAsync(G.x.p(), keep[g].p(), sizeof(double) * G.x.count(), cudaMemcpyDeviceToDevice, st));
         }
         XCUDA(cudaStreamSynchronize(st));
-        xk::set_spmv_variant(old);
         build_graph();
     }
     const long long k0 = xk::launch_count();
@@ -271,7 +267,6 @@ void Batch::solve() {
     if (use_graph) {
         XCUDA(cudaGraphLaunch(exec, st));
     } else {
-        const int old = xk::get_spmv_variant();
         for (auto &G : groups) run_init(*G);
         std::vector<int> done(groups.size(), 0);
         for (int it = 0; it < max_iters; ++it) {
@@ -287,7 +282,6 @@ void Batch::solve() {
             }
             if (!any) break;
         }
-        xk::set_spmv_variant(old);
     }
     XCUDA(cudaEventRecord(e1, st));
     XCUDA(cudaEventSynchronize(e1));

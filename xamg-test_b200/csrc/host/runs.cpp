@@ -160,7 +160,8 @@ void RunPlan::add_values(const HostCsr &h, Prec p) {
 }
 
 void DCsr::spmv(Prec p, int nv, const void *x, void *y, int mode, const void *b, cudaStream_t s) const {
-    const int var = xk::get_spmv_variant();
+    const int own = variant[p == Prec::F64 ? 0 : 1];
+    const int var = own >= 0 ? own : xk::get_spmv_variant();
     const double sv = (double)prec_size(p);
     // x read once, y written, y or b read for modes 1 and 2
     const double xy = (double)ncols * nv * sv + (double)n * nv * sv * (mode >= 1 ? 2 : 1);
@@ -173,7 +174,7 @@ void DCsr::spmv(Prec p, int nv, const void *x, void *y, int mode, const void *b,
         return;
     }
     KTimeScope kt(KClass::SPMV, n, (double)nnz * (sv + 4) + (double)(n + 1) * 4 + xy, s);
-    xk::spmv(p, nv, n, rpp(), cip(), val(p), x, y, mode, b, s);
+    xk::spmv(p, nv, n, rpp(), cip(), val(p), x, y, mode, b, s, var);
 }
 
 }  // namespace xamg

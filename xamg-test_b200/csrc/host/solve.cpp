@@ -1675,6 +1675,12 @@ const HostCsr &mg_level_A(MultiGrid *mg, int l) { return l == 0 ? mg->Afine->h :
 const HostCsr &mg_level_P(MultiGrid *mg, int l) { return mg->lv[l].hP; }
 const GsPlan &mg_level_gs(MultiGrid *mg, int l) { return mg->lv[l].gs_pre; }
 const std::vector<double> &mg_coarse_inverse(MultiGrid *mg) { return mg->coarse_inv; }
+void mg_set_spmv_variant(MultiGrid *mg, Prec p, int variant) {
+    const int k = p == Prec::F64 ? 0 : 1;
+    if (mg->Afine) mg->Afine->d.variant[k] = variant;
+    for (MGLevel &m : mg->lv)
+        for (const DCsr *d : {&m.A, &m.P, &m.R, &m.gs_pre.aoff, &m.gs_post.aoff}) d->variant[k] = variant;
+}
 void mg_level_eig(MultiGrid *mg, int l, double *mn, double *mx) {
     XCHECK(l >= 0 && l < (int)mg->lv.size(), "level out of range");
     *mn = mg->lv[l].min_eig;

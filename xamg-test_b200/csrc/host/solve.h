@@ -61,6 +61,10 @@ struct DCsr {
     i64 n = 0, ncols = 0, nnz = 0;
     DBuf rp, ci, v64, v32;
     RunPlan runs;
+    // this operator's SpMV kernel choice per precision (see
+    // xk::set_spmv_variant); -1 = the calling thread's setting.  Results are
+    // identical for every choice.
+    mutable int variant[2] = {-1, -1};
     void upload(const HostCsr &h, bool f64, bool f32);
     // y = A x (mode 0), y += A x (1), y = b - A x (2): the run kernel when this
     // operator has a plan in precision p and the shape suits it, else xk::spmv
@@ -222,6 +226,9 @@ const HostCsr &mg_level_A(MultiGrid *mg, int l);
 const HostCsr &mg_level_P(MultiGrid *mg, int l);
 const GsPlan &mg_level_gs(MultiGrid *mg, int l);
 const std::vector<double> &mg_coarse_inverse(MultiGrid *mg);
+// give every operator of the hierarchy (A, P, R, off-block parts) this SpMV
+// choice for products in precision p
+void mg_set_spmv_variant(MultiGrid *mg, Prec p, int variant);
 // spectrum bounds used by a level's Chebyshev smoother (0, 0 when none)
 void mg_level_eig(MultiGrid *mg, int l, double *mn, double *mx);
 

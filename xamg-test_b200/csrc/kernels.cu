@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(256, LOOP == 1 ? 6 : 1) k_spmv_tile(i64 n, con
 // with a plain row loop unrolled 4, 8 times; 10 + k = streaming kernel
 // walking k tiles per CTA; -1 = default (6 when NV*sizeof(T) >= 64 bytes,
 // else 0).
-static int g_spmv_variant = -1;
+static thread_local int g_spmv_variant = -1;
 void set_spmv_variant(int v) { g_spmv_variant = v; }
 static int g_run_rows = 8;
 void set_spmv_run_rows(int r) { g_run_rows = r == 8 ? 8 : 0; }
@@ -334,14 +334,15 @@ static int sm_count() {
 
 template <class T, int NV>
 static void spmv_t(i64 n, const int *rp, const int *ci, const T *va, const T *x, T *y, int mode,
-                   const T *b, cudaStream_t s) {
+                   const T *b, cudaStream_t s, int choice) {
     constexpr int RPB = 256 / Shape<T, NV>::TPR;
     if (n <= 0) return;
     note_launch();
     i64 ntiles = (n + RPB - 1) / RPB;
     // default: the tile-staged kernel when a row spans at least 4 threads (its
     // tile of RPB rows then fits the shared-memory stage), else batches of 4
-    int var = (g_spmv_variant >= 0 && g_spmv_variant != 7) ? g_spmv_variant : (Shape<T, NV>::TPR >= 4 ? 6 : 0);
+    const int want = choice >= 0 ? choice : g_spmv_variant;
+    int var = (want >= 0 && want != 7) ? want : (Shape<T, NV>::TPR >= 4 ? 6 : 0);
     if (var >= 3 && var <= 6) {
         unsigned g = (unsigned)ntiles;
 #define L(GB, LOOP)                                                                                \
@@ -370,13 +371,13 @@ static void spmv_t(i64 n, const int *rp, const int *ci, const T *va, const T *x,
 }
 
 void spmv(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val, const void *x,
-          void *y, int mode, const void *b, cudaStream_t s) {
+          void *y, int mode, const void *b, cudaStream_t s, int variant) {
     if (p == Prec::F64) {
-#define F(NV) spmv_t<double, NV>(n, rp, ci, (const double *)val, (const double *)x, (double *)y, mode, (const double *)b, s)
+#define F(NV) spmv_t<double, NV>(n, rp, ci, (const double *)val, (const double *)x, (double *)y, mode, (const double *)b, s, variant)
         NV_DISPATCH(nv, F)
 #undef F
     } else {
-#define F(NV) spmv_t<float, NV>(n, rp, ci, (const float *)val, (const float *)x, (float *)y, mode, (const float *)b, s)
+#define F(NV) spmv_t<float, NV>(n, rp, ci, (const float *)val, (const float *)x, (float *)y, mode, (const float *)b, s, variant)
         NV_DISPATCH(nv, F)
 #undef F
     }

@@ -25,15 +25,18 @@ long long launch_count();
 
 // ---- sparse matrix-vector products ---------------------------------------
 // y = A x (mode 0), y += A x (mode 1), y = b - A x (mode 2, b given).
+// variant >= 0 picks the kernel (see set_spmv_variant) for this call only;
+// -1 uses the calling thread's setting.
 void spmv(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val, const void *x,
-          void *y, int mode, const void *b, cudaStream_t s);
+          void *y, int mode, const void *b, cudaStream_t s, int variant = -1);
 // Kernel variant for spmv(): 0, 1, 2 = one CTA per row tile with gather
 // batches of 4, 8, 16 entries; 3, 4 = tile-staged entries (shared memory) with
 // gather batches of 4, 8; 5, 6 = tile-staged with a plain row loop unrolled 4,
 // 8 times; 10 + k = streaming kernel walking k tiles per CTA; -1 = default
 // (6 when NV*sizeof(T) >= 64 bytes, else 0).  All give identical results.
 // Operators with a shifted-row run plan use the run kernel under -1 and 7
-// (7 elsewhere = the default).
+// (7 elsewhere = the default).  The setting is per host thread; an operator
+// can also carry its own choice (DCsr::variant), which takes precedence.
 void set_spmv_variant(int v);
 int get_spmv_variant();
 // Rows per chunk of the run plans built when operators are uploaded (8; 0 =
