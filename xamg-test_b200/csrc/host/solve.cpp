@@ -387,6 +387,40 @@ void GsPlan::build_slots(int d, const std::vector<int> &order, const std::vector
     for (i64 r = 0; r < nr; ++r)
         if (order[r] >= 0) lslot[r] = slot[order[r]];
     if (ld.empty()) ld.assign(4, -1);
+    // Replay the sweep's data flow on the host over exactly the arrays the
+    // kernel receives: a slot is taken by a row when its load is issued (its
+    // list's level) and every read at a level (the row's own slot, the slots
+    // of its entries) must find that row in it.  Any mismatch drops the
+    // window (the gather form then runs), so the kernel never reads a slot
+    // that holds another row's value.
+    {
+        std::vector<int> occ(std::max(smax, 1), -1);
+        bool good = true;
+        auto take = [&](int a, int z) {
+            if ((a & 1) || ((z - a) & 1) || a < 0 || z > (int)(ld.size() / 2)) { good = false; return; }
+            for (int k = a; k < z; ++k) {
+                const int row = ld[2 * (size_t)k], sl = ld[2 * (size_t)k + 1];
+                if (row < 0) continue;
+                if (row >= n || sl < 0 || sl >= smax) { good = false; return; }
+                occ[sl] = row;
+            }
+        };
+        for (int b = 0; good && b < nblocks; ++b) {
+            std::fill(occ.begin(), occ.end(), -1);
+            take(ldpre[2 * (size_t)b], ldpre[2 * (size_t)b + 1]);
+            for (int g = blev[b]; good && g < blev[b + 1]; ++g) {
+                take(ldd[2 * (size_t)g], ldd[2 * (size_t)g + 1]);
+                for (int r = groups[g]; good && r < groups[g + 1]; ++r) {
+                    if (order[r] < 0) continue;
+                    const int sl = lslot[r];
+                    good = sl >= 0 && sl < smax && occ[sl] == order[r];
+                    for (int q = lrp[r]; good && q < lrp[r + 1]; ++q)
+                        if (lci[q] >= 0) good = lcs[q] >= 0 && lcs[q] < smax && occ[lcs[q]] == lci[q];
+                }
+            }
+        }
+        if (!good) return;
+    }
     upload_ints(L.lcs, lcs);
     upload_ints(L.lslot, lslot);
     upload_ints(L.ldd, ldd);
