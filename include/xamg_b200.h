@@ -73,6 +73,15 @@ int XAMG_b200_solver_info(char *buf, int cap, XAMG_solver_id sid);
  * iargs = {nx, ny, nz, config}; kind 1: 27-point anisotropic, iargs = {n},
  * dargs = {kx, ky, kz}; kind 2: 7-point from face coefficients, iargs =
  * {nx, ny, nz}, faces = kx[(nx+1)ny nz] ky[nx(ny+1)nz] kz[nx ny(nz+1)]. */
+/* The reference's channel-with-cube test system
+ * (examples/common/generator/channel_with_cube.inl, geometry lame.inl) at
+ * grid scale 1, 2 or 3: the operator into the csr matrix id and, when b_out
+ * is not NULL, nv right-hand-side columns (rows x nv, row-major): all ones
+ * when const_rhs, else the discrete divergence of the reference's
+ * pseudo-random face velocities.  XAMG_b200_channel_cube_rows gives the rows
+ * of a scale (-1 for other scales). */
+int64_t XAMG_b200_channel_cube_rows(int scale);
+int XAMG_b200_generate_channel_cube(int scale, int const_rhs, int nv, double *b_out, XAMG_csr_matrix_id id);
 int XAMG_b200_csr_matrix_generate(int kind, const int64_t *iargs, const double *dargs,
                                   const double *faces, XAMG_csr_matrix_id mcsrid);
 int64_t XAMG_b200_csr_matrix_get_nnz(XAMG_csr_matrix_id mcsrid);

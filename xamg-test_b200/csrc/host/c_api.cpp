@@ -13,6 +13,7 @@
 namespace xamg {
 void gen_cube(i64 nx, i64 ny, i64 nz, int config, HostCsr &A);
 void gen_27pt(i64 n, double kx, double ky, double kz, HostCsr &A);
+void gen_channel_cube(int scale, bool const_rhs, int nv, HostCsr &A, std::vector<double> &b);
 void gen_7pt_faces(i64 nx, i64 ny, i64 nz, const double *kx, const double *ky, const double *kz,
                    HostCsr &A);
 bool read_bin(const std::string &path, HostCsr &A, std::vector<double> &b, std::vector<double> &x);
@@ -607,6 +608,21 @@ int XAMG_b200_csr_matrix_generate(int kind, const int64_t *ia, const double *da,
             const double *kx = faces, *ky = kx + (nx + 1) * ny * nz, *kz = ky + nx * (ny + 1) * nz;
             gen_7pt_faces(nx, ny, nz, kx, ky, kz, m->h);
         } else throw Error("unknown generator kind", 2);
+    });
+}
+int64_t XAMG_b200_channel_cube_rows(int scale) {
+    if (scale == 1) return (int64_t)144 * 112 * 144;
+    if (scale == 2) return (int64_t)240 * 168 * 240;
+    if (scale == 3) return (int64_t)360 * 252 * 360;
+    return -1;
+}
+int XAMG_b200_generate_channel_cube(int scale, int const_rhs, int nv, double *b_out, XAMG_csr_matrix_id id) {
+    return guard([&] {
+        ApiCsr *m = get(mcsrlist, id, "csr matrix");
+        XCHECK(nv >= 1 && nv <= 64, "nv must be 1..64");
+        std::vector<double> b;
+        gen_channel_cube(scale, const_rhs != 0, nv, m->h, b);
+        if (b_out) std::memcpy(b_out, b.data(), sizeof(double) * b.size());
     });
 }
 int64_t XAMG_b200_csr_matrix_get_nnz(XAMG_csr_matrix_id id) {

@@ -100,6 +100,8 @@ def lib():
             "XAMG_b200_solver_level_eig": (C.c_int, [P, C.c_int, sz]),
             "XAMG_b200_csr_matrix_generate": (C.c_int, [C.c_int, P, P, P, sz]),
             "XAMG_b200_csr_matrix_get_nnz": (i64, [sz]),
+            "XAMG_b200_channel_cube_rows": (i64, [C.c_int]),
+            "XAMG_b200_generate_channel_cube": (C.c_int, [C.c_int, C.c_int, C.c_int, P, sz]),
             "XAMG_b200_csr_matrix_export": (C.c_int, [P, P, P, sz]),
             "XAMG_b200_csr_matrix_read_bin": (C.c_int, [C.c_char_p, P, P, sz]),
             "XAMG_b200_csr_matrix_write_bin": (C.c_int, [C.c_char_p, P, P, sz]),
@@ -269,6 +271,17 @@ class CsrMatrix:
         ia = np.array([nx, ny, nz, config], dtype=np.int64)
         check(lib().XAMG_b200_csr_matrix_generate(0, _ptr(ia), None, None, m.h))
         return m
+
+    @classmethod
+    def channel_cube(cls, scale=1, nv=1, const_rhs=False):
+        """The reference's channel-with-cube system: (matrix, B[rows, nv])."""
+        rows = lib().XAMG_b200_channel_cube_rows(scale)
+        if rows < 0:
+            raise XamgError("channel_cube: scale must be 1, 2 or 3")
+        m = cls()
+        B = np.zeros((rows, nv))
+        check(lib().XAMG_b200_generate_channel_cube(scale, int(const_rhs), nv, _ptr(B), m.h))
+        return m, B
 
     @classmethod
     def aniso27(cls, n, kx=1.0, ky=1.0, kz=1e-3):
