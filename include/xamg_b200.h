@@ -157,6 +157,30 @@ int XAMG_b200_rowpart_halo(size_t id, int64_t *rows_out, int *owner_out);
 int XAMG_b200_rowpart_sends(size_t id, int peer, int64_t *rows_out, int64_t *count);
 int XAMG_b200_rowpart_destroy(size_t id);
 
+/* Row-partitioned solve of one system over several GPUs, one rank per GPU
+ * (an extension: the reference distributes with MPI, part.h,
+ * matvec_comm.h:117-312, shm_allreduce.h:112-163).  Every rank uses the same
+ * NCCL unique id (rank 0 makes it with XAMG_b200_dist_unique_id, 128 bytes,
+ * and the caller broadcasts it), builds its row partition
+ * (XAMG_b200_rowpart_create) and then the solver from the GLOBAL host values
+ * (CSR order of the partitioned matrix) and a parameter list whose solver
+ * role is BiCGStab or PBiCGStab; the preconditioner role runs on the rank's
+ * diagonal block (block Jacobi across ranks).  Before each product the halo
+ * rows are exchanged by NCCL send/receive into this GPU's memory; the inner
+ * products of a step are summed by one NCCL allreduce.  With one rank the
+ * iterations equal the single-GPU solver's bit for bit.  Solve: b and x are
+ * device arrays of the rank's rows (rows x nv, row-major, FP64); x holds the
+ * initial guess on entry.  Info: {iterations, all columns converged, rows,
+ * history length}; history: squared residual norms, nv per check.  NCCL
+ * (libnccl.so.2) is loaded when first needed. */
+int XAMG_b200_dist_unique_id(void *out /* 128 bytes */);
+int XAMG_b200_dist_create(const void *unique_id, size_t rowpart_id, const double *val_global_host,
+                          XAMG_param_id pid, int nv, size_t *did);
+int XAMG_b200_dist_solve(size_t did, const double *b_dev, double *x_dev);
+int XAMG_b200_dist_info(size_t did, int64_t *out /* [4] */);
+int XAMG_b200_dist_history(size_t did, double *out, int64_t cap);
+int XAMG_b200_dist_destroy(size_t did);
+
 /* ---- Part 2: kernel-level device interface ----------------------------- */
 
 /* csr_Ax_y / csr_Axpy (blas2/detail/csr_matvec.inl:32-260):

@@ -22,7 +22,7 @@ ORACLE_LIB = os.path.join(ROOT, "oracle", "liboracle.so")
 
 CU_SOURCES = ["kernels.cu", "gs.cu", "noalloc.cu", "cnn.cu", "batch.cu"]
 CPP_SOURCES = ["host/gen.cpp", "host/amg.cpp", "host/params.cpp", "host/solve.cpp", "host/runs.cpp",
-               "host/batch.cpp", "host/dist.cpp", "host/c_api.cpp"]
+               "host/batch.cpp", "host/dist.cpp", "host/dist_solve.cpp", "host/c_api.cpp"]
 
 
 def _run(cmd):

@@ -1064,3 +1064,69 @@ int XAMG_b200_rowpart_destroy(size_t id) {
     });
 }
 }  // extern "C"
+
+// ---- row-partitioned multi-GPU solve (an extension; the reference's
+// MPI-distributed solve) ------------------------------------------------------
+namespace xamg {
+struct DistSolver;
+void dist_unique_id(void *out);
+DistSolver *dist_create(const void *uid, const RowPart &part, const double *val_global, const GlobalParams &gp,
+                        int nv);
+void dist_solve(DistSolver *d, const double *b, double *x);
+void dist_destroy(DistSolver *d);
+int dist_iters(const DistSolver *d);
+bool dist_converged(const DistSolver *d);
+const std::vector<double> &dist_history(const DistSolver *d);
+i64 dist_rows(const DistSolver *d);
+}  // namespace xamg
+static std::vector<DistSolver *> dlist;
+
+extern "C" {
+int XAMG_b200_dist_unique_id(void *out) {
+    return guard([&] {
+        XCHECK(out, "null argument");
+        dist_unique_id(out);
+    });
+}
+int XAMG_b200_dist_create(const void *uid, size_t rowpart_id, const double *val_global, XAMG_param_id pid, int nv,
+                          size_t *did) {
+    return guard([&] {
+        RowPart *P = get(rplist, rowpart_id, "row partition");
+        GlobalParams *gp = get(plist, pid, "param");
+        XCHECK(uid && val_global && did, "null argument");
+        XCHECK(nv == 1 || nv == 2 || nv == 4 || nv == 8 || nv == 16 || nv == 32, "nv must be 1, 2, 4, 8, 16 or 32");
+        dlist.push_back(dist_create(uid, *P, val_global, *gp, nv));
+        *did = dlist.size() - 1;
+    });
+}
+int XAMG_b200_dist_solve(size_t did, const double *b_dev, double *x_dev) {
+    return guard([&] {
+        DistSolver *d = get(dlist, did, "distributed solver");
+        XCHECK(b_dev && x_dev, "null argument");
+        dist_solve(d, b_dev, x_dev);
+    });
+}
+int XAMG_b200_dist_info(size_t did, int64_t *out) {
+    return guard([&] {
+        DistSolver *d = get(dlist, did, "distributed solver");
+        out[0] = dist_iters(d);
+        out[1] = dist_converged(d) ? 1 : 0;
+        out[2] = dist_rows(d);
+        out[3] = (int64_t)dist_history(d).size();
+    });
+}
+int XAMG_b200_dist_history(size_t did, double *out, int64_t cap) {
+    return guard([&] {
+        DistSolver *d = get(dlist, did, "distributed solver");
+        const auto &h = dist_history(d);
+        for (size_t k = 0; k < h.size() && (int64_t)k < cap; ++k) out[k] = h[k];
+    });
+}
+int XAMG_b200_dist_destroy(size_t did) {
+    return guard([&] {
+        DistSolver *d = get(dlist, did, "distributed solver");
+        dist_destroy(d);
+        dlist[did] = nullptr;
+    });
+}
+}  // extern "C"

@@ -685,6 +685,8 @@ static void parse_conv(const ParamList &l, Conv &c) {
     }
 }
 
+void parse_conv_settings(const ParamList &l, Conv &c) { parse_conv(l, c); }
+
 // ------------------------------------------------------------------ helpers
 static void dot1(const DVec &a, const DVec &b, DBuf &part, double *out, cudaStream_t s) {
     const void *A[1] = {a.p()}, *B[1] = {b.p()};

@@ -167,6 +167,10 @@ struct Conv {
     void record() { history.insert(history.end(), res.begin(), res.end()); }
 };
 
+// convergence flags and tolerances of a role's parameter list
+// (convergence_details, abs_tolerance, rel_tolerance, rel_tolerance_base)
+void parse_conv_settings(const ParamList &l, Conv &c);
+
 struct Solver;
 
 // One multigrid level on the device.

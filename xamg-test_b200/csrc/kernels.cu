@@ -1345,6 +1345,8 @@ __global__ void __launch_bounds__(256) k_bicg_xr(i64 n, i64 nch, const double *_
 // column k per block, then that column's scalar recurrence.
 enum { EPI_ALPHA = 0, EPI_OMEGA = 1, EPI_BETA = 2 };
 template <int EPI>
+__device__ __forceinline__ void bicg_epi_col(int k, const double *val, const BicgScalars &sc);
+template <int EPI>
 __global__ void __launch_bounds__(256) k_dot2_epi(i64 nch, int nd, int nv, const double *__restrict__ part,
                                                   double *__restrict__ out, BicgScalars sc) {
     __shared__ double q[256];
@@ -1371,6 +1373,21 @@ __global__ void __launch_bounds__(256) k_dot2_epi(i64 nch, int nd, int nv, const
         __syncthreads();
     }
     if (threadIdx.x != 0) return;
+    bicg_epi_col<EPI>(k, val, sc);
+}
+
+// the recurrence alone, from reduced values vals[d*nv + k] (one thread per column)
+template <int EPI>
+__global__ void k_bicg_epi(int nv, const double *__restrict__ vals, BicgScalars sc) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nv) return;
+    double val[3];
+    for (int d = 0; d < (EPI == EPI_OMEGA ? 3 : 1); ++d) val[d] = vals[(i64)d * nv + k];
+    bicg_epi_col<EPI>(k, val, sc);
+}
+
+template <int EPI>
+__device__ __forceinline__ void bicg_epi_col(int k, const double *val, const BicgScalars &sc) {
     if (EPI == EPI_ALPHA) {  // alpha = rho / (v, r0)
         sc.alpha[k] = __ddiv_rn(sc.rho[k], val[0]);
     } else if (EPI == EPI_OMEGA) {  // omega = (t,s)/(t,t); res = (s,s) - omega (t,s)
@@ -1464,6 +1481,48 @@ void dot_reduce_epi(int epi, i64 n, int nd, int nv, const double *part, double *
     if (epi == EPI_ALPHA) k_dot2_epi<EPI_ALPHA><<<nv, 256, 0, s>>>(nch, nd, nv, part, out, sc);
     else if (epi == EPI_OMEGA) k_dot2_epi<EPI_OMEGA><<<nv, 256, 0, s>>>(nch, nd, nv, part, out, sc);
     else k_dot2_epi<EPI_BETA><<<nv, 256, 0, s>>>(nch, nd, nv, part, out, sc);
+}
+
+void bicg_epi(int epi, int nv, const double *vals, const BicgScalars &sc, cudaStream_t s) {
+    note_launch();
+    const unsigned g = (unsigned)((nv + 127) / 128);
+    if (epi == EPI_ALPHA) k_bicg_epi<EPI_ALPHA><<<g, 128, 0, s>>>(nv, vals, sc);
+    else if (epi == EPI_OMEGA) k_bicg_epi<EPI_OMEGA><<<g, 128, 0, s>>>(nv, vals, sc);
+    else k_bicg_epi<EPI_BETA><<<g, 128, 0, s>>>(nv, vals, sc);
+}
+
+void dot_reduce(i64 n, int nd, int nv, const double *part, double *out, cudaStream_t s) {
+    const i64 nch = (n + 255) / 256;
+    if (nch == 0) {
+        cudaMemsetAsync(out, 0, sizeof(double) * nd * nv, s);
+        return;
+    }
+    note_launch();
+    k_dot2<<<nd * nv, 256, 0, s>>>(nch, part, out);
+}
+
+// dst row q = src row idx[q] of block vectors (W: 16- or 4-byte words)
+template <class W>
+__global__ void k_gather_rows(i64 cnt, int wpr, const int *__restrict__ idx, const W *__restrict__ src,
+                              W *__restrict__ dst) {
+    const i64 q = (i64)blockIdx.x * 256 + threadIdx.x;
+    if (q >= cnt * wpr) return;
+    const i64 r = q / wpr;
+    dst[q] = src[(i64)idx[r] * wpr + q % wpr];
+}
+void gather_rows(Prec p, int nv, i64 cnt, const int *idx, const void *src, void *dst, cudaStream_t s) {
+    if (cnt <= 0) return;
+    note_launch();
+    const int bytes = nv * (p == Prec::F64 ? 8 : 4);
+    if (bytes % 16 == 0) {
+        const int wpr = bytes / 16;
+        k_gather_rows<float4><<<(unsigned)((cnt * wpr + 255) / 256), 256, 0, s>>>(cnt, wpr, idx, (const float4 *)src,
+                                                                                (float4 *)dst);
+    } else {
+        const int wpr = bytes / 4;
+        k_gather_rows<float><<<(unsigned)((cnt * wpr + 255) / 256), 256, 0, s>>>(cnt, wpr, idx, (const float *)src,
+                                                                               (float *)dst);
+    }
 }
 
 void dot_partials(Prec in, int nv, i64 n, int nd, const void *const *a, const void *const *b, double *part,

@@ -156,6 +156,12 @@ void dot_partials(Prec in, int nv, i64 n, int nd, const void *const *a, const vo
 // next iconv; 2 beta = (out0/rho)(alpha/omega), rho = out0, c1 = -(omega*beta)
 void dot_reduce_epi(int epi, i64 n, int nd, int nv, const double *part, double *out, const BicgScalars &sc,
                     cudaStream_t s);
+// the same recurrences from already reduced values vals[d*nv + k] (after an
+// allreduce over ranks), and the second stage alone (no recurrence)
+void bicg_epi(int epi, int nv, const double *vals, const BicgScalars &sc, cudaStream_t s);
+void dot_reduce(i64 n, int nd, int nv, const double *part, double *out, cudaStream_t s);
+// dst row q = src row idx[q] of N x nv block vectors (halo send buffers)
+void gather_rows(Prec p, int nv, i64 cnt, const int *idx, const void *src, void *dst, cudaStream_t s);
 // s = r - alpha v (blas AXPBY_Z with 1 and -alpha); sz = 0 when given
 void bicg_s(Prec p, int nv, i64 n, const BicgScalars &sc, const void *r, const void *v, void *s_out, void *sz,
             cudaStream_t s);

@@ -123,6 +123,12 @@ def lib():
             "XAMG_b200_rowpart_halo": (C.c_int, [C.c_size_t, P, P]),
             "XAMG_b200_rowpart_sends": (C.c_int, [C.c_size_t, C.c_int, P, P]),
             "XAMG_b200_rowpart_destroy": (C.c_int, [C.c_size_t]),
+            "XAMG_b200_dist_unique_id": (C.c_int, [P]),
+            "XAMG_b200_dist_create": (C.c_int, [P, sz, P, sz, C.c_int, C.POINTER(sz)]),
+            "XAMG_b200_dist_solve": (C.c_int, [sz, P, P]),
+            "XAMG_b200_dist_info": (C.c_int, [sz, P]),
+            "XAMG_b200_dist_history": (C.c_int, [sz, P, i64]),
+            "XAMG_b200_dist_destroy": (C.c_int, [sz]),
             "xamg_spmv_runs": (C.c_int, [P, C.c_int, C.c_int, P, P, C.c_int, P, P]),
             "xamg_spmv_runs_plan_destroy": (C.c_int, [P]),
             "xamg_gs_plan_create": (P, [i64, P, P, i64, C.c_int]),
@@ -602,5 +608,49 @@ class Batch:
     def __del__(self):
         try:
             lib().XAMG_b200_batch_destroy(self.h)
+        except Exception:
+            pass
+
+
+def dist_unique_id():
+    """A new NCCL unique id (128 bytes) for DistSolver."""
+    buf = (C.c_char * 128)()
+    check(lib().XAMG_b200_dist_unique_id(buf))
+    return bytes(buf)
+
+
+class DistSolver:
+    """This rank's part of a row-partitioned (P)BiCGStab solve of one system
+    over several GPUs (XAMG_b200_dist_*).  rp, ci, v: the GLOBAL host CSR
+    arrays; uid: the same 128-byte NCCL id on every rank."""
+
+    def __init__(self, rp, ci, v, nranks, rank, params, nv, uid):
+        self.part = RowPart(rp, ci, nranks, rank)
+        v = np.ascontiguousarray(v, np.float64)
+        ub = (C.c_char * 128).from_buffer_copy(uid)
+        h = C.c_size_t()
+        check(lib().XAMG_b200_dist_create(ub, self.part.h.value, _ptr(v), params.h, nv, C.byref(h)))
+        self.h = h.value
+        self.nv = nv
+        self.params = params
+
+    def solve(self, b_ptr, x_ptr):
+        """b, x: device pointers of this rank's rows (rows x nv FP64)."""
+        check(lib().XAMG_b200_dist_solve(self.h, C.c_void_p(b_ptr), C.c_void_p(x_ptr)))
+
+    def info(self):
+        out = np.zeros(4, np.int64)
+        check(lib().XAMG_b200_dist_info(self.h, _ptr(out)))
+        return dict(iters=int(out[0]), converged=bool(out[1]), rows=int(out[2]), hist=int(out[3]))
+
+    def history(self):
+        n = self.info()["hist"]
+        out = np.zeros(max(n, 1))
+        check(lib().XAMG_b200_dist_history(self.h, _ptr(out), n))
+        return out[:n].reshape(-1, self.nv)
+
+    def __del__(self):
+        try:
+            lib().XAMG_b200_dist_destroy(self.h)
         except Exception:
             pass
