@@ -15,6 +15,9 @@ guess.  Forms (all on the same operator and right-hand sides):
                  so that its error against the FP64 solution is <= 1e-8;
   sweep        - the mixed form for nv in {1, 4, 8, 16, 32} with error against
                  an FP64 solve converged to 1e-12;
+  dist         - the system split over the ranks by row blocks (NCCL halo
+                 exchange, allreduce of the inner products, block-Jacobi AMG
+                 with the plain_hybrid settings); at N = 1 one rank;
   batch        - 64 independent 7-point lognormal-coefficient systems (sides
                  16..96, nv in {1,2,4,8}) in one CUDA-graph launch;
   learned      - held-out 64^3 bump-coefficient systems (nv = 8) from a zero
@@ -475,6 +478,55 @@ def batch_form(rank, world, warmup, steps):
 LEARNED_WEIGHTS = os.path.join(ROOT, "xamg-test_b200", "weights", "learned_64.npz")
 
 
+def dist_form(csr, B, rank, world, dist, warmup, steps):
+    """One system split over the ranks by contiguous row blocks (the
+    reference's decomposition): FP64 PBiCGStab whose preconditioner is the
+    AMG V-cycle of each rank's diagonal block (hybrid blocks inside), halo
+    rows exchanged by NCCL before every product, one allreduce per group of
+    inner products.  Timed per solve with CUDA events, max over the ranks
+    (strong scaling: the same system at every N).  With one rank it is the
+    plain_hybrid form through the distributed code path."""
+    import torch
+    import xamg
+    rp, ci, v = csr.arrays()
+    uid = xamg.dist_unique_id() if rank == 0 else None
+    if dist:
+        box = [uid]
+        dist.broadcast_object_list(box, src=0)
+        uid = box[0]
+    t0 = time.time()
+    ds = xamg.DistSolver(rp, ci, v, world, rank, xamg.Params(plain_hybrid_spec()), NV, uid)
+    setup_s = time.time() - t0
+    r0 = ds.part.first
+    nl = ds.part.nrows
+    b = torch.from_numpy(np.ascontiguousarray(B[r0:r0 + nl])).cuda()
+    x = torch.zeros_like(b)
+    ms = []
+    for k in range(warmup + steps):
+        x.zero_()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ds.solve(b.data_ptr(), x.data_ptr())
+        e1.record()
+        torch.cuda.synchronize()
+        if k >= warmup:
+            ms.append(e0.elapsed_time(e1))
+    t = float(np.mean(ms))
+    if dist:
+        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt[0])
+    info = ds.info()
+    out = {"ms": round(t, 3), "ms_per_rhs": round(t / NV, 4), "ranks": world, "rows_per_rank": nl,
+           "halo_rows": int(len(ds.part.halo)), "iters": info["iters"],
+           "converged": info["converged"], "setup_s": round(setup_s, 1), "scaling": "strong"}
+    del ds
+    return out
+
+
 def learned_form(nsys=16):
     """Learned form: held-out 64^3 bump-coefficient systems (nv = 8) solved
     from a zero guess and from the trained network's guess (2 symmetric
@@ -651,7 +703,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--forms", default="plain,plain_hybrid,mixed,mixed_tight,sweep,batch,learned")
+    ap.add_argument("--forms", default="plain,plain_hybrid,mixed,mixed_tight,sweep,dist,batch,learned")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tight-tol", type=float, default=1e-10,
                     help="outer tolerance of the mixed form run to the error target (error vs FP64 <= 1e-8)")
@@ -786,6 +838,8 @@ def main():
             extra["batch"]["ms"], extra["batch"]["rhs_all_ranks"] = float(mx[0]), int(t[1])
         tot = extra["batch"].get("rhs_all_ranks", extra["batch"]["rhs"])
         extra["batch"]["ms_per_rhs"] = round(extra["batch"]["ms"] / tot, 4)
+    if "dist" in allforms:
+        extra["dist"] = dist_form(csr, B, rank, world, dist, 1, 3)
     if "learned" in allforms and rank == 0:
         extra["learned"] = learned_form()
     roof = spmv_roofline(csr, best_var)
