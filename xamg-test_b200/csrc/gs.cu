@@ -124,8 +124,9 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long *words, unsigned
         }
         __threadfence();
     }
-    __syncthreads();
-    return *(volatile int *)err == 0;
+    // one verdict for the whole CTA (thread 0 reads the error word after its
+    // fence), so that no thread leaves a loop its neighbours stay in
+    return __syncthreads_and(threadIdx.x != 0 || *(volatile int *)err == 0) != 0;
 }
 
 __device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
@@ -192,7 +193,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
                                              const T *__restrict__ linvd,
                                              const T *__restrict__ t, T *x,
                                              const T *__restrict__ relax, i64 brows, i64 n,
-                                             int eg, unsigned *gbar, int *err, GsSlotWin sw) {
+                                             int eg, unsigned *gbar, int *err, GsSlotWin sw, GsDeps gd) {
     constexpr int V = Sh<T, NV>::V, TPR = Sh<T, NV>::TPR, E = GsBuf<T>::E, RB = GsBuf<T>::RB;
     constexpr int NB = 3;
     constexpr int LB = SL ? GsBuf<T>::LB : 2;
@@ -325,6 +326,13 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
         }
     };
     Desc dc = l0 < l1 ? dget(l0) : Desc{0, 0, 0, 0};
+    int dfirst = 0, dcnt = 0;
+    int2 dn = make_int2(0, 0);
+    if (MODE == 0 && gd.dptr && l0 + 1 < l1) {
+        dfirst = __ldg(gd.dptr + (i64)(l0 + 1) * gridDim.x + b);
+        dcnt = __ldg(gd.dptr + (i64)(l0 + 1) * gridDim.x + b + 1) - dfirst;
+        if (tid < 32 && tid < dcnt) dn = __ldg(gd.deps + dfirst + tid);
+    }
     if (SL) {
         // rows first used in the first AH levels, then AH - 1 empty groups so
         // that level l's rows are in the group that wait_group<AH> completes
@@ -371,6 +379,40 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
             // this level's rows are in (the groups finish in order)
             cp_async_wait_group<AH>();
             __syncthreads();
+        }
+        if (MODE == 0 && gd.dptr && l > l0) {
+            // point-to-point: wait until every CTA whose rows this level
+            // depends on has finished the levels it must have (bounded; the
+            // list was loaded during the previous level), then make their
+            // stores visible to the whole CTA
+            if (tid < 32) {
+                for (int k = 0; k < dcnt; k += 32) {
+                    int2 e = dn;
+                    if (k > 0) e = tid + k < dcnt ? __ldg(gd.deps + dfirst + tid + k) : make_int2(0, 0);
+                    if (tid + k >= dcnt) continue;
+                    volatile unsigned *pw = gd.prog + (size_t)e.x * 8;
+                    if (*pw >= (unsigned)e.y) continue;
+                    const unsigned long long t0 = now_ns();
+                    unsigned spins = 0;
+                    while (*pw < (unsigned)e.y) {
+                        if ((++spins & 63) == 0) {
+                            if (*(volatile int *)err) break;
+                            if (now_ns() - t0 > kLimitNs) {
+                                atomicExch(err, 1);
+                                break;
+                            }
+                        }
+                    }
+                }
+                __threadfence();
+            }
+            ok = __syncthreads_and(ok && (tid != 0 || *(volatile int *)err == 0)) != 0;
+        }
+        if (MODE == 0 && gd.dptr && ok && l + 1 < l1) {
+            // the next level's list: its range and this lane's first entry
+            dfirst = __ldg(gd.dptr + (i64)(l + 1) * gridDim.x + b);
+            dcnt = __ldg(gd.dptr + (i64)(l + 1) * gridDim.x + b + 1) - dfirst;
+            if (tid < 32 && tid < dcnt) dn = __ldg(gd.deps + dfirst + tid);
         }
         if (!TILE) {
             if (gath && V * (int)sizeof(T) == 16) {
@@ -517,13 +559,20 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
             dc = dnx;
             rotate();
         }
-        if (MODE == 0) {
-            if (l + 1 < l1 &&
+        // every thread agrees on ok before the loop test (a wait that gave up
+        // in one thread ends the sweep for the whole CTA)
+        ok = __syncthreads_and(ok) != 0;
+        if (MODE == 0 && gd.dptr) {
+            // publish: this CTA has finished level l
+            if (ok && tid == 0) {
+                __threadfence();
+                *(volatile unsigned *)(gd.prog + (size_t)b * 8) = (unsigned)(l + 1);
+            }
+        } else if (MODE == 0) {
+            if (ok && l + 1 < l1 &&
                 !grid_barrier(reinterpret_cast<unsigned long long *>(gbar),
                               (unsigned long long)(l + 1) * gridDim.x, err))
                 ok = false;
-        } else {
-            __syncthreads();
         }
     }
     // after an early exit, wait (bounded) for staging copies still in flight;
@@ -554,7 +603,8 @@ template <class T, int NV>
 static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp, const int *blev,
                          const int *lrp, const int *lci, const void *lva, const int *lrow,
                          const void *invd, const void *t, void *x, const void *relax, i64 brows,
-                         i64 n, unsigned *gbar, int *err, int emax, const GsSlotWin *win, cudaStream_t s) {
+                         i64 n, unsigned *gbar, int *err, int emax, const GsSlotWin *win, const GsDeps *deps,
+                         cudaStream_t s) {
     const T *va = (const T *)lva;
     const int4 *lev_row = (const int4 *)descp;
     const T *di = (const T *)invd;
@@ -562,6 +612,7 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp,
     T *xx = (T *)x;
     const T *rl = (const T *)relax;
     GsSlotWin none{};
+    GsDeps nodeps{nullptr, nullptr, nullptr};
     note_launch();
     if (mode == 1) {
         if (xs) {
@@ -569,7 +620,7 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp,
             auto k = k_gs3<T, NV, 1, true>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
             k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, 0, gbar, err,
-                                    none);
+                                    none, nodeps);
         } else if (win && win->nslots > 0 && Sh<T, NV>::V * (int)sizeof(T) == 16 &&
                    (size_t)win->nslots * NV * sizeof(T) <= (size_t)gs_slot_window_bytes()) {
             // lci holds slot numbers (the plan's slot-mapped copy)
@@ -577,14 +628,14 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp,
             auto k = k_gs3<T, NV, 1, false, true>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
             k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, 0, gbar, err,
-                                    *win);
+                                    *win, nodeps);
         } else {
             const int eg = gather_entries<T>(NV, emax);
             const size_t sm = (size_t)eg * NV * sizeof(T);
             auto k = k_gs3<T, NV, 1, false>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
             k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, eg, gbar, err,
-                                    none);
+                                    none, nodeps);
         }
         return cudaGetLastError();
     }
@@ -596,11 +647,17 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp,
     auto k = k_gs3<T, NV, 0, false>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    // the grid barrier's arrival counter and release word start from zero
+    // the grid barrier's arrival counter and release word start from zero,
+    // and so do the per-CTA level counts of the point-to-point waits
     e = cudaMemsetAsync(gbar, 0, 256, s);
     if (e != cudaSuccess) return e;
+    GsDeps gdv = deps ? *deps : nodeps;
+    if (gdv.dptr) {
+        e = cudaMemsetAsync(gdv.prog, 0, (size_t)nblk * 32, s);
+        if (e != cudaSuccess) return e;
+    }
     void *args[] = {&nlev, &lev_row, &blev, &lrp, &lci, &va, &lrow, &di, &tt, &xx, &rl, &brows, &n, &eg, &gbar, &err,
-                    &none};
+                    &none, &gdv};
     return cudaLaunchCooperativeKernel((const void *)k, dim3(nblk), dim3(256), args, sm, s);
 }
 
@@ -619,13 +676,13 @@ cudaError_t gs_sweep_lcsr(Prec p, int nv, int mode, int xs, int nlev, int ncta, 
                           const int *blev, const int *lrp, const int *lci, const void *lva,
                           const int *lrow, const void *invd, const void *t, void *x,
                           const void *relax, i64 brows, i64 n, unsigned *gbar, int *err,
-                          int emax, const GsSlotWin *win, cudaStream_t s) {
+                          int emax, const GsSlotWin *win, const GsDeps *deps, cudaStream_t s) {
     if (p == Prec::F64) {
-#define F(NV) gs3_t<double, NV>(mode, xs, nlev, ncta, lev_row, blev, lrp, lci, lva, lrow, invd, t, x, relax, brows, n, gbar, err, emax, win, s)
+#define F(NV) gs3_t<double, NV>(mode, xs, nlev, ncta, lev_row, blev, lrp, lci, lva, lrow, invd, t, x, relax, brows, n, gbar, err, emax, win, deps, s)
         NV_SWITCH(nv, F)
 #undef F
     } else {
-#define F(NV) gs3_t<float, NV>(mode, xs, nlev, ncta, lev_row, blev, lrp, lci, lva, lrow, invd, t, x, relax, brows, n, gbar, err, emax, win, s)
+#define F(NV) gs3_t<float, NV>(mode, xs, nlev, ncta, lev_row, blev, lrp, lci, lva, lrow, invd, t, x, relax, brows, n, gbar, err, emax, win, deps, s)
         NV_SWITCH(nv, F)
 #undef F
     }

@@ -429,6 +429,72 @@ void GsPlan::build_slots(int d, const std::vector<int> &order, const std::vector
     L.nslots = std::max(smax, 1);
 }
 
+// Point-to-point waits of the cooperative (GRID) sweep.  Instead of a grid
+// barrier after every level, CTA b publishes the number of levels it has
+// finished, and before level l it waits only for the CTAs that own rows its
+// level-l rows depend on: every row c of the symmetrised pattern of row j
+// (j's own entries and the rows that read j) with a lower level.  Those are
+// the values j reads after their update (c < j) and the rows that must have
+// read j's old value before j changes it (rows c whose entries include j).
+// Per (level, CTA) the list holds each other owner once with the most
+// levels it must have finished.
+void GsPlan::build_grid_deps(int d, const HostCsr &A, const std::vector<int> &lev, const std::vector<int> &order,
+                             const std::vector<int> &desc, int G) {
+    Lcsr &L = lc[d];
+    const int ngroups = (int)(desc.size() / 4 / G);
+    std::vector<int> own(n, -1);
+    for (int l = 0; l < ngroups; ++l)
+        for (int b = 0; b < G; ++b) {
+            const int *dd = &desc[((size_t)l * G + b) * 4];
+            for (int r = dd[0]; r < dd[1]; ++r)
+                if (order[r] >= 0) own[order[r]] = b;
+        }
+    // transpose pattern: the rows whose entries include j
+    std::vector<int> trp(n + 1, 0), tci(A.nnz());
+    for (i64 q = 0; q < A.nnz(); ++q) trp[A.ci[q] + 1]++;
+    for (i64 i = 0; i < n; ++i) trp[i + 1] += trp[i];
+    {
+        std::vector<int> at(trp.begin(), trp.end() - 1);
+        for (i64 i = 0; i < n; ++i)
+            for (int q = A.rp[i]; q < A.rp[i + 1]; ++q) tci[at[A.ci[q]]++] = (int)i;
+    }
+    std::vector<int> dptr((size_t)ngroups * G + 1, 0), deps;
+    std::vector<int> need(G, 0), touched;
+    for (int l = 0; l < ngroups; ++l)
+        for (int b = 0; b < G; ++b) {
+            const int *dd = &desc[((size_t)l * G + b) * 4];
+            touched.clear();
+            auto dep = [&](int c, int lj) {
+                if (c < 0 || c >= n || lev[c] >= lj) return;
+                const int o = own[c];
+                if (o == b || o < 0) return;
+                if (need[o] == 0) touched.push_back(o);
+                need[o] = std::max(need[o], lev[c] + 1);
+            };
+            for (int r = dd[0]; r < dd[1]; ++r) {
+                const int j = order[r];
+                if (j < 0) continue;
+                for (int q = A.rp[j]; q < A.rp[j + 1]; ++q) dep(A.ci[q], lev[j]);
+                for (int q = trp[j]; q < trp[j + 1]; ++q) dep(tci[q], lev[j]);
+            }
+            std::sort(touched.begin(), touched.end());
+            for (int o : touched) {
+                deps.push_back(o);
+                deps.push_back(need[o]);
+                need[o] = 0;
+            }
+            dptr[(size_t)l * G + b + 1] = (int)(deps.size() / 2);
+        }
+    if (deps.empty()) deps.assign(2, 0);
+    upload_ints(L.dptr, dptr);
+    upload_ints(L.deps, deps);
+    L.has_deps = true;
+    if (prog.bytes < (size_t)G * 32) {
+        prog.alloc((size_t)G * 32);
+        XCUDA(cudaMemset(prog.p, 0, prog.bytes));
+    }
+}
+
 void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
     if (mode == GsMode::LEVELS) return;
     lprec = p;
@@ -543,6 +609,7 @@ void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
         upload_ints(L.desc, desc);
         upload_ints(L.blev, blev);
         if (mode == GsMode::BLOCKS) build_slots(d, order, groups, blev, lrp, lci);
+        if (mode == GsMode::GRID) build_grid_deps(d, A, lev, order, desc, G);
         if (p == Prec::F64) {
             L.lva.alloc(sizeof(double) * lv.size());
             XCUDA(cudaMemcpy(L.lva.p, lv.data(), sizeof(double) * lv.size(), cudaMemcpyHostToDevice));
@@ -561,6 +628,12 @@ void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
 
 // The slot window can be switched off (XAMG_GS_NO_SLOT_WINDOW set) to run
 // the per-level gather form of the same sweeps, whose results are identical.
+// Likewise the point-to-point waits of the cooperative sweep
+// (XAMG_GS_GRID_BARRIER set: a grid barrier after every level instead).
+static bool grid_deps_on() {
+    static const bool on = std::getenv("XAMG_GS_GRID_BARRIER") == nullptr;
+    return on;
+}
 static bool slot_window_on() {
     static const bool on = std::getenv("XAMG_GS_NO_SLOT_WINDOW") == nullptr;
     return on;
@@ -589,13 +662,15 @@ void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val
         const double sv = (double)prec_size(p);
         KTimeScope kt(KClass::GS, n, (double)nnz_in * (4 + sv) + (double)n * (8 + sv) + 3.0 * n * nv * sv, s);
         xk::GsSlotWin win{L.lslot.as<int>(), L.ldd.as<int2>(), L.ldpre.as<int2>(), L.ld.as<int2>(), L.nslots};
+        xk::GsDeps gd{nullptr, nullptr, nullptr};
+        if (md == 0 && L.has_deps && grid_deps_on()) gd = {L.dptr.as<int>(), L.deps.as<int2>(), prog.as<unsigned>()};
         const bool slots = md == 1 && !xs && L.nslots > 0 && slot_window_on() &&
                            (size_t)L.nslots * nv * prec_size(p) <= (size_t)xk::gs_slot_window_bytes() &&
                            nv * prec_size(p) >= 16;
         XCUDA(xk::gs_sweep_lcsr(p, nv, md, xs, L.nlev, L.ncta, L.desc.as<int>(), L.blev.as<int>(),
                                 L.lrp.as<int>(), slots ? L.lcs.as<int>() : L.lci.as<int>(), L.lva.p,
                                 L.lrow.as<int>(), L.linvd.p, t, x, relax, brows, n, bar, err, L.emax,
-                                slots ? &win : nullptr, s));
+                                slots ? &win : nullptr, gd.dptr ? &gd : nullptr, s));
         return;
     }
     if (mode == GsMode::BLOCKS) {

@@ -114,7 +114,12 @@ struct GsPlan {
         // levels ahead of their first use
         DBuf lcs, lslot, ldd, ldpre, ld;
         int nslots = 0;  // 0: no window (too many rows live at once)
+        // GRID: per (level, CTA) the CTAs whose earlier levels this one's rows
+        // depend on, {cta, levels it must have finished} (see build_grid_deps)
+        DBuf dptr, deps;
+        bool has_deps = false;
     } lc[2];
+    DBuf prog;  // GRID: per-CTA count of finished levels (32-byte stride)
     bool has_lcsr = false;
     i64 nnz_in = 0;  // entries inside the rows' blocks (all entries without blocks)
     Prec lprec = Prec::F64;
@@ -127,6 +132,9 @@ struct GsPlan {
     // store the level-ordered matrix copies in precision p (values from A)
     void build_lcsr(const HostCsr &A, Prec p);
     void build_offblock(const HostCsr &A, Prec p);
+    // point-to-point dependencies of one sweep direction of a GRID plan
+    void build_grid_deps(int d, const HostCsr &A, const std::vector<int> &lev, const std::vector<int> &order,
+                         const std::vector<int> &desc, int G);
     // slot window of one sweep direction of a BLOCKS plan (called by build_lcsr)
     void build_slots(int d, const std::vector<int> &order, const std::vector<int> &groups,
                      const std::vector<int> &blev, const std::vector<int> &lrp, const std::vector<int> &lci);

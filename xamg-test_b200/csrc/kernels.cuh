@@ -106,11 +106,21 @@ struct GsSlotWin {
     const int2 *ldd, *ldpre, *ld;
     int nslots;
 };
+// Point-to-point waits of a GRID sweep (deps may be null: a grid barrier
+// after every level): CTA b publishes at prog[b * 8] the number of levels it
+// has finished; before level l it waits for deps[dptr[l*ncta + b] ..
+// dptr[l*ncta + b + 1]) = {cta, levels that CTA must have finished}.  prog
+// holds ncta * 8 words and is zeroed by the launcher.
+struct GsDeps {
+    const int *dptr;
+    const int2 *deps;
+    unsigned *prog;
+};
 cudaError_t gs_sweep_lcsr(Prec p, int nv, int mode, int xs, int nlev, int ncta, const int *lev_row,
                           const int *blev, const int *lrp, const int *lci, const void *lva,
                           const int *lrow, const void *invd, const void *t, void *x,
                           const void *relax, i64 brows, i64 n, unsigned *gbar, int *err,
-                          int emax, const GsSlotWin *win, cudaStream_t s);
+                          int emax, const GsSlotWin *win, const GsDeps *deps, cudaStream_t s);
 // Bounded-wait self-test (which 0: grid barrier with one CTA missing; 1:
 // mbarrier phase that nothing completes), limit in ns; words: 256 bytes of
 // device scratch, err: one device int (0 after a wait that did not run out).
