@@ -33,6 +33,13 @@ int xcnn_conv3d(const void *in, int ics, int ic0, int cin, const void *w, const 
  * voxel staged once per 16-channel chunk), 0 = voxel-tile kernel.  Returns the
  * previous setting. */
 int xcnn_set_box_conv(int on);
+/* 1 = xcnn_conv3d runs on the 5th-generation tensor cores (tcgen05.mma with a
+ * TMEM accumulator; the same convolution, FP32 accumulation in another order);
+ * takes precedence over the box choice.  Returns the previous setting. */
+int xcnn_set_tc_conv(int on);
+/* 1 when a tcgen05 convolution gave up waiting on its tensor pipe (bounded
+ * wait) since the last call; the flag is then cleared.  -1 on a CUDA error. */
+int xcnn_tc_error(void);
 /* dw[co][t][ci] += sum_p grad[p][gc0+co] * in[p + off(t)][ic0+ci]; cout is
  * 16, 32, 64 or 128. */
 int xcnn_conv3d_wgrad(const void *in, int ics, int ic0, int cin, const void *grad, int gcs,

@@ -67,12 +67,13 @@ def _np(t):
 @pytest.mark.gpu
 @pytest.mark.parametrize("dims", [(2, 8, 8, 8), (1, 6, 10, 12), (1, 4, 16, 24)])
 @pytest.mark.parametrize("cin,cout", [(16, 16), (48, 64), (32, 48), (16, 128)])
-@pytest.mark.parametrize("box", [1, 0])
-def test_conv3d_matches_oracle(gpu, dims, cin, cout, box):
+@pytest.mark.parametrize("kernel", ["box", "tile", "tcgen05"])
+def test_conv3d_matches_oracle(gpu, dims, cin, cout, kernel):
     import torch
     import learned
     L = learned.klib()
-    old = L.xcnn_set_box_conv(box)
+    old = L.xcnn_set_box_conv(int(kernel == "box"))
+    old_tc = L.xcnn_set_tc_conv(int(kernel == "tcgen05"))
     rng = np.random.default_rng(cin * 7 + cout)
     nb, d, h, w = dims
     # input window: channels [16, 16 + cin) of a buffer with cin + 32 channels
@@ -106,7 +107,9 @@ def test_conv3d_matches_oracle(gpu, dims, cin, cout, box):
                          nb, d, h, w, 4, None) == 0
     got = _np(O)[..., 16:16 + cout]
     assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max()
+    assert L.xcnn_tc_error() == 0
     L.xcnn_set_box_conv(old)
+    L.xcnn_set_tc_conv(old_tc)
 
 
 @pytest.mark.gpu

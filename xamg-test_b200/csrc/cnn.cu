@@ -662,6 +662,224 @@ __global__ void k_unpack_x0(const float *__restrict__ in, int cs, int c0, const 
     }
 }
 
+// ---------------------------------------------------------------- tcgen05 conv3d
+// The same convolution on the 5th-generation tensor cores: implicit GEMM with
+// M = 128 voxels, N = BN output channels, K = 16 channels of one tap per
+// step.  The 128 threads stage A (the tap's shifted voxel rows) and B (the
+// weights) by cp.async exactly as k_conv3d does: 32-byte rows with the
+// 16-byte halves swapped on bit 2 of the row, which is the canonical K-major
+// SWIZZLE_32B layout of the UMMA shared-memory descriptors (8-row groups 256
+// bytes apart).  One thread issues tcgen05.mma (kind::f16, BF16 x BF16 ->
+// FP32) into a TMEM accumulator of BN columns and commits each step to the
+// stage's mbarrier, which tells the producers when the stage may be
+// refilled.  The epilogue reads TMEM with tcgen05.ld (warp w: lanes 32w ..
+// 32w+31 = its voxels).  Every mbarrier wait is bounded; on expiry the error
+// word is set, the CTA stops issuing and frees its TMEM after the tensor
+// pipe has drained (bounded as well).
+__device__ int g_tc_err;
+
+__device__ __forceinline__ unsigned long long tc_now() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void tc_mbar_init(unsigned long long *b) {
+    asm volatile("mbarrier.init.shared.b64 [%0], 1;" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool tc_mbar_try(unsigned long long *b, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool tc_mbar_wait(unsigned long long *b, unsigned parity) {
+    if (tc_mbar_try(b, parity)) return true;
+    const unsigned long long t0 = tc_now();
+    while (!tc_mbar_try(b, parity))
+        if (tc_now() - t0 > 1000000000ull) return false;
+    return true;
+}
+// K-major SWIZZLE_32B shared-memory matrix descriptor: start address, leading
+// byte offset 1 (unused within one swizzle atom), stride between 8-row groups
+// 256 bytes, descriptor version 1, layout type 6
+__device__ __forceinline__ unsigned long long tc_desc(const void *p) {
+    const unsigned long long a = (smem_u32(p) & 0x3FFFFu) >> 4;
+    return a | (1ull << 16) | ((unsigned long long)(256 >> 4) << 32) | (1ull << 46) | (6ull << 61);
+}
+
+template <int BN>
+__global__ void __launch_bounds__(128) k_conv3d_tc(const bf16 *__restrict__ in, int ics, int ic0, int cin,
+                                                   const bf16 *__restrict__ w, const float *__restrict__ bias,
+                                                   bf16 *out, int ocs, int oc0, int cout, Vol g, int flags) {
+    constexpr int TCOLS = BN < 32 ? 32 : BN;  // TMEM columns (a power of two >= 32)
+    __shared__ __align__(1024) unsigned char sa[NS][BM * 32];
+    __shared__ __align__(1024) unsigned char sb[NS][BN * 32 < 1024 ? 1024 : BN * 32];
+    __shared__ __align__(8) unsigned long long mbar[NS];
+    __shared__ unsigned s_tmem;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const i64 nvox = g.count();
+    const i64 v0 = (i64)blockIdx.x * BM;
+    const int n0 = blockIdx.y * BN;
+    const int kc = cin / 16;
+    const int nk = 27 * kc;
+    const i64 myv = v0 + tid;
+    const bool vin = myv < nvox;
+    int vx = 0, vy = 0, vz = 0;
+    if (vin) {
+        vx = (int)(myv % g.w);
+        vy = (int)((myv / g.w) % g.h);
+        vz = (int)((myv / ((i64)g.w * g.h)) % g.d);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int q = 0; q < NS; ++q) tc_mbar_init(&mbar[q]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_fail = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = s_tmem;
+    // instruction descriptor: FP32 accumulator, BF16 A and B, both K-major,
+    // N = BN, M = 128
+    const unsigned idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(BN >> 3) << 17) | ((128u >> 4) << 24);
+
+    auto stage = [&](int k, int st) {
+        const int t = k / kc, cb = (k % kc) * 16;
+        const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+        const bool inside = vin && (unsigned)(vz + dz) < (unsigned)g.d && (unsigned)(vy + dy) < (unsigned)g.h &&
+                            (unsigned)(vx + dx) < (unsigned)g.w;
+        const i64 src = inside ? myv + ((i64)dz * g.h + dy) * g.w + dx : -1;
+        const bf16 *pa = in + (src < 0 ? 0 : src) * ics + ic0 + cb;
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh) cp16(&sa[st][sw32(tid, hh)], pa + hh * 8, src < 0 ? 0u : 16u);
+        for (int q = tid; q < BN * 2; q += 128) {
+            const int r = q >> 1, hh = q & 1;
+            const bf16 *pb = w + ((i64)(n0 + r) * 27 + t) * cin + cb + hh * 8;
+            cp16(&sb[st][sw32(r, hh)], pb, 16u);
+        }
+    };
+    unsigned uses[NS] = {0u, 0u, 0u, 0u};  // completed MMA phases awaited per stage
+    bool ok = true;
+#pragma unroll
+    for (int q = 0; q < NS - 1; ++q) {
+        if (q < nk) stage(q, q);
+        cp_commit();
+    }
+    for (int k = 0; k < nk; ++k) {
+        // refill the stage that step k-1 read once its MMA has completed
+        const int kn = k + NS - 1;
+        if (kn < nk) {
+            const int st = kn % NS;
+            if (k >= 1) {
+                if (ok && !tc_mbar_wait(&mbar[st], uses[st] & 1u)) ok = false;
+                uses[st]++;
+            }
+            stage(kn, st);
+        }
+        cp_commit();
+        cp_wait<NS - 2>();
+        // the copies of step k are complete: publish them to the tensor core
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        ok = __syncthreads_and(ok) != 0;
+        if (!ok) break;
+        if (tid == 0) {
+            const int st = k % NS;
+            const unsigned long long da = tc_desc(&sa[st][0]), db = tc_desc(&sb[st][0]);
+            const unsigned acc = k > 0 ? 1u : 0u;
+            asm volatile(
+                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem),
+                "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                : "memory");
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&mbar[st]))
+                         : "memory");
+        }
+    }
+    cp_wait<0>();
+    // the last step's commit completes after every earlier MMA
+    if (ok && nk > 0) {
+        const int st = (nk - 1) % NS;
+        // phases of this stage awaited so far, plus the ones not awaited
+        unsigned ph = uses[st];
+        for (int k = st; k < nk; k += NS) {
+            if ((unsigned)(k / NS) < ph) continue;
+            if (!tc_mbar_wait(&mbar[st], (unsigned)(k / NS) & 1u)) { ok = false; break; }
+        }
+    }
+    ok = __syncthreads_and(ok) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+        const bool relu = flags & 1, accum = flags & 2, f32out = flags & 4;
+        const i64 v = v0 + warp * 32 + lane;
+#pragma unroll
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            unsigned r[16];
+            const unsigned ta = tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(ta));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (v >= nvox) continue;
+#pragma unroll
+            for (int e = 0; e < 16; e += 2) {
+                const int n = n0 + c0 + e;
+                float y0 = __uint_as_float(r[e]), y1 = __uint_as_float(r[e + 1]);
+                if (bias) {
+                    y0 += bias[n];
+                    y1 += bias[n + 1];
+                }
+                if (relu) {
+                    y0 = fmaxf(y0, 0.f);
+                    y1 = fmaxf(y1, 0.f);
+                }
+                if (f32out) {
+                    float2 *pf = reinterpret_cast<float2 *>(reinterpret_cast<float *>(out) + v * ocs + oc0 + n);
+                    if (accum) {
+                        const float2 o = *pf;
+                        y0 += o.x;
+                        y1 += o.y;
+                    }
+                    *pf = make_float2(y0, y1);
+                } else {
+                    __nv_bfloat162 *po = reinterpret_cast<__nv_bfloat162 *>(out + v * ocs + oc0 + n);
+                    if (accum) {
+                        const float2 o = __bfloat1622float2(*po);
+                        y0 += o.x;
+                        y1 += o.y;
+                    }
+                    *po = __floats2bfloat162_rn(y0, y1);
+                }
+            }
+        }
+    } else if (tid == 0) {
+        atomicExch(&g_tc_err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS) : "memory");
+    }
+}
+
+// the tcgen05 kernel is used when switched on (xcnn_set_tc_conv(1))
+int g_tc_conv = 0;
+
 // the box kernel is the default; xcnn_set_box_conv(0) selects the
 // voxel-tile kernel (both compute the same convolution)
 int g_box_conv = 1;
@@ -700,6 +918,13 @@ int xcnn_conv3d(const void *in, int ics, int ic0, int cin, const void *w, const 
     const bf16 *pi = (const bf16 *)in;
     const bf16 *pw = (const bf16 *)w;
     bf16 *po = (bf16 *)out;
+    if (g_tc_conv) {
+        dim3 grid((unsigned)((nvox + BM - 1) / BM), (unsigned)(cout / bn));
+        if (bn == 64) k_conv3d_tc<64><<<grid, 128, 0, s>>>(pi, ics, ic0, cin, pw, bias, po, ocs, oc0, cout, g, flags);
+        else if (bn == 32) k_conv3d_tc<32><<<grid, 128, 0, s>>>(pi, ics, ic0, cin, pw, bias, po, ocs, oc0, cout, g, flags);
+        else k_conv3d_tc<16><<<grid, 128, 0, s>>>(pi, ics, ic0, cin, pw, bias, po, ocs, oc0, cout, g, flags);
+        return last_err();
+    }
     // box kernel when the volume tiles into 128-voxel boxes of at least 8 x 8
     // in (y, x): sides multiples of 8 and a depth that is a multiple of 2
     const int bx = 8, by = 8, bz = 2;
@@ -828,6 +1053,20 @@ int xcnn_unpack_x0(const void *in, int cs, int c0, const float *scale, int nv, i
     return last_err();
 }
 
+int xcnn_set_tc_conv(int on) {
+    const int old = g_tc_conv;
+    g_tc_conv = on != 0;
+    return old;
+}
+// 1 when a tcgen05 convolution gave up waiting on its tensor pipe since the
+// last call (then cleared)
+int xcnn_tc_error() {
+    int h = 0;
+    if (cudaMemcpyFromSymbol(&h, g_tc_err, sizeof(int)) != cudaSuccess) return -1;
+    const int z = 0;
+    if (h) cudaMemcpyToSymbol(g_tc_err, &z, sizeof(int));
+    return h;
+}
 int xcnn_set_box_conv(int on) {
     const int old = g_box_conv;
     g_box_conv = on != 0;

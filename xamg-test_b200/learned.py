@@ -64,6 +64,8 @@ _SIGS = {
     "xcnn_pack2": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p],
     "xcnn_unpack": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p],
     "xcnn_set_box_conv": [C.c_int],
+    "xcnn_set_tc_conv": [C.c_int],
+    "xcnn_tc_error": [],
     "xcnn_unpack_x0": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int64, C.c_void_p, C.c_void_p],
 }
 
