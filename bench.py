@@ -254,6 +254,10 @@ def spmv_roofline(csr, variant):
                     variant, "k_spmv_stream<double,16,0>")
     peak, src = peak_hbm()
     ach = byts / (ms * 1e-3) / 1e9
+    # the CSR product's bytes (values, column indices, row pointers, x, y):
+    # the operation's algorithmic bytes whatever format stores the operator
+    csr_bytes = nnz * (8 + 4) + (n + 1) * 4 + xy
+    ach_csr = csr_bytes / (ms * 1e-3) / 1e9
     # DRAM traffic per launch: the ncu capture of the same kernel on the 96^3
     # operator measured TRAFFIC_RATIO x its algorithmic bytes; traffic scales
     # with the operator, so the 128^3 figure is that ratio times the
@@ -263,7 +267,9 @@ def spmv_roofline(csr, variant):
     out = {"bound": "hbm", "kernel": kern, "variant": variant, "achieved": round(ach, 1), "peak": peak,
            "peak_source": src, "unit": "GB/s", "frac": round(ach / peak, 4),
            "traffic": traffic, "traffic_source": "ncu capture at 96^3 scaled to 128^3" if traffic else None,
-           "algorithmic_bytes": byts, "launch_ms": round(ms, 4)}
+           "algorithmic_bytes": byts, "launch_ms": round(ms, 4),
+           "csr_equivalent": {"bytes": csr_bytes, "achieved": round(ach_csr, 1),
+                              "frac": round(ach_csr / peak, 4)}}
     if info:
         out["run_plan"] = info
     return out
