@@ -158,8 +158,10 @@ def build_problem():
 
 
 # SpMV kernels timed for the roofline: CSR variants of xamg_spmv_set_variant,
-# and RUN8 = the shifted-row run kernel (chunks of 8 rows)
-RUN8 = 108
+# and RUN8 = the shifted-row run kernel (chunks of 8 rows), RUN8X = the same
+# with each segment's x rows staged in shared memory one segment ahead
+RUN8, RUN8X = 108, 109
+RUNS = (RUN8, RUN8X)
 
 
 def spmv_time(csr, prec=0, variant=-1, iters=20, info=None, mode=0):
@@ -178,7 +180,8 @@ def spmv_time(csr, prec=0, variant=-1, iters=20, info=None, mode=0):
     P = lambda t: C.c_void_p(t.data_ptr())
     L = xamg.lib()
     plan = None
-    if variant == RUN8:
+    old_form = L.xamg_spmv_set_run_form(int(variant == RUN8X))
+    if variant in RUNS:
         plan = L.xamg_spmv_runs_plan_create(n, xamg._ptr(rp), xamg._ptr(ci), xamg._ptr(np.ascontiguousarray(v)),
                                             8, int(prec == 1))
         assert plan, L.XAMG_b200_last_error()
@@ -208,6 +211,7 @@ def spmv_time(csr, prec=0, variant=-1, iters=20, info=None, mode=0):
         st.synchronize()
     finally:
         L.xamg_spmv_set_variant(old)
+        L.xamg_spmv_set_run_form(old_form)
         if plan:
             L.xamg_spmv_runs_plan_destroy(plan)
     return e0.elapsed_time(e1) / iters
@@ -217,7 +221,7 @@ def tune_spmv(csr, prec=0):
     """Autotune the SpMV kernel on this matrix (results are identical for
     every kernel; only the data layout and launch shape differ)."""
     res = {}
-    for var in (0, 3, 5, 6, RUN8):
+    for var in (0, 3, 5, 6, RUN8, RUN8X):
         res[var] = spmv_time(csr, prec, var, iters=10)
     best = min(res, key=res.get)
     return best, res
@@ -228,9 +232,10 @@ def apply_spmv_choice(var):
     plans built at matrix construction) or a CSR variant everywhere."""
     import xamg
     L = xamg.lib()
-    if var == RUN8:
+    if var in RUNS:
         L.xamg_spmv_set_run_rows(8)
         L.xamg_spmv_set_variant(-1)
+        L.xamg_spmv_set_run_form(int(var == RUN8X))
     else:
         L.xamg_spmv_set_run_rows(0)
         L.xamg_spmv_set_variant(var)
@@ -241,11 +246,11 @@ def spmv_roofline(csr, variant):
     ms = spmv_time(csr, 0, variant, iters=20, info=info)
     n, nnz = csr.nrows, csr.nnz
     xy = 2 * n * NV * 8
-    if variant == RUN8:
+    if variant in RUNS:
         # run format: each value once, each chunk's segments once (4 B), the
         # chunk descriptors (16 B) and tile offsets (16 B per four chunks), x and y
         byts = nnz * 8 + info["segments"] * 4 + info["nchunks"] * 20 + xy
-        kern = "k_spmv_runs<double,16,0>"
+        kern = "k_spmv_runs<double,16,0,128,%s>" % ("true" if variant == RUN8X else "false")
     else:
         byts = nnz * (8 + 4) + (n + 1) * 4 + xy
         kern = {0: "k_spmv<double,16,0,4>", 1: "k_spmv<double,16,0,8>", 2: "k_spmv<double,16,0,16>",

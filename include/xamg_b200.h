@@ -228,6 +228,11 @@ int xamg_spmv_runs(void *plan, int prec, int nv, const void *x, void *y, int mod
                    void *stream);
 int xamg_spmv_runs_plan_destroy(void *plan);
 int xamg_spmv_set_run_rows(int rows);
+/* Kernel form of the run products of the calling host thread: 0 (default)
+ * gathers each segment's x rows into registers, 1 copies them into shared
+ * memory one segment ahead (cp.async, fewer registers, two segments in
+ * flight).  Same results.  Returns the previous setting. */
+int xamg_spmv_set_run_form(int form);
 
 /* Gauss-Seidel plan (wavefront schedule) for blas2::SGS / csr_SGS
  * (blas2.h:184-281, csr_gs.inl:32-134).  rp/ci are HOST arrays.  block_rows

@@ -105,12 +105,16 @@ def _run_matrices():
     return out
 
 
+@pytest.mark.parametrize("form", [0, 1], ids=["x_in_registers", "x_staged"])
 @pytest.mark.parametrize("dtype,nv", [(np.float64, 8), (np.float64, 16), (np.float64, 32),
                                       (np.float32, 16), (np.float32, 32)])
-def test_spmv_runs_bit_exact(gpu, dtype, nv):
-    """Shifted-row run kernel: identical bits to the oracle's CSR product in
-    all three modes, on stencil, irregular and mixed operators."""
+def test_spmv_runs_bit_exact(gpu, dtype, nv, form):
+    """Shifted-row run kernel, both forms (x rows gathered into registers, or
+    copied into shared memory a segment ahead): identical bits to the
+    oracle's CSR product in all three modes, on stencil, irregular and mixed
+    operators."""
     L = xamg.lib()
+    old_form = L.xamg_spmv_set_run_form(form)
     prec = 0 if dtype == np.float64 else 1
     for mi, (rp, ci, v) in enumerate(_run_matrices()):
         n = len(rp) - 1
@@ -145,6 +149,7 @@ def test_spmv_runs_bit_exact(gpu, dtype, nv):
                 assert np.array_equal(got, ref), (mi, mode, np.abs(got - ref).max())
         finally:
             L.xamg_spmv_runs_plan_destroy(plan)
+    L.xamg_spmv_set_run_form(old_form)
 
 
 def test_spmv_runs_rejects_narrow_shapes(gpu):

@@ -744,6 +744,11 @@ int xamg_spmv_set_variant(int variant) {
     xk::set_spmv_variant(variant);
     return old;
 }
+int xamg_spmv_set_run_form(int form) {
+    int old = xk::get_spmv_run_form();
+    xk::set_spmv_run_form(form);
+    return old;
+}
 int xamg_spmv_set_run_rows(int rows) {
     int old = xk::get_spmv_run_rows();
     xk::set_spmv_run_rows(rows);

@@ -427,9 +427,14 @@ template <class T, int NV, int NT> struct RunShape {
     static constexpr int SMEM_BYTES = SLOTS * (4 + RUN_ROWS * (int)sizeof(T));
 };
 
-template <class T, int NV, int MODE, bool SMEM>
+// STX: the x rows of each segment are copied by cp.async into this thread's
+// own slice of a two-segment shared-memory buffer (xs, NX pieces of 16 bytes
+// per segment and thread, strided by the CTA's thread count), one segment
+// ahead of their use, instead of being held in registers: fewer registers a
+// thread and two segments of gathers in flight.  Same FMA chains.
+template <class T, int NV, int MODE, bool SMEM, bool STX = false, int NT = 128>
 __device__ __forceinline__ void run_rows(const int4 cd, int smax, const int *sg, const T *val, const T *xb,
-                                         T *__restrict__ y, const T *__restrict__ b, int l) {
+                                         T *__restrict__ y, const T *__restrict__ b, int l, T *xs = nullptr) {
     constexpr int V = Shape<T, NV>::V, R = RUN_ROWS, NX = RUN_SEG + R - 1;
     T acc[R][V];
 #pragma unroll
@@ -444,6 +449,45 @@ __device__ __forceinline__ void run_rows(const int4 cd, int smax, const int *sg,
     auto seg = [&](int s) { return s < cd.w ? (SMEM ? sg[4 * s] : __ldcs(sg + 4 * s)) : 0; };
     int e = 0;
     int sc = seg(0);
+    if constexpr (STX) {
+        // xs slice of this thread: piece k of buffer u at xs[((u * NX + k) * NT + tid) * V]
+        const int tid = threadIdx.x;
+        auto issue = [&](int scv, int u) {
+            const int c0 = scv & 0x3fffffff, len = (int)((unsigned)scv >> 30);
+            const int nx = len + cd.y - 1;
+#pragma unroll
+            for (int k = 0; k < NX; ++k)
+                if (k < nx && len > 0)
+                    cp_async16(xs + ((i64)(u * NX + k) * NT + tid) * V, xb + ((i64)c0 + k) * NV);
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        };
+        issue(sc, 0);
+        for (int s = 0; s < smax; ++s) {
+            const int c0 = sc & 0x3fffffff, len = (int)((unsigned)sc >> 30);
+            (void)c0;
+            const int scn = seg(s + 1);
+            issue(s + 1 < smax ? scn : 0, (s + 1) & 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+            const T *xu = xs + (i64)((s & 1) * NX) * NT * V + (i64)tid * V;
+#pragma unroll
+            for (int j = 0; j < RUN_SEG; ++j) {
+                if (j < len) {
+                    T a[R];
+                    ld_vals<T, R, SMEM>(val + (i64)4 * (e + j) * R, a);
+#pragma unroll
+                    for (int q = 0; q < R; ++q) {
+                        T X[V];
+                        ld<T, V>(xu + (i64)(q + j) * NT * V, X);
+#pragma unroll
+                        for (int v = 0; v < V; ++v) acc[q][v] = fma(a[q], X[v], acc[q][v]);
+                    }
+                }
+            }
+            e += len;
+            sc = scn;
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    } else {
     for (int s = 0; s < smax; ++s) {
         const int c0 = sc & 0x3fffffff, len = (int)((unsigned)sc >> 30);
         const int nx = len + cd.y - 1;
@@ -465,6 +509,7 @@ __device__ __forceinline__ void run_rows(const int4 cd, int smax, const int *sg,
         }
         e += len;
     }
+    }
 #pragma unroll
     for (int q = 0; q < R; ++q) {
         if (q >= cd.y) break;
@@ -481,8 +526,12 @@ __device__ __forceinline__ void run_rows(const int4 cd, int smax, const int *sg,
 }
 
 constexpr int RUN_NT = 128;
-template <class T, int NV, int MODE, int NT>
-__global__ void __launch_bounds__(NT, 5) k_spmv_runs(i64 nchunks, i64 ntiles, const int4 *__restrict__ chunks,
+// x staging buffer of the STX form: two segments of NX 16-byte pieces a thread
+template <int NT> struct RunXs {
+    static constexpr int BYTES = 2 * (RUN_SEG + RUN_ROWS - 1) * NT * 16;
+};
+template <class T, int NV, int MODE, int NT, bool STX = false>
+__global__ void __launch_bounds__(NT, STX ? 3 : 5) k_spmv_runs(i64 nchunks, i64 ntiles, const int4 *__restrict__ chunks,
                                                       const longlong2 *__restrict__ toff,
                                                       const int *__restrict__ sg,
                                                       const T *__restrict__ vt,
@@ -516,30 +565,40 @@ __global__ void __launch_bounds__(NT, 5) k_spmv_runs(i64 nchunks, i64 ntiles, co
     const int slot = (int)(gid & 3);
     const i64 le = ot.x - o0.x + slot, ls = ot.y - o0.y + slot;  // CTA-local first value / segment slot
     const T *xb = x + l * V;
-    if (staged) run_rows<T, NV, MODE, true>(cd, smax, s_sg + ls, s_vt + le * RUN_ROWS, xb, y, b, l);
-    else run_rows<T, NV, MODE, false>(cd, smax, sg + o0.y + ls, vt + (o0.x + le) * RUN_ROWS, xb, y, b, l);
+    T *xs = reinterpret_cast<T *>(run_smem + RunShape<T, NV, NT>::SMEM_BYTES);
+    if (staged)
+        run_rows<T, NV, MODE, true, STX, NT>(cd, smax, s_sg + ls, s_vt + le * RUN_ROWS, xb, y, b, l, xs);
+    else
+        run_rows<T, NV, MODE, false, STX, NT>(cd, smax, sg + o0.y + ls, vt + (o0.x + le) * RUN_ROWS, xb, y, b, l,
+                                             xs);
 }
+
+// kernel form of the run product: 0 = x rows in registers, 1 = x rows staged
+// in shared memory one segment ahead (per host thread; same results)
+static thread_local int g_run_form = 0;
+void set_spmv_run_form(int f) { g_run_form = f ? 1 : 0; }
+int get_spmv_run_form() { return g_run_form; }
 
 bool spmv_runs_supported(Prec p, int nv) {
     return p == Prec::F64 ? (nv == 8 || nv == 16 || nv == 32) : (nv == 16 || nv == 32);
 }
 
-template <class T, int NV, int NT>
+template <class T, int NV, int NT, bool STX>
 static void spmv_runs_p(i64 nchunks, i64 ntiles, const int4 *chunks, const longlong2 *toff, const int *sg,
                         const T *vt, const T *x, T *y, int mode, const T *b, cudaStream_t s) {
     typedef RunShape<T, NV, NT> RS;
-    constexpr int SM = RS::SMEM_BYTES;
+    constexpr int SM = RS::SMEM_BYTES + (STX ? RunXs<NT>::BYTES : 0);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_spmv_runs<T, NV, 0, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
-        cudaFuncSetAttribute(k_spmv_runs<T, NV, 1, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
-        cudaFuncSetAttribute(k_spmv_runs<T, NV, 2, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+        cudaFuncSetAttribute(k_spmv_runs<T, NV, 0, NT, STX>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+        cudaFuncSetAttribute(k_spmv_runs<T, NV, 1, NT, STX>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+        cudaFuncSetAttribute(k_spmv_runs<T, NV, 2, NT, STX>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
         attr = true;
     }
     unsigned g = (unsigned)((ntiles + RS::TPC - 1) / RS::TPC);
-    if (mode == 0) k_spmv_runs<T, NV, 0, NT><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
-    else if (mode == 1) k_spmv_runs<T, NV, 1, NT><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
-    else k_spmv_runs<T, NV, 2, NT><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
+    if (mode == 0) k_spmv_runs<T, NV, 0, NT, STX><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
+    else if (mode == 1) k_spmv_runs<T, NV, 1, NT, STX><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
+    else k_spmv_runs<T, NV, 2, NT, STX><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
 }
 
 template <class T, int NV>
@@ -548,7 +607,8 @@ static void spmv_runs_t(i64 nchunks, i64 ntiles, const int4 *chunks, const longl
     if constexpr (NV >= 8 && NV * sizeof(T) >= 64) {
         if (nchunks <= 0) return;
         note_launch();
-        spmv_runs_p<T, NV, RUN_NT>(nchunks, ntiles, chunks, toff, sg, vt, x, y, mode, b, s);
+        if (g_run_form) spmv_runs_p<T, NV, RUN_NT, true>(nchunks, ntiles, chunks, toff, sg, vt, x, y, mode, b, s);
+        else spmv_runs_p<T, NV, RUN_NT, false>(nchunks, ntiles, chunks, toff, sg, vt, x, y, mode, b, s);
     }
 }
 

@@ -54,6 +54,10 @@ int get_spmv_run_rows();
 // Same modes and the same results, bit for bit, as spmv().  FP64 nv 8, 16, 32
 // and FP32 nv 16, 32.
 bool spmv_runs_supported(Prec p, int nv);
+// kernel form of the run product (per host thread): 0 = each segment's x rows
+// gathered into registers, 1 = copied into shared memory one segment ahead
+void set_spmv_run_form(int f);
+int get_spmv_run_form();
 void spmv_runs(Prec p, int nv, i64 nchunks, i64 ntiles, const int4 *chunks, const longlong2 *toff, const int *sg,
                const void *vt, const void *x, void *y, int mode, const void *b, cudaStream_t s);
 

@@ -114,6 +114,7 @@ def lib():
             "xamg_csr_spmv": (C.c_int, [C.c_int, C.c_int, i64, P, P, P, P, P, C.c_int, P, P]),
             "xamg_spmv_set_variant": (C.c_int, [C.c_int]),
             "xamg_spmv_set_run_rows": (C.c_int, [C.c_int]),
+            "xamg_spmv_set_run_form": (C.c_int, [C.c_int]),
             "xamg_spmv_runs_plan_create": (P, [i64, P, P, P, C.c_int, C.c_int]),
             "xamg_spmv_runs_plan_info": (C.c_int, [P, P, P, P, P]),
             "xamg_spmv_runs_analyze": (C.c_int, [i64, P, P, C.c_int, P, P, P]),
