@@ -476,8 +476,11 @@ __device__ __forceinline__ void run_rows(const int4 cd, int smax, const int *sg,
                     ld_vals<T, R, SMEM>(val + (i64)4 * (e + j) * R, a);
 #pragma unroll
                     for (int q = 0; q < R; ++q) {
+                        // a shared-memory read (not the read-only global path)
+                        typedef typename VT<T, V>::type W;
+                        const W xw = *reinterpret_cast<const W *>(xu + (i64)(q + j) * NT * V);
                         T X[V];
-                        ld<T, V>(xu + (i64)(q + j) * NT * V, X);
+                        memcpy(X, &xw, sizeof(W));
 #pragma unroll
                         for (int v = 0; v < V; ++v) acc[q][v] = fma(a[q], X[v], acc[q][v]);
                     }
