@@ -326,6 +326,8 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
         }
     };
     Desc dc = l0 < l1 ? dget(l0) : Desc{0, 0, 0, 0};
+    Desc dq1 = l0 + 1 < l1 ? dget(l0 + 1) : Desc{0, 0, 0, 0};
+    Desc dq2 = l0 + 2 < l1 ? dget(l0 + 2) : Desc{0, 0, 0, 0};
     int dfirst = 0, dcnt = 0;
     int2 dn = make_int2(0, 0);
     if (MODE == 0 && gd.dptr && l0 + 1 < l1) {
@@ -363,9 +365,12 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
             }
             cp_async_commit();
         }
-        Desc dnx{0, 0, 0, 0};
+        // descriptors come through a two-level register queue: level l+3's
+        // is loaded now and used two levels later, off the critical path
+        const Desc dnx = dq1;
+        dq1 = dq2;
+        if (l + 3 < l1) dq2 = dget(l + 3);
         if (l + 1 < l1) {
-            dnx = dget(l + 1);
             wait_q((l + 1) % NB);
             prefetch(l + 1, dnx);
         }
