@@ -15,6 +15,8 @@ guess.  Forms (all on the same operator and right-hand sides):
                  so that its error against the FP64 solution is <= 1e-8;
   sweep        - the mixed form for nv in {1, 4, 8, 16, 32} with error against
                  an FP64 solve converged to 1e-12;
+  c1           - the plain method's CPU-runnable case (32^3 7-point Poisson,
+                 BiCGStab, one RHS) on the GPU beside the oracle on the host;
   dist         - the system split over the ranks by row blocks (NCCL halo
                  exchange, allreduce of the inner products, block-Jacobi AMG
                  with the plain_hybrid settings); at N = 1 one rank;
@@ -538,6 +540,34 @@ def dist_form(csr, B, rank, world, dist, warmup, steps):
     return out
 
 
+def c1_form(warmup, steps):
+    """The plain method's CPU-runnable case: 3-D 7-point Poisson on 32^3
+    (Dirichlet, the reference cube generator's configuration 0), one RHS
+    uniform[-1,1], unpreconditioned BiCGStab to 1e-8 from zero.  GPU time per
+    solve (device events) beside the oracle's on the host, and the two must
+    take the same iterations with the same residual history."""
+    import xamg
+    csr = xamg.CsrMatrix.cube(32, 32, 32, 0)
+    rp, ci, v = csr.arrays()
+    B = np.random.default_rng(SEED).uniform(-1.0, 1.0, (csr.nrows, 1))
+    spec = {"solver": {"method": "BiCGStab", "max_iters": 1000, "abs_tolerance": 0.0, "rel_tolerance": 1e-8,
+                       "convergence_details": "check-L2,noprint"}}
+    f = Form(csr, B, spec)
+    r = f.run(warmup, steps)
+    hist = f.s.history()
+    orc = oracle_mod()
+    t0 = time.perf_counter()
+    xo, it, ho, st, _ = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), None, 1000, 0.0, 1e-8)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    out = {"rows": csr.nrows, "nnz": csr.nnz, "ms": round(r["ms"], 3), "iters": r["iters"],
+           "converged": r["converged"], "launches": r["launches"], "cpu_oracle_ms": round(cpu_ms, 2),
+           "cpu_threads": orc.num_threads(), "same_iterations_and_history": bool(it == r["iters"] and
+                                                                                  np.array_equal(ho, hist))}
+    del f
+    xamg.set_nv(NV)
+    return out
+
+
 def learned_form(nsys=16):
     """Learned form: held-out 64^3 bump-coefficient systems (nv = 8) solved
     from a zero guess and from the trained network's guess (2 symmetric
@@ -714,7 +744,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--forms", default="plain,plain_hybrid,mixed,mixed_tight,sweep,dist,batch,learned")
+    ap.add_argument("--forms", default="plain,plain_hybrid,mixed,mixed_tight,sweep,dist,c1,batch,learned")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tight-tol", type=float, default=1e-10,
                     help="outer tolerance of the mixed form run to the error target (error vs FP64 <= 1e-8)")
@@ -851,6 +881,8 @@ def main():
         extra["batch"]["ms_per_rhs"] = round(extra["batch"]["ms"] / tot, 4)
     if "dist" in allforms:
         extra["dist"] = dist_form(csr, B, rank, world, dist, 1, 3)
+    if "c1" in allforms and rank == 0:
+        extra["c1"] = c1_form(args.warmup, args.steps)
     if "learned" in allforms and rank == 0:
         extra["learned"] = learned_form()
     roof = spmv_roofline(csr, best_var)
