@@ -238,11 +238,12 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
     unsigned use[NB] = {0u, 0u, 0u};
     // issuer: the last thread, which rarely owns a row of a level
     const bool issuer = tid == 255;
-    auto issue = [&](int l, const Desc &d) {
+    // the slot window's load range of level l (loaded with the level's
+    // descriptor, one iteration before it is needed)
+    auto lget = [&](int l) { return SL ? __ldg(sw.ldd + dbase + l) : make_int2(0, 0); };
+    auto issue = [&](int l, const Desc &d, int2 lr) {
         int q = l % NB;
         int nr = rspan(d), ne = d.e1 - d.e0, ra = rlo(d);
-        int2 lr = make_int2(0, 0);
-        if (SL) lr = __ldg(sw.ldd + dbase + l);
         const int nl = lr.y - lr.x;
         if (d.r1 > d.r0 && nr <= RB && ne <= E && nl <= LB) {
             unsigned bytes = (unsigned)ne * (4u + (unsigned)sizeof(T)) + (unsigned)(nr + 4) * 4u +
@@ -276,10 +277,11 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
         }
     };
     Desc dn1{0, 0, 0, 0}, dn2{0, 0, 0, 0};
+    int2 ln2 = make_int2(0, 0);
     if (issuer) {
-        if (l0 < l1) issue(l0, dget(l0));
-        if (l0 + 1 < l1) { dn1 = dget(l0 + 1); issue(l0 + 1, dn1); }
-        if (l0 + 2 < l1) dn2 = dget(l0 + 2);
+        if (l0 < l1) issue(l0, dget(l0), lget(l0));
+        if (l0 + 1 < l1) { dn1 = dget(l0 + 1); issue(l0 + 1, dn1, lget(l0 + 1)); }
+        if (l0 + 2 < l1) { dn2 = dget(l0 + 2); ln2 = lget(l0 + 2); }
     }
     __syncthreads();
     bool ok = true;
@@ -352,8 +354,8 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
     for (int l = l0; ok && l < l1; ++l) {
         const int q = l % NB;
         if (issuer && l + 2 < l1) {
-            issue(l + 2, dn2);
-            if (l + 3 < l1) dn2 = dget(l + 3);
+            issue(l + 2, dn2, ln2);
+            if (l + 3 < l1) { dn2 = dget(l + 3); ln2 = lget(l + 3); }
         }
         if (SL) {
             // the rows first used AH levels from now (list staged with this level)
