@@ -396,17 +396,32 @@ def true_res(Ah, B, X):
     return float(np.max(np.linalg.norm(B - Ah @ X, axis=0) / np.linalg.norm(B, axis=0)))
 
 
+# template instance of each recorded sweep form in the mixed (FP32, NV=16) step
+GS_FORM_KERNEL = {"gs_grid": "k_gs3<float,16,0,0,0> (cooperative grid)",
+                  "gs_tile": "k_gs3<float,16,1,1,0> (hybrid blocks, one CTA each, x tile)",
+                  "gs_window": "k_gs3<float,16,1,0,1> (hybrid blocks, one CTA each, slot window)",
+                  "gs_gather": "k_gs3<float,16,1,0,0> (hybrid blocks, one CTA each, per-level gather)",
+                  "gsw_tile": "k_gsw<float,16,1> (hybrid blocks, one warp each, x tile)",
+                  "gsw_window": "k_gsw<float,16,2> (hybrid blocks, one warp each, slot window)",
+                  "gsw_gather": "k_gsw<float,16,0> (hybrid blocks, one warp each, per-level gather)"}
+# DRAM bytes (read + write) per algorithmic byte of the slot-window sweep,
+# measured by ncu on the 27-point 96^3 case (one launch, 296 blocks, FP32)
+GS_TRAFFIC_RATIO = {"gs_window": 1.06}
+
+
 def gs_roofline(rec, solve_ms, rows):
     """Roofline of the dominant kernel of the mixed step: the hybrid
     Gauss-Seidel sweep kernel on the finest level (one launch per sweep
     direction), achieved = algorithmic bytes per launch / CUDA-event time per
     launch."""
     peak, src = peak_hbm()
-    tot = {k: sum(r["ms"] for r in rec if r["kernel"] == k) for k in ("gs", "spmv")}
-    fine = [r for r in rec if r["kernel"] == "gs" and r["rows"] == rows]
+    kind = lambda r: "gs" if r["kernel"].startswith("gs") else r["kernel"]
+    tot = {k: sum(r["ms"] for r in rec if kind(r) == k) for k in ("gs", "spmv")}
+    fine = [r for r in rec if kind(r) == "gs" and r["rows"] == rows]
     if not fine:
         return None
     f = fine[0]
+    name = GS_FORM_KERNEL.get(f["kernel"], "k_gs3") + " (finest level)"
     per_ms = f["ms"] / f["launches"]
     per_b = f["bytes"] / f["launches"]
     ach = per_b / (per_ms * 1e-3) / 1e9
@@ -415,9 +430,13 @@ def gs_roofline(rec, solve_ms, rows):
         levels.setdefault(r["kernel"], []).append(
             {"rows": r["rows"], "launches": r["launches"], "ms": round(r["ms"], 3),
              "gbs": round(r["bytes"] / (r["ms"] * 1e-3) / 1e9, 1) if r["ms"] > 0 else None})
-    return {"bound": "hbm", "kernel": "k_gs3<float,16,1,0> (hybrid blocks, finest level)",
+    return {"bound": "hbm", "kernel": name,
             "achieved": round(ach, 1), "peak": peak, "peak_source": src, "unit": "GB/s",
-            "frac": round(ach / peak, 4), "traffic": None,
+            "frac": round(ach / peak, 4),
+            "traffic": round(per_b * GS_TRAFFIC_RATIO[f["kernel"]]) if f["kernel"] in GS_TRAFFIC_RATIO else None,
+            "traffic_source": ("ncu DRAM bytes / algorithmic bytes of the same kernel on the 27-point 96^3 "
+                               "case (%.3f), times this launch's algorithmic bytes" % GS_TRAFFIC_RATIO[f["kernel"]])
+                              if f["kernel"] in GS_TRAFFIC_RATIO else None,
             "algorithmic_bytes": round(per_b), "launch_ms": round(per_ms, 4), "launches": f["launches"],
             "share_of_step": {"gs_all_levels": round(tot["gs"] / solve_ms, 3),
                               "spmv_all_operators": round(tot["spmv"] / solve_ms, 3),

@@ -33,10 +33,16 @@ int XAMG_b200_synchronize(void);
 long long XAMG_b200_kernel_launches(void);
 /* CUDA-event timing of the hot kernels inside solves (an extension; off by
  * default, it adds two event records per timed launch): on = 1 starts
- * recording every Gauss-Seidel sweep (class 0) and sparse product (class 1)
- * with its algorithmic bytes, on = 0 stops and discards; returns the previous
- * state. */
+ * recording every Gauss-Seidel sweep and sparse product (class 1) with its
+ * algorithmic bytes, on = 0 stops and discards; returns the previous state.
+ * Sweep classes: 2 cooperative grid; hybrid blocks, one CTA per block:
+ * 3 x tile in shared memory, 4 slot window, 5 x gathered per level; the same
+ * with one warp per block: 6, 7, 8; 0 any other sweep path. */
 int XAMG_b200_kernel_timing(int on);
+/* Kernel of the hybrid Gauss-Seidel sweeps in this process: 1 one warp per
+ * block, 0 one 256-thread CTA per block (XAMG_GS_SWEEP=warp|cta, read once;
+ * both give identical results). */
+int XAMG_b200_gs_sweep_kernel(void);
 /* Waits for the device, then writes per (class, operator rows) the launch
  * count, total milliseconds and total algorithmic bytes of the records so far
  * (at most cap groups) and clears them; returns the number of groups, or a

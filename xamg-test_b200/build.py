@@ -20,7 +20,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB = os.path.join(HERE, "libxamg_b200.so")
 ORACLE_LIB = os.path.join(ROOT, "oracle", "liboracle.so")
 
-CU_SOURCES = ["kernels.cu", "gs.cu", "noalloc.cu", "cnn.cu", "batch.cu"]
+CU_SOURCES = ["kernels.cu", "gs.cu", "gsw.cu", "noalloc.cu", "cnn.cu", "batch.cu"]
 CPP_SOURCES = ["host/gen.cpp", "host/amg.cpp", "host/params.cpp", "host/solve.cpp", "host/runs.cpp",
                "host/batch.cpp", "host/dist.cpp", "host/dist_solve.cpp", "host/c_api.cpp"]
 

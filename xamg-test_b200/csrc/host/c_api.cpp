@@ -985,6 +985,7 @@ long long XAMG_b200_batch_last_kernels(size_t bid) {
 }
 long long XAMG_b200_kernel_launches(void) { return xk::launch_count(); }
 int XAMG_b200_kernel_timing(int on) { return ktime_enable(on); }
+int XAMG_b200_gs_sweep_kernel(void) { return gs_warp_sweep(); }
 int XAMG_b200_kernel_timing_read(int cap, int *kclass, int64_t *rows, int64_t *launches, double *ms,
                                  double *bytes) {
     int g = -1;

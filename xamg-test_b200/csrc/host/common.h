@@ -98,8 +98,15 @@ Context &ctx();
 // Optional CUDA-event timing of the hot kernels inside solves (off unless
 // enabled through XAMG_b200_kernel_timing).  A record is one launch: its
 // kernel class, the rows of its operator, its algorithmic bytes and the
-// event pair around it on the launching stream.
-enum class KClass : int { GS = 0, SPMV = 1 };
+// event pair around it on the launching stream.  The level-ordered
+// Gauss-Seidel sweep is recorded by its form: cooperative grid, hybrid blocks
+// (one CTA per block) with the x tile in shared memory, with the slot window,
+// or gathering x per level, and the same three forms with one warp per block
+// (GS covers the other sweep paths).
+enum class KClass : int {
+    GS = 0, SPMV = 1, GS_GRID = 2, GS_TILE = 3, GS_WINDOW = 4, GS_GATHER = 5,
+    GSW_TILE = 6, GSW_WINDOW = 7, GSW_GATHER = 8
+};
 bool ktime_on();
 struct KTimeScope {
     bool on;

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <queue>
 #include <set>
 #include <tuple>
@@ -427,6 +428,8 @@ void GsPlan::build_slots(int d, const std::vector<int> &order, const std::vector
     upload_ints(L.ldpre, ldpre);
     upload_ints(L.ld, ld);
     L.nslots = std::max(smax, 1);
+    L.nlmax = 0;
+    for (int g = 0; g < ngroups; ++g) L.nlmax = std::max(L.nlmax, ldd[2 * (size_t)g + 1] - ldd[2 * (size_t)g]);
 }
 
 // Point-to-point waits of the cooperative (GRID) sweep.  Instead of a grid
@@ -602,7 +605,14 @@ void GsPlan::build_lcsr(const HostCsr &A, Prec p) {
         L.nlev = ngroups;
         L.ncta = mode == GsMode::GRID ? G : nblocks;
         L.emax = 0;
-        for (size_t q = 0; q + 3 < desc.size(); q += 4) L.emax = std::max(L.emax, desc[q + 3] - desc[q + 2]);
+        L.rmax = 0;
+        for (size_t q = 0; q + 3 < desc.size(); q += 4) {
+            L.emax = std::max(L.emax, desc[q + 3] - desc[q + 2]);
+            L.rmax = std::max(L.rmax, ((desc[q + 1] + 3) & ~3) - (desc[q] & ~3));
+        }
+        L.lmax = 0;
+        if (mode == GsMode::BLOCKS)
+            for (size_t b = 0; b + 1 < blev.size(); ++b) L.lmax = std::max(L.lmax, blev[b + 1] - blev[b]);
         upload_ints(L.lrp, lrp);
         upload_ints(L.lci, lci);
         upload_ints(L.lrow, order);
@@ -638,6 +648,21 @@ static bool slot_window_on() {
     static const bool on = std::getenv("XAMG_GS_NO_SLOT_WINDOW") == nullptr;
     return on;
 }
+// Hybrid sweeps: one 256-thread CTA per block, or one warp per block
+// (XAMG_GS_SWEEP=warp; XAMG_GS_SWEEP=cta selects the CTA kernel explicitly).
+// Results are identical.
+constexpr bool kWarpSweepDefault = false;
+static bool warp_sweep_on() {
+    static const bool on = [] {
+        const char *e = std::getenv("XAMG_GS_SWEEP");
+        if (e && std::strcmp(e, "warp") == 0) return true;
+        if (e && std::strcmp(e, "cta") == 0) return false;
+        return kWarpSweepDefault;
+    }();
+    return on;
+}
+
+int gs_warp_sweep() { return warp_sweep_on() ? 1 : 0; }
 
 void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val,
                    const void *invd, const void *t, void *x, const void *relax, bool forward,
@@ -660,13 +685,28 @@ void GsPlan::sweep(Prec p, int nv, const int *rp, const int *ci, const void *val
         // one sweep: in-block entries (column + value), per row its id, offset
         // and inverse diagonal, and t read, x read, x written
         const double sv = (double)prec_size(p);
-        KTimeScope kt(KClass::GS, n, (double)nnz_in * (4 + sv) + (double)n * (8 + sv) + 3.0 * n * nv * sv, s);
         xk::GsSlotWin win{L.lslot.as<int>(), L.ldd.as<int2>(), L.ldpre.as<int2>(), L.ld.as<int2>(), L.nslots};
         xk::GsDeps gd{nullptr, nullptr, nullptr};
         if (md == 0 && L.has_deps && grid_deps_on()) gd = {L.dptr.as<int>(), L.deps.as<int2>(), prog.as<unsigned>()};
         const bool slots = md == 1 && !xs && L.nslots > 0 && slot_window_on() &&
                            (size_t)L.nslots * nv * prec_size(p) <= (size_t)xk::gs_slot_window_bytes() &&
                            nv * prec_size(p) >= 16;
+        const double gbytes = (double)nnz_in * (4 + sv) + (double)n * (8 + sv) + 3.0 * n * nv * sv;
+        if (md == 1 && warp_sweep_on()) {
+            const int wslots = L.nslots > 0 && slot_window_on() ? L.nslots : 0;
+            const xk::GswShape z = xk::gsw_shape(prec_size(p), nv, L.ncta, sm_count(), brows, wslots, L.emax,
+                                                 L.rmax, L.lmax, L.nlmax);
+            if (z.xm >= 0) {
+                const KClass kw = z.xm == 1 ? KClass::GSW_TILE : z.xm == 2 ? KClass::GSW_WINDOW : KClass::GSW_GATHER;
+                KTimeScope kt(kw, n, gbytes, s);
+                XCUDA(xk::gs_sweep_warp(p, nv, z, L.ncta, L.desc.as<int>(), L.blev.as<int>(), L.lrp.as<int>(),
+                                        z.xm == 2 ? L.lcs.as<int>() : L.lci.as<int>(), L.lva.p, L.lrow.as<int>(),
+                                        L.linvd.p, t, x, relax, brows, n, z.xm == 2 ? &win : nullptr, L.lmax, s));
+                return;
+            }
+        }
+        const KClass kc = md == 0 ? KClass::GS_GRID : xs ? KClass::GS_TILE : slots ? KClass::GS_WINDOW : KClass::GS_GATHER;
+        KTimeScope kt(kc, n, gbytes, s);
         XCUDA(xk::gs_sweep_lcsr(p, nv, md, xs, L.nlev, L.ncta, L.desc.as<int>(), L.blev.as<int>(),
                                 L.lrp.as<int>(), slots ? L.lcs.as<int>() : L.lci.as<int>(), L.lva.p,
                                 L.lrow.as<int>(), L.linvd.p, t, x, relax, brows, n, bar, err, L.emax,

@@ -108,6 +108,9 @@ struct GsPlan {
         int nlev = 0;  // GRID: levels; BLOCKS: unused (per-block counts in blev)
         int ncta = 0;  // CTAs of the launch the descriptors were built for
         int emax = 0;  // most entries of one CTA in one level
+        int rmax = 0;  // most rows of one CTA in one level (span rounded out to 4)
+        int lmax = 0;  // BLOCKS: most levels of one block
+        int nlmax = 0; // BLOCKS with a slot window: longest load list of one level
         // BLOCKS: slot-mapped x window (see build_slots): column indices
         // remapped to window slots, each level-ordered row's slot, and per
         // level the rows whose old x is loaded into their slot kSlotAhead
@@ -247,6 +250,8 @@ void mg_level_eig(MultiGrid *mg, int l, double *mn, double *mx);
 // Kernel timing (see KTimeScope): enable/disable (returns the old state) and
 // read the per-(class, rows) aggregates.
 int ktime_enable(int on);
+// 1 when hybrid Gauss-Seidel sweeps run one warp per block, 0 one CTA per block
+int gs_warp_sweep();
 int ktime_read(int cap, int *kclass, i64 *rows, i64 *launches, double *ms, double *bytes);
 
 void dense_inverse(int n, const double *A, double *Ainv);

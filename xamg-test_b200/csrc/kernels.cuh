@@ -125,6 +125,21 @@ cudaError_t gs_sweep_lcsr(Prec p, int nv, int mode, int xs, int nlev, int ncta, 
                           const int *lrow, const void *invd, const void *t, void *x,
                           const void *relax, i64 brows, i64 n, unsigned *gbar, int *err,
                           int emax, const GsSlotWin *win, const GsDeps *deps, cudaStream_t s);
+// Hybrid sweep with one warp per block (gsw.cu): same arrays and results as
+// gs_sweep_lcsr mode 1.  gsw_shape picks the x form (xm 1 tile, 2 slot
+// window, 0 per-level gather; -1 none fits) and the record stages for the
+// plan's extremes: emax entries, rmax rows (rounded out to 4) and nlmax
+// window loads in one level of one block, lmax levels in one block.
+struct GswShape {
+    int xm = -1, ns = 0, recb = 0, xoff = 0;
+    size_t smem = 0;
+};
+GswShape gsw_shape(int s, int nv, int nblocks, int sms, i64 brows, int nslots, int emax, int rmax, int lmax,
+                   int nlmax);
+cudaError_t gs_sweep_warp(Prec p, int nv, const GswShape &z, int nblocks, const int *desc, const int *blev,
+                          const int *lrp, const int *lci, const void *lva, const int *lrow, const void *invd,
+                          const void *t, void *x, const void *relax, i64 brows, i64 n, const GsSlotWin *win,
+                          int lmax, cudaStream_t s);
 // Bounded-wait self-test (which 0: grid barrier with one CTA missing; 1:
 // mbarrier phase that nothing completes), limit in ns; words: 256 bytes of
 // device scratch, err: one device int (0 after a wait that did not run out).

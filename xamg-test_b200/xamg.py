@@ -156,6 +156,7 @@ def lib():
             "XAMG_b200_batch_last_kernels": (C.c_longlong, [sz]),
             "XAMG_b200_kernel_launches": (C.c_longlong, []),
             "XAMG_b200_kernel_timing": (C.c_int, [C.c_int]),
+            "XAMG_b200_gs_sweep_kernel": (C.c_int, []),
             "XAMG_b200_kernel_timing_read": (C.c_int, [C.c_int, P, P, P, P, P]),
             "XAMG_b200_batch_groups": (C.c_int, [sz, P, C.c_int]),
             "XAMG_b200_batch_destroy": (C.c_int, [sz]),
@@ -183,7 +184,13 @@ def kernel_launches():
     return lib().XAMG_b200_kernel_launches()
 
 
-KCLASS = {0: "gs", 1: "spmv"}
+KCLASS = {0: "gs", 1: "spmv", 2: "gs_grid", 3: "gs_tile", 4: "gs_window", 5: "gs_gather",
+          6: "gsw_tile", 7: "gsw_window", 8: "gsw_gather"}
+
+
+def gs_sweep_kernel():
+    """'warp' or 'cta': the kernel of this process's hybrid Gauss-Seidel sweeps."""
+    return "warp" if lib().XAMG_b200_gs_sweep_kernel() else "cta"
 
 
 def kernel_timing(on):
