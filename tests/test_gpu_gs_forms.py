@@ -117,10 +117,11 @@ def test_window_form(gpu, nv, prec):
     dtype = np.float64 if prec == 0 else np.float32
     brows = -(-(len(rp) - 1) // 296)
     kinds = _run(rp, ci, v, brows, nv, dtype, prec, 37)
+    row = nv * np.dtype(dtype).itemsize
     assert any(k.startswith("gs") for k in kinds), kinds
-    if not NOWIN:
+    if not NOWIN and row <= 128:  # wider FP64 rows may leave the warp kernel no room: CTA fallback
         assert any(k.startswith(PRE) for k in kinds), kinds
-    if not CTA and not NOWIN and nv * np.dtype(dtype).itemsize >= 64:
+    if not CTA and not NOWIN and 64 <= row <= 128:
         assert PRE + "window" in kinds, kinds
 
 
