@@ -167,6 +167,7 @@ def build_problem():
 # with each segment's x rows staged in shared memory one segment ahead
 RUN8, RUN8X = 108, 109
 RUNS = (RUN8, RUN8X)
+RUN_FORM = {RUN8: 0, RUN8X: 1}
 
 
 def spmv_time(csr, prec=0, variant=-1, iters=20, info=None, mode=0):
@@ -185,7 +186,7 @@ def spmv_time(csr, prec=0, variant=-1, iters=20, info=None, mode=0):
     P = lambda t: C.c_void_p(t.data_ptr())
     L = xamg.lib()
     plan = None
-    old_form = L.xamg_spmv_set_run_form(int(variant == RUN8X))
+    old_form = L.xamg_spmv_set_run_form(RUN_FORM.get(variant, 0))
     if variant in RUNS:
         plan = L.xamg_spmv_runs_plan_create(n, xamg._ptr(rp), xamg._ptr(ci), xamg._ptr(np.ascontiguousarray(v)),
                                             8, int(prec == 1))
@@ -226,7 +227,7 @@ def tune_spmv(csr, prec=0):
     """Autotune the SpMV kernel on this matrix (results are identical for
     every kernel; only the data layout and launch shape differ)."""
     res = {}
-    for var in (0, 3, 5, 6, RUN8, RUN8X):
+    for var in (0, 3, 5, 6) + RUNS:
         res[var] = spmv_time(csr, prec, var, iters=10)
     best = min(res, key=res.get)
     return best, res
@@ -240,7 +241,7 @@ def apply_spmv_choice(var):
     if var in RUNS:
         L.xamg_spmv_set_run_rows(8)
         L.xamg_spmv_set_variant(-1)
-        L.xamg_spmv_set_run_form(int(var == RUN8X))
+        L.xamg_spmv_set_run_form(RUN_FORM[var])
     else:
         L.xamg_spmv_set_run_rows(0)
         L.xamg_spmv_set_variant(var)
@@ -676,11 +677,16 @@ def learned_headline(fm, B, warmup=1, steps=2):
         # the gate needs the guess's residual: inference + one residual check
         # (one product and inner product, inside the solve's first check)
         total = ms_inf + (ms_guess if use else ms_zero)
+        # once the gate has rejected the guess for this family, later solves
+        # skip the inference: the calibrated cost is the zero-guess solve
+        calibrated = total if use else ms_zero
         return {"n": n, "rhs": nv, "ms_infer": round(ms_inf, 3), "guess_rel_res": round(guess_res, 4),
                 "gate": LEARNED_GATE, "start": "guess" if use else "zero",
                 "ms_solve_zero": round(ms_zero, 3), "ms_solve_from_guess": round(ms_guess, 3),
                 "iters_zero": it_zero[1], "iters_from_guess": it_x0[1],
                 "ms_mixed_learned": round(total, 3), "ms_per_rhs": round(total / nv, 4),
+                "ms_mixed_learned_calibrated": round(calibrated, 3),
+                "ms_per_rhs_calibrated": round(calibrated / nv, 4),
                 "weights": "learned_64.npz (trained on the 64^3 bump-coefficient family)"}
     finally:
         fm.renew(spec0)

@@ -234,6 +234,14 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
         const T *xg = x + xbase * NV;
         for (i64 q = tid; q < xrows * NV; q += 256) xs[q] = xg[q];
     }
+    // the row of zeros that padding entries (column -1, value +0) read after
+    // the x tile or the slot window: fma(-0, 0, s) == s for every s
+    const i64 zrow = XS ? (i64)brows : SL ? (i64)sw.nslots : 0;
+    if (TILE)
+        for (int q = tid; q < NV; q += 256) xs[zrow * NV + q] = T(0);
+    T rl[V];  // this thread's relaxation factors (its columns never change)
+#pragma unroll
+    for (int e = 0; e < V; ++e) rl[e] = relax[(tid % TPR) * V + e];
     __syncthreads();
     unsigned use[NB] = {0u, 0u, 0u};
     // issuer: the last thread, which rarely owns a row of a level
@@ -425,12 +433,13 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
             if (gath && V * (int)sizeof(T) == 16) {
                 // 16-byte pieces: every piece is copied by cp.async straight
                 // into shared memory, all in flight together (one L2 round
-                // trip, no registers held); padding entries (column -1) are
-                // skipped and never read
+                // trip, no registers held); padding entries (column -1) get
+                // zeros
                 const int tot = (dc.e1 - dc.e0) * TPR;
                 for (int w = tid; w < tot; w += 256) {
                     const int c = s_ci[q][w / TPR];
                     if (c >= 0) cp_async16_cg(xs + (i64)w * V, x + (i64)c * NV + (w % TPR) * V);
+                    else *reinterpret_cast<int4 *>(xs + (i64)w * V) = make_int4(0, 0, 0, 0);
                 }
                 cp_async_wait_all();
             } else if (gath) {
@@ -444,15 +453,15 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
 #pragma unroll
                     for (int u = 0; u < GU; ++u) {
                         const int w = w0 + u * 256;
-                        c[u] = w < tot ? s_ci[q][w / TPR] : -1;
+                        c[u] = w < tot ? s_ci[q][w / TPR] : -2;  // -1: padding (zeros), -2: past the end
                         if (c[u] >= 0) gld<T, V, CG>(x + (i64)c[u] * NV + (w % TPR) * V, tmp[u]);
                     }
 #pragma unroll
                     for (int u = 0; u < GU; ++u)
-                        if (c[u] >= 0) {
+                        if (c[u] != -2) {
                             T *p = xs + (i64)(w0 + u * 256) * V;
 #pragma unroll
-                            for (int e = 0; e < V; ++e) p[e] = tmp[u][e];
+                            for (int e = 0; e < V; ++e) p[e] = c[u] >= 0 ? tmp[u][e] : T(0);
                         }
                 }
             }
@@ -485,31 +494,39 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
             const int j0 = staged ? s_rp[q][r - ra] : __ldg(lrp + r);
             const int j1 = staged ? s_rp[q][r - ra + 1] : __ldg(lrp + r + 1);
             if (staged && (TILE || gath)) {
-                // every operand is in shared memory: a plain loop over the
-                // row's entries (the padding, column -1, is only at its tail)
-                const int o = j0 - dc.e0;
-                int m = j1 - j0;
-                while (m > 0 && s_ci[q][o + m - 1] < 0) --m;
+                // every operand is in shared memory: a loop over the row's
+                // entries four at a time (rows are padded to 4 entries; the
+                // padding, value +0, reads zeros)
+                const int o = j0 - dc.e0, m = j1 - j0;
                 const T *vr = &s_va[q][o];
                 if (TILE) {
                     const int *cr = &s_ci[q][o];
-#pragma unroll 4
-                    for (int k = 0; k < m; ++k) {
-                        T xv[V];
-                        gld<T, V, false>(xs + ((i64)cr[k] - xbase) * NV + lane * V, xv);
-                        const T a = vr[k];
+                    for (int k = 0; k < m; k += 4) {
+                        T xv[4][V];
 #pragma unroll
-                        for (int e = 0; e < V; ++e) sum[e] = fma(-a, xv[e], sum[e]);
+                        for (int u = 0; u < 4; ++u) {
+                            const int c = cr[k + u];
+                            gld<T, V, false>(xs + (c >= 0 ? (i64)c - xbase : zrow) * NV + lane * V, xv[u]);
+                        }
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const T a = vr[k + u];
+#pragma unroll
+                            for (int e = 0; e < V; ++e) sum[e] = fma(-a, xv[u][e], sum[e]);
+                        }
                     }
                 } else {
                     const T *xr = xs + (i64)o * NV + lane * V;
-#pragma unroll 8
-                    for (int k = 0; k < m; ++k) {
-                        T xv[V];
-                        gld<T, V, false>(xr + (i64)k * NV, xv);
-                        const T a = vr[k];
+                    for (int k = 0; k < m; k += 4) {
+                        T xv[4][V];
 #pragma unroll
-                        for (int e = 0; e < V; ++e) sum[e] = fma(-a, xv[e], sum[e]);
+                        for (int u = 0; u < 4; ++u) gld<T, V, false>(xr + (i64)(k + u) * NV, xv[u]);
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const T a = vr[k + u];
+#pragma unroll
+                            for (int e = 0; e < V; ++e) sum[e] = fma(-a, xv[u][e], sum[e]);
+                        }
                     }
                 }
             } else
@@ -551,7 +568,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
             }
 #pragma unroll
             for (int e = 0; e < V; ++e) {
-                T cf = rmul(relax[lane * V + e], di);
+                T cf = rmul(rl[e], di);
                 xo[e] = fma(cf, sum[e], xo[e]);
             }
             if (TILE) {
@@ -623,7 +640,7 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp,
     note_launch();
     if (mode == 1) {
         if (xs) {
-            size_t sm = (size_t)brows * NV * sizeof(T);
+            size_t sm = (size_t)(brows + 1) * NV * sizeof(T);  // + the zero row
             auto k = k_gs3<T, NV, 1, true>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
             k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, 0, gbar, err,
@@ -631,7 +648,7 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp,
         } else if (win && win->nslots > 0 && Sh<T, NV>::V * (int)sizeof(T) == 16 &&
                    (size_t)win->nslots * NV * sizeof(T) <= (size_t)gs_slot_window_bytes()) {
             // lci holds slot numbers (the plan's slot-mapped copy)
-            const size_t sm = (size_t)win->nslots * NV * sizeof(T);
+            const size_t sm = (size_t)(win->nslots + 1) * NV * sizeof(T);  // + the zero slot
             auto k = k_gs3<T, NV, 1, false, true>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
             k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, 0, gbar, err,

@@ -577,7 +577,9 @@ __global__ void __launch_bounds__(NT, STX ? 3 : 5) k_spmv_runs(i64 nchunks, i64 
 }
 
 // kernel form of the run product: 0 = x rows in registers, 1 = x rows staged
-// in shared memory one segment ahead (per host thread; same results)
+// in shared memory one segment ahead (per host thread; same results).  A
+// register budget of 6 or 8 CTAs per SM for form 0 spills the gathered rows
+// and runs 2-4x slower (measured), so it is not offered.
 static thread_local int g_run_form = 0;
 void set_spmv_run_form(int f) { g_run_form = f ? 1 : 0; }
 int get_spmv_run_form() { return g_run_form; }
@@ -599,9 +601,12 @@ static void spmv_runs_p(i64 nchunks, i64 ntiles, const int4 *chunks, const longl
         attr = true;
     }
     unsigned g = (unsigned)((ntiles + RS::TPC - 1) / RS::TPC);
-    if (mode == 0) k_spmv_runs<T, NV, 0, NT, STX><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
-    else if (mode == 1) k_spmv_runs<T, NV, 1, NT, STX><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
-    else k_spmv_runs<T, NV, 2, NT, STX><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
+    if (mode == 0)
+        k_spmv_runs<T, NV, 0, NT, STX><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
+    else if (mode == 1)
+        k_spmv_runs<T, NV, 1, NT, STX><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
+    else
+        k_spmv_runs<T, NV, 2, NT, STX><<<g, NT, SM, s>>>(nchunks, ntiles, chunks, toff, sg, vt, x, y, b);
 }
 
 template <class T, int NV>
