@@ -237,13 +237,16 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
     // the row of zeros that padding entries (column -1, value +0) read after
     // the x tile or the slot window: fma(-0, 0, s) == s for every s
     const i64 zrow = XS ? (i64)brows : SL ? (i64)sw.nslots : 0;
+    // shared-memory row indices fit in 32 bits (a tile or window of at most
+    // 227 KB); the block's first row does too (rows < 2^31)
+    const int zr32 = (int)zrow, xb32 = (int)xbase;
     if (TILE)
         for (int q = tid; q < NV; q += 256) xs[zrow * NV + q] = T(0);
     T rl[V];  // this thread's relaxation factors (its columns never change)
 #pragma unroll
     for (int e = 0; e < V; ++e) rl[e] = relax[(tid % TPR) * V + e];
     __syncthreads();
-    unsigned use[NB] = {0u, 0u, 0u};
+    unsigned par = 0u;  // bit q: phase parity of staging buffer q's next wait
     // issuer: the last thread, which rarely owns a row of a level
     const bool issuer = tid == 255;
     // the slot window's load range of level l (loaded with the level's
@@ -303,11 +306,11 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
     T pt[V], px[V], nt[V], nx[V];
     auto wait_q = [&](int q) {
         if (s_stage[q]) {
-            if (!mbar_wait(&mbar[q], use[q] & 1u)) {
+            if (!mbar_wait(&mbar[q], (par >> q) & 1u)) {
                 atomicExch(err, 1);
                 ok = false;
             }
-            use[q]++;
+            par ^= 1u << q;
         }
     };
     auto prefetch = [&](int l, const Desc &d) {  // into nf, nr, nt, nx
@@ -479,11 +482,9 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
             } else {
                 gld<T, V, CG>(t + (i64)row * NV + lane * V, sum);
             }
-            const i64 xrow = SL ? (i64)(staged ? s_sl[q][r - ra] : __ldg(sw.lslot + r)) : (i64)row - xbase;
+            const int xrow = SL ? (staged ? s_sl[q][r - ra] : __ldg(sw.lslot + r)) : row - xb32;
             if (TILE) {
-                const T *p = xs + xrow * NV + lane * V;
-#pragma unroll
-                for (int e = 0; e < V; ++e) xo[e] = p[e];
+                gld<T, V, false>(xs + xrow * NV + lane * V, xo);
             } else if (it == tid) {
 #pragma unroll
                 for (int e = 0; e < V; ++e) xo[e] = px[e];
@@ -506,7 +507,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
 #pragma unroll
                         for (int u = 0; u < 4; ++u) {
                             const int c = cr[k + u];
-                            gld<T, V, false>(xs + (c >= 0 ? (i64)c - xbase : zrow) * NV + lane * V, xv[u]);
+                            gld<T, V, false>(xs + (c >= 0 ? c - xb32 : zr32) * NV + lane * V, xv[u]);
                         }
 #pragma unroll
                         for (int u = 0; u < 4; ++u) {
@@ -572,9 +573,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
                 xo[e] = fma(cf, sum[e], xo[e]);
             }
             if (TILE) {
-                T *p = xs + xrow * NV + lane * V;
-#pragma unroll
-                for (int e = 0; e < V; ++e) p[e] = xo[e];
+                gst<T, V, false>(xs + xrow * NV + lane * V, xo);
             }
             if (!XS) gst<T, V, CG>(x + (i64)row * NV + lane * V, xo);
         }
@@ -605,7 +604,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
     __syncthreads();
     if (!ok && tid == 0) {
         for (int q = 0; q < NB; ++q)
-            if (s_stage[q]) mbar_wait(&mbar[q], use[q] & 1u);
+            if (s_stage[q]) mbar_wait(&mbar[q], (par >> q) & 1u);
     }
     __syncthreads();
     if (XS && ok) {
