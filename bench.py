@@ -6,8 +6,8 @@ guess.  Forms (all on the same operator and right-hand sides):
   plain        - FP64 PBiCGStab + FP64 AMG V-cycle, Gauss-Seidel in the
                  reference's single-process row order (parity form);
   plain_hybrid - the same FP64 method with the hybrid smoother split of the
-                 mixed form (every level in 296 blocks: Gauss-Seidel inside a
-                 block, Jacobi across blocks);
+                 mixed form (every level in 444 blocks, three per SM:
+                 Gauss-Seidel inside a block, Jacobi across blocks);
   mixed        - FP64 iterative refinement around an FP32 PBiCGStab (FP64
                  inner products and recurrences) with an FP32 AMG V-cycle on
                  the hybrid split;
@@ -85,9 +85,11 @@ def gpu_sms():
 
 
 def mixed_spec(blocks=None, inner_rel=1e-4):
-    """Precision form.  Hybrid SGS on two blocks per SM on every level (two
-    resident CTAs per SM interleave their latency-bound block sweeps)."""
-    blocks = blocks or 2 * gpu_sms()
+    """Precision form.  Hybrid SGS on three blocks per SM on every level (one
+    wave of 128-thread CTAs whose latency-bound block sweeps interleave; the
+    inner and outer iteration counts are the same as with two or eight blocks
+    per SM, and the sweeps are fastest with three)."""
+    blocks = blocks or 3 * gpu_sms()
     s = plain_spec()
     s["meta_solver"] = {"method": "IterativeRefinement", "max_iters": 20, "abs_tolerance": 0.0,
                         "rel_tolerance": 1e-8, "subsolver_reduced_precision": True,
@@ -294,9 +296,9 @@ TRAFFIC_RATIO = {5: 0.9457, 6: 0.9457, RUN8: 1.0287}
 
 def plain_hybrid_spec(blocks=None):
     """FP64 PBiCGStab + FP64 V-cycle with the mixed form's smoother split
-    (hybrid blocks, two per SM): separates the smoother's share of the mixed
+    (hybrid blocks, three per SM): separates the smoother's share of the mixed
     form's gain from the FP32 share."""
-    blocks = blocks or 2 * gpu_sms()
+    blocks = blocks or 3 * gpu_sms()
     s = plain_spec()
     s["pre_smoother"]["hybrid_blocks"] = blocks
     s["post_smoother"]["hybrid_blocks"] = blocks
@@ -402,9 +404,12 @@ def true_res(Ah, B, X):
 
 # template instance of each recorded sweep form in the mixed (FP32, NV=16) step
 GS_FORM_KERNEL = {"gs_grid": "k_gs3<float,16,0,0,0> (cooperative grid)",
-                  "gs_tile": "k_gs3<float,16,1,1,0> (hybrid blocks, one CTA each, x tile)",
-                  "gs_window": "k_gs3<float,16,1,0,1> (hybrid blocks, one CTA each, slot window)",
-                  "gs_gather": "k_gs3<float,16,1,0,0> (hybrid blocks, one CTA each, per-level gather)",
+                  "gs_tile": "k_gs3<float,16,1,1,0,NT> (hybrid blocks, one CTA of NT = 128 or 256 threads each, "
+                             "x tile)",
+                  "gs_window": "k_gs3<float,16,1,0,1,NT> (hybrid blocks, one CTA of NT = 128 or 256 threads each, "
+                               "slot window)",
+                  "gs_gather": "k_gs3<float,16,1,0,0,NT> (hybrid blocks, one CTA of NT = 128 or 256 threads each, "
+                               "per-level gather)",
                   "gsw_tile": "k_gsw<float,16,1> (hybrid blocks, one warp each, x tile)",
                   "gsw_window": "k_gsw<float,16,2> (hybrid blocks, one warp each, slot window)",
                   "gsw_gather": "k_gsw<float,16,0> (hybrid blocks, one warp each, per-level gather)"}

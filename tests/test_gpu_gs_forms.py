@@ -151,11 +151,24 @@ def test_falls_back_when_nothing_fits(gpu, nv):
     assert any(k.startswith("gs_") for k in kinds), kinds
 
 
+@pytest.mark.parametrize("nv", [4, 16])
+@pytest.mark.parametrize("prec", [0, 1])
+def test_many_blocks(gpu, nv, prec):
+    """27-point 64^3 in 1184 blocks of 222 rows (eight per SM): more blocks
+    than two 256-thread CTAs per SM hold, so the CTA kernel runs 128-thread
+    CTAs (four per SM); the warp kernel runs one warp per block."""
+    rp, ci, v = xamg.CsrMatrix.aniso27(64).arrays()
+    dtype = np.float64 if prec == 0 else np.float32
+    brows = -(-(len(rp) - 1) // 1184)
+    kinds = _run(rp, ci, v, brows, nv, dtype, prec, 47)
+    assert any(k.startswith("gs") for k in kinds), kinds
+
+
 def _child(**env):
     e = dict(os.environ, **env)
     return subprocess.run([sys.executable, "-m", "pytest", "-q", "-m", "gpu", "-p", "no:cacheprovider",
                            os.path.join(HERE, "test_gpu_gs_forms.py"), os.path.join(HERE, "test_gpu_kernels.py"),
-                           "-k", "form and not child or hsgs or falls_back"],
+                           "-k", "form and not child or hsgs or falls_back or many_blocks"],
                           env=e, capture_output=True, text=True, timeout=900)
 
 

@@ -27,6 +27,7 @@
 #include "kernels.cuh"
 #include <algorithm>
 #include <cstdio>
+#include <vector>
 
 namespace xk {
 
@@ -163,10 +164,13 @@ __device__ __forceinline__ void gst(T *p, const T (&r)[V]) {
 
 // Staging buffers: three levels in flight, each with up to E entries and RB
 // rows (column indices, values, row offsets, row ids, inverse diagonals).
-template <class T> struct GsBuf {
-    static constexpr int E = sizeof(T) == 8 ? 1024 : 1536;
-    static constexpr int RB = 128;
-    static constexpr int LB = sizeof(T) == 8 ? 160 : 192;  // slot-window loads staged per level (int2 each)
+// 256-thread CTAs (two per SM) stage larger levels than 128-thread CTAs (four
+// per SM, about 25 KB of static shared memory each).
+template <class T, int NT = 256> struct GsBuf {
+    static constexpr int E = NT == 256 ? (sizeof(T) == 8 ? 1024 : 1536) : (sizeof(T) == 8 ? 512 : 768);
+    static constexpr int RB = NT == 256 ? 128 : 64;
+    // slot-window loads staged per level (int2 each)
+    static constexpr int LB = NT == 256 ? (sizeof(T) == 8 ? 160 : 192) : (sizeof(T) == 8 ? 96 : 128);
 };
 
 // One level of one CTA: rows [r0, r1) and entries [e0, e1) of the
@@ -183,8 +187,8 @@ __device__ __forceinline__ int rspan(const Desc &d) { return ((d.r1 + 3) & ~3) -
 // MODE 0 = GRID, 1 = BLOCKS.  XS: x tile of the block in shared memory; SL:
 // slot window (lci then holds slot numbers).
 // desc: GRID -> desc[l*gridDim.x + b]; BLOCKS -> desc[blev[b] + (l - l0)].
-template <class T, int NV, int MODE, bool XS, bool SL = false>
-__global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const int4 *__restrict__ desc,
+template <class T, int NV, int MODE, bool XS, bool SL = false, int NT = 256>
+__global__ void __launch_bounds__(NT, MODE == 1 ? 512 / NT : 1) k_gs3(int nlev, const int4 *__restrict__ desc,
                                              const int *__restrict__ blev,
                                              const int *__restrict__ lrp,
                                              const int *__restrict__ lci,
@@ -194,9 +198,10 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
                                              const T *__restrict__ t, T *x,
                                              const T *__restrict__ relax, i64 brows, i64 n,
                                              int eg, unsigned *gbar, int *err, GsSlotWin sw, GsDeps gd) {
-    constexpr int V = Sh<T, NV>::V, TPR = Sh<T, NV>::TPR, E = GsBuf<T>::E, RB = GsBuf<T>::RB;
+    constexpr int V = Sh<T, NV>::V, TPR = Sh<T, NV>::TPR, E = GsBuf<T, NT>::E, RB = GsBuf<T, NT>::RB;
+    static_assert(NT == 256 || (NT == 128 && MODE == 1), "128-thread CTAs serve hybrid blocks only");
     constexpr int NB = 3;
-    constexpr int LB = SL ? GsBuf<T>::LB : 2;
+    constexpr int LB = SL ? GsBuf<T, NT>::LB : 2;
     constexpr bool CG = (MODE == 0);
     constexpr bool TILE = XS || SL;  // every x value is read from shared memory
     constexpr int AH = kGsSlotAhead;
@@ -232,7 +237,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
     const i64 xrows = MODE == 1 && XS ? min((i64)brows, n - xbase) : 0;
     if (XS) {
         const T *xg = x + xbase * NV;
-        for (i64 q = tid; q < xrows * NV; q += 256) xs[q] = xg[q];
+        for (i64 q = tid; q < xrows * NV; q += NT) xs[q] = xg[q];
     }
     // the row of zeros that padding entries (column -1, value +0) read after
     // the x tile or the slot window: fma(-0, 0, s) == s for every s
@@ -241,14 +246,14 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
     // 227 KB); the block's first row does too (rows < 2^31)
     const int zr32 = (int)zrow, xb32 = (int)xbase;
     if (TILE)
-        for (int q = tid; q < NV; q += 256) xs[zrow * NV + q] = T(0);
+        for (int q = tid; q < NV; q += NT) xs[zrow * NV + q] = T(0);
     T rl[V];  // this thread's relaxation factors (its columns never change)
 #pragma unroll
     for (int e = 0; e < V; ++e) rl[e] = relax[(tid % TPR) * V + e];
     __syncthreads();
     unsigned par = 0u;  // bit q: phase parity of staging buffer q's next wait
     // issuer: the last thread, which rarely owns a row of a level
-    const bool issuer = tid == 255;
+    const bool issuer = tid == NT - 1;
     // the slot window's load range of level l (loaded with the level's
     // descriptor, one iteration before it is needed)
     auto lget = [&](int l) { return SL ? __ldg(sw.ldd + dbase + l) : make_int2(0, 0); };
@@ -282,7 +287,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
     // slot window: copy the old x of the listed rows into their slots, one
     // 16-byte piece per thread and pass (entries {-1, -1} are padding)
     auto load_rows = [&](const int2 *lst, int cnt) {
-        for (int w = tid; w < cnt * TPR; w += 256) {
+        for (int w = tid; w < cnt * TPR; w += NT) {
             const int2 e = lst[w / TPR];
             if (e.x >= 0) cp_async16_cg(xs + (i64)e.y * NV + (w % TPR) * V, x + (i64)e.x * NV + (w % TPR) * V);
         }
@@ -439,7 +444,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
                 // trip, no registers held); padding entries (column -1) get
                 // zeros
                 const int tot = (dc.e1 - dc.e0) * TPR;
-                for (int w = tid; w < tot; w += 256) {
+                for (int w = tid; w < tot; w += NT) {
                     const int c = s_ci[q][w / TPR];
                     if (c >= 0) cp_async16_cg(xs + (i64)w * V, x + (i64)c * NV + (w % TPR) * V);
                     else *reinterpret_cast<int4 *>(xs + (i64)w * V) = make_int4(0, 0, 0, 0);
@@ -450,19 +455,19 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
                 // stores any, so the gather costs one or two L2 round trips
                 constexpr int GU = 8;
                 const int tot = (dc.e1 - dc.e0) * TPR;
-                for (int w0 = tid; w0 < tot; w0 += 256 * GU) {
+                for (int w0 = tid; w0 < tot; w0 += NT * GU) {
                     int c[GU];
                     T tmp[GU][V];
 #pragma unroll
                     for (int u = 0; u < GU; ++u) {
-                        const int w = w0 + u * 256;
+                        const int w = w0 + u * NT;
                         c[u] = w < tot ? s_ci[q][w / TPR] : -2;  // -1: padding (zeros), -2: past the end
                         if (c[u] >= 0) gld<T, V, CG>(x + (i64)c[u] * NV + (w % TPR) * V, tmp[u]);
                     }
 #pragma unroll
                     for (int u = 0; u < GU; ++u)
                         if (c[u] != -2) {
-                            T *p = xs + (i64)(w0 + u * 256) * V;
+                            T *p = xs + (i64)(w0 + u * NT) * V;
 #pragma unroll
                             for (int e = 0; e < V; ++e) p[e] = c[u] >= 0 ? tmp[u][e] : T(0);
                         }
@@ -471,7 +476,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
             __syncthreads();
         }
         const int ra = rlo(dc);
-        for (int it = tid; ok && it < items; it += 256) {
+        for (int it = tid; ok && it < items; it += NT) {
             const int r = dc.r0 + it / TPR, lane = it % TPR;
             const int row = it == tid ? (pv ? pr : -1) : (staged ? s_row[q][r - ra] : __ldg(lrow + r));
             if (row < 0) continue;
@@ -609,7 +614,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? 2 : 1) k_gs3(int nlev, const 
     __syncthreads();
     if (XS && ok) {
         T *xg = x + xbase * NV;
-        for (i64 q = tid; q < xrows * NV; q += 256) xg[q] = xs[q];
+        for (i64 q = tid; q < xrows * NV; q += NT) xg[q] = xs[q];
     }
 }
 
@@ -620,6 +625,65 @@ template <class T> static int gather_entries(int nv, int emax) {
     int eg = (int)std::min<long>(GsBuf<T>::E, (176l * 1024) / ((long)nv * (long)sizeof(T)));
     if (emax > 0) eg = std::min(eg, (emax + 3) & ~3);
     return std::max(eg, 4);
+}
+
+static int device_sms() {
+    thread_local int dev = -1, sms = 0;
+    int d = 0;
+    cudaGetDevice(&d);
+    if (d != dev) {
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d);
+        dev = d;
+    }
+    return sms > 0 ? sms : 1;
+}
+
+// One hybrid-block sweep launch: 256-thread CTAs, or 128-thread CTAs (smaller
+// staging buffers) when the blocks outnumber what the 256-thread kernel keeps
+// resident and more of the 128-thread one fit an SM (one wave instead of
+// two).  The choice is cached per (dynamic shared memory, blocks).
+template <class T, int NV, bool XSV, bool SLV>
+static cudaError_t gs3_blocks(size_t sm, int ncta, int nlev, const int4 *lev_row, const int *blev, const int *lrp,
+                              const int *lci, const T *va, const int *lrow, const T *di, const T *tt, T *xx,
+                              const T *rl, i64 brows, i64 n, int eg, unsigned *gbar, int *err, GsSlotWin w,
+                              cudaStream_t s) {
+    auto k2 = k_gs3<T, NV, 1, XSV, SLV, 256>;
+    auto k1 = k_gs3<T, NV, 1, XSV, SLV, 128>;
+    struct Choice {
+        size_t sm;
+        int ncta;
+        bool small;
+    };
+    thread_local std::vector<Choice> cache;
+    bool small = false, found = false;
+    for (auto &c : cache)
+        if (c.sm == sm && c.ncta == ncta) small = c.small, found = true;
+    cudaError_t e;
+    if (!found) {
+        int o2 = 0, o1 = 0;
+        if (cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) == cudaSuccess &&
+            cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k1, 128, sm) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k2, 256, sm) == cudaSuccess)
+            small = (long)o2 * device_sms() < ncta && o1 > o2;
+        cudaGetLastError();  // a refused query only rules the 128-thread kernel out
+        cache.push_back({sm, ncta, small});
+    }
+    // the dynamic shared-memory limit is a property of the kernel: set it for
+    // this launch's size every time (another plan may have set a smaller one)
+    GsDeps nodeps{nullptr, nullptr, nullptr};
+    if (small) {
+        if ((e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess)
+            return e;
+        k1<<<ncta, 128, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, eg, gbar, err, w,
+                                 nodeps);
+    } else {
+        if ((e = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess)
+            return e;
+        k2<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, eg, gbar, err, w,
+                                 nodeps);
+    }
+    return cudaGetLastError();
 }
 
 template <class T, int NV>
@@ -638,29 +702,17 @@ static cudaError_t gs3_t(int mode, int xs, int nlev, int ncta, const int *descp,
     GsDeps nodeps{nullptr, nullptr, nullptr};
     note_launch();
     if (mode == 1) {
-        if (xs) {
-            size_t sm = (size_t)(brows + 1) * NV * sizeof(T);  // + the zero row
-            auto k = k_gs3<T, NV, 1, true>;
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, 0, gbar, err,
-                                    none, nodeps);
-        } else if (win && win->nslots > 0 && Sh<T, NV>::V * (int)sizeof(T) == 16 &&
-                   (size_t)win->nslots * NV * sizeof(T) <= (size_t)gs_slot_window_bytes()) {
-            // lci holds slot numbers (the plan's slot-mapped copy)
-            const size_t sm = (size_t)(win->nslots + 1) * NV * sizeof(T);  // + the zero slot
-            auto k = k_gs3<T, NV, 1, false, true>;
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, 0, gbar, err,
-                                    *win, nodeps);
-        } else {
-            const int eg = gather_entries<T>(NV, emax);
-            const size_t sm = (size_t)eg * NV * sizeof(T);
-            auto k = k_gs3<T, NV, 1, false>;
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k<<<ncta, 256, sm, s>>>(nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, eg, gbar, err,
-                                    none, nodeps);
-        }
-        return cudaGetLastError();
+#define GS3B(XSV, SLV, SM, EG, W)                                                                              \
+    gs3_blocks<T, NV, XSV, SLV>(SM, ncta, nlev, lev_row, blev, lrp, lci, va, lrow, di, tt, xx, rl, brows, n, EG, \
+                                gbar, err, W, s)
+        if (xs) return GS3B(true, false, (size_t)(brows + 1) * NV * sizeof(T), 0, none);  // + the zero row
+        if (win && win->nslots > 0 && Sh<T, NV>::V * (int)sizeof(T) == 16 &&
+            (size_t)win->nslots * NV * sizeof(T) <= (size_t)gs_slot_window_bytes())
+            // lci holds slot numbers (the plan's slot-mapped copy); + the zero slot
+            return GS3B(false, true, (size_t)(win->nslots + 1) * NV * sizeof(T), 0, *win);
+        const int eg = gather_entries<T>(NV, emax);
+        return GS3B(false, false, (size_t)eg * NV * sizeof(T), eg, none);
+#undef GS3B
     }
     // the grid must match the per-(level, CTA) descriptors built on the host;
     // dynamic shared memory holds the per-level x gather buffer (eg entries)
