@@ -414,8 +414,9 @@ GS_FORM_KERNEL = {"gs_grid": "k_gs3<float,16,0,0,0> (cooperative grid)",
                   "gsw_window": "k_gsw<float,16,2> (hybrid blocks, one warp each, slot window)",
                   "gsw_gather": "k_gsw<float,16,0> (hybrid blocks, one warp each, per-level gather)"}
 # DRAM bytes (read + write) per algorithmic byte of the slot-window sweep,
-# measured by ncu on the 27-point 96^3 case (one launch, 296 blocks, FP32)
-GS_TRAFFIC_RATIO = {"gs_window": 1.06}
+# measured by ncu on the 27-point 96^3 case (one launch, 444 blocks, FP32,
+# 128-thread CTAs: the benchmark's configuration)
+GS_TRAFFIC_RATIO = {"gs_window": 1.063}
 
 
 def gs_roofline(rec, solve_ms, rows):
