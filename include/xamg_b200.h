@@ -283,6 +283,14 @@ int xamg_jacobi(int prec, int nv, int64_t n, const int *rp, const int *ci, const
 /* Inner products (blas::dot, blas.inl:521-589) of nd pairs (1..4), FP64
  * results out[d*nv + k]; part: xamg_dot_part_size(n, nd, nv) doubles of scratch. */
 int64_t xamg_dot_part_size(int64_t n, int nd, int nv);
+/* Inner products of the batching form (batch.cu k_segdot1/2), per segment of
+ * concatenated vectors: segment s holds rows [segoff[s], segoff[s + 1]) (host
+ * array of nseg + 1 offsets from 0); out (device, nd * nseg * nv doubles)
+ * receives at [d * nseg * nv + s * nv + k] exactly what xamg_dot returns for
+ * that segment's rows alone.  a, b: nd (1..3) device vectors each.  Allocates
+ * its own scratch and returns after the device has finished. */
+int xamg_seg_dot(int prec, int nv, int nseg, const int64_t *segoff, int nd, const void *const *a,
+                 const void *const *b, double *out, void *stream);
 int xamg_dot(int prec, int nv, int64_t n, int nd, const void *const *a, const void *const *b,
              double *part, double *out, void *stream);
 

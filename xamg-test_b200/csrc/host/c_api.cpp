@@ -917,6 +917,28 @@ int xamg_dot(int prec, int nv, int64_t n, int nd, const void *const *a, const vo
         XCUDA(cudaGetLastError());
     });
 }
+int xamg_seg_dot(int prec, int nv, int nseg, const int64_t *segoff, int nd, const void *const *a,
+                 const void *const *b, double *out, void *stream) {
+    return guard([&] {
+        XCHECK(nd >= 1 && nd <= 3, "nd must be 1..3");
+        XCHECK(nseg >= 1 && segoff && segoff[0] == 0, "segoff must start at 0 and hold nseg + 1 offsets");
+        XCHECK(nv == 1 || nv == 2 || nv == 4 || nv == 8 || nv == 16 || nv == 32, "nv must be 1, 2, 4, 8, 16 or 32");
+        std::vector<i64> off(segoff, segoff + nseg + 1), cs(1, 0);
+        for (int k = 0; k < nseg; ++k) {
+            XCHECK(off[k + 1] >= off[k], "segoff must not decrease");
+            cs.push_back(cs.back() + (off[k + 1] - off[k] + 255) / 256);
+        }
+        cudaStream_t s = strm(stream);
+        DBuf so(sizeof(i64) * off.size()), cst(sizeof(i64) * cs.size()),
+            part(sizeof(double) * std::max<i64>(cs.back() * nd * nv, 1));
+        XCUDA(cudaMemcpyAsync(so.p, off.data(), sizeof(i64) * off.size(), cudaMemcpyHostToDevice, s));
+        XCUDA(cudaMemcpyAsync(cst.p, cs.data(), sizeof(i64) * cs.size(), cudaMemcpyHostToDevice, s));
+        xk::seg_dots((Prec)prec, nv, nseg, so.as<i64>(), cst.as<i64>(), cs.back(), nd, a, b, part.as<double>(), out,
+                     s);
+        XCUDA(cudaGetLastError());
+        XCUDA(cudaStreamSynchronize(s));  // the scratch is released on return
+    });
+}
 int xamg_blas(int prec, int nv, int64_t n, int op, const double *a, const void *x, const double *b,
               const void *y, const double *c, void *z, void *stream) {
     return guard([&] {

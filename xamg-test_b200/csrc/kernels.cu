@@ -983,15 +983,41 @@ void jacobi(Prec p, int nv, i64 n, const int *rp, const int *ci, const void *val
 }
 
 // ---------------------------------------------------------------- dense
-// thread (i, k): y[i,k] = sum_j AinvT[j*n + i] * b[j*nv + k], j ascending, fma
+// thread (i, k): y[i,k] = sum_j AinvT[j*n + i] * b[j*nv + k], j ascending, fma.
+// The chain is sequential, but its operands are not: they are loaded DU
+// steps at a time, the next DU while the current DU multiply (two register
+// sets), so the chain runs at FMA latency instead of one L2 round trip per
+// few steps.
 template <class T>
 __global__ void __launch_bounds__(256) k_dense(int n, int nv, const T *__restrict__ AT,
                                                const T *__restrict__ b, T *__restrict__ y) {
+    constexpr int DU = 16;
     i64 idx = (i64)blockIdx.x * 256 + threadIdx.x;
     if (idx >= (i64)n * nv) return;
     int i = (int)(idx % n), k = (int)(idx / n);
+    T a0[DU], b0[DU], a1[DU], b1[DU];
+    auto load = [&](int j0, T(&a)[DU], T(&bb)[DU]) {
+#pragma unroll
+        for (int u = 0; u < DU; ++u) {
+            const bool in = j0 + u < n;
+            a[u] = in ? __ldg(AT + (i64)(j0 + u) * n + i) : T(0);
+            bb[u] = in ? __ldg(b + (i64)(j0 + u) * nv + k) : T(0);
+        }
+    };
+    auto chain = [&](int j0, T &s, const T(&a)[DU], const T(&bb)[DU]) {
+#pragma unroll
+        for (int u = 0; u < DU; ++u)
+            if (j0 + u < n) s = fma(a[u], bb[u], s);
+    };
     T s = T(0);
-    for (int j = 0; j < n; ++j) s = fma(__ldg(AT + (i64)j * n + i), __ldg(b + (i64)j * nv + k), s);
+    load(0, a0, b0);
+    for (int j0 = 0; j0 < n; j0 += 2 * DU) {
+        if (j0 + DU < n) load(j0 + DU, a1, b1);
+        chain(j0, s, a0, b0);
+        if (j0 + DU >= n) break;
+        if (j0 + 2 * DU < n) load(j0 + 2 * DU, a0, b0);
+        chain(j0 + DU, s, a1, b1);
+    }
     y[(i64)i * nv + k] = s;
 }
 

@@ -143,6 +143,7 @@ def lib():
             "xamg_jacobi": (C.c_int, [C.c_int, C.c_int, i64, P, P, P, P, P, P, P, P, P]),
             "xamg_dot_part_size": (i64, [i64, C.c_int, C.c_int]),
             "xamg_dot": (C.c_int, [C.c_int, C.c_int, i64, C.c_int, P, P, P, P, P]),
+            "xamg_seg_dot": (C.c_int, [C.c_int, C.c_int, C.c_int, P, C.c_int, P, P, P, P]),
             "xamg_dot_noalloc": (C.c_int, [C.c_int, C.c_int, i64, C.c_int, P, P, P, P]),
             "xamg_blas": (C.c_int, [C.c_int, C.c_int, i64, C.c_int, P, P, P, P, P, P, P]),
             "xamg_dense_gemv": (C.c_int, [C.c_int, C.c_int, C.c_int, P, P, P, P]),
