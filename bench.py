@@ -628,7 +628,7 @@ def learned_headline(fm, B, warmup=1, steps=2):
     coefficients, log k = 0) predicts x0 for the 16 right-hand sides; the
     guess is used only when its relative residual ||b - A x0|| / ||b|| is
     below LEARNED_GATE, else the solve starts from zero.  Both solves are
-    judged against ||b|| (rel_tolerance_base = rhs), so the target is the
+    measured against ||b|| (rel_tolerance_base = rhs), so the target is the
     same 1e-8.  Reports the inference time, the guess's residual, the gate's
     choice and the time to 1e-8 with inference included."""
     if not os.path.exists(LEARNED_WEIGHTS):

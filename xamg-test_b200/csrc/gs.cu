@@ -354,13 +354,19 @@ __global__ void __launch_bounds__(NT, MODE == 1 ? 512 / NT : 1) k_gs3(int nlev, 
         if (tid < 32 && tid < dcnt) dn = __ldg(gd.deps + dfirst + tid);
     }
     if (SL) {
-        // rows first used in the first AH levels, then AH - 1 empty groups so
-        // that level l's rows are in the group that wait_group<AH> completes
+        // rows first used in the first AH levels, then AH - 1 empty groups:
+        // the rows first used at level l >= AH are in the group iteration
+        // l - AH commits, which the wait at the end of iteration l - 1
+        // (all but the newest AH - 1 groups) completes
         const int2 pr2 = __ldg(sw.ldpre + b);
         if (pr2.y > pr2.x) load_rows(sw.ld + pr2.x, pr2.y - pr2.x);
         cp_async_commit();
 #pragma unroll
         for (int g = 1; g < AH; ++g) cp_async_commit();
+        // the rows of the first level are in before it starts; from then on
+        // each level's end barrier publishes the next level's (below)
+        cp_async_wait_group<AH - 1>();
+        __syncthreads();
     }
     if (l0 < l1) {
         wait_q(l0 % NB);
@@ -398,11 +404,6 @@ __global__ void __launch_bounds__(NT, MODE == 1 ? 512 / NT : 1) k_gs3(int nlev, 
         // tile is too large): gather every x value this level's entries need
         // into shared memory in one parallel round trip (xs: eg entries x NV)
         const bool gath = !TILE && ok && staged && (dc.e1 - dc.e0) <= eg;
-        if (SL) {
-            // this level's rows are in (the groups finish in order)
-            cp_async_wait_group<AH>();
-            __syncthreads();
-        }
         if (MODE == 0 && gd.dptr && l > l0) {
             // point-to-point: wait until every CTA whose rows this level
             // depends on has finished the levels it must have (bounded; the
@@ -587,6 +588,10 @@ __global__ void __launch_bounds__(NT, MODE == 1 ? 512 / NT : 1) k_gs3(int nlev, 
             dc = dnx;
             rotate();
         }
+        // the next level's window rows (committed kGsSlotAhead - 1 groups ago)
+        // are in this thread's slots; the barrier below makes every thread's
+        // visible, so the next level needs no barrier of its own for them
+        if (SL) cp_async_wait_group<AH - 1>();
         // every thread agrees on ok before the loop test (a wait that gave up
         // in one thread ends the sweep for the whole CTA)
         ok = __syncthreads_and(ok) != 0;
