@@ -1,0 +1,79 @@
+"""Compile the reference's own loop files (src/blas/detail/blas.inl,
+blas_ext.inl, blas_wrapper.inl, src/blas2/detail/csr_matvec.inl, csr_gs.inl,
+dense_matvec.inl) unchanged, where they lie under the reference tree (default
+/root/reference, or $XAMG_REFERENCE_ROOT), into CPU libraries under
+oracle/_ref/ that the tests use to check the oracle.  Nothing is copied: the
+stand-in types of oracle/ref_loops/shim.h replace the reference's runtime
+(MPI, shared memory, vector and matrix classes), and the loop files are read
+through the include path.  Without the reference tree this step does nothing
+and the tests that need the libraries skip.
+
+Three libraries, the same entry points (oracle/ref_loops/ref_loops.h):
+  libxamg_ref_loops_generic.so  every file with the reference's generic
+      release flags (Make.inc/compilerflags.inc:34,47: -std=c++11 -O3
+      -DNDEBUG); x86-64 without FMA, so every product and sum rounds apart;
+  libxamg_ref_loops_haswell.so  every file with the instruction set of its
+      Haswell machine configuration (compilerflags.inc:86, -march=haswell)
+      and FP contraction (-ffp-contract=fast), without that configuration's
+      -ffast-math (which lets the compiler reorder sums at will): a product
+      feeding a sum becomes one fused multiply-add;
+  libxamg_ref_loops_contract.so  the row loops (sparse and dense products,
+      Gauss-Seidel) as in the Haswell build, the BLAS-1 loops as in the
+      generic build: the arithmetic contract the oracle and the GPU kernels
+      follow (fused row sums, literal vector updates), assembled from the two.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC = os.path.join(HERE, "ref_loops")
+OUT = os.path.join(HERE, "_ref")
+GENERIC = ["-std=c++11", "-O3", "-DNDEBUG", "-fPIC", "-w"]
+HASWELL = GENERIC + ["-march=haswell", "-ffp-contract=fast"]
+# The row loops mark their loop over a row's entries XAMG_NOVECTOR (Intel's
+# "#pragma novector", src/xamg_macros.h:27-31); GCC 13 has no such pragma and
+# the macro is empty there, so the row loops are compiled with GCC's loop
+# vectoriser off to keep that intent.  The loops over a row's nv columns,
+# which the reference does vectorise, are independent lanes: vectorising them
+# changes no result.
+HASWELL_ROWS = HASWELL + ["-fno-tree-vectorize"]
+LIBS = {"generic": (GENERIC, GENERIC), "haswell": (HASWELL_ROWS, HASWELL), "contract": (HASWELL_ROWS, GENERIC)}
+
+
+def reference_src():
+    return os.path.join(os.environ.get("XAMG_REFERENCE_ROOT", "/root/reference"), "src")
+
+
+def library(kind):
+    return os.path.join(OUT, "libxamg_ref_loops_%s.so" % kind)
+
+
+def build():
+    ref = reference_src()
+    if not os.path.isdir(os.path.join(ref, "blas2", "detail")):
+        return []
+    os.makedirs(OUT, exist_ok=True)
+    deps = [os.path.join(SRC, f) for f in sorted(os.listdir(SRC))] + [os.path.abspath(__file__)]
+    built = []
+    for kind, (rows_flags, vec_flags) in LIBS.items():
+        lib = library(kind)
+        if os.path.exists(lib) and all(os.path.getmtime(lib) >= os.path.getmtime(d) for d in deps):
+            built.append(lib)
+            continue
+        objs = []
+        for name, flags in (("rows", rows_flags), ("vec", vec_flags)):
+            obj = os.path.join(OUT, "ref_%s_%s.o" % (name, kind))
+            subprocess.run(["g++", *flags, "-I", SRC, "-I", ref, "-c", os.path.join(SRC, name + ".cpp"),
+                            "-o", obj], check=True)
+            objs.append(obj)
+        subprocess.run(["g++", "-shared", "-o", lib, *objs], check=True)
+        for o in objs:
+            os.remove(o)
+        built.append(lib)
+    return built
+
+
+if __name__ == "__main__":
+    for b in build():
+        sys.stdout.write(b + "\n")

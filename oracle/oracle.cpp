@@ -179,6 +179,22 @@ void dot_sequential(i64 n, int nv, const T *x, const T *y, T *out) {
         for (int k = 0; k < nv; ++k) out[k] += x[i * nv + k] * y[i * nv + k];
 }
 
+// Inner products of the Krylov solvers: the fixed tree above (the order the
+// GPU kernels share), or, when g_seq_dot is set, the reference's own
+// single-core order (dot_sequential, FP64 only).  The second mode lets the
+// tests run a whole solve in the order of the reference's loops compiled
+// unchanged (oracle/ref_loops), which sum sequentially on one core.
+static int g_seq_dot = 0;
+
+template <class T>
+void kdot(i64 n, int nv, const T *x, const T *y, double *out) {
+    if (g_seq_dot && sizeof(T) == sizeof(double)) {
+        dot_sequential<double>(n, nv, (const double *)x, (const double *)y, out);
+        return;
+    }
+    dot_canonical<T, double>(n, nv, x, y, out);
+}
+
 // ---------------------------------------------------------------- dense
 
 // Gauss-Jordan inverse without pivoting, inverse.inl:31-106 (operation order
@@ -484,7 +500,7 @@ int pbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
     spmv<T>(n, A.rp.data(), A.ci.data(), av, x, r0.data(), nv, 0);
     #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < sz; ++q) r0[q] = T(1) * b[q] + T(-1) * r0[q];
-    dot_canonical<T, double>(n, nv, r0.data(), r0.data(), rho.data());
+    kdot<T>(n, nv, r0.data(), r0.data(), rho.data());
     for (int k = 0; k < nv; ++k) cv.res0[k] = rho[k];
     cv.update(rho.data());
     hist.push(cv.res, nv);
@@ -499,7 +515,7 @@ int pbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
         const T *pp = p.data();
         if (mg) { mg_apply<T>(*mg, p_.data(), p.data(), nv); pp = p_.data(); }
         spmv<T>(n, A.rp.data(), A.ci.data(), av, pp, v.data(), nv, 0);
-        dot_canonical<T, double>(n, nv, v.data(), r0.data(), s1.data());
+        kdot<T>(n, nv, v.data(), r0.data(), s1.data());
         for (int k = 0; k < nv; ++k) alpha[k] = rho[k] / s1[k];
         // s = 1*r + (-alpha)*v
         #pragma omp parallel for schedule(static)
@@ -511,9 +527,9 @@ int pbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
         const T *ss = s.data();
         if (mg) { mg_apply<T>(*mg, s_.data(), s.data(), nv); ss = s_.data(); }
         spmv<T>(n, A.rp.data(), A.ci.data(), av, ss, t.data(), nv, 0);
-        dot_canonical<T, double>(n, nv, t.data(), s.data(), s2.data());
-        dot_canonical<T, double>(n, nv, t.data(), t.data(), s3.data());
-        dot_canonical<T, double>(n, nv, s.data(), s.data(), s4.data());
+        kdot<T>(n, nv, t.data(), s.data(), s2.data());
+        kdot<T>(n, nv, t.data(), t.data(), s3.data());
+        kdot<T>(n, nv, s.data(), s.data(), s4.data());
         for (int k = 0; k < nv; ++k) omega[k] = s2[k] / s3[k];
         // x = alpha_c*p_ + omega_c*s_ + 1*x
         #pragma omp parallel for schedule(static)
@@ -538,7 +554,7 @@ int pbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
                 size_t q = (size_t)i * nv + k;
                 r[q] = (T)(1.0 * (double)s[q] + (-omega[k]) * (double)t[q]);
             }
-        dot_canonical<T, double>(n, nv, r.data(), r0.data(), s1.data());
+        kdot<T>(n, nv, r.data(), r0.data(), s1.data());
         for (int k = 0; k < nv; ++k) {
             double a2 = s1[k] / rho[k];
             double a3 = alpha[k] / omega[k];
@@ -579,7 +595,7 @@ int pcg(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iters, Con
     spmv<T>(n, A.rp.data(), A.ci.data(), av, x, r.data(), nv, 0);
     #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < sz; ++q) r[q] = T(1) * b[q] + T(-1) * r[q];
-    dot_canonical<T, double>(n, nv, r.data(), r.data(), res.data());
+    kdot<T>(n, nv, r.data(), r.data(), res.data());
     for (int k = 0; k < nv; ++k) cv.res0[k] = res[k];
     cv.update(res.data());
     hist.push(cv.res, nv);
@@ -592,8 +608,8 @@ int pcg(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iters, Con
         it++;
         if (it >= max_iters) last = true;
         spmv<T>(n, A.rp.data(), A.ci.data(), av, p.data(), Ap.data(), nv, 0);
-        dot_canonical<T, double>(n, nv, r.data(), z.data(), s1.data());
-        dot_canonical<T, double>(n, nv, p.data(), Ap.data(), s2.data());
+        kdot<T>(n, nv, r.data(), z.data(), s1.data());
+        kdot<T>(n, nv, p.data(), Ap.data(), s2.data());
         for (int k = 0; k < nv; ++k) alpha[k] = s1[k] / s2[k];
         #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q) {  // x = (iconv*alpha)*p + 1*x
@@ -604,12 +620,12 @@ int pcg(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iters, Con
         for (size_t q = 0; q < sz; ++q)  // r = (-alpha)*Ap + 1*r
             r[q] = (T)((-1.0 * alpha[at(q)]) * (double)Ap[q] + 1.0 * (double)r[q]);
         precond(z, r);
-        dot_canonical<T, double>(n, nv, r.data(), z.data(), s3.data());
+        kdot<T>(n, nv, r.data(), z.data(), s3.data());
         for (int k = 0; k < nv; ++k) beta[k] = s3[k] / s1[k];
         #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q)  // p = 1*z + beta*p
             p[q] = (T)(1.0 * (double)z[q] + beta[at(q)] * (double)p[q]);
-        dot_canonical<T, double>(n, nv, r.data(), r.data(), res.data());
+        kdot<T>(n, nv, r.data(), r.data(), res.data());
         cv.update(res.data());
         hist.push(cv.res, nv);
         if (cv.check()) return it;
@@ -643,7 +659,7 @@ int rbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
     spmv<T>(n, A.rp.data(), A.ci.data(), av, x, r0.data(), nv, 0);
     #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < sz; ++q) r0[q] = T(1) * b[q] + T(-1) * r0[q];
-    dot_canonical<T, double>(n, nv, r0.data(), r0.data(), rho.data());
+    kdot<T>(n, nv, r0.data(), r0.data(), rho.data());
     for (int k = 0; k < nv; ++k) cv.res0[k] = rho[k];
     cv.update(rho.data());
     hist.push(cv.res, nv);
@@ -657,7 +673,7 @@ int rbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
         it++;
         if (it >= max_iters) last = true;
         spmv<T>(n, A.rp.data(), A.ci.data(), av, v_.data(), v.data(), nv, 0);  // 6
-        dot_canonical<T, double>(n, nv, v.data(), r0.data(), delta.data());   // 7
+        kdot<T>(n, nv, v.data(), r0.data(), delta.data());   // 7
         precond(s, v);                                                        // 8
         for (int k = 0; k < nv; ++k) alpha[k] = rho[k] / delta[k];            // 9
         #pragma omp parallel for schedule(static)
@@ -667,10 +683,10 @@ int rbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
         #pragma omp parallel for schedule(static)
         for (size_t q = 0; q < sz; ++q)                                       // 12
             r[q] = (T)((-alpha[at(q, nv)]) * (double)v[q] + 1.0 * (double)r[q]);
-        dot_canonical<T, double>(n, nv, t.data(), r.data(), theta.data());    // 13
-        dot_canonical<T, double>(n, nv, t.data(), t.data(), phi.data());
-        dot_canonical<T, double>(n, nv, t.data(), r0.data(), psi.data());
-        dot_canonical<T, double>(n, nv, r.data(), r.data(), eta.data());
+        kdot<T>(n, nv, t.data(), r.data(), theta.data());    // 13
+        kdot<T>(n, nv, t.data(), t.data(), phi.data());
+        kdot<T>(n, nv, t.data(), r0.data(), psi.data());
+        kdot<T>(n, nv, r.data(), r.data(), eta.data());
         precond(z, t);                                                        // 14
         for (int k = 0; k < nv; ++k) omega[k] = theta[k] / phi[k];            // 15
         #pragma omp parallel for schedule(static)
@@ -772,6 +788,8 @@ extern "C" {
 // vector updates; the Gauss-Seidel sweeps stay sequential).
 int orc_num_threads() { return omp_get_max_threads(); }
 void orc_set_num_threads(int t) { omp_set_num_threads(t > 0 ? t : 1); }
+// 1: Krylov inner products in the reference's single-core order; 0: the tree
+void orc_set_seq_dot(int on) { orc::g_seq_dot = on ? 1 : 0; }
 
 void orc_spmv_d(i64 n, const int *rp, const int *ci, const double *v, const double *x, double *y,
                 int nv, int acc) { spmv<double>(n, rp, ci, v, x, y, nv, acc); }

@@ -223,6 +223,13 @@ def pbicgstab(rp, ci, v, b, x0, mg=None, max_iters=1000, abs_tol=0.0, rel_tol=1e
     return x, it, hist[: it + 1], status, res0
 
 
+def set_seq_dot(on):
+    """Krylov inner products in the reference's single-core order (FP64) instead
+    of the fixed tree the GPU shares; used only to compare whole solves with the
+    reference's loops compiled unchanged (oracle/ref_loops)."""
+    lib().orc_set_seq_dot(int(bool(on)))
+
+
 def num_threads():
     """Host threads of the oracle's parallel loops."""
     return int(lib().orc_num_threads())

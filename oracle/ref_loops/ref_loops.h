@@ -1,0 +1,58 @@
+// C entry points of the reference-loop library (oracle/_ref/libxamg_ref_loops_*.so):
+// each wraps one of the reference's own loop templates, compiled unchanged
+// from its source files, over caller-owned arrays.  Test infrastructure only:
+// the tests compare the oracle with these, never the product.
+//
+// Block vectors are row-major, x[i*nv + k]; nv must be one of 1, 2, 4, 8, 16,
+// 32 (the template widths instantiated); entry points return 0, or -1 for an
+// unsupported nv.  CSR arrays are int32 (the benchmark's index type).
+#pragma once
+#include <cstdint>
+
+extern "C" {
+
+// csr_Ax_y, src/blas2/detail/csr_matvec.inl:148-260 (y = A x)
+int ref_csr_ax_y_d(int64_t n, const int *rp, const int *ci, const double *v, const double *x,
+                   double *y, int nv);
+int ref_csr_ax_y_f(int64_t n, const int *rp, const int *ci, const float *v, const float *x,
+                   float *y, int nv);
+// csr_Axpy, csr_matvec.inl:32-144 (y += A x)
+int ref_csr_axpy_d(int64_t n, const int *rp, const int *ci, const double *v, const double *x,
+                   double *y, int nv);
+int ref_csr_axpy_f(int64_t n, const int *rp, const int *ci, const float *v, const float *x,
+                   float *y, int nv);
+// One hybrid symmetric Gauss-Seidel call as blas2::SGS (src/blas2/blas2.h:184-281)
+// runs it with one core per row block [bp[q], bp[q+1]): t = 0, t += (entries of
+// each other block, ascending) x by csr_Axpy, t = 1*b + (-1)*t, then csr_SGS
+// (src/blas2/detail/csr_gs.inl:32-134) on the block's own entries.  The t of
+// every block is formed from the incoming x before any block sweeps.
+int ref_hsgs_d(int64_t n, const int *rp, const int *ci, const double *v, const double *invd,
+               const double *b, double *x, const double *relax, int nv, int nb, const int64_t *bp);
+int ref_hsgs_f(int64_t n, const int *rp, const int *ci, const float *v, const float *invd,
+               const float *b, float *x, const float *relax, int nv, int nb, const int64_t *bp);
+// dense_Ax_y, src/blas2/detail/dense_matvec.inl:71-121 (y = M x, M n_r x n_c row-major)
+int ref_dense_ax_y_d(int64_t nr, int64_t nc, const double *m, const double *x, double *y, int nv);
+int ref_dense_ax_y_f(int64_t nr, int64_t nc, const float *m, const float *x, float *y, int nv);
+
+// BLAS-1 (src/blas/detail/blas.inl, blas_ext.inl) over n rows; a, b, c are
+// per-column scalars (nv values).
+int ref_dot_d(int64_t n, int nv, const double *x, const double *y, double *res);      // blas.inl:521-589
+int ref_axpby_d(int64_t n, int nv, const double *a, const double *x, const double *b,
+                double *y);                                                          // blas.inl:89-151
+int ref_axpby_z_d(int64_t n, int nv, const double *a, const double *x, const double *b,
+                  const double *y, double *z);                                       // blas_ext.inl:30-102
+int ref_axpbypcz_d(int64_t n, int nv, const double *a, const double *x, const double *b,
+                   const double *y, const double *c, double *z);                     // blas_ext.inl:106-189
+int ref_xdivy_z_d(int64_t n, int nv, const double *x, const double *y, double *z);    // blas_ext.inl:193-239
+int ref_ax_y_d(int64_t n, int nv, const double *a, const double *x, double *y);       // blas.inl:30-85
+int ref_scal_d(int64_t n, int nv, const double *a, double *y);                        // blas.inl:155-219
+
+// BiCGStab in the step order of src/solvers/detail/bicgstab.inl:44-197, every
+// vector operation one of the reference's loops above; convergence as
+// convergence.h (per column: sqrt(res) <= max(abs_tol, rel_tol*sqrt(res0))).
+// hist receives (iterations + 1) x nv residual values (the squared norms the
+// solver tests); returns the iteration count, or -1 for an unsupported nv.
+int ref_bicgstab_d(int64_t n, const int *rp, const int *ci, const double *v, const double *b,
+                   double *x, int nv, int max_iters, double abs_tol, double rel_tol, double *hist,
+                   int hist_cap);
+}

@@ -1,0 +1,221 @@
+// Minimal stand-ins for the XAMG types that the reference's loop files use,
+// so that those files compile unchanged, where they lie, into a CPU library
+// that checks the oracle (test infrastructure only; never part of the product).
+//
+// The reference's loop bodies (src/blas/detail/blas.inl, blas_ext.inl,
+// src/blas2/detail/csr_matvec.inl, csr_gs.inl, dense_matvec.inl) touch their
+// operands through a small surface of vector::vector and
+// matrix::csr_matrix / dense_matrix: data pointers (get_aligned_ptr), the row
+// range of the calling core (get_core_range), a handful of state flags and the
+// sharing mode.  Everything here models ONE process with ONE core: the core's
+// range is the whole vector and every offset is zero, which is the reference's
+// single-process configuration.  The MPI, shared-memory, logging and
+// performance-counter hooks the files name are inert.
+//
+// Member names and enumerators follow the reference's headers
+// (src/primitives/vector/vector.h:45-62, 221; src/xamg_types.h:90-98;
+// src/primitives/matrix/csr_matrix.h:47-120) because the included loop files
+// refer to them by name; the classes themselves hold no more than a pointer
+// and the flags.
+#pragma once
+
+#include <cassert>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <map>
+#include <typeinfo>
+#include <vector>
+
+#include "xamg_macros.h"  // the reference's own vectorisation / restrict macros
+
+typedef float float32_t;
+typedef double float64_t;
+#define XAMG_ALIGN_SIZE 64
+#define XAMG_STACK_ALIGNMENT_PREFIX alignas(XAMG_ALIGN_SIZE)
+// the constant-vector cache's definitions live in the reference's own
+// library object; its loop files skip them under this macro
+#define XAMG_SEPARATE_OBJECT
+
+// Process identity (global, as in the reference): one process that is master
+// of its node and NUMA domain.
+struct ID {
+    int gl_proc = 0;
+    int nd_numa = 0;
+    bool master_process() const { return true; }
+    bool node_master_process() const { return true; }
+    bool numa_master_process() const { return true; }
+};
+
+namespace XAMG {
+
+namespace mem {
+enum allocation { LOCAL, SHARED, DISTRIBUTED };
+enum sharing { NODE, NUMA, NUMA_NODE, CORE };
+}  // namespace mem
+
+// Performance counters: counted by the reference, ignored here.
+struct perf_info {
+    void mem_read(int) {}
+    void mem_write(int) {}
+    void flop(int) {}
+    void allreduce(int) {}
+};
+
+namespace mpi {
+enum scope { INTRA_NUMA, INTRA_NODE, CROSS_NODE, GLOBAL };
+inline void barrier(scope) {}
+// one process: the allreduce of a local value is the value itself
+template <typename T> inline void allreduce_sum(const T *in, T *out, int n) {
+    for (int i = 0; i < n; ++i) out[i] = in[i];
+}
+template <typename T> inline void allreduce_bxor(const T *in, T *out, int n) {
+    for (int i = 0; i < n; ++i) out[i] = in[i];
+}
+}  // namespace mpi
+
+template <typename T> inline T true_rand() { return T(0.5); }
+template <typename T> inline T pseudo_rand(uint64_t) { return T(0.5); }
+
+namespace vector {
+
+// A block vector of `size` rows and `nv` columns, row-major (x[i*nv + k]),
+// viewing caller-owned memory.
+struct vector {
+    enum vector_status { unallocated, allocated, nonempty, uninitialized, initialized };
+
+    mem::sharing sharing_mode = mem::NUMA_NODE;
+    size_t type_hash = typeid(void).hash_code();
+    bool if_allocated = false;
+    bool if_empty = true;
+    bool if_initialized = false;
+    bool if_zero = true;
+    uint64_t size = 0;
+    uint64_t ext_offset = 0;
+    uint16_t nv = 0;
+    void *ptr = nullptr;
+    std::vector<double> own;  // storage for the small vectors the wrappers allocate
+
+    vector() = default;
+    explicit vector(mem::sharing m) : sharing_mode(m) {}
+
+    template <typename T> void view(T *p, uint64_t n, uint16_t w, bool zero = false) {
+        ptr = (void *)p;
+        size = n;
+        nv = w;
+        type_hash = typeid(T).hash_code();
+        if_allocated = true;
+        if_empty = (n == 0);
+        if_initialized = true;
+        if_zero = zero;
+    }
+    template <typename T> T *alloc_and_get_aligned_ptr(uint64_t n, uint16_t w) {
+        own.assign((n * w * sizeof(T) + sizeof(double) - 1) / sizeof(double) + 1, 0.0);
+        view<T>((T *)own.data(), n, w, true);
+        if_initialized = false;
+        return (T *)ptr;
+    }
+    template <typename T> T *get_aligned_ptr(int = -1) const { return (T *)ptr; }
+    template <typename T> void get_core_range(uint64_t &core_size, uint64_t &core_offset) const {
+        core_size = size;
+        core_offset = 0;
+    }
+    // row range of a compressed (row-indexed) block: not used with one core
+    template <typename I, typename T>
+    void get_core_range(uint64_t &core_size, uint64_t &core_offset, const vector &) const {
+        core_size = size;
+        core_offset = 0;
+    }
+    uint64_t global_numa_offset() const { return 0; }
+    uint64_t numa_offset() const { return 0; }
+    uint64_t intra_numa_offset() const { return 0; }
+    void check(vector_status) const {}
+};
+
+struct indx_vector : vector {
+    uint64_t r1 = 0, r2 = 0;
+};
+
+}  // namespace vector
+
+namespace matrix {
+
+// CSR block: row pointers, column indices and values as vectors; one core,
+// the block covering every row (no row-index compression).
+template <typename F, typename I1, typename I2, typename I3, typename I4>
+struct csr_matrix {
+    vector::vector row, col, val, row_ind, col_ind;
+    mem::sharing sharing_mode = mem::CORE;
+    uint64_t nrows = 0, ncols = 0, nonzeros = 0;
+    uint64_t block_nrows = 0, block_ncols = 0;
+    uint64_t block_row_offset = 0, block_col_offset = 0;
+    bool if_empty = false;
+    bool if_indexed = false;
+    const vector::vector &get_row_ind_vector() const { return row_ind; }
+};
+
+template <typename F> struct dense_matrix {
+    vector::vector val;
+    mem::sharing sharing_mode = mem::CORE;
+    uint64_t nrows = 0, ncols = 0;
+    uint64_t block_nrows = 0, block_ncols = 0;
+    uint64_t block_row_offset = 0, block_col_offset = 0;
+    bool if_empty = false;
+};
+
+}  // namespace matrix
+
+// Declarations of the BLAS-1 templates whose definitions the included loop
+// files provide (their signatures are those of src/blas/blas.h:47-130).
+namespace blas {
+template <typename T, const uint16_t NV> inline void copy(const vector::vector &x, vector::vector &y);
+template <typename T, const uint16_t NV>
+inline void bxor_global(const vector::vector &x, vector::vector &res);
+template <typename T, const uint16_t NV>
+inline void dot_global(const vector::vector &x, const vector::vector &y, vector::vector &res,
+                       bool force = false);
+template <typename T, const uint16_t NV>
+inline void dot(const vector::vector &x, const vector::vector &y, vector::vector &res,
+                bool force = false);
+template <typename T, const uint16_t NV>
+inline void vector_norm(const vector::vector &x, const uint16_t &norm_type, vector::vector &res,
+                        bool force = false);
+template <typename T, const uint16_t NV>
+inline void set_const(vector::vector &x, const vector::vector &val, bool force = false);
+template <typename T, const uint16_t NV> inline void set_rand(vector::vector &x, bool true_rand = false);
+template <typename T, const uint16_t NV>
+inline void ax_y(const vector::vector &a, const vector::vector &x, vector::vector &y);
+template <typename T, const uint16_t NV>
+inline void axpby(const vector::vector &a, const vector::vector &x, const vector::vector &b,
+                  vector::vector &y);
+template <typename T, const uint16_t NV> inline void scal(const vector::vector &x, vector::vector &y);
+template <typename T, typename I, const uint16_t NV>
+inline void gather(const vector::vector &x, const vector::indx_vector &indx, vector::vector &y,
+                   bool force = true);
+template <typename T, const uint16_t NV>
+inline void forced_set_const(const vector::vector &x, const vector::vector &val);
+template <typename T, const uint16_t NV>
+inline void axpby_z(const vector::vector &a, const vector::vector &x, const vector::vector &b,
+                    const vector::vector &y, vector::vector &z);
+template <typename T, const uint16_t NV>
+inline void axpbypcz(const vector::vector &a, const vector::vector &x, const vector::vector &b,
+                     const vector::vector &y, const vector::vector &c, vector::vector &z);
+template <typename T, const uint16_t NV>
+inline void xdivy_z(const vector::vector &x, const vector::vector &y, vector::vector &z);
+template <typename T, const uint16_t NV>
+inline void upload(vector::vector &x, const T *ptr, uint64_t proc_size, uint64_t proc_offset);
+template <typename T, const uint16_t NV> inline void pwr(vector::vector &x, const float64_t deg);
+template <typename T> inline void set_const(vector::vector &x, const T a);
+template <typename T, const uint16_t NV>
+inline void set_const(vector::vector &x, const T val, bool force = false);
+template <typename T, const uint16_t NV>
+inline void set_const(vector::vector &x, const std::vector<T> &a, bool force = false);
+template <typename T, const uint16_t NV> inline void forced_set_const(const vector::vector &x, const T val);
+template <typename T, const uint16_t NV>
+inline void axpby(const T a, const vector::vector &x, const T b, vector::vector &y);
+}  // namespace blas
+
+}  // namespace XAMG
+
+extern XAMG::perf_info perf;
+extern ID id;

@@ -1,0 +1,271 @@
+"""The oracle against the reference's own loops, compiled unchanged from its
+source tree (oracle/build_ref_loops.py): sparse and dense products, the hybrid
+symmetric Gauss-Seidel call, the BLAS-1 updates, the single-core inner product
+and a whole BiCGStab solve in the reference's step order.
+
+Three builds of the same loop files (see oracle/build_ref_loops.py):
+  contract  row loops fused (FMA), BLAS-1 literal: the oracle's arithmetic
+            contract, so everything must be bit-identical;
+  haswell   the Haswell machine configuration with contraction everywhere:
+            row loops bit-identical, BLAS-1 within one rounding per product;
+  generic   the generic release flags, no FMA: row loops within a few
+            roundings, BLAS-1 and the inner product bit-identical.
+The libraries are built from the reference tree in this container; where it
+is absent (and no prebuilt library travelled) the tests skip."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import oracle as orc
+import util
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.path.join(os.path.dirname(HERE), "oracle", "_ref")
+EPS = np.finfo(np.float64).eps
+EPS32 = np.finfo(np.float32).eps
+p = orc.p
+
+
+def _load(kind):
+    path = os.path.join(REF, "libxamg_ref_loops_%s.so" % kind)
+    if not os.path.exists(path):
+        import build_ref_loops
+
+        build_ref_loops.build()
+    if not os.path.exists(path):
+        pytest.skip("reference loop library not built (reference tree absent)")
+    L = C.CDLL(path)
+    i64, vp, ci_, cd = C.c_int64, C.c_void_p, C.c_int, C.c_double
+    for name in ("ref_csr_ax_y_d", "ref_csr_ax_y_f", "ref_csr_axpy_d", "ref_csr_axpy_f"):
+        getattr(L, name).argtypes = [i64, vp, vp, vp, vp, vp, ci_]
+    for name in ("ref_hsgs_d", "ref_hsgs_f"):
+        getattr(L, name).argtypes = [i64, vp, vp, vp, vp, vp, vp, vp, ci_, ci_, vp]
+    for name in ("ref_dense_ax_y_d", "ref_dense_ax_y_f"):
+        getattr(L, name).argtypes = [i64, i64, vp, vp, vp, ci_]
+    L.ref_dot_d.argtypes = [i64, ci_, vp, vp, vp]
+    L.ref_axpby_d.argtypes = [i64, ci_, vp, vp, vp, vp]
+    L.ref_axpby_z_d.argtypes = [i64, ci_, vp, vp, vp, vp, vp]
+    L.ref_axpbypcz_d.argtypes = [i64, ci_, vp, vp, vp, vp, vp, vp]
+    L.ref_xdivy_z_d.argtypes = [i64, ci_, vp, vp, vp]
+    L.ref_ax_y_d.argtypes = [i64, ci_, vp, vp, vp]
+    L.ref_scal_d.argtypes = [i64, ci_, vp, vp]
+    L.ref_bicgstab_d.argtypes = [i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, vp, ci_]
+    return L
+
+
+@pytest.fixture(scope="module")
+def libs():
+    return {k: _load(k) for k in ("contract", "haswell", "generic")}
+
+
+def poisson7(m):
+    """7-point Poisson operator on an m^3 grid with Dirichlet boundary,
+    diagonal first in every row (the cube generator's row layout)."""
+    idx = np.arange(m ** 3).reshape(m, m, m)
+    rp, ci, v = [0], [], []
+    for z in range(m):
+        for y in range(m):
+            for x in range(m):
+                ci.append(idx[z, y, x])
+                v.append(6.0)
+                for dz, dy, dx in ((-1, 0, 0), (0, -1, 0), (0, 0, -1), (0, 0, 1), (0, 1, 0), (1, 0, 0)):
+                    if 0 <= z + dz < m and 0 <= y + dy < m and 0 <= x + dx < m:
+                        ci.append(idx[z + dz, y + dy, x + dx])
+                        v.append(-1.0)
+                rp.append(len(ci))
+    return np.array(rp, np.int32), np.array(ci, np.int32), np.array(v)
+
+
+def operators():
+    rng = np.random.default_rng(5)
+    yield "aniso27_12", orc.gen27(12)
+    yield "dd_random_700", util.dd_csr(700, rng)
+
+
+def inv_diag(rp, ci, v):
+    n = len(rp) - 1
+    d = np.zeros(n)
+    for i in range(n):
+        for j in range(rp[i], rp[i + 1]):
+            if ci[j] == i:
+                d[i] = v[j]
+    return 1.0 / d
+
+
+def abs_spmv(rp, ci, v, x):
+    return orc.spmv(rp, ci, np.abs(v), np.abs(x), x.shape[1])
+
+
+@pytest.mark.parametrize("nv", [1, 2, 4, 8, 16, 32])
+def test_spmv_matches_reference_loops(libs, nv):
+    rng = np.random.default_rng(nv)
+    for name, (rp, ci, v) in operators():
+        n = len(rp) - 1
+        x = rng.uniform(-1, 1, (n, nv))
+        yo = orc.spmv(rp, ci, v, x, nv)
+        y0 = rng.uniform(-1, 1, (n, nv))
+        yao = orc.spmv(rp, ci, v, x, nv, y=y0.copy(), acc=True)
+        for kind, L in libs.items():
+            y = np.zeros((n, nv))
+            assert L.ref_csr_ax_y_d(n, p(rp), p(ci), p(v), p(x), p(y), nv) == 0
+            ya = y0.copy()
+            assert L.ref_csr_axpy_d(n, p(rp), p(ci), p(v), p(x), p(ya), nv) == 0
+            if kind == "generic":  # no FMA: within the rounding of each product
+                bound = 2 * 32 * EPS * abs_spmv(rp, ci, v, x)
+                assert np.all(np.abs(y - yo) <= bound), (name, kind)
+                assert np.all(np.abs(ya - yao) <= bound + 2 * EPS * np.abs(y0)), (name, kind)
+            else:
+                assert np.array_equal(y, yo), (name, kind)
+                assert np.array_equal(ya, yao), (name, kind)
+        # FP32 values and vectors
+        v32, x32 = v.astype(np.float32), x.astype(np.float32)
+        y32o = orc.spmv(rp, ci, v32, x32, nv)
+        y32 = np.zeros((n, nv), np.float32)
+        assert libs["contract"].ref_csr_ax_y_f(n, p(rp), p(ci), p(v32), p(x32), p(y32), nv) == 0
+        assert np.array_equal(y32, y32o), name
+
+
+@pytest.mark.parametrize("nv", [1, 4, 16])
+@pytest.mark.parametrize("nblocks", [1, 3, 8])
+def test_hybrid_gauss_seidel_matches_reference_loops(libs, nv, nblocks):
+    rng = np.random.default_rng(10 * nv + nblocks)
+    for name, (rp, ci, v) in operators():
+        n = len(rp) - 1
+        invd = inv_diag(rp, ci, v)
+        b = rng.uniform(-1, 1, (n, nv))
+        x0 = rng.uniform(-1, 1, (n, nv))
+        relax = rng.uniform(0.5, 1.0, nv)
+        block_rows = -(-n // nblocks) if nblocks > 1 else 0
+        xo = orc.hsgs(rp, ci, v, invd, b, x0.copy(), relax, block_rows=block_rows)
+        bp = (np.append(np.arange(0, n, block_rows), n) if block_rows else np.array([0, n])).astype(np.int64)
+        for kind in ("contract", "haswell"):
+            x = x0.copy()
+            assert libs[kind].ref_hsgs_d(n, p(rp), p(ci), p(v), p(invd), p(b), p(x), p(relax), nv, len(bp) - 1,
+                                         p(bp)) == 0
+            assert np.array_equal(x, xo), (name, kind)
+        x = x0.copy()
+        libs["generic"].ref_hsgs_d(n, p(rp), p(ci), p(v), p(invd), p(b), p(x), p(relax), nv, len(bp) - 1, p(bp))
+        np.testing.assert_allclose(x, xo, rtol=1e-12, atol=1e-13 * np.abs(xo).max(), err_msg=name)
+        # FP32
+        v32, d32, b32, x32 = (a.astype(np.float32) for a in (v, invd, b, x0))
+        r32 = relax.astype(np.float32)
+        xo32 = orc.hsgs(rp, ci, v32, d32, b32, x32.copy(), r32, block_rows=block_rows)
+        xr32 = x32.copy()
+        libs["contract"].ref_hsgs_f(n, p(rp), p(ci), p(v32), p(d32), p(b32), p(xr32), p(r32), nv, len(bp) - 1,
+                                    p(bp))
+        assert np.array_equal(xr32, xo32), name
+
+
+@pytest.mark.parametrize("nv", [1, 4, 16])
+def test_dense_product_matches_reference_loops(libs, nv):
+    rng = np.random.default_rng(40 + nv)
+    nc = 57
+    A = rng.uniform(-1, 1, (nc, nc))
+    b = rng.uniform(-1, 1, (nc, nv))
+    yo = orc.dense_gemv(A, b)
+    for kind in ("contract", "haswell"):
+        y = np.zeros((nc, nv))
+        assert libs[kind].ref_dense_ax_y_d(nc, nc, p(A), p(b), p(y), nv) == 0
+        assert np.array_equal(y, yo), kind
+    A32, b32 = A.astype(np.float32), b.astype(np.float32)
+    y32 = np.zeros((nc, nv), np.float32)
+    libs["contract"].ref_dense_ax_y_f(nc, nc, p(A32), p(b32), p(y32), nv)
+    assert np.array_equal(y32, orc.dense_gemv(A32, b32))
+
+
+@pytest.mark.parametrize("nv", [1, 4, 16])
+def test_blas1_and_inner_product_match_reference_loops(libs, nv):
+    """The oracle and the GPU kernels evaluate the vector updates literally
+    (every product rounded, sums left to right), as numpy does here; the
+    reference's loops give the same bits when compiled without contraction."""
+    rng = np.random.default_rng(60 + nv)
+    n = 1000
+    x, y, z0 = (rng.uniform(-1, 1, (n, nv)) for _ in range(3))
+    a, b, c = (rng.uniform(-2, 2, nv) for _ in range(3))
+    expect = {
+        "axpby": a * x + b * z0,
+        "axpby_z": a * x + b * y,
+        "axpbypcz": a * x + b * y + c * z0,
+        "xdivy_z": x / y,
+        "ax_y": a * x,
+        "scal": a * z0,
+    }
+    for kind in ("contract", "generic", "haswell"):
+        L = libs[kind]
+        got = {}
+        z = z0.copy(); L.ref_axpby_d(n, nv, p(a), p(x), p(b), p(z)); got["axpby"] = z
+        z = np.zeros_like(z0); L.ref_axpby_z_d(n, nv, p(a), p(x), p(b), p(y), p(z)); got["axpby_z"] = z
+        z = z0.copy(); L.ref_axpbypcz_d(n, nv, p(a), p(x), p(b), p(y), p(c), p(z)); got["axpbypcz"] = z
+        z = np.zeros_like(z0); L.ref_xdivy_z_d(n, nv, p(x), p(y), p(z)); got["xdivy_z"] = z
+        z = np.zeros_like(z0); L.ref_ax_y_d(n, nv, p(a), p(x), p(z)); got["ax_y"] = z
+        z = z0.copy(); L.ref_scal_d(n, nv, p(a), p(z)); got["scal"] = z
+        for op, e in expect.items():
+            if kind == "haswell":  # a product fused into its sum: one rounding less
+                mag = np.abs(a * x) + np.abs(b * (y if op == "axpby_z" else z0)) + np.abs(c * z0)
+                assert np.all(np.abs(got[op] - e) <= 4 * EPS * mag + 4 * EPS * np.abs(e)), (op, kind)
+            else:
+                assert np.array_equal(got[op], e), (op, kind)
+        d = np.zeros(nv)
+        L.ref_dot_d(n, nv, p(x), p(y), p(d))
+        if kind == "haswell":
+            np.testing.assert_allclose(d, orc.dot_sequential(x, y), rtol=0, atol=n * EPS * np.abs(x * y).sum(0).max())
+        else:
+            assert np.array_equal(d, orc.dot_sequential(x, y)), kind
+
+
+@pytest.fixture
+def seq_dot():
+    orc.set_seq_dot(True)
+    yield
+    orc.set_seq_dot(False)
+
+
+def _ref_bicgstab(L, rp, ci, v, B, max_iters=1000, rel_tol=1e-8):
+    n, nv = B.shape
+    x = np.zeros_like(B)
+    h = np.zeros((max_iters + 2, nv))
+    it = L.ref_bicgstab_d(n, p(rp), p(ci), p(v), p(B), p(x), nv, max_iters, 0.0, rel_tol, p(h), max_iters + 2)
+    assert it >= 0
+    return x, it, h[: it + 1]
+
+
+@pytest.mark.parametrize("nv", [1, 4])
+def test_bicgstab_solve_matches_reference_loops(libs, seq_dot, nv):
+    """A whole BiCGStab solve (the first configuration: 7-point Poisson on 32^3,
+    RHS uniform[-1,1], 1e-8) in the reference's step order over its own loops
+    equals the oracle bit for bit once the oracle sums its inner products in
+    the reference's single-core order: same iterations, residual history and x."""
+    rp, ci, v = poisson7(32)
+    B = np.random.default_rng(1234).uniform(-1, 1, (len(rp) - 1, nv))
+    xo, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), None, 1000, 0.0, 1e-8)
+    for kind in ("contract", "generic"):  # this operator's products are exact either way
+        x, itr, h = _ref_bicgstab(libs[kind], rp, ci, v, B)
+        assert itr == it, kind
+        assert np.array_equal(h, hist), kind
+        assert np.array_equal(x, xo), kind
+    rp, ci, v = orc.gen27(14)
+    B = np.random.default_rng(99).uniform(-1, 1, (len(rp) - 1, nv))
+    xo, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), None, 1000, 0.0, 1e-8)
+    x, itr, h = _ref_bicgstab(libs["contract"], rp, ci, v, B)
+    assert itr == it and np.array_equal(h, hist) and np.array_equal(x, xo)
+
+
+def test_bicgstab_inner_product_order_changes_iterations(libs):
+    """What the order of the inner products does to a whole solve: the tree
+    order shared by the oracle and the GPU kernels and the reference's
+    single-core order start from the same residual and end at the same
+    tolerance, but BiCGStab's iteration count on this system moves with the
+    rounding (recorded here, so that a parity claim for the tree order is made
+    against the sequential order with this in view)."""
+    rp, ci, v = poisson7(32)
+    B = np.random.default_rng(1234).uniform(-1, 1, (len(rp) - 1, 1))
+    _, it_tree, h_tree, _, _ = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), None, 1000, 0.0, 1e-8)
+    _, it_ref, h_ref = _ref_bicgstab(libs["contract"], rp, ci, v, B)
+    k = min(it_tree, it_ref) + 1
+    rel = np.abs(h_tree[:k] - h_ref[:k]) / h_ref[:k]
+    assert rel[0] < 1e-14
+    assert rel[:10].max() < 1e-12  # the histories agree to rounding at first ...
+    assert rel.max() > 1e-3        # ... and drift apart over ~90 iterations
+    assert (it_tree, it_ref) == (90, 88)
