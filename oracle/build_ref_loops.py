@@ -1,6 +1,6 @@
 """Compile the reference's own loop files (src/blas/detail/blas.inl,
 blas_ext.inl, blas_wrapper.inl, src/blas2/detail/csr_matvec.inl, csr_gs.inl,
-dense_matvec.inl) unchanged, where they lie under the reference tree (default
+dense_matvec.inl, src/primitives/matrix/operations/inverse.inl) unchanged, where they lie under the reference tree (default
 /root/reference, or $XAMG_REFERENCE_ROOT), into CPU libraries under
 oracle/_ref/ that the tests use to check the oracle.  Nothing is copied: the
 stand-in types of oracle/ref_loops/shim.h replace the reference's runtime

@@ -10,6 +10,7 @@
 #include "blas2/detail/csr_matvec.inl"
 #include "blas2/detail/csr_gs.inl"
 #include "blas2/detail/dense_matvec.inl"
+#include "primitives/matrix/operations/inverse.inl"
 
 namespace refloops {
 

@@ -47,6 +47,11 @@ int ref_xdivy_z_d(int64_t n, int nv, const double *x, const double *y, double *z
 int ref_ax_y_d(int64_t n, int nv, const double *a, const double *x, double *y);       // blas.inl:30-85
 int ref_scal_d(int64_t n, int nv, const double *a, double *y);                        // blas.inl:155-219
 
+// Gauss-Jordan inverse of a dense n x n matrix (row-major),
+// src/primitives/matrix/operations/inverse.inl:31-106 (the coarse-grid
+// Direct solver's setup)
+int ref_dense_inverse_d(int64_t n, const double *a, double *ainv);
+
 // BiCGStab in the step order of src/solvers/detail/bicgstab.inl:44-197, every
 // vector operation one of the reference's loops above; convergence as
 // convergence.h (per column: sqrt(res) <= max(abs_tol, rel_tol*sqrt(res0))).

@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
+#include <limits>
 #include <map>
 #include <typeinfo>
 #include <vector>
@@ -54,6 +55,10 @@ enum allocation { LOCAL, SHARED, DISTRIBUTED };
 enum sharing { NODE, NUMA, NUMA_NODE, CORE };
 }  // namespace mem
 
+namespace segment {
+enum hierarchy { NODE, NUMA, CORE };
+}  // namespace segment
+
 // Performance counters: counted by the reference, ignored here.
 struct perf_info {
     void mem_read(int) {}
@@ -63,7 +68,7 @@ struct perf_info {
 };
 
 namespace mpi {
-enum scope { INTRA_NUMA, INTRA_NODE, CROSS_NODE, GLOBAL };
+enum scope { INTRA_NUMA, INTRA_NODE, CROSS_NUMA, CROSS_NODE, GLOBAL };
 inline void barrier(scope) {}
 // one process: the allreduce of a local value is the value itself
 template <typename T> inline void allreduce_sum(const T *in, T *out, int n) {
@@ -161,6 +166,40 @@ template <typename F> struct dense_matrix {
     uint64_t block_nrows = 0, block_ncols = 0;
     uint64_t block_row_offset = 0, block_col_offset = 0;
     bool if_empty = false;
+    dense_matrix() = default;
+    explicit dense_matrix(mem::sharing m) : sharing_mode(m) {}
+    // storage for nrows x ncols values, row-major
+    void alloc() {
+        val.alloc_and_get_aligned_ptr<F>(nrows * ncols, 1);
+        if_empty = (nrows * ncols == 0);
+    }
+};
+
+// The distributed matrix: only the members that the distributed inverse in
+// operations/inverse.inl names (that routine itself is never instantiated
+// here; its single-process core, the dense Gauss-Jordan inverse, is).
+enum segmentation_type { SEGMENT_BY_BLOCKS, SEGMENT_BY_SLICES };
+struct part_layer {};
+struct partitioning {
+    part_layer node_layer, numa_layer;
+};
+struct matrix_block {
+    int data = 0;  // the block's operator (a placeholder: never read here)
+    bool reduced_prec = false;
+    template <typename M> void assemble(M &, int) {}
+};
+struct matrix_layer {
+    matrix_block diag;
+    std::vector<matrix_block> offd;
+};
+struct matrix {
+    std::map<segment::hierarchy, matrix_layer> data_layer;
+    bool reduced_prec = false;
+    segmentation_type segmentation = SEGMENT_BY_BLOCKS;
+    partitioning *row_part = nullptr;
+    float64_t min_eig = 0, max_eig = 0;
+    void set_part(partitioning *p) { row_part = p; }
+    void add_data_layer(segment::hierarchy h) { data_layer[h]; }
 };
 
 }  // namespace matrix

@@ -1,7 +1,8 @@
 """The oracle against the reference's own loops, compiled unchanged from its
 source tree (oracle/build_ref_loops.py): sparse and dense products, the hybrid
 symmetric Gauss-Seidel call, the BLAS-1 updates, the single-core inner product
-and a whole BiCGStab solve in the reference's step order.
+the coarse-grid dense inverse and a whole BiCGStab solve in the reference's
+step order.
 
 Three builds of the same loop files (see oracle/build_ref_loops.py):
   contract  row loops fused (FMA), BLAS-1 literal: the oracle's arithmetic
@@ -52,6 +53,7 @@ def _load(kind):
     L.ref_ax_y_d.argtypes = [i64, ci_, vp, vp, vp]
     L.ref_scal_d.argtypes = [i64, ci_, vp, vp]
     L.ref_bicgstab_d.argtypes = [i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, vp, ci_]
+    L.ref_dense_inverse_d.argtypes = [i64, vp, vp]
     return L
 
 
@@ -173,6 +175,31 @@ def test_dense_product_matches_reference_loops(libs, nv):
     y32 = np.zeros((nc, nv), np.float32)
     libs["contract"].ref_dense_ax_y_f(nc, nc, p(A32), p(b32), p(y32), nv)
     assert np.array_equal(y32, orc.dense_gemv(A32, b32))
+
+
+@pytest.mark.parametrize("n", [1, 7, 64, 100])
+def test_dense_inverse_matches_reference_loops(libs, n):
+    """The coarse-grid Direct solver's Gauss-Jordan inverse (inverse.inl:31-106):
+    the oracle's restatement (and the library's host setup, which the GPU tests
+    hold to the oracle bit for bit) against the reference's routine compiled
+    unchanged, on a diagonally dominant and on a 27-point coarse-like matrix."""
+    rng = np.random.default_rng(n)
+    A = rng.uniform(-1, 1, (n, n)) + np.diag(rng.uniform(n, 2 * n, n))
+    for kind in ("contract", "generic"):
+        R = np.zeros_like(A)
+        assert libs[kind].ref_dense_inverse_d(n, p(A), p(R)) == 0
+        assert np.array_equal(R, orc.dense_inverse(A)), kind
+    R = np.zeros_like(A)
+    libs["haswell"].ref_dense_inverse_d(n, p(A), p(R))  # fused eliminations: within rounding
+    np.testing.assert_allclose(R, orc.dense_inverse(A), rtol=1e-12, atol=1e-15 * np.abs(R).max())
+    if n == 64:
+        rp, ci, v = orc.gen27(4)
+        D = np.zeros((64, 64))
+        for i in range(64):
+            D[i, ci[rp[i]:rp[i + 1]]] = v[rp[i]:rp[i + 1]]
+        R = np.zeros_like(D)
+        libs["contract"].ref_dense_inverse_d(64, p(D), p(R))
+        assert np.array_equal(R, orc.dense_inverse(D))
 
 
 @pytest.mark.parametrize("nv", [1, 4, 16])
