@@ -60,4 +60,18 @@ int ref_dense_inverse_d(int64_t n, const double *a, double *ainv);
 int ref_bicgstab_d(int64_t n, const int *rp, const int *ci, const double *v, const double *b,
                    double *x, int nv, int max_iters, double abs_tol, double rel_tol, double *hist,
                    int hist_cap);
+
+// PBiCGStab (pbicgstab.inl:48-207) preconditioned by one V-cycle from zero
+// (mg.inl:186-280: HSGS pre- and post-smoothing with pre_it / post_it calls
+// of the hybrid sweep above on nb[l] blocks bp[l], residual, restriction by
+// R_l, recursion, the coarsest level by the reference's Gauss-Jordan inverse
+// and dense product, prolongation by y += P_l x_H).  Level l has nrows[l]
+// rows; P_l is nrows[l] x nrows[l+1], R_l its transpose.  Returns the
+// iteration count (-1: unsupported nv or fewer than two levels).
+int ref_pbicgstab_amg_d(int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
+                        const double *const *av, const int *const *prp, const int *const *pci,
+                        const double *const *pv, const int *const *rrp, const int *const *rci,
+                        const double *const *rv, const int *nb, const int64_t *const *bp, double relax,
+                        int pre_it, int post_it, const double *b, double *x, int nv, int max_iters,
+                        double abs_tol, double rel_tol, double *hist, int hist_cap);
 }

@@ -65,16 +65,79 @@ struct Conv {
     }
 };
 
+// The AMG hierarchy handed to the PBiCGStab driver: per level the operator,
+// its inverse diagonal (csr_matrix.h:344-349), P and R = P^T, the hybrid
+// blocks; the coarsest level's inverse from the reference's own Gauss-Jordan
+// routine (Direct::init, direct.inl:31-45).
+struct Hier {
+    int nlev;
+    const int64_t *nrows;
+    const int *const *arp; const int *const *aci; const double *const *av;
+    const int *const *prp; const int *const *pci; const double *const *pv;
+    const int *const *rrp; const int *const *rci; const double *const *rv;
+    const int *nb; const int64_t *const *bp;
+    double relax; int pre_it, post_it;
+    std::vector<std::vector<double>> invd;
+    std::vector<double> ainv;
+    void init() {
+        invd.resize(nlev);
+        for (int l = 0; l < nlev; ++l) {
+            invd[l].assign(nrows[l], 0.0);
+            for (int64_t i = 0; i < nrows[l]; ++i)
+                for (int j = arp[l][i]; j < arp[l][i + 1]; ++j)
+                    if (aci[l][j] == i) invd[l][i] = 1.0 / av[l][j];
+        }
+        int64_t nc = nrows[nlev - 1];
+        std::vector<double> d((size_t)(nc * nc), 0.0);
+        for (int64_t i = 0; i < nc; ++i)
+            for (int j = arp[nlev - 1][i]; j < arp[nlev - 1][i + 1]; ++j) d[i * nc + aci[nlev - 1][j]] = av[nlev - 1][j];
+        ainv.resize(d.size());
+        ref_dense_inverse_d(nc, d.data(), ainv.data());
+    }
+    // HSGS::solve (hsgs.inl:57-91) as a smoother: relax_conv = relax, then
+    // `it` calls of blas2::SGS
+    void smooth(int l, const double *b, double *x, int nv, int it) const {
+        std::vector<double> rl(nv, relax);
+        for (int k = 0; k < it; ++k)
+            ref_hsgs_d(nrows[l], arp[l], aci[l], av[l], invd[l].data(), b, x, rl.data(), nv, nb[l], bp[l]);
+    }
+    // MultiGrid::MG_cycle, mg.inl:186-280, V-cycle, one precision
+    template <int NV> void cycle(int l, double *x, const double *b) const {
+        int64_t n = nrows[l], nc = nrows[l + 1];
+        smooth(l, b, x, NV, pre_it);
+        std::vector<double> tmp((size_t)n * NV), bH((size_t)nc * NV), xH((size_t)nc * NV, 0.0);
+        std::vector<double> one(NV, 1.0), mone(NV, -1.0);
+        vector a1 = scalars(one.data(), NV), a_1 = scalars(mone.data(), NV);
+        ref_csr_ax_y_d(n, arp[l], aci[l], av[l], x, tmp.data(), NV);
+        vector B = block(b, n, NV), T = block(tmp.data(), n, NV);
+        blas::axpby<double, NV>(a1, B, a_1, T);
+        ref_csr_ax_y_d(nc, rrp[l], rci[l], rv[l], tmp.data(), bH.data(), NV);
+        vector XH = block(xH.data(), nc, NV);
+        blas::set_const<double, NV>(XH, 0.0, true);
+        if (l + 1 == nlev - 1)
+            ref_dense_ax_y_d(nc, nc, ainv.data(), bH.data(), xH.data(), NV);  // Direct::solve
+        else
+            cycle<NV>(l + 1, xH.data(), bH.data());
+        ref_csr_axpy_d(n, prp[l], pci[l], pv[l], xH.data(), x, NV);
+        smooth(l, b, x, NV, post_it);
+    }
+};
+
+// (P)BiCGStab in the step order of pbicgstab.inl:48-207 (bicgstab.inl:44-197
+// without a preconditioner: the preconditioned vectors are p and s).
 struct Bicgstab {
     int64_t n; const int *rp, *ci; const double *v, *b; double *x; int nv, max_iters;
     double abs_tol, rel_tol; double *hist; int cap;
+    const Hier *mg;
     int iters;
     template <int NV> void run() {
         typedef double F;
         size_t sz = (size_t)n * NV;
-        std::vector<F> r0(sz, 0.0), r(sz, 0.0), p(sz, 0.0), vv(sz, 0.0), s(sz, 0.0), t(sz, 0.0);
+        std::vector<F> r0(sz, 0.0), r(sz, 0.0), p(sz, 0.0), vv(sz, 0.0), s(sz, 0.0), t(sz, 0.0),
+            p_(sz, 0.0), s_(sz, 0.0);
         vector R0 = block(r0.data(), n, NV), R = block(r.data(), n, NV), P = block(p.data(), n, NV),
-               V = block(vv.data(), n, NV), S = block(s.data(), n, NV), T = block(t.data(), n, NV);
+               V = block(vv.data(), n, NV), S = block(s.data(), n, NV), T = block(t.data(), n, NV),
+               P_ = block(p_.data(), n, NV), S_ = block(s_.data(), n, NV);
         vector X = block(x, n, NV), B = block(b, n, NV);
         std::vector<F> one(NV, 1.0), mone(NV, -1.0), ic(NV, 1.0);
         std::vector<F> rho(NV), res(NV), s1(NV), s2(NV), s3(NV), s4(NV), al(NV), be(NV), om(NV),
@@ -89,6 +152,11 @@ struct Bicgstab {
         auto Ax = [&](const vector &in, vector &out) {
             ref_csr_ax_y_d(n, rp, ci, v, in.get_aligned_ptr<F>(), out.get_aligned_ptr<F>(), NV);
         };
+        // M^{-1}: one V-cycle from zero (MultiGrid::solve with max_iters 1)
+        auto precond = [&](vector &out, const vector &in) {
+            blas::set_const<F, NV>(out, 0.0, true);
+            mg->cycle<NV>(0, out.get_aligned_ptr<F>(), in.get_aligned_ptr<F>());
+        };
         Conv cv{std::vector<double>(NV), std::vector<double>(NV), std::vector<int>(NV, 0),
                 abs_tol, rel_tol, hist, cap, 0, NV};
         // 1-2. r0 = b - A x (solver.h:183-190), rho = (r0, r0)
@@ -100,24 +168,27 @@ struct Bicgstab {
         if (cv.check(ic.data())) { iters = 0; return; }
         blas::copy<F, NV>(R0, R);
         blas::copy<F, NV>(R0, P);
+        vector &PP = mg ? P_ : P, &SS = mg ? S_ : S;
         int it = 0;
         for (bool last = false; !last;) {
             it++;
             if (it >= max_iters) last = true;
-            Ax(P, V);                                             // 5
+            if (mg) precond(P_, P);                              // 5*
+            Ax(PP, V);                                            // 5
             blas::dot<F, NV>(V, R0, S1);                          // 6
             blas::xdivy_z<F, NV>(Rho, S1, Al);
             blas::scal<F, NV>(a_1, Al);                           // 7
             blas::axpby_z<F, NV>(a1, R, Al, V, S);
             blas::scal<F, NV>(a_1, Al);
-            Ax(S, T);                                             // 8
+            if (mg) precond(S_, S);                              // 8*
+            Ax(SS, T);                                            // 8
             blas::dot<F, NV>(T, S, S2);                           // 9
             blas::dot<F, NV>(T, T, S3);
             blas::dot<F, NV>(S, S, S4);
             blas::xdivy_z<F, NV>(S2, S3, Om);
             blas::ax_y<F, NV>(iconv, Al, Alc);                    // 10
             blas::ax_y<F, NV>(iconv, Om, Omc);
-            blas::axpbypcz<F, NV>(Alc, P, Omc, S, a1, X);
+            blas::axpbypcz<F, NV>(Alc, PP, Omc, SS, a1, X);
             blas::ax_y<F, NV>(Om, S2, Res);                       // 12
             blas::axpby<F, NV>(a1, S4, a_1, Res);
             cv.update(res.data());
@@ -176,7 +247,20 @@ int ref_dense_inverse_d(int64_t n, const double *a, double *ainv) {
 int ref_bicgstab_d(int64_t n, const int *rp, const int *ci, const double *v, const double *b,
                    double *x, int nv, int max_iters, double abs_tol, double rel_tol, double *hist,
                    int hist_cap) {
-    Bicgstab f{n, rp, ci, v, b, x, nv, max_iters, abs_tol, rel_tol, hist, hist_cap, 0};
+    Bicgstab f{n, rp, ci, v, b, x, nv, max_iters, abs_tol, rel_tol, hist, hist_cap, nullptr, 0};
+    if (dispatch_nv(nv, f)) return -1;
+    return f.iters;
+}
+int ref_pbicgstab_amg_d(int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
+                        const double *const *av, const int *const *prp, const int *const *pci,
+                        const double *const *pv, const int *const *rrp, const int *const *rci,
+                        const double *const *rv, const int *nb, const int64_t *const *bp, double relax,
+                        int pre_it, int post_it, const double *b, double *x, int nv, int max_iters,
+                        double abs_tol, double rel_tol, double *hist, int hist_cap) {
+    if (nlev < 2) return -1;
+    Hier h{nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax, pre_it, post_it, {}, {}};
+    h.init();
+    Bicgstab f{nrows[0], arp[0], aci[0], av[0], b, x, nv, max_iters, abs_tol, rel_tol, hist, hist_cap, &h, 0};
     if (dispatch_nv(nv, f)) return -1;
     return f.iters;
 }

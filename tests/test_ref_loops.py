@@ -54,6 +54,9 @@ def _load(kind):
     L.ref_scal_d.argtypes = [i64, ci_, vp, vp]
     L.ref_bicgstab_d.argtypes = [i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, vp, ci_]
     L.ref_dense_inverse_d.argtypes = [i64, vp, vp]
+    PP = C.POINTER(C.c_void_p)
+    L.ref_pbicgstab_amg_d.argtypes = [ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, vp, vp,
+                                      ci_, ci_, cd, cd, vp, ci_]
     return L
 
 
@@ -296,3 +299,61 @@ def test_bicgstab_inner_product_order_changes_iterations(libs):
     assert rel[:10].max() < 1e-12  # the histories agree to rounding at first ...
     assert rel.max() > 1e-3        # ... and drift apart over ~90 iterations
     assert (it_tree, it_ref) == (90, 88)
+
+
+def _ptrs(arrs):
+    return (C.c_void_p * len(arrs))(*[a.ctypes.data if a is not None else None for a in arrs])
+
+
+def _ref_pbicgstab_amg(L, levels, blocks, B, max_iters=200, rel_tol=1e-8, relax=0.99):
+    """levels: orc.amg_setup output; blocks[l]: block row offsets of level l."""
+    nlev = len(levels)
+    nrows = np.array([lv["n"] for lv in levels], np.int64)
+    R = [orc.transpose(*lv["P"], lv["ncP"]) if lv["P"] is not None else None for lv in levels]
+    keep = [nrows]
+    cols = []
+    for k in range(3):
+        cols.append([lv["A"][k] for lv in levels])
+        cols.append([lv["P"][k] if lv["P"] is not None else None for lv in levels])
+        cols.append([r[k] if r is not None else None for r in R])
+    arp, prp, rrp, aci, pci, rci, av, pv, rv = cols
+    nb = np.array([len(b) - 1 for b in blocks], np.int32)
+    tabs = [_ptrs(x) for x in (arp, aci, av, prp, pci, pv, rrp, rci, rv, blocks)]
+    keep += [cols, R, nb, blocks, tabs]
+    n, nv = B.shape
+    x = np.zeros_like(B)
+    h = np.zeros((max_iters + 2, nv))
+    PP = C.POINTER(C.c_void_p)
+    cast = [C.cast(t, PP) for t in tabs]
+    it = L.ref_pbicgstab_amg_d(nlev, p(nrows), cast[0], cast[1], cast[2], cast[3], cast[4], cast[5], cast[6],
+                               cast[7], cast[8], p(nb), cast[9], relax, 1, 1, p(B), p(x), nv, max_iters, 0.0,
+                               rel_tol, p(h), max_iters + 2)
+    assert it >= 0
+    return x, it, h[: it + 1]
+
+
+@pytest.mark.parametrize("block_rows", [0, 300])
+def test_amg_pbicgstab_solve_matches_reference_loops(libs, seq_dot, block_rows):
+    """The benchmark's method (AMG-PBiCGStab: HMIS / extended+i hierarchy,
+    HSGS 1+1, Direct coarse solve) on a 27-point 16^3 system, NV = 4: the
+    reference's loops in the step order of pbicgstab.inl and mg.inl, its own
+    Gauss-Jordan inverse on the coarsest level, against the oracle with the
+    reference's inner-product order on the same hierarchy: same iterations,
+    residual history and x, bit for bit; single-process sweeps and hybrid
+    blocks of 300 rows on every level."""
+    rp, ci, v = orc.gen27(16)
+    levels = orc.amg_setup(rp, ci, v, mg_coarsening_type=10, mg_interpolation_type=6,
+                           mg_strength_threshold=0.25, mg_max_levels=6, mg_coarse_matrix_size=100)
+    assert len(levels) >= 3
+    B = np.random.default_rng(2024).uniform(-1, 1, (len(rp) - 1, 4))
+    mg = orc.MG(levels, block_rows=block_rows or None)
+    xo, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg, 200, 0.0, 1e-8)
+    blocks = []
+    for lv in levels:
+        n = lv["n"]
+        br = block_rows if block_rows and block_rows < n else 0
+        blocks.append((np.append(np.arange(0, n, br), n) if br else np.array([0, n])).astype(np.int64))
+    x, itr, h = _ref_pbicgstab_amg(libs["contract"], levels, blocks, B)
+    assert itr == it and it > 0
+    assert np.array_equal(h, hist)
+    assert np.array_equal(x, xo)
