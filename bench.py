@@ -5,6 +5,9 @@ A step is one complete solve of the 16 right-hand sides from a zero initial
 guess.  Forms (all on the same operator and right-hand sides):
   plain        - FP64 PBiCGStab + FP64 AMG V-cycle, Gauss-Seidel in the
                  reference's single-process row order (parity form);
+  plain_seq    - the plain form with its inner products in the reference's
+                 single-core order (dot_order = sequential: bit for bit a
+                 one-process run of the reference; not in the default list);
   plain_hybrid - the same FP64 method with the hybrid smoother split of the
                  mixed form (every level in 444 blocks, three per SM:
                  Gauss-Seidel inside a block, Jacobi across blocks);
@@ -39,10 +42,15 @@ solve; `roofline.spmv` is the FP64 NV=16 product of the tuned SpMV kernel
 timed alone.  `gpu_launches` is the library's own count of the kernels it
 launched in the timed steps of the headline form.
 
---impl reference runs the reference's method on the host cores through the
-oracle alone (the reference itself cannot be built here: it needs MPI,
-hypre, argsparser and yaml-cpp): the same operator and right-hand sides, the
-oracle's own AMG setup, one complete FP64 solve timed.
+--impl reference runs the reference's method on the host cores: the same
+operator and right-hand sides, the oracle's own AMG setup (the reference as a
+whole cannot be built here: it needs MPI, hypre, argsparser and yaml-cpp),
+and one complete FP64 solve timed, by the reference's own loop files compiled
+unchanged with its release flags (oracle/_ref, one process), else by the
+oracle.  The GPU arm's `cpu_baseline` is one iteration of the same, scaled
+by the iteration count; `parity.c2_iter1_reference_loops` compares the GPU's
+first iteration (dot_order = sequential) with the reference loops' at full
+size, bit for bit.
 """
 import argparse
 import json
@@ -715,6 +723,30 @@ def cpu_sample(csr, B, s_plain):
     return time.perf_counter() - t0, orc.num_threads(), x, hist
 
 
+def ref_loops(kind):
+    """The reference's own loop files compiled unchanged (oracle/_ref), or None."""
+    oracle_mod()
+    import reference_loops
+    return reference_loops.lib(kind, build=False)
+
+
+def ref_sample(csr, B, levels, kind, iters=1):
+    """`iters` FP64 AMG-PBiCGStab iterations of the reference's compiled loops
+    (one process: Gauss-Seidel in its single-process order, inner products in
+    its single-core order) on the GPU plain form's hierarchy.  Returns
+    (seconds, x, history) or None when the library is absent."""
+    L = ref_loops(kind)
+    if L is None:
+        return None
+    import reference_loops
+    rp, ci, v = csr.arrays()
+    lv = [dict(l) for l in levels]
+    lv[0]["A"] = (rp, ci, v)
+    t0 = time.perf_counter()
+    x, it, h = reference_loops.pbicgstab_amg(L, lv, B, max_iters=iters, rel_tol=1e-8)
+    return time.perf_counter() - t0, x, h
+
+
 class Rows:
     """Row count and nnz of the generated operator (the reference arm's config)."""
 
@@ -724,12 +756,13 @@ class Rows:
 
 
 def reference_arm(args, rank, world):
-    """The reference's method on the host cores, through the oracle alone
-    (the reference needs MPI, hypre, argsparser and yaml-cpp and cannot be
-    built here): the same 27-point operator and right-hand sides, the
-    oracle's own AMG setup (its restatement of the hypre algorithms the
-    reference configures), and one complete FP64 AMG-PBiCGStab solve to 1e-8
-    timed end to end.  Loads no product library and touches no GPU."""
+    """The reference's method on the host cores: the same 27-point operator
+    and right-hand sides, the oracle's own AMG setup (its restatement of the
+    hypre algorithms the reference configures; the reference needs MPI,
+    hypre, argsparser and yaml-cpp and cannot be built whole), and one
+    complete FP64 AMG-PBiCGStab solve to 1e-8 timed end to end by the
+    reference's own loop files compiled unchanged (oracle/_ref), else by the
+    oracle.  Loads no product library and touches no GPU."""
     if rank != 0:
         return
     orc = oracle_mod()
@@ -739,25 +772,37 @@ def reference_arm(args, rank, world):
     p = plain_spec()["preconditioner"]
     levels = orc.amg_setup(rp, ci, v, **{k: p[k] for k in ("mg_coarsening_type", "mg_strength_threshold",
                                                            "mg_max_levels")})
-    mg = orc.MG(levels)
     setup_s = time.perf_counter() - t0
-    # one complete solve is the timed unit (about two minutes on the host);
-    # the steps/warmup of the GPU arm do not apply to it
+    # one complete solve is the timed unit (about a minute on the host); the
+    # steps/warmup of the GPU arm do not apply to it.  The reference's own
+    # loop files compiled unchanged with its release flags (one process: its
+    # single-process method, which the plain form reproduces), else the oracle.
+    L = ref_loops("generic")
     t0 = time.perf_counter()
-    x, it, hist, st, _ = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg=mg, max_iters=200, rel_tol=1e-8)
+    if L is not None:
+        import reference_loops
+        x, it, hist = reference_loops.pbicgstab_amg(L, levels, B, max_iters=200, rel_tol=1e-8)
+        st = (np.sqrt(hist[-1]) <= 1e-8 * np.sqrt(hist[0])).astype(np.int32)
+        thr, kind = 1, "reference"
+        what = ("the reference's own loop files (blas, blas2, inverse) compiled unchanged with its release flags, "
+                "in its PBiCGStab / V-cycle step order, one process")
+    else:
+        mg = orc.MG(levels)
+        x, it, hist, st, _ = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg=mg, max_iters=200, rel_tol=1e-8)
+        thr, kind = orc.num_threads(), "port"
+        what = "the oracle on %d host threads, Gauss-Seidel sweeps sequential" % thr
     sec = time.perf_counter() - t0
     ms_rhs = sec / NV * 1e3
-    thr = orc.num_threads()
     line = {"impl": "reference", "metric": "time-to-1e-8 residual per RHS", "value": round(ms_rhs, 3),
             "unit": "ms/RHS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": False, "dtype": "f64", "data": "synthetic",
-            "config": bench_config(Rows(rp), world), "form": "plain FP64 (oracle on the host)",
+            "config": bench_config(Rows(rp), world), "form": "plain FP64 (reference loops on the host)"
+            if kind == "reference" else "plain FP64 (oracle on the host)",
             "iters": int(it), "converged": bool(np.all(st > 0)), "setup_s": round(setup_s, 1),
             "levels": [l["n"] for l in levels],
-            "cpu_baseline": {"value": round(ms_rhs, 3), "unit": "ms/RHS", "cores": thr, "kind": "port",
+            "cpu_baseline": {"value": round(ms_rhs, 3), "unit": "ms/RHS", "cores": thr, "kind": kind,
                              "sample": "one complete FP64 AMG-PBiCGStab solve of the 16 RHS to 1e-8 (%d iterations, "
-                                       "%.1f s) by the oracle on %d host threads, Gauss-Seidel sweeps sequential; "
-                                       "oracle AMG setup (%.1f s) untimed" % (it, sec, thr, setup_s)},
+                                       "%.1f s) by %s; oracle AMG setup (%.1f s) untimed" % (it, sec, what, setup_s)},
             "e2e": {"value": round(ms_rhs, 3), "unit": "ms/RHS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -894,7 +939,8 @@ def main():
         best_var, var_ms = tune_spmv(csr, 0)
     apply_spmv_choice(best_var)
     allforms = args.forms.split(",")
-    specs = {"plain": plain_spec(), "plain_hybrid": plain_hybrid_spec(), "mixed": mixed_spec()}
+    specs = {"plain": plain_spec(), "plain_hybrid": plain_hybrid_spec(), "mixed": mixed_spec(),
+             "plain_seq": with_top(plain_spec(), dot_order="sequential")}
     forms = [f for f in allforms if f in specs]
     res, X, objs = {}, {}, {}
     clocks = None
@@ -980,6 +1026,30 @@ def main():
         cpu = {"value": round(sec * iters / NV * 1e3, 3), "unit": "ms/RHS", "cores": thr, "kind": "port",
                "sample": "1 FP64 PBiCGStab iteration of the same problem and hierarchy on %d host threads "
                          "(Gauss-Seidel sweeps sequential) (%.1f s), x %d iterations / %d RHS" % (thr, sec, iters, NV)}
+        levels = [fo.s.level(l) for l in range(fo.s.num_levels())]
+        # the reference's own loops (release flags): the timed CPU baseline
+        rs = ref_sample(csr, B, levels, "generic")
+        if rs is not None:
+            cpu = {"value": round(rs[0] * iters / NV * 1e3, 3), "unit": "ms/RHS", "cores": 1, "kind": "reference",
+                   "sample": "1 FP64 AMG-PBiCGStab iteration of the same problem and hierarchy by the reference's "
+                             "own loop files compiled unchanged with its release flags, one process (%.1f s), "
+                             "x %d iterations / %d RHS" % (rs[0], iters, NV),
+                   "oracle_port": {"value": round(sec * iters / NV * 1e3, 3), "cores": thr}}
+        # full-size parity with the reference's own arithmetic: the GPU's first
+        # iteration with dot_order = sequential against the reference's loops
+        # (row sums fused, as its FMA configuration compiles them)
+        rc = ref_sample(csr, B, levels, "contract")
+        if rc is not None:
+            fo.renew(with_top(fo.spec, max_iters=1, dot_order="sequential"))
+            fo.solve()
+            xg, hg = fo.x.download(), fo.s.history()
+            fo.renew(fo.spec)
+            same_x, same_h = bool(np.array_equal(xg, rc[1])), bool(np.array_equal(hg, rc[2]))
+            parity["c2_iter1_reference_loops"] = "bit-exact" if (same_x and same_h) else "differs"
+            parity["c2_iter1_reference_loops_detail"] = {
+                "x_identical": same_x, "history_identical": same_h,
+                "x_max_rel_diff": float(np.max(np.abs(xg - rc[1])) / np.max(np.abs(rc[1]))),
+                "gpu_form": "plain, dot_order = sequential", "reference_s": round(rc[0], 1)}
     objs.clear()
     if "sweep" in allforms and rank == 0:
         extra["precision_sweep"] = precision_sweep(csr, Ah, 1, 3)

@@ -1,0 +1,116 @@
+"""ctypes binding of the reference-loop libraries (oracle/_ref/
+libxamg_ref_loops_{generic,haswell,contract}.so, built by
+oracle/build_ref_loops.py from the reference's own loop files): test and
+benchmark-baseline infrastructure, never part of the product.
+
+lib(kind) loads one build (None when it was not built: the reference tree
+was absent and no prebuilt library travelled with the repository);
+pbicgstab_amg() runs a whole AMG-PBiCGStab solve in the reference's step
+order over its compiled loops (see ref_loops.h)."""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.path.join(HERE, "_ref")
+_libs = {}
+
+
+def path(kind):
+    return os.path.join(REF, "libxamg_ref_loops_%s.so" % kind)
+
+
+def lib(kind, build=True):
+    if kind in _libs:
+        return _libs[kind]
+    if not os.path.exists(path(kind)) and build:
+        import build_ref_loops
+
+        build_ref_loops.build()
+    if not os.path.exists(path(kind)):
+        return None
+    L = C.CDLL(path(kind))
+    i64, vp, ci_, cd = C.c_int64, C.c_void_p, C.c_int, C.c_double
+    for name in ("ref_csr_ax_y_d", "ref_csr_ax_y_f", "ref_csr_axpy_d", "ref_csr_axpy_f"):
+        getattr(L, name).argtypes = [i64, vp, vp, vp, vp, vp, ci_]
+    for name in ("ref_hsgs_d", "ref_hsgs_f"):
+        getattr(L, name).argtypes = [i64, vp, vp, vp, vp, vp, vp, vp, ci_, ci_, vp]
+    for name in ("ref_dense_ax_y_d", "ref_dense_ax_y_f"):
+        getattr(L, name).argtypes = [i64, i64, vp, vp, vp, ci_]
+    L.ref_dot_d.argtypes = [i64, ci_, vp, vp, vp]
+    L.ref_axpby_d.argtypes = [i64, ci_, vp, vp, vp, vp]
+    L.ref_axpby_z_d.argtypes = [i64, ci_, vp, vp, vp, vp, vp]
+    L.ref_axpbypcz_d.argtypes = [i64, ci_, vp, vp, vp, vp, vp, vp]
+    L.ref_xdivy_z_d.argtypes = [i64, ci_, vp, vp, vp]
+    L.ref_ax_y_d.argtypes = [i64, ci_, vp, vp, vp]
+    L.ref_scal_d.argtypes = [i64, ci_, vp, vp]
+    L.ref_bicgstab_d.argtypes = [i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, vp, ci_]
+    L.ref_dense_inverse_d.argtypes = [i64, vp, vp]
+    PP = C.POINTER(C.c_void_p)
+    L.ref_pbicgstab_amg_d.argtypes = [ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, vp, vp,
+                                      ci_, ci_, cd, cd, vp, ci_]
+    _libs[kind] = L
+    return L
+
+
+def p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def transpose(rp, ci, v, ncols):
+    """R = P^T with each row's entries in increasing column order."""
+    n = len(rp) - 1
+    rows = np.repeat(np.arange(n, dtype=np.int32), np.diff(rp))
+    order = np.lexsort((rows, ci))
+    rrp = np.zeros(ncols + 1, np.int32)
+    np.cumsum(np.bincount(ci, minlength=ncols), out=rrp[1:])
+    return rrp, np.ascontiguousarray(rows[order]), np.ascontiguousarray(v[order])
+
+
+def bicgstab(L, rp, ci, v, B, max_iters=1000, rel_tol=1e-8):
+    """Unpreconditioned BiCGStab from x = 0: (x, iterations, history)."""
+    n, nv = B.shape
+    x = np.zeros_like(B)
+    h = np.zeros((max_iters + 2, nv))
+    it = L.ref_bicgstab_d(n, p(rp), p(ci), p(v), p(B), p(x), nv, max_iters, 0.0, rel_tol, p(h), max_iters + 2)
+    if it < 0:
+        raise ValueError("unsupported nv")
+    return x, it, h[: it + 1]
+
+
+def _ptrs(arrs):
+    return (C.c_void_p * len(arrs))(*[a.ctypes.data if a is not None else None for a in arrs])
+
+
+def pbicgstab_amg(L, levels, B, blocks=None, max_iters=200, rel_tol=1e-8, relax=0.99, pre_it=1, post_it=1):
+    """AMG-PBiCGStab from x = 0 over `levels` (dicts with n, A, P, ncP as the
+    oracle's setup or the library's hierarchy export gives them); blocks[l]:
+    hybrid block row offsets of level l (default: one block per level, the
+    single-process sweep).  Returns (x, iterations, history)."""
+    nlev = len(levels)
+    if blocks is None:
+        blocks = [np.array([0, lv["n"]], np.int64) for lv in levels]
+    nrows = np.array([lv["n"] for lv in levels], np.int64)
+    R = [transpose(*lv["P"], lv["ncP"]) if lv.get("P") is not None else None for lv in levels]
+    cols = []
+    for k in range(3):
+        cols.append([np.ascontiguousarray(lv["A"][k]) for lv in levels])
+        cols.append([np.ascontiguousarray(lv["P"][k]) if lv.get("P") is not None else None for lv in levels])
+        cols.append([r[k] if r is not None else None for r in R])
+    arp, prp, rrp, aci, pci, rci, av, pv, rv = cols
+    blocks = [np.ascontiguousarray(b, np.int64) for b in blocks]
+    nb = np.array([len(b) - 1 for b in blocks], np.int32)
+    PP = C.POINTER(C.c_void_p)
+    tabs = [_ptrs(x) for x in (arp, aci, av, prp, pci, pv, rrp, rci, rv, blocks)]
+    cast = [C.cast(t, PP) for t in tabs]
+    n, nv = B.shape
+    B = np.ascontiguousarray(B, np.float64)
+    x = np.zeros_like(B)
+    h = np.zeros((max_iters + 2, nv))
+    it = L.ref_pbicgstab_amg_d(nlev, p(nrows), cast[0], cast[1], cast[2], cast[3], cast[4], cast[5], cast[6],
+                               cast[7], cast[8], p(nb), cast[9], relax, pre_it, post_it, p(B), p(x), nv,
+                               max_iters, 0.0, rel_tol, p(h), max_iters + 2)
+    if it < 0:
+        raise ValueError("unsupported nv or hierarchy")
+    return x, it, h[: it + 1]

@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import oracle as orc
+import reference_loops
 import util
 import xamg
 
@@ -58,6 +59,88 @@ def test_bicgstab_c1_parity(gpu, nv):
     assert_same_history(s.history(), hist)
     np.testing.assert_allclose(X, xo, rtol=1e-12, atol=1e-14 * np.abs(xo).max())
     assert all(s.converged())
+
+
+def _oracle_seq(fn, *args):
+    orc.set_seq_dot(True)
+    try:
+        return fn(*args)
+    finally:
+        orc.set_seq_dot(False)
+
+
+@pytest.mark.parametrize("nv", [1, 4])
+def test_bicgstab_c1_sequential_dot_matches_reference_order(gpu, nv):
+    """dot_order = sequential: the inner products run in the reference's
+    single-core order (one dependent chain per column), and the whole C1
+    solve (7-point Poisson on 32^3, BiCGStab to 1e-8) is bit for bit the
+    oracle's in that order, itself bit for bit the reference's own loops
+    compiled unchanged (tests/test_ref_loops.py); where that library travelled
+    with the repository the GPU is compared with it directly as well.  The
+    tree order gives a different iteration count on this system."""
+    csr = xamg.CsrMatrix.cube(32, 32, 32, 0)
+    rp, ci, v = csr.arrays()
+    B = np.random.default_rng(1234).uniform(-1, 1, (csr.nrows, nv))
+    spec = util.amg_params(precond_mg=False, max_iters=1000)
+    spec["solver"]["dot_order"] = "sequential"
+    s, X, keep = solve_api(csr, spec, B)
+    xo, it, hist, st, r0 = _oracle_seq(orc.pbicgstab, rp, ci, v, B, np.zeros_like(B), None, 1000, 0.0, 1e-8)
+    assert s.iters()[0] == it
+    assert np.array_equal(s.history(), hist)
+    assert np.array_equal(X, xo)
+    L = reference_loops.lib("contract", build=False)
+    if L is not None:
+        xr, itr, hr = reference_loops.bicgstab(L, rp, ci, v, B, 1000, 1e-8)
+        assert itr == s.iters()[0]
+        assert np.array_equal(hr, s.history())
+        assert np.array_equal(xr, X)
+
+
+def test_pbicgstab_amg_sequential_dot_parity(gpu):
+    """AMG-PBiCGStab (27-point 24^3, HSGS) with the reference's single-core
+    inner-product order, bit for bit against the oracle in that order."""
+    csr = xamg.CsrMatrix.aniso27(24)
+    rp, ci, v = csr.arrays()
+    B = np.random.default_rng(78).uniform(-1, 1, (csr.nrows, 4))
+    spec = util.amg_params(max_levels=6)
+    spec["solver"]["dot_order"] = "sequential"
+    s, X, keep = solve_api(csr, spec, B)
+    mg = oracle_mg(s, spec)
+    xo, it, hist, st, r0 = _oracle_seq(orc.pbicgstab, rp, ci, v, B, np.zeros_like(B), mg, 200, 0.0, 1e-8)
+    assert s.iters()[0] == it and it > 0
+    assert np.array_equal(s.history(), hist)
+    assert np.array_equal(X, xo)
+    # the tree order reaches the same solution to rounding
+    spec["solver"]["dot_order"] = "tree"
+    s2, X2, keep2 = solve_api(csr, spec, B)
+    np.testing.assert_allclose(X2, X, rtol=1e-6, atol=1e-9 * np.abs(X).max())
+
+
+@pytest.mark.parametrize("grid,nv", [(11, 32), (13, 1), (23, 8)])
+def test_sequential_dot_ragged_sizes(gpu, grid, nv):
+    """The sequential inner products on row counts that end in a partial tile
+    (1331, 2197 and 12167 rows) and on the widest block (NV = 32, the largest
+    shared-memory stage): 40 BiCGStab iterations, converged or not, bit for
+    bit against the oracle in the same order."""
+    csr = xamg.CsrMatrix.aniso27(grid)
+    rp, ci, v = csr.arrays()
+    B = np.random.default_rng(grid).uniform(-1, 1, (csr.nrows, nv))
+    spec = util.amg_params(precond_mg=False, max_iters=40, rel=1e-14)
+    spec["solver"]["dot_order"] = "sequential"
+    s, X, keep = solve_api(csr, spec, B)
+    xo, it, hist, st, r0 = _oracle_seq(orc.pbicgstab, rp, ci, v, B, np.zeros_like(B), None, 40, 0.0, 1e-14)
+    assert s.iters()[0] == it
+    assert np.array_equal(s.history(), hist)
+    assert np.array_equal(X, xo)
+
+
+def test_dot_order_rejects_unknown_value(gpu):
+    csr = xamg.CsrMatrix.aniso27(8)
+    B = np.ones((csr.nrows, 1))
+    spec = util.amg_params(precond_mg=False)
+    spec["solver"]["dot_order"] = "pairwise"
+    with pytest.raises(Exception, match="dot_order"):
+        solve_api(csr, spec, B)
 
 
 @pytest.mark.parametrize("smoother,block_rows", [("HSGS", 0), ("HSGS", 512), ("Jacobi", 0)])

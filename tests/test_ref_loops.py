@@ -13,50 +13,22 @@ Three builds of the same loop files (see oracle/build_ref_loops.py):
             roundings, BLAS-1 and the inner product bit-identical.
 The libraries are built from the reference tree in this container; where it
 is absent (and no prebuilt library travelled) the tests skip."""
-import ctypes as C
-import os
-
 import numpy as np
 import pytest
 
 import oracle as orc
+import reference_loops
 import util
 
-HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.path.join(os.path.dirname(HERE), "oracle", "_ref")
 EPS = np.finfo(np.float64).eps
 EPS32 = np.finfo(np.float32).eps
 p = orc.p
 
 
 def _load(kind):
-    path = os.path.join(REF, "libxamg_ref_loops_%s.so" % kind)
-    if not os.path.exists(path):
-        import build_ref_loops
-
-        build_ref_loops.build()
-    if not os.path.exists(path):
+    L = reference_loops.lib(kind)
+    if L is None:
         pytest.skip("reference loop library not built (reference tree absent)")
-    L = C.CDLL(path)
-    i64, vp, ci_, cd = C.c_int64, C.c_void_p, C.c_int, C.c_double
-    for name in ("ref_csr_ax_y_d", "ref_csr_ax_y_f", "ref_csr_axpy_d", "ref_csr_axpy_f"):
-        getattr(L, name).argtypes = [i64, vp, vp, vp, vp, vp, ci_]
-    for name in ("ref_hsgs_d", "ref_hsgs_f"):
-        getattr(L, name).argtypes = [i64, vp, vp, vp, vp, vp, vp, vp, ci_, ci_, vp]
-    for name in ("ref_dense_ax_y_d", "ref_dense_ax_y_f"):
-        getattr(L, name).argtypes = [i64, i64, vp, vp, vp, ci_]
-    L.ref_dot_d.argtypes = [i64, ci_, vp, vp, vp]
-    L.ref_axpby_d.argtypes = [i64, ci_, vp, vp, vp, vp]
-    L.ref_axpby_z_d.argtypes = [i64, ci_, vp, vp, vp, vp, vp]
-    L.ref_axpbypcz_d.argtypes = [i64, ci_, vp, vp, vp, vp, vp, vp]
-    L.ref_xdivy_z_d.argtypes = [i64, ci_, vp, vp, vp]
-    L.ref_ax_y_d.argtypes = [i64, ci_, vp, vp, vp]
-    L.ref_scal_d.argtypes = [i64, ci_, vp, vp]
-    L.ref_bicgstab_d.argtypes = [i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, vp, ci_]
-    L.ref_dense_inverse_d.argtypes = [i64, vp, vp]
-    PP = C.POINTER(C.c_void_p)
-    L.ref_pbicgstab_amg_d.argtypes = [ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, vp, vp,
-                                      ci_, ci_, cd, cd, vp, ci_]
     return L
 
 
@@ -253,12 +225,7 @@ def seq_dot():
 
 
 def _ref_bicgstab(L, rp, ci, v, B, max_iters=1000, rel_tol=1e-8):
-    n, nv = B.shape
-    x = np.zeros_like(B)
-    h = np.zeros((max_iters + 2, nv))
-    it = L.ref_bicgstab_d(n, p(rp), p(ci), p(v), p(B), p(x), nv, max_iters, 0.0, rel_tol, p(h), max_iters + 2)
-    assert it >= 0
-    return x, it, h[: it + 1]
+    return reference_loops.bicgstab(L, rp, ci, v, B, max_iters, rel_tol)
 
 
 @pytest.mark.parametrize("nv", [1, 4])
@@ -301,37 +268,6 @@ def test_bicgstab_inner_product_order_changes_iterations(libs):
     assert (it_tree, it_ref) == (90, 88)
 
 
-def _ptrs(arrs):
-    return (C.c_void_p * len(arrs))(*[a.ctypes.data if a is not None else None for a in arrs])
-
-
-def _ref_pbicgstab_amg(L, levels, blocks, B, max_iters=200, rel_tol=1e-8, relax=0.99):
-    """levels: orc.amg_setup output; blocks[l]: block row offsets of level l."""
-    nlev = len(levels)
-    nrows = np.array([lv["n"] for lv in levels], np.int64)
-    R = [orc.transpose(*lv["P"], lv["ncP"]) if lv["P"] is not None else None for lv in levels]
-    keep = [nrows]
-    cols = []
-    for k in range(3):
-        cols.append([lv["A"][k] for lv in levels])
-        cols.append([lv["P"][k] if lv["P"] is not None else None for lv in levels])
-        cols.append([r[k] if r is not None else None for r in R])
-    arp, prp, rrp, aci, pci, rci, av, pv, rv = cols
-    nb = np.array([len(b) - 1 for b in blocks], np.int32)
-    tabs = [_ptrs(x) for x in (arp, aci, av, prp, pci, pv, rrp, rci, rv, blocks)]
-    keep += [cols, R, nb, blocks, tabs]
-    n, nv = B.shape
-    x = np.zeros_like(B)
-    h = np.zeros((max_iters + 2, nv))
-    PP = C.POINTER(C.c_void_p)
-    cast = [C.cast(t, PP) for t in tabs]
-    it = L.ref_pbicgstab_amg_d(nlev, p(nrows), cast[0], cast[1], cast[2], cast[3], cast[4], cast[5], cast[6],
-                               cast[7], cast[8], p(nb), cast[9], relax, 1, 1, p(B), p(x), nv, max_iters, 0.0,
-                               rel_tol, p(h), max_iters + 2)
-    assert it >= 0
-    return x, it, h[: it + 1]
-
-
 @pytest.mark.parametrize("block_rows", [0, 300])
 def test_amg_pbicgstab_solve_matches_reference_loops(libs, seq_dot, block_rows):
     """The benchmark's method (AMG-PBiCGStab: HMIS / extended+i hierarchy,
@@ -353,7 +289,7 @@ def test_amg_pbicgstab_solve_matches_reference_loops(libs, seq_dot, block_rows):
         n = lv["n"]
         br = block_rows if block_rows and block_rows < n else 0
         blocks.append((np.append(np.arange(0, n, br), n) if br else np.array([0, n])).astype(np.int64))
-    x, itr, h = _ref_pbicgstab_amg(libs["contract"], levels, blocks, B)
+    x, itr, h = reference_loops.pbicgstab_amg(libs["contract"], levels, B, blocks=blocks)
     assert itr == it and it > 0
     assert np.array_equal(h, hist)
     assert np.array_equal(x, xo)

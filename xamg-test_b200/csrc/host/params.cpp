@@ -215,7 +215,7 @@ std::string GlobalParams::validate(const std::string &key, char type) {
         {"mg_agg_P12max_elements", 'I'},
         // extensions of this library (no reference counterpart)
         {"hybrid_block_rows", 'I'}, {"inner_rel_tolerance", 'F'}, {"gs_schedule", 'S'},
-        {"rel_tolerance_base", 'S'}, {"hybrid_blocks", 'I'}};
+        {"rel_tolerance_base", 'S'}, {"hybrid_blocks", 'I'}, {"dot_order", 'S'}};
     auto it = known.find(key);
     if (it == known.end()) return "unknown parameter: " + key;
     if (it->second != type && !(it->second == 'F' && type == 'I'))

@@ -807,6 +807,16 @@ static void dot1(const DVec &a, const DVec &b, DBuf &part, double *out, cudaStre
     const void *A[1] = {a.p()}, *B[1] = {b.p()};
     xk::dots(a.prec, a.nv, a.n, 1, A, B, part.as<double>(), out, s);
 }
+// dot_order = "tree" (default: the fixed reduction tree the kernels share)
+// or "sequential" (the reference's single-core order, blas.inl:561-576;
+// one dependent chain per column, for results bit-identical to a
+// one-process run of the reference)
+static bool dot_order_sequential(const ParamList &l) {
+    if (!l.has("dot_order")) return false;
+    const std::string o = l.get_string("dot_order");
+    if (o != "tree" && o != "sequential") throw Error("dot_order must be \"tree\" or \"sequential\"", 4);
+    return o == "sequential";
+}
 static void ensure_part(DBuf &part, i64 n, int nd, int nv) {
     size_t need = sizeof(double) * std::max<i64>(xk::dot_part_size(n, nd, nv), 1);
     if (part.bytes < need) part.alloc(need);
@@ -1375,6 +1385,7 @@ struct Krylov : Solver {
     bool precond = false;
     bool reordered = false;  // RBiCGStab
     bool cg = false;         // PCG
+    bool seq_dot = false;    // dot_order = sequential
     DVec r0, r, p, v, s, t, p_, s_;
     DBuf part, sc;
     Pinned hres;
@@ -1397,6 +1408,7 @@ struct Krylov : Solver {
 
     void setup(i64 n) {
         parse_conv(prm, conv);
+        seq_dot = dot_order_sequential(prm);
         conv.init(nv);
         conv.prefix = role == "meta_solver" ? "META" : "SOLV";
         for (DVec *q : {&r0, &r, &p, &v, &s, &t}) q->alloc(n, nv, prec);
@@ -1446,6 +1458,8 @@ struct Krylov : Solver {
     }
 
     void solve(DVec &x, const DVec &b) override {
+        seq_dot = dot_order_sequential(prm);  // renewed parameters apply at the next solve
+        xk::DotOrderScope order(seq_dot);
         if (reordered) { solve_reordered(x, b); return; }
         if (cg) { solve_cg(x, b); return; }
         cudaStream_t st = ctx().stream;
@@ -1504,6 +1518,11 @@ struct Krylov : Solver {
             }
             xk::bicg_xr(prec, nv, n, sc, pp->p(), ss->p(), x.p(), s.p(), t.p(), r.p(), r0.p(), part.as<double>(),
                         st);
+            if (seq_dot) {
+                // (r, r0) in the sequential order replaces the fused pass's tree partials
+                const void *Aa[1] = {r.p()}, *Bb[1] = {r0.p()};
+                xk::dot_partials(prec, nv, n, 1, Aa, Bb, part.as<double>(), st);
+            }
             XCUDA(cudaMemcpyAsync(hres_async.h, S(RES), sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
             XCUDA(cudaEventRecord(res_ready, st));
             // the next direction is formed before the host has looked at the
@@ -1661,8 +1680,10 @@ struct IterRefine : Solver {
     DVec r, xc, ix, ib;
     DBuf part, ones;
     Pinned hres;
+    bool seq_dot = false;
     void setup(i64 n) {
         parse_conv(prm, conv);
+        seq_dot = dot_order_sequential(prm);
         conv.init(nv);
         conv.prefix = "META";
         r.alloc(n, nv, Prec::F64);
@@ -1676,6 +1697,7 @@ struct IterRefine : Solver {
     }
     bool residual_check(DVec &x, const DVec &b, bool initial) {
         cudaStream_t s = ctx().stream;
+        xk::DotOrderScope order(seq_dot);
         const DCsr &a = A->d;
         a.spmv(Prec::F64, nv, x.p(), r.p(), 2, b.p(), s);
         DBuf out(sizeof(double) * nv);
@@ -1688,6 +1710,8 @@ struct IterRefine : Solver {
         return conv.check();
     }
     void solve(DVec &x, const DVec &b) override {
+        seq_dot = dot_order_sequential(prm);
+        xk::DotOrderScope order(seq_dot);
         cudaStream_t s = ctx().stream;
         int max_iters = (int)prm.get_int("max_iters");
         conv.init(nv);

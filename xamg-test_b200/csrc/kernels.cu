@@ -1105,6 +1105,68 @@ __global__ void __launch_bounds__(256) k_dot2(i64 nch, const double *__restrict_
     }
 }
 
+// Inner products in the reference's single-core order (blas.inl:561-576):
+// per column k, res = 0; res += a_i * b_i for i = 0 .. n-1, the product and
+// the sum each rounded (no fma).  A sum in that order is one dependent chain
+// per column.  Block d serves pair d: warps 1-7 load tiles of SEQ_TILE rows
+// and store their products (each rounded) in a shared-memory double buffer
+// while lane k of warp 0 adds the previous tile's products of column k in
+// row order, so the chain waits on shared memory, not on HBM.  The sum is
+// stored as the partial of chunk 0, and the remaining blocks zero the pair's
+// other chunk partials, so the reduction stage (k_dot2, k_dot2_epi: +0 plus
+// the chunk partials in order, then a pairwise fold with zeros) returns it
+// unchanged.
+constexpr int SEQ_TILE = 128;
+// products a_i * b_i (rounded) of rows [t*SEQ_TILE, ...) into buf, by the
+// block's threads 32..255
+template <class TI, int NV>
+__device__ __forceinline__ void seq_fill(const TI *__restrict__ a, const TI *__restrict__ b, i64 n, i64 t,
+                                         double *buf) {
+    const i64 r0 = t * SEQ_TILE;
+    const int cnt = (int)(n - r0 < SEQ_TILE ? n - r0 : SEQ_TILE) * NV;
+    for (int q = (int)threadIdx.x - 32; q < cnt; q += 224)
+        buf[q] = dmul((double)a[r0 * NV + q], (double)b[r0 * NV + q]);
+}
+template <class TI, int NV>
+__global__ void __launch_bounds__(256) k_dot_seq(i64 n, i64 nch, int nd, DotPairs<TI> pr,
+                                                 double *__restrict__ part) {
+    if ((int)blockIdx.x >= nd) {
+        const i64 per = nch - 1;
+        const i64 tot = (i64)nd * NV * per;
+        const i64 stride = (i64)(gridDim.x - nd) * blockDim.x;
+        for (i64 q = (i64)(blockIdx.x - nd) * blockDim.x + threadIdx.x; q < tot; q += stride)
+            part[(q / per) * nch + 1 + q % per] = 0.0;
+        return;
+    }
+    // products of one tile, row-major [row][column]
+    extern __shared__ double prod[];  // 2 * SEQ_TILE * NV
+    const int d = blockIdx.x;
+    // constant indices keep the parameter struct out of local memory
+    const TI *__restrict__ a = d == 0 ? pr.a[0] : d == 1 ? pr.a[1] : d == 2 ? pr.a[2] : pr.a[3];
+    const TI *__restrict__ b = d == 0 ? pr.b[0] : d == 1 ? pr.b[1] : d == 2 ? pr.b[2] : pr.b[3];
+    const i64 ntiles = (n + SEQ_TILE - 1) / SEQ_TILE;
+    const int tid = threadIdx.x;
+    const bool loader = tid >= 32;
+    if (loader && ntiles > 0) seq_fill<TI, NV>(a, b, n, 0, prod);
+    __syncthreads();
+    double s = 0.0;
+    for (i64 t = 0; t < ntiles; ++t) {
+        double *cur = prod + (t & 1) * (SEQ_TILE * NV);
+        if (loader) {
+            if (t + 1 < ntiles) seq_fill<TI, NV>(a, b, n, t + 1, prod + ((t + 1) & 1) * (SEQ_TILE * NV));
+        } else if (tid < NV) {
+            const int rows = (int)(n - t * SEQ_TILE < SEQ_TILE ? n - t * SEQ_TILE : SEQ_TILE);
+            for (int r = 0; r < rows; ++r) s = dadd(s, cur[r * NV + tid]);
+        }
+        __syncthreads();
+    }
+    if (tid < NV) part[((i64)d * NV + tid) * nch] = s;
+}
+
+static thread_local bool t_dot_seq = false;
+void set_dot_sequential(bool on) { t_dot_seq = on; }
+bool dot_sequential() { return t_dot_seq; }
+
 i64 dot_part_size(i64 n, int nd, int nv) { return ((n + 255) / 256) * nd * nv; }
 
 template <class TI, int NV>
@@ -1120,6 +1182,16 @@ static void dots_t(i64 n, int nd, const void *const *a, const void *const *b, do
     for (int d = 0; d < 4; ++d) {
         pr.a[d] = (const TI *)a[d < nd ? d : 0];
         pr.b[d] = (const TI *)b[d < nd ? d : 0];
+    }
+    if (t_dot_seq) {
+        // one block per pair plus blocks that zero the other chunk partials
+        const unsigned zb = (unsigned)std::min<i64>(4 * 148, std::max<i64>(1, (nd * NV * (nch - 1) + 255) / 256));
+        note_launch(reduce ? 2 : 1);
+        const size_t smem = sizeof(double) * 2 * SEQ_TILE * NV;  // 64 KB at NV = 32
+        cudaFuncSetAttribute(k_dot_seq<TI, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_dot_seq<TI, NV><<<(unsigned)nd + zb, 256, smem, s>>>(n, nch, nd, pr, part);
+        if (reduce) k_dot2<<<nd * NV, 256, 0, s>>>(nch, part, out);
+        return;
     }
     note_launch(2);
     if (nd == 1) k_dot1<TI, NV, 1><<<g, 256, 0, s>>>(n, nch, pr, part);

@@ -167,6 +167,16 @@ void dense_gemv(Prec p, int nv, int n, const void *AinvT, const void *b, void *y
 // nd (1..4) pairs (a_d, b_d) of N x NV vectors (element type `in`), FP64
 // results out[d*nv + k].  part must hold dot_part_size(n, nd, nv) doubles.
 i64 dot_part_size(i64 n, int nd, int nv);
+// Order of the inner products of dots / dot_partials on this host thread:
+// the fixed tree (default) or the reference's single-core sequential order
+// (k_dot_seq; same partial layout, so the reduction stages are unchanged).
+void set_dot_sequential(bool on);
+bool dot_sequential();
+struct DotOrderScope {
+    bool prev;
+    explicit DotOrderScope(bool seq) : prev(dot_sequential()) { set_dot_sequential(seq); }
+    ~DotOrderScope() { set_dot_sequential(prev); }
+};
 void dots(Prec in, int nv, i64 n, int nd, const void *const *a, const void *const *b,
           double *part, double *out, cudaStream_t s);
 

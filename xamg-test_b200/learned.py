@@ -44,6 +44,17 @@ def n_params():
     return sum(27 * ci * co + co for _, ci, co, _ in LAYERS)
 
 
+# resolution level of each layer (0: n^3 cells, l: (n / 2^l)^3 cells)
+LEVEL = {"e0a": 0, "e0b": 0, "e1a": 1, "e1b": 1, "e2a": 2, "e2b": 2, "b1": 3, "b2": 3,
+         "d2a": 2, "d2b": 2, "d1a": 1, "d1b": 1, "d0a": 0, "d0b": 0, "out": 0}
+
+
+def conv_shapes():
+    """(level, input channels, output channels) of every convolution of a
+    forward pass; its multiply-adds per volume are 27 ci co (n >> level)^3."""
+    return [(LEVEL[name], ci, co) for name, ci, co, _ in LAYERS]
+
+
 _SIGS = {
     "xcnn_conv3d": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                     C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p],
@@ -557,8 +568,37 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--weights", default="")
     ap.add_argument("--load", default="")
+    ap.add_argument("--forward-only", type=int, default=0, metavar="K",
+                    help="time K forward passes (inference) of the network on random inputs of nv volumes of n^3 "
+                         "cells and exit; --tcgen05 selects the tcgen05 convolution")
+    ap.add_argument("--tcgen05", action="store_true")
     args = ap.parse_args()
     log = lambda m: print(m, file=sys.stderr, flush=True)
+    if args.forward_only:
+        L = klib()
+        L.xcnn_set_tc_conv(int(args.tcgen05))
+        net = Net(seed=1)
+        if args.load:
+            net.load(args.load)
+        g = torch.Generator().manual_seed(3)
+        a = torch.randn((args.nv, args.n, args.n, args.n), generator=g).cuda()
+        b = torch.randn((args.nv, args.n, args.n, args.n), generator=g).cuda()
+        B = net._bufs(args.nv, args.n)
+        net.pack(B, a, b)
+        net.forward(B)  # warm-up
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.forward_only):
+            net.forward(B)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.forward_only
+        flops = 2.0 * args.nv * sum(27 * ci * co * (args.n >> lev) ** 3 for lev, ci, co in conv_shapes())
+        print(json.dumps({"n": args.n, "nv": args.nv, "tcgen05": bool(args.tcgen05), "ms_forward": round(ms, 3),
+                          "conv_tflops": round(flops / ms / 1e9, 1), "tc_error": int(L.xcnn_tc_error())}),
+              flush=True)
+        return
     xamg.init(args.nv)
     net = Net(seed=1)
     res = {"n": args.n, "nv": args.nv, "params": n_params()}
