@@ -2,6 +2,7 @@
 // flags, and BiCGStab in the reference's step order over them.
 #include <algorithm>
 #include <cstring>
+#include <memory>
 
 #include "include_ref.h"
 #include "ref_loops.h"
@@ -209,6 +210,154 @@ struct Bicgstab {
     }
 };
 
+// Shared state of the PCG and RBiCGStab drivers: operator, optional V-cycle
+// preconditioner (identity without one: M^{-1} r = r), convergence.
+struct KrylovBase {
+    int64_t n; const int *rp, *ci; const double *v, *b; double *x; int nv, max_iters;
+    double abs_tol, rel_tol; double *hist; int cap;
+    const Hier *mg;
+    int iters;
+    template <int NV> void Ax(const vector &in, vector &out) const {
+        ref_csr_ax_y_d(n, rp, ci, v, in.get_aligned_ptr<double>(), out.get_aligned_ptr<double>(), NV);
+    }
+    // set_const(out, 0); precond->solve(out, in)
+    template <int NV> void precond(vector &out, const vector &in) const {
+        blas::set_const<double, NV>(out, 0.0, true);
+        if (mg)
+            mg->cycle<NV>(0, out.get_aligned_ptr<double>(), in.get_aligned_ptr<double>());
+        else
+            blas::copy<double, NV>(in, out);
+    }
+};
+
+// PCG in the step order of pcg.inl:48-160.
+struct Pcg : KrylovBase {
+    explicit Pcg(const KrylovBase &k) : KrylovBase(k) {}
+    template <int NV> void run() {
+        typedef double F;
+        size_t sz = (size_t)n * NV;
+        std::vector<F> r(sz, 0.0), z(sz, 0.0), p(sz, 0.0), ap(sz, 0.0);
+        vector R = block(r.data(), n, NV), Z = block(z.data(), n, NV), P = block(p.data(), n, NV),
+               AP = block(ap.data(), n, NV), X = block(x, n, NV), B = block(b, n, NV);
+        std::vector<F> one(NV, 1.0), mone(NV, -1.0), ic(NV, 1.0), s1(NV), s2(NV), s3(NV), al(NV), be(NV),
+            res(NV), alc(NV);
+        vector a1 = scalars(one.data(), NV), a_1 = scalars(mone.data(), NV), iconv = scalars(ic.data(), NV),
+               S1 = scalars(s1.data(), NV), S2 = scalars(s2.data(), NV), S3 = scalars(s3.data(), NV),
+               Al = scalars(al.data(), NV), Be = scalars(be.data(), NV), Res = scalars(res.data(), NV),
+               Alc = scalars(alc.data(), NV);
+        Conv cv{std::vector<double>(NV), std::vector<double>(NV), std::vector<int>(NV, 0),
+                abs_tol, rel_tol, hist, cap, 0, NV};
+        // r = b - A x, res0 = (r, r) (stats.h:208-219)
+        Ax<NV>(X, R);
+        blas::axpby<F, NV>(1.0, B, -1.0, R);
+        blas::dot<F, NV>(R, R, Res);
+        for (int k = 0; k < NV; ++k) cv.res0[k] = res[k];
+        cv.update(res.data());
+        if (cv.check(ic.data())) { iters = 0; return; }
+        precond<NV>(Z, R);
+        blas::copy<F, NV>(Z, P);
+        int it = 0;
+        for (bool last = false; !last;) {
+            it++;
+            if (it >= max_iters) last = true;
+            Ax<NV>(P, AP);
+            blas::dot<F, NV>(R, Z, S1);
+            blas::dot<F, NV>(P, AP, S2);
+            blas::xdivy_z<F, NV>(S1, S2, Al);
+            blas::ax_y<F, NV>(iconv, Al, Alc);
+            blas::axpby<F, NV>(Alc, P, a1, X);
+            blas::scal<F, NV>(a_1, Al);
+            blas::axpby<F, NV>(Al, AP, a1, R);
+            precond<NV>(Z, R);
+            blas::dot<F, NV>(R, Z, S3);
+            blas::xdivy_z<F, NV>(S3, S1, Be);
+            blas::axpby<F, NV>(a1, Z, Be, P);
+            blas::dot<F, NV>(R, R, Res);
+            cv.update(res.data());
+            if (cv.check(ic.data())) break;
+        }
+        iters = it;
+    }
+};
+
+// RBiCGStab in the step order of rbicgstab.inl:48-225 (the allreduce that
+// the reference overlaps with the preconditioner changes no value on one
+// process).
+struct Rbicgstab : KrylovBase {
+    explicit Rbicgstab(const KrylovBase &k) : KrylovBase(k) {}
+    template <int NV> void run() {
+        typedef double F;
+        size_t sz = (size_t)n * NV;
+        std::vector<F> r0(sz, 0.0), r(sz, 0.0), z(sz, 0.0), v_(sz, 0.0), vv(sz, 0.0), s(sz, 0.0),
+            t_(sz, 0.0), t(sz, 0.0);
+        vector R0 = block(r0.data(), n, NV), R = block(r.data(), n, NV), Z = block(z.data(), n, NV),
+               V_ = block(v_.data(), n, NV), V = block(vv.data(), n, NV), S = block(s.data(), n, NV),
+               T_ = block(t_.data(), n, NV), T = block(t.data(), n, NV), X = block(x, n, NV),
+               B = block(b, n, NV);
+        std::vector<F> one(NV, 1.0), mone(NV, -1.0), ic(NV, 1.0), rho(NV), delta(NV), al(NV), om(NV),
+            theta(NV), phi(NV), psi(NV), eta(NV), res(NV), alc(NV), omc(NV), be(NV), tmp(NV);
+        vector a1 = scalars(one.data(), NV), a_1 = scalars(mone.data(), NV), iconv = scalars(ic.data(), NV),
+               Rho = scalars(rho.data(), NV), Delta = scalars(delta.data(), NV), Al = scalars(al.data(), NV),
+               Om = scalars(om.data(), NV), Theta = scalars(theta.data(), NV), Phi = scalars(phi.data(), NV),
+               Psi = scalars(psi.data(), NV), Eta = scalars(eta.data(), NV), Res = scalars(res.data(), NV),
+               Alc = scalars(alc.data(), NV), Omc = scalars(omc.data(), NV), Be = scalars(be.data(), NV),
+               Tmp = scalars(tmp.data(), NV);
+        Conv cv{std::vector<double>(NV), std::vector<double>(NV), std::vector<int>(NV, 0),
+                abs_tol, rel_tol, hist, cap, 0, NV};
+        Ax<NV>(X, R0);                                             // 1
+        blas::axpby<F, NV>(1.0, B, -1.0, R0);
+        blas::dot<F, NV>(R0, R0, Rho);                            // 2
+        for (int k = 0; k < NV; ++k) cv.res0[k] = rho[k];
+        cv.update(rho.data());
+        if (cv.check(ic.data())) { iters = 0; return; }
+        blas::copy<F, NV>(R0, R);
+        precond<NV>(Z, R0);                                       // 3
+        blas::copy<F, NV>(Z, V_);                                 // 4
+        int it = 0;
+        for (bool last = false; !last;) {
+            it++;
+            if (it >= max_iters) last = true;
+            Ax<NV>(V_, V);                                        // 6
+            blas::dot<F, NV>(V, R0, Delta);                       // 7
+            precond<NV>(S, V);                                    // 8
+            blas::xdivy_z<F, NV>(Rho, Delta, Al);                 // 9
+            blas::scal<F, NV>(a_1, Al);                           // 10
+            blas::axpby_z<F, NV>(a1, Z, Al, S, T_);
+            blas::scal<F, NV>(a_1, Al);
+            Ax<NV>(T_, T);                                        // 11
+            blas::scal<F, NV>(a_1, Al);                           // 12
+            blas::axpby<F, NV>(Al, V, a1, R);
+            blas::scal<F, NV>(a_1, Al);
+            blas::dot<F, NV>(T, R, Theta);                        // 13
+            blas::dot<F, NV>(T, T, Phi);
+            blas::dot<F, NV>(T, R0, Psi);
+            blas::dot<F, NV>(R, R, Eta);
+            precond<NV>(Z, T);                                    // 14
+            blas::xdivy_z<F, NV>(Theta, Phi, Om);                 // 15
+            blas::scal<F, NV>(a_1, Om);                           // 16
+            blas::axpby<F, NV>(Om, T, a1, R);
+            blas::scal<F, NV>(a_1, Om);
+            blas::ax_y<F, NV>(Om, Theta, Res);                    // 17
+            blas::axpby<F, NV>(a1, Eta, a_1, Res);
+            blas::ax_y<F, NV>(iconv, Al, Alc);                    // 23
+            blas::ax_y<F, NV>(iconv, Om, Omc);
+            blas::axpbypcz<F, NV>(Alc, V_, Omc, T_, a1, X);
+            cv.update(res.data());
+            if (cv.check(ic.data())) break;
+            blas::ax_y<F, NV>(Om, Psi, Rho);                      // 21
+            blas::scal<F, NV>(a_1, Rho);
+            blas::ax_y<F, NV>(Delta, Om, Tmp);                    // 22
+            blas::xdivy_z<F, NV>(Rho, Tmp, Be);
+            blas::scal<F, NV>(a_1, Om);                           // 24 (omega stays negated)
+            blas::axpby<F, NV>(a1, T_, Om, Z);
+            blas::ax_y<F, NV>(Om, Be, Delta);                     // 25
+            blas::scal<F, NV>(a_1, Om);
+            blas::axpbypcz<F, NV>(a1, Z, Delta, S, Be, V_);
+        }
+        iters = it;
+    }
+};
+
 }  // namespace
 
 extern "C" {
@@ -250,6 +399,38 @@ int ref_bicgstab_d(int64_t n, const int *rp, const int *ci, const double *v, con
     Bicgstab f{n, rp, ci, v, b, x, nv, max_iters, abs_tol, rel_tol, hist, hist_cap, nullptr, 0};
     if (dispatch_nv(nv, f)) return -1;
     return f.iters;
+}
+static Hier *make_hier(int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
+                       const double *const *av, const int *const *prp, const int *const *pci,
+                       const double *const *pv, const int *const *rrp, const int *const *rci,
+                       const double *const *rv, const int *nb, const int64_t *const *bp, double relax,
+                       int pre_it, int post_it) {
+    if (nlev < 2) return nullptr;
+    Hier *h = new Hier{nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax, pre_it, post_it, {}, {}};
+    h->init();
+    return h;
+}
+int ref_krylov_d(int method, int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
+                 const double *const *av, const int *const *prp, const int *const *pci,
+                 const double *const *pv, const int *const *rrp, const int *const *rci,
+                 const double *const *rv, const int *nb, const int64_t *const *bp, double relax, int pre_it,
+                 int post_it, const double *b, double *x, int nv, int max_iters, double abs_tol,
+                 double rel_tol, double *hist, int hist_cap) {
+    std::unique_ptr<Hier> h(make_hier(nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax,
+                                      pre_it, post_it));
+    KrylovBase kb{nrows[0], arp[0], aci[0], av[0], b, x, nv, max_iters, abs_tol, rel_tol, hist, hist_cap,
+                  h.get(), 0};
+    if (method == 1) {
+        Pcg f(kb);
+        if (dispatch_nv(nv, f)) return -1;
+        return f.iters;
+    }
+    if (method == 2) {
+        Rbicgstab f(kb);
+        if (dispatch_nv(nv, f)) return -1;
+        return f.iters;
+    }
+    return -1;
 }
 int ref_pbicgstab_amg_d(int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
                         const double *const *av, const int *const *prp, const int *const *pci,

@@ -50,6 +50,8 @@ def lib(kind, build=True):
     PP = C.POINTER(C.c_void_p)
     L.ref_pbicgstab_amg_d.argtypes = [ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, vp, vp,
                                       ci_, ci_, cd, cd, vp, ci_]
+    L.ref_krylov_d.argtypes = [ci_, ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, vp, vp,
+                               ci_, ci_, cd, cd, vp, ci_]
     _libs[kind] = L
     return L
 
@@ -83,14 +85,7 @@ def _ptrs(arrs):
     return (C.c_void_p * len(arrs))(*[a.ctypes.data if a is not None else None for a in arrs])
 
 
-def pbicgstab_amg(L, levels, B, blocks=None, max_iters=200, rel_tol=1e-8, relax=0.99, pre_it=1, post_it=1):
-    """AMG-PBiCGStab from x = 0 over `levels` (dicts with n, A, P, ncP as the
-    oracle's setup or the library's hierarchy export gives them); blocks[l]:
-    hybrid block row offsets of level l (default: one block per level, the
-    single-process sweep).  Returns (x, iterations, history)."""
-    nlev = len(levels)
-    if blocks is None:
-        blocks = [np.array([0, lv["n"]], np.int64) for lv in levels]
+def _hier_args(levels, blocks):
     nrows = np.array([lv["n"] for lv in levels], np.int64)
     R = [transpose(*lv["P"], lv["ncP"]) if lv.get("P") is not None else None for lv in levels]
     cols = []
@@ -99,18 +94,45 @@ def pbicgstab_amg(L, levels, B, blocks=None, max_iters=200, rel_tol=1e-8, relax=
         cols.append([np.ascontiguousarray(lv["P"][k]) if lv.get("P") is not None else None for lv in levels])
         cols.append([r[k] if r is not None else None for r in R])
     arp, prp, rrp, aci, pci, rci, av, pv, rv = cols
+    if blocks is None:
+        blocks = [np.array([0, lv["n"]], np.int64) for lv in levels]
     blocks = [np.ascontiguousarray(b, np.int64) for b in blocks]
     nb = np.array([len(b) - 1 for b in blocks], np.int32)
     PP = C.POINTER(C.c_void_p)
     tabs = [_ptrs(x) for x in (arp, aci, av, prp, pci, pv, rrp, rci, rv, blocks)]
     cast = [C.cast(t, PP) for t in tabs]
+    keep = (nrows, R, cols, blocks, nb, tabs)
+    return nrows, cast, nb, keep
+
+
+def pbicgstab_amg(L, levels, B, blocks=None, max_iters=200, rel_tol=1e-8, relax=0.99, pre_it=1, post_it=1):
+    """AMG-PBiCGStab from x = 0 over `levels` (dicts with n, A, P, ncP as the
+    oracle's setup or the library's hierarchy export gives them); blocks[l]:
+    hybrid block row offsets of level l (default: one block per level, the
+    single-process sweep).  Returns (x, iterations, history)."""
+    nrows, cast, nb, keep = _hier_args(levels, blocks)
     n, nv = B.shape
     B = np.ascontiguousarray(B, np.float64)
     x = np.zeros_like(B)
     h = np.zeros((max_iters + 2, nv))
-    it = L.ref_pbicgstab_amg_d(nlev, p(nrows), cast[0], cast[1], cast[2], cast[3], cast[4], cast[5], cast[6],
-                               cast[7], cast[8], p(nb), cast[9], relax, pre_it, post_it, p(B), p(x), nv,
-                               max_iters, 0.0, rel_tol, p(h), max_iters + 2)
+    it = L.ref_pbicgstab_amg_d(len(levels), p(nrows), *cast[:9], p(nb), cast[9], relax, pre_it, post_it, p(B),
+                               p(x), nv, max_iters, 0.0, rel_tol, p(h), max_iters + 2)
     if it < 0:
         raise ValueError("unsupported nv or hierarchy")
+    return x, it, h[: it + 1]
+
+
+def krylov(L, method, levels, B, blocks=None, max_iters=200, rel_tol=1e-8, relax=0.99):
+    """PCG (method "PCG") or RBiCGStab ("RBiCGStab") from x = 0, preconditioned
+    by one V-cycle over `levels` when it has two or more levels, else by the
+    identity (levels = [the operator's level]).  Returns (x, iterations, history)."""
+    nrows, cast, nb, keep = _hier_args(levels, blocks)
+    n, nv = B.shape
+    B = np.ascontiguousarray(B, np.float64)
+    x = np.zeros_like(B)
+    h = np.zeros((max_iters + 2, nv))
+    it = L.ref_krylov_d({"PCG": 1, "RBiCGStab": 2}[method], len(levels), p(nrows), *cast[:9], p(nb), cast[9],
+                        relax, 1, 1, p(B), p(x), nv, max_iters, 0.0, rel_tol, p(h), max_iters + 2)
+    if it < 0:
+        raise ValueError("unsupported nv or method")
     return x, it, h[: it + 1]

@@ -293,3 +293,28 @@ def test_amg_pbicgstab_solve_matches_reference_loops(libs, seq_dot, block_rows):
     assert itr == it and it > 0
     assert np.array_equal(h, hist)
     assert np.array_equal(x, xo)
+
+
+@pytest.mark.parametrize("method", ["PCG", "RBiCGStab"])
+@pytest.mark.parametrize("precond", [False, True])
+def test_pcg_and_rbicgstab_solves_match_reference_loops(libs, seq_dot, method, precond):
+    """PCG (pcg.inl) and RBiCGStab (rbicgstab.inl) in the reference's step
+    order over its compiled loops, with the identity or one AMG V-cycle as
+    the preconditioner, against the oracle's solvers in the reference's
+    inner-product order: same iterations, residual history and x, bit for bit
+    (27-point 14^3 system, NV = 4)."""
+    rp, ci, v = orc.gen27(14)
+    B = np.random.default_rng(31).uniform(-1, 1, (len(rp) - 1, 4))
+    if precond:
+        levels = orc.amg_setup(rp, ci, v, mg_coarsening_type=10, mg_interpolation_type=6,
+                               mg_strength_threshold=0.25, mg_max_levels=6, mg_coarse_matrix_size=100)
+        mg = orc.MG(levels)
+    else:
+        levels = [dict(n=len(rp) - 1, A=(rp, ci, v), P=None, ncP=0)]
+        mg = None
+    fn = orc.pcg if method == "PCG" else orc.rbicgstab
+    xo, it, hist, st, r0 = fn(rp, ci, v, B, np.zeros_like(B), mg, 500, 0.0, 1e-8)
+    x, itr, h = reference_loops.krylov(libs["contract"], method, levels, B, max_iters=500)
+    assert itr == it and it > 0
+    assert np.array_equal(h, hist)
+    assert np.array_equal(x, xo)
