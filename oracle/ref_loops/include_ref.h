@@ -7,6 +7,7 @@
 #include "blas/detail/blas.inl"
 #include "blas/detail/blas_ext.inl"
 #include "blas/detail/blas_wrapper.inl"
+#include "blas/detail/specific/blas_merged_jacobi.inl"
 #include "blas2/detail/csr_matvec.inl"
 #include "blas2/detail/csr_gs.inl"
 #include "blas2/detail/dense_matvec.inl"

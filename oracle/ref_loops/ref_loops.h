@@ -47,6 +47,12 @@ int ref_xdivy_z_d(int64_t n, int nv, const double *x, const double *y, double *z
 int ref_ax_y_d(int64_t n, int nv, const double *a, const double *x, double *y);       // blas.inl:30-85
 int ref_scal_d(int64_t n, int nv, const double *a, double *y);                        // blas.inl:155-219
 
+// Jacobi smoother, the no-check path of Jacobi::solve (jacobi.inl:91-100):
+// `sweeps` times r = A x, then blas_merged_jacobi.inl:32-90
+// (x += relax_k * invd_i * (b - r)).
+int ref_jacobi_d(int64_t n, const int *rp, const int *ci, const double *v, const double *invd,
+                 const double *b, double *x, const double *relax, int nv, int sweeps);
+
 // Gauss-Jordan inverse of a dense n x n matrix (row-major),
 // src/primitives/matrix/operations/inverse.inl:31-106 (the coarse-grid
 // Direct solver's setup)

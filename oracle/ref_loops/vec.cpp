@@ -358,6 +358,20 @@ struct Rbicgstab : KrylovBase {
     }
 };
 
+// Jacobi::solve's no-check path (jacobi.inl:91-100)
+struct JacobiRun {
+    int64_t n; const int *rp, *ci; const double *v, *invd, *b; double *x; const double *relax; int nv, sweeps;
+    template <int NV> void run() {
+        std::vector<double> r((size_t)n * NV, 0.0);
+        vector X = block(x, n, NV), B = block(b, n, NV), R = block(r.data(), n, NV), D = block(invd, n, 1),
+               W = scalars(relax, NV);
+        for (int k = 0; k < sweeps; ++k) {
+            ref_csr_ax_y_d(n, rp, ci, v, x, r.data(), NV);
+            XAMG::blas::specific::merged_jacobi<double, NV>(X, B, D, R, W);
+        }
+    }
+};
+
 }  // namespace
 
 extern "C" {
@@ -383,6 +397,11 @@ int ref_ax_y_d(int64_t n, int nv, const double *a, const double *x, double *y) {
 }
 int ref_scal_d(int64_t n, int nv, const double *a, double *y) {
     return run_blas(Blas{6, n, nv, a, nullptr, nullptr, nullptr, nullptr, y});
+}
+int ref_jacobi_d(int64_t n, const int *rp, const int *ci, const double *v, const double *invd,
+                 const double *b, double *x, const double *relax, int nv, int sweeps) {
+    JacobiRun f{n, rp, ci, v, invd, b, x, relax, nv, sweeps};
+    return dispatch_nv(nv, f);
 }
 int ref_dense_inverse_d(int64_t n, const double *a, double *ainv) {
     XAMG::matrix::dense_matrix<double> m(XAMG::mem::CORE), mi(XAMG::mem::CORE);

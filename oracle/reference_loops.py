@@ -47,6 +47,7 @@ def lib(kind, build=True):
     L.ref_scal_d.argtypes = [i64, ci_, vp, vp]
     L.ref_bicgstab_d.argtypes = [i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, vp, ci_]
     L.ref_dense_inverse_d.argtypes = [i64, vp, vp]
+    L.ref_jacobi_d.argtypes = [i64, vp, vp, vp, vp, vp, vp, vp, ci_, ci_]
     PP = C.POINTER(C.c_void_p)
     L.ref_pbicgstab_amg_d.argtypes = [ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, vp, vp,
                                       ci_, ci_, cd, cd, vp, ci_]

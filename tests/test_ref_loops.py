@@ -136,6 +136,30 @@ def test_hybrid_gauss_seidel_matches_reference_loops(libs, nv, nblocks):
 
 
 @pytest.mark.parametrize("nv", [1, 4, 16])
+def test_jacobi_matches_reference_loops(libs, nv):
+    """Two Jacobi sweeps (the smoother's no-check path, merged update
+    x += relax*invd*(b - Ax)): the oracle fuses the update, as the Haswell
+    build compiles the reference's loop; the generic build rounds the product
+    apart (within a rounding per sweep)."""
+    rng = np.random.default_rng(70 + nv)
+    for name, (rp, ci, v) in operators():
+        n = len(rp) - 1
+        invd = inv_diag(rp, ci, v)
+        b = rng.uniform(-1, 1, (n, nv))
+        x0 = rng.uniform(-1, 1, (n, nv))
+        relax = rng.uniform(0.5, 1.0, nv)
+        xo = x0.copy()
+        for _ in range(2):
+            orc.jacobi(rp, ci, v, invd, b, xo, relax)
+        x = x0.copy()
+        assert libs["haswell"].ref_jacobi_d(n, p(rp), p(ci), p(v), p(invd), p(b), p(x), p(relax), nv, 2) == 0
+        assert np.array_equal(x, xo), name
+        x = x0.copy()
+        libs["generic"].ref_jacobi_d(n, p(rp), p(ci), p(v), p(invd), p(b), p(x), p(relax), nv, 2)
+        np.testing.assert_allclose(x, xo, rtol=1e-12, atol=1e-14 * np.abs(xo).max(), err_msg=name)
+
+
+@pytest.mark.parametrize("nv", [1, 4, 16])
 def test_dense_product_matches_reference_loops(libs, nv):
     rng = np.random.default_rng(40 + nv)
     nc = 57
