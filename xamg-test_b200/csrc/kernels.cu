@@ -1116,7 +1116,7 @@ __global__ void __launch_bounds__(256) k_dot2(i64 nch, const double *__restrict_
 // other chunk partials, so the reduction stage (k_dot2, k_dot2_epi: +0 plus
 // the chunk partials in order, then a pairwise fold with zeros) returns it
 // unchanged.
-constexpr int SEQ_TILE = 128;
+constexpr int SEQ_TILE = 256;
 // products a_i * b_i (rounded) of rows [t*SEQ_TILE, ...) into buf, by the
 // block's threads 32..255
 template <class TI, int NV>
@@ -1156,7 +1156,16 @@ __global__ void __launch_bounds__(256) k_dot_seq(i64 n, i64 nch, int nd, DotPair
             if (t + 1 < ntiles) seq_fill<TI, NV>(a, b, n, t + 1, prod + ((t + 1) & 1) * (SEQ_TILE * NV));
         } else if (tid < NV) {
             const int rows = (int)(n - t * SEQ_TILE < SEQ_TILE ? n - t * SEQ_TILE : SEQ_TILE);
-            for (int r = 0; r < rows; ++r) s = dadd(s, cur[r * NV + tid]);
+            int r = 0;
+            // eight products read ahead of their adds (same order)
+            for (; r + 8 <= rows; r += 8) {
+                double q[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) q[e] = cur[(r + e) * NV + tid];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) s = dadd(s, q[e]);
+            }
+            for (; r < rows; ++r) s = dadd(s, cur[r * NV + tid]);
         }
         __syncthreads();
     }
@@ -1187,7 +1196,7 @@ static void dots_t(i64 n, int nd, const void *const *a, const void *const *b, do
         // one block per pair plus blocks that zero the other chunk partials
         const unsigned zb = (unsigned)std::min<i64>(4 * 148, std::max<i64>(1, (nd * NV * (nch - 1) + 255) / 256));
         note_launch(reduce ? 2 : 1);
-        const size_t smem = sizeof(double) * 2 * SEQ_TILE * NV;  // 64 KB at NV = 32
+        const size_t smem = sizeof(double) * 2 * SEQ_TILE * NV;  // 128 KB at NV = 32
         cudaFuncSetAttribute(k_dot_seq<TI, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_dot_seq<TI, NV><<<(unsigned)nd + zb, 256, smem, s>>>(n, nch, nd, pr, part);
         if (reduce) k_dot2<<<nd * NV, 256, 0, s>>>(nch, part, out);
