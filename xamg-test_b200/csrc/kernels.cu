@@ -1124,8 +1124,18 @@ __device__ __forceinline__ void seq_fill(const TI *__restrict__ a, const TI *__r
                                          double *buf) {
     const i64 r0 = t * SEQ_TILE;
     const int cnt = (int)(n - r0 < SEQ_TILE ? n - r0 : SEQ_TILE) * NV;
-    for (int q = (int)threadIdx.x - 32; q < cnt; q += 224)
-        buf[q] = dmul((double)a[r0 * NV + q], (double)b[r0 * NV + q]);
+    const TI *__restrict__ at = a + r0 * NV;
+    const TI *__restrict__ bt = b + r0 * NV;
+    int q = (int)threadIdx.x - 32;
+    // eight loads of each operand in flight before the products are stored
+    for (; q + 7 * 224 < cnt; q += 8 * 224) {
+        double xa[8], xb[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) { xa[e] = (double)at[q + e * 224]; xb[e] = (double)bt[q + e * 224]; }
+#pragma unroll
+        for (int e = 0; e < 8; ++e) buf[q + e * 224] = dmul(xa[e], xb[e]);
+    }
+    for (; q < cnt; q += 224) buf[q] = dmul((double)at[q], (double)bt[q]);
 }
 template <class TI, int NV>
 __global__ void __launch_bounds__(256) k_dot_seq(i64 n, i64 nch, int nd, DotPairs<TI> pr,
