@@ -18,8 +18,8 @@ Three libraries, the same entry points (oracle/ref_loops/ref_loops.h):
       -ffast-math (which lets the compiler reorder sums at will): a product
       feeding a sum becomes one fused multiply-add;
   libxamg_ref_loops_contract.so  the row loops (sparse and dense products,
-      Gauss-Seidel) as in the Haswell build, the BLAS-1 loops as in the
-      generic build: the arithmetic contract the oracle and the GPU kernels
+      Gauss-Seidel, the Jacobi update) as in the Haswell build, the BLAS-1
+      loops as in the generic build: the arithmetic contract the oracle and the GPU kernels
       follow (fused row sums, literal vector updates), assembled from the two.
 """
 import os
@@ -62,10 +62,11 @@ def build():
             built.append(lib)
             continue
         objs = []
-        for name, flags in (("rows", rows_flags), ("vec", vec_flags)):
+        for name, flags in (("rows", rows_flags), ("smooth", rows_flags), ("vec", vec_flags)):
             obj = os.path.join(OUT, "ref_%s_%s.o" % (name, kind))
-            subprocess.run(["g++", *flags, "-I", SRC, "-I", ref, "-c", os.path.join(SRC, name + ".cpp"),
-                            "-o", obj], check=True)
+            # XAMG renamed per unit: no template instance is shared between units
+            subprocess.run(["g++", *flags, "-DXAMG=XAMG_" + name, "-I", SRC, "-I", ref, "-c",
+                            os.path.join(SRC, name + ".cpp"), "-o", obj], check=True)
             objs.append(obj)
         subprocess.run(["g++", "-shared", "-o", lib, *objs], check=True)
         for o in objs:

@@ -38,4 +38,7 @@ template <class T> vector block(const T *p, int64_t n, int nv) {
     return v;
 }
 
+// per-column scalars: a vector of one row and nv columns
+template <class T> vector scalars(const T *p, int nv) { return block<T>(p, 1, nv); }
+
 }  // namespace refloops

@@ -81,14 +81,16 @@ int ref_pbicgstab_amg_d(int nlev, const int64_t *nrows, const int *const *arp, c
                         int pre_it, int post_it, const double *b, double *x, int nv, int max_iters,
                         double abs_tol, double rel_tol, double *hist, int hist_cap);
 
-// PCG (method 1, pcg.inl:48-160) or RBiCGStab (method 2, rbicgstab.inl:48-225)
-// in the reference's step order, preconditioned by the V-cycle above when
-// nlev >= 2, else by the identity (M^{-1} r = r; nrows[0], arp[0], aci[0],
-// av[0] give the operator).  Returns the iteration count, -1 on bad input.
+// (P)BiCGStab (method 0, as above), PCG (method 1, pcg.inl:48-160) or
+// RBiCGStab (method 2, rbicgstab.inl:48-225) in the reference's step order,
+// preconditioned by the V-cycle above when nlev >= 2 (smoother 0: HSGS,
+// 1: Jacobi, pre_it / post_it sweeps), else by the identity (M^{-1} r = r;
+// nrows[0], arp[0], aci[0], av[0] give the operator; for method 0 no
+// preconditioner at all).  Returns the iteration count, -1 on bad input.
 int ref_krylov_d(int method, int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
                  const double *const *av, const int *const *prp, const int *const *pci,
                  const double *const *pv, const int *const *rrp, const int *const *rci,
                  const double *const *rv, const int *nb, const int64_t *const *bp, double relax, int pre_it,
-                 int post_it, const double *b, double *x, int nv, int max_iters, double abs_tol,
+                 int post_it, int smoother, const double *b, double *x, int nv, int max_iters, double abs_tol,
                  double rel_tol, double *hist, int hist_cap);
 }

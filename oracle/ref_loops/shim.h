@@ -12,6 +12,11 @@
 // single-process configuration.  The MPI, shared-memory, logging and
 // performance-counter hooks the files name are inert.
 //
+// Each translation unit of a library is compiled with XAMG defined to a name
+// of its own (build_ref_loops.py), so that the reference's inline templates
+// instantiated under different floating-point flags cannot be merged by the
+// linker; units talk to each other only through the C entry points.
+//
 // Member names and enumerators follow the reference's headers
 // (src/primitives/vector/vector.h:45-62, 221; src/xamg_types.h:90-98;
 // src/primitives/matrix/csr_matrix.h:47-120) because the included loop files
@@ -256,5 +261,7 @@ inline void axpby(const T a, const vector::vector &x, const T b, vector::vector 
 
 }  // namespace XAMG
 
-extern XAMG::perf_info perf;
-extern ID id;
+// one of each per translation unit (internal linkage): the units of one
+// library are compiled with different flags and share no symbol
+static XAMG::perf_info perf;
+static ID id;

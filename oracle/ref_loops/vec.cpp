@@ -7,16 +7,10 @@
 #include "include_ref.h"
 #include "ref_loops.h"
 
-XAMG::perf_info perf;
-ID id;
-
 using namespace refloops;
 namespace blas = XAMG::blas;
 
 namespace {
-
-// per-column scalars: a vector of one row and nv columns
-template <class T> vector scalars(const T *p, int nv) { return block<T>(p, 1, nv); }
 
 struct Blas {
     int op;
@@ -78,6 +72,7 @@ struct Hier {
     const int *const *rrp; const int *const *rci; const double *const *rv;
     const int *nb; const int64_t *const *bp;
     double relax; int pre_it, post_it;
+    int smoother;  // 0: HSGS (hsgs.inl), 1: Jacobi (jacobi.inl, no-check path)
     std::vector<std::vector<double>> invd;
     std::vector<double> ainv;
     void init() {
@@ -97,8 +92,13 @@ struct Hier {
     }
     // HSGS::solve (hsgs.inl:57-91) as a smoother: relax_conv = relax, then
     // `it` calls of blas2::SGS
+    // or Jacobi::solve's no-check path: `it` sweeps
     void smooth(int l, const double *b, double *x, int nv, int it) const {
         std::vector<double> rl(nv, relax);
+        if (smoother == 1) {
+            ref_jacobi_d(nrows[l], arp[l], aci[l], av[l], invd[l].data(), b, x, rl.data(), nv, it);
+            return;
+        }
         for (int k = 0; k < it; ++k)
             ref_hsgs_d(nrows[l], arp[l], aci[l], av[l], invd[l].data(), b, x, rl.data(), nv, nb[l], bp[l]);
     }
@@ -358,20 +358,6 @@ struct Rbicgstab : KrylovBase {
     }
 };
 
-// Jacobi::solve's no-check path (jacobi.inl:91-100)
-struct JacobiRun {
-    int64_t n; const int *rp, *ci; const double *v, *invd, *b; double *x; const double *relax; int nv, sweeps;
-    template <int NV> void run() {
-        std::vector<double> r((size_t)n * NV, 0.0);
-        vector X = block(x, n, NV), B = block(b, n, NV), R = block(r.data(), n, NV), D = block(invd, n, 1),
-               W = scalars(relax, NV);
-        for (int k = 0; k < sweeps; ++k) {
-            ref_csr_ax_y_d(n, rp, ci, v, x, r.data(), NV);
-            XAMG::blas::specific::merged_jacobi<double, NV>(X, B, D, R, W);
-        }
-    }
-};
-
 }  // namespace
 
 extern "C" {
@@ -398,11 +384,6 @@ int ref_ax_y_d(int64_t n, int nv, const double *a, const double *x, double *y) {
 int ref_scal_d(int64_t n, int nv, const double *a, double *y) {
     return run_blas(Blas{6, n, nv, a, nullptr, nullptr, nullptr, nullptr, y});
 }
-int ref_jacobi_d(int64_t n, const int *rp, const int *ci, const double *v, const double *invd,
-                 const double *b, double *x, const double *relax, int nv, int sweeps) {
-    JacobiRun f{n, rp, ci, v, invd, b, x, relax, nv, sweeps};
-    return dispatch_nv(nv, f);
-}
 int ref_dense_inverse_d(int64_t n, const double *a, double *ainv) {
     XAMG::matrix::dense_matrix<double> m(XAMG::mem::CORE), mi(XAMG::mem::CORE);
     m.nrows = m.block_nrows = (uint64_t)n;
@@ -423,9 +404,10 @@ static Hier *make_hier(int nlev, const int64_t *nrows, const int *const *arp, co
                        const double *const *av, const int *const *prp, const int *const *pci,
                        const double *const *pv, const int *const *rrp, const int *const *rci,
                        const double *const *rv, const int *nb, const int64_t *const *bp, double relax,
-                       int pre_it, int post_it) {
+                       int pre_it, int post_it, int smoother) {
     if (nlev < 2) return nullptr;
-    Hier *h = new Hier{nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax, pre_it, post_it, {}, {}};
+    Hier *h = new Hier{nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax, pre_it, post_it,
+                       smoother, {}, {}};
     h->init();
     return h;
 }
@@ -433,12 +415,17 @@ int ref_krylov_d(int method, int nlev, const int64_t *nrows, const int *const *a
                  const double *const *av, const int *const *prp, const int *const *pci,
                  const double *const *pv, const int *const *rrp, const int *const *rci,
                  const double *const *rv, const int *nb, const int64_t *const *bp, double relax, int pre_it,
-                 int post_it, const double *b, double *x, int nv, int max_iters, double abs_tol,
+                 int post_it, int smoother, const double *b, double *x, int nv, int max_iters, double abs_tol,
                  double rel_tol, double *hist, int hist_cap) {
     std::unique_ptr<Hier> h(make_hier(nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax,
-                                      pre_it, post_it));
+                                      pre_it, post_it, smoother));
     KrylovBase kb{nrows[0], arp[0], aci[0], av[0], b, x, nv, max_iters, abs_tol, rel_tol, hist, hist_cap,
                   h.get(), 0};
+    if (method == 0) {
+        Bicgstab f{kb.n, kb.rp, kb.ci, kb.v, b, x, nv, max_iters, abs_tol, rel_tol, hist, hist_cap, h.get(), 0};
+        if (dispatch_nv(nv, f)) return -1;
+        return f.iters;
+    }
     if (method == 1) {
         Pcg f(kb);
         if (dispatch_nv(nv, f)) return -1;
@@ -458,7 +445,7 @@ int ref_pbicgstab_amg_d(int nlev, const int64_t *nrows, const int *const *arp, c
                         int pre_it, int post_it, const double *b, double *x, int nv, int max_iters,
                         double abs_tol, double rel_tol, double *hist, int hist_cap) {
     if (nlev < 2) return -1;
-    Hier h{nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax, pre_it, post_it, {}, {}};
+    Hier h{nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax, pre_it, post_it, 0, {}, {}};
     h.init();
     Bicgstab f{nrows[0], arp[0], aci[0], av[0], b, x, nv, max_iters, abs_tol, rel_tol, hist, hist_cap, &h, 0};
     if (dispatch_nv(nv, f)) return -1;

@@ -51,8 +51,8 @@ def lib(kind, build=True):
     PP = C.POINTER(C.c_void_p)
     L.ref_pbicgstab_amg_d.argtypes = [ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, vp, vp,
                                       ci_, ci_, cd, cd, vp, ci_]
-    L.ref_krylov_d.argtypes = [ci_, ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, vp, vp,
-                               ci_, ci_, cd, cd, vp, ci_]
+    L.ref_krylov_d.argtypes = [ci_, ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, ci_, vp,
+                               vp, ci_, ci_, cd, cd, vp, ci_]
     _libs[kind] = L
     return L
 
@@ -123,17 +123,21 @@ def pbicgstab_amg(L, levels, B, blocks=None, max_iters=200, rel_tol=1e-8, relax=
     return x, it, h[: it + 1]
 
 
-def krylov(L, method, levels, B, blocks=None, max_iters=200, rel_tol=1e-8, relax=0.99):
-    """PCG (method "PCG") or RBiCGStab ("RBiCGStab") from x = 0, preconditioned
-    by one V-cycle over `levels` when it has two or more levels, else by the
-    identity (levels = [the operator's level]).  Returns (x, iterations, history)."""
+def krylov(L, method, levels, B, blocks=None, max_iters=200, rel_tol=1e-8, relax=0.99, smoother="HSGS",
+           sweeps=1):
+    """PBiCGStab ("PBiCGStab"), PCG ("PCG") or RBiCGStab ("RBiCGStab") from
+    x = 0, preconditioned by one V-cycle over `levels` (HSGS or Jacobi
+    smoothing, `sweeps` before and after) when it has two or more levels, else
+    by the identity (levels = [the operator's level]).  Returns (x,
+    iterations, history)."""
     nrows, cast, nb, keep = _hier_args(levels, blocks)
     n, nv = B.shape
     B = np.ascontiguousarray(B, np.float64)
     x = np.zeros_like(B)
     h = np.zeros((max_iters + 2, nv))
-    it = L.ref_krylov_d({"PCG": 1, "RBiCGStab": 2}[method], len(levels), p(nrows), *cast[:9], p(nb), cast[9],
-                        relax, 1, 1, p(B), p(x), nv, max_iters, 0.0, rel_tol, p(h), max_iters + 2)
+    it = L.ref_krylov_d({"PBiCGStab": 0, "PCG": 1, "RBiCGStab": 2}[method], len(levels), p(nrows), *cast[:9],
+                        p(nb), cast[9], relax, sweeps, sweeps, {"HSGS": 0, "Jacobi": 1}[smoother], p(B), p(x), nv,
+                        max_iters, 0.0, rel_tol, p(h), max_iters + 2)
     if it < 0:
         raise ValueError("unsupported nv or method")
     return x, it, h[: it + 1]

@@ -342,3 +342,19 @@ def test_pcg_and_rbicgstab_solves_match_reference_loops(libs, seq_dot, method, p
     assert itr == it and it > 0
     assert np.array_equal(h, hist)
     assert np.array_equal(x, xo)
+
+
+def test_amg_pbicgstab_jacobi_smoothing_matches_reference_loops(libs, seq_dot):
+    """AMG-PBiCGStab with two Jacobi sweeps before and after (the no-check
+    path of jacobi.inl with the merged update) on a 27-point 16^3 system,
+    NV = 4, bit for bit against the oracle on the same hierarchy."""
+    rp, ci, v = orc.gen27(16)
+    levels = orc.amg_setup(rp, ci, v, mg_coarsening_type=10, mg_interpolation_type=6,
+                           mg_strength_threshold=0.25, mg_max_levels=6, mg_coarse_matrix_size=100)
+    B = np.random.default_rng(2025).uniform(-1, 1, (len(rp) - 1, 4))
+    mg = orc.MG(levels, pre=(orc.SM_JACOBI, 2, 0.99), post=(orc.SM_JACOBI, 2, 0.99))
+    xo, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg, 200, 0.0, 1e-8)
+    x, itr, h = reference_loops.krylov(libs["contract"], "PBiCGStab", levels, B, smoother="Jacobi", sweeps=2)
+    assert itr == it and it > 0
+    assert np.array_equal(h, hist)
+    assert np.array_equal(x, xo)
