@@ -1,6 +1,9 @@
 """Compile the reference's own loop files (src/blas/detail/blas.inl,
-blas_ext.inl, blas_wrapper.inl, src/blas2/detail/csr_matvec.inl, csr_gs.inl,
-dense_matvec.inl, src/primitives/matrix/operations/inverse.inl) unchanged, where they lie under the reference tree (default
+blas_ext.inl, blas_wrapper.inl, specific/blas_merged_jacobi.inl,
+src/blas2/detail/csr_matvec.inl, csr_gs.inl, dense_matvec.inl,
+src/primitives/matrix/operations/inverse.inl, src/misc/rand.h) and its
+channel-with-cube generator (examples/common/generator/channel_with_cube.inl,
+lame.inl) unchanged, where they lie under the reference tree (default
 /root/reference, or $XAMG_REFERENCE_ROOT), into CPU libraries under
 oracle/_ref/ that the tests use to check the oracle.  Nothing is copied: the
 stand-in types of oracle/ref_loops/shim.h replace the reference's runtime
@@ -54,7 +57,8 @@ def build():
     if not os.path.isdir(os.path.join(ref, "blas2", "detail")):
         return []
     os.makedirs(OUT, exist_ok=True)
-    deps = [os.path.join(SRC, f) for f in sorted(os.listdir(SRC))] + [os.path.abspath(__file__)]
+    deps = [os.path.join(d, f) for d in (SRC, os.path.join(SRC, "stub")) for f in sorted(os.listdir(d))
+            if os.path.isfile(os.path.join(d, f))] + [os.path.abspath(__file__)]
     built = []
     for kind, (rows_flags, vec_flags) in LIBS.items():
         lib = library(kind)
@@ -62,10 +66,13 @@ def build():
             built.append(lib)
             continue
         objs = []
-        for name, flags in (("rows", rows_flags), ("smooth", rows_flags), ("vec", vec_flags)):
+        for name, flags in (("rows", rows_flags), ("smooth", rows_flags), ("vec", vec_flags),
+                            ("gen", GENERIC)):
             obj = os.path.join(OUT, "ref_%s_%s.o" % (name, kind))
-            # XAMG renamed per unit: no template instance is shared between units
-            subprocess.run(["g++", *flags, "-DXAMG=XAMG_" + name, "-I", SRC, "-I", ref, "-c",
+            # XAMG renamed per unit: no template instance is shared between units;
+            # ref_loops/stub comes first so that its xamg_types.h stands in
+            subprocess.run(["g++", *flags, "-DXAMG=XAMG_" + name, "-I", os.path.join(SRC, "stub"), "-I", SRC,
+                            "-I", ref, "-I", os.path.join(os.path.dirname(ref), "examples", "common"), "-c",
                             os.path.join(SRC, name + ".cpp"), "-o", obj], check=True)
             objs.append(obj)
         subprocess.run(["g++", "-shared", "-o", lib, *objs], check=True)

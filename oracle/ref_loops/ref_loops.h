@@ -34,6 +34,14 @@ int ref_hsgs_f(int64_t n, const int *rp, const int *ci, const float *v, const fl
 int ref_dense_ax_y_d(int64_t nr, int64_t nc, const double *m, const double *x, double *y, int nv);
 int ref_dense_ax_y_f(int64_t nr, int64_t nc, const float *m, const float *x, float *y, int nv);
 
+// The reference's channel-with-cube generator
+// (examples/common/generator/channel_with_cube.inl:40-245, grid scale 1-3,
+// constant or divergence right-hand sides, one process): returns the row
+// count and *nnz; copies the CSR arrays (entries in the generator's own
+// order) and the n x nv right-hand sides into every non-null output.
+int64_t ref_channel_cube_d(int scale, int const_rhs, int nv, int64_t *nnz, int *rp, int *ci, double *v,
+                           double *b);
+
 // BLAS-1 (src/blas/detail/blas.inl, blas_ext.inl) over n rows; a, b, c are
 // per-column scalars (nv values).
 int ref_dot_d(int64_t n, int nv, const double *x, const double *y, double *res);      // blas.inl:521-589

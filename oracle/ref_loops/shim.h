@@ -34,6 +34,7 @@
 #include <vector>
 
 #include "xamg_macros.h"  // the reference's own vectorisation / restrict macros
+#include "misc/rand.h"     // the reference's pseudo-random stream (xorshift32 + LCG)
 
 typedef float float32_t;
 typedef double float64_t;
@@ -47,6 +48,7 @@ typedef double float64_t;
 // of its node and NUMA domain.
 struct ID {
     int gl_proc = 0;
+    int gl_nprocs = 1;
     int nd_numa = 0;
     bool master_process() const { return true; }
     bool node_master_process() const { return true; }
@@ -83,9 +85,6 @@ template <typename T> inline void allreduce_bxor(const T *in, T *out, int n) {
     for (int i = 0; i < n; ++i) out[i] = in[i];
 }
 }  // namespace mpi
-
-template <typename T> inline T true_rand() { return T(0.5); }
-template <typename T> inline T pseudo_rand(uint64_t) { return T(0.5); }
 
 namespace vector {
 
@@ -125,6 +124,7 @@ struct vector {
         if_initialized = false;
         return (T *)ptr;
     }
+    template <typename T> void alloc(uint64_t n, uint16_t w) { alloc_and_get_aligned_ptr<T>(n, w); }
     template <typename T> T *get_aligned_ptr(int = -1) const { return (T *)ptr; }
     template <typename T> void get_core_range(uint64_t &core_size, uint64_t &core_offset) const {
         core_size = size;
@@ -162,6 +162,24 @@ struct csr_matrix {
     bool if_empty = false;
     bool if_indexed = false;
     const vector::vector &get_row_ind_vector() const { return row_ind; }
+    // storage for nrows rows and `nonzeros` entries (the generators fill it)
+    void alloc() {
+        row.alloc_and_get_aligned_ptr<I1>(nrows + 1, 1);
+        col.alloc_and_get_aligned_ptr<I2>(nonzeros, 1);
+        val.alloc_and_get_aligned_ptr<F>(nonzeros, 1);
+    }
+    // row nrow's entries in the given order (rows filled in sequence)
+    void upload_row(uint64_t nrow, const std::vector<uint64_t> &c, const std::vector<F> &v, uint32_t size) {
+        I1 *rp = row.template get_aligned_ptr<I1>();
+        I2 *cp = col.template get_aligned_ptr<I2>();
+        F *vp = val.template get_aligned_ptr<F>();
+        if (!nrow) rp[0] = 0;
+        for (uint32_t i = 0; i < size; ++i) {
+            cp[rp[nrow] + i] = (I2)c[i];
+            vp[rp[nrow] + i] = v[i];
+        }
+        rp[nrow + 1] = rp[nrow] + size;
+    }
 };
 
 template <typename F> struct dense_matrix {

@@ -48,6 +48,8 @@ def lib(kind, build=True):
     L.ref_bicgstab_d.argtypes = [i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, vp, ci_]
     L.ref_dense_inverse_d.argtypes = [i64, vp, vp]
     L.ref_jacobi_d.argtypes = [i64, vp, vp, vp, vp, vp, vp, vp, ci_, ci_]
+    L.ref_channel_cube_d.restype = C.c_int64
+    L.ref_channel_cube_d.argtypes = [ci_, ci_, ci_, vp, vp, vp, vp, vp]
     PP = C.POINTER(C.c_void_p)
     L.ref_pbicgstab_amg_d.argtypes = [ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, vp, vp,
                                       ci_, ci_, cd, cd, vp, ci_]
@@ -141,3 +143,17 @@ def krylov(L, method, levels, B, blocks=None, max_iters=200, rel_tol=1e-8, relax
     if it < 0:
         raise ValueError("unsupported nv or method")
     return x, it, h[: it + 1]
+
+
+def channel_cube(L, scale, nv, const_rhs=False):
+    """The reference's channel-with-cube problem: (rp, ci, v, B)."""
+    nnz = np.zeros(1, np.int64)
+    n = L.ref_channel_cube_d(scale, int(const_rhs), nv, p(nnz), None, None, None, None)
+    if n < 0:
+        raise ValueError("unsupported scale or nv")
+    rp = np.zeros(n + 1, np.int32)
+    ci = np.zeros(int(nnz[0]), np.int32)
+    v = np.zeros(int(nnz[0]))
+    B = np.zeros((n, nv))
+    L.ref_channel_cube_d(scale, int(const_rhs), nv, None, p(rp), p(ci), p(v), p(B))
+    return rp, ci, v, B

@@ -4,13 +4,16 @@
 CPU: the properties the generator's construction fixes (sizes, the solid
 block's identity rows, symmetry of the finite-volume couplings up to rounding
 except the identity last row, zero row sums of interior fluid rows, the
-right-hand-side forms).  GPU: the reference's own solver configuration for this
+right-hand-side forms), and bit for bit against the reference's own generator
+compiled unchanged (oracle/build_ref_loops.py).  GPU: the reference's own
+solver configuration for this
 case (examples/test/yaml/multi_node/config-channel-cube1.yaml: PBiCGStab, 20
 iterations, aggressive-coarsening AMG with HSGS) reduces the residual."""
 import numpy as np
 import pytest
 import scipy.sparse as sp
 
+import reference_loops
 import xamg
 
 
@@ -89,3 +92,19 @@ def test_channel_cube_reference_config_converges(gpu, channel1):
     rel = np.linalg.norm(B1 - As @ X) / np.linalg.norm(B1)
     assert rel < 1e-6, rel
     assert s.num_levels() >= 4
+
+
+def test_channel_cube_matches_reference_generator(channel1):
+    """The reference's generator (channel_with_cube.inl + lame.inl, its
+    pseudo-random velocity stream from misc/rand.h) compiled unchanged: grid
+    scale 1, divergence right-hand sides, NV = 2.  Row pointers, entry order,
+    values and right-hand sides are identical bit for bit."""
+    L = reference_loops.lib("generic")
+    if L is None:
+        pytest.skip("reference loop library not built (reference tree absent)")
+    m, (rp, ci, v), B = channel1
+    rrp, rci, rv, rB = reference_loops.channel_cube(L, 1, 2, const_rhs=False)
+    assert np.array_equal(rp, rrp)
+    assert np.array_equal(ci, rci)
+    assert np.array_equal(v, rv)
+    assert np.array_equal(B, rB)
