@@ -1,12 +1,14 @@
-// The reference's channel-with-cube test problem generator
-// (examples/common/generator/channel_with_cube.inl + lame.inl), compiled
-// unchanged with the release flags: the matrix rows in its own entry order
-// and the right-hand sides of its constant and divergence forms.
+// The reference's test problem generators, compiled unchanged with the
+// release flags: the channel with a cube
+// (examples/common/generator/channel_with_cube.inl + lame.inl; the matrix
+// rows in its own entry order and the right-hand sides of its constant and
+// divergence forms) and the cube configurations 0-4 (cube.inl).
 #include <cstring>
 
 #include "include_ref.h"
 #include "ref_loops.h"
 #include "generator/channel_with_cube.inl"
+#include "generator/cube.inl"
 
 using namespace refloops;
 
@@ -18,6 +20,16 @@ struct Channel {
     vector x, b;
     template <int NV> void run() {
         generate_channel_with_cube<double, int, int, int, int, NV>(m, x, b, (uint8_t)scale, const_rhs != 0);
+    }
+};
+
+struct Cube {
+    int64_t nx, ny, nz; int config;
+    XAMG::matrix::csr_matrix<double, int, int, int, int> m;
+    vector x, b;
+    template <int NV> void run() {
+        generate_cube<double, int, int, int, int, NV>(m, x, b, (uint64_t)nx, (uint64_t)ny, (uint64_t)nz,
+                                                      (size_t)config);
     }
 };
 
@@ -51,6 +63,18 @@ int64_t ref_channel_cube_d(int scale, int const_rhs, int nv, int64_t *nnz, int *
         delete g_last;
         g_last = nullptr;
     }
+    return n;
+}
+int64_t ref_cube_d(int64_t nx, int64_t ny, int64_t nz, int config, int64_t *nnz, int *rp, int *ci,
+                   double *v) {
+    if (config < 0 || config > 4 || nx < 1 || ny < 1 || nz < 1) return -1;
+    Cube f{nx, ny, nz, config, {}, {}, {}};
+    f.run<1>();
+    const int64_t n = (int64_t)f.m.nrows, z = (int64_t)f.m.nonzeros;
+    if (nnz) *nnz = z;
+    if (rp) std::memcpy(rp, f.m.row.get_aligned_ptr<int>(), sizeof(int) * (size_t)(n + 1));
+    if (ci) std::memcpy(ci, f.m.col.get_aligned_ptr<int>(), sizeof(int) * (size_t)z);
+    if (v) std::memcpy(v, f.m.val.get_aligned_ptr<double>(), sizeof(double) * (size_t)z);
     return n;
 }
 }

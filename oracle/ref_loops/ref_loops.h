@@ -42,6 +42,12 @@ int ref_dense_ax_y_f(int64_t nr, int64_t nc, const float *m, const float *x, flo
 int64_t ref_channel_cube_d(int scale, int const_rhs, int nv, int64_t *nnz, int *rp, int *ci, double *v,
                            double *b);
 
+// The reference's cube generator (examples/common/generator/cube.inl:71-225,
+// configurations 0-4, one process): row count, *nnz and, into non-null
+// outputs, the CSR arrays (diagonal first, then its neighbour order).
+int64_t ref_cube_d(int64_t nx, int64_t ny, int64_t nz, int config, int64_t *nnz, int *rp, int *ci,
+                   double *v);
+
 // BLAS-1 (src/blas/detail/blas.inl, blas_ext.inl) over n rows; a, b, c are
 // per-column scalars (nv values).
 int ref_dot_d(int64_t n, int nv, const double *x, const double *y, double *res);      // blas.inl:521-589

@@ -50,6 +50,8 @@ def lib(kind, build=True):
     L.ref_jacobi_d.argtypes = [i64, vp, vp, vp, vp, vp, vp, vp, ci_, ci_]
     L.ref_channel_cube_d.restype = C.c_int64
     L.ref_channel_cube_d.argtypes = [ci_, ci_, ci_, vp, vp, vp, vp, vp]
+    L.ref_cube_d.restype = C.c_int64
+    L.ref_cube_d.argtypes = [i64, i64, i64, ci_, vp, vp, vp, vp]
     PP = C.POINTER(C.c_void_p)
     L.ref_pbicgstab_amg_d.argtypes = [ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, vp, vp,
                                       ci_, ci_, cd, cd, vp, ci_]
@@ -157,3 +159,16 @@ def channel_cube(L, scale, nv, const_rhs=False):
     B = np.zeros((n, nv))
     L.ref_channel_cube_d(scale, int(const_rhs), nv, None, p(rp), p(ci), p(v), p(B))
     return rp, ci, v, B
+
+
+def cube(L, nx, ny, nz, config=0):
+    """The reference's cube generator (configurations 0-4): (rp, ci, v)."""
+    nnz = np.zeros(1, np.int64)
+    n = L.ref_cube_d(nx, ny, nz, config, p(nnz), None, None, None)
+    if n < 0:
+        raise ValueError("unsupported configuration")
+    rp = np.zeros(n + 1, np.int32)
+    ci = np.zeros(int(nnz[0]), np.int32)
+    v = np.zeros(int(nnz[0]))
+    L.ref_cube_d(nx, ny, nz, config, None, p(rp), p(ci), p(v))
+    return rp, ci, v
