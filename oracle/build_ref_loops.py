@@ -1,8 +1,9 @@
 """Compile the reference's own loop files (src/blas/detail/blas.inl,
 blas_ext.inl, blas_wrapper.inl, specific/blas_merged_jacobi.inl,
 src/blas2/detail/csr_matvec.inl, csr_gs.inl, dense_matvec.inl,
-src/primitives/matrix/operations/inverse.inl, src/misc/rand.h) and its
-channel-with-cube generator (examples/common/generator/channel_with_cube.inl,
+src/primitives/matrix/operations/inverse.inl, src/misc/rand.h), its binary
+system reader (src/io/detail/reader.inl) and its cube and channel-with-cube
+generators (examples/common/generator/cube.inl, channel_with_cube.inl,
 lame.inl) unchanged, where they lie under the reference tree (default
 /root/reference, or $XAMG_REFERENCE_ROOT), into CPU libraries under
 oracle/_ref/ that the tests use to check the oracle.  Nothing is copied: the
@@ -67,7 +68,7 @@ def build():
             continue
         objs = []
         for name, flags in (("rows", rows_flags), ("smooth", rows_flags), ("vec", vec_flags),
-                            ("gen", GENERIC)):
+                            ("gen", GENERIC), ("io", GENERIC)):
             obj = os.path.join(OUT, "ref_%s_%s.o" % (name, kind))
             # XAMG renamed per unit: no template instance is shared between units;
             # ref_loops/stub comes first so that its xamg_types.h stands in

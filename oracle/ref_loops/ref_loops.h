@@ -42,6 +42,12 @@ int ref_dense_ax_y_f(int64_t nr, int64_t nc, const float *m, const float *x, flo
 int64_t ref_channel_cube_d(int scale, int const_rhs, int nv, int64_t *nnz, int *rp, int *ci, double *v,
                            double *b);
 
+// The reference's binary system reader (src/io/detail/reader.inl:30-180,
+// read_system, one process): row count, *nnz, and into non-null outputs the
+// CSR arrays and the n x nv b and x it reads.
+int64_t ref_read_system_d(const char *path, int nv, int64_t *nnz, int *rp, int *ci, double *v, double *b,
+                          double *x);
+
 // The reference's cube generator (examples/common/generator/cube.inl:71-225,
 // configurations 0-4, one process): row count, *nnz and, into non-null
 // outputs, the CSR arrays (diagonal first, then its neighbour order).

@@ -74,6 +74,13 @@ struct perf_info {
     void allreduce(int) {}
 };
 
+// The log stream: discards what the reference prints.
+enum out_modifier { DBG, ALLRANKS };
+struct null_stream {
+    template <typename T> const null_stream &operator<<(const T &) const { return *this; }
+};
+static const null_stream out = {};
+
 namespace mpi {
 enum scope { INTRA_NUMA, INTRA_NODE, CROSS_NUMA, CROSS_NODE, GLOBAL };
 inline void barrier(scope) {}
@@ -154,6 +161,9 @@ namespace matrix {
 // the block covering every row (no row-index compression).
 template <typename F, typename I1, typename I2, typename I3, typename I4>
 struct csr_matrix {
+    typedef F float_type;
+    typedef I1 row_idx_type;
+    typedef I2 col_idx_type;
     vector::vector row, col, val, row_ind, col_ind;
     mem::sharing sharing_mode = mem::CORE;
     uint64_t nrows = 0, ncols = 0, nonzeros = 0;

@@ -50,6 +50,8 @@ def lib(kind, build=True):
     L.ref_jacobi_d.argtypes = [i64, vp, vp, vp, vp, vp, vp, vp, ci_, ci_]
     L.ref_channel_cube_d.restype = C.c_int64
     L.ref_channel_cube_d.argtypes = [ci_, ci_, ci_, vp, vp, vp, vp, vp]
+    L.ref_read_system_d.restype = C.c_int64
+    L.ref_read_system_d.argtypes = [C.c_char_p, ci_, vp, vp, vp, vp, vp, vp]
     L.ref_cube_d.restype = C.c_int64
     L.ref_cube_d.argtypes = [i64, i64, i64, ci_, vp, vp, vp, vp]
     PP = C.POINTER(C.c_void_p)
@@ -172,3 +174,18 @@ def cube(L, nx, ny, nz, config=0):
     v = np.zeros(int(nnz[0]))
     L.ref_cube_d(nx, ny, nz, config, None, p(rp), p(ci), p(v))
     return rp, ci, v
+
+
+def read_system(L, path, nv=1):
+    """The reference's binary system reader: (rp, ci, v, B, X)."""
+    nnz = np.zeros(1, np.int64)
+    n = L.ref_read_system_d(path.encode(), nv, p(nnz), None, None, None, None, None)
+    if n < 0:
+        raise ValueError("unsupported nv")
+    rp = np.zeros(n + 1, np.int32)
+    ci = np.zeros(int(nnz[0]), np.int32)
+    v = np.zeros(int(nnz[0]))
+    B = np.zeros((n, nv))
+    X = np.zeros((n, nv))
+    L.ref_read_system_d(path.encode(), nv, None, p(rp), p(ci), p(v), p(B), p(X))
+    return rp, ci, v, B, X
