@@ -313,6 +313,7 @@ struct MG {
     double cheb_fraction = 0.3;
     std::vector<double> min_eig, max_eig;  // per level
     int nc = 0;
+    int cycle = 0;  // mg_cycle: 0 V, 1 F, 2 W (mg.inl:186-280)
     std::vector<double> Ainv64;
     std::vector<float> Ainv32;
 };
@@ -408,13 +409,15 @@ void smooth(const MG &mg, int l, int method, int iters, double relaxd, const T *
     }
 }
 
-// V-cycle, MG_cycle mg.inl:186-280 with T1 == T2 (the precision form runs the
-// whole cycle in one type).  x is overwritten in place; b is read only.
+// One multigrid cycle, MG_cycle mg.inl:186-280 with T1 == T2 (the precision
+// form runs the whole cycle in one type): cyc 0 V, 1 F (no pre-smoothing on
+// this level; the coarser level gets an F- then a V-cycle), 2 W (two W-cycles
+// on the coarser level).  x is overwritten in place; b is read only.
 template <class T>
-void vcycle(const MG &mg, int l, T *x, const T *b, int nv) {
+void vcycle(const MG &mg, int l, T *x, const T *b, int nv, int cyc = 0) {
     const Level &L = mg.lv[l];
     i64 n = L.A.n, nc = L.P.ncols;
-    smooth<T>(mg, l, mg.pre_m, mg.pre_it, mg.pre_relax, b, x, nv);
+    if (cyc != 1) smooth<T>(mg, l, mg.pre_m, mg.pre_it, mg.pre_relax, b, x, nv);
     std::vector<T> tmp((size_t)n * nv), bH((size_t)nc * nv), xH((size_t)nc * nv, T(0));
     spmv<T>(n, L.A.rp.data(), L.A.ci.data(), vals<T>(L.A), x, tmp.data(), nv, 0);
     #pragma omp parallel for schedule(static)
@@ -423,7 +426,9 @@ void vcycle(const MG &mg, int l, T *x, const T *b, int nv) {
     if (l + 1 == (int)mg.lv.size() - 1) {
         dense_gemv<T>((int)nc, ainv<T>(mg), bH.data(), xH.data(), nv);
     } else {
-        vcycle<T>(mg, l + 1, xH.data(), bH.data(), nv);
+        vcycle<T>(mg, l + 1, xH.data(), bH.data(), nv, cyc);
+        if (cyc == 2) vcycle<T>(mg, l + 1, xH.data(), bH.data(), nv, 2);
+        else if (cyc == 1) vcycle<T>(mg, l + 1, xH.data(), bH.data(), nv, 0);
     }
     spmv<T>(n, L.P.rp.data(), L.P.ci.data(), vals<T>(L.P), xH.data(), x, nv, 1);  // Axpy(P,xH,x)
     smooth<T>(mg, l, mg.post_m, mg.post_it, mg.post_relax, b, x, nv);
@@ -438,7 +443,7 @@ void mg_apply(const MG &mg, T *x, const T *b, int nv) {
         dense_gemv<T>((int)mg.lv[0].A.n, ainv<T>(mg), b, x, nv);
         return;
     }
-    vcycle<T>(mg, 0, x, b, nv);
+    vcycle<T>(mg, 0, x, b, nv, mg.cycle);
 }
 
 // ---------------------------------------------------------------- Krylov
@@ -896,6 +901,7 @@ void orc_mg_set_smoothers(void *h, int pre_m, int pre_it, double pre_relax, int 
 }
 // Coarse operator: dense inverse of the last level's A (Direct::init
 // direct.inl:37-44), FP32 copy rounded from the FP64 inverse.
+void orc_mg_set_cycle(void *h, int cycle) { ((MG *)h)->cycle = cycle; }
 void orc_mg_finalize(void *h, int fp32) {
     MG *m = (MG *)h;
     m->fp32 = fp32;

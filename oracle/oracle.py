@@ -46,6 +46,7 @@ def lib():
             "orc_mg_set_smoothers": (None, [P, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_double]),
             "orc_mg_set_cheb": (None, [P, C.c_int, C.c_double, P, P]),
             "orc_mg_finalize": (None, [P, C.c_int]),
+            "orc_mg_set_cycle": (None, [P, C.c_int]),
             "orc_mg_get_coarse_inverse": (None, [P, P]),
             "orc_mg_get_R": (None, [P, C.c_int, P, P, P]),
             "orc_mg_apply_d": (None, [P, P, P, C.c_int]),
@@ -162,9 +163,10 @@ class MG:
     """Oracle multigrid hierarchy (levels exported from the product's setup)."""
 
     def __init__(self, levels, fp32=False, pre=(SM_HSGS, 1, 0.99), post=(SM_HSGS, 1, 0.99), block_rows=None,
-                 cheb=None):
+                 cheb=None, cycle=0):
         """cheb = (order, spectrum_fraction, [(min_eig, max_eig) per level])
-        for the Chebyshev smoother (method SM_CHEB)."""
+        for the Chebyshev smoother (method SM_CHEB); cycle = mg_cycle (0 V,
+        1 F, 2 W)."""
         self.h = lib().orc_mg_create(len(levels))
         self.keep = []
         for l, lv in enumerate(levels):
@@ -187,6 +189,7 @@ class MG:
             mx = np.array([e[1] for e in eig], np.float64)
             self.keep += [mn, mx]
             lib().orc_mg_set_cheb(self.h, int(order), float(frac), p(mn), p(mx))
+        lib().orc_mg_set_cycle(self.h, int(cycle))  # mg_cycle: 0 V, 1 F, 2 W
         lib().orc_mg_finalize(self.h, int(fp32))
         self.nc = len(levels[-1]["A"][0]) - 1
 

@@ -73,6 +73,7 @@ struct Hier {
     const int *nb; const int64_t *const *bp;
     double relax; int pre_it, post_it;
     int smoother;  // 0: HSGS (hsgs.inl), 1: Jacobi (jacobi.inl, no-check path)
+    int mg_cycle;  // 0 V, 1 F, 2 W
     std::vector<std::vector<double>> invd;
     std::vector<double> ainv;
     void init() {
@@ -102,10 +103,11 @@ struct Hier {
         for (int k = 0; k < it; ++k)
             ref_hsgs_d(nrows[l], arp[l], aci[l], av[l], invd[l].data(), b, x, rl.data(), nv, nb[l], bp[l]);
     }
-    // MultiGrid::MG_cycle, mg.inl:186-280, V-cycle, one precision
-    template <int NV> void cycle(int l, double *x, const double *b) const {
+    // MultiGrid::MG_cycle, mg.inl:186-280, one precision; cyc = mg_cycle
+    // (0 V, 1 F: no pre-smoothing, then F and V on the coarser level, 2 W)
+    template <int NV> void cycle(int l, double *x, const double *b, int cyc) const {
         int64_t n = nrows[l], nc = nrows[l + 1];
-        smooth(l, b, x, NV, pre_it);
+        if (cyc != 1) smooth(l, b, x, NV, pre_it);
         std::vector<double> tmp((size_t)n * NV), bH((size_t)nc * NV), xH((size_t)nc * NV, 0.0);
         std::vector<double> one(NV, 1.0), mone(NV, -1.0);
         vector a1 = scalars(one.data(), NV), a_1 = scalars(mone.data(), NV);
@@ -117,8 +119,11 @@ struct Hier {
         blas::set_const<double, NV>(XH, 0.0, true);
         if (l + 1 == nlev - 1)
             ref_dense_ax_y_d(nc, nc, ainv.data(), bH.data(), xH.data(), NV);  // Direct::solve
-        else
-            cycle<NV>(l + 1, xH.data(), bH.data());
+        else {
+            cycle<NV>(l + 1, xH.data(), bH.data(), cyc);
+            if (cyc == 2) cycle<NV>(l + 1, xH.data(), bH.data(), 2);
+            else if (cyc == 1) cycle<NV>(l + 1, xH.data(), bH.data(), 0);
+        }
         ref_csr_axpy_d(n, prp[l], pci[l], pv[l], xH.data(), x, NV);
         smooth(l, b, x, NV, post_it);
     }
@@ -156,7 +161,7 @@ struct Bicgstab {
         // M^{-1}: one V-cycle from zero (MultiGrid::solve with max_iters 1)
         auto precond = [&](vector &out, const vector &in) {
             blas::set_const<F, NV>(out, 0.0, true);
-            mg->cycle<NV>(0, out.get_aligned_ptr<F>(), in.get_aligned_ptr<F>());
+            mg->cycle<NV>(0, out.get_aligned_ptr<F>(), in.get_aligned_ptr<F>(), mg->mg_cycle);
         };
         Conv cv{std::vector<double>(NV), std::vector<double>(NV), std::vector<int>(NV, 0),
                 abs_tol, rel_tol, hist, cap, 0, NV};
@@ -224,7 +229,7 @@ struct KrylovBase {
     template <int NV> void precond(vector &out, const vector &in) const {
         blas::set_const<double, NV>(out, 0.0, true);
         if (mg)
-            mg->cycle<NV>(0, out.get_aligned_ptr<double>(), in.get_aligned_ptr<double>());
+            mg->cycle<NV>(0, out.get_aligned_ptr<double>(), in.get_aligned_ptr<double>(), mg->mg_cycle);
         else
             blas::copy<double, NV>(in, out);
     }
@@ -407,7 +412,7 @@ static Hier *make_hier(int nlev, const int64_t *nrows, const int *const *arp, co
                        int pre_it, int post_it, int smoother) {
     if (nlev < 2) return nullptr;
     Hier *h = new Hier{nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax, pre_it, post_it,
-                       smoother, {}, {}};
+                       smoother & 15, smoother >> 4, {}, {}};
     h->init();
     return h;
 }
@@ -445,7 +450,7 @@ int ref_pbicgstab_amg_d(int nlev, const int64_t *nrows, const int *const *arp, c
                         int pre_it, int post_it, const double *b, double *x, int nv, int max_iters,
                         double abs_tol, double rel_tol, double *hist, int hist_cap) {
     if (nlev < 2) return -1;
-    Hier h{nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax, pre_it, post_it, 0, {}, {}};
+    Hier h{nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax, pre_it, post_it, 0, 0, {}, {}};
     h.init();
     Bicgstab f{nrows[0], arp[0], aci[0], av[0], b, x, nv, max_iters, abs_tol, rel_tol, hist, hist_cap, &h, 0};
     if (dispatch_nv(nv, f)) return -1;
