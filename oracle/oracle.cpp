@@ -200,35 +200,37 @@ void kdot(i64 n, int nv, const T *x, const T *y, double *out) {
 // Gauss-Jordan inverse without pivoting, inverse.inl:31-106 (operation order
 // kept: row scaling right-to-left, elimination below, then back-elimination on
 // the right half).  Used by the Direct coarse-grid solver.
-void dense_inverse(int n, const double *A, double *Ainv) {
+template <class T>
+void dense_inverse_t(int n, const T *A, T *Ainv) {
     int m = 2 * n;
-    std::vector<double> e((size_t)n * m, 0.0);
+    std::vector<T> e((size_t)n * m, T(0));
     for (int i = 0; i < n; ++i) {
-        e[(size_t)i * m + i + n] = 1.0;
+        e[(size_t)i * m + i + n] = T(1);
         for (int j = 0; j < n; ++j) e[(size_t)i * m + j] = A[(size_t)i * n + j];
     }
     for (int i = 0; i < n; ++i) {
-        double *ri = &e[(size_t)i * m];
+        T *ri = &e[(size_t)i * m];
         for (int k = m - 1; k > i; --k) ri[k] /= ri[i];
-        ri[i] = 1.0;
+        ri[i] = T(1);
         for (int j = i + 1; j < n; ++j) {
-            double *rj = &e[(size_t)j * m];
+            T *rj = &e[(size_t)j * m];
             for (int k = m - 1; k > i; --k) rj[k] -= rj[i] * ri[k];
-            rj[i] = 0.0;
+            rj[i] = T(0);
         }
     }
     for (int ii = 0; ii < n; ++ii) {
         int row = n - 1 - ii;
-        double *ri = &e[(size_t)row * m];
+        T *ri = &e[(size_t)row * m];
         for (int j = 0; j < row; ++j) {
-            double *rj = &e[(size_t)j * m];
+            T *rj = &e[(size_t)j * m];
             for (int k = n; k < m; ++k) rj[k] -= rj[row] * ri[k];
-            rj[row] = 0.0;
+            rj[row] = T(0);
         }
     }
     for (int i = 0; i < n; ++i)
         for (int j = 0; j < n; ++j) Ainv[(size_t)i * n + j] = e[(size_t)i * m + n + j];
 }
+void dense_inverse(int n, const double *A, double *Ainv) { dense_inverse_t<double>(n, A, Ainv); }
 
 // y = Ainv b, dense_Ax_y dense_matvec.inl:109-117, fma in column order.
 template <class T>
@@ -314,6 +316,8 @@ struct MG {
     std::vector<double> min_eig, max_eig;  // per level
     int nc = 0;
     int cycle = 0;  // mg_cycle: 0 V, 1 F, 2 W (mg.inl:186-280)
+    int reduced = 0;  // mg_reduced_precision: level 0 in FP64, the coarser levels in FP32
+    std::vector<float> Ainv32r;  // the FP32 coarse inverse computed in FP32 (Direct<float>)
     std::vector<double> Ainv64;
     std::vector<float> Ainv32;
 };
@@ -326,7 +330,7 @@ template <> const double *invd<double>(const Level &l) { return l.invd64.data();
 template <> const float *invd<float>(const Level &l) { return l.invd32.data(); }
 template <class T> const T *ainv(const MG &m);
 template <> const double *ainv<double>(const MG &m) { return m.Ainv64.data(); }
-template <> const float *ainv<float>(const MG &m) { return m.Ainv32.data(); }
+template <> const float *ainv<float>(const MG &m) { return m.reduced ? m.Ainv32r.data() : m.Ainv32.data(); }
 
 // Smoother call (HSGS::solve hsgs.inl:53-91 / Jacobi::solve jacobi.inl:91-100);
 // both are used with nocheck, so exactly `iters` sweeps run.  The convergence
@@ -434,6 +438,14 @@ void vcycle(const MG &mg, int l, T *x, const T *b, int nv, int cyc = 0) {
     smooth<T>(mg, l, mg.post_m, mg.post_it, mg.post_relax, b, x, nv);
 }
 
+// MG_cycle<double, float> on level 0 with mg_reduced_precision
+// (mg.inl:186-280, 320-321): level 0 and its smoothers in FP64, the residual
+// converted to FP32 before restriction by R_0 (FP32 values), the coarser
+// levels as an FP32 cycle (the coarsest solved by the FP32 Direct solver,
+// whose inverse the reference computes in FP32, mg.inl:147-149), the
+// correction P_0 x_H formed in FP32, converted, and added: x = 1*temp + 1*x.
+void cycle_reduced(const MG &mg, double *x, const double *b, int nv, int cyc);
+
 template <class T>
 void mg_apply(const MG &mg, T *x, const T *b, int nv) {
     size_t sz = (size_t)mg.lv[0].A.n * nv;
@@ -443,7 +455,34 @@ void mg_apply(const MG &mg, T *x, const T *b, int nv) {
         dense_gemv<T>((int)mg.lv[0].A.n, ainv<T>(mg), b, x, nv);
         return;
     }
+    if (mg.reduced && sizeof(T) == sizeof(double)) {
+        cycle_reduced(mg, (double *)x, (const double *)b, nv, mg.cycle);
+        return;
+    }
     vcycle<T>(mg, 0, x, b, nv, mg.cycle);
+}
+
+void cycle_reduced(const MG &mg, double *x, const double *b, int nv, int cyc) {
+    const Level &L = mg.lv[0];
+    i64 n = L.A.n, nc = L.P.ncols;
+    if (cyc != 1) smooth<double>(mg, 0, mg.pre_m, mg.pre_it, mg.pre_relax, b, x, nv);
+    std::vector<double> tmp((size_t)n * nv);
+    std::vector<float> t32((size_t)n * nv), bH((size_t)nc * nv), xH((size_t)nc * nv, 0.f);
+    spmv<double>(n, L.A.rp.data(), L.A.ci.data(), vals<double>(L.A), x, tmp.data(), nv, 0);
+    for (size_t q = 0; q < tmp.size(); ++q) tmp[q] = 1.0 * b[q] + (-1.0) * tmp[q];
+    for (size_t q = 0; q < tmp.size(); ++q) t32[q] = (float)tmp[q];
+    spmv<float>(L.R.n, L.R.rp.data(), L.R.ci.data(), vals<float>(L.R), t32.data(), bH.data(), nv, 0);
+    if (1 == (int)mg.lv.size() - 1) {
+        dense_gemv<float>((int)nc, mg.Ainv32r.data(), bH.data(), xH.data(), nv);
+    } else {
+        vcycle<float>(mg, 1, xH.data(), bH.data(), nv, cyc);
+        if (cyc == 2) vcycle<float>(mg, 1, xH.data(), bH.data(), nv, 2);
+        else if (cyc == 1) vcycle<float>(mg, 1, xH.data(), bH.data(), nv, 0);
+    }
+    spmv<float>(n, L.P.rp.data(), L.P.ci.data(), vals<float>(L.P), xH.data(), t32.data(), nv, 0);
+    for (size_t q = 0; q < tmp.size(); ++q) tmp[q] = (double)t32[q];
+    for (size_t q = 0; q < tmp.size(); ++q) x[q] = 1.0 * tmp[q] + 1.0 * x[q];
+    smooth<double>(mg, 0, mg.post_m, mg.post_it, mg.post_relax, b, x, nv);
 }
 
 // ---------------------------------------------------------------- Krylov
@@ -902,6 +941,7 @@ void orc_mg_set_smoothers(void *h, int pre_m, int pre_it, double pre_relax, int 
 // Coarse operator: dense inverse of the last level's A (Direct::init
 // direct.inl:37-44), FP32 copy rounded from the FP64 inverse.
 void orc_mg_set_cycle(void *h, int cycle) { ((MG *)h)->cycle = cycle; }
+void orc_mg_set_reduced(void *h, int on) { ((MG *)h)->reduced = on ? 1 : 0; }
 void orc_mg_finalize(void *h, int fp32) {
     MG *m = (MG *)h;
     m->fp32 = fp32;
@@ -915,6 +955,12 @@ void orc_mg_finalize(void *h, int fp32) {
     dense_inverse(n, D.data(), m->Ainv64.data());
     m->Ainv32.resize((size_t)n * n);
     for (size_t q = 0; q < m->Ainv64.size(); ++q) m->Ainv32[q] = (float)m->Ainv64[q];
+    // Direct<float> on a reduced hierarchy: Gauss-Jordan of the FP32 matrix in FP32
+    std::vector<float> D32((size_t)n * n, 0.f);
+    for (int i = 0; i < n; ++i)
+        for (int j = L.A.rp[i]; j < L.A.rp[i + 1]; ++j) D32[(size_t)i * n + L.A.ci[j]] = L.A.v32[j];
+    m->Ainv32r.resize((size_t)n * n);
+    dense_inverse_t<float>(n, D32.data(), m->Ainv32r.data());
 }
 void orc_mg_get_coarse_inverse(void *h, double *out) {
     MG *m = (MG *)h;

@@ -47,6 +47,7 @@ def lib():
             "orc_mg_set_cheb": (None, [P, C.c_int, C.c_double, P, P]),
             "orc_mg_finalize": (None, [P, C.c_int]),
             "orc_mg_set_cycle": (None, [P, C.c_int]),
+            "orc_mg_set_reduced": (None, [P, C.c_int]),
             "orc_mg_get_coarse_inverse": (None, [P, P]),
             "orc_mg_get_R": (None, [P, C.c_int, P, P, P]),
             "orc_mg_apply_d": (None, [P, P, P, C.c_int]),
@@ -163,10 +164,11 @@ class MG:
     """Oracle multigrid hierarchy (levels exported from the product's setup)."""
 
     def __init__(self, levels, fp32=False, pre=(SM_HSGS, 1, 0.99), post=(SM_HSGS, 1, 0.99), block_rows=None,
-                 cheb=None, cycle=0):
+                 cheb=None, cycle=0, reduced=False):
         """cheb = (order, spectrum_fraction, [(min_eig, max_eig) per level])
         for the Chebyshev smoother (method SM_CHEB); cycle = mg_cycle (0 V,
-        1 F, 2 W)."""
+        1 F, 2 W); reduced = mg_reduced_precision (level 0 in FP64, the
+        coarser levels in FP32, an FP64 solve's preconditioner)."""
         self.h = lib().orc_mg_create(len(levels))
         self.keep = []
         for l, lv in enumerate(levels):
@@ -190,6 +192,7 @@ class MG:
             self.keep += [mn, mx]
             lib().orc_mg_set_cheb(self.h, int(order), float(frac), p(mn), p(mx))
         lib().orc_mg_set_cycle(self.h, int(cycle))  # mg_cycle: 0 V, 1 F, 2 W
+        lib().orc_mg_set_reduced(self.h, int(bool(reduced)))
         lib().orc_mg_finalize(self.h, int(fp32))
         self.nc = len(levels[-1]["A"][0]) - 1
 

@@ -12,6 +12,7 @@
 #include "blas2/detail/csr_gs.inl"
 #include "blas2/detail/dense_matvec.inl"
 #include "primitives/matrix/operations/inverse.inl"
+#include "primitives/vector/operations/convert.inl"
 
 namespace refloops {
 

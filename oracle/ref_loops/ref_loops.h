@@ -104,8 +104,9 @@ int ref_pbicgstab_amg_d(int nlev, const int64_t *nrows, const int *const *arp, c
 // (P)BiCGStab (method 0, as above), PCG (method 1, pcg.inl:48-160) or
 // RBiCGStab (method 2, rbicgstab.inl:48-225) in the reference's step order,
 // preconditioned by one multigrid cycle when nlev >= 2 (smoother & 15:
-// 0 HSGS, 1 Jacobi, pre_it / post_it sweeps; smoother >> 4: mg_cycle, 0 V,
-// 1 F, 2 W), else by the identity (M^{-1} r = r;
+// 0 HSGS, 1 Jacobi, pre_it / post_it sweeps; (smoother >> 4) & 15: mg_cycle,
+// 0 V, 1 F, 2 W; bit 8: mg_reduced_precision, MG_cycle<double, float> on the
+// first level and FP32 below, HSGS only), else by the identity (M^{-1} r = r;
 // nrows[0], arp[0], aci[0], av[0] give the operator; for method 0 no
 // preconditioner at all).  Returns the iteration count, -1 on bad input.
 int ref_krylov_d(int method, int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,

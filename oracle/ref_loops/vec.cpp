@@ -74,9 +74,92 @@ struct Hier {
     double relax; int pre_it, post_it;
     int smoother;  // 0: HSGS (hsgs.inl), 1: Jacobi (jacobi.inl, no-check path)
     int mg_cycle;  // 0 V, 1 F, 2 W
+    int reduced;   // mg_reduced_precision: levels >= 1, P_0 and R_0 in FP32 (HSGS only)
     std::vector<std::vector<double>> invd;
     std::vector<double> ainv;
+    std::vector<std::vector<float>> av32, pv32, rv32, invd32;
+    std::vector<float> ainv32;
+    void init_reduced() {
+        av32.resize(nlev); pv32.resize(nlev); rv32.resize(nlev); invd32.resize(nlev);
+        for (int l = 0; l < nlev; ++l) {
+            const int64_t n = nrows[l];
+            av32[l].assign(av[l], av[l] + arp[l][n]);
+            invd32[l].assign(n, 0.f);
+            for (int64_t i = 0; i < n; ++i)
+                for (int j = arp[l][i]; j < arp[l][i + 1]; ++j)
+                    if (aci[l][j] == i) invd32[l][i] = (float)(1.0 / (double)av32[l][j]);  // csr_matrix.h:344-349, F = float
+            if (l + 1 < nlev) {
+                pv32[l].assign(pv[l], pv[l] + prp[l][n]);
+                rv32[l].assign(rv[l], rv[l] + rrp[l][nrows[l + 1]]);
+            }
+        }
+        // the coarsest level's Direct<float> (mg.inl:147-149): the inverse of the FP32 matrix in FP32
+        int64_t nc = nrows[nlev - 1];
+        std::vector<float> d((size_t)(nc * nc), 0.f);
+        for (int64_t i = 0; i < nc; ++i)
+            for (int j = arp[nlev - 1][i]; j < arp[nlev - 1][i + 1]; ++j)
+                d[i * nc + aci[nlev - 1][j]] = av32[nlev - 1][j];
+        ainv32.resize(d.size());
+        XAMG::matrix::dense_matrix<float> m(XAMG::mem::CORE), mi(XAMG::mem::CORE);
+        m.nrows = m.block_nrows = (uint64_t)nc;
+        m.ncols = m.block_ncols = (uint64_t)nc;
+        m.val = block(d.data(), nc * nc, 1);
+        XAMG::matrix::inverse<float>(m, mi);
+        std::memcpy(ainv32.data(), mi.val.get_aligned_ptr<float>(), sizeof(float) * d.size());
+    }
+    // MG_cycle<float, float> on levels >= 1 of a reduced hierarchy
+    template <int NV> void cycle32(int l, float *x, const float *b, int cyc) const {
+        int64_t n = nrows[l], nc = nrows[l + 1];
+        std::vector<float> rl(NV, (float)relax);
+        if (cyc != 1)
+            for (int k = 0; k < pre_it; ++k)
+                ref_hsgs_f(n, arp[l], aci[l], av32[l].data(), invd32[l].data(), b, x, rl.data(), NV, nb[l], bp[l]);
+        std::vector<float> tmp((size_t)n * NV), bH((size_t)nc * NV), xH((size_t)nc * NV, 0.f);
+        std::vector<float> one(NV, 1.f), mone(NV, -1.f);
+        vector a1 = scalars(one.data(), NV), a_1 = scalars(mone.data(), NV);
+        ref_csr_ax_y_f(n, arp[l], aci[l], av32[l].data(), x, tmp.data(), NV);
+        vector B = block(b, n, NV), T = block(tmp.data(), n, NV);
+        blas::axpby<float, NV>(a1, B, a_1, T);
+        ref_csr_ax_y_f(nc, rrp[l], rci[l], rv32[l].data(), tmp.data(), bH.data(), NV);
+        if (l + 1 == nlev - 1)
+            ref_dense_ax_y_f(nc, nc, ainv32.data(), bH.data(), xH.data(), NV);
+        else {
+            cycle32<NV>(l + 1, xH.data(), bH.data(), cyc);
+            if (cyc == 2) cycle32<NV>(l + 1, xH.data(), bH.data(), 2);
+            else if (cyc == 1) cycle32<NV>(l + 1, xH.data(), bH.data(), 0);
+        }
+        ref_csr_axpy_f(n, prp[l], pci[l], pv32[l].data(), xH.data(), x, NV);
+        for (int k = 0; k < post_it; ++k)
+            ref_hsgs_f(n, arp[l], aci[l], av32[l].data(), invd32[l].data(), b, x, rl.data(), NV, nb[l], bp[l]);
+    }
+    // MG_cycle<double, float> on level 0 (mg.inl:186-280, 320-321)
+    template <int NV> void cycle_reduced(double *x, const double *b, int cyc) const {
+        int64_t n = nrows[0], nc = nrows[1];
+        if (cyc != 1) smooth(0, b, x, NV, pre_it);
+        std::vector<double> tmp((size_t)n * NV);
+        std::vector<float> t32((size_t)n * NV), bH((size_t)nc * NV), xH((size_t)nc * NV, 0.f);
+        std::vector<double> one(NV, 1.0), mone(NV, -1.0);
+        vector a1 = scalars(one.data(), NV), a_1 = scalars(mone.data(), NV);
+        ref_csr_ax_y_d(n, arp[0], aci[0], av[0], x, tmp.data(), NV);
+        vector B = block(b, n, NV), T = block(tmp.data(), n, NV), T32 = block(t32.data(), n, NV),
+               X = block(x, n, NV);
+        blas::axpby<double, NV>(a1, B, a_1, T);
+        XAMG::vector::convert<double, float>(T, T32);
+        ref_csr_ax_y_f(nc, rrp[0], rci[0], rv32[0].data(), t32.data(), bH.data(), NV);
+        if (nlev == 2)
+            ref_dense_ax_y_f(nc, nc, ainv32.data(), bH.data(), xH.data(), NV);
+        else {
+            cycle32<NV>(1, xH.data(), bH.data(), cyc);
+            if (cyc == 2) cycle32<NV>(1, xH.data(), bH.data(), 2);
+            else if (cyc == 1) cycle32<NV>(1, xH.data(), bH.data(), 0);
+        }
+        ref_csr_ax_y_f(n, prp[0], pci[0], pv32[0].data(), xH.data(), t32.data(), NV);
+        XAMG::vector::convert<float, double>(T32, T);
+        blas::axpby<double, NV>(a1, T, a1, X);
+        smooth(0, b, x, NV, post_it);
+    }
     void init() {
+        if (reduced) init_reduced();
         invd.resize(nlev);
         for (int l = 0; l < nlev; ++l) {
             invd[l].assign(nrows[l], 0.0);
@@ -161,7 +244,10 @@ struct Bicgstab {
         // M^{-1}: one V-cycle from zero (MultiGrid::solve with max_iters 1)
         auto precond = [&](vector &out, const vector &in) {
             blas::set_const<F, NV>(out, 0.0, true);
-            mg->cycle<NV>(0, out.get_aligned_ptr<F>(), in.get_aligned_ptr<F>(), mg->mg_cycle);
+            if (mg->reduced)
+                mg->cycle_reduced<NV>(out.get_aligned_ptr<F>(), in.get_aligned_ptr<F>(), mg->mg_cycle);
+            else
+                mg->cycle<NV>(0, out.get_aligned_ptr<F>(), in.get_aligned_ptr<F>(), mg->mg_cycle);
         };
         Conv cv{std::vector<double>(NV), std::vector<double>(NV), std::vector<int>(NV, 0),
                 abs_tol, rel_tol, hist, cap, 0, NV};
@@ -228,7 +314,9 @@ struct KrylovBase {
     // set_const(out, 0); precond->solve(out, in)
     template <int NV> void precond(vector &out, const vector &in) const {
         blas::set_const<double, NV>(out, 0.0, true);
-        if (mg)
+        if (mg && mg->reduced)
+            mg->cycle_reduced<NV>(out.get_aligned_ptr<double>(), in.get_aligned_ptr<double>(), mg->mg_cycle);
+        else if (mg)
             mg->cycle<NV>(0, out.get_aligned_ptr<double>(), in.get_aligned_ptr<double>(), mg->mg_cycle);
         else
             blas::copy<double, NV>(in, out);
@@ -412,7 +500,7 @@ static Hier *make_hier(int nlev, const int64_t *nrows, const int *const *arp, co
                        int pre_it, int post_it, int smoother) {
     if (nlev < 2) return nullptr;
     Hier *h = new Hier{nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax, pre_it, post_it,
-                       smoother & 15, smoother >> 4, {}, {}};
+                       smoother & 15, (smoother >> 4) & 15, (smoother >> 8) & 1, {}, {}, {}, {}, {}, {}, {}};
     h->init();
     return h;
 }
@@ -450,7 +538,8 @@ int ref_pbicgstab_amg_d(int nlev, const int64_t *nrows, const int *const *arp, c
                         int pre_it, int post_it, const double *b, double *x, int nv, int max_iters,
                         double abs_tol, double rel_tol, double *hist, int hist_cap) {
     if (nlev < 2) return -1;
-    Hier h{nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax, pre_it, post_it, 0, 0, {}, {}};
+    Hier h{nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax, pre_it, post_it, 0, 0, 0,
+           {}, {}, {}, {}, {}, {}, {}};
     h.init();
     Bicgstab f{nrows[0], arp[0], aci[0], av[0], b, x, nv, max_iters, abs_tol, rel_tol, hist, hist_cap, &h, 0};
     if (dispatch_nv(nv, f)) return -1;

@@ -130,11 +130,12 @@ def pbicgstab_amg(L, levels, B, blocks=None, max_iters=200, rel_tol=1e-8, relax=
 
 
 def krylov(L, method, levels, B, blocks=None, max_iters=200, rel_tol=1e-8, relax=0.99, smoother="HSGS",
-           sweeps=1, cycle="V"):
+           sweeps=1, cycle="V", reduced=False):
     """PBiCGStab ("PBiCGStab"), PCG ("PCG") or RBiCGStab ("RBiCGStab") from
     x = 0, preconditioned by one multigrid cycle ("V", "F" or "W") over
     `levels` (HSGS or Jacobi smoothing, `sweeps` before and after) when it
-    has two or more levels, else
+    has two or more levels (reduced: mg_reduced_precision, the levels below
+    the first and the first level's transfers in FP32, HSGS only), else
     by the identity (levels = [the operator's level]).  Returns (x,
     iterations, history)."""
     nrows, cast, nb, keep = _hier_args(levels, blocks)
@@ -142,7 +143,7 @@ def krylov(L, method, levels, B, blocks=None, max_iters=200, rel_tol=1e-8, relax
     B = np.ascontiguousarray(B, np.float64)
     x = np.zeros_like(B)
     h = np.zeros((max_iters + 2, nv))
-    code = {"HSGS": 0, "Jacobi": 1}[smoother] | ({"V": 0, "F": 1, "W": 2}[cycle] << 4)
+    code = {"HSGS": 0, "Jacobi": 1}[smoother] | ({"V": 0, "F": 1, "W": 2}[cycle] << 4) | (int(reduced) << 8)
     it = L.ref_krylov_d({"PBiCGStab": 0, "PCG": 1, "RBiCGStab": 2}[method], len(levels), p(nrows), *cast[:9],
                         p(nb), cast[9], relax, sweeps, sweeps, code, p(B), p(x), nv, max_iters, 0.0, rel_tol, p(h),
                         max_iters + 2)

@@ -415,3 +415,24 @@ def test_amg_pbicgstab_f_and_w_cycles_match_reference_loops(libs, seq_dot, cycle
     assert itr == it and it > 0
     assert np.array_equal(h, hist)
     assert np.array_equal(x, xo)
+
+
+@pytest.mark.parametrize("cycle", ["V", "W"])
+def test_amg_pbicgstab_reduced_precision_matches_reference_loops(libs, seq_dot, cycle):
+    """mg_reduced_precision (mg.inl:147-149, 320-321): the first level and its
+    smoothers in FP64, the residual converted to FP32 for R_0, every coarser
+    level (operators, inverse diagonals, HSGS, the coarse Direct solver with
+    its Gauss-Jordan inverse computed in FP32) in FP32, the correction
+    converted back and added.  The oracle's reduced cycle against the
+    reference's loops in FP64 and FP32 (convert.inl for the conversions):
+    AMG-PBiCGStab on 27-point 16^3, NV = 4, bit for bit."""
+    rp, ci, v = orc.gen27(16)
+    levels = orc.amg_setup(rp, ci, v, mg_coarsening_type=10, mg_interpolation_type=6,
+                           mg_strength_threshold=0.25, mg_max_levels=6, mg_coarse_matrix_size=100)
+    B = np.random.default_rng(2027).uniform(-1, 1, (len(rp) - 1, 4))
+    mg = orc.MG(levels, cycle={"V": 0, "W": 2}[cycle], reduced=True)
+    xo, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg, 200, 0.0, 1e-8)
+    x, itr, h = reference_loops.krylov(libs["contract"], "PBiCGStab", levels, B, cycle=cycle, reduced=True)
+    assert itr == it and it > 0
+    assert np.array_equal(h, hist)
+    assert np.array_equal(x, xo)
