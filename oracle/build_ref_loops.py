@@ -54,33 +54,40 @@ def library(kind):
 
 
 def build():
+    from concurrent.futures import ThreadPoolExecutor
+
     ref = reference_src()
     if not os.path.isdir(os.path.join(ref, "blas2", "detail")):
         return []
     os.makedirs(OUT, exist_ok=True)
     deps = [os.path.join(d, f) for d in (SRC, os.path.join(SRC, "stub")) for f in sorted(os.listdir(d))
             if os.path.isfile(os.path.join(d, f))] + [os.path.abspath(__file__)]
-    built = []
+    todo = {}
     for kind, (rows_flags, vec_flags) in LIBS.items():
         lib = library(kind)
         if os.path.exists(lib) and all(os.path.getmtime(lib) >= os.path.getmtime(d) for d in deps):
-            built.append(lib)
             continue
-        objs = []
+        todo[kind] = []
         for name, flags in (("rows", rows_flags), ("smooth", rows_flags), ("vec", vec_flags),
                             ("gen", GENERIC), ("io", GENERIC)):
             obj = os.path.join(OUT, "ref_%s_%s.o" % (name, kind))
             # XAMG renamed per unit: no template instance is shared between units;
             # ref_loops/stub comes first so that its xamg_types.h stands in
-            subprocess.run(["g++", *flags, "-DXAMG=XAMG_" + name, "-I", os.path.join(SRC, "stub"), "-I", SRC,
-                            "-I", ref, "-I", os.path.join(os.path.dirname(ref), "examples", "common"), "-c",
-                            os.path.join(SRC, name + ".cpp"), "-o", obj], check=True)
-            objs.append(obj)
-        subprocess.run(["g++", "-shared", "-o", lib, *objs], check=True)
+            todo[kind].append((obj, ["g++", *flags, "-DXAMG=XAMG_" + name, "-I", os.path.join(SRC, "stub"),
+                                     "-I", SRC, "-I", ref, "-I", os.path.join(os.path.dirname(ref), "examples",
+                                                                              "common"),
+                                     "-c", os.path.join(SRC, name + ".cpp"), "-o", obj]))
+    jobs = [cmd for units in todo.values() for _, cmd in units]
+    with ThreadPoolExecutor(max_workers=max(2, os.cpu_count() or 2)) as ex:
+        for r in ex.map(lambda cmd: subprocess.run(cmd).returncode, jobs):
+            if r != 0:
+                raise RuntimeError("reference loop build failed")
+    for kind, units in todo.items():
+        objs = [o for o, _ in units]
+        subprocess.run(["g++", "-shared", "-o", library(kind), *objs], check=True)
         for o in objs:
             os.remove(o)
-        built.append(lib)
-    return built
+    return [library(k) for k in LIBS]
 
 
 if __name__ == "__main__":
