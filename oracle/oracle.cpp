@@ -940,6 +940,20 @@ void orc_mg_set_smoothers(void *h, int pre_m, int pre_it, double pre_relax, int 
 }
 // Coarse operator: dense inverse of the last level's A (Direct::init
 // direct.inl:37-44), FP32 copy rounded from the FP64 inverse.
+// One Chebyshev smoothing of x on the operator alone (the smoother of
+// chebyshev.inl:142-183 with the given spectrum bounds), for the checks
+// against the reference's own smoother.
+void orc_chebyshev_d(i64 n, const int *rp, const int *ci, const double *v, const double *b, double *x, int nv,
+                     int order, double fraction, double min_eig, double max_eig) {
+    MG m;
+    m.lv.resize(1);
+    fill(m.lv[0].A, n, n, rp, ci, v);
+    m.cheb_order = order;
+    m.cheb_fraction = fraction;
+    m.min_eig = {min_eig};
+    m.max_eig = {max_eig};
+    chebyshev<double>(m, 0, b, x, nv);
+}
 void orc_mg_set_cycle(void *h, int cycle) { ((MG *)h)->cycle = cycle; }
 void orc_mg_set_reduced(void *h, int on) { ((MG *)h)->reduced = on ? 1 : 0; }
 void orc_mg_finalize(void *h, int fp32) {

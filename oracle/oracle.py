@@ -48,6 +48,8 @@ def lib():
             "orc_mg_finalize": (None, [P, C.c_int]),
             "orc_mg_set_cycle": (None, [P, C.c_int]),
             "orc_mg_set_reduced": (None, [P, C.c_int]),
+            "orc_chebyshev_d": (None, [C.c_int64, P, P, P, P, P, C.c_int, C.c_int, C.c_double, C.c_double,
+                                        C.c_double]),
             "orc_mg_get_coarse_inverse": (None, [P, P]),
             "orc_mg_get_R": (None, [P, C.c_int, P, P, P]),
             "orc_mg_apply_d": (None, [P, P, P, C.c_int]),
@@ -234,6 +236,13 @@ def set_seq_dot(on):
     of the fixed tree the GPU shares; used only to compare whole solves with the
     reference's loops compiled unchanged (oracle/ref_loops)."""
     lib().orc_set_seq_dot(int(bool(on)))
+
+
+def chebyshev(rp, ci, v, b, x, order, fraction, min_eig, max_eig):
+    """One Chebyshev smoothing of x (in place) with the given spectrum bounds."""
+    n, nv = b.shape
+    lib().orc_chebyshev_d(n, p(rp), p(ci), p(v), p(b), p(x), nv, order, fraction, min_eig, max_eig)
+    return x
 
 
 def num_threads():

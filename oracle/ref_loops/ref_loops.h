@@ -73,6 +73,12 @@ int ref_scal_d(int64_t n, int nv, const double *a, double *y);                  
 int ref_jacobi_d(int64_t n, const int *rp, const int *ci, const double *v, const double *invd,
                  const double *b, double *x, const double *relax, int nv, int sweeps);
 
+// The Chebyshev smoother (src/solvers/detail/chebyshev.inl: its coefficient
+// table and Chebyshev::solve, compiled unchanged) applied once to x with the
+// given spectrum bounds of D^-1/2 A D^-1/2.
+int ref_chebyshev_d(int64_t n, const int *rp, const int *ci, const double *v, const double *b, double *x, int nv,
+                    int order, double fraction, double min_eig, double max_eig);
+
 // Gauss-Jordan inverse of a dense n x n matrix (row-major),
 // src/primitives/matrix/operations/inverse.inl:31-106 (the coarse-grid
 // Direct solver's setup)

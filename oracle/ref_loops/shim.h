@@ -114,6 +114,15 @@ struct vector {
 
     vector() = default;
     explicit vector(mem::sharing m) : sharing_mode(m) {}
+    // a copy of a vector that owns its storage views its own copy of it
+    vector(const vector &o) { *this = o; }
+    vector &operator=(const vector &o) {
+        sharing_mode = o.sharing_mode; type_hash = o.type_hash; if_allocated = o.if_allocated;
+        if_empty = o.if_empty; if_initialized = o.if_initialized; if_zero = o.if_zero; size = o.size;
+        ext_offset = o.ext_offset; nv = o.nv; own = o.own;
+        ptr = o.own.empty() ? o.ptr : (void *)own.data();
+        return *this;
+    }
 
     template <typename T> void view(T *p, uint64_t n, uint16_t w, bool zero = false) {
         ptr = (void *)p;
@@ -220,19 +229,32 @@ struct matrix_block {
     int data = 0;  // the block's operator (a placeholder: never read here)
     bool reduced_prec = false;
     template <typename M> void assemble(M &, int) {}
+    void get_inv_sqrt_diag() {}
 };
 struct matrix_layer {
     matrix_block diag;
     std::vector<matrix_block> offd;
 };
+struct matrix_info_stub {
+    void print(const char *) const {}
+};
+// One process's operator for the solver classes: a CSR block over caller
+// arrays (the type-erased products of blas2.h reduce to one csr_Ax_y here),
+// its spectrum bounds and D^{-1/2}.
 struct matrix {
     std::map<segment::hierarchy, matrix_layer> data_layer;
     bool reduced_prec = false;
     segmentation_type segmentation = SEGMENT_BY_BLOCKS;
     partitioning *row_part = nullptr;
     float64_t min_eig = 0, max_eig = 0;
+    matrix_info_stub info;
+    int64_t n = 0;
+    const int *rp = nullptr, *ci = nullptr;
+    const double *v = nullptr;
+    vector::vector isd;
     void set_part(partitioning *p) { row_part = p; }
     void add_data_layer(segment::hierarchy h) { data_layer[h]; }
+    const vector::vector &inv_sqrt_diag() const { return isd; }
 };
 
 }  // namespace matrix

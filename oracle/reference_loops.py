@@ -48,6 +48,7 @@ def lib(kind, build=True):
     L.ref_bicgstab_d.argtypes = [i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, vp, ci_]
     L.ref_dense_inverse_d.argtypes = [i64, vp, vp]
     L.ref_jacobi_d.argtypes = [i64, vp, vp, vp, vp, vp, vp, vp, ci_, ci_]
+    L.ref_chebyshev_d.argtypes = [i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, cd]
     L.ref_channel_cube_d.restype = C.c_int64
     L.ref_channel_cube_d.argtypes = [ci_, ci_, ci_, vp, vp, vp, vp, vp]
     L.ref_read_system_d.restype = C.c_int64

@@ -436,3 +436,22 @@ def test_amg_pbicgstab_reduced_precision_matches_reference_loops(libs, seq_dot, 
     assert itr == it and it > 0
     assert np.array_equal(h, hist)
     assert np.array_equal(x, xo)
+
+
+@pytest.mark.parametrize("order", [1, 2, 3, 4])
+@pytest.mark.parametrize("nv", [1, 4])
+def test_chebyshev_smoother_matches_reference_solver(libs, order, nv):
+    """The reference's Chebyshev smoother class (chebyshev.inl: coefficient
+    table of orders 1-4, the polynomial applied in D^-1/2 A D^-1/2 from the
+    residual b - A x) compiled unchanged, against the oracle's smoother with
+    the same spectrum bounds: bit for bit."""
+    rng = np.random.default_rng(10 * order + nv)
+    rp, ci, v = orc.gen27(10)
+    n = len(rp) - 1
+    b = rng.uniform(-1, 1, (n, nv))
+    x0 = rng.uniform(-1, 1, (n, nv))
+    lo, hi, frac = 0.013, 1.97, 0.3
+    xo = orc.chebyshev(rp, ci, v, b, x0.copy(), order, frac, lo, hi)
+    x = x0.copy()
+    assert libs["contract"].ref_chebyshev_d(n, p(rp), p(ci), p(v), p(b), p(x), nv, order, frac, lo, hi) == 0
+    assert np.array_equal(x, xo)
