@@ -185,6 +185,9 @@ void dot_sequential(i64 n, int nv, const T *x, const T *y, T *out) {
 // tests run a whole solve in the order of the reference's loops compiled
 // unchanged (oracle/ref_loops), which sum sequentially on one core.
 static int g_seq_dot = 0;
+// 1: the direction update of the reference's MergedBiCGStab (its only
+// difference from BiCGStab in arithmetic); used only by the tests
+static int g_merged_bicgstab = 0;
 
 template <class T>
 void kdot(i64 n, int nv, const T *x, const T *y, double *out) {
@@ -576,21 +579,34 @@ int pbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
         kdot<T>(n, nv, s.data(), s.data(), s4.data());
         for (int k = 0; k < nv; ++k) omega[k] = s2[k] / s3[k];
         // x = alpha_c*p_ + omega_c*s_ + 1*x
-        #pragma omp parallel for schedule(static)
-        for (i64 i = 0; i < n; ++i)
-            for (int k = 0; k < nv; ++k) {
-                size_t q = (size_t)i * nv + k;
-                double ac = iconv[k] * alpha[k], oc = iconv[k] * omega[k];
-                x[q] = (T)(ac * (double)pp[q] + oc * (double)ss[q] + 1.0 * (double)x[q]);
-            }
+        auto update_x = [&]() {
+            #pragma omp parallel for schedule(static)
+            for (i64 i = 0; i < n; ++i)
+                for (int k = 0; k < nv; ++k) {
+                    size_t q = (size_t)i * nv + k;
+                    double ac = iconv[k] * alpha[k], oc = iconv[k] * omega[k];
+                    x[q] = (T)(ac * (double)pp[q] + oc * (double)ss[q] + 1.0 * (double)x[q]);
+                }
+        };
+        // MergedBiCGStab (merged_bicgstab.inl:150-190) updates x after the
+        // check: with the old masks when every column has converged, else in
+        // its last group with the masks the check has just updated, so a
+        // column that converges before the others keeps the x of the
+        // iteration before
+        const bool merged_x = g_merged_bicgstab && !mg;
+        if (!merged_x) update_x();
         for (int k = 0; k < nv; ++k) {
             double rr = omega[k] * s2[k];
             res[k] = 1.0 * s4[k] + (-1.0) * rr;
         }
         cv.update(res.data());
         hist.push(cv.res, nv);
-        if (cv.check()) return it;
+        if (cv.check()) {
+            if (merged_x) update_x();
+            return it;
+        }
         for (int k = 0; k < nv; ++k) if (cv.status[k]) iconv[k] = 0;
+        if (merged_x) update_x();
         // r = 1*s + (-omega)*t
         #pragma omp parallel for schedule(static)
         for (i64 i = 0; i < n; ++i)
@@ -607,12 +623,18 @@ int pbicgstab(const Csr &A, const MG *mg, const T *b, T *x, int nv, int max_iter
             double c1 = -(omega[k] * beta[k]);
             s1[k] = c1;
         }
-        // p = 1*r + c1*v + beta*p
+        // p = 1*r + c1*v + beta*p; MergedBiCGStab without a preconditioner
+        // (merged_bicgstab.inl:186-189, blas_merged_bicgstab.inl:238-252):
+        // p = r + beta*p - (beta*omega)*v, left to right
+        const bool merged = g_merged_bicgstab && !mg;
         #pragma omp parallel for schedule(static)
         for (i64 i = 0; i < n; ++i)
             for (int k = 0; k < nv; ++k) {
                 size_t q = (size_t)i * nv + k;
-                p[q] = (T)(1.0 * (double)r[q] + s1[k] * (double)v[q] + beta[k] * (double)p[q]);
+                if (merged)
+                    p[q] = (T)(((double)r[q] + beta[k] * (double)p[q]) - (beta[k] * omega[k]) * (double)v[q]);
+                else
+                    p[q] = (T)(1.0 * (double)r[q] + s1[k] * (double)v[q] + beta[k] * (double)p[q]);
             }
     }
     return it;
@@ -834,6 +856,7 @@ int orc_num_threads() { return omp_get_max_threads(); }
 void orc_set_num_threads(int t) { omp_set_num_threads(t > 0 ? t : 1); }
 // 1: Krylov inner products in the reference's single-core order; 0: the tree
 void orc_set_seq_dot(int on) { orc::g_seq_dot = on ? 1 : 0; }
+void orc_set_merged_bicgstab(int on) { orc::g_merged_bicgstab = on ? 1 : 0; }
 
 void orc_spmv_d(i64 n, const int *rp, const int *ci, const double *v, const double *x, double *y,
                 int nv, int acc) { spmv<double>(n, rp, ci, v, x, y, nv, acc); }

@@ -245,6 +245,13 @@ def chebyshev(rp, ci, v, b, x, order, fraction, min_eig, max_eig):
     return x
 
 
+def set_merged_bicgstab(on):
+    """Unpreconditioned solves with the direction update of the reference's
+    MergedBiCGStab (p = r + beta p - (beta omega) v, left to right) instead of
+    BiCGStab's (r + (-omega beta) v + beta p)."""
+    lib().orc_set_merged_bicgstab(int(bool(on)))
+
+
 def num_threads():
     """Host threads of the oracle's parallel loops."""
     return int(lib().orc_num_threads())

@@ -107,6 +107,27 @@ int ref_pbicgstab_amg_d(int nlev, const int64_t *nrows, const int *const *arp, c
                         int pre_it, int post_it, const double *b, double *x, int nv, int max_iters,
                         double abs_tol, double rel_tol, double *hist, int hist_cap);
 
+// The multigrid preconditioner of the drivers as an object: created from a
+// hierarchy (arguments as ref_krylov_d), applied as one cycle from the x given
+// (MultiGrid::solve with max_iters 1 as a preconditioner), destroyed.
+void *ref_hier_create(int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
+                      const double *const *av, const int *const *prp, const int *const *pci,
+                      const double *const *pv, const int *const *rrp, const int *const *rci,
+                      const double *const *rv, const int *nb, const int64_t *const *bp, double relax, int pre_it,
+                      int post_it, int smoother);
+int ref_hier_apply_d(void *h, const double *b, double *x, int nv);
+void ref_hier_destroy(void *h);
+
+// The reference's own solver classes compiled unchanged (krylov.cpp):
+// method 0 BiCGStab (bicgstab.inl), 1 PBiCGStab (pbicgstab.inl), 2 PCG
+// (pcg.inl), 3 RBiCGStab (rbicgstab.inl), 4 MergedBiCGStab, 5
+// MergedPBiCGStab (merged/*.inl); the preconditioned ones use hier (from
+// ref_hier_create; PCG and RBiCGStab the identity when hier is null).
+// Returns the iteration count (-1 on bad input); hist as ref_bicgstab_d.
+int ref_solver_d(int method, void *hier, int64_t n, const int *rp, const int *ci, const double *v,
+                 const double *b, double *x, int nv, int max_iters, double abs_tol, double rel_tol,
+                 double *hist, int hist_cap);
+
 // (P)BiCGStab (method 0, as above), PCG (method 1, pcg.inl:48-160) or
 // RBiCGStab (method 2, rbicgstab.inl:48-225) in the reference's step order,
 // preconditioned by one multigrid cycle when nlev >= 2 (smoother & 15:

@@ -72,6 +72,8 @@ struct perf_info {
     void mem_write(int) {}
     void flop(int) {}
     void allreduce(int) {}
+    void start() {}
+    void stop() {}
 };
 
 // The log stream: discards what the reference prints.

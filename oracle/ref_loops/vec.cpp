@@ -451,6 +451,15 @@ struct Rbicgstab : KrylovBase {
     }
 };
 
+// one cycle of a created hierarchy (ref_hier_apply_d)
+struct HierApply {
+    const Hier *h; const double *b; double *x;
+    template <int NV> void run() {
+        if (h->reduced) h->cycle_reduced<NV>(x, b, h->mg_cycle);
+        else h->cycle<NV>(0, x, b, h->mg_cycle);
+    }
+};
+
 }  // namespace
 
 extern "C" {
@@ -503,6 +512,19 @@ static Hier *make_hier(int nlev, const int64_t *nrows, const int *const *arp, co
                        smoother & 15, (smoother >> 4) & 15, (smoother >> 8) & 1, {}, {}, {}, {}, {}, {}, {}};
     h->init();
     return h;
+}
+void *ref_hier_create(int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
+                      const double *const *av, const int *const *prp, const int *const *pci,
+                      const double *const *pv, const int *const *rrp, const int *const *rci,
+                      const double *const *rv, const int *nb, const int64_t *const *bp, double relax, int pre_it,
+                      int post_it, int smoother) {
+    return make_hier(nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax, pre_it, post_it,
+                     smoother);
+}
+void ref_hier_destroy(void *h) { delete (Hier *)h; }
+int ref_hier_apply_d(void *h, const double *b, double *x, int nv) {
+    HierApply f{(const Hier *)h, b, x};
+    return dispatch_nv(nv, f);
 }
 int ref_krylov_d(int method, int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
                  const double *const *av, const int *const *prp, const int *const *pci,

@@ -32,6 +32,7 @@ def lib(kind, build=True):
         return None
     L = C.CDLL(path(kind))
     i64, vp, ci_, cd = C.c_int64, C.c_void_p, C.c_int, C.c_double
+    PP = C.POINTER(C.c_void_p)
     for name in ("ref_csr_ax_y_d", "ref_csr_ax_y_f", "ref_csr_axpy_d", "ref_csr_axpy_f"):
         getattr(L, name).argtypes = [i64, vp, vp, vp, vp, vp, ci_]
     for name in ("ref_hsgs_d", "ref_hsgs_f"):
@@ -48,6 +49,11 @@ def lib(kind, build=True):
     L.ref_bicgstab_d.argtypes = [i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, vp, ci_]
     L.ref_dense_inverse_d.argtypes = [i64, vp, vp]
     L.ref_jacobi_d.argtypes = [i64, vp, vp, vp, vp, vp, vp, vp, ci_, ci_]
+    L.ref_hier_create.restype = vp
+    L.ref_hier_create.argtypes = [ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, ci_]
+    L.ref_hier_apply_d.argtypes = [vp, vp, vp, ci_]
+    L.ref_hier_destroy.argtypes = [vp]
+    L.ref_solver_d.argtypes = [ci_, vp, i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, vp, ci_]
     L.ref_chebyshev_d.argtypes = [i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, cd]
     L.ref_channel_cube_d.restype = C.c_int64
     L.ref_channel_cube_d.argtypes = [ci_, ci_, ci_, vp, vp, vp, vp, vp]
@@ -55,7 +61,6 @@ def lib(kind, build=True):
     L.ref_read_system_d.argtypes = [C.c_char_p, ci_, vp, vp, vp, vp, vp, vp]
     L.ref_cube_d.restype = C.c_int64
     L.ref_cube_d.argtypes = [i64, i64, i64, ci_, vp, vp, vp, vp]
-    PP = C.POINTER(C.c_void_p)
     L.ref_pbicgstab_amg_d.argtypes = [ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, vp, vp,
                                       ci_, ci_, cd, cd, vp, ci_]
     L.ref_krylov_d.argtypes = [ci_, ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, ci_, vp,
@@ -193,3 +198,32 @@ def read_system(L, path, nv=1):
     X = np.zeros((n, nv))
     L.ref_read_system_d(path.encode(), nv, None, p(rp), p(ci), p(v), p(B), p(X))
     return rp, ci, v, B, X
+
+
+SOLVERS = {"BiCGStab": 0, "PBiCGStab": 1, "PCG": 2, "RBiCGStab": 3, "MergedBiCGStab": 4, "MergedPBiCGStab": 5}
+
+
+def solver(L, method, rp, ci, v, B, levels=None, max_iters=1000, rel_tol=1e-8, relax=0.99, cycle="V"):
+    """The reference's own solver class `method` (compiled unchanged) from
+    x = 0 on (rp, ci, v), preconditioned by one multigrid cycle over
+    `levels` when given (the preconditioned methods; PCG and RBiCGStab use
+    the identity without levels).  Returns (x, iterations, history)."""
+    n, nv = B.shape
+    B = np.ascontiguousarray(B, np.float64)
+    h = None
+    keep = None
+    if levels is not None:
+        nrows, cast, nb, keep = _hier_args(levels, None)
+        h = L.ref_hier_create(len(levels), p(nrows), *cast[:9], p(nb), cast[9], relax, 1, 1,
+                              {"V": 0, "F": 1, "W": 2}[cycle] << 4)
+    try:
+        x = np.zeros_like(B)
+        hist = np.zeros((max_iters + 2, nv))
+        it = L.ref_solver_d(SOLVERS[method], h, n, p(rp), p(ci), p(v), p(B), p(x), nv, max_iters, 0.0, rel_tol,
+                            p(hist), max_iters + 2)
+    finally:
+        if h:
+            L.ref_hier_destroy(h)
+    if it < 0:
+        raise ValueError("unsupported nv or method")
+    return x, it, hist[: it + 1]

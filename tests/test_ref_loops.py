@@ -455,3 +455,47 @@ def test_chebyshev_smoother_matches_reference_solver(libs, order, nv):
     x = x0.copy()
     assert libs["contract"].ref_chebyshev_d(n, p(rp), p(ci), p(v), p(b), p(x), nv, order, frac, lo, hi) == 0
     assert np.array_equal(x, xo)
+
+
+@pytest.mark.parametrize("method", ["BiCGStab", "MergedBiCGStab"])
+@pytest.mark.parametrize("nv", [1, 4])
+def test_reference_bicgstab_classes_match_oracle(libs, seq_dot, method, nv):
+    """The reference's BiCGStab and MergedBiCGStab solver classes themselves
+    (bicgstab.inl, merged/merged_bicgstab.inl with the merged BLAS groups),
+    compiled unchanged against stand-ins for the solver framework, on the C1
+    system: the same iterations, residual history and x as the oracle, bit for
+    bit.  MergedBiCGStab forms the new direction as r + beta p - (beta omega) v
+    (blas_merged_bicgstab.inl), which rounds differently from BiCGStab's
+    r + (-omega beta) v + beta p: the oracle follows it under
+    set_merged_bicgstab, and the iteration counts of the two classes differ."""
+    rp, ci, v = poisson7(32)
+    B = np.random.default_rng(1234).uniform(-1, 1, (len(rp) - 1, nv))
+    orc.set_merged_bicgstab(method == "MergedBiCGStab")
+    try:
+        xo, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), None, 1000, 0.0, 1e-8)
+    finally:
+        orc.set_merged_bicgstab(False)
+    x, itr, h = reference_loops.solver(libs["contract"], method, rp, ci, v, B)
+    assert itr == it
+    assert np.array_equal(h, hist)
+    assert np.array_equal(x, xo)
+
+
+@pytest.mark.parametrize("method", ["PBiCGStab", "MergedPBiCGStab", "PCG", "RBiCGStab"])
+def test_reference_preconditioned_solver_classes_match_oracle(libs, seq_dot, method):
+    """The reference's PBiCGStab, MergedPBiCGStab, PCG and RBiCGStab classes
+    compiled unchanged, preconditioned by one V-cycle of its loops on the
+    oracle's AMG hierarchy (27-point 16^3, NV = 4): bit for bit the oracle's
+    solvers (MergedPBiCGStab forms its direction as PBiCGStab does)."""
+    rp, ci, v = orc.gen27(16)
+    levels = orc.amg_setup(rp, ci, v, mg_coarsening_type=10, mg_interpolation_type=6,
+                           mg_strength_threshold=0.25, mg_max_levels=6, mg_coarse_matrix_size=100)
+    B = np.random.default_rng(4).uniform(-1, 1, (len(rp) - 1, 4))
+    mg = orc.MG(levels)
+    fn = {"PBiCGStab": orc.pbicgstab, "MergedPBiCGStab": orc.pbicgstab, "PCG": orc.pcg,
+          "RBiCGStab": orc.rbicgstab}[method]
+    xo, it, hist, st, r0 = fn(rp, ci, v, B, np.zeros_like(B), mg, 200, 0.0, 1e-8)
+    x, itr, h = reference_loops.solver(libs["contract"], method, rp, ci, v, B, levels=levels, max_iters=200)
+    assert itr == it and it > 0
+    assert np.array_equal(h, hist)
+    assert np.array_equal(x, xo)
