@@ -731,10 +731,11 @@ def ref_loops(kind):
 
 
 def ref_sample(csr, B, levels, kind, iters=1):
-    """`iters` FP64 AMG-PBiCGStab iterations of the reference's compiled loops
-    (one process: Gauss-Seidel in its single-process order, inner products in
-    its single-core order) on the GPU plain form's hierarchy.  Returns
-    (seconds, x, history) or None when the library is absent."""
+    """`iters` FP64 AMG-PBiCGStab iterations of the reference's own PBiCGStab
+    class and loops, compiled unchanged (one process: Gauss-Seidel in its
+    single-process order, inner products in its single-core order), on the
+    GPU plain form's hierarchy.  Returns (seconds, x, history) or None when
+    the library is absent."""
     L = ref_loops(kind)
     if L is None:
         return None
@@ -743,7 +744,7 @@ def ref_sample(csr, B, levels, kind, iters=1):
     lv = [dict(l) for l in levels]
     lv[0]["A"] = (rp, ci, v)
     t0 = time.perf_counter()
-    x, it, h = reference_loops.pbicgstab_amg(L, lv, B, max_iters=iters, rel_tol=1e-8)
+    x, it, h = reference_loops.solver(L, "PBiCGStab", rp, ci, v, B, levels=lv, max_iters=iters, rel_tol=1e-8)
     return time.perf_counter() - t0, x, h
 
 
@@ -781,11 +782,12 @@ def reference_arm(args, rank, world):
     t0 = time.perf_counter()
     if L is not None:
         import reference_loops
-        x, it, hist = reference_loops.pbicgstab_amg(L, levels, B, max_iters=200, rel_tol=1e-8)
+        x, it, hist = reference_loops.solver(L, "PBiCGStab", rp, ci, v, B, levels=levels, max_iters=200,
+                                             rel_tol=1e-8)
         st = (np.sqrt(hist[-1]) <= 1e-8 * np.sqrt(hist[0])).astype(np.int32)
         thr, kind = 1, "reference"
-        what = ("the reference's own loop files (blas, blas2, inverse) compiled unchanged with its release flags, "
-                "in its PBiCGStab / V-cycle step order, one process")
+        what = ("the reference's own PBiCGStab class and loop files (blas, blas2, inverse) compiled unchanged "
+                "with its release flags, V-cycle in its step order, one process")
     else:
         mg = orc.MG(levels)
         x, it, hist, st, _ = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg=mg, max_iters=200, rel_tol=1e-8)
@@ -1032,7 +1034,8 @@ def main():
         if rs is not None:
             cpu = {"value": round(rs[0] * iters / NV * 1e3, 3), "unit": "ms/RHS", "cores": 1, "kind": "reference",
                    "sample": "1 FP64 AMG-PBiCGStab iteration of the same problem and hierarchy by the reference's "
-                             "own loop files compiled unchanged with its release flags, one process (%.1f s), "
+                             "own PBiCGStab class and loop files compiled unchanged with its release flags, one "
+                             "process (%.1f s), "
                              "x %d iterations / %d RHS" % (rs[0], iters, NV),
                    "oracle_port": {"value": round(sec * iters / NV * 1e3, 3), "cores": thr}}
         # full-size parity with the reference's own arithmetic: the GPU's first
