@@ -84,32 +84,16 @@ int ref_chebyshev_d(int64_t n, const int *rp, const int *ci, const double *v, co
 // Direct solver's setup)
 int ref_dense_inverse_d(int64_t n, const double *a, double *ainv);
 
-// BiCGStab in the step order of src/solvers/detail/bicgstab.inl:44-197, every
-// vector operation one of the reference's loops above; convergence as
-// convergence.h (per column: sqrt(res) <= max(abs_tol, rel_tol*sqrt(res0))).
-// hist receives (iterations + 1) x nv residual values (the squared norms the
-// solver tests); returns the iteration count, or -1 for an unsupported nv.
-int ref_bicgstab_d(int64_t n, const int *rp, const int *ci, const double *v, const double *b,
-                   double *x, int nv, int max_iters, double abs_tol, double rel_tol, double *hist,
-                   int hist_cap);
-
-// PBiCGStab (pbicgstab.inl:48-207) preconditioned by one V-cycle from zero
-// (mg.inl:186-280: HSGS pre- and post-smoothing with pre_it / post_it calls
-// of the hybrid sweep above on nb[l] blocks bp[l], residual, restriction by
-// R_l, recursion, the coarsest level by the reference's Gauss-Jordan inverse
-// and dense product, prolongation by y += P_l x_H).  Level l has nrows[l]
-// rows; P_l is nrows[l] x nrows[l+1], R_l its transpose.  Returns the
-// iteration count (-1: unsupported nv or fewer than two levels).
-int ref_pbicgstab_amg_d(int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
-                        const double *const *av, const int *const *prp, const int *const *pci,
-                        const double *const *pv, const int *const *rrp, const int *const *rci,
-                        const double *const *rv, const int *nb, const int64_t *const *bp, double relax,
-                        int pre_it, int post_it, const double *b, double *x, int nv, int max_iters,
-                        double abs_tol, double rel_tol, double *hist, int hist_cap);
-
-// The multigrid preconditioner of the drivers as an object: created from a
-// hierarchy (arguments as ref_krylov_d), applied as one cycle from the x given
-// (MultiGrid::solve with max_iters 1 as a preconditioner), destroyed.
+// The multigrid preconditioner of the solver classes: one cycle of the
+// reference's loops in its MG_cycle order (mg.inl:186-280) over a hierarchy
+// given per level l: nrows[l] rows, the operator (arp, aci, av), P_l
+// (nrows[l] x nrows[l+1]: prp, pci, pv) and R_l = P_l^T (rrp, rci, rv), hybrid
+// blocks nb[l] with offsets bp[l]; HSGS (smoother & 15 = 0, the sweep above)
+// or Jacobi (1) with relax and pre_it / post_it sweeps, (smoother >> 4) & 15 =
+// mg_cycle (0 V, 1 F, 2 W), bit 8 = mg_reduced_precision (FP32 below the
+// first level, HSGS only); the coarsest level by the reference's Gauss-Jordan
+// inverse (FP64, or FP32 when reduced) and dense product.  Applied as one
+// cycle from the x given (MultiGrid::solve with max_iters 1), then destroyed.
 void *ref_hier_create(int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
                       const double *const *av, const int *const *prp, const int *const *pci,
                       const double *const *pv, const int *const *rrp, const int *const *rci,
@@ -122,24 +106,11 @@ void ref_hier_destroy(void *h);
 // method 0 BiCGStab (bicgstab.inl), 1 PBiCGStab (pbicgstab.inl), 2 PCG
 // (pcg.inl), 3 RBiCGStab (rbicgstab.inl), 4 MergedBiCGStab, 5
 // MergedPBiCGStab (merged/*.inl); the preconditioned ones use hier (from
-// ref_hier_create; PCG and RBiCGStab the identity when hier is null).
-// Returns the iteration count (-1 on bad input); hist as ref_bicgstab_d.
+// ref_hier_create; PCG and RBiCGStab the identity when hier is null), from
+// x = 0, to max(abs_tol, rel_tol * initial residual) per column.  hist
+// receives the (iterations + 1) x nv squared residual norms the solver
+// checks; returns the iteration count (-1 on bad input).
 int ref_solver_d(int method, void *hier, int64_t n, const int *rp, const int *ci, const double *v,
                  const double *b, double *x, int nv, int max_iters, double abs_tol, double rel_tol,
                  double *hist, int hist_cap);
-
-// (P)BiCGStab (method 0, as above), PCG (method 1, pcg.inl:48-160) or
-// RBiCGStab (method 2, rbicgstab.inl:48-225) in the reference's step order,
-// preconditioned by one multigrid cycle when nlev >= 2 (smoother & 15:
-// 0 HSGS, 1 Jacobi, pre_it / post_it sweeps; (smoother >> 4) & 15: mg_cycle,
-// 0 V, 1 F, 2 W; bit 8: mg_reduced_precision, MG_cycle<double, float> on the
-// first level and FP32 below, HSGS only), else by the identity (M^{-1} r = r;
-// nrows[0], arp[0], aci[0], av[0] give the operator; for method 0 no
-// preconditioner at all).  Returns the iteration count, -1 on bad input.
-int ref_krylov_d(int method, int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
-                 const double *const *av, const int *const *prp, const int *const *pci,
-                 const double *const *pv, const int *const *rrp, const int *const *rci,
-                 const double *const *rv, const int *nb, const int64_t *const *bp, double relax, int pre_it,
-                 int post_it, int smoother, const double *b, double *x, int nv, int max_iters, double abs_tol,
-                 double rel_tol, double *hist, int hist_cap);
 }

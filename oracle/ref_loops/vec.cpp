@@ -1,5 +1,7 @@
-// BLAS-1 loops of the reference, compiled unchanged with its generic release
-// flags, and BiCGStab in the reference's step order over them.
+// BLAS-1 loops and the dense inverse of the reference, compiled unchanged
+// (with the generic release flags in the generic and contract builds), and
+// the multigrid cycle of the reference's loops in its MG_cycle order, the
+// preconditioner of the solver classes in krylov.cpp.
 #include <algorithm>
 #include <cstring>
 #include <memory>
@@ -34,33 +36,7 @@ struct Blas {
 
 int run_blas(Blas f) { return dispatch_nv(f.nv, f); }
 
-// Convergence as convergence.h:85-130 + stats.h:195-245: squared residual
-// norms per column, a column freezes once sqrt(res) <= max(abs, rel*sqrt(res0)).
-struct Conv {
-    std::vector<double> res0, res;
-    std::vector<int> done;
-    double abs_tol, rel_tol;
-    double *hist; int cap, cnt, nv;
-    void push() {
-        if (hist && cnt < cap) std::memcpy(hist + (size_t)cnt * nv, res.data(), sizeof(double) * nv);
-        cnt++;
-    }
-    void update(const double *r) {
-        for (int k = 0; k < nv; ++k) if (!done[k]) res[k] = r[k];
-        push();
-    }
-    bool check(double *iconv) {
-        bool all = true;
-        for (int k = 0; k < nv; ++k) {
-            if (done[k]) continue;
-            if (std::sqrt(res[k]) > std::max(abs_tol, rel_tol * std::sqrt(res0[k]))) all = false;
-            else { done[k] = 1; iconv[k] = 0.0; }
-        }
-        return all;
-    }
-};
-
-// The AMG hierarchy handed to the PBiCGStab driver: per level the operator,
+// The AMG hierarchy of the multigrid preconditioner: per level the operator,
 // its inverse diagonal (csr_matrix.h:344-349), P and R = P^T, the hybrid
 // blocks; the coarsest level's inverse from the reference's own Gauss-Jordan
 // routine (Direct::init, direct.inl:31-45).
@@ -212,245 +188,6 @@ struct Hier {
     }
 };
 
-// (P)BiCGStab in the step order of pbicgstab.inl:48-207 (bicgstab.inl:44-197
-// without a preconditioner: the preconditioned vectors are p and s).
-struct Bicgstab {
-    int64_t n; const int *rp, *ci; const double *v, *b; double *x; int nv, max_iters;
-    double abs_tol, rel_tol; double *hist; int cap;
-    const Hier *mg;
-    int iters;
-    template <int NV> void run() {
-        typedef double F;
-        size_t sz = (size_t)n * NV;
-        std::vector<F> r0(sz, 0.0), r(sz, 0.0), p(sz, 0.0), vv(sz, 0.0), s(sz, 0.0), t(sz, 0.0),
-            p_(sz, 0.0), s_(sz, 0.0);
-        vector R0 = block(r0.data(), n, NV), R = block(r.data(), n, NV), P = block(p.data(), n, NV),
-               V = block(vv.data(), n, NV), S = block(s.data(), n, NV), T = block(t.data(), n, NV),
-               P_ = block(p_.data(), n, NV), S_ = block(s_.data(), n, NV);
-        vector X = block(x, n, NV), B = block(b, n, NV);
-        std::vector<F> one(NV, 1.0), mone(NV, -1.0), ic(NV, 1.0);
-        std::vector<F> rho(NV), res(NV), s1(NV), s2(NV), s3(NV), s4(NV), al(NV), be(NV), om(NV),
-            alc(NV), omc(NV);
-        vector a1 = scalars(one.data(), NV), a_1 = scalars(mone.data(), NV),
-               iconv = scalars(ic.data(), NV), Rho = scalars(rho.data(), NV),
-               Res = scalars(res.data(), NV), S1 = scalars(s1.data(), NV),
-               S2 = scalars(s2.data(), NV), S3 = scalars(s3.data(), NV),
-               S4 = scalars(s4.data(), NV), Al = scalars(al.data(), NV),
-               Be = scalars(be.data(), NV), Om = scalars(om.data(), NV),
-               Alc = scalars(alc.data(), NV), Omc = scalars(omc.data(), NV);
-        auto Ax = [&](const vector &in, vector &out) {
-            ref_csr_ax_y_d(n, rp, ci, v, in.get_aligned_ptr<F>(), out.get_aligned_ptr<F>(), NV);
-        };
-        // M^{-1}: one V-cycle from zero (MultiGrid::solve with max_iters 1)
-        auto precond = [&](vector &out, const vector &in) {
-            blas::set_const<F, NV>(out, 0.0, true);
-            if (mg->reduced)
-                mg->cycle_reduced<NV>(out.get_aligned_ptr<F>(), in.get_aligned_ptr<F>(), mg->mg_cycle);
-            else
-                mg->cycle<NV>(0, out.get_aligned_ptr<F>(), in.get_aligned_ptr<F>(), mg->mg_cycle);
-        };
-        Conv cv{std::vector<double>(NV), std::vector<double>(NV), std::vector<int>(NV, 0),
-                abs_tol, rel_tol, hist, cap, 0, NV};
-        // 1-2. r0 = b - A x (solver.h:183-190), rho = (r0, r0)
-        Ax(X, R0);
-        blas::axpby<F, NV>(1.0, B, -1.0, R0);
-        blas::dot<F, NV>(R0, R0, Rho);
-        for (int k = 0; k < NV; ++k) cv.res0[k] = rho[k];
-        cv.update(rho.data());
-        if (cv.check(ic.data())) { iters = 0; return; }
-        blas::copy<F, NV>(R0, R);
-        blas::copy<F, NV>(R0, P);
-        vector &PP = mg ? P_ : P, &SS = mg ? S_ : S;
-        int it = 0;
-        for (bool last = false; !last;) {
-            it++;
-            if (it >= max_iters) last = true;
-            if (mg) precond(P_, P);                              // 5*
-            Ax(PP, V);                                            // 5
-            blas::dot<F, NV>(V, R0, S1);                          // 6
-            blas::xdivy_z<F, NV>(Rho, S1, Al);
-            blas::scal<F, NV>(a_1, Al);                           // 7
-            blas::axpby_z<F, NV>(a1, R, Al, V, S);
-            blas::scal<F, NV>(a_1, Al);
-            if (mg) precond(S_, S);                              // 8*
-            Ax(SS, T);                                            // 8
-            blas::dot<F, NV>(T, S, S2);                           // 9
-            blas::dot<F, NV>(T, T, S3);
-            blas::dot<F, NV>(S, S, S4);
-            blas::xdivy_z<F, NV>(S2, S3, Om);
-            blas::ax_y<F, NV>(iconv, Al, Alc);                    // 10
-            blas::ax_y<F, NV>(iconv, Om, Omc);
-            blas::axpbypcz<F, NV>(Alc, PP, Omc, SS, a1, X);
-            blas::ax_y<F, NV>(Om, S2, Res);                       // 12
-            blas::axpby<F, NV>(a1, S4, a_1, Res);
-            cv.update(res.data());
-            if (cv.check(ic.data())) break;
-            blas::scal<F, NV>(a_1, Om);                           // 11
-            blas::axpby_z<F, NV>(a1, S, Om, T, R);
-            blas::scal<F, NV>(a_1, Om);
-            blas::dot<F, NV>(R, R0, S1);                          // 15
-            blas::xdivy_z<F, NV>(S1, Rho, S2);                    // 16
-            blas::xdivy_z<F, NV>(Al, Om, S3);
-            blas::ax_y<F, NV>(S2, S3, Be);
-            blas::copy<F, NV>(S1, Rho);
-            blas::ax_y<F, NV>(Om, Be, S1);                        // 17
-            blas::scal<F, NV>(a_1, S1);
-            blas::axpbypcz<F, NV>(a1, R, S1, V, Be, P);
-        }
-        iters = it;
-    }
-};
-
-// Shared state of the PCG and RBiCGStab drivers: operator, optional V-cycle
-// preconditioner (identity without one: M^{-1} r = r), convergence.
-struct KrylovBase {
-    int64_t n; const int *rp, *ci; const double *v, *b; double *x; int nv, max_iters;
-    double abs_tol, rel_tol; double *hist; int cap;
-    const Hier *mg;
-    int iters;
-    template <int NV> void Ax(const vector &in, vector &out) const {
-        ref_csr_ax_y_d(n, rp, ci, v, in.get_aligned_ptr<double>(), out.get_aligned_ptr<double>(), NV);
-    }
-    // set_const(out, 0); precond->solve(out, in)
-    template <int NV> void precond(vector &out, const vector &in) const {
-        blas::set_const<double, NV>(out, 0.0, true);
-        if (mg && mg->reduced)
-            mg->cycle_reduced<NV>(out.get_aligned_ptr<double>(), in.get_aligned_ptr<double>(), mg->mg_cycle);
-        else if (mg)
-            mg->cycle<NV>(0, out.get_aligned_ptr<double>(), in.get_aligned_ptr<double>(), mg->mg_cycle);
-        else
-            blas::copy<double, NV>(in, out);
-    }
-};
-
-// PCG in the step order of pcg.inl:48-160.
-struct Pcg : KrylovBase {
-    explicit Pcg(const KrylovBase &k) : KrylovBase(k) {}
-    template <int NV> void run() {
-        typedef double F;
-        size_t sz = (size_t)n * NV;
-        std::vector<F> r(sz, 0.0), z(sz, 0.0), p(sz, 0.0), ap(sz, 0.0);
-        vector R = block(r.data(), n, NV), Z = block(z.data(), n, NV), P = block(p.data(), n, NV),
-               AP = block(ap.data(), n, NV), X = block(x, n, NV), B = block(b, n, NV);
-        std::vector<F> one(NV, 1.0), mone(NV, -1.0), ic(NV, 1.0), s1(NV), s2(NV), s3(NV), al(NV), be(NV),
-            res(NV), alc(NV);
-        vector a1 = scalars(one.data(), NV), a_1 = scalars(mone.data(), NV), iconv = scalars(ic.data(), NV),
-               S1 = scalars(s1.data(), NV), S2 = scalars(s2.data(), NV), S3 = scalars(s3.data(), NV),
-               Al = scalars(al.data(), NV), Be = scalars(be.data(), NV), Res = scalars(res.data(), NV),
-               Alc = scalars(alc.data(), NV);
-        Conv cv{std::vector<double>(NV), std::vector<double>(NV), std::vector<int>(NV, 0),
-                abs_tol, rel_tol, hist, cap, 0, NV};
-        // r = b - A x, res0 = (r, r) (stats.h:208-219)
-        Ax<NV>(X, R);
-        blas::axpby<F, NV>(1.0, B, -1.0, R);
-        blas::dot<F, NV>(R, R, Res);
-        for (int k = 0; k < NV; ++k) cv.res0[k] = res[k];
-        cv.update(res.data());
-        if (cv.check(ic.data())) { iters = 0; return; }
-        precond<NV>(Z, R);
-        blas::copy<F, NV>(Z, P);
-        int it = 0;
-        for (bool last = false; !last;) {
-            it++;
-            if (it >= max_iters) last = true;
-            Ax<NV>(P, AP);
-            blas::dot<F, NV>(R, Z, S1);
-            blas::dot<F, NV>(P, AP, S2);
-            blas::xdivy_z<F, NV>(S1, S2, Al);
-            blas::ax_y<F, NV>(iconv, Al, Alc);
-            blas::axpby<F, NV>(Alc, P, a1, X);
-            blas::scal<F, NV>(a_1, Al);
-            blas::axpby<F, NV>(Al, AP, a1, R);
-            precond<NV>(Z, R);
-            blas::dot<F, NV>(R, Z, S3);
-            blas::xdivy_z<F, NV>(S3, S1, Be);
-            blas::axpby<F, NV>(a1, Z, Be, P);
-            blas::dot<F, NV>(R, R, Res);
-            cv.update(res.data());
-            if (cv.check(ic.data())) break;
-        }
-        iters = it;
-    }
-};
-
-// RBiCGStab in the step order of rbicgstab.inl:48-225 (the allreduce that
-// the reference overlaps with the preconditioner changes no value on one
-// process).
-struct Rbicgstab : KrylovBase {
-    explicit Rbicgstab(const KrylovBase &k) : KrylovBase(k) {}
-    template <int NV> void run() {
-        typedef double F;
-        size_t sz = (size_t)n * NV;
-        std::vector<F> r0(sz, 0.0), r(sz, 0.0), z(sz, 0.0), v_(sz, 0.0), vv(sz, 0.0), s(sz, 0.0),
-            t_(sz, 0.0), t(sz, 0.0);
-        vector R0 = block(r0.data(), n, NV), R = block(r.data(), n, NV), Z = block(z.data(), n, NV),
-               V_ = block(v_.data(), n, NV), V = block(vv.data(), n, NV), S = block(s.data(), n, NV),
-               T_ = block(t_.data(), n, NV), T = block(t.data(), n, NV), X = block(x, n, NV),
-               B = block(b, n, NV);
-        std::vector<F> one(NV, 1.0), mone(NV, -1.0), ic(NV, 1.0), rho(NV), delta(NV), al(NV), om(NV),
-            theta(NV), phi(NV), psi(NV), eta(NV), res(NV), alc(NV), omc(NV), be(NV), tmp(NV);
-        vector a1 = scalars(one.data(), NV), a_1 = scalars(mone.data(), NV), iconv = scalars(ic.data(), NV),
-               Rho = scalars(rho.data(), NV), Delta = scalars(delta.data(), NV), Al = scalars(al.data(), NV),
-               Om = scalars(om.data(), NV), Theta = scalars(theta.data(), NV), Phi = scalars(phi.data(), NV),
-               Psi = scalars(psi.data(), NV), Eta = scalars(eta.data(), NV), Res = scalars(res.data(), NV),
-               Alc = scalars(alc.data(), NV), Omc = scalars(omc.data(), NV), Be = scalars(be.data(), NV),
-               Tmp = scalars(tmp.data(), NV);
-        Conv cv{std::vector<double>(NV), std::vector<double>(NV), std::vector<int>(NV, 0),
-                abs_tol, rel_tol, hist, cap, 0, NV};
-        Ax<NV>(X, R0);                                             // 1
-        blas::axpby<F, NV>(1.0, B, -1.0, R0);
-        blas::dot<F, NV>(R0, R0, Rho);                            // 2
-        for (int k = 0; k < NV; ++k) cv.res0[k] = rho[k];
-        cv.update(rho.data());
-        if (cv.check(ic.data())) { iters = 0; return; }
-        blas::copy<F, NV>(R0, R);
-        precond<NV>(Z, R0);                                       // 3
-        blas::copy<F, NV>(Z, V_);                                 // 4
-        int it = 0;
-        for (bool last = false; !last;) {
-            it++;
-            if (it >= max_iters) last = true;
-            Ax<NV>(V_, V);                                        // 6
-            blas::dot<F, NV>(V, R0, Delta);                       // 7
-            precond<NV>(S, V);                                    // 8
-            blas::xdivy_z<F, NV>(Rho, Delta, Al);                 // 9
-            blas::scal<F, NV>(a_1, Al);                           // 10
-            blas::axpby_z<F, NV>(a1, Z, Al, S, T_);
-            blas::scal<F, NV>(a_1, Al);
-            Ax<NV>(T_, T);                                        // 11
-            blas::scal<F, NV>(a_1, Al);                           // 12
-            blas::axpby<F, NV>(Al, V, a1, R);
-            blas::scal<F, NV>(a_1, Al);
-            blas::dot<F, NV>(T, R, Theta);                        // 13
-            blas::dot<F, NV>(T, T, Phi);
-            blas::dot<F, NV>(T, R0, Psi);
-            blas::dot<F, NV>(R, R, Eta);
-            precond<NV>(Z, T);                                    // 14
-            blas::xdivy_z<F, NV>(Theta, Phi, Om);                 // 15
-            blas::scal<F, NV>(a_1, Om);                           // 16
-            blas::axpby<F, NV>(Om, T, a1, R);
-            blas::scal<F, NV>(a_1, Om);
-            blas::ax_y<F, NV>(Om, Theta, Res);                    // 17
-            blas::axpby<F, NV>(a1, Eta, a_1, Res);
-            blas::ax_y<F, NV>(iconv, Al, Alc);                    // 23
-            blas::ax_y<F, NV>(iconv, Om, Omc);
-            blas::axpbypcz<F, NV>(Alc, V_, Omc, T_, a1, X);
-            cv.update(res.data());
-            if (cv.check(ic.data())) break;
-            blas::ax_y<F, NV>(Om, Psi, Rho);                      // 21
-            blas::scal<F, NV>(a_1, Rho);
-            blas::ax_y<F, NV>(Delta, Om, Tmp);                    // 22
-            blas::xdivy_z<F, NV>(Rho, Tmp, Be);
-            blas::scal<F, NV>(a_1, Om);                           // 24 (omega stays negated)
-            blas::axpby<F, NV>(a1, T_, Om, Z);
-            blas::ax_y<F, NV>(Om, Be, Delta);                     // 25
-            blas::scal<F, NV>(a_1, Om);
-            blas::axpbypcz<F, NV>(a1, Z, Delta, S, Be, V_);
-        }
-        iters = it;
-    }
-};
-
 // one cycle of a created hierarchy (ref_hier_apply_d)
 struct HierApply {
     const Hier *h; const double *b; double *x;
@@ -495,13 +232,6 @@ int ref_dense_inverse_d(int64_t n, const double *a, double *ainv) {
     std::memcpy(ainv, mi.val.get_aligned_ptr<double>(), sizeof(double) * (size_t)(n * n));
     return 0;
 }
-int ref_bicgstab_d(int64_t n, const int *rp, const int *ci, const double *v, const double *b,
-                   double *x, int nv, int max_iters, double abs_tol, double rel_tol, double *hist,
-                   int hist_cap) {
-    Bicgstab f{n, rp, ci, v, b, x, nv, max_iters, abs_tol, rel_tol, hist, hist_cap, nullptr, 0};
-    if (dispatch_nv(nv, f)) return -1;
-    return f.iters;
-}
 static Hier *make_hier(int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
                        const double *const *av, const int *const *prp, const int *const *pci,
                        const double *const *pv, const int *const *rrp, const int *const *rci,
@@ -525,46 +255,5 @@ void ref_hier_destroy(void *h) { delete (Hier *)h; }
 int ref_hier_apply_d(void *h, const double *b, double *x, int nv) {
     HierApply f{(const Hier *)h, b, x};
     return dispatch_nv(nv, f);
-}
-int ref_krylov_d(int method, int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
-                 const double *const *av, const int *const *prp, const int *const *pci,
-                 const double *const *pv, const int *const *rrp, const int *const *rci,
-                 const double *const *rv, const int *nb, const int64_t *const *bp, double relax, int pre_it,
-                 int post_it, int smoother, const double *b, double *x, int nv, int max_iters, double abs_tol,
-                 double rel_tol, double *hist, int hist_cap) {
-    std::unique_ptr<Hier> h(make_hier(nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax,
-                                      pre_it, post_it, smoother));
-    KrylovBase kb{nrows[0], arp[0], aci[0], av[0], b, x, nv, max_iters, abs_tol, rel_tol, hist, hist_cap,
-                  h.get(), 0};
-    if (method == 0) {
-        Bicgstab f{kb.n, kb.rp, kb.ci, kb.v, b, x, nv, max_iters, abs_tol, rel_tol, hist, hist_cap, h.get(), 0};
-        if (dispatch_nv(nv, f)) return -1;
-        return f.iters;
-    }
-    if (method == 1) {
-        Pcg f(kb);
-        if (dispatch_nv(nv, f)) return -1;
-        return f.iters;
-    }
-    if (method == 2) {
-        Rbicgstab f(kb);
-        if (dispatch_nv(nv, f)) return -1;
-        return f.iters;
-    }
-    return -1;
-}
-int ref_pbicgstab_amg_d(int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
-                        const double *const *av, const int *const *prp, const int *const *pci,
-                        const double *const *pv, const int *const *rrp, const int *const *rci,
-                        const double *const *rv, const int *nb, const int64_t *const *bp, double relax,
-                        int pre_it, int post_it, const double *b, double *x, int nv, int max_iters,
-                        double abs_tol, double rel_tol, double *hist, int hist_cap) {
-    if (nlev < 2) return -1;
-    Hier h{nlev, nrows, arp, aci, av, prp, pci, pv, rrp, rci, rv, nb, bp, relax, pre_it, post_it, 0, 0, 0,
-           {}, {}, {}, {}, {}, {}, {}};
-    h.init();
-    Bicgstab f{nrows[0], arp[0], aci[0], av[0], b, x, nv, max_iters, abs_tol, rel_tol, hist, hist_cap, &h, 0};
-    if (dispatch_nv(nv, f)) return -1;
-    return f.iters;
 }
 }

@@ -4,9 +4,10 @@ oracle/build_ref_loops.py from the reference's own loop files): test and
 benchmark-baseline infrastructure, never part of the product.
 
 lib(kind) loads one build (None when it was not built: the reference tree
-was absent and no prebuilt library travelled with the repository);
-pbicgstab_amg() runs a whole AMG-PBiCGStab solve in the reference's step
-order over its compiled loops (see ref_loops.h)."""
+was absent and no prebuilt library travelled with the repository); solver()
+runs one of the reference's own Krylov solver classes over its compiled
+loops, the generators and the reader return the reference's problems (see
+ref_loops.h)."""
 import ctypes as C
 import os
 
@@ -46,7 +47,6 @@ def lib(kind, build=True):
     L.ref_xdivy_z_d.argtypes = [i64, ci_, vp, vp, vp]
     L.ref_ax_y_d.argtypes = [i64, ci_, vp, vp, vp]
     L.ref_scal_d.argtypes = [i64, ci_, vp, vp]
-    L.ref_bicgstab_d.argtypes = [i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, vp, ci_]
     L.ref_dense_inverse_d.argtypes = [i64, vp, vp]
     L.ref_jacobi_d.argtypes = [i64, vp, vp, vp, vp, vp, vp, vp, ci_, ci_]
     L.ref_hier_create.restype = vp
@@ -61,10 +61,6 @@ def lib(kind, build=True):
     L.ref_read_system_d.argtypes = [C.c_char_p, ci_, vp, vp, vp, vp, vp, vp]
     L.ref_cube_d.restype = C.c_int64
     L.ref_cube_d.argtypes = [i64, i64, i64, ci_, vp, vp, vp, vp]
-    L.ref_pbicgstab_amg_d.argtypes = [ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, vp, vp,
-                                      ci_, ci_, cd, cd, vp, ci_]
-    L.ref_krylov_d.argtypes = [ci_, ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, ci_, vp,
-                               vp, ci_, ci_, cd, cd, vp, ci_]
     _libs[kind] = L
     return L
 
@@ -81,17 +77,6 @@ def transpose(rp, ci, v, ncols):
     rrp = np.zeros(ncols + 1, np.int32)
     np.cumsum(np.bincount(ci, minlength=ncols), out=rrp[1:])
     return rrp, np.ascontiguousarray(rows[order]), np.ascontiguousarray(v[order])
-
-
-def bicgstab(L, rp, ci, v, B, max_iters=1000, rel_tol=1e-8):
-    """Unpreconditioned BiCGStab from x = 0: (x, iterations, history)."""
-    n, nv = B.shape
-    x = np.zeros_like(B)
-    h = np.zeros((max_iters + 2, nv))
-    it = L.ref_bicgstab_d(n, p(rp), p(ci), p(v), p(B), p(x), nv, max_iters, 0.0, rel_tol, p(h), max_iters + 2)
-    if it < 0:
-        raise ValueError("unsupported nv")
-    return x, it, h[: it + 1]
 
 
 def _ptrs(arrs):
@@ -116,46 +101,6 @@ def _hier_args(levels, blocks):
     cast = [C.cast(t, PP) for t in tabs]
     keep = (nrows, R, cols, blocks, nb, tabs)
     return nrows, cast, nb, keep
-
-
-def pbicgstab_amg(L, levels, B, blocks=None, max_iters=200, rel_tol=1e-8, relax=0.99, pre_it=1, post_it=1):
-    """AMG-PBiCGStab from x = 0 over `levels` (dicts with n, A, P, ncP as the
-    oracle's setup or the library's hierarchy export gives them); blocks[l]:
-    hybrid block row offsets of level l (default: one block per level, the
-    single-process sweep).  Returns (x, iterations, history)."""
-    nrows, cast, nb, keep = _hier_args(levels, blocks)
-    n, nv = B.shape
-    B = np.ascontiguousarray(B, np.float64)
-    x = np.zeros_like(B)
-    h = np.zeros((max_iters + 2, nv))
-    it = L.ref_pbicgstab_amg_d(len(levels), p(nrows), *cast[:9], p(nb), cast[9], relax, pre_it, post_it, p(B),
-                               p(x), nv, max_iters, 0.0, rel_tol, p(h), max_iters + 2)
-    if it < 0:
-        raise ValueError("unsupported nv or hierarchy")
-    return x, it, h[: it + 1]
-
-
-def krylov(L, method, levels, B, blocks=None, max_iters=200, rel_tol=1e-8, relax=0.99, smoother="HSGS",
-           sweeps=1, cycle="V", reduced=False):
-    """PBiCGStab ("PBiCGStab"), PCG ("PCG") or RBiCGStab ("RBiCGStab") from
-    x = 0, preconditioned by one multigrid cycle ("V", "F" or "W") over
-    `levels` (HSGS or Jacobi smoothing, `sweeps` before and after) when it
-    has two or more levels (reduced: mg_reduced_precision, the levels below
-    the first and the first level's transfers in FP32, HSGS only), else
-    by the identity (levels = [the operator's level]).  Returns (x,
-    iterations, history)."""
-    nrows, cast, nb, keep = _hier_args(levels, blocks)
-    n, nv = B.shape
-    B = np.ascontiguousarray(B, np.float64)
-    x = np.zeros_like(B)
-    h = np.zeros((max_iters + 2, nv))
-    code = {"HSGS": 0, "Jacobi": 1}[smoother] | ({"V": 0, "F": 1, "W": 2}[cycle] << 4) | (int(reduced) << 8)
-    it = L.ref_krylov_d({"PBiCGStab": 0, "PCG": 1, "RBiCGStab": 2}[method], len(levels), p(nrows), *cast[:9],
-                        p(nb), cast[9], relax, sweeps, sweeps, code, p(B), p(x), nv, max_iters, 0.0, rel_tol, p(h),
-                        max_iters + 2)
-    if it < 0:
-        raise ValueError("unsupported nv or method")
-    return x, it, h[: it + 1]
 
 
 def channel_cube(L, scale, nv, const_rhs=False):
@@ -203,19 +148,26 @@ def read_system(L, path, nv=1):
 SOLVERS = {"BiCGStab": 0, "PBiCGStab": 1, "PCG": 2, "RBiCGStab": 3, "MergedBiCGStab": 4, "MergedPBiCGStab": 5}
 
 
-def solver(L, method, rp, ci, v, B, levels=None, max_iters=1000, rel_tol=1e-8, relax=0.99, cycle="V"):
-    """The reference's own solver class `method` (compiled unchanged) from
-    x = 0 on (rp, ci, v), preconditioned by one multigrid cycle over
-    `levels` when given (the preconditioned methods; PCG and RBiCGStab use
-    the identity without levels).  Returns (x, iterations, history)."""
+def solver(L, method, rp, ci, v, B, levels=None, max_iters=1000, rel_tol=1e-8, relax=0.99, cycle="V",
+           smoother="HSGS", sweeps=1, reduced=False, blocks=None):
+    """The reference's own solver class `method` (one of SOLVERS, compiled
+    unchanged) from x = 0 on (rp, ci, v).  With `levels` (dicts with n, A, P,
+    ncP as the oracle's setup or the library's hierarchy export gives them)
+    the preconditioned methods apply one multigrid cycle of the reference's
+    loops in its MG_cycle order: `cycle` "V", "F" or "W", `smoother` "HSGS"
+    (on the hybrid blocks `blocks[l]`, default one block per level) or
+    "Jacobi" with `sweeps` before and after, `reduced` for
+    mg_reduced_precision (FP32 below the first level, HSGS only).  Without
+    levels PCG and RBiCGStab use the identity.  Returns (x, iterations,
+    history of the checked squared residual norms)."""
     n, nv = B.shape
     B = np.ascontiguousarray(B, np.float64)
     h = None
     keep = None
     if levels is not None:
-        nrows, cast, nb, keep = _hier_args(levels, None)
-        h = L.ref_hier_create(len(levels), p(nrows), *cast[:9], p(nb), cast[9], relax, 1, 1,
-                              {"V": 0, "F": 1, "W": 2}[cycle] << 4)
+        nrows, cast, nb, keep = _hier_args(levels, blocks)
+        code = {"HSGS": 0, "Jacobi": 1}[smoother] | ({"V": 0, "F": 1, "W": 2}[cycle] << 4) | (int(reduced) << 8)
+        h = L.ref_hier_create(len(levels), p(nrows), *cast[:9], p(nb), cast[9], relax, sweeps, sweeps, code)
     try:
         x = np.zeros_like(B)
         hist = np.zeros((max_iters + 2, nv))

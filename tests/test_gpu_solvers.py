@@ -90,7 +90,7 @@ def test_bicgstab_c1_sequential_dot_matches_reference_order(gpu, nv):
     assert np.array_equal(X, xo)
     L = reference_loops.lib("contract", build=False)
     if L is not None:
-        xr, itr, hr = reference_loops.bicgstab(L, rp, ci, v, B, 1000, 1e-8)
+        xr, itr, hr = reference_loops.solver(L, "BiCGStab", rp, ci, v, B, max_iters=1000, rel_tol=1e-8)
         assert itr == s.iters()[0]
         assert np.array_equal(hr, s.history())
         assert np.array_equal(xr, X)

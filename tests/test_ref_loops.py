@@ -249,7 +249,7 @@ def seq_dot():
 
 
 def _ref_bicgstab(L, rp, ci, v, B, max_iters=1000, rel_tol=1e-8):
-    return reference_loops.bicgstab(L, rp, ci, v, B, max_iters, rel_tol)
+    return reference_loops.solver(L, "BiCGStab", rp, ci, v, B, max_iters=max_iters, rel_tol=rel_tol)
 
 
 @pytest.mark.parametrize("nv", [1, 4])
@@ -313,7 +313,8 @@ def test_amg_pbicgstab_solve_matches_reference_loops(libs, seq_dot, block_rows):
         n = lv["n"]
         br = block_rows if block_rows and block_rows < n else 0
         blocks.append((np.append(np.arange(0, n, br), n) if br else np.array([0, n])).astype(np.int64))
-    x, itr, h = reference_loops.pbicgstab_amg(libs["contract"], levels, B, blocks=blocks)
+    x, itr, h = reference_loops.solver(libs["contract"], "PBiCGStab", rp, ci, v, B, levels=levels, blocks=blocks,
+                                       max_iters=200)
     assert itr == it and it > 0
     assert np.array_equal(h, hist)
     assert np.array_equal(x, xo)
@@ -338,7 +339,8 @@ def test_pcg_and_rbicgstab_solves_match_reference_loops(libs, seq_dot, method, p
         mg = None
     fn = orc.pcg if method == "PCG" else orc.rbicgstab
     xo, it, hist, st, r0 = fn(rp, ci, v, B, np.zeros_like(B), mg, 500, 0.0, 1e-8)
-    x, itr, h = reference_loops.krylov(libs["contract"], method, levels, B, max_iters=500)
+    x, itr, h = reference_loops.solver(libs["contract"], method, rp, ci, v, B, levels=levels if precond else None,
+                                       max_iters=500)
     assert itr == it and it > 0
     assert np.array_equal(h, hist)
     assert np.array_equal(x, xo)
@@ -354,7 +356,8 @@ def test_amg_pbicgstab_jacobi_smoothing_matches_reference_loops(libs, seq_dot):
     B = np.random.default_rng(2025).uniform(-1, 1, (len(rp) - 1, 4))
     mg = orc.MG(levels, pre=(orc.SM_JACOBI, 2, 0.99), post=(orc.SM_JACOBI, 2, 0.99))
     xo, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg, 200, 0.0, 1e-8)
-    x, itr, h = reference_loops.krylov(libs["contract"], "PBiCGStab", levels, B, smoother="Jacobi", sweeps=2)
+    x, itr, h = reference_loops.solver(libs["contract"], "PBiCGStab", rp, ci, v, B, levels=levels, max_iters=200,
+                                       smoother="Jacobi", sweeps=2)
     assert itr == it and it > 0
     assert np.array_equal(h, hist)
     assert np.array_equal(x, xo)
@@ -411,7 +414,8 @@ def test_amg_pbicgstab_f_and_w_cycles_match_reference_loops(libs, seq_dot, cycle
     B = np.random.default_rng(2026).uniform(-1, 1, (len(rp) - 1, 4))
     mg = orc.MG(levels, cycle={"F": 1, "W": 2}[cycle])
     xo, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg, 200, 0.0, 1e-8)
-    x, itr, h = reference_loops.krylov(libs["contract"], "PBiCGStab", levels, B, cycle=cycle)
+    x, itr, h = reference_loops.solver(libs["contract"], "PBiCGStab", rp, ci, v, B, levels=levels, max_iters=200,
+                                       cycle=cycle)
     assert itr == it and it > 0
     assert np.array_equal(h, hist)
     assert np.array_equal(x, xo)
@@ -432,7 +436,8 @@ def test_amg_pbicgstab_reduced_precision_matches_reference_loops(libs, seq_dot, 
     B = np.random.default_rng(2027).uniform(-1, 1, (len(rp) - 1, 4))
     mg = orc.MG(levels, cycle={"V": 0, "W": 2}[cycle], reduced=True)
     xo, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg, 200, 0.0, 1e-8)
-    x, itr, h = reference_loops.krylov(libs["contract"], "PBiCGStab", levels, B, cycle=cycle, reduced=True)
+    x, itr, h = reference_loops.solver(libs["contract"], "PBiCGStab", rp, ci, v, B, levels=levels, max_iters=200,
+                                       cycle=cycle, reduced=True)
     assert itr == it and it > 0
     assert np.array_equal(h, hist)
     assert np.array_equal(x, xo)
