@@ -70,7 +70,7 @@ def build():
         todo[kind] = []
         for name, flags in (("rows", rows_flags), ("smooth", rows_flags), ("vec", vec_flags),
                             ("gen", GENERIC), ("io", GENERIC), ("cheb", vec_flags),
-                            ("krylov", vec_flags)):
+                            ("krylov", vec_flags), ("mg", rows_flags)):
             obj = os.path.join(OUT, "ref_%s_%s.o" % (name, kind))
             # XAMG renamed per unit: no template instance is shared between units;
             # ref_loops/stub comes first so that its xamg_types.h stands in

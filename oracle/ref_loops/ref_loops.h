@@ -83,6 +83,7 @@ int ref_chebyshev_d(int64_t n, const int *rp, const int *ci, const double *v, co
 // src/primitives/matrix/operations/inverse.inl:31-106 (the coarse-grid
 // Direct solver's setup)
 int ref_dense_inverse_d(int64_t n, const double *a, double *ainv);
+int ref_dense_inverse_f(int64_t n, const float *a, float *ainv);
 
 // The multigrid preconditioner of the solver classes: one cycle of the
 // reference's loops in its MG_cycle order (mg.inl:186-280) over a hierarchy
@@ -102,11 +103,23 @@ void *ref_hier_create(int nlev, const int64_t *nrows, const int *const *arp, con
 int ref_hier_apply_d(void *h, const double *b, double *x, int nv);
 void ref_hier_destroy(void *h);
 
+// The reference's MultiGrid class (mg.inl) with its HSGS / Jacobi smoother
+// classes (hsgs.inl, jacobi.inl), compiled unchanged (mg.cpp), over a
+// hierarchy given as for ref_hier_create; applied as MultiGrid::solve with
+// max_iters 1 (the preconditioner role) from the x given.
+void *ref_mg_create(int nv, int nlev, const int64_t *nrows, const int *const *arp, const int *const *aci,
+                    const double *const *av, const int *const *prp, const int *const *pci, const double *const *pv,
+                    const int *const *rrp, const int *const *rci, const double *const *rv, const int *nb,
+                    const int64_t *const *bp, double relax, int pre_it, int post_it, int smoother);
+int ref_mg_apply_d(void *h, const double *b, double *x);
+void ref_mg_destroy(void *h);
+
 // The reference's own solver classes compiled unchanged (krylov.cpp):
 // method 0 BiCGStab (bicgstab.inl), 1 PBiCGStab (pbicgstab.inl), 2 PCG
 // (pcg.inl), 3 RBiCGStab (rbicgstab.inl), 4 MergedBiCGStab, 5
 // MergedPBiCGStab (merged/*.inl); the preconditioned ones use hier (from
-// ref_hier_create; PCG and RBiCGStab the identity when hier is null), from
+// ref_hier_create, or from ref_mg_create when method has bit 4 (16) set;
+// PCG and RBiCGStab the identity when hier is null), from
 // x = 0, to max(abs_tol, rel_tol * initial residual) per column.  hist
 // receives the (iterations + 1) x nv squared residual norms the solver
 // checks; returns the iteration count (-1 on bad input).

@@ -30,6 +30,8 @@
 #include <cstdlib>
 #include <limits>
 #include <map>
+#include <memory>
+#include <string>
 #include <typeinfo>
 #include <vector>
 
@@ -65,6 +67,8 @@ enum sharing { NODE, NUMA, NUMA_NODE, CORE };
 namespace segment {
 enum hierarchy { NODE, NUMA, CORE };
 }  // namespace segment
+
+enum multigrid_cycle { V_cycle = 0, F_cycle = 1, W_cycle = 2 };  // xamg_types.h:84
 
 // Performance counters: counted by the reference, ignored here.
 struct perf_info {
@@ -116,6 +120,8 @@ struct vector {
 
     vector() = default;
     explicit vector(mem::sharing m) : sharing_mode(m) {}
+    explicit vector(mem::allocation) {}
+    template <typename P> void set_part(const P &) {}
     // a copy of a vector that owns its storage views its own copy of it
     vector(const vector &o) { *this = o; }
     vector &operator=(const vector &o) {
@@ -223,7 +229,9 @@ template <typename F> struct dense_matrix {
 // operations/inverse.inl names (that routine itself is never instantiated
 // here; its single-process core, the dense Gauss-Jordan inverse, is).
 enum segmentation_type { SEGMENT_BY_BLOCKS, SEGMENT_BY_SLICES };
-struct part_layer {};
+struct part_layer {
+    std::vector<uint32_t> block_size = std::vector<uint32_t>(1, 0);
+};
 struct partitioning {
     part_layer node_layer, numa_layer;
 };
@@ -232,14 +240,18 @@ struct matrix_block {
     bool reduced_prec = false;
     template <typename M> void assemble(M &, int) {}
     void get_inv_sqrt_diag() {}
+    void get_inv_diag() {}
 };
 struct matrix_layer {
     matrix_block diag;
     std::vector<matrix_block> offd;
 };
 struct matrix_info_stub {
-    void print(const char *) const {}
+    void print(const std::string &, bool = false) const {}
+    void print_header() const {}
+    void print_footer() const {}
 };
+
 // One process's operator for the solver classes: a CSR block over caller
 // arrays (the type-erased products of blas2.h reduce to one csr_Ax_y here),
 // its spectrum bounds and D^{-1/2}.
@@ -250,13 +262,26 @@ struct matrix {
     partitioning *row_part = nullptr;
     float64_t min_eig = 0, max_eig = 0;
     matrix_info_stub info;
-    int64_t n = 0;
+    int64_t n = 0, ncols = 0;
     const int *rp = nullptr, *ci = nullptr;
     const double *v = nullptr;
-    vector::vector isd;
+    std::vector<float> v32;   // FP32 values (reduced levels)
+    vector::vector isd, invd;
+    int nb = 1;               // hybrid Gauss-Seidel blocks (one per core)
+    std::vector<int64_t> bp;  // their row offsets
     void set_part(partitioning *p) { row_part = p; }
     void add_data_layer(segment::hierarchy h) { data_layer[h]; }
     const vector::vector &inv_sqrt_diag() const { return isd; }
+    const vector::vector &inv_diag() const { return invd; }
+    template <typename F> void construct_core_layer() {}
+};
+// mg_layer (matrix.h:447-461): a level's operators and work vectors
+struct mg_layer {
+    matrix A, R, P;
+    std::vector<vector::vector> buffer;
+    matrix &get_A() { return A; }
+    matrix &get_R() { return R; }
+    matrix &get_P() { return P; }
 };
 
 }  // namespace matrix

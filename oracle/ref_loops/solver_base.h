@@ -21,6 +21,23 @@ struct param_list {
     std::map<std::string, double> v;
     int64_t get_int(const std::string &k) const { return (int64_t)v.at(k); }
     float64_t get_float(const std::string &k) const { return v.at(k); }
+    bool get_bool(const std::string &k) const { return v.count(k) && v.at(k) != 0; }
+};
+// the solver tree's parameter sets: only looked up by setup code that the
+// checks never run
+struct global_param_list {
+    param_list l;
+    bool find(const std::string &) const { return false; }
+    const param_list &get(const std::string &, int = -1) const { return l; }
+    template <typename T>
+    const param_list &get_if(const std::map<std::string, T> &, std::string &) const { return l; }
+};
+struct xamg_overrides_holder {
+    param_list l;
+    explicit xamg_overrides_holder(size_t) {}
+    void fill_in(const param_list &) {}
+    bool find(size_t) const { return false; }
+    const param_list &get(size_t) const { return l; }
 };
 }  // namespace params
 namespace mpi {
@@ -59,18 +76,72 @@ void Ax_y(matrix::matrix &A, const vector::vector &x, vector::vector &y, uint16_
         blas::set_const<F, NV>(y, 0.0, true);
         return;
     }
-    ref_csr_ax_y_d(A.n, A.rp, A.ci, A.v, x.get_aligned_ptr<double>(), y.get_aligned_ptr<double>(), NV);
+    if (sizeof(F) == sizeof(float))
+        ref_csr_ax_y_f(A.n, A.rp, A.ci, A.v32.data(), x.get_aligned_ptr<float>(), y.get_aligned_ptr<float>(), NV);
+    else
+        ref_csr_ax_y_d(A.n, A.rp, A.ci, A.v, x.get_aligned_ptr<double>(), y.get_aligned_ptr<double>(), NV);
     y.if_initialized = true;
     y.if_zero = false;
 }
+// y += A x (blas2.h:283-303 reduces to csr_Axpy)
+template <typename F, uint16_t NV>
+void Axpy(matrix::matrix &A, const vector::vector &x, vector::vector &y, uint16_t) {
+    if (x.if_zero) return;  // csr_matvec.inl:40-42
+    if (sizeof(F) == sizeof(float))
+        ref_csr_axpy_f(A.n, A.rp, A.ci, A.v32.data(), x.get_aligned_ptr<float>(), y.get_aligned_ptr<float>(), NV);
+    else
+        ref_csr_axpy_d(A.n, A.rp, A.ci, A.v, x.get_aligned_ptr<double>(), y.get_aligned_ptr<double>(), NV);
+    y.if_zero = false;
+}
+// blas2::SGS (blas2.h:184-281) on one process with the operator's hybrid
+// blocks as its cores: ref_hsgs_* (t from the incoming x, then csr_SGS per
+// block); a flagged-zero x is zeroed first, as blas2.h:264-265 does before
+// the sweep (its off-block products of a zero x add nothing to t)
+template <typename F, uint16_t NV>
+void SGS(matrix::matrix &A, const vector::vector &b, vector::vector &x, vector::vector &, const vector::vector &relax,
+         uint16_t) {
+    if (x.if_zero) blas::set_const<F, NV>(x, 0.0, true);
+    if (sizeof(F) == sizeof(float))
+        ref_hsgs_f(A.n, A.rp, A.ci, A.v32.data(), A.invd.get_aligned_ptr<float>(), b.get_aligned_ptr<float>(),
+                   x.get_aligned_ptr<float>(), relax.get_aligned_ptr<float>(), NV, A.nb, A.bp.data());
+    else
+        ref_hsgs_d(A.n, A.rp, A.ci, A.v, A.invd.get_aligned_ptr<double>(), b.get_aligned_ptr<double>(),
+                   x.get_aligned_ptr<double>(), relax.get_aligned_ptr<double>(), NV, A.nb, A.bp.data());
+    x.if_zero = false;
+}
 }  // namespace blas2
 namespace solver {
-// what a solver sees of its preconditioner
+// what a solver sees of its preconditioner and smoothers (solver.h:77-103)
 struct base_solver_interface {
     virtual ~base_solver_interface() {}
     virtual void solve(vector::vector &, const vector::vector &, mpi::token & = mpi::null_token) {}
+    virtual void solve(vector::vector &x, const vector::vector &b, const vector::vector &,
+                       mpi::token &tok = mpi::null_token) {
+        solve(x, b, tok);
+    }
     virtual void matrix_info() {}
+    virtual void setup(const params::global_param_list &) {}
+    virtual void renew_params(const params::global_param_list &, bool = true) {}
+    virtual void renew_param_list(const params::param_list &) {}
 };
+// the solver factory and the hypre hierarchy import, named by
+// MultiGrid::setup (which the checks never run: they hand the class its
+// hierarchy and solvers)
+template <typename F, uint16_t NV>
+std::shared_ptr<base_solver_interface> construct_basic_solver(const params::global_param_list &,
+                                                              const params::param_list &, matrix::matrix &,
+                                                              const std::string & = "solver") {
+    return nullptr;
+}
+}  // namespace solver
+namespace hypre {
+template <typename F>
+void get_full_hierarchy(matrix::matrix &, std::vector<matrix::mg_layer> &, const params::global_param_list &) {}
+template <typename F>
+void get_per_level_hierarchy(matrix::matrix &, std::vector<matrix::mg_layer> &,
+                             const params::global_param_list &) {}
+}  // namespace hypre
+namespace solver {
 template <typename F, uint16_t NV> struct base_solver;
 // one process: the allreduce of a local value is the value itself
 struct allreduce_stub {
@@ -99,8 +170,12 @@ template <typename F, uint16_t NV> struct stats_stub {
             for (int k = 0; k < NV; ++k) st->res0[k] = r.get_aligned_ptr<F>()[k];
         }
     } convergence_status{this};
-    void init(vector::vector &) {}
-    void init(vector::vector &, vector::vector &iconv) { p_iconv = &iconv; }
+    // stats.h:90-99: every solve starts its iteration count afresh
+    void init(vector::vector &) { iters = 0; }
+    void init(vector::vector &, vector::vector &iconv) {
+        iters = 0;
+        p_iconv = &iconv;
+    }
     int increment_iters_counter() { return ++iters; }
     bool check_and_record(const vector::vector &r) {
         if (!conv_check) return false;
@@ -139,7 +214,10 @@ template <typename F, uint16_t NV> struct stats_stub {
         return check_and_record(t);
     }
     bool is_converged_simple(vector::vector &r_norm) { return check_and_record(r_norm); }
+    // the smoothers' and the preconditioner's own checks: off in those roles
+    bool is_converged_initial() { return false; }
     bool is_converged() { return false; }
+    bool is_converged(vector::vector &) { return false; }
     void print_residuals_footer() {}
 };
 template <typename F, uint16_t NV> struct base_solver : base_solver_interface {
@@ -178,6 +256,17 @@ template <typename F, uint16_t NV> struct base_solver : base_solver_interface {
     virtual void init(const params::param_list &, const std::string &) {}
     virtual void solve(const vector::vector &conv, mpi::token &tok = mpi::null_token) = 0;
     virtual void matrix_info() = 0;
+    // solver.h:227-245: point at x and b, then the class's own solve
+    void solve(vector::vector &x_, const vector::vector &b_, const vector::vector &conv,
+               mpi::token &tok = mpi::null_token) override {
+        x = &x_;
+        b = &b_;
+        if (buffer.empty()) {
+            buffer.resize(buffer_nvecs);
+            for (auto &v : buffer) v.template alloc<F>(x_.size, NV);
+        }
+        solve(conv, tok);
+    }
     using base_solver_interface::solve;
 };
 }  // namespace solver

@@ -223,6 +223,15 @@ int ref_ax_y_d(int64_t n, int nv, const double *a, const double *x, double *y) {
 int ref_scal_d(int64_t n, int nv, const double *a, double *y) {
     return run_blas(Blas{6, n, nv, a, nullptr, nullptr, nullptr, nullptr, y});
 }
+int ref_dense_inverse_f(int64_t n, const float *a, float *ainv) {
+    XAMG::matrix::dense_matrix<float> m(XAMG::mem::CORE), mi(XAMG::mem::CORE);
+    m.nrows = m.block_nrows = (uint64_t)n;
+    m.ncols = m.block_ncols = (uint64_t)n;
+    m.val = block(a, n * n, 1);
+    XAMG::matrix::inverse<float>(m, mi);
+    std::memcpy(ainv, mi.val.get_aligned_ptr<float>(), sizeof(float) * (size_t)(n * n));
+    return 0;
+}
 int ref_dense_inverse_d(int64_t n, const double *a, double *ainv) {
     XAMG::matrix::dense_matrix<double> m(XAMG::mem::CORE), mi(XAMG::mem::CORE);
     m.nrows = m.block_nrows = (uint64_t)n;

@@ -53,6 +53,10 @@ def lib(kind, build=True):
     L.ref_hier_create.argtypes = [ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, ci_]
     L.ref_hier_apply_d.argtypes = [vp, vp, vp, ci_]
     L.ref_hier_destroy.argtypes = [vp]
+    L.ref_mg_create.restype = vp
+    L.ref_mg_create.argtypes = [ci_, ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, ci_]
+    L.ref_mg_apply_d.argtypes = [vp, vp, vp]
+    L.ref_mg_destroy.argtypes = [vp]
     L.ref_solver_d.argtypes = [ci_, vp, i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, vp, ci_]
     L.ref_chebyshev_d.argtypes = [i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, cd]
     L.ref_channel_cube_d.restype = C.c_int64
@@ -149,12 +153,13 @@ SOLVERS = {"BiCGStab": 0, "PBiCGStab": 1, "PCG": 2, "RBiCGStab": 3, "MergedBiCGS
 
 
 def solver(L, method, rp, ci, v, B, levels=None, max_iters=1000, rel_tol=1e-8, relax=0.99, cycle="V",
-           smoother="HSGS", sweeps=1, reduced=False, blocks=None):
+           smoother="HSGS", sweeps=1, reduced=False, blocks=None, mg_class=True):
     """The reference's own solver class `method` (one of SOLVERS, compiled
     unchanged) from x = 0 on (rp, ci, v).  With `levels` (dicts with n, A, P,
     ncP as the oracle's setup or the library's hierarchy export gives them)
-    the preconditioned methods apply one multigrid cycle of the reference's
-    loops in its MG_cycle order: `cycle` "V", "F" or "W", `smoother` "HSGS"
+    the preconditioned methods apply the reference's MultiGrid class with
+    its HSGS / Jacobi smoother classes (mg_class; else the cycle restated
+    over its loops): `cycle` "V", "F" or "W", `smoother` "HSGS"
     (on the hybrid blocks `blocks[l]`, default one block per level) or
     "Jacobi" with `sweeps` before and after, `reduced` for
     mg_reduced_precision (FP32 below the first level, HSGS only).  Without
@@ -167,15 +172,18 @@ def solver(L, method, rp, ci, v, B, levels=None, max_iters=1000, rel_tol=1e-8, r
     if levels is not None:
         nrows, cast, nb, keep = _hier_args(levels, blocks)
         code = {"HSGS": 0, "Jacobi": 1}[smoother] | ({"V": 0, "F": 1, "W": 2}[cycle] << 4) | (int(reduced) << 8)
-        h = L.ref_hier_create(len(levels), p(nrows), *cast[:9], p(nb), cast[9], relax, sweeps, sweeps, code)
+        if mg_class:
+            h = L.ref_mg_create(nv, len(levels), p(nrows), *cast[:9], p(nb), cast[9], relax, sweeps, sweeps, code)
+        else:
+            h = L.ref_hier_create(len(levels), p(nrows), *cast[:9], p(nb), cast[9], relax, sweeps, sweeps, code)
     try:
         x = np.zeros_like(B)
         hist = np.zeros((max_iters + 2, nv))
-        it = L.ref_solver_d(SOLVERS[method], h, n, p(rp), p(ci), p(v), p(B), p(x), nv, max_iters, 0.0, rel_tol,
-                            p(hist), max_iters + 2)
+        it = L.ref_solver_d(SOLVERS[method] | (16 if (mg_class and h) else 0), h, n, p(rp), p(ci), p(v), p(B),
+                            p(x), nv, max_iters, 0.0, rel_tol, p(hist), max_iters + 2)
     finally:
         if h:
-            L.ref_hier_destroy(h)
+            (L.ref_mg_destroy if mg_class else L.ref_hier_destroy)(h)
     if it < 0:
         raise ValueError("unsupported nv or method")
     return x, it, hist[: it + 1]

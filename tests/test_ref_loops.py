@@ -407,7 +407,10 @@ def test_amg_pbicgstab_f_and_w_cycles_match_reference_loops(libs, seq_dot, cycle
     """F- and W-cycle preconditioning (mg_cycle 1 and 2 of mg.inl:186-280: the
     F-cycle skips pre-smoothing on its level and follows its coarse F-cycle
     with a V-cycle, the W-cycle recurses twice) in AMG-PBiCGStab, 27-point
-    16^3, NV = 4: bit for bit against the oracle's cycles."""
+    16^3, NV = 4: bit for bit against the oracle's cycles; W through the
+    reference's MultiGrid class itself, F through the cycle restated over its
+    loops (the class's F-cycle reuses stale coarse vectors, see the next
+    test)."""
     rp, ci, v = orc.gen27(16)
     levels = orc.amg_setup(rp, ci, v, mg_coarsening_type=10, mg_interpolation_type=6,
                            mg_strength_threshold=0.25, mg_max_levels=6, mg_coarse_matrix_size=100)
@@ -415,7 +418,7 @@ def test_amg_pbicgstab_f_and_w_cycles_match_reference_loops(libs, seq_dot, cycle
     mg = orc.MG(levels, cycle={"F": 1, "W": 2}[cycle])
     xo, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg, 200, 0.0, 1e-8)
     x, itr, h = reference_loops.solver(libs["contract"], "PBiCGStab", rp, ci, v, B, levels=levels, max_iters=200,
-                                       cycle=cycle)
+                                       cycle=cycle, mg_class=(cycle == "W"))
     assert itr == it and it > 0
     assert np.array_equal(h, hist)
     assert np.array_equal(x, xo)
@@ -504,3 +507,31 @@ def test_reference_preconditioned_solver_classes_match_oracle(libs, seq_dot, met
     assert itr == it and it > 0
     assert np.array_equal(h, hist)
     assert np.array_equal(x, xo)
+
+
+def test_reference_f_cycle_reuses_stale_coarse_vectors(libs):
+    """The reference's MultiGrid class with mg_cycle = F: its first application
+    equals the F-cycle of the oracle and of the restated cycle, the second does
+    not.  MG_cycle clears the coarse vector x_H by flag only
+    (set_const without force, mg.inl:226), an F-cycle skips the pre-smoother
+    that would clear it (mg.inl:218), and csr_Axpy adds the prolongated
+    correction into its previous contents (csr_matvec.inl:32-144), so from the
+    second application on the coarse levels start from the last cycle's x_H.
+    The oracle and the library start every coarse level from zero."""
+    rp, ci, v = orc.gen27(12)
+    levels = orc.amg_setup(rp, ci, v, mg_coarsening_type=10, mg_interpolation_type=6,
+                           mg_strength_threshold=0.25, mg_max_levels=4, mg_coarse_matrix_size=10)
+    b = np.random.default_rng(1).uniform(-1, 1, (len(rp) - 1, 1))
+    L = libs["contract"]
+    nrows, cast, nb, keep = reference_loops._hier_args(levels, None)
+    h = L.ref_mg_create(1, len(levels), p(nrows), *cast[:9], p(nb), cast[9], 0.99, 1, 1, 1 << 4)
+    try:
+        mg = orc.MG(levels, cycle=1)
+        expect = mg.apply(b)
+        first, second = np.zeros_like(b), np.zeros_like(b)
+        L.ref_mg_apply_d(h, p(b), p(first))
+        L.ref_mg_apply_d(h, p(b), p(second))
+    finally:
+        L.ref_mg_destroy(h)
+    assert np.array_equal(first, expect)
+    assert not np.array_equal(second, expect)
