@@ -731,10 +731,10 @@ def ref_loops(kind):
 
 
 def ref_sample(csr, B, levels, kind, iters=1):
-    """`iters` FP64 AMG-PBiCGStab iterations of the reference's own PBiCGStab
-    class and loops, compiled unchanged (one process: Gauss-Seidel in its
-    single-process order, inner products in its single-core order), on the
-    GPU plain form's hierarchy.  Returns (seconds, x, history) or None when
+    """`iters` FP64 AMG-PBiCGStab iterations of the reference's own PBiCGStab,
+    MultiGrid and HSGS classes and loops, compiled unchanged (one process:
+    Gauss-Seidel in its single-process order, inner products in its
+    single-core order), on the GPU plain form's hierarchy.  Returns (seconds, x, history) or None when
     the library is absent."""
     L = ref_loops(kind)
     if L is None:
@@ -786,8 +786,8 @@ def reference_arm(args, rank, world):
                                              rel_tol=1e-8)
         st = (np.sqrt(hist[-1]) <= 1e-8 * np.sqrt(hist[0])).astype(np.int32)
         thr, kind = 1, "reference"
-        what = ("the reference's own PBiCGStab class and loop files (blas, blas2, inverse) compiled unchanged "
-                "with its release flags, V-cycle in its step order, one process")
+        what = ("the reference's own PBiCGStab, MultiGrid and HSGS classes and loop files compiled unchanged "
+                "with its release flags, one process")
     else:
         mg = orc.MG(levels)
         x, it, hist, st, _ = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg=mg, max_iters=200, rel_tol=1e-8)
@@ -1034,8 +1034,8 @@ def main():
         if rs is not None:
             cpu = {"value": round(rs[0] * iters / NV * 1e3, 3), "unit": "ms/RHS", "cores": 1, "kind": "reference",
                    "sample": "1 FP64 AMG-PBiCGStab iteration of the same problem and hierarchy by the reference's "
-                             "own PBiCGStab class and loop files compiled unchanged with its release flags, one "
-                             "process (%.1f s), "
+                             "own PBiCGStab, MultiGrid and HSGS classes and loop files compiled unchanged with its "
+                             "release flags, one process (%.1f s), "
                              "x %d iterations / %d RHS" % (rs[0], iters, NV),
                    "oracle_port": {"value": round(sec * iters / NV * 1e3, 3), "cores": thr}}
         # full-size parity with the reference's own arithmetic: the GPU's first
