@@ -35,9 +35,26 @@ struct Coarse : XAMG::solver::base_solver_interface {
     }
 };
 
+// The Chebyshev smoother class, compiled in its own unit with the BLAS
+// flags (cheb.cpp: its vector updates round apart, as the oracle's), called
+// as a smoother of this cycle; a flag-cleared x is zeroed first
+struct ChebSmoother : XAMG::solver::base_solver_interface {
+    matrix *A;
+    int nv, order;
+    double fraction;
+    void solve(vector &x, const vector &b, XAMG::mpi::token & = XAMG::mpi::null_token) override {
+        if (x.if_zero) std::memset(x.get_aligned_ptr<double>(), 0, sizeof(double) * x.size * nv);
+        ref_chebyshev_d(A->n, A->rp, A->ci, A->v, b.get_aligned_ptr<double>(), x.get_aligned_ptr<double>(), nv,
+                        order, fraction, A->min_eig, A->max_eig);
+        x.if_initialized = true;
+        x.if_zero = false;
+    }
+};
+
 struct MGBase {
     virtual ~MGBase() {}
     virtual void apply(const double *b, double *x) = 0;
+    virtual void set_chebyshev(int order, double fraction, const double *min_eig, const double *max_eig) = 0;
 };
 
 template <int NV> struct MGImpl : MGBase {
@@ -158,6 +175,27 @@ template <int NV> struct MGImpl : MGBase {
         return s;
     }
 
+    // Chebyshev smoothers on every level but the coarsest (FP64 levels),
+    // with the given spectrum bounds of D^-1/2 A D^-1/2 per level
+    void set_chebyshev(int order, double fraction, const double *min_eig, const double *max_eig) override {
+        const int nlev = (int)mg.mg_tree.size();
+        mg.pre_smooth.clear();
+        mg.post_smooth.clear();
+        for (int l = 0; l + 1 < nlev; ++l) {
+            matrix &A = mg.mg_tree[l].get_A();
+            A.min_eig = min_eig[l];
+            A.max_eig = max_eig[l];
+            for (int role = 0; role < 2; ++role) {
+                auto c = std::make_shared<ChebSmoother>();
+                c->A = &A;
+                c->nv = NV;
+                c->order = order;
+                c->fraction = fraction;
+                (role ? mg.post_smooth : mg.pre_smooth).push_back(c);
+            }
+        }
+    }
+
     void apply(const double *b, double *x) override {
         const int64_t n = mg.mg_tree[0].get_A().n;
         vector X = block(x, n, NV), B = block(b, n, NV);
@@ -200,4 +238,7 @@ int ref_mg_apply_d(void *h, const double *b, double *x) {
     return 0;
 }
 void ref_mg_destroy(void *h) { delete (MGBase *)h; }
+void ref_mg_set_chebyshev(void *h, int order, double fraction, const double *min_eig, const double *max_eig) {
+    ((MGBase *)h)->set_chebyshev(order, fraction, min_eig, max_eig);
+}
 }

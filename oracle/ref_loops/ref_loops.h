@@ -113,6 +113,9 @@ void *ref_mg_create(int nv, int nlev, const int64_t *nrows, const int *const *ar
                     const int64_t *const *bp, double relax, int pre_it, int post_it, int smoother);
 int ref_mg_apply_d(void *h, const double *b, double *x);
 void ref_mg_destroy(void *h);
+// Chebyshev smoothing (chebyshev.inl, order and spectrum_fraction, the given
+// spectrum bounds per level) in place of the object's smoothers.
+void ref_mg_set_chebyshev(void *h, int order, double fraction, const double *min_eig, const double *max_eig);
 
 // The reference's own solver classes compiled unchanged (krylov.cpp):
 // method 0 BiCGStab (bicgstab.inl), 1 PBiCGStab (pbicgstab.inl), 2 PCG

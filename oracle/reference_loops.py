@@ -57,6 +57,7 @@ def lib(kind, build=True):
     L.ref_mg_create.argtypes = [ci_, ci_, vp, PP, PP, PP, PP, PP, PP, PP, PP, PP, vp, PP, cd, ci_, ci_, ci_]
     L.ref_mg_apply_d.argtypes = [vp, vp, vp]
     L.ref_mg_destroy.argtypes = [vp]
+    L.ref_mg_set_chebyshev.argtypes = [vp, ci_, cd, vp, vp]
     L.ref_solver_d.argtypes = [ci_, vp, i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, vp, ci_]
     L.ref_chebyshev_d.argtypes = [i64, vp, vp, vp, vp, vp, ci_, ci_, cd, cd, cd]
     L.ref_channel_cube_d.restype = C.c_int64
@@ -153,7 +154,7 @@ SOLVERS = {"BiCGStab": 0, "PBiCGStab": 1, "PCG": 2, "RBiCGStab": 3, "MergedBiCGS
 
 
 def solver(L, method, rp, ci, v, B, levels=None, max_iters=1000, rel_tol=1e-8, relax=0.99, cycle="V",
-           smoother="HSGS", sweeps=1, reduced=False, blocks=None, mg_class=True):
+           smoother="HSGS", sweeps=1, reduced=False, blocks=None, mg_class=True, cheb=None):
     """The reference's own solver class `method` (one of SOLVERS, compiled
     unchanged) from x = 0 on (rp, ci, v).  With `levels` (dicts with n, A, P,
     ncP as the oracle's setup or the library's hierarchy export gives them)
@@ -174,6 +175,10 @@ def solver(L, method, rp, ci, v, B, levels=None, max_iters=1000, rel_tol=1e-8, r
         code = {"HSGS": 0, "Jacobi": 1}[smoother] | ({"V": 0, "F": 1, "W": 2}[cycle] << 4) | (int(reduced) << 8)
         if mg_class:
             h = L.ref_mg_create(nv, len(levels), p(nrows), *cast[:9], p(nb), cast[9], relax, sweeps, sweeps, code)
+            if cheb is not None:  # (order, spectrum_fraction, [(min_eig, max_eig) per level])
+                mn = np.array([e[0] for e in cheb[2]], np.float64)
+                mx = np.array([e[1] for e in cheb[2]], np.float64)
+                L.ref_mg_set_chebyshev(h, int(cheb[0]), float(cheb[1]), p(mn), p(mx))
         else:
             h = L.ref_hier_create(len(levels), p(nrows), *cast[:9], p(nb), cast[9], relax, sweeps, sweeps, code)
     try:

@@ -535,3 +535,23 @@ def test_reference_f_cycle_reuses_stale_coarse_vectors(libs):
         L.ref_mg_destroy(h)
     assert np.array_equal(first, expect)
     assert not np.array_equal(second, expect)
+
+
+@pytest.mark.parametrize("order", [2, 3])
+def test_amg_pbicgstab_chebyshev_smoothing_matches_reference_classes(libs, seq_dot, order):
+    """AMG-PBiCGStab with Chebyshev smoothing: the reference's PBiCGStab,
+    MultiGrid and Chebyshev classes against the oracle with the same spectrum
+    bounds per level (27-point 16^3, NV = 4), bit for bit."""
+    rp, ci, v = orc.gen27(16)
+    levels = orc.amg_setup(rp, ci, v, mg_coarsening_type=10, mg_interpolation_type=6,
+                           mg_strength_threshold=0.25, mg_max_levels=6, mg_coarse_matrix_size=100)
+    B = np.random.default_rng(2028).uniform(-1, 1, (len(rp) - 1, 4))
+    eig = [(0.02 + 0.01 * l, 1.9 - 0.05 * l) for l in range(len(levels))]
+    cheb = (order, 0.3, eig)
+    mg = orc.MG(levels, pre=(orc.SM_CHEB, 1, 0.99), post=(orc.SM_CHEB, 1, 0.99), cheb=cheb)
+    xo, it, hist, st, r0 = orc.pbicgstab(rp, ci, v, B, np.zeros_like(B), mg, 200, 0.0, 1e-8)
+    x, itr, h = reference_loops.solver(libs["contract"], "PBiCGStab", rp, ci, v, B, levels=levels, max_iters=200,
+                                       cheb=cheb)
+    assert itr == it and it > 0
+    assert np.array_equal(h, hist)
+    assert np.array_equal(x, xo)
